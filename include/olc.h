@@ -1,0 +1,245 @@
+/*
+ * olc.h — C ABI of libolc.so, the B200 (sm_100a) implementation of one
+ * Oncolytica simulation step.
+ *
+ * The reference's boundary for this path is the backend protocol
+ * ISimulationBackend (framework/src/oncolytica/core/runtime/_backend.py:7-36):
+ *   compile(sim), run_step(collect_metrics), sync_to_host(), sync_to_device(),
+ *   get_metrics().
+ * Its GPU implementation (framework/src/oncolytica/gpu/runtime/_gpu_backend.py)
+ * drives wgpu directly.  Here the Python backend class
+ * oncolytica_b200.backend.CudaBackend implements that protocol and calls the
+ * entry points below through ctypes; any other host language binds the same
+ * symbols.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: OLC_OK (0) or an OLC_ERR_* code.
+ *     A per-handle message is available from olc_last_error(); stateless entry
+ *     points report through olc_last_error(NULL).  No C++ exception crosses
+ *     the ABI.
+ *   - Pointers named *_dev are device pointers owned by the caller (the Python
+ *     backend allocates them with torch).  The library borrows them and never
+ *     frees them.  The library owns only its scratch (sort temporaries,
+ *     histograms, look-back words, bin table, status word), sized in
+ *     olc_create() and released by olc_destroy().
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream).  Calls on one handle must not run concurrently.
+ *   - Device-side non-fatal conditions (capacity overflow, a bounded wait that
+ *     gave up) set bits in a status word that olc_read_counters() returns.
+ */
+#ifndef OLC_H
+#define OLC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OLC_OK            0
+#define OLC_ERR_ARG       1
+#define OLC_ERR_NVRTC     2
+#define OLC_ERR_CUDA      3
+#define OLC_ERR_CAPACITY  4
+#define OLC_ERR_TIMEOUT   5
+#define OLC_ERR_STATE     6
+
+/* Status-word bits (OlcCounters.status). */
+#define OLC_STATUS_CAPACITY     0x1u  /* births dropped: agent capacity reached */
+#define OLC_STATUS_TIMEOUT      0x2u  /* a bounded device wait gave up          */
+#define OLC_STATUS_MULTI_DIVIDE 0x4u  /* a rule called divide() twice in a call  */
+
+#define OLC_MAX_AGENT_FIELDS 64  /* 4-byte SoA columns per agent (vec3 = 3)   */
+#define OLC_MAX_FIELDS       8   /* diffusing chemistry fields                 */
+#define OLC_MAX_RULES        16  /* compiled rule kernels                      */
+#define OLC_RADIAL_BINS      64  /* radial histogram of live agents            */
+#define OLC_STATE_BINS       8   /* histogram of the designated state column   */
+
+typedef struct OlcSim OlcSim;
+
+/* Geometry.  The bin grid is the reference's tissue grid
+ * (framework/src/oncolytica/core/runtime/_engine.py:71-82): agents are binned
+ * by trunc(pos / tissue_voxel_size) and keyed by the hierarchical Morton key of
+ * framework/src/oncolytica/gpu/compiler/template.wgsl:100-132.  The chemistry
+ * grid holds the diffusing fields, row-major with x fastest; it may be decoupled
+ * from the bin grid (engine/assets/shaders/tumor_sim.wgsl:219-236 does the
+ * same). */
+typedef struct {
+    int32_t tissue_dims[3];
+    float   tissue_voxel_size;
+    int32_t chem_dims[3];
+    float   chem_voxel_size;
+    float   domain_lo[3];       /* agent positions are clamped into          */
+    float   domain_hi[3];       /* [lo + margin, hi - margin] by mechanics    */
+} OlcGeom;
+
+typedef struct {
+    uint32_t max_agents;        /* capacity of every agent column            */
+    uint32_t n_agent_fields;    /* bound 4-byte columns (pos.x/y/z are 0,1,2) */
+    uint32_t n_fields;          /* chemistry fields                           */
+    int32_t  state_field;       /* column holding an i32 state, or -1         */
+    float    radial_bin_width;  /* width of the radial histogram bins         */
+    float    center[3];         /* origin of radial statistics                */
+    float    dt;                /* step length (fields and contact)           */
+} OlcCaps;
+
+/* One diffusing field: explicit 7-point FTCS substeps with Dirichlet outer
+ * faces (engine/assets/shaders/tumor_sim.wgsl:414-446) and an implicit
+ * first-order sink (tumor_sim.wgsl:387-412). */
+typedef struct {
+    float   diffusion;          /* D, length^2 / time                        */
+    float   decay;              /* lambda, 1 / time (applied every substep)   */
+    float   boundary;           /* value pinned on the outer faces            */
+    int32_t substeps;           /* S >= 1, D*dt/S/dx^2 <= 1/6 is checked      */
+    int32_t has_sink;           /* rules deposit uptake rates into this field */
+} OlcDiffusion;
+
+/* Hertz-like contact repulsion (engine/assets/shaders/tumor_sim.wgsl:505-628):
+ * for d < r_i + r_j, F += k * delta^(3/2) * (p_i - p_j)/d with
+ * delta = r_i + r_j - d; overdamped displacement mobility * F * dt, capped at
+ * max_disp, then clamped into the domain. */
+typedef struct {
+    int32_t enabled;
+    int32_t radius_field;       /* agent column holding the radius, or -1    */
+    float   radius_const;       /* radius when radius_field < 0               */
+    float   stiffness;
+    float   mobility;
+    float   max_disp;
+    float   margin;
+} OlcContact;
+
+typedef struct {
+    uint32_t n_agents;          /* agents entering the next step              */
+    uint32_t n_total;           /* rows in use incl. this step's dead         */
+    uint32_t births;            /* births in the last step                    */
+    uint32_t deaths;            /* agents removed by the last sort            */
+    uint32_t status;            /* OLC_STATUS_* bits (sticky)                 */
+    uint32_t pad;
+    uint64_t steps;             /* steps run on this handle                   */
+} OlcCounters;
+
+/* Per-step reductions (engine metrics, tumor_sim.wgsl:248-361, restated as
+ * exact integer counts and FP64 sums). */
+typedef struct {
+    uint32_t n_live;
+    uint32_t state_counts[OLC_STATE_BINS];
+    uint32_t radial_hist[OLC_RADIAL_BINS];
+    uint32_t pad;
+    double   sum_pos[3];
+    double   sum_r2;            /* sum |p - center|^2                         */
+    double   max_r;
+    double   field_mass[OLC_MAX_FIELDS];   /* FP64 sum over the field grid   */
+    double   field_min[OLC_MAX_FIELDS];
+    double   field_max[OLC_MAX_FIELDS];
+} OlcReductions;
+
+/* ------------------------------------------------------------------ handle */
+
+/* Replaces GpuBackend.compile()'s buffer/pipeline creation
+ * (framework/src/oncolytica/gpu/runtime/_gpu_backend.py:79-104). */
+int olc_create(const OlcGeom* geom, const OlcCaps* caps, OlcSim** out);
+int olc_destroy(OlcSim* sim);
+const char* olc_last_error(const OlcSim* sim);
+const char* olc_version(void);
+
+/* Binds agent column `index` (4-byte elements, capacity max_agents) as a
+ * ping-pong pair.  Replaces the Cells_In/Cells_Out AoS buffers
+ * (framework/src/oncolytica/gpu/runtime/_device_manager.py:76-119). */
+int olc_bind_agent_column(OlcSim* sim, int index, void* a_dev, void* b_dev);
+
+/* Binds chemistry field `index` (float, chem_dims voxels) as a ping-pong pair
+ * plus an optional sink buffer (NULL when the field has no sink).  Replaces
+ * Chem_In/Chem_Out (_device_manager.py:76-119). */
+int olc_bind_field(OlcSim* sim, int index, float* a_dev, float* b_dev, float* sink_dev,
+                   const OlcDiffusion* spec);
+
+int olc_set_contact(OlcSim* sim, const OlcContact* spec);
+
+/* Compiles CUDA C emitted by the rule translator with NVRTC for sm_100a
+ * (replaces WGSLCompiler.compile + create_shader_module,
+ * framework/src/oncolytica/gpu/compiler/_compiler.py:233-352).  `kinds[i]` is
+ * 0 for a cell rule, 1 for a metric rule.  `include_dir` holds
+ * olc_device.cuh and olc_rule_rt.cuh. */
+int olc_set_rule_source(OlcSim* sim, const char* cuda_src, const char* const* kernels,
+                        const int* kinds, int n, const char* include_dir);
+
+/* Uploads the Params blob (replaces pack_uniforms, _device_manager.py:180-204;
+ * unlike the reference, later calls do reach the device). */
+int olc_set_params(OlcSim* sim, const void* blob, size_t bytes, void* stream);
+
+/* Sets the agent count after the host wrote agent columns into the current
+ * buffer (replaces sync_to_device, _gpu_backend.py:353-371). */
+int olc_set_agent_count(OlcSim* sim, uint32_t n, void* stream);
+
+/* Which of the pair (0 = a, 1 = b) currently holds agent / field state. */
+int olc_current_buffers(const OlcSim* sim, int* agent_buf, int* field_buf);
+
+/* Runs `nsteps` steps (replaces GpuBackend.run_step,
+ * framework/src/oncolytica/gpu/runtime/_gpu_backend.py:113-171).  Stage order:
+ * fields (sink, substeps) -> keys + stable radix sort + compaction + bin table ->
+ * cell rules -> contact -> reductions/metric rules (when collect != 0).
+ * No host synchronisation inside. */
+int olc_step(OlcSim* sim, int nsteps, int collect, void* stream);
+
+/* Synchronises `stream` and copies the counters. */
+int olc_read_counters(OlcSim* sim, OlcCounters* out, void* stream);
+
+/* Copies the last step's reductions / metric-rule accumulators to host memory
+ * (replaces the MetricsBuffer readback, _gpu_backend.py:166-169). */
+int olc_read_reductions(OlcSim* sim, OlcReductions* out, void* stream);
+int olc_read_user_metrics(OlcSim* sim, void* out, size_t bytes, void* stream);
+int olc_set_user_metrics_size(OlcSim* sim, size_t bytes);
+
+/* ---------------------------------------------------- stateless stages */
+/* These run one stage on caller buffers; the parity tests call them. */
+
+/* RNG known answers: for each of n states, `draws` xorshift32 draws
+ * (template.wgsl:75-82) written to out_dev[i*draws + k]; the final state is
+ * written back.  When dirs_dev != NULL, one _rand_dir (template.wgsl:84-98)
+ * per state follows and is stored as xyz triples. */
+int olc_stage_rng(uint32_t* states_dev, uint32_t n, int draws, float* out_dev,
+                  float* dirs_dev, void* stream);
+
+/* Bin keys (template.wgsl:174-186, Kernel_CountAndOffset's key): keys_dev[i] =
+ * tissue_key(clamp(trunc(pos / vs))); agents with dead_dev[i] != 0 get the
+ * sentinel tissue_key(tissue_dims) = voxel_table_size - 1 (the key that die()
+ * produces, framework/src/oncolytica/gpu/compiler/translator/_stmt_translator.py:431-440).
+ * dead_dev may be NULL. */
+int olc_stage_keys(const float* x_dev, const float* y_dev, const float* z_dev,
+                   const uint8_t* dead_dev, uint32_t n, const OlcGeom* geom,
+                   uint32_t* keys_dev, void* stream);
+
+/* Stable LSD radix sort of (key, value) pairs on the low `key_bits` bits
+ * (onesweep: one upfront digit histogram, then one decoupled-look-back pass
+ * per 8-bit digit).  Replaces the counting sort of template.wgsl:165-343.
+ * vals_in_dev == NULL means values 0..n-1.  Scratch is caller memory of at
+ * least olc_sort_scratch_bytes(n, key_bits) bytes, 256-byte aligned. */
+size_t olc_sort_scratch_bytes(uint32_t n, int key_bits);
+int olc_stage_sort_pairs(const uint32_t* keys_in_dev, const uint32_t* vals_in_dev,
+                         uint32_t* keys_out_dev, uint32_t* vals_out_dev, uint32_t n,
+                         int key_bits, void* scratch_dev, size_t scratch_bytes, void* stream);
+
+/* Bin table from sorted keys: ranges_dev[2k] = first index of key k,
+ * ranges_dev[2k+1] = one past the last (both 0 when empty); keys >= n_bins are
+ * ignored.  Replaces VoxelTable.startIndex/count (template.wgsl:42-45). */
+int olc_stage_bin_ranges(const uint32_t* sorted_keys_dev, uint32_t n, uint32_t n_bins,
+                         uint32_t* ranges_dev, void* stream);
+
+/* One step of one field: sink f <- f / (1 + K dt) then S substeps, result in
+ * f_dev (tmp_dev is a same-sized temporary; sink_dev may be NULL and is zeroed
+ * after use). */
+int olc_stage_diffuse(float* f_dev, float* tmp_dev, float* sink_dev, const int32_t dims[3],
+                      float dx, float dt, const OlcDiffusion* spec, void* stream);
+
+/* Contact pass over n sorted agents: posr_dev holds (x, y, z, radius) with
+ * radius < 0 marking a dead agent; writes the new positions. */
+int olc_stage_contact(const float* posr_dev, const uint32_t* ranges_dev, uint32_t n,
+                      const OlcGeom* geom, const OlcContact* spec, float dt,
+                      float* x_dev, float* y_dev, float* z_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OLC_H */

@@ -1,0 +1,188 @@
+"""ctypes binding of libolc.so (include/olc.h).
+
+The library is the only implementation of the step: there is no CPU path.  If
+it cannot be loaded, every entry point raises ``OlcError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libolc.so")
+CSRC_DIR = os.path.join(HERE, "csrc")
+
+OLC_OK = 0
+OLC_ERR_ARG = 1
+OLC_ERR_NVRTC = 2
+OLC_ERR_CUDA = 3
+OLC_ERR_CAPACITY = 4
+OLC_ERR_TIMEOUT = 5
+OLC_ERR_STATE = 6
+
+OLC_STATUS_CAPACITY = 0x1
+OLC_STATUS_TIMEOUT = 0x2
+OLC_STATUS_MULTI_DIVIDE = 0x4
+
+OLC_MAX_AGENT_FIELDS = 64
+OLC_MAX_FIELDS = 8
+OLC_MAX_RULES = 16
+OLC_RADIAL_BINS = 64
+OLC_STATE_BINS = 8
+
+# Every symbol include/olc.h declares (the loader checks each one).
+EXPORTS = (
+    "olc_create", "olc_destroy", "olc_last_error", "olc_version",
+    "olc_bind_agent_column", "olc_bind_field", "olc_set_contact", "olc_set_rule_source",
+    "olc_set_params", "olc_set_agent_count", "olc_current_buffers", "olc_step",
+    "olc_read_counters", "olc_read_reductions", "olc_read_user_metrics",
+    "olc_set_user_metrics_size",
+    "olc_stage_rng", "olc_stage_keys", "olc_sort_scratch_bytes", "olc_stage_sort_pairs",
+    "olc_stage_bin_ranges", "olc_stage_diffuse", "olc_stage_contact",
+)
+
+
+class OlcError(RuntimeError):
+    """A libolc entry point returned an error status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"libolc error {code}: {message}")
+        self.code = code
+
+
+class OlcGeom(C.Structure):
+    _fields_ = [
+        ("tissue_dims", C.c_int32 * 3),
+        ("tissue_voxel_size", C.c_float),
+        ("chem_dims", C.c_int32 * 3),
+        ("chem_voxel_size", C.c_float),
+        ("domain_lo", C.c_float * 3),
+        ("domain_hi", C.c_float * 3),
+    ]
+
+
+class OlcCaps(C.Structure):
+    _fields_ = [
+        ("max_agents", C.c_uint32),
+        ("n_agent_fields", C.c_uint32),
+        ("n_fields", C.c_uint32),
+        ("state_field", C.c_int32),
+        ("radial_bin_width", C.c_float),
+        ("center", C.c_float * 3),
+        ("dt", C.c_float),
+    ]
+
+
+class OlcDiffusion(C.Structure):
+    _fields_ = [
+        ("diffusion", C.c_float),
+        ("decay", C.c_float),
+        ("boundary", C.c_float),
+        ("substeps", C.c_int32),
+        ("has_sink", C.c_int32),
+    ]
+
+
+class OlcContact(C.Structure):
+    _fields_ = [
+        ("enabled", C.c_int32),
+        ("radius_field", C.c_int32),
+        ("radius_const", C.c_float),
+        ("stiffness", C.c_float),
+        ("mobility", C.c_float),
+        ("max_disp", C.c_float),
+        ("margin", C.c_float),
+    ]
+
+
+class OlcCounters(C.Structure):
+    _fields_ = [
+        ("n_agents", C.c_uint32),
+        ("n_total", C.c_uint32),
+        ("births", C.c_uint32),
+        ("deaths", C.c_uint32),
+        ("status", C.c_uint32),
+        ("pad", C.c_uint32),
+        ("steps", C.c_uint64),
+    ]
+
+
+class OlcReductions(C.Structure):
+    _fields_ = [
+        ("n_live", C.c_uint32),
+        ("state_counts", C.c_uint32 * OLC_STATE_BINS),
+        ("radial_hist", C.c_uint32 * OLC_RADIAL_BINS),
+        ("pad", C.c_uint32),
+        ("sum_pos", C.c_double * 3),
+        ("sum_r2", C.c_double),
+        ("max_r", C.c_double),
+        ("field_mass", C.c_double * OLC_MAX_FIELDS),
+        ("field_min", C.c_double * OLC_MAX_FIELDS),
+        ("field_max", C.c_double * OLC_MAX_FIELDS),
+    ]
+
+
+_VP = C.c_void_p
+_SIGS = {
+    "olc_create": (C.c_int, [C.POINTER(OlcGeom), C.POINTER(OlcCaps), C.POINTER(_VP)]),
+    "olc_destroy": (C.c_int, [_VP]),
+    "olc_last_error": (C.c_char_p, [_VP]),
+    "olc_version": (C.c_char_p, []),
+    "olc_bind_agent_column": (C.c_int, [_VP, C.c_int, _VP, _VP]),
+    "olc_bind_field": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, C.POINTER(OlcDiffusion)]),
+    "olc_set_contact": (C.c_int, [_VP, C.POINTER(OlcContact)]),
+    "olc_set_rule_source": (C.c_int, [_VP, C.c_char_p, C.POINTER(C.c_char_p), C.POINTER(C.c_int), C.c_int,
+                                      C.c_char_p]),
+    "olc_set_params": (C.c_int, [_VP, _VP, C.c_size_t, _VP]),
+    "olc_set_agent_count": (C.c_int, [_VP, C.c_uint32, _VP]),
+    "olc_current_buffers": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "olc_step": (C.c_int, [_VP, C.c_int, C.c_int, _VP]),
+    "olc_read_counters": (C.c_int, [_VP, C.POINTER(OlcCounters), _VP]),
+    "olc_read_reductions": (C.c_int, [_VP, C.POINTER(OlcReductions), _VP]),
+    "olc_read_user_metrics": (C.c_int, [_VP, _VP, C.c_size_t, _VP]),
+    "olc_set_user_metrics_size": (C.c_int, [_VP, C.c_size_t]),
+    "olc_stage_rng": (C.c_int, [_VP, C.c_uint32, C.c_int, _VP, _VP, _VP]),
+    "olc_stage_keys": (C.c_int, [_VP, _VP, _VP, _VP, C.c_uint32, C.POINTER(OlcGeom), _VP, _VP]),
+    "olc_sort_scratch_bytes": (C.c_size_t, [C.c_uint32, C.c_int]),
+    "olc_stage_sort_pairs": (C.c_int, [_VP, _VP, _VP, _VP, C.c_uint32, C.c_int, _VP, C.c_size_t, _VP]),
+    "olc_stage_bin_ranges": (C.c_int, [_VP, C.c_uint32, C.c_uint32, _VP, _VP]),
+    "olc_stage_diffuse": (C.c_int, [_VP, _VP, _VP, C.POINTER(C.c_int32 * 3), C.c_float, C.c_float,
+                                    C.POINTER(OlcDiffusion), _VP]),
+    "olc_stage_contact": (C.c_int, [_VP, _VP, C.c_uint32, C.POINTER(OlcGeom), C.POINTER(OlcContact), C.c_float,
+                                    _VP, _VP, _VP, _VP]),
+}
+
+_lock = threading.Lock()
+_lib: C.CDLL | None = None
+
+
+def load(build_if_missing: bool = True) -> C.CDLL:
+    """Loads libolc.so (building it with nvcc first when it is missing or stale)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if build_if_missing:
+            from oncolytica_b200.build_lib import build
+            build()
+        if not os.path.exists(LIB_PATH):
+            raise OlcError(OLC_ERR_STATE, f"{LIB_PATH} is missing; run python -m oncolytica_b200.build_lib")
+        lib = C.CDLL(LIB_PATH)
+        for name in EXPORTS:
+            fn = getattr(lib, name)
+            res, args = _SIGS[name]
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def last_error(handle=None) -> str:
+    msg = load().olc_last_error(handle)
+    return msg.decode(errors="replace") if msg else ""
+
+
+def check(rc: int, handle=None) -> None:
+    if rc != OLC_OK:
+        raise OlcError(rc, last_error(handle))

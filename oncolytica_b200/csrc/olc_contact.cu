@@ -1,0 +1,90 @@
+// Contact mechanics over the Moore neighbourhood of each agent's bin.
+//
+// Reference force law: engine/assets/shaders/tumor_sim.wgsl:505-628
+// (Kernel_Interaction): for dist < r_i + r_j the repulsion
+// k * overlap * sqrt(overlap) acts along n_ij = (p_i - p_j) / dist.
+// The reference integrates a damped velocity and draws a random jitter for
+// coincident points; this path is overdamped (displacement = mobility * F * dt,
+// capped at max_disp, then clamped into the domain, :606-625) and pushes
+// coincident points apart along x in index order, so it needs no RNG draw.
+// Neighbours come from the sorted bin table (27 bins, out-of-range bins
+// skipped, self skipped) in the order of the reference's MooreOffsets
+// (framework/src/oncolytica/gpu/compiler/template.wgsl:11-21): x fastest,
+// then y, then z; within a bin by sorted row.  The force sum follows that
+// order with separately rounded operations.
+#include "olc_internal.h"
+
+namespace olc {
+
+__global__ void __launch_bounds__(256) k_contact(const float4* __restrict__ posr, const uint2* __restrict__ ranges,
+                                                 const olc_u32* n_dev, olc_u32 n_host, ContactDev c,
+                                                 float* __restrict__ xo, float* __restrict__ yo,
+                                                 float* __restrict__ zo) {
+    const olc_u32 n = n_dev ? *n_dev : n_host;
+    const float md = __fmul_rn(c.mobility, c.dt);
+    for (olc_u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 p = posr[i];
+        if (p.w < 0.0f) continue;  // dead this step: no move, no force
+        const int cx = olc_bin_coord(p.x, c.tvs, c.tdims[0]);
+        const int cy = olc_bin_coord(p.y, c.tvs, c.tdims[1]);
+        const int cz = olc_bin_coord(p.z, c.tvs, c.tdims[2]);
+        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+        for (int dz = -1; dz <= 1; ++dz) {
+            const int nz = cz + dz;
+            if (nz < 0 || nz >= c.tdims[2]) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int ny = cy + dy;
+                if (ny < 0 || ny >= c.tdims[1]) continue;
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int nx = cx + dx;
+                    if (nx < 0 || nx >= c.tdims[0]) continue;
+                    const uint2 rg = __ldg(ranges + olc_tissue_key(nx, ny, nz));
+                    for (olc_u32 j = rg.x; j < rg.y; ++j) {
+                        if (j == i) continue;
+                        const float4 q = __ldg(posr + j);
+                        if (q.w < 0.0f) continue;
+                        const float ddx = __fsub_rn(p.x, q.x);
+                        const float ddy = __fsub_rn(p.y, q.y);
+                        const float ddz = __fsub_rn(p.z, q.z);
+                        const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)),
+                                                   __fmul_rn(ddz, ddz));
+                        const float rsum = __fadd_rn(p.w, q.w);
+                        const float dist = sqrtf(d2);
+                        if (!(dist < rsum)) continue;
+                        const float ov = __fsub_rn(rsum, dist);
+                        const float f = __fmul_rn(__fmul_rn(c.stiffness, ov), sqrtf(ov));
+                        if (dist < 1e-5f) {
+                            fx = __fadd_rn(fx, i < j ? -f : f);
+                        } else {
+                            const float s = __fdiv_rn(f, dist);
+                            fx = __fadd_rn(fx, __fmul_rn(ddx, s));
+                            fy = __fadd_rn(fy, __fmul_rn(ddy, s));
+                            fz = __fadd_rn(fz, __fmul_rn(ddz, s));
+                        }
+                    }
+                }
+            }
+        }
+        float mx = __fmul_rn(fx, md), my = __fmul_rn(fy, md), mz = __fmul_rn(fz, md);
+        const float len = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz)));
+        if (len > c.max_disp) {
+            const float sc = __fdiv_rn(c.max_disp, len);
+            mx = __fmul_rn(mx, sc);
+            my = __fmul_rn(my, sc);
+            mz = __fmul_rn(mz, sc);
+        }
+        xo[i] = fminf(fmaxf(__fadd_rn(p.x, mx), c.lo[0]), c.hi[0]);
+        yo[i] = fminf(fmaxf(__fadd_rn(p.y, my), c.lo[1]), c.hi[1]);
+        zo[i] = fminf(fmaxf(__fadd_rn(p.z, mz), c.lo[2]), c.hi[2]);
+    }
+}
+
+void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
+                    olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s) {
+    olc_u32 blocks = (n_cap + 255) / 256;
+    if (blocks == 0) blocks = 1;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_contact<<<blocks, 256, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_dev, n_host, c, x, y, z);
+}
+
+}  // namespace olc

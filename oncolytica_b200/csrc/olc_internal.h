@@ -1,0 +1,139 @@
+// Host-side declarations shared by the translation units of libolc.so.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+#include <string>
+
+#include "olc_device.cuh"
+#include "olc_rule_rt.cuh"
+#include "../../include/olc.h"
+
+namespace olc {
+
+constexpr int RADIX = 256;
+constexpr int SORT_THREADS = 256;
+constexpr int SORT_IPT = 16;
+constexpr int SORT_TILE = SORT_THREADS * SORT_IPT;
+constexpr int MAX_PASSES = 4;
+
+// Geometry of the bin grid as the kernels see it.
+struct BinGrid {
+    int dims[3];
+    float vs;
+    olc_u32 sentinel;  // tissue_key(dims): key of dead rows, voxel_table_size - 1
+};
+
+BinGrid make_bin_grid(const OlcGeom& g);
+int key_bits_for(olc_u32 max_key);
+
+// Thread-local error message for stateless entry points.
+void set_error(const std::string& msg);
+const char* get_error();
+int cuda_status(cudaError_t e, const char* what);
+
+// ------------------------------------------------------------------ grid
+// Keys of rows [0, n) (n = n_dev ? *n_dev : n_host); dead rows get the
+// sentinel.  When hist != null the 8-bit digit histograms of `passes` passes
+// are accumulated into hist (passes x 256 words) and dead rows are counted
+// into dead_ctr.
+// With counters != null the row count is olc_total_rows(counters).
+void launch_keys(const float* x, const float* y, const float* z, const unsigned char* dead,
+                 const olc_u32* n_dev, olc_u32 n_host, const olc_u32* counters, olc_u32 n_cap,
+                 const BinGrid& g, olc_u32* keys, olc_u32* hist, int passes, olc_u32* dead_ctr,
+                 cudaStream_t s);
+
+void launch_digit_hist(const olc_u32* keys, const olc_u32* n_dev, olc_u32 n_host, olc_u32 n_cap,
+                       olc_u32* hist, int passes, cudaStream_t s);
+
+// Exclusive scan of each pass's histogram into base; zeroes the pass tile
+// counters.  With counters != null also commits the step's compaction:
+// N <- rows - dead, DEAD <- dead, births and rule tile counters reset.
+void launch_scan_hist(const olc_u32* hist, olc_u32* base, int passes, olc_u32* tile_ctrs,
+                      olc_u32* counters, olc_u32 capacity, cudaStream_t s);
+
+void launch_onesweep(const olc_u32* kin, const olc_u32* vin, olc_u32* kout, olc_u32* vout,
+                     const olc_u32* n_dev, olc_u32 n_host, olc_u32 n_cap, int shift, int bits,
+                     const olc_u32* base, olc_u32* lookback, olc_u32* tile_ctr, olc_u32* status,
+                     cudaStream_t s);
+
+size_t sort_scratch_bytes(olc_u32 n, int key_bits);
+
+// Full sort on caller scratch (n rows; n_dev optional).  keys/vals in may
+// alias nothing in scratch; the result lands in kout/vout.  When `keys_ready`
+// the histogram in scratch was already accumulated by launch_keys.
+struct SortScratch {
+    olc_u32* hist;      // MAX_PASSES x 256
+    olc_u32* base;      // MAX_PASSES x 256
+    olc_u32* tile_ctr;  // MAX_PASSES
+    olc_u32* status;    // 1
+    olc_u32* lookback;  // passes x tiles x 256
+    olc_u32* kalt;      // n
+    olc_u32* valt;      // n
+    size_t lookback_words;
+};
+bool carve_sort_scratch(void* base, size_t bytes, olc_u32 n_cap, int key_bits, SortScratch* out);
+void run_sort(const olc_u32* kin, const olc_u32* vin, olc_u32* kout, olc_u32* vout,
+              const olc_u32* n_dev, olc_u32 n_host, olc_u32 n_cap, int key_bits,
+              const SortScratch& sc, bool hist_ready, olc_u32* counters, olc_u32 capacity,
+              cudaStream_t s);
+
+void launch_bin_ranges(const olc_u32* keys, const olc_u32* n_dev, olc_u32 n_host, olc_u32 n_cap,
+                       olc_u32 n_bins, olc_u32* ranges, cudaStream_t s);
+
+struct PermuteArgs {
+    const void* src[OLC_MAX_AGENT_COLS];
+    void* dst[OLC_MAX_AGENT_COLS];
+    int ncols;
+    int radius_col;
+    float radius_const;
+    int write_posr;
+    float4* posr;
+};
+void launch_permute(const olc_u32* idx, olc_u32* counters, olc_u32 n_cap, const PermuteArgs& a,
+                    cudaStream_t s);
+
+// ------------------------------------------------------------------ field
+struct FieldStep {
+    int dims[3];
+    float r;          // D * dt_sub / dx^2
+    float inv_decay;  // 1 / (1 + lambda * dt_sub)
+    float bval;
+    float sink_dt;    // dt of the implicit sink
+    int substeps;
+};
+bool make_field_step(const OlcDiffusion& d, const int dims[3], float dx, float dt, FieldStep* out,
+                     std::string* err);
+void launch_sink(float* f, float* sink, const FieldStep& fs, cudaStream_t s);
+void launch_substep(const float* in, float* out, const FieldStep& fs, cudaStream_t s);
+// Runs sink + S substeps starting from a; returns the buffer holding the result.
+float* run_field_step(float* a, float* b, float* sink, const FieldStep& fs, cudaStream_t s);
+
+// ------------------------------------------------------------------ contact
+struct ContactDev {
+    int tdims[3];
+    float tvs;
+    float stiffness, mobility, max_disp, dt;
+    float lo[3], hi[3];
+};
+void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
+                    olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s);
+
+// ------------------------------------------------------------------ reductions
+struct ReduceArgs {
+    const float* x;
+    const float* y;
+    const float* z;
+    const int* state;       // may be null
+    const unsigned char* life;
+    float cx, cy, cz;
+    float bin_width;
+};
+void launch_reduce_agents(const ReduceArgs& a, const olc_u32* counters, olc_u32 n_cap,
+                          OlcReductions* out_dev, cudaStream_t s);
+void launch_reduce_field(const float* f, size_t nvox, int slot, OlcReductions* out_dev, cudaStream_t s);
+void launch_reset_reductions(OlcReductions* out_dev, int nfields, cudaStream_t s);
+
+void launch_rng(olc_u32* states, olc_u32 n, int draws, float* out, float* dirs, cudaStream_t s);
+
+}  // namespace olc

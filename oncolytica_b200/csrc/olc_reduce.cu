@@ -1,0 +1,196 @@
+// Per-step reductions and the RNG known-answer stage.
+//
+// Reductions restate the engine's metrics (engine/assets/shaders/tumor_sim.wgsl:248-361,
+// Kernel_ClearMetrics/CollectMetrics/FinalizeMetrics) without its fixed-point
+// scaling: counts are exact integers, sums are FP64, the maximum radius is
+// exact.  Field masses are FP64 sums over the field grid.
+#include "olc_internal.h"
+
+namespace olc {
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ olc_u32 warp_sum_u(olc_u32 v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_min_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Non-negative doubles order like their bit patterns as unsigned 64-bit ints.
+__device__ __forceinline__ void atomic_max_nonneg(double* p, double v) {
+    atomicMax(reinterpret_cast<unsigned long long*>(p), (unsigned long long)__double_as_longlong(v));
+}
+__device__ __forceinline__ void atomic_min_nonneg(double* p, double v) {
+    atomicMin(reinterpret_cast<unsigned long long*>(p), (unsigned long long)__double_as_longlong(v));
+}
+
+__global__ void __launch_bounds__(256) k_reduce_agents(ReduceArgs a, const olc_u32* counters,
+                                                       OlcReductions* out) {
+    __shared__ olc_u32 s_hist[OLC_RADIAL_BINS];
+    __shared__ olc_u32 s_state[OLC_STATE_BINS];
+    __shared__ double s_sum[5][8];
+    __shared__ olc_u32 s_live[8];
+    const olc_u32 n = olc_total_rows(counters);
+    for (int i = threadIdx.x; i < OLC_RADIAL_BINS; i += blockDim.x) s_hist[i] = 0u;
+    if (threadIdx.x < OLC_STATE_BINS) s_state[threadIdx.x] = 0u;
+    __syncthreads();
+    double sx = 0.0, sy = 0.0, sz = 0.0, sr2 = 0.0, mr = 0.0;
+    olc_u32 live = 0;
+    for (olc_u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (a.life[i]) continue;
+        const float px = a.x[i], py = a.y[i], pz = a.z[i];
+        ++live;
+        sx += (double)px;
+        sy += (double)py;
+        sz += (double)pz;
+        const double dx = (double)px - (double)a.cx, dy = (double)py - (double)a.cy,
+                     dz = (double)pz - (double)a.cz;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        sr2 += r2;
+        const double r = sqrt(r2);
+        mr = fmax(mr, r);
+        int b = (int)(r / (double)a.bin_width);
+        if (b >= OLC_RADIAL_BINS) b = OLC_RADIAL_BINS - 1;
+        atomicAdd(&s_hist[b], 1u);
+        if (a.state) {
+            int st = a.state[i];
+            if (st >= 0 && st < OLC_STATE_BINS) atomicAdd(&s_state[st], 1u);
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    sx = warp_sum_d(sx);
+    sy = warp_sum_d(sy);
+    sz = warp_sum_d(sz);
+    sr2 = warp_sum_d(sr2);
+    mr = warp_max_d(mr);
+    live = warp_sum_u(live);
+    if (lane == 0) {
+        s_sum[0][warp] = sx;
+        s_sum[1][warp] = sy;
+        s_sum[2][warp] = sz;
+        s_sum[3][warp] = sr2;
+        s_sum[4][warp] = mr;
+        s_live[warp] = live;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t[4] = {0, 0, 0, 0};
+        double m = 0.0;
+        olc_u32 l = 0;
+        for (int w = 0; w < 8; ++w) {
+            for (int k = 0; k < 4; ++k) t[k] += s_sum[k][w];
+            m = fmax(m, s_sum[4][w]);
+            l += s_live[w];
+        }
+        if (l) {
+            atomicAdd(&out->n_live, l);
+            atomicAdd(&out->sum_pos[0], t[0]);
+            atomicAdd(&out->sum_pos[1], t[1]);
+            atomicAdd(&out->sum_pos[2], t[2]);
+            atomicAdd(&out->sum_r2, t[3]);
+            atomic_max_nonneg(&out->max_r, m);
+        }
+    }
+    for (int i = threadIdx.x; i < OLC_RADIAL_BINS; i += blockDim.x)
+        if (s_hist[i]) atomicAdd(&out->radial_hist[i], s_hist[i]);
+    if (threadIdx.x < OLC_STATE_BINS && s_state[threadIdx.x])
+        atomicAdd(&out->state_counts[threadIdx.x], s_state[threadIdx.x]);
+}
+
+__global__ void __launch_bounds__(256) k_reduce_field(const float* __restrict__ f, size_t nvox, int slot,
+                                                      OlcReductions* out) {
+    __shared__ double s_v[3][8];
+    double sum = 0.0, mn = 1e300, mx = 0.0;
+    const size_t n4 = nvox / 4;
+    const float4* f4 = reinterpret_cast<const float4*>(f);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
+        float4 v = __ldg(f4 + i);
+        sum += ((double)v.x + (double)v.y) + ((double)v.z + (double)v.w);
+        mn = fmin(mn, fmin(fmin((double)v.x, (double)v.y), fmin((double)v.z, (double)v.w)));
+        mx = fmax(mx, fmax(fmax((double)v.x, (double)v.y), fmax((double)v.z, (double)v.w)));
+    }
+    if (blockIdx.x == 0) {
+        for (size_t i = n4 * 4 + threadIdx.x; i < nvox; i += blockDim.x) {
+            double v = (double)f[i];
+            sum += v;
+            mn = fmin(mn, v);
+            mx = fmax(mx, v);
+        }
+    }
+    sum = warp_sum_d(sum);
+    mn = warp_min_d(mn);
+    mx = warp_max_d(mx);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_v[0][warp] = sum;
+        s_v[1][warp] = mn;
+        s_v[2][warp] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0, a = 1e300, b = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            t += s_v[0][w];
+            a = fmin(a, s_v[1][w]);
+            b = fmax(b, s_v[2][w]);
+        }
+        atomicAdd(&out->field_mass[slot], t);
+        atomic_min_nonneg(&out->field_min[slot], a);
+        atomic_max_nonneg(&out->field_max[slot], b);
+    }
+}
+
+void launch_reduce_agents(const ReduceArgs& a, const olc_u32* counters, olc_u32 n_cap, OlcReductions* out,
+                          cudaStream_t s) {
+    olc_u32 blocks = (n_cap + 255) / 256;
+    if (blocks == 0) blocks = 1;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    k_reduce_agents<<<blocks, 256, 0, s>>>(a, counters, out);
+}
+
+void launch_reduce_field(const float* f, size_t nvox, int slot, OlcReductions* out, cudaStream_t s) {
+    size_t blocks = (nvox / 4 + 255) / 256;
+    if (blocks == 0) blocks = 1;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    k_reduce_field<<<(unsigned)blocks, 256, 0, s>>>(f, nvox, slot, out);
+}
+
+// field_min starts at +inf (all ones in the exponent) for the unsigned min.
+__global__ void k_init_reductions(OlcReductions* out, int nfields) {
+    if (threadIdx.x < OLC_MAX_FIELDS) out->field_min[threadIdx.x] = 1e300;
+}
+
+void launch_reset_reductions(OlcReductions* out, int nfields, cudaStream_t s) {
+    cudaMemsetAsync(out, 0, sizeof(OlcReductions), s);
+    k_init_reductions<<<1, 32, 0, s>>>(out, nfields);
+}
+
+__global__ void k_rng(olc_u32* states, olc_u32 n, int draws, float* out, float* dirs) {
+    olc_u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    olc_u32 s = states[i];
+    for (int k = 0; k < draws; ++k) out[(size_t)i * draws + k] = olc_next_rand(s);
+    if (dirs) {
+        float3 d = olc_rand_dir(s);
+        dirs[3 * (size_t)i + 0] = d.x;
+        dirs[3 * (size_t)i + 1] = d.y;
+        dirs[3 * (size_t)i + 2] = d.z;
+    }
+    states[i] = s;
+}
+
+void launch_rng(olc_u32* states, olc_u32 n, int draws, float* out, float* dirs, cudaStream_t s) {
+    if (n == 0) return;
+    k_rng<<<(n + 255) / 256, 256, 0, s>>>(states, n, draws, out, dirs);
+}
+
+}  // namespace olc

@@ -1,0 +1,255 @@
+// Runtime for rule kernels: the argument block every rule kernel receives and
+// the device functions the translated rule bodies call.  Compiled twice: by
+// nvcc into libolc.so (for the layout of OlcRuleParams) and by NVRTC together
+// with the CUDA C that oncolytica_b200.compiler emits for a model.
+//
+// Reference semantics restated:
+//   * per-agent rule wrapper: load agent, local RNG, body, store RNG, write
+//     the Out buffer (framework/src/oncolytica/gpu/compiler/_shader_builder.py:207-221)
+//   * die() removes the agent at the next sort; divide() appends a child
+//     (framework/src/oncolytica/gpu/compiler/translator/_stmt_translator.py:431-453),
+//     here at a deterministic slot: rows + exclusive scan of births in parent order.
+//   * Moore neighbourhood of the agent's bin, out-of-range bins skipped, self
+//     skipped (_stmt_translator.py:459-491; offsets template.wgsl:11-21).
+//   * chemistry_at / tissue_at: nearest voxel, clamped to the grid
+//     (framework/src/oncolytica/core/utils/_types.py:314-346).
+#pragma once
+#include "olc_device.cuh"
+
+#define OLC_MAX_AGENT_COLS 64
+#define OLC_MAX_FIELD_COLS 8
+#define OLC_MAX_RULE_KERNELS 16
+
+// Device counter block (u32 words).
+#define OLC_CTR_N          0    // live agents after this step's sort
+#define OLC_CTR_DEAD       1    // dead rows removed by this step's sort
+#define OLC_CTR_STATUS     2    // sticky OLC_ST_* bits
+#define OLC_CTR_DEAD_TMP   3    // dead rows counted by the key kernel
+#define OLC_CTR_ROWS       4    // rows entering this step's sort (live + dead)
+#define OLC_CTR_SORT_TILE  8    // 4 words: tile counters of the sort passes
+#define OLC_CTR_RULE_TILE  12   // OLC_MAX_RULE_KERNELS words: tile counters
+#define OLC_CTR_BIRTHS     28   // OLC_MAX_RULE_KERNELS words: births per rule
+#define OLC_CTR_WORDS      64
+
+#define OLC_RULE_THREADS 256
+
+struct OlcRuleParams {
+    const void* in[OLC_MAX_AGENT_COLS];
+    void* out[OLC_MAX_AGENT_COLS];
+    const float* field[OLC_MAX_FIELD_COLS];
+    float* sink[OLC_MAX_FIELD_COLS];
+    const olc_u32* ranges;        // bin table, 2 words per key
+    unsigned char* life;          // 0 alive, 1 dead (removed at the next sort)
+    float4* posr;                 // (x, y, z, radius) for the contact pass, or null
+    olc_u32* counters;            // OLC_CTR_* block
+    olc_u32* birth_lb;            // look-back words of this rule kernel
+    const unsigned char* params;  // Params blob
+    void* metrics;                // metric accumulators
+    const unsigned char* tissue;  // tissue grid columns (Morton-indexed), or null
+    int tdims[3];
+    float tvs;
+    int cdims[3];
+    float cvs;
+    olc_u32 capacity;
+    olc_u32 n_cols;
+    int radius_col;
+    float radius_const;
+    int rule_index;
+    int n_tissue_cols;
+    olc_u32 tissue_stride;        // bytes between tissue columns
+    int pad;
+};
+
+// Rows processed by rule kernel k: live agents plus children of earlier rules.
+__device__ __forceinline__ olc_u32 olc_rule_rows(const olc_u32* ctr, int k) {
+    olc_u32 r = ctr[OLC_CTR_N];
+    for (int j = 0; j < k; ++j) r += ctr[OLC_CTR_BIRTHS + j];
+    return r;
+}
+
+// Rows in use after all rules of the step (children are stored only below
+// the capacity, so the sum never exceeds it).
+__device__ __forceinline__ olc_u32 olc_total_rows(const olc_u32* ctr) {
+    olc_u32 r = ctr[OLC_CTR_N];
+    for (int j = 0; j < OLC_MAX_RULE_KERNELS; ++j) r += ctr[OLC_CTR_BIRTHS + j];
+    return r;
+}
+
+// ------------------------------------------------------------- vector helpers
+struct olc_vec3 {
+    float x, y, z;
+};
+struct olc_ivec3 {
+    int x, y, z;
+};
+
+__device__ __forceinline__ olc_vec3 olc_v3(float x, float y, float z) { olc_vec3 v; v.x = x; v.y = y; v.z = z; return v; }
+__device__ __forceinline__ olc_ivec3 olc_iv3(int x, int y, int z) { olc_ivec3 v; v.x = x; v.y = y; v.z = z; return v; }
+__device__ __forceinline__ olc_vec3 operator+(olc_vec3 a, olc_vec3 b) { return olc_v3(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)); }
+__device__ __forceinline__ olc_vec3 operator-(olc_vec3 a, olc_vec3 b) { return olc_v3(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)); }
+__device__ __forceinline__ olc_vec3 operator*(olc_vec3 a, olc_vec3 b) { return olc_v3(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y), __fmul_rn(a.z, b.z)); }
+__device__ __forceinline__ olc_vec3 operator*(olc_vec3 a, float s) { return olc_v3(__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s)); }
+__device__ __forceinline__ olc_vec3 operator*(float s, olc_vec3 a) { return olc_v3(__fmul_rn(s, a.x), __fmul_rn(s, a.y), __fmul_rn(s, a.z)); }
+__device__ __forceinline__ olc_vec3 operator/(olc_vec3 a, float s) { return olc_v3(__fdiv_rn(a.x, s), __fdiv_rn(a.y, s), __fdiv_rn(a.z, s)); }
+__device__ __forceinline__ olc_vec3 operator-(olc_vec3 a) { return olc_v3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ bool operator==(olc_vec3 a, olc_vec3 b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+__device__ __forceinline__ bool operator!=(olc_vec3 a, olc_vec3 b) { return !(a == b); }
+__device__ __forceinline__ olc_ivec3 operator+(olc_ivec3 a, olc_ivec3 b) { return olc_iv3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ olc_ivec3 operator-(olc_ivec3 a, olc_ivec3 b) { return olc_iv3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ olc_ivec3 operator*(olc_ivec3 a, olc_ivec3 b) { return olc_iv3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ olc_ivec3 operator*(olc_ivec3 a, int s) { return olc_iv3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ olc_ivec3 operator*(int s, olc_ivec3 a) { return olc_iv3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ olc_ivec3 operator-(olc_ivec3 a) { return olc_iv3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ bool operator==(olc_ivec3 a, olc_ivec3 b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+__device__ __forceinline__ bool operator!=(olc_ivec3 a, olc_ivec3 b) { return !(a == b); }
+
+// ------------------------------------------------------------- ol.math
+// Each helper evaluates its formula with separately rounded IEEE operations,
+// so results match a float32 CPU evaluation of the same formula.
+__device__ __forceinline__ float olc_dot(olc_vec3 a, olc_vec3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ float olc_length_sq(olc_vec3 v) { return olc_dot(v, v); }
+__device__ __forceinline__ float olc_length(olc_vec3 v) { return sqrtf(olc_dot(v, v)); }
+__device__ __forceinline__ float olc_distance_sq(olc_vec3 a, olc_vec3 b) { return olc_length_sq(a - b); }
+__device__ __forceinline__ float olc_distance(olc_vec3 a, olc_vec3 b) { return olc_length(a - b); }
+__device__ __forceinline__ olc_vec3 olc_normalize(olc_vec3 v) {
+    float n = olc_length(v);
+    if (n == 0.0f) return olc_v3(0.0f, 0.0f, 0.0f);
+    float inv = __fdiv_rn(1.0f, n);
+    return v * inv;
+}
+__device__ __forceinline__ olc_vec3 olc_cross(olc_vec3 a, olc_vec3 b) {
+    return olc_v3(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)),
+                  __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+                  __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ olc_vec3 olc_reflect(olc_vec3 v, olc_vec3 n) {
+    float d = __fmul_rn(2.0f, olc_dot(v, n));
+    return v - n * d;
+}
+__device__ __forceinline__ float olc_lerp(float a, float b, float t) { return __fadd_rn(a, __fmul_rn(__fsub_rn(b, a), t)); }
+__device__ __forceinline__ olc_vec3 olc_lerp_vec(olc_vec3 a, olc_vec3 b, float t) {
+    float it = __fsub_rn(1.0f, t);
+    return olc_v3(__fadd_rn(__fmul_rn(a.x, it), __fmul_rn(b.x, t)),
+                  __fadd_rn(__fmul_rn(a.y, it), __fmul_rn(b.y, t)),
+                  __fadd_rn(__fmul_rn(a.z, it), __fmul_rn(b.z, t)));
+}
+__device__ __forceinline__ float olc_clampf(float v, float lo, float hi) { return fmaxf(lo, fminf(hi, v)); }
+__device__ __forceinline__ int olc_clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+__device__ __forceinline__ olc_vec3 olc_clampv(olc_vec3 v, olc_vec3 lo, olc_vec3 hi) {
+    return olc_v3(olc_clampf(v.x, lo.x, hi.x), olc_clampf(v.y, lo.y, hi.y), olc_clampf(v.z, lo.z, hi.z));
+}
+__device__ __forceinline__ float olc_sign(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
+__device__ __forceinline__ int olc_signi(int x) { return x > 0 ? 1 : (x < 0 ? -1 : 0); }
+__device__ __forceinline__ float olc_smoothstep(float e0, float e1, float x) {
+    float t = olc_clampf(__fdiv_rn(__fsub_rn(x, e0), __fsub_rn(e1, e0)), 0.0f, 1.0f);
+    return __fmul_rn(__fmul_rn(t, t), __fsub_rn(3.0f, __fmul_rn(2.0f, t)));
+}
+__device__ __forceinline__ float olc_step_fn(float edge, float x) { return x < edge ? 0.0f : 1.0f; }
+__device__ __forceinline__ float olc_fract(float x) { return __fsub_rn(x, floorf(x)); }
+// Python semantics for // and % on integers and floats.
+__device__ __forceinline__ int olc_floordiv_i(int a, int b) {
+    int q = a / b;
+    if ((a % b != 0) && ((a < 0) != (b < 0))) --q;
+    return q;
+}
+__device__ __forceinline__ int olc_mod_i(int a, int b) {
+    int r = a % b;
+    if (r != 0 && ((r < 0) != (b < 0))) r += b;
+    return r;
+}
+__device__ __forceinline__ float olc_floordiv_f(float a, float b) { return floorf(__fdiv_rn(a, b)); }
+__device__ __forceinline__ float olc_mod_f(float a, float b) {
+    float r = fmodf(a, b);
+    if (r != 0.0f && ((r < 0.0f) != (b < 0.0f))) r = __fadd_rn(r, b);
+    return r;
+}
+
+// ------------------------------------------------------------- grid lookups
+__device__ __forceinline__ olc_u32 olc_chem_index(const OlcRuleParams& P, olc_vec3 p) {
+    int cx = olc_bin_coord(p.x, P.cvs, P.cdims[0]);
+    int cy = olc_bin_coord(p.y, P.cvs, P.cdims[1]);
+    int cz = olc_bin_coord(p.z, P.cvs, P.cdims[2]);
+    return ((olc_u32)cz * (olc_u32)P.cdims[1] + (olc_u32)cy) * (olc_u32)P.cdims[0] + (olc_u32)cx;
+}
+
+__device__ __forceinline__ olc_u32 olc_tissue_index(const OlcRuleParams& P, olc_vec3 p) {
+    int tx = olc_bin_coord(p.x, P.tvs, P.tdims[0]);
+    int ty = olc_bin_coord(p.y, P.tvs, P.tdims[1]);
+    int tz = olc_bin_coord(p.z, P.tvs, P.tdims[2]);
+    return olc_tissue_key(tx, ty, tz);
+}
+
+__device__ __forceinline__ olc_ivec3 olc_tissue_coord(const OlcRuleParams& P, olc_vec3 p) {
+    return olc_iv3(olc_bin_coord(p.x, P.tvs, P.tdims[0]), olc_bin_coord(p.y, P.tvs, P.tdims[1]),
+                   olc_bin_coord(p.z, P.tvs, P.tdims[2]));
+}
+
+// Deposit into a field's sink (sum of first-order uptake rates of a voxel).
+__device__ __forceinline__ void olc_deposit(const OlcRuleParams& P, int field, olc_vec3 p, float rate) {
+    float* s = P.sink[field];
+    if (s) atomicAdd(s + olc_chem_index(P, p), rate);
+}
+
+template <typename T>
+__device__ __forceinline__ T olc_param(const OlcRuleParams& P, int offset) {
+    return *reinterpret_cast<const T*>(P.params + offset);
+}
+
+template <typename T>
+__device__ __forceinline__ T olc_col_in(const OlcRuleParams& P, int col, olc_u32 i) {
+    return reinterpret_cast<const T*>(P.in[col])[i];
+}
+
+template <typename T>
+__device__ __forceinline__ void olc_col_out(const OlcRuleParams& P, int col, olc_u32 i, T v) {
+    reinterpret_cast<T*>(P.out[col])[i] = v;
+}
+
+template <typename T>
+__device__ __forceinline__ T olc_tissue_col(const OlcRuleParams& P, int col, olc_u32 key) {
+    return reinterpret_cast<const T*>(P.tissue + (size_t)col * P.tissue_stride)[key];
+}
+
+// Metric accumulators: one 4-byte word per metric field.
+__device__ __forceinline__ void olc_metric_add_i(const OlcRuleParams& P, int slot, int v) {
+    if (v != 0) atomicAdd(reinterpret_cast<int*>(P.metrics) + slot, v);
+}
+__device__ __forceinline__ void olc_metric_add_u(const OlcRuleParams& P, int slot, olc_u32 v) {
+    if (v != 0u) atomicAdd(reinterpret_cast<olc_u32*>(P.metrics) + slot, v);
+}
+__device__ __forceinline__ void olc_metric_add_f(const OlcRuleParams& P, int slot, float v) {
+    if (v != 0.0f) atomicAdd(reinterpret_cast<float*>(P.metrics) + slot, v);
+}
+
+// Block-wide birth scan + decoupled look-back.  Returns the row of this
+// thread's child (or 0xffffffff when it has none).  All threads must call it.
+__device__ __forceinline__ olc_u32 olc_birth_slot(const OlcRuleParams& P, bool born, olc_u32 tile,
+                                                  olc_u32 base_rows, olc_u32* s_warp, olc_u32* s_excl) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    olc_u32 ballot = __ballot_sync(0xffffffffu, born);
+    olc_u32 before = __popc(ballot & ((1u << lane) - 1u));
+    if (lane == 0) s_warp[warp] = __popc(ballot);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        olc_u32 total = 0;
+        for (int w = 0; w < OLC_RULE_THREADS / 32; ++w) {
+            olc_u32 c = s_warp[w];
+            s_warp[w] = total;
+            total += c;
+        }
+        olc_u32 excl = olc_lookback(P.birth_lb, 1u, tile, total, P.counters + OLC_CTR_STATUS);
+        // Children past the capacity are dropped (and flagged); only stored
+        // children count, so the row count never exceeds the capacity.
+        olc_u32 first = base_rows + excl;
+        olc_u32 room = P.capacity > first ? P.capacity - first : 0u;
+        olc_u32 stored = total < room ? total : room;
+        if (stored) atomicAdd(P.counters + OLC_CTR_BIRTHS + P.rule_index, stored);
+        if (stored < total) atomicOr(P.counters + OLC_CTR_STATUS, OLC_ST_CAPACITY);
+        *s_excl = excl;
+    }
+    __syncthreads();
+    olc_u32 slot = base_rows + *s_excl + s_warp[warp] + before;
+    return born ? slot : 0xffffffffu;
+}

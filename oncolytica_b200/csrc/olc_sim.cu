@@ -1,0 +1,656 @@
+// libolc.so: simulation handle, NVRTC rule compilation, step orchestration and
+// the C ABI declared in include/olc.h.
+//
+// One step (replaces GpuBackend.run_step,
+// framework/src/oncolytica/gpu/runtime/_gpu_backend.py:113-171):
+//   1. fields: implicit sink, then S explicit substeps per field
+//   2. grid: keys (+ digit histograms, dead count) -> onesweep passes ->
+//      bin table -> payload permute into the other agent buffer
+//      (compaction: dead rows sort to the tail and are dropped)
+//   3. cell rules (NVRTC kernels), In -> Out with a buffer flip per rule
+//   4. contact pass, in place on the current positions
+//   5. reductions and metric rules when collect != 0
+// Everything is enqueued on one stream; no host synchronisation.
+#include "olc_internal.h"
+
+#include <nvrtc.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace olc {
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+const char* get_error() { return g_err.c_str(); }
+int cuda_status(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return OLC_OK;
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return OLC_ERR_CUDA;
+}
+
+}  // namespace olc
+
+using namespace olc;
+
+struct OlcSim {
+    OlcGeom geom;
+    OlcCaps caps;
+    BinGrid bins;
+    int key_bits = 0;
+    olc_u32 n_table = 0;  // bin table entries = sentinel + 1
+
+    void* col[2][OLC_MAX_AGENT_COLS] = {};
+    int agent_cur = 0;
+
+    float* field[2][OLC_MAX_FIELDS] = {};
+    float* sink[OLC_MAX_FIELDS] = {};
+    OlcDiffusion fspec[OLC_MAX_FIELDS] = {};
+    FieldStep fstep[OLC_MAX_FIELDS] = {};
+    int field_cur[OLC_MAX_FIELDS] = {};
+    bool field_bound[OLC_MAX_FIELDS] = {};
+
+    OlcContact contact = {};
+    ContactDev contact_dev = {};
+
+    // library-owned device memory
+    olc_u32* counters = nullptr;
+    unsigned char* life = nullptr;
+    olc_u32* keys_in = nullptr;
+    olc_u32* keys = nullptr;
+    olc_u32* vals = nullptr;
+    void* sort_mem = nullptr;
+    SortScratch sc = {};
+    olc_u32* ranges = nullptr;
+    float4* posr = nullptr;
+    olc_u32* birth_lb = nullptr;
+    olc_u32 rule_tiles = 0;
+    unsigned char* params_dev = nullptr;
+    size_t params_cap = 0;
+    unsigned char* params_host = nullptr;  // pinned staging
+    OlcReductions* red_dev = nullptr;
+    OlcReductions* red_host = nullptr;     // pinned
+    void* metrics_dev = nullptr;
+    size_t metrics_bytes = 0;
+    olc_u32* ctr_host_words = nullptr;     // pinned copy of the counter block
+
+    cudaLibrary_t module = nullptr;
+    std::vector<cudaKernel_t> funcs;
+    std::vector<int> kinds;
+    int n_cell_rules = 0;
+
+    uint64_t steps = 0;
+    std::string err;
+};
+
+namespace {
+
+int fail(OlcSim* s, int code, const std::string& msg) {
+    if (s) s->err = msg;
+    set_error(msg);
+    return code;
+}
+
+int check(OlcSim* s, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return OLC_OK;
+    return fail(s, OLC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define OLC_TRY(expr)                 \
+    do {                              \
+        int _rc = (expr);             \
+        if (_rc != OLC_OK) return _rc; \
+    } while (0)
+
+template <typename T>
+int dev_alloc(OlcSim* s, T** p, size_t bytes, const char* what) {
+    if (bytes == 0) bytes = 256;
+    return check(s, cudaMalloc(reinterpret_cast<void**>(p), bytes), what);
+}
+
+bool geom_ok(const OlcGeom& g, std::string* err) {
+    for (int i = 0; i < 3; ++i) {
+        if (g.tissue_dims[i] <= 0 || g.tissue_dims[i] > 240 || (g.tissue_dims[i] & 1)) {
+            *err = "tissue_dims must be even and in [2, 240] (reference limit, _engine.py:84-96)";
+            return false;
+        }
+        if (g.chem_dims[i] < 0) {
+            *err = "chem_dims must be >= 0";
+            return false;
+        }
+    }
+    if (!(g.tissue_voxel_size > 0.0f)) {
+        *err = "tissue_voxel_size must be > 0";
+        return false;
+    }
+    return true;
+}
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Initialises the runtime on the current device (the primary context that
+// torch shares).
+int ensure_context(OlcSim* s) { return check(s, cudaFree(nullptr), "cudaFree(0)"); }
+
+OlcRuleParams make_rule_params(OlcSim* s, int rule_index, int in_buf) {
+    OlcRuleParams P;
+    std::memset(&P, 0, sizeof(P));
+    for (olc_u32 c = 0; c < s->caps.n_agent_fields; ++c) {
+        P.in[c] = s->col[in_buf][c];
+        P.out[c] = s->col[1 - in_buf][c];
+    }
+    for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
+        P.field[f] = s->field[s->field_cur[f]][f];
+        P.sink[f] = s->sink[f];
+    }
+    P.ranges = s->ranges;
+    P.life = s->life;
+    P.posr = s->contact.enabled ? s->posr : nullptr;
+    P.counters = s->counters;
+    P.birth_lb = s->birth_lb + (size_t)rule_index * s->rule_tiles;
+    P.params = s->params_dev;
+    P.metrics = s->metrics_dev;
+    P.tissue = nullptr;
+    for (int i = 0; i < 3; ++i) {
+        P.tdims[i] = s->geom.tissue_dims[i];
+        P.cdims[i] = s->geom.chem_dims[i];
+    }
+    P.tvs = s->geom.tissue_voxel_size;
+    P.cvs = s->geom.chem_voxel_size;
+    P.capacity = s->caps.max_agents;
+    P.n_cols = s->caps.n_agent_fields;
+    P.radius_col = s->contact.radius_field;
+    P.radius_const = s->contact.radius_const;
+    P.rule_index = rule_index;
+    return P;
+}
+
+int launch_rule(OlcSim* s, int k, const OlcRuleParams& P, cudaStream_t st) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    olc_u32 blocks = (s->caps.max_agents + OLC_RULE_THREADS - 1) / OLC_RULE_THREADS;
+    if (blocks == 0) blocks = 1;
+    const olc_u32 cap_blocks = (olc_u32)sms * 8u;
+    if (blocks > cap_blocks) blocks = cap_blocks;
+    void* args[] = {const_cast<OlcRuleParams*>(&P)};
+    return check(s, cudaLaunchKernel(reinterpret_cast<const void*>(s->funcs[k]), dim3(blocks), dim3(OLC_RULE_THREADS),
+                                     args, 0, st),
+                 "cudaLaunchKernel(rule)");
+}
+
+int step_once(OlcSim* s, int collect, cudaStream_t st) {
+    const olc_u32 cap = s->caps.max_agents;
+    // 1. fields
+    for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
+        if (!s->field_bound[f]) continue;
+        int cur = s->field_cur[f];
+        float* a = s->field[cur][f];
+        float* b = s->field[1 - cur][f];
+        float* res = run_field_step(a, b, s->sink[f], s->fstep[f], st);
+        s->field_cur[f] = (res == a) ? cur : 1 - cur;
+    }
+    // 2. grid + compaction
+    const int passes = (s->key_bits + 7) / 8;
+    const int ac = s->agent_cur;
+    OLC_TRY(check(s, cudaMemsetAsync(s->sc.hist, 0, MAX_PASSES * RADIX * 4, st), "memset hist"));
+    launch_keys(static_cast<const float*>(s->col[ac][0]), static_cast<const float*>(s->col[ac][1]),
+                static_cast<const float*>(s->col[ac][2]), s->life, nullptr, 0, s->counters, cap, s->bins,
+                s->keys_in, s->sc.hist, passes, s->counters + OLC_CTR_DEAD_TMP, st);
+    run_sort(s->keys_in, nullptr, s->keys, s->vals, s->counters + OLC_CTR_ROWS, 0, cap, s->key_bits, s->sc,
+             true, s->counters, cap, st);
+    OLC_TRY(check(s, cudaMemsetAsync(s->ranges, 0, (size_t)s->n_table * 8, st), "memset ranges"));
+    launch_bin_ranges(s->keys, s->counters + OLC_CTR_ROWS, 0, cap, s->bins.sentinel, s->ranges, st);
+    PermuteArgs pa;
+    std::memset(&pa, 0, sizeof(pa));
+    pa.ncols = (int)s->caps.n_agent_fields;
+    for (int c = 0; c < pa.ncols; ++c) {
+        pa.src[c] = s->col[ac][c];
+        pa.dst[c] = s->col[1 - ac][c];
+    }
+    pa.radius_col = s->contact.radius_field;
+    pa.radius_const = s->contact.radius_const;
+    pa.write_posr = (s->contact.enabled && s->n_cell_rules == 0) ? 1 : 0;
+    pa.posr = s->posr;
+    launch_permute(s->vals, s->counters, cap, pa, st);
+    s->agent_cur = 1 - ac;
+    // 3. cell rules
+    if (s->n_cell_rules > 0) {
+        OLC_TRY(check(s, cudaMemsetAsync(s->birth_lb, 0, (size_t)s->n_cell_rules * s->rule_tiles * 4, st),
+                      "memset birth look-back"));
+    }
+    int cell_idx = 0;
+    for (size_t k = 0; k < s->funcs.size(); ++k) {
+        if (s->kinds[k] != 0) continue;
+        OlcRuleParams P = make_rule_params(s, cell_idx, s->agent_cur);
+        OLC_TRY(launch_rule(s, (int)k, P, st));
+        s->agent_cur = 1 - s->agent_cur;
+        ++cell_idx;
+    }
+    // 4. contact
+    const int cc = s->agent_cur;
+    if (s->contact.enabled) {
+        launch_contact(s->posr, s->ranges, s->counters + OLC_CTR_N, 0, cap, s->contact_dev,
+                       static_cast<float*>(s->col[cc][0]), static_cast<float*>(s->col[cc][1]),
+                       static_cast<float*>(s->col[cc][2]), st);
+    }
+    // 5. reductions + metric rules
+    if (collect) {
+        launch_reset_reductions(s->red_dev, (int)s->caps.n_fields, st);
+        ReduceArgs ra;
+        ra.x = static_cast<const float*>(s->col[cc][0]);
+        ra.y = static_cast<const float*>(s->col[cc][1]);
+        ra.z = static_cast<const float*>(s->col[cc][2]);
+        ra.state = s->caps.state_field >= 0 ? static_cast<const int*>(s->col[cc][s->caps.state_field]) : nullptr;
+        ra.life = s->life;
+        ra.cx = s->caps.center[0];
+        ra.cy = s->caps.center[1];
+        ra.cz = s->caps.center[2];
+        ra.bin_width = s->caps.radial_bin_width > 0.0f ? s->caps.radial_bin_width : 1.0f;
+        launch_reduce_agents(ra, s->counters, cap, s->red_dev, st);
+        for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
+            if (!s->field_bound[f]) continue;
+            const size_t nvox = (size_t)s->geom.chem_dims[0] * s->geom.chem_dims[1] * s->geom.chem_dims[2];
+            launch_reduce_field(s->field[s->field_cur[f]][f], nvox, (int)f, s->red_dev, st);
+        }
+        if (s->metrics_dev && s->metrics_bytes) {
+            OLC_TRY(check(s, cudaMemsetAsync(s->metrics_dev, 0, s->metrics_bytes, st), "memset metrics"));
+        }
+        for (size_t k = 0; k < s->funcs.size(); ++k) {
+            if (s->kinds[k] != 1) continue;
+            OlcRuleParams P = make_rule_params(s, 0, cc);
+            OLC_TRY(launch_rule(s, (int)k, P, st));
+        }
+    }
+    s->steps++;
+    return check(s, cudaGetLastError(), "step launch");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* olc_version(void) { return "oncolytica_b200 libolc 0.1 (sm_100a)"; }
+
+const char* olc_last_error(const OlcSim* sim) {
+    if (sim) return sim->err.c_str();
+    return get_error();
+}
+
+int olc_create(const OlcGeom* geom, const OlcCaps* caps, OlcSim** out) {
+    if (!geom || !caps || !out) return fail(nullptr, OLC_ERR_ARG, "olc_create: null argument");
+    std::string err;
+    if (!geom_ok(*geom, &err)) return fail(nullptr, OLC_ERR_ARG, "olc_create: " + err);
+    if (caps->max_agents == 0 || caps->max_agents > (1u << 30))
+        return fail(nullptr, OLC_ERR_ARG, "olc_create: max_agents must be in [1, 2^30]");
+    if (caps->n_agent_fields < 3 || caps->n_agent_fields > OLC_MAX_AGENT_FIELDS)
+        return fail(nullptr, OLC_ERR_ARG, "olc_create: n_agent_fields must be in [3, 64] (pos.x/y/z first)");
+    if (caps->n_fields > OLC_MAX_FIELDS) return fail(nullptr, OLC_ERR_ARG, "olc_create: too many fields");
+    if (caps->state_field >= (int)caps->n_agent_fields)
+        return fail(nullptr, OLC_ERR_ARG, "olc_create: state_field out of range");
+    OlcSim* s = new OlcSim();
+    s->geom = *geom;
+    s->caps = *caps;
+    s->bins = make_bin_grid(*geom);
+    s->key_bits = key_bits_for(s->bins.sentinel);
+    s->n_table = s->bins.sentinel + 1u;
+    const olc_u32 cap = caps->max_agents;
+    int rc = OLC_OK;
+    auto A = [&](int r) {
+        if (rc == OLC_OK) rc = r;
+    };
+    A(ensure_context(s));
+    A(dev_alloc(s, &s->counters, OLC_CTR_WORDS * 4, "counters"));
+    A(dev_alloc(s, &s->life, cap, "life"));
+    A(dev_alloc(s, &s->keys_in, (size_t)cap * 4, "keys_in"));
+    A(dev_alloc(s, &s->keys, (size_t)cap * 4, "keys"));
+    A(dev_alloc(s, &s->vals, (size_t)cap * 4, "vals"));
+    const size_t sbytes = sort_scratch_bytes(cap, s->key_bits);
+    A(dev_alloc(s, &s->sort_mem, sbytes, "sort scratch"));
+    A(dev_alloc(s, &s->ranges, (size_t)s->n_table * 8, "bin table"));
+    A(dev_alloc(s, &s->posr, (size_t)cap * sizeof(float4), "posr"));
+    s->rule_tiles = (cap + OLC_RULE_THREADS - 1) / OLC_RULE_THREADS;
+    A(dev_alloc(s, &s->birth_lb, (size_t)OLC_MAX_RULES * s->rule_tiles * 4, "birth look-back"));
+    A(dev_alloc(s, &s->red_dev, sizeof(OlcReductions), "reductions"));
+    A(check(s, cudaMallocHost(reinterpret_cast<void**>(&s->red_host), sizeof(OlcReductions)), "pinned reductions"));
+    A(check(s, cudaMallocHost(reinterpret_cast<void**>(&s->ctr_host_words), OLC_CTR_WORDS * 4), "pinned counters"));
+    if (rc == OLC_OK && !carve_sort_scratch(s->sort_mem, sbytes, cap, s->key_bits, &s->sc))
+        rc = fail(s, OLC_ERR_STATE, "sort scratch layout");
+    if (rc == OLC_OK) {
+        A(check(s, cudaMemset(s->counters, 0, OLC_CTR_WORDS * 4), "memset counters"));
+        A(check(s, cudaMemset(s->life, 0, cap), "memset life"));
+        A(check(s, cudaMemset(s->red_dev, 0, sizeof(OlcReductions)), "memset reductions"));
+    }
+    if (rc != OLC_OK) {
+        std::string msg = s->err;
+        olc_destroy(s);
+        return fail(nullptr, rc, msg);
+    }
+    *out = s;
+    return OLC_OK;
+}
+
+int olc_destroy(OlcSim* s) {
+    if (!s) return OLC_OK;
+    cudaDeviceSynchronize();
+    if (s->module) cudaLibraryUnload(s->module);
+    cudaFree(s->counters);
+    cudaFree(s->life);
+    cudaFree(s->keys_in);
+    cudaFree(s->keys);
+    cudaFree(s->vals);
+    cudaFree(s->sort_mem);
+    cudaFree(s->ranges);
+    cudaFree(s->posr);
+    cudaFree(s->birth_lb);
+    cudaFree(s->params_dev);
+    cudaFree(s->red_dev);
+    cudaFree(s->metrics_dev);
+    if (s->params_host) cudaFreeHost(s->params_host);
+    if (s->red_host) cudaFreeHost(s->red_host);
+    if (s->ctr_host_words) cudaFreeHost(s->ctr_host_words);
+    delete s;
+    return OLC_OK;
+}
+
+int olc_bind_agent_column(OlcSim* s, int index, void* a, void* b) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (index < 0 || index >= (int)s->caps.n_agent_fields || !a || !b)
+        return fail(s, OLC_ERR_ARG, "olc_bind_agent_column: bad index or null buffer");
+    s->col[0][index] = a;
+    s->col[1][index] = b;
+    return OLC_OK;
+}
+
+int olc_bind_field(OlcSim* s, int index, float* a, float* b, float* sink, const OlcDiffusion* spec) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (index < 0 || index >= (int)s->caps.n_fields || !a || !b || !spec)
+        return fail(s, OLC_ERR_ARG, "olc_bind_field: bad index or null argument");
+    std::string err;
+    FieldStep fs;
+    if (!make_field_step(*spec, s->geom.chem_dims, s->geom.chem_voxel_size, s->caps.dt, &fs, &err))
+        return fail(s, OLC_ERR_ARG, "olc_bind_field: " + err);
+    if (spec->has_sink && !sink) return fail(s, OLC_ERR_ARG, "olc_bind_field: has_sink without a sink buffer");
+    s->field[0][index] = a;
+    s->field[1][index] = b;
+    s->sink[index] = spec->has_sink ? sink : nullptr;
+    s->fspec[index] = *spec;
+    s->fstep[index] = fs;
+    s->field_cur[index] = 0;
+    s->field_bound[index] = true;
+    return OLC_OK;
+}
+
+int olc_set_contact(OlcSim* s, const OlcContact* c) {
+    if (!s || !c) return fail(s, OLC_ERR_ARG, "olc_set_contact: null argument");
+    if (c->enabled && (c->radius_field >= (int)s->caps.n_agent_fields))
+        return fail(s, OLC_ERR_ARG, "olc_set_contact: radius_field out of range");
+    s->contact = *c;
+    ContactDev& d = s->contact_dev;
+    for (int i = 0; i < 3; ++i) {
+        d.tdims[i] = s->geom.tissue_dims[i];
+        d.lo[i] = s->geom.domain_lo[i] + c->margin;
+        d.hi[i] = s->geom.domain_hi[i] - c->margin;
+    }
+    d.tvs = s->geom.tissue_voxel_size;
+    d.stiffness = c->stiffness;
+    d.mobility = c->mobility;
+    d.max_disp = c->max_disp;
+    d.dt = s->caps.dt;
+    return OLC_OK;
+}
+
+int olc_set_rule_source(OlcSim* s, const char* src, const char* const* kernels, const int* kinds, int n,
+                        const char* include_dir) {
+    if (!s || !src || (n > 0 && (!kernels || !kinds)) || n < 0 || n > OLC_MAX_RULES)
+        return fail(s, OLC_ERR_ARG, "olc_set_rule_source: bad arguments");
+    int ncell = 0;
+    for (int i = 0; i < n; ++i) {
+        if (kinds[i] != 0 && kinds[i] != 1) return fail(s, OLC_ERR_ARG, "olc_set_rule_source: kind must be 0 or 1");
+        ncell += kinds[i] == 0;
+    }
+    OLC_TRY(ensure_context(s));
+    nvrtcProgram prog;
+    if (nvrtcCreateProgram(&prog, src, "olc_rules.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS)
+        return fail(s, OLC_ERR_NVRTC, "nvrtcCreateProgram failed");
+    std::string inc = std::string("-I") + (include_dir ? include_dir : ".");
+    const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--fmad=false", "-lineinfo",
+                          "--device-as-default-execution-space", inc.c_str()};
+    nvrtcResult r = nvrtcCompileProgram(prog, (int)(sizeof(opts) / sizeof(opts[0])), opts);
+    size_t log_size = 0;
+    nvrtcGetProgramLogSize(prog, &log_size);
+    std::string log(log_size, '\0');
+    if (log_size > 1) nvrtcGetProgramLog(prog, &log[0]);
+    if (r != NVRTC_SUCCESS) {
+        nvrtcDestroyProgram(&prog);
+        return fail(s, OLC_ERR_NVRTC, std::string("NVRTC: ") + nvrtcGetErrorString(r) + "\n" + log);
+    }
+    size_t cubin_size = 0;
+    nvrtcGetCUBINSize(prog, &cubin_size);
+    std::vector<char> cubin(cubin_size);
+    nvrtcGetCUBIN(prog, cubin.data());
+    nvrtcDestroyProgram(&prog);
+    if (s->module) {
+        cudaDeviceSynchronize();
+        cudaLibraryUnload(s->module);
+        s->module = nullptr;
+    }
+    s->funcs.clear();
+    s->kinds.clear();
+    OLC_TRY(check(s, cudaLibraryLoadData(&s->module, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0),
+                  "cudaLibraryLoadData"));
+    for (int i = 0; i < n; ++i) {
+        cudaKernel_t fn;
+        OLC_TRY(check(s, cudaLibraryGetKernel(&fn, s->module, kernels[i]), kernels[i]));
+        s->funcs.push_back(fn);
+        s->kinds.push_back(kinds[i]);
+    }
+    s->n_cell_rules = ncell;
+    return OLC_OK;
+}
+
+int olc_set_params(OlcSim* s, const void* blob, size_t bytes, void* stream) {
+    if (!s || (bytes && !blob)) return fail(s, OLC_ERR_ARG, "olc_set_params: bad arguments");
+    if (bytes == 0) return OLC_OK;
+    cudaStream_t st = as_stream(stream);
+    if (bytes > s->params_cap) {
+        cudaStreamSynchronize(st);
+        cudaFree(s->params_dev);
+        if (s->params_host) cudaFreeHost(s->params_host);
+        s->params_dev = nullptr;
+        s->params_host = nullptr;
+        size_t cap = (bytes + 255) & ~size_t(255);
+        OLC_TRY(dev_alloc(s, &s->params_dev, cap, "params"));
+        OLC_TRY(check(s, cudaMallocHost(reinterpret_cast<void**>(&s->params_host), cap), "pinned params"));
+        s->params_cap = cap;
+    } else {
+        // the staging buffer may still feed an earlier copy
+        OLC_TRY(check(s, cudaStreamSynchronize(st), "sync before params upload"));
+    }
+    std::memcpy(s->params_host, blob, bytes);
+    return check(s, cudaMemcpyAsync(s->params_dev, s->params_host, bytes, cudaMemcpyHostToDevice, st),
+                 "params upload");
+}
+
+int olc_set_user_metrics_size(OlcSim* s, size_t bytes) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    cudaFree(s->metrics_dev);
+    s->metrics_dev = nullptr;
+    s->metrics_bytes = bytes;
+    if (bytes) {
+        OLC_TRY(dev_alloc(s, &s->metrics_dev, bytes, "metrics"));
+        OLC_TRY(check(s, cudaMemset(s->metrics_dev, 0, bytes), "memset metrics"));
+    }
+    return OLC_OK;
+}
+
+int olc_set_agent_count(OlcSim* s, uint32_t n, void* stream) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (n > s->caps.max_agents) return fail(s, OLC_ERR_CAPACITY, "olc_set_agent_count: n exceeds max_agents");
+    for (olc_u32 c = 0; c < s->caps.n_agent_fields; ++c)
+        if (!s->col[0][c]) return fail(s, OLC_ERR_STATE, "olc_set_agent_count: agent column not bound");
+    cudaStream_t st = as_stream(stream);
+    olc_u32 words[OLC_CTR_WORDS];
+    std::memset(words, 0, sizeof(words));
+    OLC_TRY(check(s, cudaStreamSynchronize(st), "sync"));
+    OLC_TRY(check(s, cudaMemcpy(words, s->counters, sizeof(words), cudaMemcpyDeviceToHost), "read counters"));
+    const olc_u32 status = words[OLC_CTR_STATUS];
+    std::memset(words, 0, sizeof(words));
+    words[OLC_CTR_N] = n;
+    words[OLC_CTR_ROWS] = n;
+    words[OLC_CTR_STATUS] = status;
+    OLC_TRY(check(s, cudaMemcpy(s->counters, words, sizeof(words), cudaMemcpyHostToDevice), "write counters"));
+    OLC_TRY(check(s, cudaMemset(s->life, 0, s->caps.max_agents), "memset life"));
+    return OLC_OK;
+}
+
+int olc_current_buffers(const OlcSim* s, int* agent_buf, int* field_buf) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (agent_buf) *agent_buf = s->agent_cur;
+    if (field_buf) {
+        int m = 0;
+        for (int f = 0; f < OLC_MAX_FIELDS; ++f) m |= (s->field_cur[f] & 1) << f;
+        *field_buf = m;
+    }
+    return OLC_OK;
+}
+
+int olc_step(OlcSim* s, int nsteps, int collect, void* stream) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (nsteps < 0) return fail(s, OLC_ERR_ARG, "olc_step: nsteps < 0");
+    for (olc_u32 c = 0; c < s->caps.n_agent_fields; ++c)
+        if (!s->col[0][c]) return fail(s, OLC_ERR_STATE, "olc_step: agent column not bound");
+    cudaStream_t st = as_stream(stream);
+    for (int i = 0; i < nsteps; ++i) OLC_TRY(step_once(s, (collect && i == nsteps - 1) ? 1 : 0, st));
+    return OLC_OK;
+}
+
+int olc_read_counters(OlcSim* s, OlcCounters* out, void* stream) {
+    if (!s || !out) return fail(s, OLC_ERR_ARG, "olc_read_counters: null argument");
+    cudaStream_t st = as_stream(stream);
+    OLC_TRY(check(s, cudaMemcpyAsync(s->ctr_host_words, s->counters, OLC_CTR_WORDS * 4, cudaMemcpyDeviceToHost, st),
+                  "counters readback"));
+    OLC_TRY(check(s, cudaStreamSynchronize(st), "sync"));
+    const olc_u32* w = s->ctr_host_words;
+    olc_u32 births = 0;
+    for (int j = 0; j < OLC_MAX_RULE_KERNELS; ++j) births += w[OLC_CTR_BIRTHS + j];
+    out->n_agents = w[OLC_CTR_N] + births;
+    out->n_total = w[OLC_CTR_N] + births;
+    out->births = births;
+    out->deaths = w[OLC_CTR_DEAD];
+    out->status = w[OLC_CTR_STATUS];
+    out->pad = 0;
+    out->steps = s->steps;
+    return OLC_OK;
+}
+
+int olc_read_reductions(OlcSim* s, OlcReductions* out, void* stream) {
+    if (!s || !out) return fail(s, OLC_ERR_ARG, "olc_read_reductions: null argument");
+    cudaStream_t st = as_stream(stream);
+    OLC_TRY(check(s, cudaMemcpyAsync(s->red_host, s->red_dev, sizeof(OlcReductions), cudaMemcpyDeviceToHost, st),
+                  "reductions readback"));
+    OLC_TRY(check(s, cudaStreamSynchronize(st), "sync"));
+    std::memcpy(out, s->red_host, sizeof(OlcReductions));
+    return OLC_OK;
+}
+
+int olc_read_user_metrics(OlcSim* s, void* out, size_t bytes, void* stream) {
+    if (!s || (bytes && !out)) return fail(s, OLC_ERR_ARG, "olc_read_user_metrics: bad arguments");
+    if (bytes > s->metrics_bytes) return fail(s, OLC_ERR_ARG, "olc_read_user_metrics: more bytes than allocated");
+    if (!bytes) return OLC_OK;
+    cudaStream_t st = as_stream(stream);
+    OLC_TRY(check(s, cudaMemcpyAsync(out, s->metrics_dev, bytes, cudaMemcpyDeviceToHost, st), "metrics readback"));
+    return check(s, cudaStreamSynchronize(st), "sync");
+}
+
+// ------------------------------------------------------------------ stages
+
+int olc_stage_rng(uint32_t* states, uint32_t n, int draws, float* out, float* dirs, void* stream) {
+    if (n && (!states || (draws > 0 && !out))) return fail(nullptr, OLC_ERR_ARG, "olc_stage_rng: null buffer");
+    if (draws < 0) return fail(nullptr, OLC_ERR_ARG, "olc_stage_rng: draws < 0");
+    launch_rng(states, n, draws, out, dirs, as_stream(stream));
+    return cuda_status(cudaGetLastError(), "olc_stage_rng");
+}
+
+int olc_stage_keys(const float* x, const float* y, const float* z, const uint8_t* dead, uint32_t n,
+                   const OlcGeom* geom, uint32_t* keys, void* stream) {
+    if (!geom || (n && (!x || !y || !z || !keys))) return fail(nullptr, OLC_ERR_ARG, "olc_stage_keys: null argument");
+    std::string err;
+    if (!geom_ok(*geom, &err)) return fail(nullptr, OLC_ERR_ARG, "olc_stage_keys: " + err);
+    if (n == 0) return OLC_OK;
+    BinGrid g = make_bin_grid(*geom);
+    launch_keys(x, y, z, dead, nullptr, n, nullptr, n, g, keys, nullptr, 0, nullptr, as_stream(stream));
+    return cuda_status(cudaGetLastError(), "olc_stage_keys");
+}
+
+size_t olc_sort_scratch_bytes(uint32_t n, int key_bits) {
+    if (key_bits < 1 || key_bits > 32) return 0;
+    return sort_scratch_bytes(n, key_bits);
+}
+
+int olc_stage_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, uint32_t n,
+                         int key_bits, void* scratch, size_t bytes, void* stream) {
+    if (key_bits < 1 || key_bits > 32) return fail(nullptr, OLC_ERR_ARG, "olc_stage_sort_pairs: key_bits in [1, 32]");
+    if (n == 0) return OLC_OK;
+    if (!kin || !kout || !vout || !scratch)
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_sort_pairs: null buffer");
+    if (n > (1u << 30)) return fail(nullptr, OLC_ERR_ARG, "olc_stage_sort_pairs: n > 2^30");
+    SortScratch sc;
+    if (!carve_sort_scratch(scratch, bytes, n, key_bits, &sc))
+        return fail(nullptr, OLC_ERR_ARG,
+                    "olc_stage_sort_pairs: scratch too small or not 256-byte aligned (need " +
+                        std::to_string(sort_scratch_bytes(n, key_bits)) + " bytes)");
+    cudaStream_t st = as_stream(stream);
+    cudaMemsetAsync(sc.status, 0, 4, st);
+    run_sort(kin, vin, kout, vout, nullptr, n, n, key_bits, sc, false, nullptr, 0, st);
+    return cuda_status(cudaGetLastError(), "olc_stage_sort_pairs");
+}
+
+int olc_stage_bin_ranges(const uint32_t* keys, uint32_t n, uint32_t n_bins, uint32_t* ranges, void* stream) {
+    if (n_bins == 0 || !ranges || (n && !keys)) return fail(nullptr, OLC_ERR_ARG, "olc_stage_bin_ranges: bad arguments");
+    cudaStream_t st = as_stream(stream);
+    cudaMemsetAsync(ranges, 0, (size_t)n_bins * 8, st);
+    if (n) launch_bin_ranges(keys, nullptr, n, n, n_bins, ranges, st);
+    return cuda_status(cudaGetLastError(), "olc_stage_bin_ranges");
+}
+
+int olc_stage_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], float dx, float dt,
+                      const OlcDiffusion* spec, void* stream) {
+    if (!f || !tmp || !dims || !spec) return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse: null argument");
+    std::string err;
+    FieldStep fs;
+    if (!make_field_step(*spec, dims, dx, dt, &fs, &err)) return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse: " + err);
+    cudaStream_t st = as_stream(stream);
+    float* res = run_field_step(f, tmp, spec->has_sink ? sink : nullptr, fs, st);
+    if (res != f) {
+        const size_t bytes = (size_t)dims[0] * dims[1] * dims[2] * 4;
+        cudaMemcpyAsync(f, res, bytes, cudaMemcpyDeviceToDevice, st);
+    }
+    return cuda_status(cudaGetLastError(), "olc_stage_diffuse");
+}
+
+int olc_stage_contact(const float* posr, const uint32_t* ranges, uint32_t n, const OlcGeom* geom,
+                      const OlcContact* spec, float dt, float* x, float* y, float* z, void* stream) {
+    if (!geom || !spec || (n && (!posr || !ranges || !x || !y || !z)))
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_contact: null argument");
+    std::string err;
+    if (!geom_ok(*geom, &err)) return fail(nullptr, OLC_ERR_ARG, "olc_stage_contact: " + err);
+    if (n == 0) return OLC_OK;
+    ContactDev d;
+    for (int i = 0; i < 3; ++i) {
+        d.tdims[i] = geom->tissue_dims[i];
+        d.lo[i] = geom->domain_lo[i] + spec->margin;
+        d.hi[i] = geom->domain_hi[i] - spec->margin;
+    }
+    d.tvs = geom->tissue_voxel_size;
+    d.stiffness = spec->stiffness;
+    d.mobility = spec->mobility;
+    d.max_disp = spec->max_disp;
+    d.dt = dt;
+    launch_contact(reinterpret_cast<const float4*>(posr), ranges, nullptr, n, n, d, x, y, z, as_stream(stream));
+    return cuda_status(cudaGetLastError(), "olc_stage_contact");
+}
+
+}  // extern "C"

@@ -1,0 +1,254 @@
+"""numpy front end of the C oracle (TEST INFRASTRUCTURE).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, as the checker.  The product package oncolytica_b200 never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+if HERE not in sys.path:
+    sys.path.insert(0, HERE)
+
+from build import build  # noqa: E402
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        path = build()
+        L = C.CDLL(path)
+        P = C.c_void_p
+        L.orc_next_rand.restype = C.c_float
+        L.orc_next_rand.argtypes = [C.POINTER(C.c_uint32)]
+        L.orc_seed_rng.restype = C.c_uint32
+        L.orc_seed_rng.argtypes = [C.c_uint32, C.c_uint32]
+        L.orc_rng_batch.argtypes = [P, C.c_uint32, C.c_int, P, P]
+        L.orc_tissue_key.restype = C.c_uint32
+        L.orc_tissue_key.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.orc_chem_key.restype = C.c_uint32
+        L.orc_chem_key.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.orc_keys.argtypes = [P, P, P, P, C.c_uint32, P, C.c_float, P]
+        L.orc_sort_pairs.argtypes = [P, P, P, P, C.c_uint32]
+        L.orc_bin_ranges.argtypes = [P, C.c_uint32, C.c_uint32, P]
+        L.orc_diffuse.restype = C.c_int
+        L.orc_diffuse.argtypes = [P, P, P, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
+                                  C.c_int]
+        L.orc_contact.argtypes = [P, P, C.c_uint32, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                                  P, P, P, P, P, C.c_int]
+        L.orc_tumour_step.restype = C.c_int
+        L.orc_tumour_step.argtypes = [P, C.c_int]
+        L.orc_tumour_fields.restype = C.c_int
+        L.orc_tumour_fields.argtypes = [P, C.c_int]
+        L.orc_tumour_agents.restype = C.c_int
+        L.orc_tumour_agents.argtypes = [P, C.c_int]
+        L.orc_tumour_sizeof.restype = C.c_size_t
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+# ------------------------------------------------------------------ stages
+
+def seed_rng(seed: int, n: int) -> np.ndarray:
+    L = lib()
+    return np.array([L.orc_seed_rng(seed & 0xFFFFFFFF, i) for i in range(n)], dtype=np.uint32)
+
+
+def rng_batch(states: np.ndarray, draws: int, dirs: bool = False):
+    s = np.ascontiguousarray(states, dtype=np.uint32).copy()
+    out = np.zeros((len(s), max(draws, 0)), dtype=np.float32)
+    d = np.zeros((len(s), 3), dtype=np.float32) if dirs else None
+    lib().orc_rng_batch(_p(s), len(s), draws, _p(out), _p(d))
+    return s, out, d
+
+
+def tissue_key(cx: int, cy: int, cz: int) -> int:
+    return int(lib().orc_tissue_key(cx, cy, cz))
+
+
+def chem_key(cx: int, cy: int, cz: int) -> int:
+    return int(lib().orc_chem_key(cx, cy, cz))
+
+
+def keys(pos: np.ndarray, dims, vs: float, dead: np.ndarray | None = None) -> np.ndarray:
+    pos = np.ascontiguousarray(pos, dtype=np.float32)
+    x, y, z = (np.ascontiguousarray(pos[:, k]) for k in range(3))
+    out = np.zeros(len(pos), dtype=np.uint32)
+    d = None if dead is None else np.ascontiguousarray(dead, dtype=np.uint8)
+    dims_a = np.array(dims, dtype=np.int32)
+    lib().orc_keys(_p(x), _p(y), _p(z), _p(d), len(pos), _p(dims_a), C.c_float(vs), _p(out))
+    return out
+
+
+def sort_pairs(k: np.ndarray, v: np.ndarray | None = None):
+    k = np.ascontiguousarray(k, dtype=np.uint32)
+    vv = None if v is None else np.ascontiguousarray(v, dtype=np.uint32)
+    ko = np.zeros_like(k)
+    vo = np.zeros(len(k), dtype=np.uint32)
+    lib().orc_sort_pairs(_p(k), _p(vv), _p(ko), _p(vo), len(k))
+    return ko, vo
+
+
+def bin_ranges(sorted_keys: np.ndarray, n_bins: int) -> np.ndarray:
+    k = np.ascontiguousarray(sorted_keys, dtype=np.uint32)
+    out = np.zeros(2 * n_bins, dtype=np.uint32)
+    lib().orc_bin_ranges(_p(k), len(k), n_bins, _p(out))
+    return out
+
+
+def diffuse(f: np.ndarray, sink: np.ndarray | None, dx: float, dt: float, D: float, decay: float,
+            boundary: float, substeps: int, nthreads: int = 0) -> np.ndarray:
+    """f is indexed [z, y, x]; returns the field after sink + substeps."""
+    f = np.ascontiguousarray(f, dtype=np.float32).copy()
+    tmp = np.zeros_like(f)
+    s = None if sink is None else np.ascontiguousarray(sink, dtype=np.float32).copy()
+    dims = np.array([f.shape[2], f.shape[1], f.shape[0]], dtype=np.int32)
+    rc = lib().orc_diffuse(_p(f), _p(tmp), _p(s), _p(dims), C.c_float(dx), C.c_float(dt), C.c_float(D),
+                           C.c_float(decay), C.c_float(boundary), substeps, nthreads)
+    if rc != 0:
+        raise ValueError("oracle diffuse: unstable or bad arguments")
+    return f
+
+
+def contact(posr: np.ndarray, ranges: np.ndarray, tdims, tvs: float, stiffness: float, mobility: float,
+            max_disp: float, dt: float, lo, hi, nthreads: int = 0):
+    posr = np.ascontiguousarray(posr, dtype=np.float32)
+    n = len(posr)
+    x = posr[:, 0].copy()
+    y = posr[:, 1].copy()
+    z = posr[:, 2].copy()
+    td = np.array(tdims, dtype=np.int32)
+    lo_a = np.array(lo, dtype=np.float32)
+    hi_a = np.array(hi, dtype=np.float32)
+    r = np.ascontiguousarray(ranges, dtype=np.uint32)
+    lib().orc_contact(_p(posr), _p(r), n, _p(td), C.c_float(tvs), C.c_float(stiffness), C.c_float(mobility),
+                      C.c_float(max_disp), C.c_float(dt), _p(lo_a), _p(hi_a), _p(x), _p(y), _p(z), nthreads)
+    return np.stack([x, y, z], axis=1)
+
+
+# ------------------------------------------------------------------ tumour workload
+
+class OrcTumour(C.Structure):
+    _fields_ = [
+        ("cap", C.c_uint32), ("n", C.c_uint32),
+        ("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p), ("radius", C.c_void_p), ("volume", C.c_void_p),
+        ("state", C.c_void_p), ("rng", C.c_void_p),
+        ("x2", C.c_void_p), ("y2", C.c_void_p), ("z2", C.c_void_p), ("radius2", C.c_void_p),
+        ("volume2", C.c_void_p), ("state2", C.c_void_p), ("rng2", C.c_void_p),
+        ("dead", C.c_void_p),
+        ("tdims", C.c_int32 * 3), ("tvs", C.c_float),
+        ("cdims", C.c_int32 * 3), ("cvs", C.c_float),
+        ("lo", C.c_float * 3), ("hi", C.c_float * 3),
+        ("o2", C.c_void_p), ("o2_tmp", C.c_void_p), ("o2_sink", C.c_void_p),
+        ("drug", C.c_void_p), ("drug_tmp", C.c_void_p),
+        ("has_drug", C.c_int),
+        ("dt", C.c_float), ("growth", C.c_float), ("v_div", C.c_float), ("o2_necrotic", C.c_float),
+        ("o2_quiescent", C.c_float), ("uptake", C.c_float), ("death_k", C.c_float),
+        ("D_o2", C.c_float), ("D_drug", C.c_float), ("decay_drug", C.c_float), ("bnd_o2", C.c_float),
+        ("bnd_drug", C.c_float),
+        ("S_o2", C.c_int), ("S_drug", C.c_int),
+        ("stiffness", C.c_float), ("mobility", C.c_float), ("max_disp", C.c_float), ("margin", C.c_float),
+        ("births", C.c_uint32), ("deaths", C.c_uint32),
+    ]
+
+
+AGENT_COLS = ("x", "y", "z", "radius", "volume", "state", "rng")
+_DT = {"x": np.float32, "y": np.float32, "z": np.float32, "radius": np.float32, "volume": np.float32,
+       "state": np.int32, "rng": np.uint32}
+
+
+class TumourOracle:
+    """Owns numpy buffers for the C tumour step.  `spec` is a workloads.TumourSpec."""
+
+    def __init__(self, spec, agents: dict, o2: np.ndarray, drug: np.ndarray | None, capacity: int):
+        assert lib().orc_tumour_sizeof() == C.sizeof(OrcTumour)
+        self.spec = spec
+        self.cap = capacity
+        self.bufs = {}
+        for k in AGENT_COLS:
+            a = np.zeros(capacity, dtype=_DT[k])
+            b = np.zeros(capacity, dtype=_DT[k])
+            a[: len(agents[k])] = agents[k]
+            self.bufs[k] = a
+            self.bufs[k + "2"] = b
+        self.dead = np.zeros(capacity, dtype=np.uint8)
+        self.o2 = np.ascontiguousarray(o2, dtype=np.float32).copy()
+        self.o2_tmp = np.zeros_like(self.o2)
+        self.o2_sink = np.zeros_like(self.o2)
+        self.has_drug = drug is not None
+        self.drug = np.ascontiguousarray(drug, dtype=np.float32).copy() if drug is not None else np.zeros(1, np.float32)
+        self.drug_tmp = np.zeros_like(self.drug)
+        t = OrcTumour()
+        t.cap = capacity
+        t.n = len(agents["x"])
+        t.tdims[:] = spec.tissue_dims
+        t.tvs = spec.bin_size
+        t.cdims[:] = spec.field_dims
+        t.cvs = spec.dx
+        t.lo[:] = (0.0, 0.0, 0.0)
+        t.hi[:] = (spec.domain,) * 3
+        t.has_drug = int(self.has_drug)
+        for name in ("dt", "growth", "v_div", "o2_necrotic", "o2_quiescent", "uptake", "death_k", "D_o2",
+                     "D_drug", "decay_drug", "bnd_o2", "bnd_drug", "stiffness", "mobility", "max_disp",
+                     "margin"):
+            setattr(t, name, float(getattr(spec, name)))
+        t.S_o2 = int(spec.S_o2)
+        t.S_drug = int(spec.S_drug)
+        self.t = t
+        self._bind()
+
+    def _bind(self):
+        t = self.t
+        for k in AGENT_COLS:
+            setattr(t, k, self.bufs[k].ctypes.data)
+            setattr(t, k + "2", self.bufs[k + "2"].ctypes.data)
+        t.dead = self.dead.ctypes.data
+        t.o2 = self.o2.ctypes.data
+        t.o2_tmp = self.o2_tmp.ctypes.data
+        t.o2_sink = self.o2_sink.ctypes.data
+        t.drug = self.drug.ctypes.data
+        t.drug_tmp = self.drug_tmp.ctypes.data
+
+    def _sync_after(self):
+        # the C side swaps its agent buffer pointers; mirror that here
+        t = self.t
+        for k in AGENT_COLS:
+            if getattr(t, k) != self.bufs[k].ctypes.data:
+                self.bufs[k], self.bufs[k + "2"] = self.bufs[k + "2"], self.bufs[k]
+        self._bind()
+
+    def step(self, nthreads: int = 0):
+        rc = lib().orc_tumour_step(C.byref(self.t), nthreads)
+        self._sync_after()
+        if rc != 0:
+            raise RuntimeError("oracle tumour step failed")
+
+    def fields(self, nthreads: int = 0):
+        if lib().orc_tumour_fields(C.byref(self.t), nthreads) != 0:
+            raise RuntimeError("oracle fields failed")
+
+    def agents_part(self, nthreads: int = 0):
+        rc = lib().orc_tumour_agents(C.byref(self.t), nthreads)
+        self._sync_after()
+        if rc != 0:
+            raise RuntimeError("oracle agents failed")
+
+    @property
+    def rows(self) -> int:
+        return int(self.t.n)
+
+    def live_agents(self) -> dict:
+        n = self.rows
+        keep = self.dead[:n] == 0
+        return {k: self.bufs[k][:n][keep].copy() for k in AGENT_COLS}

@@ -1,0 +1,257 @@
+"""Stage parity on the GPU: each libolc stage entry point against the CPU
+oracle on identical inputs.  Integer stages (RNG states, keys, sort, bin
+table) must match bit for bit; floating-point stages that use only separately
+rounded + - * / sqrt (diffusion, sink, contact) must match bit for bit too;
+the random direction (cos/sin) within 2 ulp."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+import oracle
+from oncolytica_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+def dptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def to_dev(a: np.ndarray, cuda):
+    import torch
+
+    if a.dtype == np.uint32:
+        return torch.from_numpy(a.view(np.int32).copy()).to(cuda)
+    if a.dtype == np.uint8:
+        return torch.from_numpy(a.copy()).to(cuda)
+    return torch.from_numpy(np.ascontiguousarray(a).copy()).to(cuda)
+
+
+def to_host(t, dtype=None) -> np.ndarray:
+    import torch
+
+    torch.cuda.synchronize()
+    a = t.cpu().numpy()
+    return a.view(dtype) if dtype is not None else a
+
+
+def geom(dims, vs, lo=(0, 0, 0), hi=None) -> _lib.OlcGeom:
+    g = _lib.OlcGeom()
+    g.tissue_dims[:] = dims
+    g.tissue_voxel_size = vs
+    g.chem_dims[:] = (0, 0, 0)
+    g.chem_voxel_size = 1.0
+    g.domain_lo[:] = lo
+    g.domain_hi[:] = hi if hi is not None else tuple(d * vs for d in dims)
+    return g
+
+
+# ------------------------------------------------------------------ RNG
+
+def test_rng_bit_exact(cuda, olc):
+    import torch
+
+    n, draws = 5000, 7
+    states = oracle.seed_rng(11, n)
+    s_ref, d_ref, dir_ref = oracle.rng_batch(states, draws, dirs=True)
+    st = to_dev(states, cuda)
+    out = torch.empty(n * draws, dtype=torch.float32, device=cuda)
+    dirs = torch.empty(n * 3, dtype=torch.float32, device=cuda)
+    _lib.check(olc.olc_stage_rng(dptr(st), n, draws, dptr(out), dptr(dirs), None))
+    np.testing.assert_array_equal(to_host(st, np.uint32), s_ref)
+    np.testing.assert_array_equal(to_host(out).reshape(n, draws), d_ref)
+    got = to_host(dirs).reshape(n, 3)
+    # cos/sin are library functions on both sides: allow 2 ulp
+    np.testing.assert_array_max_ulp(got, dir_ref, maxulp=2)
+
+
+# ------------------------------------------------------------------ keys
+
+def test_keys_sort_contract_golden(cuda, olc):
+    import torch
+
+    d = np.load(os.path.join(GOLDEN, "sort_contract.npz"))
+    pos = d["pos"]
+    n = len(pos)
+    x, y, z = (to_dev(np.ascontiguousarray(pos[:, k]), cuda) for k in range(3))
+    keys = torch.empty(n, dtype=torch.int32, device=cuda)
+    g = geom(tuple(int(v) for v in d["dims"]), float(d["vs"]))
+    _lib.check(olc.olc_stage_keys(dptr(x), dptr(y), dptr(z), None, n, C.byref(g), dptr(keys), None))
+    np.testing.assert_array_equal(to_host(keys, np.uint32), d["keys"])
+
+
+def test_keys_edge_positions_and_dead(cuda, olc):
+    import torch
+
+    rng = np.random.default_rng(5)
+    dims, vs = (26, 26, 26), 10.0
+    n = 20000
+    pos = rng.uniform(-20.0, 280.0, size=(n, 3)).astype(np.float32)
+    pos[:10] = [[0, 0, 0], [259.99998, 0, 0], [260, 260, 260], [-0.0, 5, 5], [9.999999, 10, 10.000001],
+                [np.nan, 1, 1], [np.inf, -np.inf, 3], [1e30, -1e30, 0], [130, 130, 130], [255.0, 1.0, 2.0]]
+    dead = (rng.random(n) < 0.1).astype(np.uint8)
+    ref = oracle.keys(pos, dims, vs, dead)
+    x, y, z = (to_dev(np.ascontiguousarray(pos[:, k]), cuda) for k in range(3))
+    dd = to_dev(dead, cuda)
+    keys = torch.empty(n, dtype=torch.int32, device=cuda)
+    g = geom(dims, vs)
+    _lib.check(olc.olc_stage_keys(dptr(x), dptr(y), dptr(z), dptr(dd), n, C.byref(g), dptr(keys), None))
+    got = to_host(keys, np.uint32)
+    np.testing.assert_array_equal(got, ref)
+    assert np.all(got[dead == 1] == oracle.tissue_key(*dims))
+
+
+# ------------------------------------------------------------------ sort
+
+def _gpu_sort(olc, cuda, k: np.ndarray, bits: int, v: np.ndarray | None = None):
+    import torch
+
+    n = len(k)
+    kin = to_dev(k, cuda)
+    vin = to_dev(v, cuda) if v is not None else None
+    kout = torch.empty(max(n, 1), dtype=torch.int32, device=cuda)
+    vout = torch.empty(max(n, 1), dtype=torch.int32, device=cuda)
+    nbytes = olc.olc_sort_scratch_bytes(n, bits)
+    scratch = torch.empty(nbytes, dtype=torch.uint8, device=cuda)
+    _lib.check(olc.olc_stage_sort_pairs(dptr(kin), dptr(vin) if vin is not None else None, dptr(kout), dptr(vout),
+                                        n, bits, dptr(scratch), nbytes, None))
+    return to_host(kout, np.uint32)[:n], to_host(vout, np.uint32)[:n]
+
+
+@pytest.mark.parametrize("n,bits", [(1, 8), (100, 8), (4095, 13), (4096, 16), (4097, 21), (65537, 24),
+                                    (1_000_003, 21), (300_000, 32), (2_500_000, 24)])
+def test_sort_pairs_bit_exact(cuda, olc, n, bits):
+    rng = np.random.default_rng(n + bits)
+    hi = (1 << bits) if bits < 32 else (1 << 32)
+    # few distinct keys for small widths: exercises stability heavily
+    k = rng.integers(0, min(hi, max(2, n // 7)), size=n, dtype=np.uint64).astype(np.uint32)
+    if bits == 32:
+        k = rng.integers(0, 1 << 32, size=n, dtype=np.uint64).astype(np.uint32)
+    ko, vo = _gpu_sort(olc, cuda, k, bits)
+    rk, rv = oracle.sort_pairs(k)
+    np.testing.assert_array_equal(ko, rk)
+    np.testing.assert_array_equal(vo, rv)
+
+
+def test_sort_pairs_with_values_and_nearly_sorted_keys(cuda, olc):
+    rng = np.random.default_rng(9)
+    n = 777_777
+    k = np.sort(rng.integers(0, 2_064_833, size=n)).astype(np.uint32)
+    swap = rng.integers(0, n - 1, size=n // 50)
+    k[swap], k[swap + 1] = k[swap + 1].copy(), k[swap].copy()
+    v = rng.integers(0, 1 << 32, size=n, dtype=np.uint64).astype(np.uint32)
+    ko, vo = _gpu_sort(olc, cuda, k, 21, v)
+    rk, rv = oracle.sort_pairs(k, v)
+    np.testing.assert_array_equal(ko, rk)
+    np.testing.assert_array_equal(vo, rv)
+
+
+def test_sort_contract_golden_ids(cuda, olc):
+    """framework/tests/test_gpu.py:54-61 on the GPU sort: per-key id sets."""
+    d = np.load(os.path.join(GOLDEN, "sort_contract.npz"))
+    keys = d["keys"]
+    bits = int(np.ceil(np.log2(int(d["n_table"]))))
+    ko, vo = _gpu_sort(olc, cuda, keys, bits)
+    assert sorted(vo.tolist()) == list(range(len(keys)))
+    np.testing.assert_array_equal(keys[vo], ko)
+    rk, rv = oracle.sort_pairs(keys)
+    np.testing.assert_array_equal(vo, rv)
+
+
+def test_sort_is_deterministic(cuda, olc):
+    rng = np.random.default_rng(4)
+    k = rng.integers(0, 5000, size=300_001).astype(np.uint32)
+    runs = [_gpu_sort(olc, cuda, k, 13) for _ in range(3)]
+    for ko, vo in runs[1:]:
+        np.testing.assert_array_equal(ko, runs[0][0])
+        np.testing.assert_array_equal(vo, runs[0][1])
+
+
+# ------------------------------------------------------------------ bin table
+
+def test_bin_ranges_bit_exact(cuda, olc):
+    import torch
+
+    rng = np.random.default_rng(2)
+    n_table = 32313
+    k = np.sort(rng.integers(0, n_table + 5, size=200_000)).astype(np.uint32)
+    kd = to_dev(k, cuda)
+    rg = torch.empty(2 * n_table, dtype=torch.int32, device=cuda)
+    _lib.check(olc.olc_stage_bin_ranges(dptr(kd), len(k), n_table, dptr(rg), None))
+    np.testing.assert_array_equal(to_host(rg, np.uint32), oracle.bin_ranges(k, n_table))
+
+
+# ------------------------------------------------------------------ diffusion
+
+@pytest.mark.parametrize("dims,substeps,decay,with_sink", [((32, 24, 20), 5, 0.0, True),
+                                                          ((64, 64, 64), 8, 0.1, False),
+                                                          ((33, 17, 9), 3, 0.05, True)])
+def test_diffuse_bit_exact(cuda, olc, dims, substeps, decay, with_sink):
+    import torch
+
+    rng = np.random.default_rng(sum(dims))
+    nx, ny, nz = dims
+    f = rng.random((nz, ny, nx), dtype=np.float32)
+    sink = None
+    if with_sink:
+        sink = np.zeros_like(f)
+        m = rng.random(f.shape) < 0.1
+        sink[m] = rng.random(int(m.sum())).astype(np.float32) * 0.5
+    dx, dt, D = 4.0, 0.1, 2000.0
+    S = substeps
+    D = min(D, (1.0 / 6.0) * dx * dx * S / dt * 0.999)
+    ref = oracle.diffuse(f, sink, dx=dx, dt=dt, D=D, decay=decay, boundary=0.7, substeps=S)
+    fd = to_dev(f, cuda)
+    tmp = torch.empty_like(fd)
+    sd = to_dev(sink, cuda) if sink is not None else None
+    spec = _lib.OlcDiffusion(diffusion=D, decay=decay, boundary=0.7, substeps=S, has_sink=int(with_sink))
+    dims_c = (C.c_int32 * 3)(nx, ny, nz)
+    _lib.check(olc.olc_stage_diffuse(dptr(fd), dptr(tmp), dptr(sd) if sd is not None else None, C.byref(dims_c),
+                                     dx, dt, C.byref(spec), None))
+    np.testing.assert_array_equal(to_host(fd), ref)
+    if sd is not None:
+        assert float(to_host(sd).max()) == 0.0
+
+
+# ------------------------------------------------------------------ contact
+
+def test_contact_bit_exact(cuda, olc):
+    import torch
+
+    rng = np.random.default_rng(8)
+    dims, vs = (20, 20, 20), 10.0
+    n = 30000
+    pos = rng.normal(100.0, 25.0, size=(n, 3)).astype(np.float32)
+    pos = np.clip(pos, 0.0, 199.0).astype(np.float32)
+    pos[5] = pos[6]  # a coincident pair
+    radius = rng.uniform(4.0, 6.0, size=n).astype(np.float32)
+    k = oracle.keys(pos, dims, vs)
+    ks, perm = oracle.sort_pairs(k)
+    n_table = oracle.tissue_key(*dims)
+    ranges = oracle.bin_ranges(ks, n_table)
+    posr = np.concatenate([pos[perm], radius[perm, None]], axis=1).astype(np.float32)
+    posr[rng.random(n) < 0.02, 3] = -1.0  # a few dead rows
+    params = dict(stiffness=1.0, mobility=10.0, max_disp=1.0, dt=0.1)
+    lo, hi = (0.1, 0.1, 0.1), (199.9, 199.9, 199.9)
+    ref = oracle.contact(posr, ranges, dims, vs, params["stiffness"], params["mobility"], params["max_disp"],
+                         params["dt"], lo, hi)
+    pr = to_dev(posr, cuda)
+    rg = to_dev(ranges, cuda)
+    x = to_dev(np.ascontiguousarray(posr[:, 0]), cuda)
+    y = to_dev(np.ascontiguousarray(posr[:, 1]), cuda)
+    z = to_dev(np.ascontiguousarray(posr[:, 2]), cuda)
+    g = geom(dims, vs, lo=(0, 0, 0), hi=(200, 200, 200))
+    spec = _lib.OlcContact(enabled=1, radius_field=-1, radius_const=0.0, stiffness=params["stiffness"],
+                           mobility=params["mobility"], max_disp=params["max_disp"], margin=0.1)
+    _lib.check(olc.olc_stage_contact(dptr(pr), dptr(rg), n, C.byref(g), C.byref(spec), params["dt"], dptr(x),
+                                     dptr(y), dptr(z), None))
+    got = np.stack([to_host(x), to_host(y), to_host(z)], axis=1)
+    np.testing.assert_array_equal(got, ref)
+    moved = np.any(got != posr[:, :3], axis=1)
+    assert moved.sum() > n // 2
