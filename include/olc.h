@@ -91,7 +91,8 @@ typedef struct {
     float   diffusion;          /* D, length^2 / time                        */
     float   decay;              /* lambda, 1 / time (applied every substep)   */
     float   boundary;           /* value pinned on the outer faces            */
-    int32_t substeps;           /* S >= 1, D*dt/S/dx^2 <= 1/6 is checked      */
+    int32_t substeps;           /* S >= 1, D*dt/S/dx^2 <= 1/6 is checked;
+                                   0 = static field (read by rules only)       */
     int32_t has_sink;           /* rules deposit uptake rates into this field */
 } OlcDiffusion;
 
@@ -164,6 +165,10 @@ int olc_set_contact(OlcSim* sim, const OlcContact* spec);
 int olc_set_rule_source(OlcSim* sim, const char* cuda_src, const char* const* kernels,
                         const int* kinds, int n, const char* include_dir);
 
+/* Compiles `cuda_src` with NVRTC for sm_100a without loading it (needs no
+ * GPU); on failure the compiler log is copied into `log` (NUL-terminated). */
+int olc_nvrtc_check(const char* cuda_src, const char* include_dir, char* log, size_t log_size);
+
 /* Uploads the Params blob (replaces pack_uniforms, _device_manager.py:180-204;
  * unlike the reference, later calls do reach the device). */
 int olc_set_params(OlcSim* sim, const void* blob, size_t bytes, void* stream);
@@ -189,6 +194,11 @@ int olc_read_counters(OlcSim* sim, OlcCounters* out, void* stream);
  * (replaces the MetricsBuffer readback, _gpu_backend.py:166-169). */
 int olc_read_reductions(OlcSim* sim, OlcReductions* out, void* stream);
 int olc_read_user_metrics(OlcSim* sim, void* out, size_t bytes, void* stream);
+
+/* Copies the life flags of rows [0, rows) (0 alive, 1 died this step) to host
+ * memory; sync_to_host drops dead rows as the reference's sort does
+ * (template.wgsl:152-159). */
+int olc_read_life(OlcSim* sim, uint8_t* out, uint32_t rows, void* stream);
 int olc_set_user_metrics_size(OlcSim* sim, size_t bytes);
 
 /* ---------------------------------------------------- stateless stages */

@@ -1,0 +1,314 @@
+"""CudaBackend: the reference's backend protocol
+(ISimulationBackend, framework/src/oncolytica/core/runtime/_backend.py:7-36)
+implemented on libolc.so.
+
+State lives on the device in torch tensors laid out as columns (one array per
+scalar field, three per vec3), double-buffered for the sort permute and the
+rule kernels; chemistry fields are float32 arrays (x fastest) with a ping-pong
+partner and an optional sink.  torch owns the memory; libolc borrows the
+pointers.  Replaces GpuBackend (framework/src/oncolytica/gpu/runtime/_gpu_backend.py).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Any
+
+import numpy as np
+
+from oncolytica_b200 import _lib
+from oncolytica_b200._types import metric_fields
+from oncolytica_b200.compiler.emit_cuda import make_layout, pack_params, translate_model
+
+
+def seed_rng(seed: int, idx: np.ndarray) -> np.ndarray:
+    """Initial RNG states: MurmurHash3 fmix32 of seed*golden + index, forced odd
+    (the device and the oracle use the same function)."""
+    with np.errstate(over="ignore"):
+        h = np.uint32(seed & 0xFFFFFFFF) * np.uint32(0x9E3779B9) + idx.astype(np.uint32)
+        h = h.astype(np.uint32)
+        h ^= h >> np.uint32(16)
+        h *= np.uint32(0x85EBCA6B)
+        h ^= h >> np.uint32(13)
+        h *= np.uint32(0xC2B2AE35)
+        h ^= h >> np.uint32(16)
+    return h | np.uint32(1)
+
+
+class CudaBackend:
+    """ISimulationBackend on CUDA: compile / run_step / sync_to_host / sync_to_device / get_metrics."""
+
+    def __init__(self, engine: Any) -> None:
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("oncolytica_b200 needs a CUDA device: the step has no CPU implementation")
+        self.engine = engine
+        self.torch = torch
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self.lib = _lib.load()
+        self.handle = C.c_void_p()
+        self.layout = None
+        self.program = None
+        self.cols_dev: list[tuple[Any, Any]] = []
+        self.fields_dev: list[tuple[Any, Any, Any]] = []
+        self._params_dirty = True
+        self._last_reductions: dict | None = None
+
+    # ---- helpers -------------------------------------------------------------
+    def _check(self, rc: int) -> None:
+        if rc != _lib.OLC_OK:
+            raise _lib.OlcError(rc, _lib.last_error(self.handle))
+
+    def _stream(self):
+        return C.c_void_p(self.torch.cuda.current_stream(self.device).cuda_stream)
+
+    def _torch_dtype(self, dt):
+        t = self.torch
+        return t.float32 if dt == np.float32 else t.int32
+
+    # ---- ISimulationBackend ---------------------------------------------------
+    def compile(self, sim: Any) -> None:
+        eng = self.engine
+        spec = sim._spec
+        contact = eng._contact
+        radius_field = contact.radius if (contact and isinstance(contact.radius, str)) else None
+        self.layout = L = make_layout(spec, radius_field)
+        if eng._cell_rules or eng._metric_rules:
+            self.program = translate_model(sim, L, radius_field)
+        cap = eng.max_agents
+        tdims = tuple(int(v) for v in eng.tissue_shape)
+        cdims = tuple(int(v) for v in eng.chemistry_shape)
+        lo = eng.domain_lo or (0.0, 0.0, 0.0)
+        hi = eng.domain_hi or tuple(d * eng.tissue_voxel_size for d in tdims)
+        g = _lib.OlcGeom()
+        g.tissue_dims[:] = tdims
+        g.tissue_voxel_size = eng.tissue_voxel_size
+        g.chem_dims[:] = cdims
+        g.chem_voxel_size = eng.chemistry_voxel_size
+        g.domain_lo[:] = lo
+        g.domain_hi[:] = hi
+        caps = _lib.OlcCaps()
+        caps.max_agents = cap
+        caps.n_agent_fields = len(L.cell_cols)
+        caps.n_fields = len(L.chem_fields)
+        state_col = -1
+        for i, (col, _, dt) in enumerate(L.cell_cols):
+            if col == "state" and dt == np.int32:
+                state_col = i
+        caps.state_field = state_col
+        caps.radial_bin_width = eng.tissue_voxel_size
+        caps.center[:] = tuple((a + b) * 0.5 for a, b in zip(lo, hi))
+        caps.dt = eng.dt
+        self._check(self.lib.olc_create(C.byref(g), C.byref(caps), C.byref(self.handle)))
+        self.geom, self.caps = g, caps
+        torch = self.torch
+        for i, (col, _, dt) in enumerate(L.cell_cols):
+            a = torch.zeros(cap, dtype=self._torch_dtype(dt), device=self.device)
+            b = torch.zeros(cap, dtype=self._torch_dtype(dt), device=self.device)
+            self.cols_dev.append((a, b))
+            self._check(self.lib.olc_bind_agent_column(self.handle, i, C.c_void_p(a.data_ptr()),
+                                                       C.c_void_p(b.data_ptr())))
+        nvox = int(np.prod(cdims))
+        sinks = self.program.sink_fields if self.program else set()
+        for i, name in enumerate(L.chem_fields):
+            a = torch.zeros(nvox, dtype=torch.float32, device=self.device)
+            b = torch.zeros(nvox, dtype=torch.float32, device=self.device)
+            s = torch.zeros(nvox, dtype=torch.float32, device=self.device) if name in sinks else None
+            self.fields_dev.append((a, b, s))
+            d = _lib.OlcDiffusion()
+            spec_d = eng._diffusion.get(name)
+            if spec_d is None:
+                if name in sinks:
+                    raise ValueError(f"sink_at(...).{name} needs Engine.setup_diffusion({name!r}, ...)")
+                d.substeps = 0  # static field: read by rules, never updated
+            else:
+                d.diffusion = spec_d.diffusion
+                d.decay = spec_d.decay
+                d.boundary = spec_d.boundary
+                d.substeps = eng.substeps_for(name)
+                d.has_sink = int(s is not None)
+            self._check(self.lib.olc_bind_field(self.handle, i, C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()),
+                                                C.c_void_p(s.data_ptr()) if s is not None else None, C.byref(d)))
+        ct = _lib.OlcContact()
+        if contact is not None:
+            ct.enabled = 1
+            if radius_field is not None:
+                ct.radius_field = L.col_index(radius_field)
+                ct.radius_const = 0.0
+            else:
+                ct.radius_field = -1
+                ct.radius_const = float(contact.radius)
+            ct.stiffness, ct.mobility = contact.stiffness, contact.mobility
+            ct.max_disp, ct.margin = contact.max_disp, contact.margin
+        self._check(self.lib.olc_set_contact(self.handle, C.byref(ct)))
+        if self.program is not None:
+            names = (C.c_char_p * len(self.program.kernels))(*[k.encode() for k, _ in self.program.kernels])
+            kinds = (C.c_int * len(self.program.kernels))(*[kind for _, kind in self.program.kernels])
+            self._check(self.lib.olc_set_rule_source(self.handle, self.program.source.encode(), names, kinds,
+                                                     len(self.program.kernels), _lib.CSRC_DIR.encode()))
+        self._check(self.lib.olc_set_user_metrics_size(self.handle, 4 * max(1, len(L.metrics))))
+        self.upload_params()
+        self.sync_to_device()
+
+    def upload_params(self) -> None:
+        sim = self.engine._sim
+        blob = pack_params(self.layout, sim._params)
+        buf = C.create_string_buffer(blob, len(blob))
+        self._check(self.lib.olc_set_params(self.handle, C.cast(buf, C.c_void_p), len(blob), self._stream()))
+
+    def run_step(self, collect_metrics: bool = False) -> None:
+        self.run_steps(1, collect_metrics)
+
+    def run_steps(self, n: int, collect_metrics: bool = False) -> None:
+        self._check(self.lib.olc_step(self.handle, int(n), int(bool(collect_metrics)), self._stream()))
+        if collect_metrics:
+            self._read_metrics()
+
+    def _read_metrics(self) -> None:
+        L = self.layout
+        nm = max(1, len(L.metrics))
+        raw = (C.c_uint32 * nm)()
+        self._check(self.lib.olc_read_user_metrics(self.handle, C.cast(raw, C.c_void_p), 4 * nm, self._stream()))
+        words = np.frombuffer(bytes(raw), dtype=np.uint32)
+        m = self.engine._metrics
+        for name, (slot, ty) in L.metrics.items():
+            w = words[slot:slot + 1]
+            if ty == "f32":
+                v = np.float32(w.view(np.float32)[0])
+            elif ty == "u32":
+                v = int(w[0])
+            elif ty == "bool":
+                v = bool(w.view(np.int32)[0])
+            else:
+                v = int(w.view(np.int32)[0])
+            object.__setattr__(m, name, v)
+        self._last_reductions = None
+
+    def get_metrics(self) -> Any:
+        return self.engine._metrics
+
+    def counters(self) -> dict:
+        c = _lib.OlcCounters()
+        self._check(self.lib.olc_read_counters(self.handle, C.byref(c), self._stream()))
+        return {"n_agents": c.n_agents, "births": c.births, "deaths": c.deaths, "status": c.status,
+                "steps": c.steps}
+
+    def get_reductions(self) -> dict:
+        r = _lib.OlcReductions()
+        self._check(self.lib.olc_read_reductions(self.handle, C.byref(r), self._stream()))
+        n = len(self.layout.chem_fields)
+        return {"n_live": r.n_live, "state_counts": list(r.state_counts), "radial_hist": list(r.radial_hist),
+                "sum_pos": list(r.sum_pos), "sum_r2": r.sum_r2, "max_r": r.max_r,
+                "field_mass": {f: r.field_mass[i] for i, f in enumerate(self.layout.chem_fields)},
+                "field_min": {f: r.field_min[i] for i, f in enumerate(self.layout.chem_fields[:n])},
+                "field_max": {f: r.field_max[i] for i, f in enumerate(self.layout.chem_fields[:n])}}
+
+    def _current(self) -> tuple[int, int]:
+        a, f = C.c_int(), C.c_int()
+        self._check(self.lib.olc_current_buffers(self.handle, C.byref(a), C.byref(f)))
+        return a.value, f.value
+
+    def sync_to_device(self) -> None:
+        """Host agents and fields -> device (replaces _gpu_backend.py:353-371)."""
+        torch = self.torch
+        eng = self.engine
+        L = self.layout
+        cols = eng.cells.columns(L.cell_class)
+        n = len(next(iter(cols.values()))) if cols else 0
+        if n > eng.max_agents:
+            raise _lib.OlcError(_lib.OLC_ERR_CAPACITY, f"{n} agents exceed max_agents={eng.max_agents}")
+        rng = cols.get("_rng_state", np.zeros(n, np.uint32)).astype(np.uint32)
+        zero = rng == 0
+        if zero.any():
+            rng = rng.copy()
+            rng[zero] = seed_rng(eng.seed, np.nonzero(zero)[0].astype(np.uint32))
+        ab, fb = self._current()
+        self.torch.cuda.synchronize(self.device)
+        for i, (col, _, dt) in enumerate(L.cell_cols):
+            host = rng if col == "_rng_state" else cols[col]
+            arr = np.ascontiguousarray(host.astype(dt))
+            if dt == np.uint32:
+                arr = arr.view(np.int32)
+            if n:
+                self.cols_dev[i][ab][:n].copy_(torch.from_numpy(arr))
+        for i, name in enumerate(L.chem_fields):
+            host = np.asarray(eng.chemistry.column(name), dtype=np.float32)
+            spec_d = eng._diffusion.get(name)
+            if spec_d is not None:
+                host = host.copy(order="F")
+                b = np.float32(spec_d.boundary)
+                host[0, :, :] = host[-1, :, :] = b
+                host[:, 0, :] = host[:, -1, :] = b
+                host[:, :, 0] = host[:, :, -1] = b
+            flat = np.ascontiguousarray(host.ravel(order="F"))
+            cur = (fb >> i) & 1
+            self.fields_dev[i][cur].copy_(torch.from_numpy(flat))
+            if self.fields_dev[i][2] is not None:
+                self.fields_dev[i][2].zero_()
+        self.torch.cuda.synchronize(self.device)
+        self._check(self.lib.olc_set_agent_count(self.handle, n, self._stream()))
+
+    def sync_to_host(self) -> None:
+        """Device -> host agents (live only) and fields (replaces _gpu_backend.py:373-405)."""
+        eng = self.engine
+        L = self.layout
+        cnt = self.counters()
+        rows = cnt["n_agents"]
+        ab, fb = self._current()
+        self.torch.cuda.synchronize(self.device)
+        cols = {}
+        life = self._life(rows)
+        keep = life == 0
+        for i, (col, _, dt) in enumerate(L.cell_cols):
+            a = self.cols_dev[i][ab][:rows].cpu().numpy()
+            if dt == np.uint32:
+                a = a.view(np.uint32)
+            cols[col] = a[keep].copy()
+        eng.cells._set_columns(cols, L.cell_class)
+        for i, name in enumerate(L.chem_fields):
+            cur = (fb >> i) & 1
+            flat = self.fields_dev[i][cur].cpu().numpy()
+            eng.chemistry.column(name)[...] = flat.reshape(eng.chemistry_shape, order="F")
+
+    def _life(self, rows: int) -> np.ndarray:
+        buf = (C.c_uint8 * max(rows, 1))()
+        self._check(self.lib.olc_read_life(self.handle, C.cast(buf, C.c_void_p), rows, self._stream()))
+        return np.frombuffer(bytes(buf), dtype=np.uint8)[:rows]
+
+    def snapshot(self) -> dict:
+        """Raw device state: every row in use (dead rows included, in device
+        order) with its life flag, the current fields and their sinks."""
+        cnt = self.counters()
+        rows = cnt["n_agents"]
+        ab, fb = self._current()
+        self.torch.cuda.synchronize(self.device)
+        out = {"rows": rows, "life": self._life(rows).copy(), "cols": {}, "fields": {}, "sinks": {}}
+        for i, (col, _, dt) in enumerate(self.layout.cell_cols):
+            a = self.cols_dev[i][ab][:rows].cpu().numpy()
+            out["cols"][col] = a.view(np.uint32).copy() if dt == np.uint32 else a.copy()
+        for i, name in enumerate(self.layout.chem_fields):
+            out["fields"][name] = self.fields_dev[i][(fb >> i) & 1].cpu().numpy().copy()
+            s = self.fields_dev[i][2]
+            out["sinks"][name] = s.cpu().numpy().copy() if s is not None else None
+        return out
+
+    def field_tensor(self, name: str):
+        """The device tensor currently holding chemistry field ``name`` (x fastest)."""
+        _, fb = self._current()
+        i = self.layout.chem_fields.index(name)
+        return self.fields_dev[i][(fb >> i) & 1]
+
+    def column_tensor(self, col: str):
+        ab, _ = self._current()
+        return self.cols_dev[self.layout.col_index(col)][ab]
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.olc_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -248,8 +248,12 @@ __global__ void __launch_bounds__(SORT_THREADS) k_onesweep(const olc_u32* __rest
         olc_u32 k = s_keys[i];
         olc_u32 d = (k >> shift) & mask;
         olc_u32 o = s_gbase[d] + i;
-        kout[o] = k;
-        vout[o] = s_vals[i];
+        // Offsets are exact unless a look-back wait gave up (status flagged);
+        // the bound keeps even that case inside the output.
+        if (o < n) {
+            kout[o] = k;
+            vout[o] = s_vals[i];
+        }
     }
 }
 

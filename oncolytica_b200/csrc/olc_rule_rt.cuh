@@ -212,12 +212,18 @@ __device__ __forceinline__ T olc_tissue_col(const OlcRuleParams& P, int col, olc
     return reinterpret_cast<const T*>(P.tissue + (size_t)col * P.tissue_stride)[key];
 }
 
-// Metric accumulators: one 4-byte word per metric field.
+// Metric accumulators: one 4-byte word per metric field.  Integer adds are
+// reduced across the converged lanes first, so a warp issues one atomic.
 __device__ __forceinline__ void olc_metric_add_i(const OlcRuleParams& P, int slot, int v) {
-    if (v != 0) atomicAdd(reinterpret_cast<int*>(P.metrics) + slot, v);
+    const olc_u32 m = __activemask();
+    const int s = __reduce_add_sync(m, v);
+    if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && s != 0) atomicAdd(reinterpret_cast<int*>(P.metrics) + slot, s);
 }
 __device__ __forceinline__ void olc_metric_add_u(const OlcRuleParams& P, int slot, olc_u32 v) {
-    if (v != 0u) atomicAdd(reinterpret_cast<olc_u32*>(P.metrics) + slot, v);
+    const olc_u32 m = __activemask();
+    const olc_u32 s = __reduce_add_sync(m, v);
+    if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && s != 0u)
+        atomicAdd(reinterpret_cast<olc_u32*>(P.metrics) + slot, s);
 }
 __device__ __forceinline__ void olc_metric_add_f(const OlcRuleParams& P, int slot, float v) {
     if (v != 0.0f) atomicAdd(reinterpret_cast<float*>(P.metrics) + slot, v);

@@ -185,7 +185,7 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
     const olc_u32 cap = s->caps.max_agents;
     // 1. fields
     for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
-        if (!s->field_bound[f]) continue;
+        if (!s->field_bound[f] || s->fstep[f].substeps == 0) continue;  // unbound or static
         int cur = s->field_cur[f];
         float* a = s->field[cur][f];
         float* b = s->field[1 - cur][f];
@@ -369,8 +369,9 @@ int olc_bind_field(OlcSim* s, int index, float* a, float* b, float* sink, const 
     if (index < 0 || index >= (int)s->caps.n_fields || !a || !b || !spec)
         return fail(s, OLC_ERR_ARG, "olc_bind_field: bad index or null argument");
     std::string err;
-    FieldStep fs;
-    if (!make_field_step(*spec, s->geom.chem_dims, s->geom.chem_voxel_size, s->caps.dt, &fs, &err))
+    FieldStep fs = {};
+    if (spec->substeps != 0 &&
+        !make_field_step(*spec, s->geom.chem_dims, s->geom.chem_voxel_size, s->caps.dt, &fs, &err))
         return fail(s, OLC_ERR_ARG, "olc_bind_field: " + err);
     if (spec->has_sink && !sink) return fail(s, OLC_ERR_ARG, "olc_bind_field: has_sink without a sink buffer");
     s->field[0][index] = a;
@@ -402,6 +403,48 @@ int olc_set_contact(OlcSim* s, const OlcContact* c) {
     return OLC_OK;
 }
 
+static int nvrtc_compile(const char* src, const char* include_dir, std::vector<char>* cubin, std::string* log) {
+    nvrtcProgram prog;
+    if (nvrtcCreateProgram(&prog, src, "olc_rules.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS) {
+        *log = "nvrtcCreateProgram failed";
+        return OLC_ERR_NVRTC;
+    }
+    std::string inc = std::string("-I") + (include_dir ? include_dir : ".");
+    const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--fmad=false", "-lineinfo",
+                          "--device-as-default-execution-space", inc.c_str()};
+    nvrtcResult r = nvrtcCompileProgram(prog, (int)(sizeof(opts) / sizeof(opts[0])), opts);
+    size_t log_size = 0;
+    nvrtcGetProgramLogSize(prog, &log_size);
+    log->assign(log_size, '\0');
+    if (log_size > 1) nvrtcGetProgramLog(prog, &(*log)[0]);
+    if (r != NVRTC_SUCCESS) {
+        *log = std::string("NVRTC: ") + nvrtcGetErrorString(r) + "\n" + *log;
+        nvrtcDestroyProgram(&prog);
+        return OLC_ERR_NVRTC;
+    }
+    if (cubin) {
+        size_t cubin_size = 0;
+        nvrtcGetCUBINSize(prog, &cubin_size);
+        cubin->resize(cubin_size);
+        nvrtcGetCUBIN(prog, cubin->data());
+    }
+    nvrtcDestroyProgram(&prog);
+    return OLC_OK;
+}
+
+int olc_nvrtc_check(const char* src, const char* include_dir, char* log, size_t log_size) {
+    if (!src) return fail(nullptr, OLC_ERR_ARG, "olc_nvrtc_check: null source");
+    std::string msg;
+    int rc = nvrtc_compile(src, include_dir, nullptr, &msg);
+    if (log && log_size) {
+        size_t k = msg.size() < log_size - 1 ? msg.size() : log_size - 1;
+        std::memcpy(log, msg.data(), k);
+        log[k] = '\0';
+    }
+    if (rc != OLC_OK) set_error(msg);
+    return rc;
+}
+
 int olc_set_rule_source(OlcSim* s, const char* src, const char* const* kernels, const int* kinds, int n,
                         const char* include_dir) {
     if (!s || !src || (n > 0 && (!kernels || !kinds)) || n < 0 || n > OLC_MAX_RULES)
@@ -412,26 +455,9 @@ int olc_set_rule_source(OlcSim* s, const char* src, const char* const* kernels, 
         ncell += kinds[i] == 0;
     }
     OLC_TRY(ensure_context(s));
-    nvrtcProgram prog;
-    if (nvrtcCreateProgram(&prog, src, "olc_rules.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS)
-        return fail(s, OLC_ERR_NVRTC, "nvrtcCreateProgram failed");
-    std::string inc = std::string("-I") + (include_dir ? include_dir : ".");
-    const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--fmad=false", "-lineinfo",
-                          "--device-as-default-execution-space", inc.c_str()};
-    nvrtcResult r = nvrtcCompileProgram(prog, (int)(sizeof(opts) / sizeof(opts[0])), opts);
-    size_t log_size = 0;
-    nvrtcGetProgramLogSize(prog, &log_size);
-    std::string log(log_size, '\0');
-    if (log_size > 1) nvrtcGetProgramLog(prog, &log[0]);
-    if (r != NVRTC_SUCCESS) {
-        nvrtcDestroyProgram(&prog);
-        return fail(s, OLC_ERR_NVRTC, std::string("NVRTC: ") + nvrtcGetErrorString(r) + "\n" + log);
-    }
-    size_t cubin_size = 0;
-    nvrtcGetCUBINSize(prog, &cubin_size);
-    std::vector<char> cubin(cubin_size);
-    nvrtcGetCUBIN(prog, cubin.data());
-    nvrtcDestroyProgram(&prog);
+    std::vector<char> cubin;
+    std::string log;
+    if (nvrtc_compile(src, include_dir, &cubin, &log) != OLC_OK) return fail(s, OLC_ERR_NVRTC, log);
     if (s->module) {
         cudaDeviceSynchronize();
         cudaLibraryUnload(s->module);
@@ -544,6 +570,15 @@ int olc_read_counters(OlcSim* s, OlcCounters* out, void* stream) {
     out->pad = 0;
     out->steps = s->steps;
     return OLC_OK;
+}
+
+int olc_read_life(OlcSim* s, uint8_t* out, uint32_t rows, void* stream) {
+    if (!s || (rows && !out)) return fail(s, OLC_ERR_ARG, "olc_read_life: bad arguments");
+    if (rows > s->caps.max_agents) return fail(s, OLC_ERR_ARG, "olc_read_life: rows exceed max_agents");
+    if (!rows) return OLC_OK;
+    cudaStream_t st = as_stream(stream);
+    OLC_TRY(check(s, cudaMemcpyAsync(out, s->life, rows, cudaMemcpyDeviceToHost, st), "life readback"));
+    return check(s, cudaStreamSynchronize(st), "sync");
 }
 
 int olc_read_reductions(OlcSim* s, OlcReductions* out, void* stream) {

@@ -1,0 +1,256 @@
+"""Engine: the reference's orchestrator API (framework/src/oncolytica/core/runtime/_engine.py)
+with the CUDA backend as its only implementation.
+
+Reference API kept: ``Engine(backend, max_agents)``, ``setup_geometry``,
+``setup_tissue``, ``setup_chemistry``, ``setup_params``, ``update_params``,
+``load_model``, ``run_step(collect_metrics)``, ``get_metrics``,
+``sync_to_host``, ``step``, ``cells``, ``tissue``, ``chemistry``.
+
+Extensions (no reference counterpart): a chemistry grid decoupled from the
+bin grid (``setup_chemistry(cls, shape=, voxel_size=)``), built-in diffusion
+of chemistry fields (``setup_diffusion``), built-in contact mechanics
+(``setup_contact``), ``dt``, ``seed``, ``setup_domain``, ``sync_to_device``,
+``run_steps``, ``get_reductions``.
+"""
+from __future__ import annotations
+
+import inspect
+import math
+from dataclasses import dataclass
+from typing import Any, Optional, Type
+
+from oncolytica_b200._containers import AgentList, Grid
+from oncolytica_b200._errors import CompilationError
+from oncolytica_b200._types import Cell, Chemistry, Simulation, Tissue
+
+
+@dataclass
+class DiffusionSpec:
+    diffusion: float
+    decay: float = 0.0
+    boundary: float = 0.0
+    substeps: Optional[int] = None
+
+
+@dataclass
+class ContactSpec:
+    radius: str | float = "radius"
+    stiffness: float = 1.0
+    mobility: float = 10.0
+    max_disp: float = 1.0
+    margin: float = 0.1
+
+
+def stable_substeps(D: float, dt: float, dx: float, margin: float = 1.05) -> int:
+    """Smallest S with D*dt/(S*dx^2) <= 1/6 (explicit 7-point FTCS), times a margin."""
+    if D <= 0.0 or dt <= 0.0:
+        return 1
+    return max(1, int(math.ceil(6.0 * D * dt / (dx * dx) * margin)))
+
+
+class Engine:
+    """Holds the model state and dispatches steps to the CUDA backend."""
+
+    def __init__(self, backend: str = "cuda", max_agents: int = 1024 * 256):
+        if backend == "gpu":
+            backend = "cuda"
+        if backend != "cuda":
+            raise ValueError(f"Unknown backend {backend!r}: oncolytica_b200 runs the step on CUDA only "
+                             f"(backend='cuda'; 'gpu' is accepted as an alias).")
+        self.backend = backend
+        self.max_agents = int(max_agents)
+        # geometry defaults (reference _engine.py:34-39)
+        self.tissue_voxel_size: float = 1.4
+        self.chemistry_voxel_size: float = 2.8
+        self.cell_diameter: float = 1.0
+        self.tissue_shape: Optional[tuple[int, int, int]] = (64, 64, 64)
+        self.chemistry_shape: Optional[tuple[int, int, int]] = (32, 32, 32)
+        self.domain_lo: Optional[tuple[float, float, float]] = None
+        self.domain_hi: Optional[tuple[float, float, float]] = None
+        self.dt: float = 1.0
+        self.seed: int = 0
+        self._step = 0
+        self.cells = AgentList(self)
+        self.tissue: Optional[Grid] = None
+        self.chemistry: Optional[Grid] = None
+        self._metrics = None
+        self._sim: Optional[Simulation] = None
+        self._tissue_rules: list = []
+        self._chemistry_rules: list = []
+        self._cell_rules: list = []
+        self._metric_rules: list = []
+        self._diffusion: dict[str, DiffusionSpec] = {}
+        self._contact: Optional[ContactSpec] = None
+        self._tissue_class = None
+        self._chem_class = None
+        self._backend_impl = None
+
+    # ---- state initialisation ---------------------------------------------
+    def setup_params(self, params: Any) -> None:
+        self._sim._params = params
+        if self._backend_impl is not None:
+            self._backend_impl.upload_params()
+
+    def update_params(self, **kwargs: Any) -> None:
+        """Changes parameter values; unlike the reference (whose uniforms are
+        packed once), the new values reach the device before the next step."""
+        for name, value in kwargs.items():
+            self._sim._params._validate_field(name, value)
+        for name, value in kwargs.items():
+            object.__setattr__(self._sim._params, name, value)
+        if self._backend_impl is not None:
+            self._backend_impl.upload_params()
+
+    def setup_geometry(self, tissue_shape: tuple[int, int, int] = (120, 120, 120), tissue_voxel_size: float = 1.4,
+                       cell_diameter: float = 1.0) -> None:
+        self._validate_geometry(tissue_shape)
+        self.tissue_shape = tuple(tissue_shape)
+        self.chemistry_shape = (tissue_shape[0] // 2, tissue_shape[1] // 2, tissue_shape[2] // 2)
+        self.cell_diameter = cell_diameter
+        self.tissue_voxel_size = float(tissue_voxel_size)
+        self.chemistry_voxel_size = 2.0 * float(tissue_voxel_size)
+
+    @staticmethod
+    def _validate_geometry(tissue_shape) -> None:
+        if not isinstance(tissue_shape, (list, tuple)) or len(tissue_shape) != 3:
+            raise TypeError(f"tissue_shape must be a tuple of 3 ints, got {tissue_shape!r}")
+        for i, dim in enumerate(tissue_shape):
+            if not isinstance(dim, int) or isinstance(dim, bool):
+                raise TypeError(f"tissue_shape component {i} must be int, got {type(dim).__name__!r}")
+            if dim <= 0:
+                raise ValueError(f"tissue_shape component {i} must be positive, got {dim}")
+            if dim > 240:
+                raise ValueError(f"tissue_shape component {i} must be ≤ 240, got {dim}")
+            if dim % 2 != 0:
+                raise ValueError(f"tissue_shape component {i} must be even, got {dim}")
+
+    def setup_tissue(self, tissue_class: Type) -> None:
+        if not (isinstance(tissue_class, type) and issubclass(tissue_class, Tissue)):
+            raise ValueError(f"tissue_class must be a subclass of ol.Tissue, got {tissue_class}")
+        self._tissue_class = tissue_class
+        self.tissue = Grid(tissue_class, self.tissue_shape, self)
+
+    def setup_chemistry(self, chemistry_class: Type, shape: Optional[tuple[int, int, int]] = None,
+                        voxel_size: Optional[float] = None) -> None:
+        """Chemistry grid.  Without ``shape``/``voxel_size`` it is the
+        reference's tied grid (tissue/2 at twice the voxel size)."""
+        if not (isinstance(chemistry_class, type) and issubclass(chemistry_class, Chemistry)):
+            raise ValueError(f"chemistry_class must be a subclass of ol.Chemistry, got {chemistry_class}")
+        if shape is not None:
+            if len(shape) != 3 or any(int(s) < 3 for s in shape):
+                raise ValueError("chemistry shape must be 3 ints >= 3")
+            self.chemistry_shape = tuple(int(s) for s in shape)
+        if voxel_size is not None:
+            if voxel_size <= 0:
+                raise ValueError("chemistry voxel_size must be > 0")
+            self.chemistry_voxel_size = float(voxel_size)
+        self._chem_class = chemistry_class
+        self.chemistry = Grid(chemistry_class, self.chemistry_shape, self)
+
+    def setup_diffusion(self, field: str, diffusion: float, decay: float = 0.0, boundary: float = 0.0,
+                        substeps: Optional[int] = None) -> None:
+        """Built-in diffusion of one chemistry field: per step an implicit sink
+        (rates deposited with ``self.sink_at(pos).field += k``), then S explicit
+        7-point substeps with the outer faces pinned to ``boundary``
+        (engine tumor_sim.wgsl:387-446; substeps as chemistry_rule(iterations=S))."""
+        self._diffusion[field] = DiffusionSpec(float(diffusion), float(decay), float(boundary), substeps)
+
+    def setup_contact(self, radius: str | float = "radius", stiffness: float = 1.0, mobility: float = 10.0,
+                      max_disp: float = 1.0, margin: float = 0.1) -> None:
+        """Built-in Hertz-like contact repulsion over the 27 bins
+        (engine tumor_sim.wgsl:505-628), overdamped."""
+        self._contact = ContactSpec(radius, float(stiffness), float(mobility), float(max_disp), float(margin))
+
+    def setup_domain(self, lo: tuple[float, float, float], hi: tuple[float, float, float]) -> None:
+        self.domain_lo = tuple(float(v) for v in lo)
+        self.domain_hi = tuple(float(v) for v in hi)
+
+    def substeps_for(self, field: str) -> int:
+        spec = self._diffusion[field]
+        if spec.substeps:
+            return int(spec.substeps)
+        return stable_substeps(spec.diffusion, self.dt, self.chemistry_voxel_size)
+
+    @property
+    def step(self) -> int:
+        return self._step
+
+    # ---- model loading ----------------------------------------------------
+    def load_model(self, sim_instance: Any) -> None:
+        if not isinstance(sim_instance, Simulation):
+            raise CompilationError(f"Expected an instance of 'ol.Simulation', got '{type(sim_instance).__name__}'.")
+        self._sim = sim_instance
+        self._metrics = sim_instance._spec.metrics_class(sim_instance)
+        sim_instance._engine = self
+        self._tissue_rules.clear()
+        self._chemistry_rules.clear()
+        self._cell_rules.clear()
+        self._metric_rules.clear()
+        # rule discovery by tag, in dir() order (reference _engine.py:130-147)
+        for name in dir(sim_instance):
+            if name.startswith("_"):
+                continue
+            try:
+                method = getattr(sim_instance, name)
+            except Exception:
+                continue
+            if not callable(method):
+                continue
+            kind = getattr(method, "_rule_type", None)
+            {"tissue": self._tissue_rules, "chemistry": self._chemistry_rules, "cell": self._cell_rules,
+             "metric": self._metric_rules}.get(kind, []).append(method)
+        if self._tissue_rules or self._chemistry_rules:
+            names = [m.__name__ for m in self._tissue_rules + self._chemistry_rules]
+            raise CompilationError(
+                f"tissue/chemistry rules {names} are not compiled by this backend; declare diffusing chemistry "
+                f"fields with Engine.setup_diffusion (built-in 7-point stencil) instead")
+        if self.tissue is None and self._tissue_class is None:
+            self._tissue_class = sim_instance._spec.tissue_class
+        if self.chemistry is None:
+            self.setup_chemistry(sim_instance._spec.chemistry_class)
+        for f in self._diffusion:
+            if f not in self.chemistry._fields:
+                raise CompilationError(f"setup_diffusion: chemistry class has no field {f!r}")
+        from oncolytica_b200.backend import CudaBackend
+
+        self._backend_impl = CudaBackend(self)
+        self._backend_impl.compile(sim_instance)
+
+    # ---- execution ---------------------------------------------------------
+    def run_step(self, collect_metrics: bool = False) -> None:
+        if self._sim is None or self._backend_impl is None:
+            raise RuntimeError("Engine.run_step() called before load_model().")
+        self._step += 1
+        self._backend_impl.run_step(collect_metrics=collect_metrics)
+
+    def run_steps(self, n: int, collect_metrics: bool = False) -> None:
+        """n steps enqueued back to back (metrics after the last when asked)."""
+        if self._sim is None or self._backend_impl is None:
+            raise RuntimeError("Engine.run_steps() called before load_model().")
+        self._step += n
+        self._backend_impl.run_steps(n, collect_metrics=collect_metrics)
+
+    def get_metrics(self) -> Any:
+        return self._metrics
+
+    def get_reductions(self) -> dict:
+        return self._backend_impl.get_reductions()
+
+    def sync_to_host(self) -> None:
+        self._backend_impl.sync_to_host()
+
+    def sync_to_device(self) -> None:
+        self._backend_impl.sync_to_device()
+
+    def _resolve_container_for(self, bound_method: Any) -> Any:
+        sig = inspect.signature(bound_method)
+        params = list(sig.parameters.values())
+        if not params:
+            return ()
+        ann = params[0].annotation
+        if isinstance(ann, type) and issubclass(ann, Cell):
+            return self.cells
+        return ()
+
+    def __repr__(self) -> str:
+        return f"Engine(backend={self.backend!r}, step={self._step}, cells={len(self.cells)})"

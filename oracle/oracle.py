@@ -208,6 +208,21 @@ class TumourOracle:
         self.t = t
         self._bind()
 
+    @classmethod
+    def from_snapshot(cls, spec, snap: dict, capacity: int) -> "TumourOracle":
+        """Oracle state equal to a device snapshot (CudaBackend.snapshot())."""
+        c = snap["cols"]
+        agents = {"x": c["pos.x"], "y": c["pos.y"], "z": c["pos.z"], "radius": c["radius"], "volume": c["volume"],
+                  "state": c["state"], "rng": c["_rng_state"]}
+        shp = tuple(spec.field_dims[::-1])
+        o2 = snap["fields"]["o2"].reshape(shp)
+        drug = snap["fields"]["drug"].reshape(shp) if spec.has_drug else None
+        o = cls(spec, agents, o2, drug, capacity)
+        o.dead[: snap["rows"]] = snap["life"]
+        if snap["sinks"].get("o2") is not None:
+            o.o2_sink[...] = snap["sinks"]["o2"].reshape(shp)
+        return o
+
     def _bind(self):
         t = self.t
         for k in AGENT_COLS:

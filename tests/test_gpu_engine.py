@@ -1,0 +1,346 @@
+"""Engine-level GPU tests: the reference's own GPU end-to-end tests
+(framework/tests/test_gpu.py, framework/tests/test_oncolytica.py) run on the
+CUDA backend, and the tumour workload step against the C oracle."""
+from __future__ import annotations
+
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+import oncolytica_b200 as ol
+from oncolytica_b200 import workloads as W
+from oncolytica_b200._geometry import get_tissue_voxel_key, voxel_table_size
+
+pytestmark = pytest.mark.gpu
+
+
+# ---------------------------------------------------------------- fixtures of the reference tests
+
+class MockCell(ol.Cell):
+    pos: ol.vec3
+    id: int
+
+
+class MockTissue(ol.Tissue):
+    pad: int = 0
+
+
+class MockChemistry(ol.Chemistry):
+    pad: ol.f32 = 0.0
+
+
+class MockMetrics(ol.Metrics):
+    pad: int = 0
+
+
+class MockParams(ol.Params):
+    pass
+
+
+class FakeSim(ol.Simulation[MockTissue, MockChemistry, MockCell, MockMetrics, MockParams]):
+    pass
+
+
+class MyCell(ol.Cell):
+    pos: ol.vec3 = ol.vec3(50.0, 50.0, 50.0)
+    health: ol.f32
+    mutated: ol.bool
+
+
+class MyTissue(ol.Tissue):
+    oxygen: ol.f32 = 1.0
+
+
+class MyChem(ol.Chemistry):
+    drug_conc: ol.f32 = 0.0
+
+
+class MyMetrics(ol.Metrics):
+    alive_cells: ol.u32 = 0
+
+
+class MyParams(ol.Params):
+    pass
+
+
+class BasicSim(ol.Simulation[MyTissue, MyChem, MyCell, MyMetrics, MyParams]):
+    @ol.cell_rule
+    def cell_logic(self, cell: MyCell):
+        cell.health -= 10.0
+        if cell.health <= 0.0:
+            cell.die()
+
+    @ol.metric_rule
+    def track_deaths(self, cell: MyCell, metrics: MyMetrics):
+        metrics.alive_cells += 1
+
+
+def test_sort_contract_through_engine(cuda):
+    """framework/tests/test_gpu.py:17-61 on Engine(backend='cuda')."""
+    d = np.load(os.path.join(GOLDEN, "sort_contract.npz"))
+    pos = d["pos"]
+    n = len(pos)
+    gdim = tuple(int(v) for v in d["dims"])
+    vs = float(d["vs"])
+    eng = ol.Engine(backend="cuda", max_agents=n)
+    eng.setup_geometry(gdim, vs)
+    for i in range(n):
+        c = MockCell()
+        c.pos, c.id = ol.vec3(*pos[i]), i
+        eng.cells.add(c)
+    eng.load_model(FakeSim())
+    eng.run_step()
+    eng.sync_to_host()
+    nv = voxel_table_size(gdim)
+    buckets: dict[int, list[int]] = {}
+    for c in eng.cells._data:
+        vk = get_tissue_voxel_key(*(int(float(v) / vs) for v in (c.pos.x, c.pos.y, c.pos.z)))
+        buckets.setdefault(vk, []).append(c.id)
+    ref: dict[int, list[int]] = {}
+    for i, k in enumerate(d["keys"].tolist()):
+        ref.setdefault(k, []).append(i)
+    for vk in range(nv):
+        assert sorted(buckets.get(vk, [])) == sorted(ref.get(vk, [])), vk
+    ids = [c.id for c in eng.cells._data]
+    assert sorted(ids) == list(range(n))
+    # deterministic refinement: stable, so ids ascend within each key
+    for vk, lst in buckets.items():
+        assert lst == sorted(lst)
+
+
+def test_die_removes_agent_and_metrics_skip_it(cuda):
+    """framework/tests/test_oncolytica.py:300-365 (die + metrics + count)."""
+
+    class TestCell(ol.Cell):
+        pos: ol.vec3
+        type_id: ol.i32 = 0
+
+    class TestMetrics(ol.Metrics):
+        alive_count: ol.u32 = 0
+
+    class TestParams(ol.Params):
+        pass
+
+    class DieSim(ol.Simulation[MyTissue, MyChem, TestCell, TestMetrics, TestParams]):
+        @ol.cell_rule
+        def rule(self, cell: TestCell):
+            if cell.type_id == 1:
+                cell.die()
+
+        @ol.metric_rule
+        def calc_metrics(self, cell: TestCell, m: TestMetrics):
+            m.alive_count += 1
+
+    eng = ol.Engine(backend="cuda", max_agents=4)
+    eng.setup_geometry(tissue_shape=(10, 10, 10), tissue_voxel_size=2.0)
+    eng.cells.add(TestCell(pos=ol.vec3(5.0, 5.0, 5.0), type_id=2))
+    eng.cells.add(TestCell(pos=ol.vec3(1.0, 1.0, 1.0), type_id=1))
+    eng.load_model(DieSim())
+    eng.run_step(collect_metrics=True)
+    assert eng.get_metrics().alive_count == 1
+    eng.sync_to_host()
+    types = [c.type_id for c in eng.cells._data]
+    assert types == [2]
+    assert math.isclose(eng.cells._data[0].pos.x, 5.0)
+    eng.run_step(collect_metrics=True)
+    assert eng.get_metrics().alive_count == 1
+    assert eng._backend_impl.counters()["deaths"] == 1
+
+
+def test_divide_appends_child(cuda):
+    """framework/tests/test_oncolytica.py:367-405."""
+
+    class DivCell(ol.Cell):
+        pos: ol.vec3
+        generation: ol.i32 = 0
+
+    class DivideSim(ol.Simulation[MyTissue, MyChem, DivCell, MyMetrics, MyParams]):
+        @ol.cell_rule
+        def rule(self, cell: DivCell):
+            if cell.generation == 0:
+                new_cell = DivCell()
+                new_cell.pos = cell.pos + ol.vec3(1.0, 0.0, 0.0)
+                new_cell.generation = 1
+                cell.divide(new_cell)
+                cell.generation = 1
+
+    eng = ol.Engine(backend="cuda", max_agents=10)
+    eng.setup_geometry(tissue_shape=(10, 10, 10))
+    eng.cells.add(DivCell(pos=ol.vec3(5.0, 5.0, 5.0)))
+    eng.load_model(DivideSim())
+    eng.run_step()
+    eng.sync_to_host()
+    assert len(eng.cells._data) == 2
+    assert [c.generation for c in eng.cells._data] == [1, 1]
+    assert eng.cells._data[1].pos.x == np.float32(6.0)
+
+
+def test_cpu_lifecycle_golden(cuda):
+    """framework/tests/test_oncolytica.py:58-93, per-step counts from the
+    reference CPUBackend run (tests/golden/cpu_lifecycle.json)."""
+    g = json.load(open(os.path.join(GOLDEN, "cpu_lifecycle.json")))
+    for key, health in (("A_default_health", None), ("B_health_100", 100.0)):
+        eng = ol.Engine(backend="cuda")
+        for i in range(5):
+            cell = MyCell()
+            cell.pos = ol.vec3(50.0, 50.0, 50.0) + 5.0 * ol.vec3(float(i))
+            if health is not None:
+                cell.health = health
+            eng.cells.add(cell)
+        eng.load_model(BasicSim())
+        for rec in g[key]:
+            collect = "metric_alive_cells" in rec
+            eng.run_step(collect_metrics=collect)
+            eng.sync_to_host()
+            assert len(eng.cells._data) == rec["alive_after"], (key, rec)
+            if collect:
+                assert eng.get_metrics().alive_cells == rec["metric_alive_cells"]
+
+
+def test_noncubic_grid_runs(cuda):
+    """framework/tests/test_oncolytica.py:267-298 (cell rule part)."""
+
+    class FullSim(ol.Simulation[MyTissue, MyChem, MyCell, MyMetrics, MyParams]):
+        @ol.cell_rule
+        def cell_logic(self, cell: MyCell):
+            if cell.health > 50.0:
+                cell.pos.x += 0.5
+
+    eng = ol.Engine(backend="cuda")
+    eng.setup_geometry(tissue_shape=(120, 64, 32))
+    for i in range(4):
+        eng.cells.add(MyCell(pos=ol.vec3(float(i) * 5.0, 0.0, 0.0), health=60.0))
+    eng.load_model(FullSim())
+    eng.run_step()
+    eng.run_step()
+    eng.sync_to_host()
+    xs = sorted(float(c.pos.x) for c in eng.cells._data)
+    assert xs == [1.0, 6.0, 11.0, 16.0]
+
+
+def test_randomness_runs_and_is_reproducible(cuda):
+    """framework/tests/test_oncolytica.py:437-459, plus reproducibility."""
+
+    class RandSim(ol.Simulation[MyTissue, MyChem, MyCell, MyMetrics, MyParams]):
+        @ol.cell_rule
+        def rule(self, cell: MyCell):
+            dist = ol.random() * 2.0
+            direction = ol.random_dir()
+            cell.pos += direction * dist
+
+    def run():
+        eng = ol.Engine(backend="cuda")
+        eng.setup_geometry(tissue_shape=(20, 20, 20), tissue_voxel_size=2.0)
+        for i in range(100):
+            eng.cells.add(MyCell(pos=ol.vec3(20.0 + 0.1 * i, 20.0, 20.0)))
+        eng.load_model(RandSim())
+        for _ in range(3):
+            eng.run_step()
+        eng.sync_to_host()
+        return np.array([[c.pos.x, c.pos.y, c.pos.z] for c in eng.cells._data])
+
+    a, b = run(), run()
+    np.testing.assert_array_equal(a, b)
+    assert np.abs(a - 20.0).max() > 0.1
+
+
+def test_update_params_reaches_device(cuda):
+    class PCell(ol.Cell):
+        pos: ol.vec3
+        v: ol.f32 = 0.0
+
+    class PParams(ol.Params):
+        inc: ol.f32 = 1.0
+
+    class PSim(ol.Simulation[MyTissue, MyChem, PCell, MyMetrics, PParams]):
+        @ol.cell_rule
+        def rule(self, cell: PCell):
+            cell.v += self.params.inc
+
+    eng = ol.Engine(backend="cuda")
+    eng.cells.add(PCell(pos=ol.vec3(1.0, 1.0, 1.0)))
+    eng.load_model(PSim())
+    eng.run_step()
+    eng.update_params(inc=10.0)
+    eng.run_step()
+    eng.sync_to_host()
+    assert eng.cells._data[0].v == np.float32(11.0)
+
+
+# ---------------------------------------------------------------- tumour workload vs the C oracle
+
+def _parity_spec():
+    return W.scaled(W.SCALE, n_agents=20_000, domain=200.0, ball_radius=55.0, field_dims=(48, 48, 48),
+                    capacity=100_000, seed=3, uptake=4.0, death_k=0.5, init_drug=0.2, v_lo=1.85, v_hi=2.0)
+
+
+def test_tumour_step_parity_with_oracle(cuda):
+    """Each step from an identical state: integer columns, life flags, volumes,
+    radii and both fields bit-exact; positions to 1e-4 µm (children are placed
+    with cos/sin of the random direction, which the two math libraries may
+    round differently by an ulp)."""
+    import oracle
+
+    spec = _parity_spec()
+    eng = W.build_engine(spec)
+    be = eng._backend_impl
+    seen = {"div": 0, "dead": 0, "quiescent": 0, "necrotic": 0}
+    for step in range(6):
+        snap = be.snapshot()
+        orc = oracle.TumourOracle.from_snapshot(spec, snap, spec.capacity)
+        eng.run_step()
+        orc.step(nthreads=4)
+        got = be.snapshot()
+        n = got["rows"]
+        assert n == orc.rows, step
+        np.testing.assert_array_equal(got["life"], orc.dead[:n])
+        for col, key in (("state", "state"), ("_rng_state", "rng"), ("volume", "volume"), ("radius", "radius")):
+            np.testing.assert_array_equal(got["cols"][col], orc.bufs[key][:n], err_msg=f"{col} step {step}")
+        for a, key in (("pos.x", "x"), ("pos.y", "y"), ("pos.z", "z")):
+            np.testing.assert_allclose(got["cols"][a], orc.bufs[key][:n], rtol=0, atol=1e-4)
+        np.testing.assert_array_equal(got["fields"]["o2"], orc.o2.ravel())
+        np.testing.assert_array_equal(got["fields"]["drug"], orc.drug.ravel())
+        np.testing.assert_array_equal(got["sinks"]["o2"], orc.o2_sink.ravel())
+        seen["div"] += int(orc.t.births)
+        seen["dead"] += int(orc.dead[:n].sum())
+        st = got["cols"]["state"]
+        seen["quiescent"] += int((st == 2).sum())
+        seen["necrotic"] += int((st == 3).sum())
+    # the case exercises every branch of the rule
+    assert all(v > 0 for v in seen.values()), seen
+
+
+def test_tumour_long_run_statistics(cuda):
+    """Independent 60-step runs (GPU vs oracle, same seed): population counts
+    within 1 % and radial profiles within 3 % of the live count."""
+    import oracle
+
+    spec = W.scaled(W.PLAIN_SMALL, n_agents=4000, domain=160.0, ball_radius=40.0, field_dims=(40, 40, 40),
+                    capacity=40_000, seed=11, uptake=0.5)
+    eng = W.build_engine(spec)
+    st = W.initial_state(spec)
+    o2, _ = W.initial_fields(spec)
+    orc = oracle.TumourOracle(spec, st, o2, None, spec.capacity)
+    for _ in range(60):
+        eng.run_step()
+        orc.step(nthreads=4)
+    eng.sync_to_host()
+    cols = eng.cells.columns()
+    live_g = len(cols["state"])
+    live_o = orc.live_agents()
+    assert abs(live_g - len(live_o["state"])) <= 0.01 * live_g
+    for s in (1, 2, 3):
+        a = int((cols["state"] == s).sum())
+        b = int((live_o["state"] == s).sum())
+        assert abs(a - b) <= max(5, 0.02 * live_g), (s, a, b)
+    c = np.array(spec.center)
+    rg = np.linalg.norm(np.stack([cols["pos.x"], cols["pos.y"], cols["pos.z"]], 1) - c, axis=1)
+    ro = np.linalg.norm(np.stack([live_o["x"], live_o["y"], live_o["z"]], 1) - c, axis=1)
+    hg, _ = np.histogram(rg, bins=16, range=(0, 80))
+    ho, _ = np.histogram(ro, bins=16, range=(0, 80))
+    assert np.abs(hg - ho).max() <= 0.03 * live_g
