@@ -157,6 +157,14 @@ int olc_bind_field(OlcSim* sim, int index, float* a_dev, float* b_dev, float* si
 
 int olc_set_contact(OlcSim* sim, const OlcContact* spec);
 
+/* Binds the tissue grid for tissue_at(): `n_cols` 4-byte columns, each with
+ * voxel_table_size entries indexed by the tissue (Morton) key, `stride_bytes`
+ * apart starting at cols_dev.  Replaces Tissue_In
+ * (framework/src/oncolytica/gpu/compiler/translator/_expr_translator.py:243-250
+ * reads it by Morton key; the reference host packs it row-major,
+ * _gpu_backend.py:365-367 — here the host packs it by key). */
+int olc_bind_tissue(OlcSim* sim, const void* cols_dev, int n_cols, size_t stride_bytes);
+
 /* Compiles CUDA C emitted by the rule translator with NVRTC for sm_100a
  * (replaces WGSLCompiler.compile + create_shader_module,
  * framework/src/oncolytica/gpu/compiler/_compiler.py:233-352).  `kinds[i]` is

@@ -37,7 +37,7 @@ EXPORTS = (
     "olc_bind_agent_column", "olc_bind_field", "olc_set_contact", "olc_set_rule_source",
     "olc_set_params", "olc_set_agent_count", "olc_current_buffers", "olc_step",
     "olc_read_counters", "olc_read_reductions", "olc_read_user_metrics",
-    "olc_set_user_metrics_size", "olc_read_life", "olc_nvrtc_check",
+    "olc_set_user_metrics_size", "olc_read_life", "olc_nvrtc_check", "olc_bind_tissue",
     "olc_stage_rng", "olc_stage_keys", "olc_sort_scratch_bytes", "olc_stage_sort_pairs",
     "olc_stage_bin_ranges", "olc_stage_diffuse", "olc_stage_contact",
 )
@@ -144,6 +144,7 @@ _SIGS = {
     "olc_set_user_metrics_size": (C.c_int, [_VP, C.c_size_t]),
     "olc_read_life": (C.c_int, [_VP, _VP, C.c_uint32, _VP]),
     "olc_nvrtc_check": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t]),
+    "olc_bind_tissue": (C.c_int, [_VP, _VP, C.c_int, C.c_size_t]),
     "olc_stage_rng": (C.c_int, [_VP, C.c_uint32, C.c_int, _VP, _VP, _VP]),
     "olc_stage_keys": (C.c_int, [_VP, _VP, _VP, _VP, C.c_uint32, C.POINTER(OlcGeom), _VP, _VP]),
     "olc_sort_scratch_bytes": (C.c_size_t, [C.c_uint32, C.c_int]),

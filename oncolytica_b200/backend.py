@@ -245,8 +245,32 @@ class CudaBackend:
             self.fields_dev[i][cur].copy_(torch.from_numpy(flat))
             if self.fields_dev[i][2] is not None:
                 self.fields_dev[i][2].zero_()
+        self._upload_tissue()
         self.torch.cuda.synchronize(self.device)
         self._check(self.lib.olc_set_agent_count(self.handle, n, self._stream()))
+
+    def _upload_tissue(self) -> None:
+        """Tissue grid columns packed by tissue (Morton) key for tissue_at()."""
+        eng = self.engine
+        L = self.layout
+        if eng.tissue is None or not L.tissue_fields:
+            return
+        from oncolytica_b200._geometry import get_tissue_voxel_key, voxel_table_size
+
+        dims = eng.tissue_shape
+        v = voxel_table_size(dims)
+        ix, iy, iz = np.meshgrid(*(np.arange(d) for d in dims), indexing="ij")
+        keys = np.asarray(get_tissue_voxel_key(ix.ravel(), iy.ravel(), iz.ravel()), dtype=np.int64)
+        packed = np.zeros((len(L.tissue_fields), v), dtype=np.float32)
+        for i, name in enumerate(L.tissue_fields):
+            col = np.asarray(eng.tissue.column(name))
+            if col.dtype == np.float32:
+                packed[i, keys] = col.ravel(order="C")
+            else:
+                packed[i].view(np.int32)[keys] = col.astype(np.int32).ravel(order="C")
+        self.tissue_dev = self.torch.from_numpy(packed).to(self.device)
+        self._check(self.lib.olc_bind_tissue(self.handle, C.c_void_p(self.tissue_dev.data_ptr()),
+                                             len(L.tissue_fields), v * 4))
 
     def sync_to_host(self) -> None:
         """Device -> host agents (live only) and fields (replaces _gpu_backend.py:373-405)."""

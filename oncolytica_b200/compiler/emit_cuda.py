@@ -214,6 +214,24 @@ def pack_params(layout: ModelLayout, params_obj: Any) -> bytes:
 
 # ------------------------------------------------------------------ function sources
 
+def resolve_hints(fn, spec) -> dict:
+    """Type hints of a rule or helper.  String annotations (PEP 563) are
+    evaluated in the function's module plus the model's own classes, so models
+    whose classes are defined inside a function still resolve."""
+    fn = getattr(fn, "__func__", fn)
+    ns = dict(fn.__globals__)
+    for cls in (spec.cell_class, spec.tissue_class, spec.chemistry_class, spec.metrics_class, spec.params_class):
+        ns.setdefault(cls.__name__, cls)
+    out = {}
+    for name, ann in inspect.get_annotations(fn).items():
+        if isinstance(ann, str):
+            try:
+                ann = eval(ann, ns)  # noqa: S307 - the user's own annotation text
+            except Exception as exc:
+                raise CompilationError(f"cannot resolve annotation {ann!r} of {fn.__qualname__}: {exc}")
+        out[name] = ann
+    return out
+
 def func_ast(fn) -> tuple[ast.FunctionDef, str, str, int]:
     fn = getattr(fn, "__func__", fn)
     src = textwrap.dedent(inspect.getsource(fn))
@@ -291,7 +309,7 @@ class Translator:
 
     def _register(self, cname: str, fn, kind: str) -> FuncInfo:
         node, src, filename, line0 = func_ast(fn)
-        hints = typing.get_type_hints(fn)
+        hints = resolve_hints(fn, self.spec)
         params = []
         args = node.args.args
         start = 1  # skip self
@@ -353,7 +371,7 @@ class Translator:
             args = node.args.args
             if len(args) != 3:
                 raise CompilationError("a metric rule takes (self, item, metrics)", node, src, filename, line0)
-            hints = typing.get_type_hints(rule)
+            hints = resolve_hints(rule, self.spec)
             item_t = ty_of_py(hints.get(args[1].arg))
             if item_t != ("struct", "Cell"):
                 raise CompilationError("metric rules over tissue/chemistry voxels are not supported by this backend",
@@ -555,8 +573,9 @@ class Translator:
             {fn}(P, rng, ctx, c);
             c._rng_state = rng;
             olc_store_cell(P, i, c);
-            P.life[i] = ctx.dead ? 1 : 0;
-            if (P.posr) P.posr[i] = make_float4(c.pos.x, c.pos.y, c.pos.z, ctx.dead ? -1.0f : {radius});
+            const bool dead = ctx.dead || P.life[i] != 0;  // an earlier rule's die() stands
+            if (ctx.dead) P.life[i] = 1;
+            if (P.posr) P.posr[i] = make_float4(c.pos.x, c.pos.y, c.pos.z, dead ? -1.0f : {radius});
         }} else if (i < rows) {{
             olc_copy_row(P, i);  // child of an earlier rule this step: carried unchanged
         }}
@@ -625,8 +644,10 @@ class FuncEmitter:
         self.indent = 1
         self.tmp = 0
         self.loop_labels: list[str | None] = []
-        self.g = info.pyfunc.__globals__ if hasattr(info.pyfunc, "__globals__") else \
-            getattr(info.pyfunc, "__func__", info.pyfunc).__globals__
+        self.g = dict(getattr(info.pyfunc, "__func__", info.pyfunc).__globals__)
+        sp = tr.spec
+        for cls in (sp.cell_class, sp.tissue_class, sp.chemistry_class, sp.metrics_class, sp.params_class):
+            self.g.setdefault(cls.__name__, cls)
         self.self_kind = info.kind if info.kind in KINDS else "sim"
         self.main = info.params[0][0] if info.kind in ("rule", "metric") else None
         self.metrics_name = getattr(info, "metrics_name", None)

@@ -276,6 +276,7 @@ __global__ void __launch_bounds__(256) k_permute(const olc_u32* __restrict__ idx
     const olc_u32 n = counters[OLC_CTR_N];
     for (olc_u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const olc_u32 s = idx[i];
+        if (a.life) a.life[i] = 0;  // every row that survives the sort is alive; rules only set flags
         for (int c = 0; c < a.ncols; ++c)
             reinterpret_cast<olc_u32*>(a.dst[c])[i] = reinterpret_cast<const olc_u32*>(a.src[c])[s];
         if (a.write_posr) {

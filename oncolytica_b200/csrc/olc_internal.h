@@ -89,6 +89,7 @@ struct PermuteArgs {
     float radius_const;
     int write_posr;
     float4* posr;
+    unsigned char* life;
 };
 void launch_permute(const olc_u32* idx, olc_u32* counters, olc_u32 n_cap, const PermuteArgs& a,
                     cudaStream_t s);

@@ -55,6 +55,10 @@ struct OlcSim {
     OlcContact contact = {};
     ContactDev contact_dev = {};
 
+    const unsigned char* tissue = nullptr;  // borrowed tissue columns (Morton-indexed)
+    int tissue_cols = 0;
+    size_t tissue_stride = 0;
+
     // library-owned device memory
     olc_u32* counters = nullptr;
     unsigned char* life = nullptr;
@@ -152,7 +156,9 @@ OlcRuleParams make_rule_params(OlcSim* s, int rule_index, int in_buf) {
     P.birth_lb = s->birth_lb + (size_t)rule_index * s->rule_tiles;
     P.params = s->params_dev;
     P.metrics = s->metrics_dev;
-    P.tissue = nullptr;
+    P.tissue = s->tissue_cols > 0 ? s->tissue : nullptr;
+    P.n_tissue_cols = s->tissue_cols;
+    P.tissue_stride = (olc_u32)s->tissue_stride;
     for (int i = 0; i < 3; ++i) {
         P.tdims[i] = s->geom.tissue_dims[i];
         P.cdims[i] = s->geom.chem_dims[i];
@@ -214,6 +220,7 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
     pa.radius_const = s->contact.radius_const;
     pa.write_posr = (s->contact.enabled && s->n_cell_rules == 0) ? 1 : 0;
     pa.posr = s->posr;
+    pa.life = s->life;
     launch_permute(s->vals, s->counters, cap, pa, st);
     s->agent_cur = 1 - ac;
     // 3. cell rules
@@ -381,6 +388,16 @@ int olc_bind_field(OlcSim* s, int index, float* a, float* b, float* sink, const 
     s->fstep[index] = fs;
     s->field_cur[index] = 0;
     s->field_bound[index] = true;
+    return OLC_OK;
+}
+
+int olc_bind_tissue(OlcSim* s, const void* cols, int n_cols, size_t stride_bytes) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (n_cols < 0 || (n_cols > 0 && (!cols || stride_bytes < (size_t)s->n_table * 4)))
+        return fail(s, OLC_ERR_ARG, "olc_bind_tissue: columns must hold voxel_table_size entries");
+    s->tissue = static_cast<const unsigned char*>(cols);
+    s->tissue_cols = n_cols;
+    s->tissue_stride = stride_bytes;
     return OLC_OK;
 }
 

@@ -1,0 +1,188 @@
+"""The rule translator on CPU: rules translate to CUDA C that NVRTC compiles
+for sm_100a (no GPU needed), and unsupported constructs raise
+CompilationError with the offending line."""
+from __future__ import annotations
+
+import ctypes as C
+from types import SimpleNamespace
+
+import pytest
+
+import oncolytica_b200 as ol
+from oncolytica_b200 import _lib
+from oncolytica_b200 import workloads as W
+from oncolytica_b200.compiler.emit_cuda import make_layout, pack_params, translate_model
+
+
+def _translate(sim_cls, radius=None):
+    sim = sim_cls()
+    rules = {"cell": [], "metric": []}
+    for name in dir(sim):
+        m = getattr(sim, name, None)
+        kind = getattr(m, "_rule_type", None)
+        if kind in rules:
+            rules[kind].append(m)
+    sim._engine = SimpleNamespace(_cell_rules=rules["cell"], _metric_rules=rules["metric"])
+    layout = make_layout(sim._spec, radius)
+    return translate_model(sim, layout, radius)
+
+
+def _nvrtc_ok(prog):
+    log = C.create_string_buffer(1 << 16)
+    rc = _lib.load().olc_nvrtc_check(prog.source.encode(), _lib.CSRC_DIR.encode(), log, len(log))
+    assert rc == 0, log.value.decode()[:3000]
+
+
+def test_tumour_models_compile():
+    for cls in (W.TumourSim, W.TumourDrugSim):
+        prog = _translate(cls, "radius")
+        assert [k for k, _ in prog.kernels] == ["Kernel_CellRule_0", "Kernel_MetricRule_0"]
+        assert prog.sink_fields == {"o2"}
+        _nvrtc_ok(prog)
+
+
+# ---- a model exercising helpers, tuples, neighbours, loops and casts ----
+
+K_HILL: ol.f32 = 100.0
+TYPE_A: ol.i32 = 1
+
+
+class GTissue(ol.Tissue):
+    capacity: ol.i32 = 10
+
+    def crowded(self, n: ol.i32) -> ol.bool:
+        return n >= self.capacity
+
+
+class GChem(ol.Chemistry):
+    pdgf: ol.f32 = 0.0
+
+
+class GCell(ol.Cell):
+    pos: ol.vec3
+    kind: ol.i32 = 0
+    clock: ol.f32 = 0.0
+    moving: ol.bool = False
+    p_pot: ol.f32 = 0.025
+
+    def gamma(self, c: ol.f32) -> ol.f32:
+        return c / (c + K_HILL)
+
+    def phenotype(self, c: ol.f32, am: ol.bool) -> tuple[ol.f32, ol.f32]:
+        g: ol.f32 = self.gamma(c)
+        p: ol.f32 = self.p_pot * g
+        m: ol.f32 = p * (0.1 if am else 1.0)
+        return p, m
+
+    def tick(self, p: ol.f32):
+        self.clock += p
+        if self.clock >= 1.0:
+            self.clock -= 1.0
+            self.spawn()
+
+    def spawn(self):
+        angle: ol.f32 = ol.random() * 6.2831853
+        child: GCell = GCell(pos=self.pos + ol.vec3(ol.math.cos(angle), ol.math.sin(angle), 0.0), kind=self.kind)
+        self.divide(child)
+
+
+class GMetrics(ol.Metrics):
+    count: ol.i32 = 0
+    total: ol.f32 = 0.0
+
+
+class GParams(ol.Params):
+    am: ol.bool = False
+    scale: ol.f32 = 2.0
+
+
+class GSim(ol.Simulation[GTissue, GChem, GCell, GMetrics, GParams]):
+    def clamp01(self, v: ol.f32) -> ol.f32:
+        return ol.math.clamp(v, 0.0, 1.0)
+
+    @ol.cell_rule
+    def behave(self, cell: GCell):
+        chem: GChem = self.chemistry_at(cell.pos)
+        tissue: GTissue = self.tissue_at(cell.pos)
+        p, m = cell.phenotype(chem.pdgf, self.params.am)
+        active: ol.i32 = 0
+        for nb in cell.neighbors:
+            if nb.kind != 0:
+                active += 1
+            if active > 20:
+                break
+        total: ol.f32 = 0.0
+        for i in range(3):
+            total += float(i) * 0.5
+        if not tissue.crowded(active):
+            cell.tick(self.clamp01(p * self.params.scale + total))
+        cell.moving = not cell.moving
+        if cell.moving and m > 0.0:
+            cell.pos.x = ol.math.clamp(cell.pos.x + m, 0.0, 100.0)
+        q = 7 // 2 + 7 % 3
+        if q == 5 and cell.kind == TYPE_A and chem.pdgf < -1.0:
+            cell.die()
+
+    @ol.metric_rule
+    def collect(self, cell: GCell, mt: GMetrics):
+        mt.count += 1
+        mt.total += cell.clock
+
+
+def test_rich_model_compiles():
+    prog = _translate(GSim)
+    src = prog.source
+    assert "cell_phenotype" in src and "gtissue" not in src.lower().replace("tissue_t", "")
+    assert "Tup_f32_f32" in src
+    assert "olc_tissue_key" in src  # neighbour loop
+    _nvrtc_ok(prog)
+
+
+def test_params_blob_layout():
+    prog = _translate(GSim)
+    blob = pack_params(prog.layout, GParams(am=True, scale=3.0))
+    assert len(blob) == 8
+    import numpy as np
+
+    assert np.frombuffer(blob[:4], np.int32)[0] == 1  # "am" sorts first
+    assert np.frombuffer(blob[4:], np.float32)[0] == np.float32(3.0)
+
+
+# ---- errors ----------------------------------------------------------------
+
+class ECell(ol.Cell):
+    pos: ol.vec3
+    n: ol.i32 = 0
+
+
+class EMetrics(ol.Metrics):
+    c: ol.i32 = 0
+
+
+class EParams(ol.Params):
+    pass
+
+
+def _err_sim(body):
+    ns = {}
+    src = ("class S(ol.Simulation[GTissue, GChem, ECell, EMetrics, EParams]):\n"
+           "    @ol.cell_rule\n"
+           "    def rule(self, cell: ECell):\n" + "".join("        " + line + "\n" for line in body.splitlines()))
+    import linecache
+
+    fname = f"<err-model-{abs(hash(src))}>"
+    linecache.cache[fname] = (len(src), None, src.splitlines(True), fname)
+    exec(compile(src, fname, "exec"), {**globals(), "ol": ol}, ns)
+    return ns["S"]
+
+
+@pytest.mark.parametrize("body,msg", [
+    ("cell.n = 1.5", "float -> int"),
+    ("x = undefined_name + 1", "unknown name"),
+    ("for c in self.cells:\n    pass", ""),
+    ("cell.n = len([1])", ""),
+    ("with open('f') as f:\n    pass", "unsupported statement"),
+])
+def test_unsupported_constructs_raise(body, msg):
+    with pytest.raises(ol.CompilationError, match=msg):
+        _translate(_err_sim(body))
