@@ -1,0 +1,362 @@
+#!/usr/bin/env python
+"""Benchmark of the Oncolytica step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload scale|plain_small]
+    python bench.py --impl reference ...        # the CPU reference arm
+
+A step is one simulation step of the tumour-spheroid workload (fields, grid,
+rule, contact).  The default workload ``scale`` is 1,000,000 agents with two
+256^3 FP32 fields (O2 and drug).  ``value`` is agent-steps/s of the whole job
+(sum over replicas / max device time over ranks) with the state resident in
+HBM; ``e2e`` runs the same steps through Engine.run_step(collect_metrics=True)
+with a parameter upload from host memory before each step and the metric
+readback after it.  One JSON line is printed by rank 0.
+
+Multi-GPU: the step does not shard (the stencil and the agents share one
+domain), so N GPUs run N independent replicas (different seeds), no
+collective in the step ("replicas only"); the timed region is bracketed by
+barriers and the slowest rank's device time is used.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from dataclasses import replace
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "agent-steps/s + voxel-updates/s, plain FP32 on 1 B200"
+UNIT = "agent-steps/s"
+
+
+def parse() -> argparse.Namespace:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="scale")
+    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def env_ranks() -> tuple[int, int, int]:
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "src": "measured"}
+    return {"hbm_gbs": 6650.0, "src": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def start(self) -> None:
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "50"]
+        if self.gpu_id:
+            cmd += ["-i", self.gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx.append(float(f[2]))
+                except ValueError:
+                    continue
+                for name, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def read_traffic(kernel: str, nvox: int) -> int | None:
+    """DRAM bytes per launch of `kernel` from a committed ncu summary
+    (profiles/<kernel>*.txt line "dram_bytes_per_launch <bytes> voxels <n>"),
+    scaled to this workload's voxels."""
+    d = os.path.join(REPO, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for name in sorted(os.listdir(d)):
+        if not (name.startswith(kernel) and name.endswith(".txt")):
+            continue
+        with open(os.path.join(d, name)) as fh:
+            for line in fh:
+                p = line.split()
+                if len(p) >= 4 and p[0] == "dram_bytes_per_launch" and p[2] == "voxels":
+                    return int(round(int(p[1]) * nvox / int(p[3])))
+    return None
+
+
+# ------------------------------------------------------------------ CPU (oracle) timing
+
+def time_oracle_step(spec, orc, nthreads: int = 0, field_sample: int = 2) -> dict:
+    """One bounded sample of a step on the host: the full agent phase, and
+    `field_sample` substeps per field scaled to the full substep count."""
+    t0 = time.perf_counter()
+    orc.agents_part(nthreads)
+    t_agents = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    orc.fields_sample(field_sample, nthreads)
+    t_fields_sample = time.perf_counter() - t0
+    full = spec.S_o2 + (spec.S_drug if spec.has_drug else 0)
+    sample = field_sample * (2 if spec.has_drug else 1)
+    t_fields = t_fields_sample * full / sample
+    return {"t_agents": t_agents, "t_fields": t_fields, "agents": int(orc.rows)}
+
+
+def make_oracle(spec):
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle  # the CPU restatement (checker and CPU baseline only)
+
+    from oncolytica_b200 import workloads as W
+
+    st = W.initial_state(spec)
+    o2, drug = W.initial_fields(spec)
+    return oracle.TumourOracle(spec, st, o2, drug, spec.capacity)
+
+
+def cpu_baseline(spec, samples: int = 1) -> dict:
+    orc = make_oracle(spec)
+    cores = os.cpu_count() or 1
+    tot_t, tot_a = 0.0, 0
+    for _ in range(samples):
+        r = time_oracle_step(spec, orc)
+        tot_t += r["t_agents"] + r["t_fields"]
+        tot_a += r["agents"]
+    return {"value": tot_a / tot_t, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{samples} step(s) of {spec.name}: full agent phase ({spec.n_agents} agents, sort + rule + "
+                      f"contact) plus 2 substeps per field scaled to {spec.S_o2}+{spec.S_drug} substeps; "
+                      f"C oracle, OpenMP on {cores} threads"}
+
+
+def run_reference(args) -> None:
+    rank, world, _ = env_ranks()
+    if rank != 0:
+        return
+    from oncolytica_b200 import workloads as W
+
+    spec = W.CONFIGS[args.workload]
+    orc = make_oracle(spec)
+    cores = os.cpu_count() or 1
+    for _ in range(max(0, min(args.warmup, 1))):
+        time_oracle_step(spec, orc)
+    tot_t, tot_a = 0.0, 0
+    for _ in range(args.steps):
+        r = time_oracle_step(spec, orc)
+        tot_t += r["t_agents"] + r["t_fields"]
+        tot_a += r["agents"]
+    value = tot_a / tot_t
+    vox = spec.voxel_updates_per_step() * args.steps / tot_t
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (numpy default_rng, seed 0)",
+            "config": {"workload": spec.name, "agents": spec.n_agents,
+                       "fields": "o2+drug" if spec.has_drug else "o2", "field_dims": list(spec.field_dims),
+                       "substeps": [spec.S_o2, spec.S_drug]},
+            "voxel_updates_per_s": vox,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "each step: the full agent phase plus 2 substeps per field scaled to the "
+                                       "full substep count; C oracle (the reference's algorithm restated; the "
+                                       "reference's own GPU path needs a graphics adapter, unavailable here)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+
+def run_b200(args) -> None:
+    import torch
+
+    rank, world, local = env_ranks()
+    if world != args.gpus and not (world == 1 and args.gpus == 1):
+        print(f"warning: --gpus {args.gpus} but WORLD_SIZE={world}", file=sys.stderr)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from oncolytica_b200 import workloads as W
+
+    base = W.CONFIGS[args.workload]
+    spec = replace(base, seed=base.seed + rank)
+    eng = W.build_engine(spec)
+    be = eng._backend_impl
+    dev = torch.device("cuda", local)
+    props = torch.cuda.get_device_properties(dev)
+    gpu_id = None
+    try:
+        gpu_id = "GPU-" + str(props.uuid)
+    except Exception:
+        pass
+
+    # warm-up (untimed)
+    eng.run_steps(args.warmup)
+    torch.cuda.synchronize(dev)
+    c0 = be.counters()
+    be.set_profiling(True)
+    stream = torch.cuda.current_stream(dev)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(gpu_id)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    start.record(stream)
+    eng.run_steps(args.steps)
+    end.record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+    ms = start.elapsed_time(end)
+    c1 = be.counters()
+    prof = be.profile()
+    be.set_profiling(False)
+    agent_steps = c1["agent_steps"] - c0["agent_steps"]
+    vox = spec.voxel_updates_per_step() * args.steps
+    tot = torch.tensor([ms, float(agent_steps), float(vox)], dtype=torch.float64, device=dev)
+    if dist:
+        mx = tot.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        ms_max = float(mx[0])
+    else:
+        ms_max = float(tot[0])
+    total_agent_steps, total_vox = float(tot[1]), float(tot[2])
+    value = total_agent_steps / (ms_max / 1e3)
+
+    # e2e through the public API: params H2D before, metrics D2H after each step
+    from oncolytica_b200.compiler.emit_cuda import pack_params
+
+    params = eng._sim._params
+    kw = {k: getattr(params, k) for k in eng._sim._params.__dataclass_fields__}
+    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    torch.cuda.synchronize(dev)
+    c2 = be.counters()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        eng.update_params(**kw)
+        eng.run_step(collect_metrics=True)
+    torch.cuda.synchronize(dev)
+    e2e_s = time.perf_counter() - t0
+    c3 = be.counters()
+    e2e_agents = c3["agent_steps"] - c2["agent_steps"]
+    t2 = torch.tensor([e2e_s, float(e2e_agents)], dtype=torch.float64, device=dev)
+    if dist:
+        m2 = t2.clone()
+        dist.all_reduce(m2, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t2, op=dist.ReduceOp.SUM)
+        e2e_s = float(m2[0])
+    e2e_value = float(t2[1]) / e2e_s
+    h2d = len(pack_params(be.layout, params))
+    d2h = 4 * max(1, len(be.layout.metrics))
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    # roofline of the dominant kernel (the 7-point substep)
+    import numpy as np
+
+    nvox = int(np.prod(spec.field_dims))
+    peaks = measured_peaks()
+    sub_ms = prof["ms_substeps"] / max(1, prof["substep_launches"])
+    alg_bytes = 8 * nvox  # stream model: read 4 B + write 4 B per voxel (FP32)
+    achieved = alg_bytes / (sub_ms / 1e3) / 1e9
+    traffic = read_traffic("k_substep", nvox)
+    steps_done = max(1, prof["steps"])
+    stages = {k[3:]: prof[k] / steps_done for k in ("ms_sink", "ms_substeps", "ms_grid", "ms_rules",
+                                                     "ms_contact", "ms_collect")}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (numpy default_rng, seed 0 + rank)",
+        "config": {"workload": spec.name, "agents": spec.n_agents, "fields": "o2+drug" if spec.has_drug else "o2",
+                   "field_dims": list(spec.field_dims), "substeps": [spec.S_o2, spec.S_drug],
+                   "bins": list(spec.tissue_dims), "l2": "inputs larger than L2 (field state "
+                   f"{(5 if spec.has_drug else 3) * 4 * nvox / 1e6:.0f} MB)",
+                   "parallelism": f"replicas x{world}"},
+        "voxel_updates_per_s": total_vox / (ms_max / 1e3),
+        "agents_end": c1["n_agents"],
+        "roofline": {"bound": "hbm", "kernel": "k_substep (7-point FTCS, FP32)", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                     "peak_src": peaks["src"], "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                     "launch_ms": sub_ms},
+        "stages_ms_per_step": stages,
+        "gpu_launches": int(prof["kernel_launches"]),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps, "api": "Engine.update_params + Engine.run_step(collect_metrics=True)"},
+        "clocks": clk,
+        "status": c1["status"],
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(spec)
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -118,7 +118,22 @@ typedef struct {
     uint32_t status;            /* OLC_STATUS_* bits (sticky)                 */
     uint32_t pad;
     uint64_t steps;             /* steps run on this handle                   */
+    uint64_t agent_steps;       /* sum over steps of live agents at the rule  */
 } OlcCounters;
+
+/* Stage timing of the steps run since profiling was enabled (CUDA events
+ * recorded on the step's stream around each stage). */
+typedef struct {
+    uint32_t steps;
+    uint32_t substep_launches;  /* 7-point substep kernels                    */
+    uint64_t kernel_launches;   /* all kernels this library launched          */
+    double   ms_sink;
+    double   ms_substeps;
+    double   ms_grid;           /* keys, sort, bin table, permute             */
+    double   ms_rules;
+    double   ms_contact;
+    double   ms_collect;        /* reductions and metric rules                */
+} OlcProfile;
 
 /* Per-step reductions (engine metrics, tumor_sim.wgsl:248-361, restated as
  * exact integer counts and FP64 sums). */
@@ -197,6 +212,11 @@ int olc_step(OlcSim* sim, int nsteps, int collect, void* stream);
 
 /* Synchronises `stream` and copies the counters. */
 int olc_read_counters(OlcSim* sim, OlcCounters* out, void* stream);
+
+/* Enables (1) or disables (0) stage timing; enabling clears what was
+ * recorded.  olc_read_profile synchronises and sums the recorded steps. */
+int olc_set_profiling(OlcSim* sim, int enable);
+int olc_read_profile(OlcSim* sim, OlcProfile* out);
 
 /* Copies the last step's reductions / metric-rule accumulators to host memory
  * (replaces the MetricsBuffer readback, _gpu_backend.py:166-169). */

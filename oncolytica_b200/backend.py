@@ -191,7 +191,15 @@ class CudaBackend:
         c = _lib.OlcCounters()
         self._check(self.lib.olc_read_counters(self.handle, C.byref(c), self._stream()))
         return {"n_agents": c.n_agents, "births": c.births, "deaths": c.deaths, "status": c.status,
-                "steps": c.steps}
+                "steps": c.steps, "agent_steps": c.agent_steps}
+
+    def set_profiling(self, enable: bool) -> None:
+        self._check(self.lib.olc_set_profiling(self.handle, int(bool(enable))))
+
+    def profile(self) -> dict:
+        p = _lib.OlcProfile()
+        self._check(self.lib.olc_read_profile(self.handle, C.byref(p)))
+        return {k: getattr(p, k) for k, _ in _lib.OlcProfile._fields_}
 
     def get_reductions(self) -> dict:
         r = _lib.OlcReductions()

@@ -119,6 +119,18 @@ void launch_substep(const float* in, float* out, const FieldStep& fs, cudaStream
                                                        fs.inv_decay, fs.bval);
 }
 
+float* run_substeps(float* a, float* b, const FieldStep& fs, cudaStream_t s) {
+    float* cur = a;
+    float* nxt = b;
+    for (int i = 0; i < fs.substeps; ++i) {
+        launch_substep(cur, nxt, fs, s);
+        float* t = cur;
+        cur = nxt;
+        nxt = t;
+    }
+    return cur;
+}
+
 float* run_field_step(float* a, float* b, float* sink, const FieldStep& fs, cudaStream_t s) {
     launch_sink(a, sink, fs, s);
     float* cur = a;

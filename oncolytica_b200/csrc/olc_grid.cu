@@ -148,6 +148,7 @@ __global__ void __launch_bounds__(256) k_scan_hist(const olc_u32* __restrict__ h
         olc_u32 dead = counters[OLC_CTR_DEAD_TMP];
         counters[OLC_CTR_ROWS] = rows;
         counters[OLC_CTR_N] = rows - dead;
+        *reinterpret_cast<unsigned long long*>(counters + OLC_CTR_AGENT_STEPS) += (unsigned long long)(rows - dead);
         counters[OLC_CTR_DEAD] = dead;
         counters[OLC_CTR_DEAD_TMP] = 0u;
         for (int j = 0; j < OLC_MAX_RULE_KERNELS; ++j) {

@@ -109,6 +109,8 @@ void launch_sink(float* f, float* sink, const FieldStep& fs, cudaStream_t s);
 void launch_substep(const float* in, float* out, const FieldStep& fs, cudaStream_t s);
 // Runs sink + S substeps starting from a; returns the buffer holding the result.
 float* run_field_step(float* a, float* b, float* sink, const FieldStep& fs, cudaStream_t s);
+// The S substeps alone.
+float* run_substeps(float* a, float* b, const FieldStep& fs, cudaStream_t s);
 
 // ------------------------------------------------------------------ contact
 struct ContactDev {

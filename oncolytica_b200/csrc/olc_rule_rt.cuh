@@ -29,6 +29,7 @@
 #define OLC_CTR_SORT_TILE  8    // 4 words: tile counters of the sort passes
 #define OLC_CTR_RULE_TILE  12   // OLC_MAX_RULE_KERNELS words: tile counters
 #define OLC_CTR_BIRTHS     28   // OLC_MAX_RULE_KERNELS words: births per rule
+#define OLC_CTR_AGENT_STEPS 60  // 2 words (u64): sum of N over steps
 #define OLC_CTR_WORDS      64
 
 #define OLC_RULE_THREADS 256

@@ -15,6 +15,7 @@
 
 #include <nvrtc.h>
 
+#include <array>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -34,6 +35,8 @@ int cuda_status(cudaError_t e, const char* what) {
 }  // namespace olc
 
 using namespace olc;
+
+#define OLC_PROF_EVENTS 7
 
 struct OlcSim {
     OlcGeom geom;
@@ -86,7 +89,15 @@ struct OlcSim {
     int n_cell_rules = 0;
 
     uint64_t steps = 0;
+    uint64_t total_launches = 0;
     std::string err;
+
+    // stage profiling
+    bool profiling = false;
+    int prof_step = 0;
+    uint64_t prof_launches = 0;
+    uint32_t prof_substeps = 0;
+    std::vector<std::array<cudaEvent_t, OLC_PROF_EVENTS>> events;
 };
 
 namespace {
@@ -187,17 +198,42 @@ int launch_rule(OlcSim* s, int k, const OlcRuleParams& P, cudaStream_t st) {
                  "cudaLaunchKernel(rule)");
 }
 
+// Records stage event `k` of the current profiled step.
+void mark(OlcSim* s, int k, cudaStream_t st) {
+    if (!s->profiling) return;
+    cudaEventRecord(s->events[s->prof_step][k], st);
+}
+
 int step_once(OlcSim* s, int collect, cudaStream_t st) {
     const olc_u32 cap = s->caps.max_agents;
-    // 1. fields
+    if (s->profiling) {
+        if ((size_t)s->prof_step >= s->events.size()) {
+            std::array<cudaEvent_t, OLC_PROF_EVENTS> ev;
+            for (auto& e : ev) OLC_TRY(check(s, cudaEventCreate(&e), "cudaEventCreate"));
+            s->events.push_back(ev);
+        }
+    }
+    uint64_t launches = 0;
+    uint32_t substeps = 0;
+    mark(s, 0, st);
+    // 1. fields: implicit sinks, then the substeps of every field
+    for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
+        if (!s->field_bound[f] || s->fstep[f].substeps == 0 || !s->sink[f]) continue;
+        launch_sink(s->field[s->field_cur[f]][f], s->sink[f], s->fstep[f], st);
+        ++launches;
+    }
+    mark(s, 1, st);
     for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
         if (!s->field_bound[f] || s->fstep[f].substeps == 0) continue;  // unbound or static
         int cur = s->field_cur[f];
         float* a = s->field[cur][f];
         float* b = s->field[1 - cur][f];
-        float* res = run_field_step(a, b, s->sink[f], s->fstep[f], st);
+        float* res = run_substeps(a, b, s->fstep[f], st);
         s->field_cur[f] = (res == a) ? cur : 1 - cur;
+        substeps += (uint32_t)s->fstep[f].substeps;
     }
+    launches += substeps;
+    mark(s, 2, st);
     // 2. grid + compaction
     const int passes = (s->key_bits + 7) / 8;
     const int ac = s->agent_cur;
@@ -223,6 +259,8 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
     pa.life = s->life;
     launch_permute(s->vals, s->counters, cap, pa, st);
     s->agent_cur = 1 - ac;
+    launches += 4 + (uint64_t)passes;  // keys, scan, passes, bin table, permute
+    mark(s, 3, st);
     // 3. cell rules
     if (s->n_cell_rules > 0) {
         OLC_TRY(check(s, cudaMemsetAsync(s->birth_lb, 0, (size_t)s->n_cell_rules * s->rule_tiles * 4, st),
@@ -235,17 +273,22 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
         OLC_TRY(launch_rule(s, (int)k, P, st));
         s->agent_cur = 1 - s->agent_cur;
         ++cell_idx;
+        ++launches;
     }
+    mark(s, 4, st);
     // 4. contact
     const int cc = s->agent_cur;
     if (s->contact.enabled) {
         launch_contact(s->posr, s->ranges, s->counters + OLC_CTR_N, 0, cap, s->contact_dev,
                        static_cast<float*>(s->col[cc][0]), static_cast<float*>(s->col[cc][1]),
                        static_cast<float*>(s->col[cc][2]), st);
+        ++launches;
     }
+    mark(s, 5, st);
     // 5. reductions + metric rules
     if (collect) {
         launch_reset_reductions(s->red_dev, (int)s->caps.n_fields, st);
+        launches += 2;
         ReduceArgs ra;
         ra.x = static_cast<const float*>(s->col[cc][0]);
         ra.y = static_cast<const float*>(s->col[cc][1]);
@@ -261,6 +304,7 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
             if (!s->field_bound[f]) continue;
             const size_t nvox = (size_t)s->geom.chem_dims[0] * s->geom.chem_dims[1] * s->geom.chem_dims[2];
             launch_reduce_field(s->field[s->field_cur[f]][f], nvox, (int)f, s->red_dev, st);
+            ++launches;
         }
         if (s->metrics_dev && s->metrics_bytes) {
             OLC_TRY(check(s, cudaMemsetAsync(s->metrics_dev, 0, s->metrics_bytes, st), "memset metrics"));
@@ -269,8 +313,16 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
             if (s->kinds[k] != 1) continue;
             OlcRuleParams P = make_rule_params(s, 0, cc);
             OLC_TRY(launch_rule(s, (int)k, P, st));
+            ++launches;
         }
     }
+    mark(s, 6, st);
+    if (s->profiling) {
+        s->prof_step++;
+        s->prof_launches += launches;
+        s->prof_substeps += substeps;
+    }
+    s->total_launches += launches;
     s->steps++;
     return check(s, cudaGetLastError(), "step launch");
 }
@@ -343,6 +395,8 @@ int olc_destroy(OlcSim* s) {
     if (!s) return OLC_OK;
     cudaDeviceSynchronize();
     if (s->module) cudaLibraryUnload(s->module);
+    for (auto& ev : s->events)
+        for (auto e : ev) cudaEventDestroy(e);
     cudaFree(s->counters);
     cudaFree(s->life);
     cudaFree(s->keys_in);
@@ -540,10 +594,13 @@ int olc_set_agent_count(OlcSim* s, uint32_t n, void* stream) {
     OLC_TRY(check(s, cudaStreamSynchronize(st), "sync"));
     OLC_TRY(check(s, cudaMemcpy(words, s->counters, sizeof(words), cudaMemcpyDeviceToHost), "read counters"));
     const olc_u32 status = words[OLC_CTR_STATUS];
+    const olc_u32 as_lo = words[OLC_CTR_AGENT_STEPS], as_hi = words[OLC_CTR_AGENT_STEPS + 1];
     std::memset(words, 0, sizeof(words));
     words[OLC_CTR_N] = n;
     words[OLC_CTR_ROWS] = n;
     words[OLC_CTR_STATUS] = status;
+    words[OLC_CTR_AGENT_STEPS] = as_lo;
+    words[OLC_CTR_AGENT_STEPS + 1] = as_hi;
     OLC_TRY(check(s, cudaMemcpy(s->counters, words, sizeof(words), cudaMemcpyHostToDevice), "write counters"));
     OLC_TRY(check(s, cudaMemset(s->life, 0, s->caps.max_agents), "memset life"));
     return OLC_OK;
@@ -586,6 +643,36 @@ int olc_read_counters(OlcSim* s, OlcCounters* out, void* stream) {
     out->status = w[OLC_CTR_STATUS];
     out->pad = 0;
     out->steps = s->steps;
+    out->agent_steps = (uint64_t)w[OLC_CTR_AGENT_STEPS] | ((uint64_t)w[OLC_CTR_AGENT_STEPS + 1] << 32);
+    return OLC_OK;
+}
+
+int olc_set_profiling(OlcSim* s, int enable) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    OLC_TRY(check(s, cudaDeviceSynchronize(), "sync"));
+    s->profiling = enable != 0;
+    s->prof_step = 0;
+    s->prof_launches = 0;
+    s->prof_substeps = 0;
+    return OLC_OK;
+}
+
+int olc_read_profile(OlcSim* s, OlcProfile* out) {
+    if (!s || !out) return fail(s, OLC_ERR_ARG, "olc_read_profile: null argument");
+    std::memset(out, 0, sizeof(*out));
+    double* slots[6] = {&out->ms_sink, &out->ms_substeps, &out->ms_grid, &out->ms_rules, &out->ms_contact,
+                        &out->ms_collect};
+    for (int i = 0; i < s->prof_step; ++i) {
+        OLC_TRY(check(s, cudaEventSynchronize(s->events[i][OLC_PROF_EVENTS - 1]), "event sync"));
+        for (int k = 0; k < 6; ++k) {
+            float ms = 0.0f;
+            OLC_TRY(check(s, cudaEventElapsedTime(&ms, s->events[i][k], s->events[i][k + 1]), "elapsed"));
+            *slots[k] += ms;
+        }
+    }
+    out->steps = (uint32_t)s->prof_step;
+    out->substep_launches = s->prof_substeps;
+    out->kernel_launches = s->prof_launches;
     return OLC_OK;
 }
 

@@ -253,6 +253,23 @@ class TumourOracle:
         if lib().orc_tumour_fields(C.byref(self.t), nthreads) != 0:
             raise RuntimeError("oracle fields failed")
 
+    def fields_sample(self, substeps: int, nthreads: int = 0) -> None:
+        """`substeps` substeps of every field in place, at the same diffusion
+        number as the full step (dt scaled by substeps / S) — a bounded sample
+        of the field phase for timing."""
+        sp = self.spec
+        dims = np.array(sp.field_dims, dtype=np.int32)
+        L = lib()
+        for f, tmp, D, decay, bnd, S in ((self.o2, self.o2_tmp, sp.D_o2, 0.0, sp.bnd_o2, sp.S_o2),
+                                         (self.drug, self.drug_tmp, sp.D_drug, sp.decay_drug, sp.bnd_drug,
+                                          sp.S_drug)):
+            if S == 0 or f.size < 8:
+                continue
+            rc = L.orc_diffuse(_p(f), _p(tmp), None, _p(dims), C.c_float(sp.dx), C.c_float(sp.dt * substeps / S),
+                               C.c_float(D), C.c_float(decay), C.c_float(bnd), substeps, nthreads)
+            if rc != 0:
+                raise RuntimeError("oracle fields sample failed")
+
     def agents_part(self, nthreads: int = 0):
         rc = lib().orc_tumour_agents(C.byref(self.t), nthreads)
         self._sync_after()

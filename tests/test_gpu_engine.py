@@ -288,6 +288,10 @@ def test_tumour_step_parity_with_oracle(cuda):
 
     spec = _parity_spec()
     eng = W.build_engine(spec)
+    # an O2 ramp along x puts agents in every branch of the rule
+    x = (np.arange(spec.field_dims[0], dtype=np.float32) + 0.5) / spec.field_dims[0]
+    eng.chemistry.column("o2")[...] = np.clip(2.2 * x - 0.6, 0.0, 1.0)[:, None, None]
+    eng.sync_to_device()
     be = eng._backend_impl
     seen = {"div": 0, "dead": 0, "quiescent": 0, "necrotic": 0}
     for step in range(6):

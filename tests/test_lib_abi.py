@@ -33,7 +33,8 @@ def test_struct_sizes_match_header_layout():
     assert C.sizeof(_lib.OlcCaps) == 4 * 9
     assert C.sizeof(_lib.OlcDiffusion) == 20
     assert C.sizeof(_lib.OlcContact) == 28
-    assert C.sizeof(_lib.OlcCounters) == 32
+    assert C.sizeof(_lib.OlcCounters) == 40
+    assert C.sizeof(_lib.OlcProfile) == 16 + 6 * 8
 
 
 def test_version_string(olc):
