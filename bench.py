@@ -43,7 +43,7 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="scale")
-    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="0 = as many as --steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -276,12 +276,17 @@ def run_b200(args) -> None:
     total_agent_steps, total_vox = float(tot[1]), float(tot[2])
     value = total_agent_steps / (ms_max / 1e3)
 
-    # e2e through the public API: params H2D before, metrics D2H after each step
+    # e2e through the public API on a fresh engine over the same warm-up and
+    # steps as the timed region: params H2D before, metrics D2H after each step
     from oncolytica_b200.compiler.emit_cuda import pack_params
 
+    del eng, be
+    eng = W.build_engine(spec)
+    be = eng._backend_impl
+    eng.run_steps(args.warmup)
     params = eng._sim._params
     kw = {k: getattr(params, k) for k in eng._sim._params.__dataclass_fields__}
-    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    e2e_steps = args.steps if args.e2e_steps <= 0 else max(1, min(args.e2e_steps, args.steps))
     torch.cuda.synchronize(dev)
     c2 = be.counters()
     if dist:

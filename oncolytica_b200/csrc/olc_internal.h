@@ -1,5 +1,6 @@
 // Host-side declarations shared by the translation units of libolc.so.
 #pragma once
+#include <cuda.h>  // CUtensorMap type; no driver-library link (entry points via the runtime)
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stddef.h>
@@ -111,6 +112,13 @@ void launch_substep(const float* in, float* out, const FieldStep& fs, cudaStream
 float* run_field_step(float* a, float* b, float* sink, const FieldStep& fs, cudaStream_t s);
 // The S substeps alone.
 float* run_substeps(float* a, float* b, const FieldStep& fs, cudaStream_t s);
+// TMA tile path: a tensor map per buffer (x extent must be a multiple of 4).
+bool make_field_map(CUtensorMap* map, float* base, const int dims[3]);
+float* run_substeps_tma(float* a, float* b, const CUtensorMap& map_a, const CUtensorMap& map_b,
+                        const FieldStep& fs, olc_u32* status, cudaStream_t s);
+// OLC_STENCIL=plain in the environment selects the register-column kernel.
+bool stencil_tma_enabled();
+olc_u32* stage_status_word();
 
 // ------------------------------------------------------------------ contact
 struct ContactDev {

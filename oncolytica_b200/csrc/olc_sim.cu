@@ -54,6 +54,8 @@ struct OlcSim {
     FieldStep fstep[OLC_MAX_FIELDS] = {};
     int field_cur[OLC_MAX_FIELDS] = {};
     bool field_bound[OLC_MAX_FIELDS] = {};
+    CUtensorMap fmap[2][OLC_MAX_FIELDS];      // TMA descriptors of both buffers
+    bool fmap_ok[OLC_MAX_FIELDS] = {};
 
     OlcContact contact = {};
     ContactDev contact_dev = {};
@@ -228,7 +230,10 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
         int cur = s->field_cur[f];
         float* a = s->field[cur][f];
         float* b = s->field[1 - cur][f];
-        float* res = run_substeps(a, b, s->fstep[f], st);
+        float* res = (s->fmap_ok[f] && stencil_tma_enabled())
+                         ? run_substeps_tma(a, b, s->fmap[cur][f], s->fmap[1 - cur][f], s->fstep[f],
+                                            s->counters + OLC_CTR_STATUS, st)
+                         : run_substeps(a, b, s->fstep[f], st);
         s->field_cur[f] = (res == a) ? cur : 1 - cur;
         substeps += (uint32_t)s->fstep[f].substeps;
     }
@@ -437,6 +442,8 @@ int olc_bind_field(OlcSim* s, int index, float* a, float* b, float* sink, const 
     if (spec->has_sink && !sink) return fail(s, OLC_ERR_ARG, "olc_bind_field: has_sink without a sink buffer");
     s->field[0][index] = a;
     s->field[1][index] = b;
+    s->fmap_ok[index] = spec->substeps > 0 && make_field_map(&s->fmap[0][index], a, s->geom.chem_dims) &&
+                        make_field_map(&s->fmap[1][index], b, s->geom.chem_dims);
     s->sink[index] = spec->has_sink ? sink : nullptr;
     s->fspec[index] = *spec;
     s->fstep[index] = fs;
@@ -762,7 +769,15 @@ int olc_stage_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], 
     FieldStep fs;
     if (!make_field_step(*spec, dims, dx, dt, &fs, &err)) return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse: " + err);
     cudaStream_t st = as_stream(stream);
-    float* res = run_field_step(f, tmp, spec->has_sink ? sink : nullptr, fs, st);
+    CUtensorMap mf, mt;
+    olc_u32* status = stage_status_word();
+    float* res;
+    if (stencil_tma_enabled() && status && make_field_map(&mf, f, dims) && make_field_map(&mt, tmp, dims)) {
+        launch_sink(f, spec->has_sink ? sink : nullptr, fs, st);
+        res = run_substeps_tma(f, tmp, mf, mt, fs, status, st);
+    } else {
+        res = run_field_step(f, tmp, spec->has_sink ? sink : nullptr, fs, st);
+    }
     if (res != f) {
         const size_t bytes = (size_t)dims[0] * dims[1] * dims[2] * 4;
         cudaMemcpyAsync(f, res, bytes, cudaMemcpyDeviceToDevice, st);
