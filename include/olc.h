@@ -258,6 +258,19 @@ int olc_stage_sort_pairs(const uint32_t* keys_in_dev, const uint32_t* vals_in_de
                          uint32_t* keys_out_dev, uint32_t* vals_out_dev, uint32_t n,
                          int key_bits, void* scratch_dev, size_t scratch_bytes, void* stream);
 
+/* The same stable sort for callers that cannot allocate device memory (a
+ * process whose HBM is owned by an allocator it does not expose, or a caller
+ * that must not pay cudaMalloc's implicit synchronisation): no scratch
+ * argument.  The temporary memory is a file-scope device array of this library
+ * (about 9.4 MB, held by every GPU that loads it until exit), so n is limited
+ * to 1,048,576 keys (larger n: OLC_ERR_CAPACITY).  All calls share the array:
+ * calls whose work overlaps on the GPU race and must be serialised.  The first
+ * call on a device looks up the array's address; make it before any stream
+ * capture.  Has no counterpart in the reference. */
+int olc_stage_sort_pairs_noalloc(const uint32_t* keys_in_dev, const uint32_t* vals_in_dev,
+                                 uint32_t* keys_out_dev, uint32_t* vals_out_dev, uint32_t n,
+                                 int key_bits, void* stream);
+
 /* Bin table from sorted keys: ranges_dev[2k] = first index of key k,
  * ranges_dev[2k+1] = one past the last (both 0 when empty); keys >= n_bins are
  * ignored.  Replaces VoxelTable.startIndex/count (template.wgsl:42-45). */

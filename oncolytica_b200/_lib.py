@@ -38,7 +38,7 @@ EXPORTS = (
     "olc_set_params", "olc_set_agent_count", "olc_current_buffers", "olc_step",
     "olc_read_counters", "olc_read_reductions", "olc_read_user_metrics",
     "olc_set_user_metrics_size", "olc_read_life", "olc_nvrtc_check", "olc_bind_tissue",
-    "olc_set_profiling", "olc_read_profile",
+    "olc_set_profiling", "olc_read_profile", "olc_stage_sort_pairs_noalloc",
     "olc_stage_rng", "olc_stage_keys", "olc_sort_scratch_bytes", "olc_stage_sort_pairs",
     "olc_stage_bin_ranges", "olc_stage_diffuse", "olc_stage_contact",
 )
@@ -163,6 +163,7 @@ _SIGS = {
     "olc_bind_tissue": (C.c_int, [_VP, _VP, C.c_int, C.c_size_t]),
     "olc_set_profiling": (C.c_int, [_VP, C.c_int]),
     "olc_read_profile": (C.c_int, [_VP, C.POINTER(OlcProfile)]),
+    "olc_stage_sort_pairs_noalloc": (C.c_int, [_VP, _VP, _VP, _VP, C.c_uint32, C.c_int, _VP]),
     "olc_stage_rng": (C.c_int, [_VP, C.c_uint32, C.c_int, _VP, _VP, _VP]),
     "olc_stage_keys": (C.c_int, [_VP, _VP, _VP, _VP, C.c_uint32, C.POINTER(OlcGeom), _VP, _VP]),
     "olc_sort_scratch_bytes": (C.c_size_t, [C.c_uint32, C.c_int]),
