@@ -16,6 +16,8 @@
 
 namespace olc {
 
+// One thread per agent, grid-stride.  The force sum runs over the Moore bins
+// in the order above and the rows of each bin ascending.
 __global__ void __launch_bounds__(256) k_contact(const float4* __restrict__ posr, const uint2* __restrict__ ranges,
                                                  const olc_u32* n_dev, olc_u32 n_host, ContactDev c,
                                                  float* __restrict__ xo, float* __restrict__ yo,
@@ -49,6 +51,9 @@ __global__ void __launch_bounds__(256) k_contact(const float4* __restrict__ posr
                         const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)),
                                                    __fmul_rn(ddz, ddz));
                         const float rsum = __fadd_rn(p.w, q.w);
+                        // d2 > rsum^2 (1 + 2^-20) implies sqrt(d2) >= rsum exactly, so the
+                        // exact test below would reject the pair: skip the sqrt.
+                        if (d2 > __fmul_rn(__fmul_rn(rsum, rsum), 1.00000095367431640625f)) continue;
                         const float dist = sqrtf(d2);
                         if (!(dist < rsum)) continue;
                         const float ov = __fsub_rn(rsum, dist);

@@ -18,6 +18,7 @@
 #include <cuda.h>  // CUtensorMap (types only; the encoder comes from cudaGetDriverEntryPoint)
 
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <string>
 
@@ -148,12 +149,18 @@ __global__ void __launch_bounds__(256) k_substep_tma(const __grid_constant__ CUt
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
     const olc_u32 bar_a = smem_u32(&bar);
+    // Programmatic dependent launch: the next substep may start its launch once
+    // every block of this one is running; it waits (griddepcontrol.wait) for
+    // this grid to finish before touching memory.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncthreads();
+    // the input is the previous substep's output: wait for that grid
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(BYTES) : "memory");
         asm volatile(
@@ -208,6 +215,158 @@ __global__ void __launch_bounds__(256) k_substep_tma(const __grid_constant__ CUt
     }
 }
 
+// ---------------------------------------------------------------- temporal blocking
+// k_substep_tb<T, TY, TZ> advances a 32 x TY x TZ block of outputs by T
+// substeps in one pass over HBM.  One TMA box brings the block plus a halo of
+// T planes (4 columns in x, for 16-byte alignment) into shared buffer A;
+// level t = 1..T-1 is computed on the block grown by T-t in every direction
+// into the other buffer (A and B alternate); level T is stored to global
+// memory.  Every voxel of every level goes through the same separately
+// rounded update as k_substep, so T substeps here equal T launches of it bit
+// for bit.  Voxels outside the domain are never read by interior voxels
+// (faces are pinned), so the TMA zero fill beyond the faces is harmless.
+template <int T, int TY, int TZ>
+struct TbShape {
+    static constexpr int TX = 32, HX = 4;
+    static constexpr int W0 = TX + 2 * HX, H0 = TY + 2 * T, D0 = TZ + 2 * T;
+    static constexpr int size0 = W0 * H0 * D0;
+    // largest level >= 1 region (level 1)
+    static constexpr int W1 = TX + 2 * (T - 1), H1 = TY + 2 * (T - 1), D1 = TZ + 2 * (T - 1);
+    static constexpr int size1 = W1 * H1 * D1;
+    static constexpr int sizeA = (size0 > size1 ? size0 : size1);
+    static constexpr size_t smem_bytes = (size_t)(((sizeA + 31) / 32) * 32 + size1) * 4 + 16;
+};
+
+template <int T, int TY, int TZ>
+__global__ void __launch_bounds__(256) k_substep_tb(const __grid_constant__ CUtensorMap in_map,
+                                                    float* __restrict__ out, int nx, int ny, int nz, float r,
+                                                    float inv_decay, float bval, olc_u32* status) {
+    using S = TbShape<T, TY, TZ>;
+    constexpr int TX = S::TX;
+    extern __shared__ __align__(128) float smem_raw[];
+    // TMA destinations want 128-byte alignment: round the dynamic base up
+    float* const smem = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    float* const bufA = smem;
+    float* const bufB = smem + ((S::sizeA + 31) / 32) * 32;
+    unsigned long long* bar =
+        reinterpret_cast<unsigned long long*>((reinterpret_cast<uintptr_t>(bufB + S::size1) + 7) & ~uintptr_t(7));
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+    const olc_u32 bar_a = smem_u32(bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a),
+                     "r"((olc_u32)(S::size0 * 4))
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+            "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(bufA)),
+            "l"(reinterpret_cast<unsigned long long>(&in_map)), "r"(x0 - S::HX), "r"(y0 - T), "r"(z0 - T),
+            "r"(bar_a)
+            : "memory");
+    }
+    bool ready = false;
+    for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it) {
+        if (mbar_try_wait(bar_a, 0)) {
+            ready = true;
+            break;
+        }
+    }
+    if (!ready) {
+        if (threadIdx.x == 0) atomicOr(status, OLC_ST_TIMEOUT);
+        for (olc_u32 it = 0; it < OLC_SPIN_LIMIT && !mbar_try_wait(bar_a, 0); ++it) {
+        }
+        return;
+    }
+
+    // levels 1 .. T-1 in shared memory
+    const float* src = bufA;
+    int sw = S::W0, sh = S::H0;           // source dims
+    int sox = x0 - S::HX, soy = y0 - T, soz = z0 - T;  // source origin (global coords)
+#pragma unroll
+    for (int t = 1; t < T; ++t) {
+        float* dst = (t & 1) ? bufB : bufA;
+        const int g = T - t;
+        const int dw = TX + 2 * g, dh = TY + 2 * g, dd = TZ + 2 * g;
+        const int dox = x0 - g, doy = y0 - g, doz = z0 - g;
+        for (int col = threadIdx.x; col < dw * dh; col += blockDim.x) {
+            const int cx = col % dw, cy = col / dw;
+            const int gx = dox + cx, gy = doy + cy;
+            const int sx = gx - sox, sy = gy - soy;
+            const bool edge_xy = gx <= 0 || gy <= 0 || gx >= nx - 1 || gy >= ny - 1;
+            int sidx = ((doz - soz - 1) * sh + sy) * sw + sx;
+            float zm = src[sidx];
+            sidx += sw * sh;
+            float c = src[sidx];
+            float* d = dst + cy * dw + cx;
+            for (int cz = 0; cz < dd; ++cz) {
+                const int gz = doz + cz;
+                const float zp = src[sidx + sw * sh];
+                float v;
+                if (edge_xy || gz <= 0 || gz >= nz - 1) {
+                    v = bval;
+                } else {
+                    const float xm = src[sidx - 1], xp = src[sidx + 1];
+                    const float ym = src[sidx - sw], yp = src[sidx + sw];
+                    const float s = __fadd_rn(__fadd_rn(__fadd_rn(xm, xp), __fadd_rn(ym, yp)), __fadd_rn(zm, zp));
+                    const float u = __fadd_rn(c, __fmul_rn(r, __fsub_rn(s, __fmul_rn(6.0f, c))));
+                    v = fmaxf(__fmul_rn(u, inv_decay), 0.0f);
+                }
+                d[cz * dw * dh] = v;
+                zm = c;
+                c = zp;
+                sidx += sw * sh;
+            }
+        }
+        __syncthreads();
+        src = dst;
+        sw = dw;
+        sh = dh;
+        sox = dox;
+        soy = doy;
+        soz = doz;
+    }
+
+    // level T: the block's outputs, one column per thread
+    for (int col = threadIdx.x; col < TX * TY; col += blockDim.x) {
+        const int cx = col % TX, cy = col / TX;
+        const int gx = x0 + cx, gy = y0 + cy;
+        if (gx >= nx || gy >= ny) continue;
+        const int sx = gx - sox, sy = gy - soy;
+        const bool edge_xy = gx == 0 || gy == 0 || gx == nx - 1 || gy == ny - 1;
+        int sidx = ((z0 - soz - 1) * sh + sy) * sw + sx;
+        float zm = src[sidx];
+        sidx += sw * sh;
+        float c = src[sidx];
+        float* o = out + ((size_t)z0 * ny + gy) * nx + gx;
+        const size_t sz = (size_t)nx * ny;
+        for (int cz = 0; cz < TZ; ++cz) {
+            const int gz = z0 + cz;
+            if (gz >= nz) break;
+            const float zp = src[sidx + sw * sh];
+            float v;
+            if (edge_xy || gz == 0 || gz == nz - 1) {
+                v = bval;
+            } else {
+                const float xm = src[sidx - 1], xp = src[sidx + 1];
+                const float ym = src[sidx - sw], yp = src[sidx + sw];
+                const float s = __fadd_rn(__fadd_rn(__fadd_rn(xm, xp), __fadd_rn(ym, yp)), __fadd_rn(zm, zp));
+                const float u = __fadd_rn(c, __fmul_rn(r, __fsub_rn(s, __fmul_rn(6.0f, c))));
+                v = fmaxf(__fmul_rn(u, inv_decay), 0.0f);
+            }
+            *o = v;
+            o += sz;
+            zm = c;
+            c = zp;
+            sidx += sw * sh;
+        }
+    }
+}
+
 namespace {
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -228,37 +387,125 @@ EncodeTiledFn encode_fn() {
 }
 }  // namespace
 
-bool make_field_map(CUtensorMap* map, float* base, const int dims[3]) {
-    using namespace tma;
+static bool encode_map(CUtensorMap* map, float* base, const int dims[3], const cuuint32_t box[3]) {
     if ((dims[0] * 4) % 16 != 0 || (reinterpret_cast<uintptr_t>(base) & 15u) != 0) return false;
     EncodeTiledFn fn = encode_fn();
     if (!fn) return false;
     cuuint64_t gdim[3] = {(cuuint64_t)dims[0], (cuuint64_t)dims[1], (cuuint64_t)dims[2]};
     cuuint64_t gstride[2] = {(cuuint64_t)dims[0] * 4, (cuuint64_t)dims[0] * dims[1] * 4};
-    cuuint32_t box[3] = {WX, WY, WZ};
     cuuint32_t estride[3] = {1, 1, 1};
     return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, gdim, gstride, box, estride,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Temporal-block shapes compiled in; OLC_TB="T,TY,TZ" selects one (default 2,8,16).
+#define OLC_TB_SHAPES(X) X(2, 8, 16) X(2, 8, 32) X(2, 16, 16) X(3, 8, 16) X(3, 16, 16) X(4, 16, 16) X(2, 4, 32)
+
+// Default T = 1: on B200 the single-substep TMA kernel (26.9 us per 256^3 FP32
+// substep) beats every temporal block measured (T=2: 32 us, T=3: 40 us; the
+// intermediate levels make the kernel shared-memory bound at low occupancy).
+static void tb_from_env(FieldMaps* m) {
+    m->T = 1;
+    m->TY = 8;
+    m->TZ = 16;
+    const char* v = getenv("OLC_TB");
+    if (!v) return;
+    int T = 0, TY = 0, TZ = 0;
+    if (sscanf(v, "%d,%d,%d", &T, &TY, &TZ) != 3) return;
+    bool known = T == 1;
+#define OLC_TB_MATCH(a, b, c) known = known || (T == a && TY == b && TZ == c);
+    OLC_TB_SHAPES(OLC_TB_MATCH)
+#undef OLC_TB_MATCH
+    if (known) {
+        m->T = T;
+        m->TY = TY;
+        m->TZ = TZ;
+    }
+}
+
+bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3]) {
+    using namespace tma;
+    m->ok = false;
+    tb_from_env(m);
+    const cuuint32_t box1[3] = {WX, WY, WZ};
+    if (!encode_map(&m->single[0], a, dims, box1) || !encode_map(&m->single[1], b, dims, box1)) return false;
+    if (m->T > 1) {
+        const cuuint32_t boxT[3] = {(cuuint32_t)(32 + 8), (cuuint32_t)(m->TY + 2 * m->T),
+                                    (cuuint32_t)(m->TZ + 2 * m->T)};
+        if (!encode_map(&m->block[0], a, dims, boxT) || !encode_map(&m->block[1], b, dims, boxT)) m->T = 1;
+    }
+    m->ok = true;
+    return true;
+}
+
+template <int T, int TY, int TZ>
+static void launch_tb(const CUtensorMap& map, float* out, const FieldStep& fs, olc_u32* status, cudaStream_t s) {
+    using S = TbShape<T, TY, TZ>;
+    const int bytes = (int)S::smem_bytes + 128;
+    static int configured_mask = 0;  // per device (up to 32)
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 32 && !(configured_mask & (1 << dev))) {
+        cudaFuncSetAttribute(k_substep_tb<T, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        configured_mask |= 1 << dev;
+    }
+    dim3 grid((fs.dims[0] + 31) / 32, (fs.dims[1] + TY - 1) / TY, (fs.dims[2] + TZ - 1) / TZ);
+    k_substep_tb<T, TY, TZ><<<grid, 256, bytes, s>>>(map, out, fs.dims[0], fs.dims[1], fs.dims[2], fs.r,
+                                                     fs.inv_decay, fs.bval, status);
+}
+
+static void launch_block(const FieldMaps& m, const CUtensorMap& map, float* out, const FieldStep& fs,
+                         olc_u32* status, cudaStream_t s) {
+#define OLC_TB_LAUNCH(a, b, c)                              \
+    if (m.T == a && m.TY == b && m.TZ == c) {               \
+        launch_tb<a, b, c>(map, out, fs, status, s);        \
+        return;                                             \
+    }
+    OLC_TB_SHAPES(OLC_TB_LAUNCH)
+#undef OLC_TB_LAUNCH
+}
+
 void launch_substep_tma(const CUtensorMap& in_map, float* out, const FieldStep& fs, olc_u32* status,
                         cudaStream_t s) {
     using namespace tma;
-    dim3 grid((fs.dims[0] + TX - 1) / TX, (fs.dims[1] + TY - 1) / TY, (fs.dims[2] + TZ - 1) / TZ);
-    k_substep_tma<<<grid, 256, 0, s>>>(in_map, out, fs.dims[0], fs.dims[1], fs.dims[2], fs.r, fs.inv_decay,
-                                       fs.bval, status);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((fs.dims[0] + TX - 1) / TX, (fs.dims[1] + TY - 1) / TY, (fs.dims[2] + TZ - 1) / TZ);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_substep_tma, in_map, out, fs.dims[0], fs.dims[1], fs.dims[2], fs.r, fs.inv_decay,
+                       fs.bval, status);
 }
 
-float* run_substeps_tma(float* a, float* b, const CUtensorMap& map_a, const CUtensorMap& map_b,
-                        const FieldStep& fs, olc_u32* status, cudaStream_t s) {
-    float* cur = a;
-    for (int i = 0; i < fs.substeps; ++i) {
-        const bool from_a = cur == a;
-        launch_substep_tma(from_a ? map_a : map_b, from_a ? b : a, fs, status, s);
-        cur = from_a ? b : a;
+float* run_substeps_tma(float* a, float* b, const FieldMaps& m, int a_index, const FieldStep& fs, olc_u32* status,
+                        cudaStream_t s) {
+    float* bufs[2];
+    bufs[a_index] = a;
+    bufs[1 - a_index] = b;
+    int cur = a_index;
+    int left = fs.substeps;
+    while (left > 0) {
+        if (m.T > 1 && left >= m.T) {
+            launch_block(m, m.block[cur], bufs[1 - cur], fs, status, s);
+            left -= m.T;
+        } else {
+            launch_substep_tma(m.single[cur], bufs[1 - cur], fs, status, s);
+            left -= 1;
+        }
+        cur = 1 - cur;
     }
-    return cur;
+    return bufs[cur];
+}
+
+int launches_for(const FieldMaps& m, int substeps) {
+    if (m.T <= 1) return substeps;
+    return substeps / m.T + substeps % m.T;
 }
 
 bool stencil_tma_enabled() {

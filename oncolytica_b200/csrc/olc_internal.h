@@ -112,10 +112,19 @@ void launch_substep(const float* in, float* out, const FieldStep& fs, cudaStream
 float* run_field_step(float* a, float* b, float* sink, const FieldStep& fs, cudaStream_t s);
 // The S substeps alone.
 float* run_substeps(float* a, float* b, const FieldStep& fs, cudaStream_t s);
-// TMA tile path: a tensor map per buffer (x extent must be a multiple of 4).
-bool make_field_map(CUtensorMap* map, float* base, const int dims[3]);
-float* run_substeps_tma(float* a, float* b, const CUtensorMap& map_a, const CUtensorMap& map_b,
-                        const FieldStep& fs, olc_u32* status, cudaStream_t s);
+// TMA tile path (x extent must be a multiple of 4): tensor maps of both
+// buffers for the single-substep kernel and for the T-substep temporal block.
+struct FieldMaps {
+    bool ok = false;
+    int T = 1, TY = 8, TZ = 16;
+    CUtensorMap single[2];
+    CUtensorMap block[2];
+};
+bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3]);
+// Runs fs.substeps substeps starting from a (buffer index a_index of m).
+float* run_substeps_tma(float* a, float* b, const FieldMaps& m, int a_index, const FieldStep& fs, olc_u32* status,
+                        cudaStream_t s);
+int launches_for(const FieldMaps& m, int substeps);
 // OLC_STENCIL=plain in the environment selects the register-column kernel.
 bool stencil_tma_enabled();
 olc_u32* stage_status_word();

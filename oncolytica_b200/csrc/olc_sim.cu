@@ -54,8 +54,7 @@ struct OlcSim {
     FieldStep fstep[OLC_MAX_FIELDS] = {};
     int field_cur[OLC_MAX_FIELDS] = {};
     bool field_bound[OLC_MAX_FIELDS] = {};
-    CUtensorMap fmap[2][OLC_MAX_FIELDS];      // TMA descriptors of both buffers
-    bool fmap_ok[OLC_MAX_FIELDS] = {};
+    FieldMaps fmaps[OLC_MAX_FIELDS];           // TMA descriptors of both buffers
 
     OlcContact contact = {};
     ContactDev contact_dev = {};
@@ -230,14 +229,13 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
         int cur = s->field_cur[f];
         float* a = s->field[cur][f];
         float* b = s->field[1 - cur][f];
-        float* res = (s->fmap_ok[f] && stencil_tma_enabled())
-                         ? run_substeps_tma(a, b, s->fmap[cur][f], s->fmap[1 - cur][f], s->fstep[f],
-                                            s->counters + OLC_CTR_STATUS, st)
-                         : run_substeps(a, b, s->fstep[f], st);
+        const bool tma_path = s->fmaps[f].ok && stencil_tma_enabled();
+        float* res = tma_path ? run_substeps_tma(a, b, s->fmaps[f], cur, s->fstep[f], s->counters + OLC_CTR_STATUS, st)
+                              : run_substeps(a, b, s->fstep[f], st);
         s->field_cur[f] = (res == a) ? cur : 1 - cur;
         substeps += (uint32_t)s->fstep[f].substeps;
+        launches += (uint64_t)(tma_path ? launches_for(s->fmaps[f], s->fstep[f].substeps) : s->fstep[f].substeps);
     }
-    launches += substeps;
     mark(s, 2, st);
     // 2. grid + compaction
     const int passes = (s->key_bits + 7) / 8;
@@ -442,8 +440,8 @@ int olc_bind_field(OlcSim* s, int index, float* a, float* b, float* sink, const 
     if (spec->has_sink && !sink) return fail(s, OLC_ERR_ARG, "olc_bind_field: has_sink without a sink buffer");
     s->field[0][index] = a;
     s->field[1][index] = b;
-    s->fmap_ok[index] = spec->substeps > 0 && make_field_map(&s->fmap[0][index], a, s->geom.chem_dims) &&
-                        make_field_map(&s->fmap[1][index], b, s->geom.chem_dims);
+    s->fmaps[index].ok = false;
+    if (spec->substeps > 0) make_field_maps(&s->fmaps[index], a, b, s->geom.chem_dims);
     s->sink[index] = spec->has_sink ? sink : nullptr;
     s->fspec[index] = *spec;
     s->fstep[index] = fs;
@@ -769,12 +767,12 @@ int olc_stage_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], 
     FieldStep fs;
     if (!make_field_step(*spec, dims, dx, dt, &fs, &err)) return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse: " + err);
     cudaStream_t st = as_stream(stream);
-    CUtensorMap mf, mt;
+    FieldMaps maps;
     olc_u32* status = stage_status_word();
     float* res;
-    if (stencil_tma_enabled() && status && make_field_map(&mf, f, dims) && make_field_map(&mt, tmp, dims)) {
+    if (stencil_tma_enabled() && status && make_field_maps(&maps, f, tmp, dims)) {
         launch_sink(f, spec->has_sink ? sink : nullptr, fs, st);
-        res = run_substeps_tma(f, tmp, mf, mt, fs, status, st);
+        res = run_substeps_tma(f, tmp, maps, 0, fs, status, st);
     } else {
         res = run_field_step(f, tmp, spec->has_sink ? sink : nullptr, fs, st);
     }

@@ -219,26 +219,33 @@ def test_diffuse_bit_exact(cuda, olc, dims, substeps, decay, with_sink):
         assert float(to_host(sd).max()) == 0.0
 
 
+TB_SHAPES = ["1,8,16", "2,8,16", "2,8,32", "2,16,16", "3,8,16", "3,16,16", "4,16,16", "2,4,32"]
+
+
 def test_diffuse_plain_and_tma_paths_agree(cuda, olc, monkeypatch):
-    """The TMA tile kernel and the register-column kernel give the same bits."""
+    """The TMA tile kernel, every temporal-block shape (T substeps per pass)
+    and the register-column kernel give the same bits, 7 substeps so odd
+    remainders run too."""
     import torch
 
     rng = np.random.default_rng(77)
-    nx, ny, nz = 64, 40, 36
+    nx, ny, nz = 68, 41, 37
     f = rng.random((nz, ny, nx), dtype=np.float32)
-    spec = _lib.OlcDiffusion(diffusion=1.0, decay=0.02, boundary=0.4, substeps=6, has_sink=0)
+    spec = _lib.OlcDiffusion(diffusion=1.0, decay=0.02, boundary=0.4, substeps=7, has_sink=0)
     dims_c = (C.c_int32 * 3)(nx, ny, nz)
     outs = []
-    for mode in ("tma", "plain"):
+    for mode in TB_SHAPES + ["plain"]:
         if mode == "plain":
             monkeypatch.setenv("OLC_STENCIL", "plain")
+        else:
+            monkeypatch.setenv("OLC_TB", mode)
         fd = to_dev(f, cuda)
         tmp = torch.empty_like(fd)
         _lib.check(olc.olc_stage_diffuse(dptr(fd), dptr(tmp), None, C.byref(dims_c), 1.0, 0.5, C.byref(spec), None))
         outs.append(to_host(fd))
-    np.testing.assert_array_equal(outs[0], outs[1])
-    ref = oracle.diffuse(f, None, dx=1.0, dt=0.5, D=1.0, decay=0.02, boundary=0.4, substeps=6)
-    np.testing.assert_array_equal(outs[0], ref)
+    ref = oracle.diffuse(f, None, dx=1.0, dt=0.5, D=1.0, decay=0.02, boundary=0.4, substeps=7)
+    for mode, out in zip(TB_SHAPES + ["plain"], outs):
+        np.testing.assert_array_equal(out, ref, err_msg=mode)
 
 
 # ------------------------------------------------------------------ contact
