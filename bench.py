@@ -322,7 +322,7 @@ def run_b200(args) -> None:
     sub_ms = prof["ms_substeps"] / max(1, prof["substep_launches"])
     alg_bytes = 8 * nvox  # stream model: read 4 B + write 4 B per voxel (FP32)
     achieved = alg_bytes / (sub_ms / 1e3) / 1e9
-    traffic = read_traffic("k_substep", nvox)
+    traffic = read_traffic("k_substep_tma", nvox)
     steps_done = max(1, prof["steps"])
     stages = {k[3:]: prof[k] / steps_done for k in ("ms_sink", "ms_substeps", "ms_grid", "ms_rules",
                                                      "ms_contact", "ms_collect")}
@@ -337,7 +337,7 @@ def run_b200(args) -> None:
                    "parallelism": f"replicas x{world}"},
         "voxel_updates_per_s": total_vox / (ms_max / 1e3),
         "agents_end": c1["n_agents"],
-        "roofline": {"bound": "hbm", "kernel": "k_substep (7-point FTCS, FP32)", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": "k_substep_tma (7-point FTCS, FP32, TMA tiles)", "achieved": achieved,
                      "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                      "peak_src": peaks["src"], "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
                      "launch_ms": sub_ms},
