@@ -210,6 +210,15 @@ int olc_current_buffers(const OlcSim* sim, int* agent_buf, int* field_buf);
  * No host synchronisation inside. */
 int olc_step(OlcSim* sim, int nsteps, int collect, void* stream);
 
+/* Enables (1) or disables (0) running olc_step through CUDA graphs of whole
+ * steps; no counterpart in the reference (its step is a fixed list of wgpu
+ * compute passes).  Results are identical to eager steps.  A graph is cached
+ * per buffer-parity state at step start and captured the second time that
+ * state is met; every binding call (columns, fields, tissue, contact, rules,
+ * a params blob that grows, metrics size) drops the cache.  Steps taken while
+ * profiling is on run eagerly. */
+int olc_set_graphs(OlcSim* sim, int enable);
+
 /* Synchronises `stream` and copies the counters. */
 int olc_read_counters(OlcSim* sim, OlcCounters* out, void* stream);
 

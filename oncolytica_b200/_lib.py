@@ -35,7 +35,7 @@ OLC_STATE_BINS = 8
 EXPORTS = (
     "olc_create", "olc_destroy", "olc_last_error", "olc_version",
     "olc_bind_agent_column", "olc_bind_field", "olc_set_contact", "olc_set_rule_source",
-    "olc_set_params", "olc_set_agent_count", "olc_current_buffers", "olc_step",
+    "olc_set_params", "olc_set_agent_count", "olc_current_buffers", "olc_step", "olc_set_graphs",
     "olc_read_counters", "olc_read_reductions", "olc_read_user_metrics",
     "olc_set_user_metrics_size", "olc_read_life", "olc_nvrtc_check", "olc_bind_tissue",
     "olc_set_profiling", "olc_read_profile", "olc_stage_sort_pairs_noalloc",
@@ -154,6 +154,7 @@ _SIGS = {
     "olc_set_agent_count": (C.c_int, [_VP, C.c_uint32, _VP]),
     "olc_current_buffers": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "olc_step": (C.c_int, [_VP, C.c_int, C.c_int, _VP]),
+    "olc_set_graphs": (C.c_int, [_VP, C.c_int]),
     "olc_read_counters": (C.c_int, [_VP, C.POINTER(OlcCounters), _VP]),
     "olc_read_reductions": (C.c_int, [_VP, C.POINTER(OlcReductions), _VP]),
     "olc_read_user_metrics": (C.c_int, [_VP, _VP, C.c_size_t, _VP]),

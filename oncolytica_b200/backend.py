@@ -149,6 +149,7 @@ class CudaBackend:
         self._check(self.lib.olc_set_user_metrics_size(self.handle, 4 * max(1, len(L.metrics))))
         self.upload_params()
         self.sync_to_device()
+        self.set_graphs(self.engine.use_graphs)
 
     def upload_params(self) -> None:
         sim = self.engine._sim
@@ -192,6 +193,9 @@ class CudaBackend:
         self._check(self.lib.olc_read_counters(self.handle, C.byref(c), self._stream()))
         return {"n_agents": c.n_agents, "births": c.births, "deaths": c.deaths, "status": c.status,
                 "steps": c.steps, "agent_steps": c.agent_steps}
+
+    def set_graphs(self, enable: bool) -> None:
+        self._check(self.lib.olc_set_graphs(self.handle, int(bool(enable))))
 
     def set_profiling(self, enable: bool) -> None:
         self._check(self.lib.olc_set_profiling(self.handle, int(bool(enable))))

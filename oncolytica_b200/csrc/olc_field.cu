@@ -215,6 +215,214 @@ __global__ void __launch_bounds__(256) k_substep_tma(const __grid_constant__ CUt
     }
 }
 
+// ---------------------------------------------------------------- 4-wide TMA tile path
+// k_substep_x4<TYR, TZ>: the same single substep with each thread owning four
+// consecutive x voxels of a row, so the x neighbours of the inner voxels are
+// already in registers and the z, y rows come from shared memory as 16-byte
+// vectors.  A CTA of 16 x TYR threads owns a 64 x TYR x TZ block of outputs;
+// one TMA box (72 x (TYR+2) x (TZ+2) floats, x starting 4 columns early so it
+// is 16-byte aligned) holds the block and its halo.  Per four voxels a thread
+// issues three 128-bit and two 32-bit shared loads and one 128-bit store; the
+// arithmetic per voxel is unchanged (same operations, same order, separately
+// rounded), so results equal k_substep_tma bit for bit.  Needs nx % 4 == 0,
+// which the TMA row-stride rule already imposes.
+template <int TYR, int TZ>
+struct X4Shape {
+    static constexpr int TX = 64, HX = 4, WX = TX + 2 * HX, WY = TYR + 2, WZ = TZ + 2;
+    static constexpr int THREADS = 16 * TYR;
+    static constexpr unsigned BYTES = (unsigned)(WX * WY * WZ * 4);
+    static constexpr size_t SMEM = BYTES + 16 + 128;  // tile + mbarrier + alignment slack
+};
+
+__device__ __forceinline__ float stencil_update(float xm, float xp, float ym, float yp, float zm, float zp, float c,
+                                                float r, float inv_decay) {
+    const float s = __fadd_rn(__fadd_rn(__fadd_rn(xm, xp), __fadd_rn(ym, yp)), __fadd_rn(zm, zp));
+    const float u = __fadd_rn(c, __fmul_rn(r, __fsub_rn(s, __fmul_rn(6.0f, c))));
+    return fmaxf(__fmul_rn(u, inv_decay), 0.0f);
+}
+
+// The 64 x TYR x TZ output block at (x0, y0, z0) from its staged box.
+template <int TYR, int TZ>
+__device__ __forceinline__ void x4_tile(const float* tile, float* __restrict__ out, int x0, int y0, int z0, int nx,
+                                        int ny, int nz, float r, float inv_decay, float bval) {
+    using S = X4Shape<TYR, TZ>;
+    const int g = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int x = x0 + 4 * g, y = y0 + ty;
+    if (x >= nx || y >= ny) return;
+    const bool edge_y = y == 0 || y == ny - 1;
+    const bool ex0 = x == 0, ex3 = x + 3 == nx - 1;
+    constexpr int PS = S::WY * S::WX;  // plane stride (floats)
+    const float* col = tile + (ty + 1) * S::WX + S::HX + 4 * g;  // plane 0 of this thread's four voxels
+    float4 zm = *reinterpret_cast<const float4*>(col);
+    float4 c = *reinterpret_cast<const float4*>(col + PS);
+    const size_t sz = (size_t)nx * ny;
+    float* o = out + (size_t)z0 * sz + (size_t)y * nx + x;
+#pragma unroll 4
+    for (int lz = 1; lz <= TZ; ++lz) {
+        const int z = z0 + lz - 1;
+        if (z >= nz) break;
+        const float* pc = col + lz * PS;
+        const float4 zp = *reinterpret_cast<const float4*>(pc + PS);
+        const float4 ym = *reinterpret_cast<const float4*>(pc - S::WX);
+        const float4 yp = *reinterpret_cast<const float4*>(pc + S::WX);
+        const float xl = pc[-1], xr = pc[4];
+        float4 v;
+        v.x = stencil_update(xl, c.y, ym.x, yp.x, zm.x, zp.x, c.x, r, inv_decay);
+        v.y = stencil_update(c.x, c.z, ym.y, yp.y, zm.y, zp.y, c.y, r, inv_decay);
+        v.z = stencil_update(c.y, c.w, ym.z, yp.z, zm.z, zp.z, c.z, r, inv_decay);
+        v.w = stencil_update(c.z, xr, ym.w, yp.w, zm.w, zp.w, c.w, r, inv_decay);
+        if (edge_y || z == 0 || z == nz - 1) {
+            v = make_float4(bval, bval, bval, bval);
+        } else {
+            if (ex0) v.x = bval;
+            if (ex3) v.w = bval;
+        }
+        *reinterpret_cast<float4*>(o) = v;
+        o += sz;
+        zm = c;
+        c = zp;
+    }
+}
+
+template <int TYR, int TZ>
+__global__ void __launch_bounds__(16 * TYR, 1) k_substep_x4(const __grid_constant__ CUtensorMap in_map,
+                                                        float* __restrict__ out, int nx, int ny, int nz, float r,
+                                                        float inv_decay, float bval, olc_u32* status, int rev) {
+    using S = X4Shape<TYR, TZ>;
+    extern __shared__ unsigned char x4_raw[];
+    const olc_u32 pad = (128u - (smem_u32(x4_raw) & 127u)) & 127u;
+    float* tile = reinterpret_cast<float*>(x4_raw + pad);
+    const olc_u32 bar_a = smem_u32(x4_raw + pad + S::BYTES);
+    // rev != 0 walks the tiles in reverse launch order, so a substep starts on
+    // the tiles the previous one wrote last, while they are still in L2
+    const int bx = rev ? gridDim.x - 1 - blockIdx.x : blockIdx.x;
+    const int by = rev ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
+    const int bz = rev ? gridDim.z - 1 - blockIdx.z : blockIdx.z;
+    const int x0 = bx * S::TX, y0 = by * TYR, z0 = bz * TZ;
+    // programmatic dependent launch, as in k_substep_tma
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(S::BYTES) : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+            "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(tile)),
+            "l"(reinterpret_cast<unsigned long long>(&in_map)), "r"(x0 - S::HX), "r"(y0 - 1), "r"(z0 - 1),
+            "r"(bar_a)
+            : "memory");
+    }
+    bool ready = false;
+    for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it) {
+        if (mbar_try_wait(bar_a, 0)) {
+            ready = true;
+            break;
+        }
+    }
+    if (!ready) {
+        if (threadIdx.x == 0) atomicOr(status, OLC_ST_TIMEOUT);
+        for (olc_u32 it = 0; it < OLC_SPIN_LIMIT && !mbar_try_wait(bar_a, 0); ++it) {
+        }
+        return;
+    }
+    x4_tile<TYR, TZ>(tile, out, x0, y0, z0, nx, ny, nz, r, inv_decay, bval);
+}
+
+// ---------------------------------------------------------------- persistent pipeline
+// k_substep_pipe<TYR, TZ, NS>: the 4-wide substep as a persistent kernel.  The
+// grid holds as many CTAs as fit on the GPU at once; CTA b takes tiles b,
+// b + G, b + 2G, ... (so the tiles in flight at any moment form one
+// contiguous slab of the field, as a wave of k_substep_x4 does), through a
+// ring of NS shared-memory stages: while it computes tile k, the TMA loads of
+// tiles k+1 .. k+NS-1 are in flight.  One barrier per tile both makes the
+// timeout decision uniform and tells thread 0 that the stage read last is
+// free for the next load.  Same tile arithmetic as k_substep_x4.
+template <int TYR, int TZ, int NS>
+struct PipeShape {
+    using S = X4Shape<TYR, TZ>;
+    static constexpr size_t SMEM = (size_t)NS * S::BYTES + 8 * NS + 128;
+};
+
+template <int TYR, int TZ, int NS>
+__global__ void __launch_bounds__(16 * TYR, 1) k_substep_pipe(const __grid_constant__ CUtensorMap in_map,
+                                                             float* __restrict__ out, int nx, int ny, int nz,
+                                                             float r, float inv_decay, float bval, olc_u32* status,
+                                                             int rev) {
+    using S = X4Shape<TYR, TZ>;
+    extern __shared__ unsigned char pipe_raw[];
+    const olc_u32 pad = (128u - (smem_u32(pipe_raw) & 127u)) & 127u;
+    float* stages = reinterpret_cast<float*>(pipe_raw + pad);
+    const olc_u32 bar0 = smem_u32(pipe_raw + pad + (size_t)NS * S::BYTES);
+    const int ntx = (nx + S::TX - 1) / S::TX, nty = (ny + TYR - 1) / TYR, ntz = (nz + TZ - 1) / TZ;
+    const int ntiles = ntx * nty * ntz;
+    const int G = (int)gridDim.x;
+    const int mine = ((int)blockIdx.x < ntiles) ? (ntiles - (int)blockIdx.x + G - 1) / G : 0;
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < NS; ++k) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0 + 8 * k) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    auto origin = [&](int k, int* x0, int* y0, int* z0) {
+        int t = (int)blockIdx.x + k * G;
+        if (rev) t = ntiles - 1 - t;
+        *x0 = (t % ntx) * S::TX;
+        t /= ntx;
+        *y0 = (t % nty) * TYR;
+        *z0 = (t / nty) * TZ;
+    };
+    auto issue = [&](int k) {  // thread 0: TMA load of this CTA's k-th tile into stage k % NS
+        if (k >= mine) return;
+        int x0, y0, z0;
+        origin(k, &x0, &y0, &z0);
+        const olc_u32 bar = bar0 + 8 * (k % NS);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(S::BYTES) : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+            "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(stages + (size_t)(k % NS) * (S::BYTES / 4))),
+            "l"(reinterpret_cast<unsigned long long>(&in_map)), "r"(x0 - S::HX), "r"(y0 - 1), "r"(z0 - 1), "r"(bar)
+            : "memory");
+    };
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NS; ++k) issue(k);
+    for (int k = 0; k < mine; ++k) {
+        const olc_u32 bar = bar0 + 8 * (k % NS), parity = (olc_u32)((k / NS) & 1);
+        bool ok = false;
+        for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it) {
+            if (mbar_try_wait(bar, parity)) {
+                ok = true;
+                break;
+            }
+        }
+        if (__syncthreads_or(!ok)) {
+            // loads k .. k+NS-2 (k+NS-1 once k = 0) may still be in flight: give
+            // each a bounded chance to land before the shared memory is released
+            if (threadIdx.x == 0) {
+                atomicOr(status, OLC_ST_TIMEOUT);
+                const int last = min(mine - 1, k == 0 ? NS - 1 : k + NS - 2);
+                for (int j = k; j <= last; ++j)
+                    for (olc_u32 it = 0;
+                         it < OLC_SPIN_LIMIT && !mbar_try_wait(bar0 + 8 * (j % NS), (olc_u32)((j / NS) & 1)); ++it) {
+                    }
+            }
+            return;
+        }
+        // every thread is past tile k-1: its stage may be refilled
+        if (threadIdx.x == 0 && k > 0) issue(k - 1 + NS);
+        int x0, y0, z0;
+        origin(k, &x0, &y0, &z0);
+        x4_tile<TYR, TZ>(stages + (size_t)(k % NS) * (S::BYTES / 4), out, x0, y0, z0, nx, ny, nz, r, inv_decay,
+                         bval);
+    }
+}
+
 // ---------------------------------------------------------------- temporal blocking
 // k_substep_tb<T, TY, TZ> advances a 32 x TY x TZ block of outputs by T
 // substeps in one pass over HBM.  One TMA box brings the block plus a halo of
@@ -424,12 +632,71 @@ static void tb_from_env(FieldMaps* m) {
     }
 }
 
+// 4-wide single-substep shapes compiled in (TYR, TZ); OLC_VX="TYR,TZ" selects
+// one, OLC_VX=0 the scalar k_substep_tma.
+#define OLC_VX_SHAPES(X) X(16, 8) X(16, 4) X(8, 8) X(8, 16) X(16, 16) X(32, 4)
+
+// Default (8, 8): on B200 with a 256^3 FP32 field, 21.2 us per substep against
+// 21.5 for (16, 8), 22.1 for (8, 16) and 25.4 for the scalar kernel.
+static void vx_from_env(FieldMaps* m) {
+    m->VY = 8;
+    m->VZ = 8;
+    const char* v = getenv("OLC_VX");
+    if (!v) return;
+    int a = 0, b = 0;
+    if (sscanf(v, "%d,%d", &a, &b) != 2) {
+        m->VY = m->VZ = 0;
+        return;
+    }
+    bool known = false;
+#define OLC_VX_MATCH(p, q) known = known || (a == p && b == q);
+    OLC_VX_SHAPES(OLC_VX_MATCH)
+#undef OLC_VX_MATCH
+    if (known) {
+        m->VY = a;
+        m->VZ = b;
+    }
+}
+
+// Persistent pipeline shapes compiled in (TYR, TZ, NS); OLC_PIPE="TYR,TZ,NS"
+// selects one, OLC_PIPE=0 the one-tile-per-CTA kernels.
+#define OLC_PIPE_SHAPES(X) X(8, 8, 2) X(8, 8, 3) X(8, 8, 4) X(16, 4, 2) X(16, 4, 3) X(16, 8, 2) X(32, 4, 2)
+
+static void pipe_from_env(FieldMaps* m) {
+    m->PY = 0;
+    m->PZ = 0;
+    m->PN = 0;
+    const char* v = getenv("OLC_PIPE");
+    if (!v) return;
+    int a = 0, b = 0, c = 0;
+    if (sscanf(v, "%d,%d,%d", &a, &b, &c) != 3) return;
+    bool known = false;
+#define OLC_PIPE_MATCH(p, q, n) known = known || (a == p && b == q && c == n);
+    OLC_PIPE_SHAPES(OLC_PIPE_MATCH)
+#undef OLC_PIPE_MATCH
+    if (known) {
+        m->PY = a;
+        m->PZ = b;
+        m->PN = c;
+    }
+}
+
 bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3]) {
     using namespace tma;
     m->ok = false;
     tb_from_env(m);
+    vx_from_env(m);
+    pipe_from_env(m);
     const cuuint32_t box1[3] = {WX, WY, WZ};
     if (!encode_map(&m->single[0], a, dims, box1) || !encode_map(&m->single[1], b, dims, box1)) return false;
+    if (m->VY > 0) {
+        const cuuint32_t boxv[3] = {72, (cuuint32_t)(m->VY + 2), (cuuint32_t)(m->VZ + 2)};
+        if (!encode_map(&m->vec[0], a, dims, boxv) || !encode_map(&m->vec[1], b, dims, boxv)) m->VY = m->VZ = 0;
+    }
+    if (m->PY > 0) {
+        const cuuint32_t boxp[3] = {72, (cuuint32_t)(m->PY + 2), (cuuint32_t)(m->PZ + 2)};
+        if (!encode_map(&m->pipe[0], a, dims, boxp) || !encode_map(&m->pipe[1], b, dims, boxp)) m->PY = 0;
+    }
     if (m->T > 1) {
         const cuuint32_t boxT[3] = {(cuuint32_t)(32 + 8), (cuuint32_t)(m->TY + 2 * m->T),
                                     (cuuint32_t)(m->TZ + 2 * m->T)};
@@ -483,6 +750,86 @@ void launch_substep_tma(const CUtensorMap& in_map, float* out, const FieldStep& 
                        fs.bval, status);
 }
 
+template <int TYR, int TZ>
+static void launch_x4(const CUtensorMap& map, float* out, const FieldStep& fs, olc_u32* status, int rev,
+                      cudaStream_t s) {
+    using S = X4Shape<TYR, TZ>;
+    static int configured_mask = 0;  // per device (up to 32)
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 32 && !(configured_mask & (1 << dev))) {
+        cudaFuncSetAttribute(k_substep_x4<TYR, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
+        configured_mask |= 1 << dev;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((fs.dims[0] + S::TX - 1) / S::TX, (fs.dims[1] + TYR - 1) / TYR, (fs.dims[2] + TZ - 1) / TZ);
+    cfg.blockDim = dim3(S::THREADS);
+    cfg.dynamicSmemBytes = S::SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_substep_x4<TYR, TZ>, map, out, fs.dims[0], fs.dims[1], fs.dims[2], fs.r,
+                       fs.inv_decay, fs.bval, status, rev);
+}
+
+template <int TYR, int TZ, int NS>
+static void launch_pipe(const CUtensorMap& map, float* out, const FieldStep& fs, olc_u32* status, int rev,
+                        cudaStream_t s) {
+    using P = PipeShape<TYR, TZ, NS>;
+    static int configured_mask = 0;  // per device (up to 32)
+    static int per_sm[32] = {};
+    static int sms[32] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 32) return;
+    if (!(configured_mask & (1 << dev))) {
+        cudaFuncSetAttribute(k_substep_pipe<TYR, TZ, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P::SMEM);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[dev], k_substep_pipe<TYR, TZ, NS>, 16 * TYR, P::SMEM);
+        cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+        if (per_sm[dev] < 1) per_sm[dev] = 1;
+        configured_mask |= 1 << dev;
+    }
+    const int ntiles = ((fs.dims[0] + 63) / 64) * ((fs.dims[1] + TYR - 1) / TYR) * ((fs.dims[2] + TZ - 1) / TZ);
+    const int gmax = per_sm[dev] * sms[dev];
+    // as many CTAs as fit, then evened out so every CTA takes the same number of tiles (+-1)
+    const int per_cta = (ntiles + gmax - 1) / gmax;
+    const int grid = (ntiles + per_cta - 1) / per_cta;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(16 * TYR);
+    cfg.dynamicSmemBytes = P::SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_substep_pipe<TYR, TZ, NS>, map, out, fs.dims[0], fs.dims[1], fs.dims[2], fs.r,
+                       fs.inv_decay, fs.bval, status, rev);
+}
+
+static void launch_single(const FieldMaps& m, int cur, float* out, const FieldStep& fs, olc_u32* status, int rev,
+                          cudaStream_t s) {
+#define OLC_PIPE_LAUNCH(p, q, n)                                  \
+    if (m.PY == p && m.PZ == q && m.PN == n) {                    \
+        launch_pipe<p, q, n>(m.pipe[cur], out, fs, status, rev, s); \
+        return;                                                   \
+    }
+    OLC_PIPE_SHAPES(OLC_PIPE_LAUNCH)
+#undef OLC_PIPE_LAUNCH
+#define OLC_VX_LAUNCH(p, q)                                \
+    if (m.VY == p && m.VZ == q) {                          \
+        launch_x4<p, q>(m.vec[cur], out, fs, status, rev, s); \
+        return;                                            \
+    }
+    OLC_VX_SHAPES(OLC_VX_LAUNCH)
+#undef OLC_VX_LAUNCH
+    launch_substep_tma(m.single[cur], out, fs, status, s);
+}
+
 float* run_substeps_tma(float* a, float* b, const FieldMaps& m, int a_index, const FieldStep& fs, olc_u32* status,
                         cudaStream_t s) {
     float* bufs[2];
@@ -490,12 +837,15 @@ float* run_substeps_tma(float* a, float* b, const FieldMaps& m, int a_index, con
     bufs[1 - a_index] = b;
     int cur = a_index;
     int left = fs.substeps;
+    // alternate the tile order between substeps (OLC_STENCIL_ORDER=forward keeps one order)
+    const char* order = getenv("OLC_STENCIL_ORDER");
+    const bool alternate = !(order && std::string(order) == "forward");
     while (left > 0) {
         if (m.T > 1 && left >= m.T) {
             launch_block(m, m.block[cur], bufs[1 - cur], fs, status, s);
             left -= m.T;
         } else {
-            launch_substep_tma(m.single[cur], bufs[1 - cur], fs, status, s);
+            launch_single(m, cur, bufs[1 - cur], fs, status, alternate ? (fs.substeps - left) & 1 : 0, s);
             left -= 1;
         }
         cur = 1 - cur;

@@ -117,8 +117,12 @@ float* run_substeps(float* a, float* b, const FieldStep& fs, cudaStream_t s);
 struct FieldMaps {
     bool ok = false;
     int T = 1, TY = 8, TZ = 16;
+    int VY = 0, VZ = 0;          // 4-wide single-substep kernel shape (0 = scalar k_substep_tma)
+    int PY = 0, PZ = 0, PN = 0;  // persistent pipelined shape (0 = one tile per CTA)
     CUtensorMap single[2];
     CUtensorMap block[2];
+    CUtensorMap vec[2];
+    CUtensorMap pipe[2];
 };
 bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3]);
 // Runs fs.substeps substeps starting from a (buffer index a_index of m).
@@ -149,9 +153,19 @@ struct ReduceArgs {
     float cx, cy, cz;
     float bin_width;
 };
+// Block partials of the FP64 sums (4 agent sums, then one per field, each
+// RED_MAX_BLOCKS long) and one ticket per reduction kernel (zero at rest).
+constexpr olc_u32 RED_MAX_BLOCKS = 148 * 4;
+constexpr size_t RED_PARTIALS = (size_t)(4 + OLC_MAX_FIELDS) * RED_MAX_BLOCKS;
+constexpr int RED_TICKETS = 1 + OLC_MAX_FIELDS;
+struct RedScratch {
+    double* partials;
+    olc_u32* tickets;
+};
 void launch_reduce_agents(const ReduceArgs& a, const olc_u32* counters, olc_u32 n_cap,
-                          OlcReductions* out_dev, cudaStream_t s);
-void launch_reduce_field(const float* f, size_t nvox, int slot, OlcReductions* out_dev, cudaStream_t s);
+                          OlcReductions* out_dev, const RedScratch& rs, cudaStream_t s);
+void launch_reduce_field(const float* f, size_t nvox, int slot, OlcReductions* out_dev, const RedScratch& rs,
+                         cudaStream_t s);
 void launch_reset_reductions(OlcReductions* out_dev, int nfields, cudaStream_t s);
 
 void launch_rng(olc_u32* states, olc_u32 n, int draws, float* out, float* dirs, cudaStream_t s);

@@ -33,12 +33,43 @@ __device__ __forceinline__ void atomic_min_nonneg(double* p, double v) {
     atomicMin(reinterpret_cast<unsigned long long*>(p), (unsigned long long)__double_as_longlong(v));
 }
 
+// The FP64 sums are deterministic: every block writes its partial sums to
+// `partials`, and the last block to finish (a ticket counter, no waiting) adds
+// them in block order with a fixed-shape tree.  Counts, the maximum and the
+// minima are exact whatever the order, so they stay plain atomics.
+__device__ __forceinline__ double block_sum_fixed(double v, double* s_w) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_sum_d(v);
+    if (lane == 0) s_w[warp] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_w[w];
+    __syncthreads();
+    return t;  // valid in thread 0
+}
+
+// Thread 0 of each block publishes `k` partials; returns true in the last block.
+__device__ __forceinline__ bool publish_partials(const double* vals, int k, double* partials, olc_u32* ticket,
+                                                 bool* s_last) {
+    if (threadIdx.x == 0) {
+        for (int j = 0; j < k; ++j) partials[(size_t)j * gridDim.x + blockIdx.x] = vals[j];
+        __threadfence();
+        const olc_u32 t = atomicAdd(ticket, 1u);
+        *s_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (*s_last) __threadfence();
+    return *s_last;
+}
+
 __global__ void __launch_bounds__(256) k_reduce_agents(ReduceArgs a, const olc_u32* counters,
-                                                       OlcReductions* out) {
+                                                       OlcReductions* out, double* partials, olc_u32* ticket) {
     __shared__ olc_u32 s_hist[OLC_RADIAL_BINS];
     __shared__ olc_u32 s_state[OLC_STATE_BINS];
     __shared__ double s_sum[5][8];
     __shared__ olc_u32 s_live[8];
+    __shared__ bool s_last;
     const olc_u32 n = olc_total_rows(counters);
     for (int i = threadIdx.x; i < OLC_RADIAL_BINS; i += blockDim.x) s_hist[i] = 0u;
     if (threadIdx.x < OLC_STATE_BINS) s_state[threadIdx.x] = 0u;
@@ -82,8 +113,8 @@ __global__ void __launch_bounds__(256) k_reduce_agents(ReduceArgs a, const olc_u
         s_live[warp] = live;
     }
     __syncthreads();
+    double t[4] = {0, 0, 0, 0};
     if (threadIdx.x == 0) {
-        double t[4] = {0, 0, 0, 0};
         double m = 0.0;
         olc_u32 l = 0;
         for (int w = 0; w < 8; ++w) {
@@ -93,10 +124,6 @@ __global__ void __launch_bounds__(256) k_reduce_agents(ReduceArgs a, const olc_u
         }
         if (l) {
             atomicAdd(&out->n_live, l);
-            atomicAdd(&out->sum_pos[0], t[0]);
-            atomicAdd(&out->sum_pos[1], t[1]);
-            atomicAdd(&out->sum_pos[2], t[2]);
-            atomicAdd(&out->sum_r2, t[3]);
             atomic_max_nonneg(&out->max_r, m);
         }
     }
@@ -104,11 +131,27 @@ __global__ void __launch_bounds__(256) k_reduce_agents(ReduceArgs a, const olc_u
         if (s_hist[i]) atomicAdd(&out->radial_hist[i], s_hist[i]);
     if (threadIdx.x < OLC_STATE_BINS && s_state[threadIdx.x])
         atomicAdd(&out->state_counts[threadIdx.x], s_state[threadIdx.x]);
+    if (!publish_partials(t, 4, partials, ticket, &s_last)) return;
+    __shared__ double s_w[8];
+    double r[4];
+    for (int k = 0; k < 4; ++k) {
+        double v = 0.0;
+        for (olc_u32 b = threadIdx.x; b < gridDim.x; b += blockDim.x) v += __ldcg(partials + (size_t)k * gridDim.x + b);
+        r[k] = block_sum_fixed(v, s_w);
+    }
+    if (threadIdx.x == 0) {
+        out->sum_pos[0] = r[0];
+        out->sum_pos[1] = r[1];
+        out->sum_pos[2] = r[2];
+        out->sum_r2 = r[3];
+        *ticket = 0u;
+    }
 }
 
 __global__ void __launch_bounds__(256) k_reduce_field(const float* __restrict__ f, size_t nvox, int slot,
-                                                      OlcReductions* out) {
+                                                      OlcReductions* out, double* partials, olc_u32* ticket) {
     __shared__ double s_v[3][8];
+    __shared__ bool s_last;
     double sum = 0.0, mn = 1e300, mx = 0.0;
     const size_t n4 = nvox / 4;
     const float4* f4 = reinterpret_cast<const float4*>(f);
@@ -136,32 +179,43 @@ __global__ void __launch_bounds__(256) k_reduce_field(const float* __restrict__ 
         s_v[2][warp] = mx;
     }
     __syncthreads();
+    double t = 0.0;
     if (threadIdx.x == 0) {
-        double t = 0.0, a = 1e300, b = 0.0;
+        double a = 1e300, b = 0.0;
         for (int w = 0; w < 8; ++w) {
             t += s_v[0][w];
             a = fmin(a, s_v[1][w]);
             b = fmax(b, s_v[2][w]);
         }
-        atomicAdd(&out->field_mass[slot], t);
         atomic_min_nonneg(&out->field_min[slot], a);
         atomic_max_nonneg(&out->field_max[slot], b);
+    }
+    if (!publish_partials(&t, 1, partials, ticket, &s_last)) return;
+    __shared__ double s_w[8];
+    double v = 0.0;
+    for (olc_u32 b = threadIdx.x; b < gridDim.x; b += blockDim.x) v += __ldcg(partials + b);
+    const double r = block_sum_fixed(v, s_w);
+    if (threadIdx.x == 0) {
+        out->field_mass[slot] = r;
+        *ticket = 0u;
     }
 }
 
 void launch_reduce_agents(const ReduceArgs& a, const olc_u32* counters, olc_u32 n_cap, OlcReductions* out,
-                          cudaStream_t s) {
+                          const RedScratch& rs, cudaStream_t s) {
     olc_u32 blocks = (n_cap + 255) / 256;
     if (blocks == 0) blocks = 1;
-    if (blocks > 148 * 4) blocks = 148 * 4;
-    k_reduce_agents<<<blocks, 256, 0, s>>>(a, counters, out);
+    if (blocks > RED_MAX_BLOCKS) blocks = RED_MAX_BLOCKS;
+    k_reduce_agents<<<blocks, 256, 0, s>>>(a, counters, out, rs.partials, rs.tickets);
 }
 
-void launch_reduce_field(const float* f, size_t nvox, int slot, OlcReductions* out, cudaStream_t s) {
+void launch_reduce_field(const float* f, size_t nvox, int slot, OlcReductions* out, const RedScratch& rs,
+                         cudaStream_t s) {
     size_t blocks = (nvox / 4 + 255) / 256;
     if (blocks == 0) blocks = 1;
-    if (blocks > 148 * 4) blocks = 148 * 4;
-    k_reduce_field<<<(unsigned)blocks, 256, 0, s>>>(f, nvox, slot, out);
+    if (blocks > RED_MAX_BLOCKS) blocks = RED_MAX_BLOCKS;
+    k_reduce_field<<<(unsigned)blocks, 256, 0, s>>>(f, nvox, slot, out, rs.partials + (size_t)(4 + slot) * RED_MAX_BLOCKS,
+                                                     rs.tickets + 1 + slot);
 }
 
 // field_min starts at +inf (all ones in the exponent) for the unsigned min.

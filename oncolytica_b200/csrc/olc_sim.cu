@@ -38,6 +38,14 @@ using namespace olc;
 
 #define OLC_PROF_EVENTS 7
 
+struct StepGraph {
+    int key = 0;  // (agent buffer << 16) | (field parity mask << 1) | collect
+    int agent_after = 0;
+    int field_after = 0;
+    uint64_t launches = 0;
+    cudaGraphExec_t exec = nullptr;
+};
+
 struct OlcSim {
     OlcGeom geom;
     OlcCaps caps;
@@ -79,6 +87,7 @@ struct OlcSim {
     size_t params_cap = 0;
     unsigned char* params_host = nullptr;  // pinned staging
     OlcReductions* red_dev = nullptr;
+    RedScratch red_scratch = {};
     OlcReductions* red_host = nullptr;     // pinned
     void* metrics_dev = nullptr;
     size_t metrics_bytes = 0;
@@ -99,6 +108,12 @@ struct OlcSim {
     uint64_t prof_launches = 0;
     uint32_t prof_substeps = 0;
     std::vector<std::array<cudaEvent_t, OLC_PROF_EVENTS>> events;
+
+    // CUDA graphs of whole steps, keyed by the buffer parities at step start
+    bool use_graphs = false;
+    cudaStream_t capture_stream = nullptr;
+    std::vector<StepGraph> graphs;
+    std::vector<int> graph_seen;
 };
 
 namespace {
@@ -302,11 +317,11 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
         ra.cy = s->caps.center[1];
         ra.cz = s->caps.center[2];
         ra.bin_width = s->caps.radial_bin_width > 0.0f ? s->caps.radial_bin_width : 1.0f;
-        launch_reduce_agents(ra, s->counters, cap, s->red_dev, st);
+        launch_reduce_agents(ra, s->counters, cap, s->red_dev, s->red_scratch, st);
         for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
             if (!s->field_bound[f]) continue;
             const size_t nvox = (size_t)s->geom.chem_dims[0] * s->geom.chem_dims[1] * s->geom.chem_dims[2];
-            launch_reduce_field(s->field[s->field_cur[f]][f], nvox, (int)f, s->red_dev, st);
+            launch_reduce_field(s->field[s->field_cur[f]][f], nvox, (int)f, s->red_dev, s->red_scratch, st);
             ++launches;
         }
         if (s->metrics_dev && s->metrics_bytes) {
@@ -328,6 +343,81 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
     s->total_launches += launches;
     s->steps++;
     return check(s, cudaGetLastError(), "step launch");
+}
+
+int field_mask(const OlcSim* s) {
+    int m = 0;
+    for (int f = 0; f < OLC_MAX_FIELDS; ++f) m |= (s->field_cur[f] & 1) << f;
+    return m;
+}
+
+void set_field_mask(OlcSim* s, int m) {
+    for (int f = 0; f < OLC_MAX_FIELDS; ++f) s->field_cur[f] = (m >> f) & 1;
+}
+
+void drop_graphs(OlcSim* s) {
+    if (!s->graphs.empty()) {
+        cudaDeviceSynchronize();
+        for (auto& g : s->graphs) cudaGraphExecDestroy(g.exec);
+        s->graphs.clear();
+    }
+    s->graph_seen.clear();
+}
+
+// One step through a cached CUDA graph.  A step's launches depend only on the
+// bindings and on the buffer parities at its start (agent buffer, one bit per
+// field) plus `collect`, so graphs are cached by that state; the parity pattern
+// repeats with period <= 2, so only a few graphs ever exist.  The first step
+// from a given state runs eagerly (which also loads every kernel it uses); the
+// second captures it.  Capture runs on the handle's own stream (the legacy
+// default stream cannot be captured); the graph is launched on the caller's.
+int step_graph(OlcSim* s, int collect, cudaStream_t st) {
+    const int ac = s->agent_cur, fm = field_mask(s);
+    const int key = (ac << 16) | (fm << 1) | collect;
+    StepGraph* g = nullptr;
+    for (auto& e : s->graphs)
+        if (e.key == key) g = &e;
+    if (!g) {
+        bool seen = false;
+        for (int k : s->graph_seen) seen |= (k == key);
+        if (!seen) {
+            s->graph_seen.push_back(key);
+            return step_once(s, collect, st);
+        }
+        if (!s->capture_stream)
+            OLC_TRY(check(s, cudaStreamCreateWithFlags(&s->capture_stream, cudaStreamNonBlocking), "capture stream"));
+        const uint64_t steps0 = s->steps, launches0 = s->total_launches;
+        OLC_TRY(check(s, cudaStreamBeginCapture(s->capture_stream, cudaStreamCaptureModeThreadLocal), "begin capture"));
+        const int rc = step_once(s, collect, s->capture_stream);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(s->capture_stream, &graph);
+        StepGraph ng;
+        ng.key = key;
+        ng.agent_after = s->agent_cur;
+        ng.field_after = field_mask(s);
+        ng.launches = s->total_launches - launches0;
+        // nothing ran yet: restore the state the graph starts from
+        s->steps = steps0;
+        s->total_launches = launches0;
+        s->agent_cur = ac;
+        set_field_mask(s, fm);
+        if (rc != OLC_OK || e != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            return rc != OLC_OK ? rc : check(s, e, "end capture");
+        }
+        e = cudaGraphInstantiate(&ng.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        OLC_TRY(check(s, e, "graph instantiate"));
+        s->graphs.push_back(ng);
+        g = &s->graphs.back();
+    }
+    OLC_TRY(check(s, cudaGraphLaunch(g->exec, st), "graph launch"));
+    s->agent_cur = g->agent_after;
+    set_field_mask(s, g->field_after);
+    s->total_launches += g->launches;
+    s->steps++;
+    return OLC_OK;
 }
 
 }  // namespace
@@ -376,6 +466,8 @@ int olc_create(const OlcGeom* geom, const OlcCaps* caps, OlcSim** out) {
     s->rule_tiles = (cap + OLC_RULE_THREADS - 1) / OLC_RULE_THREADS;
     A(dev_alloc(s, &s->birth_lb, (size_t)OLC_MAX_RULES * s->rule_tiles * 4, "birth look-back"));
     A(dev_alloc(s, &s->red_dev, sizeof(OlcReductions), "reductions"));
+    A(dev_alloc(s, &s->red_scratch.partials, RED_PARTIALS * sizeof(double), "reduction partials"));
+    A(dev_alloc(s, &s->red_scratch.tickets, RED_TICKETS * sizeof(olc_u32), "reduction tickets"));
     A(check(s, cudaMallocHost(reinterpret_cast<void**>(&s->red_host), sizeof(OlcReductions)), "pinned reductions"));
     A(check(s, cudaMallocHost(reinterpret_cast<void**>(&s->ctr_host_words), OLC_CTR_WORDS * 4), "pinned counters"));
     if (rc == OLC_OK && !carve_sort_scratch(s->sort_mem, sbytes, cap, s->key_bits, &s->sc))
@@ -384,6 +476,7 @@ int olc_create(const OlcGeom* geom, const OlcCaps* caps, OlcSim** out) {
         A(check(s, cudaMemset(s->counters, 0, OLC_CTR_WORDS * 4), "memset counters"));
         A(check(s, cudaMemset(s->life, 0, cap), "memset life"));
         A(check(s, cudaMemset(s->red_dev, 0, sizeof(OlcReductions)), "memset reductions"));
+        A(check(s, cudaMemset(s->red_scratch.tickets, 0, RED_TICKETS * sizeof(olc_u32)), "memset tickets"));
     }
     if (rc != OLC_OK) {
         std::string msg = s->err;
@@ -397,6 +490,8 @@ int olc_create(const OlcGeom* geom, const OlcCaps* caps, OlcSim** out) {
 int olc_destroy(OlcSim* s) {
     if (!s) return OLC_OK;
     cudaDeviceSynchronize();
+    drop_graphs(s);
+    if (s->capture_stream) cudaStreamDestroy(s->capture_stream);
     if (s->module) cudaLibraryUnload(s->module);
     for (auto& ev : s->events)
         for (auto e : ev) cudaEventDestroy(e);
@@ -411,6 +506,8 @@ int olc_destroy(OlcSim* s) {
     cudaFree(s->birth_lb);
     cudaFree(s->params_dev);
     cudaFree(s->red_dev);
+    cudaFree(s->red_scratch.partials);
+    cudaFree(s->red_scratch.tickets);
     cudaFree(s->metrics_dev);
     if (s->params_host) cudaFreeHost(s->params_host);
     if (s->red_host) cudaFreeHost(s->red_host);
@@ -423,6 +520,7 @@ int olc_bind_agent_column(OlcSim* s, int index, void* a, void* b) {
     if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
     if (index < 0 || index >= (int)s->caps.n_agent_fields || !a || !b)
         return fail(s, OLC_ERR_ARG, "olc_bind_agent_column: bad index or null buffer");
+    drop_graphs(s);
     s->col[0][index] = a;
     s->col[1][index] = b;
     return OLC_OK;
@@ -438,6 +536,7 @@ int olc_bind_field(OlcSim* s, int index, float* a, float* b, float* sink, const 
         !make_field_step(*spec, s->geom.chem_dims, s->geom.chem_voxel_size, s->caps.dt, &fs, &err))
         return fail(s, OLC_ERR_ARG, "olc_bind_field: " + err);
     if (spec->has_sink && !sink) return fail(s, OLC_ERR_ARG, "olc_bind_field: has_sink without a sink buffer");
+    drop_graphs(s);
     s->field[0][index] = a;
     s->field[1][index] = b;
     s->fmaps[index].ok = false;
@@ -454,6 +553,7 @@ int olc_bind_tissue(OlcSim* s, const void* cols, int n_cols, size_t stride_bytes
     if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
     if (n_cols < 0 || (n_cols > 0 && (!cols || stride_bytes < (size_t)s->n_table * 4)))
         return fail(s, OLC_ERR_ARG, "olc_bind_tissue: columns must hold voxel_table_size entries");
+    drop_graphs(s);
     s->tissue = static_cast<const unsigned char*>(cols);
     s->tissue_cols = n_cols;
     s->tissue_stride = stride_bytes;
@@ -464,6 +564,7 @@ int olc_set_contact(OlcSim* s, const OlcContact* c) {
     if (!s || !c) return fail(s, OLC_ERR_ARG, "olc_set_contact: null argument");
     if (c->enabled && (c->radius_field >= (int)s->caps.n_agent_fields))
         return fail(s, OLC_ERR_ARG, "olc_set_contact: radius_field out of range");
+    drop_graphs(s);
     s->contact = *c;
     ContactDev& d = s->contact_dev;
     for (int i = 0; i < 3; ++i) {
@@ -534,6 +635,7 @@ int olc_set_rule_source(OlcSim* s, const char* src, const char* const* kernels, 
     std::vector<char> cubin;
     std::string log;
     if (nvrtc_compile(src, include_dir, &cubin, &log) != OLC_OK) return fail(s, OLC_ERR_NVRTC, log);
+    drop_graphs(s);
     if (s->module) {
         cudaDeviceSynchronize();
         cudaLibraryUnload(s->module);
@@ -558,6 +660,7 @@ int olc_set_params(OlcSim* s, const void* blob, size_t bytes, void* stream) {
     if (bytes == 0) return OLC_OK;
     cudaStream_t st = as_stream(stream);
     if (bytes > s->params_cap) {
+        drop_graphs(s);
         cudaStreamSynchronize(st);
         cudaFree(s->params_dev);
         if (s->params_host) cudaFreeHost(s->params_host);
@@ -578,6 +681,7 @@ int olc_set_params(OlcSim* s, const void* blob, size_t bytes, void* stream) {
 
 int olc_set_user_metrics_size(OlcSim* s, size_t bytes) {
     if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    drop_graphs(s);
     cudaFree(s->metrics_dev);
     s->metrics_dev = nullptr;
     s->metrics_bytes = bytes;
@@ -622,13 +726,27 @@ int olc_current_buffers(const OlcSim* s, int* agent_buf, int* field_buf) {
     return OLC_OK;
 }
 
+int olc_set_graphs(OlcSim* s, int enable) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    drop_graphs(s);
+    s->use_graphs = enable != 0;
+    return OLC_OK;
+}
+
 int olc_step(OlcSim* s, int nsteps, int collect, void* stream) {
     if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
     if (nsteps < 0) return fail(s, OLC_ERR_ARG, "olc_step: nsteps < 0");
     for (olc_u32 c = 0; c < s->caps.n_agent_fields; ++c)
         if (!s->col[0][c]) return fail(s, OLC_ERR_STATE, "olc_step: agent column not bound");
     cudaStream_t st = as_stream(stream);
-    for (int i = 0; i < nsteps; ++i) OLC_TRY(step_once(s, (collect && i == nsteps - 1) ? 1 : 0, st));
+    for (int i = 0; i < nsteps; ++i) {
+        const int c = (collect && i == nsteps - 1) ? 1 : 0;
+        if (s->use_graphs && !s->profiling) {
+            OLC_TRY(step_graph(s, c, st));
+        } else {
+            OLC_TRY(step_once(s, c, st));
+        }
+    }
     return OLC_OK;
 }
 

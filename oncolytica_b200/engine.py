@@ -69,6 +69,8 @@ class Engine:
         self.domain_hi: Optional[tuple[float, float, float]] = None
         self.dt: float = 1.0
         self.seed: int = 0
+        # replay each step as one CUDA graph (same results; fewer launch gaps)
+        self.use_graphs: bool = False
         self._step = 0
         self.cells = AgentList(self)
         self.tissue: Optional[Grid] = None
@@ -229,6 +231,13 @@ class Engine:
             raise RuntimeError("Engine.run_steps() called before load_model().")
         self._step += n
         self._backend_impl.run_steps(n, collect_metrics=collect_metrics)
+
+    def set_graphs(self, enable: bool) -> None:
+        """Runs later steps through cached CUDA graphs of whole steps (no
+        counterpart in the reference); results are identical to eager steps."""
+        self.use_graphs = bool(enable)
+        if self._backend_impl is not None:
+            self._backend_impl.set_graphs(self.use_graphs)
 
     def get_metrics(self) -> Any:
         return self._metrics

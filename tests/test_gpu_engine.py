@@ -15,6 +15,7 @@ from conftest import GOLDEN
 import oncolytica_b200 as ol
 from oncolytica_b200 import workloads as W
 from oncolytica_b200._geometry import get_tissue_voxel_key, voxel_table_size
+from oncolytica_b200._types import metric_fields
 
 pytestmark = pytest.mark.gpu
 
@@ -348,3 +349,38 @@ def test_tumour_long_run_statistics(cuda):
     hg, _ = np.histogram(rg, bins=16, range=(0, 80))
     ho, _ = np.histogram(ro, bins=16, range=(0, 80))
     assert np.abs(hg - ho).max() <= 0.03 * live_g
+
+
+def test_graph_steps_match_eager_steps(cuda):
+    """Steps replayed from cached CUDA graphs give bit-identical state,
+    counters, reductions and metrics to eager steps, across parity states,
+    metric collection, a params update and a host re-upload."""
+    spec = W.scaled(_parity_spec(), n_agents=8000, capacity=60_000)
+    engines = [W.build_engine(spec) for _ in range(2)]
+    engines[1].set_graphs(True)
+
+    def run(eng, k):
+        if k == 3:
+            eng.update_params(death_k=0.25)
+        if k == 5:
+            eng.sync_to_host()
+            eng.sync_to_device()
+        eng.run_steps(2, collect_metrics=(k % 2 == 1))
+
+    for k in range(8):
+        for eng in engines:
+            run(eng, k)
+        a, b = (e._backend_impl.snapshot() for e in engines)
+        assert a["rows"] == b["rows"], k
+        np.testing.assert_array_equal(a["life"], b["life"])
+        for col in a["cols"]:
+            np.testing.assert_array_equal(a["cols"][col], b["cols"][col], err_msg=f"{col} round {k}")
+        for f in a["fields"]:
+            np.testing.assert_array_equal(a["fields"][f], b["fields"][f])
+        ca, cb = (e._backend_impl.counters() for e in engines)
+        assert ca == cb, k
+        if k % 2 == 1:
+            assert engines[0].get_reductions() == engines[1].get_reductions()
+            ma, mb = (e.get_metrics() for e in engines)
+            assert {k: getattr(ma, k) for k in metric_fields(type(ma))} == \
+                   {k: getattr(mb, k) for k in metric_fields(type(mb))}

@@ -219,33 +219,45 @@ def test_diffuse_bit_exact(cuda, olc, dims, substeps, decay, with_sink):
         assert float(to_host(sd).max()) == 0.0
 
 
-TB_SHAPES = ["1,8,16", "2,8,16", "2,8,32", "2,16,16", "3,8,16", "3,16,16", "4,16,16", "2,4,32"]
+TB_SHAPES = ["2,8,16", "2,8,32", "2,16,16", "3,8,16", "3,16,16", "4,16,16", "2,4,32"]
+VX_SHAPES = ["16,8", "16,4", "8,8", "8,16", "16,16", "32,4"]
+PIPE_SHAPES = ["8,8,2", "8,8,3", "8,8,4", "16,4,2", "16,4,3", "16,8,2", "32,4,2"]
+_ONE = {"OLC_TB": "1,8,16", "OLC_VX": "0", "OLC_PIPE": "0"}
+# environment of each stencil path: scalar TMA tiles, 4-wide tiles, persistent
+# pipelines, temporal blocks (alone and with 4-wide remainders), register columns
+STENCIL_MODES = ([dict(_ONE)] + [dict(_ONE, OLC_VX=v) for v in VX_SHAPES]
+                 + [dict(_ONE, OLC_PIPE=p) for p in PIPE_SHAPES]
+                 + [dict(_ONE, OLC_TB=t) for t in TB_SHAPES] + [dict(_ONE, OLC_TB=TB_SHAPES[0], OLC_VX="8,8")]
+                 + [dict(_ONE, OLC_STENCIL_ORDER="forward", OLC_VX="8,8")]
+                 + [dict(_ONE, OLC_STENCIL="plain")])
 
 
-def test_diffuse_plain_and_tma_paths_agree(cuda, olc, monkeypatch):
-    """The TMA tile kernel, every temporal-block shape (T substeps per pass)
-    and the register-column kernel give the same bits, 7 substeps so odd
-    remainders run too."""
+@pytest.mark.parametrize("dims", [(68, 41, 37), (128, 34, 19)])
+def test_diffuse_plain_and_tma_paths_agree(cuda, olc, monkeypatch, dims):
+    """The scalar TMA tile kernel, every 4-wide tile shape, every
+    temporal-block shape (T substeps per pass) and the register-column kernel
+    give the oracle's bits; 7 substeps so odd remainders run too, and ragged
+    tiles in every direction."""
     import torch
 
     rng = np.random.default_rng(77)
-    nx, ny, nz = 68, 41, 37
+    nx, ny, nz = dims
     f = rng.random((nz, ny, nx), dtype=np.float32)
     spec = _lib.OlcDiffusion(diffusion=1.0, decay=0.02, boundary=0.4, substeps=7, has_sink=0)
     dims_c = (C.c_int32 * 3)(nx, ny, nz)
     outs = []
-    for mode in TB_SHAPES + ["plain"]:
-        if mode == "plain":
-            monkeypatch.setenv("OLC_STENCIL", "plain")
-        else:
-            monkeypatch.setenv("OLC_TB", mode)
+    for mode in STENCIL_MODES:
+        for k in ("OLC_STENCIL", "OLC_STENCIL_ORDER"):
+            monkeypatch.delenv(k, raising=False)
+        for k, v in mode.items():
+            monkeypatch.setenv(k, v)
         fd = to_dev(f, cuda)
         tmp = torch.empty_like(fd)
         _lib.check(olc.olc_stage_diffuse(dptr(fd), dptr(tmp), None, C.byref(dims_c), 1.0, 0.5, C.byref(spec), None))
         outs.append(to_host(fd))
     ref = oracle.diffuse(f, None, dx=1.0, dt=0.5, D=1.0, decay=0.02, boundary=0.4, substeps=7)
-    for mode, out in zip(TB_SHAPES + ["plain"], outs):
-        np.testing.assert_array_equal(out, ref, err_msg=mode)
+    for mode, out in zip(STENCIL_MODES, outs):
+        np.testing.assert_array_equal(out, ref, err_msg=str(mode))
 
 
 # ------------------------------------------------------------------ contact
