@@ -241,6 +241,64 @@ __device__ __forceinline__ float stencil_update(float xm, float xp, float ym, fl
     return fmaxf(__fmul_rn(u, inv_decay), 0.0f);
 }
 
+// Paired FP32: sm_100's add/sub/mul.rn.f32x2 round each half exactly like the
+// scalar .rn instruction.  The assembler does, however, fuse a paired multiply
+// that feeds a paired add or subtract into one fused multiply-add (one
+// rounding instead of two; measured on B200), so every product that feeds a
+// sum is formed with scalar __fmul_rn; the sums and the final product (which
+// only feeds the clamp) are paired.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pk2(float lo, float hi) {
+    f32x2 d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+    return d;
+}
+__device__ __forceinline__ float2 upk2(f32x2 d) {
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(d));
+    return make_float2(lo, hi);
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// stencil_update on two voxels at once (every argument a pair).
+__device__ __forceinline__ float2 stencil_update2(f32x2 xm, f32x2 xp, f32x2 ym, f32x2 yp, f32x2 zm, f32x2 zp,
+                                                  f32x2 c, f32x2 r2, f32x2 id2) {
+    const f32x2 s = add2(add2(add2(xm, xp), add2(ym, yp)), add2(zm, zp));
+    const float2 cc = upk2(c);
+    const float2 d = upk2(sub2(s, pk2(__fmul_rn(6.0f, cc.x), __fmul_rn(6.0f, cc.y))));
+    const float2 rr = upk2(r2);
+    const f32x2 u = add2(c, pk2(__fmul_rn(rr.x, d.x), __fmul_rn(rr.y, d.y)));
+    const float2 w = upk2(mul2(u, id2));
+    return make_float2(fmaxf(w.x, 0.0f), fmaxf(w.y, 0.0f));
+}
+
+// Four consecutive x voxels: centre row c, rows ym/yp, planes zm/zp, and the
+// left/right neighbours xl/xr of the group.
+__device__ __forceinline__ float4 stencil_update4(float xl, float xr, float4 c, float4 ym, float4 yp, float4 zm,
+                                                  float4 zp, float r, float inv_decay) {
+    const f32x2 r2 = pk2(r, r), id2 = pk2(inv_decay, inv_decay);
+    const f32x2 mid = pk2(c.y, c.z);  // x+1 of the first pair, x-1 of the second
+    const float2 a = stencil_update2(pk2(xl, c.x), mid, pk2(ym.x, ym.y), pk2(yp.x, yp.y), pk2(zm.x, zm.y),
+                                     pk2(zp.x, zp.y), pk2(c.x, c.y), r2, id2);
+    const float2 b = stencil_update2(mid, pk2(c.w, xr), pk2(ym.z, ym.w), pk2(yp.z, yp.w), pk2(zm.z, zm.w),
+                                     pk2(zp.z, zp.w), pk2(c.z, c.w), r2, id2);
+    return make_float4(a.x, a.y, b.x, b.y);
+}
+
 // The 64 x TYR x TZ output block at (x0, y0, z0) from its staged box.
 template <int TYR, int TZ>
 __device__ __forceinline__ void x4_tile(const float* tile, float* __restrict__ out, int x0, int y0, int z0, int nx,
@@ -266,11 +324,7 @@ __device__ __forceinline__ void x4_tile(const float* tile, float* __restrict__ o
         const float4 ym = *reinterpret_cast<const float4*>(pc - S::WX);
         const float4 yp = *reinterpret_cast<const float4*>(pc + S::WX);
         const float xl = pc[-1], xr = pc[4];
-        float4 v;
-        v.x = stencil_update(xl, c.y, ym.x, yp.x, zm.x, zp.x, c.x, r, inv_decay);
-        v.y = stencil_update(c.x, c.z, ym.y, yp.y, zm.y, zp.y, c.y, r, inv_decay);
-        v.z = stencil_update(c.y, c.w, ym.z, yp.z, zm.z, zp.z, c.z, r, inv_decay);
-        v.w = stencil_update(c.z, xr, ym.w, yp.w, zm.w, zp.w, c.w, r, inv_decay);
+        float4 v = stencil_update4(xl, xr, c, ym, yp, zm, zp, r, inv_decay);
         if (edge_y || z == 0 || z == nz - 1) {
             v = make_float4(bval, bval, bval, bval);
         } else {
@@ -420,6 +474,156 @@ __global__ void __launch_bounds__(16 * TYR, 1) k_substep_pipe(const __grid_const
         origin(k, &x0, &y0, &z0);
         x4_tile<TYR, TZ>(stages + (size_t)(k % NS) * (S::BYTES / 4), out, x0, y0, z0, nx, ny, nz, r, inv_decay,
                          bval);
+    }
+}
+
+// ---------------------------------------------------------------- two substeps per pass
+// k_substep_t2<TYR, ZC, NS>: two substeps in one pass over HBM, marching in z.
+// A CTA owns a 64 x TYR column patch of outputs over ZC planes.  Input planes
+// (80 x (TYR+4) floats: x from x0-8 so the box is 16-byte aligned, y from
+// y0-2) stream through a ring of NS shared-memory slots by TMA, NS-2 planes
+// ahead of use.  For each plane the CTA first computes the intermediate
+// (first-substep) plane over the patch grown by one voxel in x and y (18
+// four-wide groups x TYR+2 rows) into a ring of four shared planes, then the
+// output plane two planes behind it from three intermediate planes, and
+// stores that.  Every voxel of both levels goes through the single-substep
+// update (same operations, same order) with the face voxels pinned, so one
+// pass equals two k_substep_x4 launches bit for bit.  Intermediate voxels
+// outside the domain are computed from the TMA zero fill and only feed face
+// outputs, which are pinned.
+template <int TYR, int ZC, int NS>
+struct T2Shape {
+    static constexpr int TX = 64;
+    static constexpr int PW = 80, PH = TYR + 4;  // input plane (floats)
+    static constexpr int LW = 72, LH = TYR + 2;  // intermediate plane
+    static constexpr unsigned PBYTES = (unsigned)(PW * PH * 4);
+    static constexpr unsigned LBYTES = (unsigned)(LW * LH * 4);
+    static constexpr int L1_TASKS = 18 * LH, L2_TASKS = 16 * TYR;
+    static constexpr int THREADS = ((L1_TASKS > L2_TASKS ? L1_TASKS : L2_TASKS) + 31) / 32 * 32;
+    static constexpr size_t SMEM = (size_t)NS * PBYTES + 4 * (size_t)LBYTES + 8 * NS + 128;
+};
+
+// Four voxels at `c` (16-byte aligned) of a plane with row stride `W`, with
+// the planes below and above at the same offsets `zm`, `zp`.
+template <int W>
+__device__ __forceinline__ float4 update4(const float* zm, const float* c, const float* zp, float r,
+                                          float inv_decay) {
+    const float4 cc = *reinterpret_cast<const float4*>(c);
+    const float4 m = *reinterpret_cast<const float4*>(zm);
+    const float4 p = *reinterpret_cast<const float4*>(zp);
+    const float4 ym = *reinterpret_cast<const float4*>(c - W);
+    const float4 yp = *reinterpret_cast<const float4*>(c + W);
+    const float xl = c[-1], xr = c[4];
+    return stencil_update4(xl, xr, cc, ym, yp, m, p, r, inv_decay);
+}
+
+// Face voxels of the group starting at x (row y, plane z) take the boundary value.
+__device__ __forceinline__ float4 pin_faces(float4 v, int x, int y, int z, int nx, int ny, int nz, float bval) {
+    if (y == 0 || y == ny - 1 || z == 0 || z == nz - 1) return make_float4(bval, bval, bval, bval);
+    if (x == 0) v.x = bval;
+    if (x + 3 == nx - 1) v.w = bval;
+    return v;
+}
+
+template <int TYR, int ZC, int NS>
+__global__ void __launch_bounds__(T2Shape<TYR, ZC, NS>::THREADS, 1) k_substep_t2(
+    const __grid_constant__ CUtensorMap in_map, float* __restrict__ out, int nx, int ny, int nz, float r,
+    float inv_decay, float bval, olc_u32* status, int rev) {
+    using S = T2Shape<TYR, ZC, NS>;
+    static_assert(NS >= 4, "the ring holds the three planes in use plus at least one in flight");
+    extern __shared__ unsigned char t2_raw[];
+    const olc_u32 pad = (128u - (smem_u32(t2_raw) & 127u)) & 127u;
+    float* pin = reinterpret_cast<float*>(t2_raw + pad);                          // NS input planes
+    float* mid = reinterpret_cast<float*>(t2_raw + pad + (size_t)NS * S::PBYTES);  // 4 intermediate planes
+    const olc_u32 bar0 = smem_u32(t2_raw + pad + (size_t)NS * S::PBYTES + 4 * (size_t)S::LBYTES);
+    // tile order: x fastest, then y, then z chunk; reversed when rev != 0
+    const int ntx = (nx + S::TX - 1) / S::TX, nty = (ny + TYR - 1) / TYR;
+    int t = rev ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+    const int x0 = (t % ntx) * S::TX;
+    t /= ntx;
+    const int y0 = (t % nty) * TYR;
+    const int z0 = (t / nty) * ZC;
+    constexpr int NP = ZC + 4;  // input planes z0-2 .. z0+ZC+1
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < NS; ++k) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0 + 8 * k) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    auto issue = [&](int sidx) {  // thread 0: TMA load of input plane z0-2+sidx into slot sidx % NS
+        if (sidx >= NP) return;
+        const olc_u32 bar = bar0 + 8 * (sidx % NS);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(S::PBYTES) : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+            "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(pin + (size_t)(sidx % NS) * (S::PBYTES / 4))),
+            "l"(reinterpret_cast<unsigned long long>(&in_map)), "r"(x0 - 8), "r"(y0 - 2), "r"(z0 - 2 + sidx), "r"(bar)
+            : "memory");
+    };
+    auto wait_plane = [&](int sidx) -> bool {
+        const olc_u32 bar = bar0 + 8 * (sidx % NS), parity = (olc_u32)((sidx / NS) & 1);
+        for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it)
+            if (mbar_try_wait(bar, parity)) return true;
+        return false;
+    };
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NS; ++k) issue(k);
+    // this thread's intermediate task (group g1 of 18, row r1 of TYR+2) and output task
+    const int tid = threadIdx.x;
+    const bool has1 = tid < S::L1_TASKS, has2 = tid < S::L2_TASKS;
+    const int g1 = tid % 18, r1 = tid / 18;
+    const int g2 = tid & 15, r2 = tid >> 4;
+    const int x1 = x0 - 4 + 4 * g1, y1 = y0 - 1 + r1;
+    const int x2 = x0 + 4 * g2, y2 = y0 + r2;
+    const int poff = (r1 + 1) * S::PW + 4 + 4 * g1;  // intermediate voxel's centre in an input plane
+    const int moff1 = r1 * S::LW + 4 * g1;           // its slot in an intermediate plane
+    const int moff2 = (r2 + 1) * S::LW + 4 + 4 * g2;  // output voxel's centre in an intermediate plane
+    const size_t sz = (size_t)nx * ny;
+    // Iteration u computes intermediate plane u (input planes u..u+2) and
+    // output plane u-3 (intermediate planes u-3..u-1, finished in earlier
+    // iterations): the two are independent, so one barrier per iteration
+    // suffices; before it every thread has waited for input plane u+3, which
+    // the next iteration needs, and after it thread 0 refills input plane u's
+    // slot (last read by intermediate plane u).
+    auto fail = [&](int from, int last_issued) {  // thread 0: these planes may still be in flight
+        atomicOr(status, OLC_ST_TIMEOUT);
+        for (int sidx = from; sidx <= last_issued && sidx < NP; ++sidx) wait_plane(sidx);
+    };
+    {
+        const bool ok = wait_plane(0) && wait_plane(1) && wait_plane(2);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) fail(0, NS - 1);
+            return;
+        }
+    }
+    for (int u = 0; u <= ZC + 2; ++u) {
+        if (u < ZC + 2 && has1) {
+            const float* pm = pin + (size_t)(u % NS) * (S::PBYTES / 4) + poff;
+            const float* pc = pin + (size_t)((u + 1) % NS) * (S::PBYTES / 4) + poff;
+            const float* pp = pin + (size_t)((u + 2) % NS) * (S::PBYTES / 4) + poff;
+            float4 v = update4<S::PW>(pm, pc, pp, r, inv_decay);
+            v = pin_faces(v, x1, y1, z0 - 1 + u, nx, ny, nz, bval);
+            *reinterpret_cast<float4*>(mid + (size_t)(u & 3) * (S::LBYTES / 4) + moff1) = v;
+        }
+        if (u >= 3 && has2) {
+            const int z = z0 + u - 3;
+            if (z < nz && x2 < nx && y2 < ny) {
+                const float* mm = mid + (size_t)((u - 3) & 3) * (S::LBYTES / 4) + moff2;
+                const float* mc = mid + (size_t)((u - 2) & 3) * (S::LBYTES / 4) + moff2;
+                const float* mp = mid + (size_t)((u - 1) & 3) * (S::LBYTES / 4) + moff2;
+                float4 v = update4<S::LW>(mm, mc, mp, r, inv_decay);
+                v = pin_faces(v, x2, y2, z, nx, ny, nz, bval);
+                *reinterpret_cast<float4*>(out + (size_t)z * sz + (size_t)y2 * nx + x2) = v;
+            }
+        }
+        const bool ok = (u + 3 < NP) ? wait_plane(u + 3) : true;
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) fail(u + 3, u - 1 + NS);  // issued so far: planes < u + NS
+            return;
+        }
+        if (threadIdx.x == 0) issue(u + NS);
     }
 }
 
@@ -681,17 +885,51 @@ static void pipe_from_env(FieldMaps* m) {
     }
 }
 
+// Two-substep shapes compiled in (TYR, ZC, NS); OLC_T2="TYR,ZC,NS" selects
+// one, OLC_T2=0 runs one substep per pass.
+#define OLC_T2_SHAPES(X) X(8, 16, 6) X(8, 32, 6) X(12, 16, 6) X(12, 32, 6) X(16, 16, 6) X(16, 32, 6) X(8, 32, 8) X(8, 16, 8) X(16, 16, 8)
+
+// Off by default: on B200 with a 256^3 FP32 field the best shape, (16,16,8),
+// takes 27.1 us per substep against 21.0 for k_substep_x4.  It halves the
+// DRAM traffic but executes 2.3x the instructions of two single passes (the
+// intermediate plane covers the patch plus a one-voxel ring, and every plane
+// costs a barrier and a TMA wait), so it is issue-bound.
+static void t2_from_env(FieldMaps* m) {
+    m->T2Y = m->T2Z = m->T2N = 0;
+    const char* v = getenv("OLC_T2");
+    if (!v) return;
+    int a = 0, b = 0, c = 0;
+    if (sscanf(v, "%d,%d,%d", &a, &b, &c) != 3) {
+        m->T2Y = m->T2Z = m->T2N = 0;
+        return;
+    }
+    bool known = false;
+#define OLC_T2_MATCH(p, q, n) known = known || (a == p && b == q && c == n);
+    OLC_T2_SHAPES(OLC_T2_MATCH)
+#undef OLC_T2_MATCH
+    if (known) {
+        m->T2Y = a;
+        m->T2Z = b;
+        m->T2N = c;
+    }
+}
+
 bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3]) {
     using namespace tma;
     m->ok = false;
     tb_from_env(m);
     vx_from_env(m);
     pipe_from_env(m);
+    t2_from_env(m);
     const cuuint32_t box1[3] = {WX, WY, WZ};
     if (!encode_map(&m->single[0], a, dims, box1) || !encode_map(&m->single[1], b, dims, box1)) return false;
     if (m->VY > 0) {
         const cuuint32_t boxv[3] = {72, (cuuint32_t)(m->VY + 2), (cuuint32_t)(m->VZ + 2)};
         if (!encode_map(&m->vec[0], a, dims, boxv) || !encode_map(&m->vec[1], b, dims, boxv)) m->VY = m->VZ = 0;
+    }
+    if (m->T2Y > 0) {
+        const cuuint32_t boxt[3] = {80, (cuuint32_t)(m->T2Y + 4), 1};
+        if (!encode_map(&m->t2[0], a, dims, boxt) || !encode_map(&m->t2[1], b, dims, boxt)) m->T2Y = 0;
     }
     if (m->PY > 0) {
         const cuuint32_t boxp[3] = {72, (cuuint32_t)(m->PY + 2), (cuuint32_t)(m->PZ + 2)};
@@ -830,6 +1068,44 @@ static void launch_single(const FieldMaps& m, int cur, float* out, const FieldSt
     launch_substep_tma(m.single[cur], out, fs, status, s);
 }
 
+template <int TYR, int ZC, int NS>
+static void launch_t2(const CUtensorMap& map, float* out, const FieldStep& fs, olc_u32* status, int rev,
+                      cudaStream_t s) {
+    using S = T2Shape<TYR, ZC, NS>;
+    static int configured_mask = 0;  // per device (up to 32)
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 32 && !(configured_mask & (1 << dev))) {
+        cudaFuncSetAttribute(k_substep_t2<TYR, ZC, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
+        configured_mask |= 1 << dev;
+    }
+    const int tiles = ((fs.dims[0] + S::TX - 1) / S::TX) * ((fs.dims[1] + TYR - 1) / TYR) * ((fs.dims[2] + ZC - 1) / ZC);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(tiles);
+    cfg.blockDim = dim3(S::THREADS);
+    cfg.dynamicSmemBytes = S::SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_substep_t2<TYR, ZC, NS>, map, out, fs.dims[0], fs.dims[1], fs.dims[2], fs.r,
+                       fs.inv_decay, fs.bval, status, rev);
+}
+
+static bool launch_pair(const FieldMaps& m, int cur, float* out, const FieldStep& fs, olc_u32* status, int rev,
+                        cudaStream_t s) {
+#define OLC_T2_LAUNCH(p, q, n)                                   \
+    if (m.T2Y == p && m.T2Z == q && m.T2N == n) {                \
+        launch_t2<p, q, n>(m.t2[cur], out, fs, status, rev, s);  \
+        return true;                                             \
+    }
+    OLC_T2_SHAPES(OLC_T2_LAUNCH)
+#undef OLC_T2_LAUNCH
+    return false;
+}
+
 float* run_substeps_tma(float* a, float* b, const FieldMaps& m, int a_index, const FieldStep& fs, olc_u32* status,
                         cudaStream_t s) {
     float* bufs[2];
@@ -840,20 +1116,26 @@ float* run_substeps_tma(float* a, float* b, const FieldMaps& m, int a_index, con
     // alternate the tile order between substeps (OLC_STENCIL_ORDER=forward keeps one order)
     const char* order = getenv("OLC_STENCIL_ORDER");
     const bool alternate = !(order && std::string(order) == "forward");
+    int launch = 0;
     while (left > 0) {
-        if (m.T > 1 && left >= m.T) {
+        const int rev = alternate ? (launch & 1) : 0;
+        if (m.T2Y > 0 && left >= 2 && launch_pair(m, cur, bufs[1 - cur], fs, status, rev, s)) {
+            left -= 2;
+        } else if (m.T > 1 && left >= m.T) {
             launch_block(m, m.block[cur], bufs[1 - cur], fs, status, s);
             left -= m.T;
         } else {
-            launch_single(m, cur, bufs[1 - cur], fs, status, alternate ? (fs.substeps - left) & 1 : 0, s);
+            launch_single(m, cur, bufs[1 - cur], fs, status, rev, s);
             left -= 1;
         }
         cur = 1 - cur;
+        ++launch;
     }
     return bufs[cur];
 }
 
 int launches_for(const FieldMaps& m, int substeps) {
+    if (m.T2Y > 0) return substeps / 2 + substeps % 2;
     if (m.T <= 1) return substeps;
     return substeps / m.T + substeps % m.T;
 }

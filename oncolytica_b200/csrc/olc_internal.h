@@ -119,10 +119,12 @@ struct FieldMaps {
     int T = 1, TY = 8, TZ = 16;
     int VY = 0, VZ = 0;          // 4-wide single-substep kernel shape (0 = scalar k_substep_tma)
     int PY = 0, PZ = 0, PN = 0;  // persistent pipelined shape (0 = one tile per CTA)
+    int T2Y = 0, T2Z = 0, T2N = 0;  // two-substeps-per-pass shape (0 = one substep per pass)
     CUtensorMap single[2];
     CUtensorMap block[2];
     CUtensorMap vec[2];
     CUtensorMap pipe[2];
+    CUtensorMap t2[2];
 };
 bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3]);
 // Runs fs.substeps substeps starting from a (buffer index a_index of m).

@@ -222,22 +222,26 @@ def test_diffuse_bit_exact(cuda, olc, dims, substeps, decay, with_sink):
 TB_SHAPES = ["2,8,16", "2,8,32", "2,16,16", "3,8,16", "3,16,16", "4,16,16", "2,4,32"]
 VX_SHAPES = ["16,8", "16,4", "8,8", "8,16", "16,16", "32,4"]
 PIPE_SHAPES = ["8,8,2", "8,8,3", "8,8,4", "16,4,2", "16,4,3", "16,8,2", "32,4,2"]
-_ONE = {"OLC_TB": "1,8,16", "OLC_VX": "0", "OLC_PIPE": "0"}
+T2_SHAPES = ["8,16,6", "8,32,6", "12,16,6", "12,32,6", "16,16,6", "16,32,6", "8,32,8", "8,16,8", "16,16,8"]
+_ONE = {"OLC_TB": "1,8,16", "OLC_VX": "0", "OLC_PIPE": "0", "OLC_T2": "0"}
 # environment of each stencil path: scalar TMA tiles, 4-wide tiles, persistent
 # pipelines, temporal blocks (alone and with 4-wide remainders), register columns
 STENCIL_MODES = ([dict(_ONE)] + [dict(_ONE, OLC_VX=v) for v in VX_SHAPES]
                  + [dict(_ONE, OLC_PIPE=p) for p in PIPE_SHAPES]
+                 + [dict(_ONE, OLC_T2=t, OLC_VX="8,8") for t in T2_SHAPES]
+                 + [dict(_ONE, OLC_T2=T2_SHAPES[0], OLC_VX="8,8", OLC_STENCIL_ORDER="forward")]
                  + [dict(_ONE, OLC_TB=t) for t in TB_SHAPES] + [dict(_ONE, OLC_TB=TB_SHAPES[0], OLC_VX="8,8")]
                  + [dict(_ONE, OLC_STENCIL_ORDER="forward", OLC_VX="8,8")]
                  + [dict(_ONE, OLC_STENCIL="plain")])
 
 
-@pytest.mark.parametrize("dims", [(68, 41, 37), (128, 34, 19)])
+@pytest.mark.parametrize("dims", [(68, 41, 37), (128, 34, 19), (64, 64, 70)])
 def test_diffuse_plain_and_tma_paths_agree(cuda, olc, monkeypatch, dims):
-    """The scalar TMA tile kernel, every 4-wide tile shape, every
-    temporal-block shape (T substeps per pass) and the register-column kernel
-    give the oracle's bits; 7 substeps so odd remainders run too, and ragged
-    tiles in every direction."""
+    """The scalar TMA tile kernel, every 4-wide tile shape, every persistent
+    pipeline shape, every two-substeps-per-pass shape, every temporal-block
+    shape (T substeps per pass) and the register-column kernel give the
+    oracle's bits; 7 substeps so odd remainders run too, and ragged tiles and
+    z chunks in every direction."""
     import torch
 
     rng = np.random.default_rng(77)
