@@ -238,6 +238,43 @@ int olc_read_user_metrics(OlcSim* sim, void* out, size_t bytes, void* stream);
 int olc_read_life(OlcSim* sim, uint8_t* out, uint32_t rows, void* stream);
 int olc_set_user_metrics_size(OlcSim* sim, size_t bytes);
 
+/* ------------------------------------------------------------- batched mode
+ * Many independent simulations of one model in one handle, advanced by one
+ * launch per stage (no counterpart in the reference, which runs one
+ * simulation per engine).  The model is translated with a `_sim` column (the
+ * simulation index of each row, u32) after `_rng_state`; agent columns are
+ * shared by all simulations.  Each field buffer holds the simulations' grids
+ * back to back (olc_batch_field_offsets); each simulation's grid must have an
+ * x extent that is a multiple of 4.  Every simulation reproduces its solo run
+ * bit for bit (same keys, sort order, rule decisions, contact and stencil
+ * arithmetic); per-simulation FP64 reduction sums are exact up to order.
+ * olc_bind_agent_column, olc_set_contact (its margin applies to every
+ * simulation's domain), olc_set_rule_source, olc_set_user_metrics_size (bytes
+ * per simulation), olc_set_agent_count (all rows), olc_step, olc_read_counters,
+ * olc_read_life, olc_set_graphs, olc_set_profiling and olc_current_buffers
+ * (agent buffer) work on batch handles too; olc_bind_field, olc_set_params,
+ * olc_read_reductions and olc_bind_tissue do not. */
+int olc_create_batch(const OlcGeom* geoms, int n_sims, const OlcCaps* caps, OlcSim** out);
+
+/* n_sims + 1 voxel offsets: simulation k's grid is [offsets[k], offsets[k+1])
+ * of every field buffer (x fastest). */
+int olc_batch_field_offsets(const OlcSim* sim, uint64_t* offsets);
+
+/* Binds field `index` for every simulation; specs[k] is simulation k's
+ * diffusion (its own substep count; 0 = static). */
+int olc_bind_field_batch(OlcSim* sim, int index, float* a, float* b, float* sink, const OlcDiffusion* specs);
+
+/* n_sims Params blobs of `stride` bytes each, back to back. */
+int olc_set_params_batch(OlcSim* sim, const void* blob, size_t stride, void* stream);
+
+/* Which buffer (0 = a, 1 = b) holds each simulation's field: n_sims x
+ * n_fields bytes, simulation-major. */
+int olc_read_field_parity(OlcSim* sim, uint8_t* out, void* stream);
+
+/* Last collected step's reductions / metric accumulators of every simulation. */
+int olc_read_reductions_batch(OlcSim* sim, OlcReductions* out, void* stream);
+int olc_read_user_metrics_batch(OlcSim* sim, void* out, size_t bytes_per_sim, void* stream);
+
 /* ---------------------------------------------------- stateless stages */
 /* These run one stage on caller buffers; the parity tests call them. */
 

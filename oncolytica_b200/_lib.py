@@ -41,6 +41,8 @@ EXPORTS = (
     "olc_set_profiling", "olc_read_profile", "olc_stage_sort_pairs_noalloc",
     "olc_stage_rng", "olc_stage_keys", "olc_sort_scratch_bytes", "olc_stage_sort_pairs",
     "olc_stage_bin_ranges", "olc_stage_diffuse", "olc_stage_contact",
+    "olc_create_batch", "olc_batch_field_offsets", "olc_bind_field_batch", "olc_set_params_batch",
+    "olc_read_field_parity", "olc_read_reductions_batch", "olc_read_user_metrics_batch",
 )
 
 
@@ -158,6 +160,13 @@ _SIGS = {
     "olc_read_counters": (C.c_int, [_VP, C.POINTER(OlcCounters), _VP]),
     "olc_read_reductions": (C.c_int, [_VP, C.POINTER(OlcReductions), _VP]),
     "olc_read_user_metrics": (C.c_int, [_VP, _VP, C.c_size_t, _VP]),
+    "olc_create_batch": (C.c_int, [C.POINTER(OlcGeom), C.c_int, C.POINTER(OlcCaps), C.POINTER(_VP)]),
+    "olc_batch_field_offsets": (C.c_int, [_VP, C.POINTER(C.c_uint64)]),
+    "olc_bind_field_batch": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, C.POINTER(OlcDiffusion)]),
+    "olc_set_params_batch": (C.c_int, [_VP, _VP, C.c_size_t, _VP]),
+    "olc_read_field_parity": (C.c_int, [_VP, C.POINTER(C.c_uint8), _VP]),
+    "olc_read_reductions_batch": (C.c_int, [_VP, C.POINTER(OlcReductions), _VP]),
+    "olc_read_user_metrics_batch": (C.c_int, [_VP, _VP, C.c_size_t, _VP]),
     "olc_set_user_metrics_size": (C.c_int, [_VP, C.c_size_t]),
     "olc_read_life": (C.c_int, [_VP, _VP, C.c_uint32, _VP]),
     "olc_nvrtc_check": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_size_t]),

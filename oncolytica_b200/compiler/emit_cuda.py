@@ -143,6 +143,7 @@ class ModelLayout:
     params_size: int
     metrics: dict                   # name -> (slot, ty)
     radius_field: str | None = None
+    batched: bool = False           # a `_sim` column (simulation index) follows `_rng_state`
 
     def col_index(self, col: str) -> int:
         for i, (c, _, _) in enumerate(self.cell_cols):
@@ -160,7 +161,7 @@ class Program:
     digest: str = ""
 
 
-def make_layout(spec, radius_field: str | None = None) -> ModelLayout:
+def make_layout(spec, radius_field: str | None = None, batched: bool = False) -> ModelLayout:
     cell_fields = T.data_fields(spec.cell_class)
     if cell_fields.get("pos") is not T.vec3:
         raise CompilationError(f"Class '{spec.cell_class.__name__}' must have attribute 'pos: ol.vec3'.")
@@ -170,6 +171,9 @@ def make_layout(spec, radius_field: str | None = None) -> ModelLayout:
     ordered = {"pos": cell_fields["pos"]}
     ordered.update({k: v for k, v in cell_fields.items() if k != "pos"})
     cols = column_names(ordered) + [("_rng_state", "_rng_state", np.uint32)]
+    rng_col = len(cols) - 1
+    if batched:
+        cols.append(("_sim", "_sim", np.uint32))
     # device fields are the float32 chemistry fields; others stay on the host
     chem_fields = {k: v for k, v in T.data_fields(spec.chemistry_class).items() if ty_of_py(v) == F32}
     tissue_fields = {k: v for k, v in T.data_fields(spec.tissue_class).items()}
@@ -191,8 +195,8 @@ def make_layout(spec, radius_field: str | None = None) -> ModelLayout:
     if radius_field is not None and ty_of_py(cell_fields.get(radius_field)) != F32:
         raise CompilationError(f"contact radius field {radius_field!r} must be an ol.f32 field of the cell class")
     return ModelLayout(spec.cell_class, spec.chemistry_class, spec.tissue_class, spec.metrics_class,
-                       spec.params_class, ordered, cols, len(cols) - 1, list(chem_fields), tissue_fields, params,
-                       max(off, 4), metrics, radius_field)
+                       spec.params_class, ordered, cols, rng_col, list(chem_fields), tissue_fields, params,
+                       max(off, 4), metrics, radius_field, batched)
 
 
 def pack_params(layout: ModelLayout, params_obj: Any) -> bytes:
@@ -407,6 +411,8 @@ class Translator:
         src = "\n".join([
             "// Generated by oncolytica_b200.compiler from the model's Python rules.",
             '#include "olc_rule_rt.cuh"',
+            # rule bodies see the whole argument block, or one simulation of a batch
+            "typedef OlcSimView OlcP;" if self.L.batched else "typedef OlcRuleParams OlcP;",
             "",
             self.emit_constants(),
             self.emit_structs(),
@@ -427,7 +433,7 @@ class Translator:
         out = []
         cf = self.L.cell_fields
         out.append("struct Cell_t {\n" + "".join(f"    {ctype(ty_of_py(t))} {n};\n" for n, t in cf.items()) +
-                   "    olc_u32 _rng_state;\n};")
+                   "    olc_u32 _rng_state;\n" + ("    olc_u32 _sim;\n" if self.L.batched else "") + "};")
         chem = self.L.chem_fields
         out.append("struct Chem_t {\n" + ("".join(f"    float {n};\n" for n in chem) or "    int _unused;\n") +
                    "};")
@@ -455,18 +461,18 @@ class Translator:
                 st.append(f"    olc_col_out<{t}>(P, {idx}, i, c.{fname}.{a});")
             else:
                 fty = L.cell_fields.get(fname)
-                if fname != "_rng_state" and ty_of_py(fty) == BOOL:
+                if fname not in ("_rng_state", "_sim") and ty_of_py(fty) == BOOL:
                     ld.append(f"    c.{fname} = olc_col_in<int>(P, {idx}, i) != 0;")
                     st.append(f"    olc_col_out<int>(P, {idx}, i, c.{fname} ? 1 : 0);")
                 else:
                     ld.append(f"    c.{fname} = olc_col_in<{t}>(P, {idx}, i);")
                     st.append(f"    olc_col_out<{t}>(P, {idx}, i, c.{fname});")
             cp.append(f"    olc_col_out<olc_u32>(P, {idx}, i, olc_col_in<olc_u32>(P, {idx}, i));")
-        lines.append("__device__ __forceinline__ Cell_t olc_load_cell(const OlcRuleParams& P, olc_u32 i) {\n"
+        lines.append("__device__ __forceinline__ Cell_t olc_load_cell(const OlcP& P, olc_u32 i) {\n"
                      "    Cell_t c;\n" + "\n".join(ld) + "\n    return c;\n}")
-        lines.append("__device__ __forceinline__ void olc_store_cell(const OlcRuleParams& P, olc_u32 i, "
+        lines.append("__device__ __forceinline__ void olc_store_cell(const OlcP& P, olc_u32 i, "
                      "const Cell_t& c) {\n" + "\n".join(st) + "\n}")
-        lines.append("__device__ __forceinline__ void olc_copy_row(const OlcRuleParams& P, olc_u32 i) {\n" +
+        lines.append("__device__ __forceinline__ void olc_copy_row(const OlcP& P, olc_u32 i) {\n" +
                      "\n".join(cp) + "\n}")
         # defaults
         for kind in KINDS:
@@ -481,6 +487,8 @@ class Translator:
                 body.append(f"    c.{n} = {self.literal_of(getattr(proto, n), ty_of_py(t))};")
             if kind == "Cell":
                 body.append("    c._rng_state = 0u;")
+                if self.L.batched:
+                    body.append("    c._sim = 0u;")
             lines.append(f"__device__ __forceinline__ {STRUCT_NAME[kind]} olc_default_{kind.lower()}() {{\n" +
                          "\n".join(body) + "\n    return c;\n}")
             # copy_from keeps the receiver's private state
@@ -490,7 +498,7 @@ class Translator:
         # chemistry / tissue lookups
         chem_reads = "\n".join(f"    c.{n} = P.field[{i}] ? P.field[{i}][v] : 0.0f;"
                                for i, n in enumerate(L.chem_fields))
-        lines.append("__device__ __forceinline__ Chem_t olc_chem_at(const OlcRuleParams& P, olc_vec3 p) {\n"
+        lines.append("__device__ __forceinline__ Chem_t olc_chem_at(const OlcP& P, olc_vec3 p) {\n"
                      "    Chem_t c = olc_default_chemistry();\n    const olc_u32 v = olc_chem_index(P, p);\n" +
                      chem_reads + "\n    return c;\n}")
         tis_reads = []
@@ -504,7 +512,7 @@ class Translator:
                 tis_reads.append(f"    c.{n} = olc_tissue_col<olc_u32>(P, {i}, k);")
             else:
                 tis_reads.append(f"    c.{n} = olc_tissue_col<int>(P, {i}, k);")
-        lines.append("__device__ __forceinline__ Tissue_t olc_tissue_at(const OlcRuleParams& P, olc_vec3 p) {\n"
+        lines.append("__device__ __forceinline__ Tissue_t olc_tissue_at(const OlcP& P, olc_vec3 p) {\n"
                      "    Tissue_t c = olc_default_tissue();\n    if (!P.tissue) return c;\n"
                      "    const olc_u32 k = olc_tissue_index(P, p);\n" + "\n".join(tis_reads) +
                      "\n    return c;\n}")
@@ -530,7 +538,7 @@ class Translator:
 
     def prototype(self, info: FuncInfo) -> str:
         ret = ctype(info.ret) if info.ret is not None else "void"
-        ps = ["const OlcRuleParams& P", "olc_u32& _rng", "OlcCtx& _ctx"]
+        ps = ["const OlcP& P", "olc_u32& _rng", "OlcCtx& _ctx"]
         if info.kind in KINDS:
             ps.append(f"{STRUCT_NAME[info.kind]}& self" if info.self_by_ref
                       else f"{STRUCT_NAME[info.kind]} self")
@@ -567,40 +575,59 @@ class Translator:
         ctx.dead = false;
         ctx.born = false;
         ctx.multi = false;
+{self.view_decl("i < rows")}
         if (i < n_live) {{
-            Cell_t c = olc_load_cell(P, i);
+            Cell_t c = olc_load_cell({self.pv}, i);
             olc_u32 rng = c._rng_state;
-            {fn}(P, rng, ctx, c);
+            {fn}({self.pv}, rng, ctx, c);
             c._rng_state = rng;
-            olc_store_cell(P, i, c);
+            olc_store_cell({self.pv}, i, c);
             const bool dead = ctx.dead || P.life[i] != 0;  // an earlier rule's die() stands
             if (ctx.dead) P.life[i] = 1;
-            if (P.posr) P.posr[i] = make_float4(c.pos.x, c.pos.y, c.pos.z, dead ? -1.0f : {radius});
+            if (P.posr) P.posr[i] = make_float4(c.pos.x, c.pos.y, c.pos.z, dead ? -1.0f : {radius});{self.child_sim()}
         }} else if (i < rows) {{
-            olc_copy_row(P, i);  // child of an earlier rule this step: carried unchanged
+            olc_copy_row({self.pv}, i);  // child of an earlier rule this step: carried unchanged
         }}
         const olc_u32 slot = olc_birth_slot(P, ctx.born, tile, rows, s_warp, &s_excl);
         if (ctx.born && slot < P.capacity) {{
-            olc_store_cell(P, slot, ctx.child);
+            olc_store_cell({self.pv}, slot, ctx.child);
             P.life[slot] = 0;
         }}
         if (ctx.multi) atomicOr(P.counters + OLC_CTR_STATUS, OLC_ST_MULTI_DIVIDE);
     }}
 }}"""
 
+    @property
+    def pv(self) -> str:
+        """What the kernel passes to rule bodies: the argument block, or the view
+        of the agent's simulation in batched mode."""
+        return "V" if self.L.batched else "P"
+
+    def view_decl(self, has_row: str) -> str:
+        if not self.L.batched:
+            return ""
+        sim_col = len(self.L.cell_cols) - 1
+        return (f"        const olc_u32 sim = ({has_row}) ? reinterpret_cast<const olc_u32*>(P.cols_in[{sim_col}])[i] "
+                f": 0u;\n        const OlcSimView V = olc_sim_view(P, sim);")
+
+    def child_sim(self) -> str:
+        return "\n            ctx.child._sim = c._sim;  // a child belongs to its parent's simulation" \
+            if self.L.batched else ""
+
     def metric_kernel(self, kname: str, fn: str) -> str:
         return f"""extern "C" __global__ void __launch_bounds__(OLC_RULE_THREADS) {kname}(OlcRuleParams P) {{
     const olc_u32 rows = olc_total_rows(P.counters);
     for (olc_u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {{
         if (P.life[i]) continue;
-        Cell_t c = olc_load_cell(P, i);
+{self.view_decl("true")}
+        Cell_t c = olc_load_cell({self.pv}, i);
         olc_u32 rng = c._rng_state;
         OlcCtx ctx;
         ctx.i = i;
         ctx.dead = false;
         ctx.born = false;
         ctx.multi = false;
-        {fn}(P, rng, ctx, c);
+        {fn}({self.pv}, rng, ctx, c);
     }}
 }}"""
 

@@ -172,4 +172,35 @@ void launch_reset_reductions(OlcReductions* out_dev, int nfields, cudaStream_t s
 
 void launch_rng(olc_u32* states, olc_u32 n, int draws, float* out, float* dirs, cudaStream_t s);
 
+// ------------------------------------------------------------------ batched mode (olc_batch.cu)
+struct BatchArgs {
+    const OlcSimDesc* sims;  // device, n_sims records
+    int shift;               // sort key = (simulation << shift) | bin key
+    olc_u32 sentinel;        // key of dead rows: n_sims << shift
+    olc_u32 n_sims;
+};
+void launch_keys_batch(const BatchArgs& b, const float* x, const float* y, const float* z, const olc_u32* sim,
+                       const unsigned char* dead, const olc_u32* counters, olc_u32 n_cap, olc_u32* keys,
+                       olc_u32* hist, int passes, olc_u32* dead_ctr, cudaStream_t s);
+void launch_bin_ranges_batch(const BatchArgs& b, const olc_u32* keys, const olc_u32* n_dev, olc_u32 n_cap,
+                             olc_u32* ranges, cudaStream_t s);
+void launch_contact_batch(const BatchArgs& b, const float4* posr, const olc_u32* ranges, const olc_u32* sim,
+                          const olc_u32* n_dev, olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z,
+                          cudaStream_t s);
+// Field tiles: uint4 (simulation, tile x, tile y, tile z) of BATCH_TILE_X x
+// BATCH_TILE_Y x BATCH_TILE_Z voxels.
+constexpr int BATCH_TILE_X = 32, BATCH_TILE_Y = 16, BATCH_TILE_Z = 16;
+void launch_substep_batch(const BatchArgs& b, const uint4* tiles, olc_u32 n_tiles, const FieldStep* steps, int field,
+                          int n_fields, const unsigned char* fpar, int sub, float* fa, float* fb, cudaStream_t s);
+void launch_sink_batch(const BatchArgs& b, const uint4* tiles, olc_u32 n_tiles, const FieldStep* steps, int field,
+                       int n_fields, const unsigned char* fpar, float* fa, float* fb, float* sink, cudaStream_t s);
+void launch_flip_parity(const FieldStep* steps, int field, int n_fields, olc_u32 n_sims, unsigned char* fpar,
+                        cudaStream_t s);
+void launch_reduce_agents_batch(const BatchArgs& b, const ReduceArgs& a, const olc_u32* sim, const olc_u32* counters,
+                                olc_u32 n_cap, OlcReductions* out, cudaStream_t s);
+void launch_reduce_field_batch(const BatchArgs& b, const uint4* tiles, olc_u32 n_tiles, int field, int n_fields,
+                               const unsigned char* fpar, const float* fa, const float* fb, OlcReductions* out,
+                               cudaStream_t s);
+void launch_reset_reductions_batch(OlcReductions* out, olc_u32 n_sims, cudaStream_t s);
+
 }  // namespace olc

@@ -34,6 +34,25 @@
 
 #define OLC_RULE_THREADS 256
 
+// Batched mode: one record per simulation, in device memory.  Every
+// simulation of a batch runs the same model; geometry, parameters, metric
+// accumulators, field grids and bin table differ.
+struct OlcSimDesc {
+    int tdims[3];
+    float tvs;
+    int cdims[3];
+    float cvs;
+    float lo[3];                   // contact clamp box (domain shrunk by the margin)
+    float hi[3];
+    float center[3];               // radial-profile centre
+    float bin_width;               // radial-profile bin width
+    olc_u32 ranges_base;           // first entry of this simulation in the shared bin table
+    olc_u32 params_off;            // bytes into the params blob
+    olc_u32 metrics_off;           // bytes into the metric accumulators
+    olc_u32 substeps_mask;         // bit f: field f takes an odd number of substeps
+    unsigned long long field_off;  // first voxel of this simulation in every field buffer
+};
+
 struct OlcRuleParams {
     const void* in[OLC_MAX_AGENT_COLS];
     void* out[OLC_MAX_AGENT_COLS];
@@ -59,7 +78,65 @@ struct OlcRuleParams {
     int n_tissue_cols;
     olc_u32 tissue_stride;        // bytes between tissue columns
     int pad;
+    // batched mode (sims != null): per-simulation records, the agent-column
+    // tables in device memory, the second buffer of every field and the
+    // buffer parity of every (simulation, field)
+    const OlcSimDesc* sims;
+    const void* const* cols_in;
+    void* const* cols_out;
+    const float* field_alt[OLC_MAX_FIELD_COLS];
+    const unsigned char* fpar;
+    int n_fields;
+    int sim_col;
 };
+
+// What a rule body sees of one simulation of a batch (batched mode).  Member
+// names follow OlcRuleParams, so the same helpers serve both.
+struct OlcSimView {
+    const void* const* in;
+    void* const* out;
+    const float* field[OLC_MAX_FIELD_COLS];
+    float* sink[OLC_MAX_FIELD_COLS];
+    const olc_u32* ranges;
+    float4* posr;
+    const unsigned char* params;
+    void* metrics;
+    const unsigned char* tissue;
+    int tdims[3];
+    float tvs;
+    int cdims[3];
+    float cvs;
+    int n_tissue_cols;
+    olc_u32 tissue_stride;
+};
+
+__device__ __forceinline__ OlcSimView olc_sim_view(const OlcRuleParams& P, olc_u32 sim) {
+    const OlcSimDesc& d = P.sims[sim];
+    OlcSimView V;
+    V.in = P.cols_in;
+    V.out = P.cols_out;
+#pragma unroll
+    for (int f = 0; f < OLC_MAX_FIELD_COLS; ++f) {
+        const bool alt = f < P.n_fields && P.fpar[sim * (olc_u32)P.n_fields + f] != 0;
+        const float* base = alt ? P.field_alt[f] : P.field[f];
+        V.field[f] = base ? base + d.field_off : nullptr;
+        V.sink[f] = P.sink[f] ? P.sink[f] + d.field_off : nullptr;
+    }
+    V.ranges = P.ranges + 2ull * d.ranges_base;
+    V.posr = P.posr;
+    V.params = P.params + d.params_off;
+    V.metrics = static_cast<unsigned char*>(P.metrics) + d.metrics_off;
+    V.tissue = nullptr;  // tissue grids are not bound in batched mode
+    for (int k = 0; k < 3; ++k) {
+        V.tdims[k] = d.tdims[k];
+        V.cdims[k] = d.cdims[k];
+    }
+    V.tvs = d.tvs;
+    V.cvs = d.cvs;
+    V.n_tissue_cols = 0;
+    V.tissue_stride = 0;
+    return V;
+}
 
 // Rows processed by rule kernel k: live agents plus children of earlier rules.
 __device__ __forceinline__ olc_u32 olc_rule_rows(const olc_u32* ctr, int k) {
@@ -168,65 +245,75 @@ __device__ __forceinline__ float olc_mod_f(float a, float b) {
 }
 
 // ------------------------------------------------------------- grid lookups
-__device__ __forceinline__ olc_u32 olc_chem_index(const OlcRuleParams& P, olc_vec3 p) {
+template <class PT>
+__device__ __forceinline__ olc_u32 olc_chem_index(const PT& P, olc_vec3 p) {
     int cx = olc_bin_coord(p.x, P.cvs, P.cdims[0]);
     int cy = olc_bin_coord(p.y, P.cvs, P.cdims[1]);
     int cz = olc_bin_coord(p.z, P.cvs, P.cdims[2]);
     return ((olc_u32)cz * (olc_u32)P.cdims[1] + (olc_u32)cy) * (olc_u32)P.cdims[0] + (olc_u32)cx;
 }
 
-__device__ __forceinline__ olc_u32 olc_tissue_index(const OlcRuleParams& P, olc_vec3 p) {
+template <class PT>
+__device__ __forceinline__ olc_u32 olc_tissue_index(const PT& P, olc_vec3 p) {
     int tx = olc_bin_coord(p.x, P.tvs, P.tdims[0]);
     int ty = olc_bin_coord(p.y, P.tvs, P.tdims[1]);
     int tz = olc_bin_coord(p.z, P.tvs, P.tdims[2]);
     return olc_tissue_key(tx, ty, tz);
 }
 
-__device__ __forceinline__ olc_ivec3 olc_tissue_coord(const OlcRuleParams& P, olc_vec3 p) {
+template <class PT>
+__device__ __forceinline__ olc_ivec3 olc_tissue_coord(const PT& P, olc_vec3 p) {
     return olc_iv3(olc_bin_coord(p.x, P.tvs, P.tdims[0]), olc_bin_coord(p.y, P.tvs, P.tdims[1]),
                    olc_bin_coord(p.z, P.tvs, P.tdims[2]));
 }
 
 // Deposit into a field's sink (sum of first-order uptake rates of a voxel).
-__device__ __forceinline__ void olc_deposit(const OlcRuleParams& P, int field, olc_vec3 p, float rate) {
+template <class PT>
+__device__ __forceinline__ void olc_deposit(const PT& P, int field, olc_vec3 p, float rate) {
     float* s = P.sink[field];
     if (s) atomicAdd(s + olc_chem_index(P, p), rate);
 }
 
-template <typename T>
-__device__ __forceinline__ T olc_param(const OlcRuleParams& P, int offset) {
+template <typename T, class PT>
+__device__ __forceinline__ T olc_param(const PT& P, int offset) {
     return *reinterpret_cast<const T*>(P.params + offset);
 }
 
-template <typename T>
-__device__ __forceinline__ T olc_col_in(const OlcRuleParams& P, int col, olc_u32 i) {
+template <typename T, class PT>
+__device__ __forceinline__ T olc_col_in(const PT& P, int col, olc_u32 i) {
     return reinterpret_cast<const T*>(P.in[col])[i];
 }
 
-template <typename T>
-__device__ __forceinline__ void olc_col_out(const OlcRuleParams& P, int col, olc_u32 i, T v) {
+template <typename T, class PT>
+__device__ __forceinline__ void olc_col_out(const PT& P, int col, olc_u32 i, T v) {
     reinterpret_cast<T*>(P.out[col])[i] = v;
 }
 
-template <typename T>
-__device__ __forceinline__ T olc_tissue_col(const OlcRuleParams& P, int col, olc_u32 key) {
+template <typename T, class PT>
+__device__ __forceinline__ T olc_tissue_col(const PT& P, int col, olc_u32 key) {
     return reinterpret_cast<const T*>(P.tissue + (size_t)col * P.tissue_stride)[key];
 }
 
 // Metric accumulators: one 4-byte word per metric field.  Integer adds are
-// reduced across the converged lanes first, so a warp issues one atomic.
-__device__ __forceinline__ void olc_metric_add_i(const OlcRuleParams& P, int slot, int v) {
-    const olc_u32 m = __activemask();
+// reduced across the converged lanes that target the same word first (in a
+// batch, lanes of one warp can belong to different simulations), so each
+// group issues one atomic.
+template <class PT>
+__device__ __forceinline__ void olc_metric_add_i(const PT& P, int slot, int v) {
+    int* dst = reinterpret_cast<int*>(P.metrics) + slot;
+    const olc_u32 m = __match_any_sync(__activemask(), reinterpret_cast<unsigned long long>(dst));
     const int s = __reduce_add_sync(m, v);
-    if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && s != 0) atomicAdd(reinterpret_cast<int*>(P.metrics) + slot, s);
+    if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && s != 0) atomicAdd(dst, s);
 }
-__device__ __forceinline__ void olc_metric_add_u(const OlcRuleParams& P, int slot, olc_u32 v) {
-    const olc_u32 m = __activemask();
+template <class PT>
+__device__ __forceinline__ void olc_metric_add_u(const PT& P, int slot, olc_u32 v) {
+    olc_u32* dst = reinterpret_cast<olc_u32*>(P.metrics) + slot;
+    const olc_u32 m = __match_any_sync(__activemask(), reinterpret_cast<unsigned long long>(dst));
     const olc_u32 s = __reduce_add_sync(m, v);
-    if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && s != 0u)
-        atomicAdd(reinterpret_cast<olc_u32*>(P.metrics) + slot, s);
+    if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && s != 0u) atomicAdd(dst, s);
 }
-__device__ __forceinline__ void olc_metric_add_f(const OlcRuleParams& P, int slot, float v) {
+template <class PT>
+__device__ __forceinline__ void olc_metric_add_f(const PT& P, int slot, float v) {
     if (v != 0.0f) atomicAdd(reinterpret_cast<float*>(P.metrics) + slot, v);
 }
 

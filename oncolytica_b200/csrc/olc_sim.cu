@@ -15,6 +15,7 @@
 
 #include <nvrtc.h>
 
+#include <algorithm>
 #include <array>
 #include <cstdio>
 #include <cstring>
@@ -109,6 +110,26 @@ struct OlcSim {
     uint32_t prof_substeps = 0;
     std::vector<std::array<cudaEvent_t, OLC_PROF_EVENTS>> events;
 
+    // batched mode (n_sims > 0): many simulations of one model in one handle
+    olc_u32 n_sims = 0;
+    std::vector<OlcGeom> geoms;
+    std::vector<OlcSimDesc> desc_host;
+    OlcSimDesc* desc_dev = nullptr;
+    BatchArgs bargs = {};
+    std::vector<unsigned long long> field_off;        // n_sims + 1 voxel offsets into every field buffer
+    void** cols_dev = nullptr;                        // agent column tables: [2][OLC_MAX_AGENT_COLS]
+    bool cols_dirty = true;
+    unsigned char* fpar_dev = nullptr;                // field buffer parity per (simulation, field)
+    FieldStep* bsteps_dev = nullptr;                  // per (simulation, field)
+    std::vector<FieldStep> bsteps_host;
+    uint4* btiles_all = nullptr;                      // every field tile, simulation order
+    olc_u32 n_btiles = 0;
+    uint4* btiles_field[OLC_MAX_FIELDS] = {};         // per field, by substep count (descending)
+    std::vector<olc_u32> btile_count[OLC_MAX_FIELDS];  // [s] = tiles of simulations taking > s substeps
+    OlcReductions* red_batch_dev = nullptr;
+    OlcReductions* red_batch_host = nullptr;          // pinned
+    size_t params_stride = 0;
+
     // CUDA graphs of whole steps, keyed by the buffer parities at step start
     bool use_graphs = false;
     cudaStream_t capture_stream = nullptr;
@@ -197,6 +218,20 @@ OlcRuleParams make_rule_params(OlcSim* s, int rule_index, int in_buf) {
     P.radius_col = s->contact.radius_field;
     P.radius_const = s->contact.radius_const;
     P.rule_index = rule_index;
+    if (s->n_sims) {
+        P.sims = s->desc_dev;
+        P.cols_in = s->cols_dev + (size_t)in_buf * OLC_MAX_AGENT_COLS;
+        P.cols_out = s->cols_dev + (size_t)(1 - in_buf) * OLC_MAX_AGENT_COLS;
+        for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
+            P.field[f] = s->field[0][f];
+            P.field_alt[f] = s->field[1][f];
+        }
+        P.fpar = s->fpar_dev;
+        P.n_fields = (int)s->caps.n_fields;
+        P.sim_col = (int)s->caps.n_agent_fields - 1;
+        P.tissue = nullptr;
+        P.n_tissue_cols = 0;
+    }
     return P;
 }
 
@@ -345,6 +380,151 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
     return check(s, cudaGetLastError(), "step launch");
 }
 
+// One step of a batch: the stages of step_once over every simulation at once
+// (olc_batch.cu holds the kernels and the layout).
+int step_once_batch(OlcSim* s, int collect, cudaStream_t st) {
+    const olc_u32 cap = s->caps.max_agents;
+    const olc_u32 F = s->caps.n_fields;
+    if (s->cols_dirty) {
+        void* tab[2 * OLC_MAX_AGENT_COLS] = {};
+        for (int b = 0; b < 2; ++b)
+            for (olc_u32 c = 0; c < s->caps.n_agent_fields; ++c) tab[b * OLC_MAX_AGENT_COLS + c] = s->col[b][c];
+        OLC_TRY(check(s, cudaMemcpy(s->cols_dev, tab, sizeof(tab), cudaMemcpyHostToDevice), "column tables"));
+        s->cols_dirty = false;
+    }
+    if (s->profiling && (size_t)s->prof_step >= s->events.size()) {
+        std::array<cudaEvent_t, OLC_PROF_EVENTS> ev;
+        for (auto& e : ev) OLC_TRY(check(s, cudaEventCreate(&e), "cudaEventCreate"));
+        s->events.push_back(ev);
+    }
+    uint64_t launches = 0;
+    uint32_t substeps = 0;
+    const BatchArgs& B = s->bargs;
+    mark(s, 0, st);
+    // 1. fields: sinks, then every field's substeps over the simulations that take them
+    for (olc_u32 f = 0; f < F; ++f) {
+        if (!s->field_bound[f] || !s->sink[f]) continue;
+        launch_sink_batch(B, s->btiles_all, s->n_btiles, s->bsteps_dev, (int)f, (int)F, s->fpar_dev, s->field[0][f],
+                          s->field[1][f], s->sink[f], st);
+        ++launches;
+    }
+    mark(s, 1, st);
+    for (olc_u32 f = 0; f < F; ++f) {
+        if (!s->field_bound[f]) continue;
+        const std::vector<olc_u32>& cnt = s->btile_count[f];
+        for (size_t sub = 0; sub < cnt.size(); ++sub) {
+            launch_substep_batch(B, s->btiles_field[f], cnt[sub], s->bsteps_dev, (int)f, (int)F, s->fpar_dev, (int)sub,
+                                 s->field[0][f], s->field[1][f], st);
+            ++launches;
+        }
+        substeps += (uint32_t)cnt.size();
+        launch_flip_parity(s->bsteps_dev, (int)f, (int)F, s->n_sims, s->fpar_dev, st);
+        ++launches;
+    }
+    mark(s, 2, st);
+    // 2. grid + compaction
+    const int passes = (s->key_bits + 7) / 8;
+    const int ac = s->agent_cur;
+    const int sim_col = (int)s->caps.n_agent_fields - 1;
+    OLC_TRY(check(s, cudaMemsetAsync(s->sc.hist, 0, MAX_PASSES * RADIX * 4, st), "memset hist"));
+    launch_keys_batch(B, static_cast<const float*>(s->col[ac][0]), static_cast<const float*>(s->col[ac][1]),
+                      static_cast<const float*>(s->col[ac][2]), static_cast<const olc_u32*>(s->col[ac][sim_col]),
+                      s->life, s->counters, cap, s->keys_in, s->sc.hist, passes, s->counters + OLC_CTR_DEAD_TMP, st);
+    run_sort(s->keys_in, nullptr, s->keys, s->vals, s->counters + OLC_CTR_ROWS, 0, cap, s->key_bits, s->sc, true,
+             s->counters, cap, st);
+    OLC_TRY(check(s, cudaMemsetAsync(s->ranges, 0, (size_t)s->n_table * 8, st), "memset ranges"));
+    launch_bin_ranges_batch(B, s->keys, s->counters + OLC_CTR_ROWS, cap, s->ranges, st);
+    PermuteArgs pa;
+    std::memset(&pa, 0, sizeof(pa));
+    pa.ncols = (int)s->caps.n_agent_fields;
+    for (int c = 0; c < pa.ncols; ++c) {
+        pa.src[c] = s->col[ac][c];
+        pa.dst[c] = s->col[1 - ac][c];
+    }
+    pa.radius_col = s->contact.radius_field;
+    pa.radius_const = s->contact.radius_const;
+    pa.write_posr = (s->contact.enabled && s->n_cell_rules == 0) ? 1 : 0;
+    pa.posr = s->posr;
+    pa.life = s->life;
+    launch_permute(s->vals, s->counters, cap, pa, st);
+    s->agent_cur = 1 - ac;
+    launches += 4 + (uint64_t)passes;
+    mark(s, 3, st);
+    // 3. cell rules
+    if (s->n_cell_rules > 0) {
+        OLC_TRY(check(s, cudaMemsetAsync(s->birth_lb, 0, (size_t)s->n_cell_rules * s->rule_tiles * 4, st),
+                      "memset birth look-back"));
+    }
+    int cell_idx = 0;
+    for (size_t k = 0; k < s->funcs.size(); ++k) {
+        if (s->kinds[k] != 0) continue;
+        OlcRuleParams P = make_rule_params(s, cell_idx, s->agent_cur);
+        OLC_TRY(launch_rule(s, (int)k, P, st));
+        s->agent_cur = 1 - s->agent_cur;
+        ++cell_idx;
+        ++launches;
+    }
+    mark(s, 4, st);
+    // 4. contact
+    const int cc = s->agent_cur;
+    if (s->contact.enabled) {
+        launch_contact_batch(B, s->posr, s->ranges, static_cast<const olc_u32*>(s->col[cc][sim_col]),
+                             s->counters + OLC_CTR_N, cap, s->contact_dev, static_cast<float*>(s->col[cc][0]),
+                             static_cast<float*>(s->col[cc][1]), static_cast<float*>(s->col[cc][2]), st);
+        ++launches;
+    }
+    mark(s, 5, st);
+    // 5. per-simulation reductions + metric rules
+    if (collect) {
+        launch_reset_reductions_batch(s->red_batch_dev, s->n_sims, st);
+        ReduceArgs ra;
+        ra.x = static_cast<const float*>(s->col[cc][0]);
+        ra.y = static_cast<const float*>(s->col[cc][1]);
+        ra.z = static_cast<const float*>(s->col[cc][2]);
+        ra.state = s->caps.state_field >= 0 ? static_cast<const int*>(s->col[cc][s->caps.state_field]) : nullptr;
+        ra.life = s->life;
+        ra.cx = ra.cy = ra.cz = 0.0f;
+        ra.bin_width = 1.0f;
+        launch_reduce_agents_batch(B, ra, static_cast<const olc_u32*>(s->col[cc][sim_col]), s->counters, cap,
+                                   s->red_batch_dev, st);
+        launches += 3;
+        for (olc_u32 f = 0; f < F; ++f) {
+            if (!s->field_bound[f]) continue;
+            launch_reduce_field_batch(B, s->btiles_all, s->n_btiles, (int)f, (int)F, s->fpar_dev, s->field[0][f],
+                                      s->field[1][f], s->red_batch_dev, st);
+            ++launches;
+        }
+        if (s->metrics_dev && s->metrics_bytes) {
+            OLC_TRY(check(s, cudaMemsetAsync(s->metrics_dev, 0, s->metrics_bytes * s->n_sims, st), "memset metrics"));
+        }
+        for (size_t k = 0; k < s->funcs.size(); ++k) {
+            if (s->kinds[k] != 1) continue;
+            OlcRuleParams P = make_rule_params(s, 0, cc);
+            OLC_TRY(launch_rule(s, (int)k, P, st));
+            ++launches;
+        }
+    }
+    mark(s, 6, st);
+    if (s->profiling) {
+        s->prof_step++;
+        s->prof_launches += launches;
+        s->prof_substeps += substeps;
+    }
+    s->total_launches += launches;
+    s->steps++;
+    return check(s, cudaGetLastError(), "batch step launch");
+}
+
+int step_any(OlcSim* s, int collect, cudaStream_t st) {
+    return s->n_sims ? step_once_batch(s, collect, st) : step_once(s, collect, st);
+}
+
+int upload_desc(OlcSim* s) {
+    return check(s, cudaMemcpy(s->desc_dev, s->desc_host.data(), sizeof(OlcSimDesc) * s->n_sims,
+                               cudaMemcpyHostToDevice),
+                 "upload simulation records");
+}
+
 int field_mask(const OlcSim* s) {
     int m = 0;
     for (int f = 0; f < OLC_MAX_FIELDS; ++f) m |= (s->field_cur[f] & 1) << f;
@@ -382,13 +562,13 @@ int step_graph(OlcSim* s, int collect, cudaStream_t st) {
         for (int k : s->graph_seen) seen |= (k == key);
         if (!seen) {
             s->graph_seen.push_back(key);
-            return step_once(s, collect, st);
+            return step_any(s, collect, st);
         }
         if (!s->capture_stream)
             OLC_TRY(check(s, cudaStreamCreateWithFlags(&s->capture_stream, cudaStreamNonBlocking), "capture stream"));
         const uint64_t steps0 = s->steps, launches0 = s->total_launches;
         OLC_TRY(check(s, cudaStreamBeginCapture(s->capture_stream, cudaStreamCaptureModeThreadLocal), "begin capture"));
-        const int rc = step_once(s, collect, s->capture_stream);
+        const int rc = step_any(s, collect, s->capture_stream);
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamEndCapture(s->capture_stream, &graph);
         StepGraph ng;
@@ -431,24 +611,34 @@ const char* olc_last_error(const OlcSim* sim) {
     return get_error();
 }
 
-int olc_create(const OlcGeom* geom, const OlcCaps* caps, OlcSim** out) {
-    if (!geom || !caps || !out) return fail(nullptr, OLC_ERR_ARG, "olc_create: null argument");
-    std::string err;
-    if (!geom_ok(*geom, &err)) return fail(nullptr, OLC_ERR_ARG, "olc_create: " + err);
-    if (caps->max_agents == 0 || caps->max_agents > (1u << 30))
-        return fail(nullptr, OLC_ERR_ARG, "olc_create: max_agents must be in [1, 2^30]");
-    if (caps->n_agent_fields < 3 || caps->n_agent_fields > OLC_MAX_AGENT_FIELDS)
-        return fail(nullptr, OLC_ERR_ARG, "olc_create: n_agent_fields must be in [3, 64] (pos.x/y/z first)");
-    if (caps->n_fields > OLC_MAX_FIELDS) return fail(nullptr, OLC_ERR_ARG, "olc_create: too many fields");
-    if (caps->state_field >= (int)caps->n_agent_fields)
-        return fail(nullptr, OLC_ERR_ARG, "olc_create: state_field out of range");
-    OlcSim* s = new OlcSim();
-    s->geom = *geom;
-    s->caps = *caps;
-    s->bins = make_bin_grid(*geom);
-    s->key_bits = key_bits_for(s->bins.sentinel);
-    s->n_table = s->bins.sentinel + 1u;
-    const olc_u32 cap = caps->max_agents;
+}  // extern "C"
+
+namespace {
+
+bool caps_ok(const OlcCaps* caps, const char* who, std::string* err) {
+    if (caps->max_agents == 0 || caps->max_agents > (1u << 30)) {
+        *err = std::string(who) + ": max_agents must be in [1, 2^30]";
+        return false;
+    }
+    if (caps->n_agent_fields < 3 || caps->n_agent_fields > OLC_MAX_AGENT_FIELDS) {
+        *err = std::string(who) + ": n_agent_fields must be in [3, 64] (pos.x/y/z first)";
+        return false;
+    }
+    if (caps->n_fields > OLC_MAX_FIELDS) {
+        *err = std::string(who) + ": too many fields";
+        return false;
+    }
+    if (caps->state_field >= (int)caps->n_agent_fields) {
+        *err = std::string(who) + ": state_field out of range";
+        return false;
+    }
+    return true;
+}
+
+// Allocates the library-owned buffers of a handle whose geometry fields
+// (geom, caps, bins, key_bits, n_table) are set.
+int alloc_common(OlcSim* s) {
+    const olc_u32 cap = s->caps.max_agents;
     int rc = OLC_OK;
     auto A = [&](int r) {
         if (rc == OLC_OK) rc = r;
@@ -478,12 +668,129 @@ int olc_create(const OlcGeom* geom, const OlcCaps* caps, OlcSim** out) {
         A(check(s, cudaMemset(s->red_dev, 0, sizeof(OlcReductions)), "memset reductions"));
         A(check(s, cudaMemset(s->red_scratch.tickets, 0, RED_TICKETS * sizeof(olc_u32)), "memset tickets"));
     }
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int olc_create(const OlcGeom* geom, const OlcCaps* caps, OlcSim** out) {
+    if (!geom || !caps || !out) return fail(nullptr, OLC_ERR_ARG, "olc_create: null argument");
+    std::string err;
+    if (!geom_ok(*geom, &err)) return fail(nullptr, OLC_ERR_ARG, "olc_create: " + err);
+    if (!caps_ok(caps, "olc_create", &err)) return fail(nullptr, OLC_ERR_ARG, err);
+    OlcSim* s = new OlcSim();
+    s->geom = *geom;
+    s->caps = *caps;
+    s->bins = make_bin_grid(*geom);
+    s->key_bits = key_bits_for(s->bins.sentinel);
+    s->n_table = s->bins.sentinel + 1u;
+    const int rc = alloc_common(s);
     if (rc != OLC_OK) {
         std::string msg = s->err;
         olc_destroy(s);
         return fail(nullptr, rc, msg);
     }
     *out = s;
+    return OLC_OK;
+}
+
+int olc_create_batch(const OlcGeom* geoms, int n_sims, const OlcCaps* caps, OlcSim** out) {
+    if (!geoms || !caps || !out || n_sims < 1) return fail(nullptr, OLC_ERR_ARG, "olc_create_batch: bad arguments");
+    std::string err;
+    if (!caps_ok(caps, "olc_create_batch", &err)) return fail(nullptr, OLC_ERR_ARG, err);
+    int shift = 1;
+    olc_u64 n_table = 0, voxels = 0;
+    for (int k = 0; k < n_sims; ++k) {
+        if (!geom_ok(geoms[k], &err))
+            return fail(nullptr, OLC_ERR_ARG, "olc_create_batch: simulation " + std::to_string(k) + ": " + err);
+        const olc_u32 top = olc_tissue_key(geoms[k].tissue_dims[0], geoms[k].tissue_dims[1], geoms[k].tissue_dims[2]);
+        shift = std::max(shift, key_bits_for(top));
+        n_table += (olc_u64)top + 1u;
+        voxels += (olc_u64)geoms[k].chem_dims[0] * geoms[k].chem_dims[1] * geoms[k].chem_dims[2];
+    }
+    if (shift + key_bits_for((olc_u32)n_sims) > 32)
+        return fail(nullptr, OLC_ERR_ARG, "olc_create_batch: simulation index and bin key exceed 32 key bits");
+    if (n_table >= (1ull << 31)) return fail(nullptr, OLC_ERR_ARG, "olc_create_batch: bin tables too large");
+    OlcSim* s = new OlcSim();
+    s->geom = geoms[0];
+    s->caps = *caps;
+    s->n_sims = (olc_u32)n_sims;
+    s->geoms.assign(geoms, geoms + n_sims);
+    s->bins = make_bin_grid(geoms[0]);
+    s->bargs.shift = shift;
+    s->bargs.n_sims = (olc_u32)n_sims;
+    s->bargs.sentinel = (olc_u32)n_sims << shift;
+    s->key_bits = key_bits_for(s->bargs.sentinel);
+    s->n_table = (olc_u32)n_table;
+    // per-simulation records, bin-table bases, field offsets, field tiles
+    s->desc_host.resize(n_sims);
+    s->field_off.assign(n_sims + 1, 0ull);
+    std::vector<uint4> tiles;
+    olc_u64 base = 0;
+    for (int k = 0; k < n_sims; ++k) {
+        const OlcGeom& g = geoms[k];
+        OlcSimDesc& d = s->desc_host[k];
+        std::memset(&d, 0, sizeof(d));
+        for (int i = 0; i < 3; ++i) {
+            d.tdims[i] = g.tissue_dims[i];
+            d.cdims[i] = g.chem_dims[i];
+            d.lo[i] = g.domain_lo[i];
+            d.hi[i] = g.domain_hi[i];
+            d.center[i] = 0.5f * (g.domain_lo[i] + g.domain_hi[i]);
+        }
+        d.tvs = g.tissue_voxel_size;
+        d.cvs = g.chem_voxel_size;
+        d.bin_width = caps->radial_bin_width > 0.0f ? caps->radial_bin_width : 1.0f;
+        d.ranges_base = (olc_u32)base;
+        base += (olc_u64)olc_tissue_key(g.tissue_dims[0], g.tissue_dims[1], g.tissue_dims[2]) + 1u;
+        d.field_off = s->field_off[k];
+        s->field_off[k + 1] = s->field_off[k] + (olc_u64)g.chem_dims[0] * g.chem_dims[1] * g.chem_dims[2];
+        const int tx = (g.chem_dims[0] + BATCH_TILE_X - 1) / BATCH_TILE_X;
+        const int ty = (g.chem_dims[1] + BATCH_TILE_Y - 1) / BATCH_TILE_Y;
+        const int tz = (g.chem_dims[2] + BATCH_TILE_Z - 1) / BATCH_TILE_Z;
+        for (int z = 0; z < tz; ++z)
+            for (int y = 0; y < ty; ++y)
+                for (int x = 0; x < tx; ++x) tiles.push_back(make_uint4((unsigned)k, (unsigned)x, (unsigned)y, (unsigned)z));
+    }
+    s->n_btiles = (olc_u32)tiles.size();
+    s->bsteps_host.assign((size_t)n_sims * std::max<olc_u32>(1u, caps->n_fields), FieldStep{});
+    int rc = alloc_common(s);
+    auto A = [&](int r) {
+        if (rc == OLC_OK) rc = r;
+    };
+    A(dev_alloc(s, &s->desc_dev, sizeof(OlcSimDesc) * n_sims, "simulation records"));
+    A(dev_alloc(s, &s->cols_dev, sizeof(void*) * 2 * OLC_MAX_AGENT_COLS, "column tables"));
+    A(dev_alloc(s, &s->fpar_dev, (size_t)n_sims * OLC_MAX_FIELDS, "field parity"));
+    A(dev_alloc(s, &s->bsteps_dev, sizeof(FieldStep) * s->bsteps_host.size(), "field steps"));
+    A(dev_alloc(s, &s->btiles_all, sizeof(uint4) * tiles.size(), "field tiles"));
+    A(dev_alloc(s, &s->red_batch_dev, sizeof(OlcReductions) * n_sims, "batch reductions"));
+    A(check(s, cudaMallocHost(reinterpret_cast<void**>(&s->red_batch_host), sizeof(OlcReductions) * n_sims),
+            "pinned batch reductions"));
+    if (rc == OLC_OK) {
+        A(check(s, cudaMemcpy(s->desc_dev, s->desc_host.data(), sizeof(OlcSimDesc) * n_sims, cudaMemcpyHostToDevice),
+                "upload simulation records"));
+        A(check(s, cudaMemcpy(s->btiles_all, tiles.data(), sizeof(uint4) * tiles.size(), cudaMemcpyHostToDevice),
+                "upload field tiles"));
+        A(check(s, cudaMemset(s->fpar_dev, 0, (size_t)n_sims * OLC_MAX_FIELDS), "memset field parity"));
+        A(check(s, cudaMemset(s->bsteps_dev, 0, sizeof(FieldStep) * s->bsteps_host.size()), "memset field steps"));
+        A(check(s, cudaMemset(s->red_batch_dev, 0, sizeof(OlcReductions) * n_sims), "memset batch reductions"));
+    }
+    s->bargs.sims = s->desc_dev;
+    if (rc != OLC_OK) {
+        std::string msg = s->err;
+        olc_destroy(s);
+        return fail(nullptr, rc, msg);
+    }
+    *out = s;
+    return OLC_OK;
+}
+
+int olc_batch_field_offsets(const OlcSim* s, uint64_t* offsets) {
+    if (!s || !offsets) return fail(nullptr, OLC_ERR_ARG, "olc_batch_field_offsets: null argument");
+    if (!s->n_sims) return fail(const_cast<OlcSim*>(s), OLC_ERR_STATE, "olc_batch_field_offsets: not a batch handle");
+    for (olc_u32 k = 0; k <= s->n_sims; ++k) offsets[k] = s->field_off[k];
     return OLC_OK;
 }
 
@@ -508,6 +815,14 @@ int olc_destroy(OlcSim* s) {
     cudaFree(s->red_dev);
     cudaFree(s->red_scratch.partials);
     cudaFree(s->red_scratch.tickets);
+    cudaFree(s->desc_dev);
+    cudaFree(s->cols_dev);
+    cudaFree(s->fpar_dev);
+    cudaFree(s->bsteps_dev);
+    cudaFree(s->btiles_all);
+    for (int f = 0; f < OLC_MAX_FIELDS; ++f) cudaFree(s->btiles_field[f]);
+    cudaFree(s->red_batch_dev);
+    if (s->red_batch_host) cudaFreeHost(s->red_batch_host);
     cudaFree(s->metrics_dev);
     if (s->params_host) cudaFreeHost(s->params_host);
     if (s->red_host) cudaFreeHost(s->red_host);
@@ -523,6 +838,7 @@ int olc_bind_agent_column(OlcSim* s, int index, void* a, void* b) {
     drop_graphs(s);
     s->col[0][index] = a;
     s->col[1][index] = b;
+    s->cols_dirty = true;
     return OLC_OK;
 }
 
@@ -530,6 +846,7 @@ int olc_bind_field(OlcSim* s, int index, float* a, float* b, float* sink, const 
     if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
     if (index < 0 || index >= (int)s->caps.n_fields || !a || !b || !spec)
         return fail(s, OLC_ERR_ARG, "olc_bind_field: bad index or null argument");
+    if (s->n_sims) return fail(s, OLC_ERR_STATE, "olc_bind_field: batch handle (use olc_bind_field_batch)");
     std::string err;
     FieldStep fs = {};
     if (spec->substeps != 0 &&
@@ -553,6 +870,7 @@ int olc_bind_tissue(OlcSim* s, const void* cols, int n_cols, size_t stride_bytes
     if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
     if (n_cols < 0 || (n_cols > 0 && (!cols || stride_bytes < (size_t)s->n_table * 4)))
         return fail(s, OLC_ERR_ARG, "olc_bind_tissue: columns must hold voxel_table_size entries");
+    if (s->n_sims && n_cols > 0) return fail(s, OLC_ERR_STATE, "olc_bind_tissue: tissue grids are not bound in batched mode");
     drop_graphs(s);
     s->tissue = static_cast<const unsigned char*>(cols);
     s->tissue_cols = n_cols;
@@ -577,6 +895,14 @@ int olc_set_contact(OlcSim* s, const OlcContact* c) {
     d.mobility = c->mobility;
     d.max_disp = c->max_disp;
     d.dt = s->caps.dt;
+    if (s->n_sims) {
+        for (olc_u32 k = 0; k < s->n_sims; ++k)
+            for (int i = 0; i < 3; ++i) {
+                s->desc_host[k].lo[i] = s->geoms[k].domain_lo[i] + c->margin;
+                s->desc_host[k].hi[i] = s->geoms[k].domain_hi[i] - c->margin;
+            }
+        return upload_desc(s);
+    }
     return OLC_OK;
 }
 
@@ -657,6 +983,7 @@ int olc_set_rule_source(OlcSim* s, const char* src, const char* const* kernels, 
 
 int olc_set_params(OlcSim* s, const void* blob, size_t bytes, void* stream) {
     if (!s || (bytes && !blob)) return fail(s, OLC_ERR_ARG, "olc_set_params: bad arguments");
+    if (s->n_sims) return fail(s, OLC_ERR_STATE, "olc_set_params: batch handle (use olc_set_params_batch)");
     if (bytes == 0) return OLC_OK;
     cudaStream_t st = as_stream(stream);
     if (bytes > s->params_cap) {
@@ -685,9 +1012,14 @@ int olc_set_user_metrics_size(OlcSim* s, size_t bytes) {
     cudaFree(s->metrics_dev);
     s->metrics_dev = nullptr;
     s->metrics_bytes = bytes;
+    const size_t copies = s->n_sims ? s->n_sims : 1;  // one accumulator block per simulation
     if (bytes) {
-        OLC_TRY(dev_alloc(s, &s->metrics_dev, bytes, "metrics"));
-        OLC_TRY(check(s, cudaMemset(s->metrics_dev, 0, bytes), "memset metrics"));
+        OLC_TRY(dev_alloc(s, &s->metrics_dev, bytes * copies, "metrics"));
+        OLC_TRY(check(s, cudaMemset(s->metrics_dev, 0, bytes * copies), "memset metrics"));
+    }
+    if (s->n_sims) {
+        for (olc_u32 k = 0; k < s->n_sims; ++k) s->desc_host[k].metrics_off = (olc_u32)(k * bytes);
+        return upload_desc(s);
     }
     return OLC_OK;
 }
@@ -744,7 +1076,7 @@ int olc_step(OlcSim* s, int nsteps, int collect, void* stream) {
         if (s->use_graphs && !s->profiling) {
             OLC_TRY(step_graph(s, c, st));
         } else {
-            OLC_TRY(step_once(s, c, st));
+            OLC_TRY(step_any(s, c, st));
         }
     }
     return OLC_OK;
@@ -810,6 +1142,7 @@ int olc_read_life(OlcSim* s, uint8_t* out, uint32_t rows, void* stream) {
 
 int olc_read_reductions(OlcSim* s, OlcReductions* out, void* stream) {
     if (!s || !out) return fail(s, OLC_ERR_ARG, "olc_read_reductions: null argument");
+    if (s->n_sims) return fail(s, OLC_ERR_STATE, "olc_read_reductions: batch handle (use olc_read_reductions_batch)");
     cudaStream_t st = as_stream(stream);
     OLC_TRY(check(s, cudaMemcpyAsync(s->red_host, s->red_dev, sizeof(OlcReductions), cudaMemcpyDeviceToHost, st),
                   "reductions readback"));
@@ -824,6 +1157,149 @@ int olc_read_user_metrics(OlcSim* s, void* out, size_t bytes, void* stream) {
     if (!bytes) return OLC_OK;
     cudaStream_t st = as_stream(stream);
     OLC_TRY(check(s, cudaMemcpyAsync(out, s->metrics_dev, bytes, cudaMemcpyDeviceToHost, st), "metrics readback"));
+    return check(s, cudaStreamSynchronize(st), "sync");
+}
+
+// ------------------------------------------------------------------ batched mode
+
+int olc_bind_field_batch(OlcSim* s, int index, float* a, float* b, float* sink, const OlcDiffusion* specs) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (!s->n_sims) return fail(s, OLC_ERR_STATE, "olc_bind_field_batch: not a batch handle");
+    if (index < 0 || index >= (int)s->caps.n_fields || !a || !b || !specs)
+        return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: bad index or null argument");
+    const olc_u32 F = s->caps.n_fields;
+    bool any_sink = false;
+    std::vector<std::pair<int, olc_u32>> order;  // (substeps, simulation)
+    for (olc_u32 k = 0; k < s->n_sims; ++k) {
+        const OlcDiffusion& spec = specs[k];
+        const OlcGeom& g = s->geoms[k];
+        if (g.chem_dims[0] % 4 != 0)
+            return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: simulation " + std::to_string(k) +
+                                            ": field x extent must be a multiple of 4");
+        FieldStep fs = {};
+        std::string err;
+        if (spec.substeps != 0 && !make_field_step(spec, g.chem_dims, g.chem_voxel_size, s->caps.dt, &fs, &err))
+            return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: simulation " + std::to_string(k) + ": " + err);
+        if (spec.substeps == 0) {
+            for (int i = 0; i < 3; ++i) fs.dims[i] = g.chem_dims[i];
+            fs.substeps = 0;
+        }
+        any_sink = any_sink || (spec.has_sink && spec.substeps != 0);
+        s->bsteps_host[(size_t)k * F + index] = fs;
+        order.push_back({fs.substeps, k});
+    }
+    if (any_sink && !sink) return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: has_sink without a sink buffer");
+    drop_graphs(s);
+    // tiles of this field, simulations taking the most substeps first (stable)
+    std::stable_sort(order.begin(), order.end(),
+                     [](const std::pair<int, olc_u32>& x, const std::pair<int, olc_u32>& y) { return x.first > y.first; });
+    std::vector<uint4> all(s->n_btiles);
+    OLC_TRY(check(s, cudaMemcpy(all.data(), s->btiles_all, sizeof(uint4) * all.size(), cudaMemcpyDeviceToHost),
+                  "read field tiles"));
+    std::vector<std::vector<uint4>> per_sim(s->n_sims);
+    for (const uint4& t : all) per_sim[t.x].push_back(t);
+    std::vector<uint4> tiles;
+    std::vector<int> tile_steps;
+    for (const auto& o : order)
+        for (const uint4& t : per_sim[o.second]) {
+            tiles.push_back(t);
+            tile_steps.push_back(o.first);
+        }
+    const int max_s = order.empty() ? 0 : order.front().first;
+    std::vector<olc_u32> count(max_s, 0u);
+    for (int sub = 0; sub < max_s; ++sub) {
+        olc_u32 c = 0;
+        while (c < tiles.size() && tile_steps[c] > sub) ++c;
+        count[sub] = c;
+    }
+    cudaFree(s->btiles_field[index]);
+    s->btiles_field[index] = nullptr;
+    OLC_TRY(dev_alloc(s, &s->btiles_field[index], sizeof(uint4) * std::max<size_t>(1, tiles.size()), "field tiles"));
+    if (!tiles.empty())
+        OLC_TRY(check(s, cudaMemcpy(s->btiles_field[index], tiles.data(), sizeof(uint4) * tiles.size(),
+                                    cudaMemcpyHostToDevice),
+                      "upload field tiles"));
+    s->btile_count[index] = count;
+    OLC_TRY(check(s, cudaMemcpy(s->bsteps_dev, s->bsteps_host.data(), sizeof(FieldStep) * s->bsteps_host.size(),
+                                cudaMemcpyHostToDevice),
+                  "upload field steps"));
+    // every simulation's grid starts in buffer a
+    std::vector<unsigned char> par((size_t)s->n_sims * OLC_MAX_FIELDS);
+    OLC_TRY(check(s, cudaMemcpy(par.data(), s->fpar_dev, par.size(), cudaMemcpyDeviceToHost), "read field parity"));
+    for (olc_u32 k = 0; k < s->n_sims; ++k) par[(size_t)k * F + index] = 0;
+    OLC_TRY(check(s, cudaMemcpy(s->fpar_dev, par.data(), par.size(), cudaMemcpyHostToDevice), "write field parity"));
+    s->field[0][index] = a;
+    s->field[1][index] = b;
+    s->sink[index] = any_sink ? sink : nullptr;
+    s->fspec[index] = specs[0];
+    s->field_cur[index] = 0;
+    s->field_bound[index] = true;
+    return OLC_OK;
+}
+
+int olc_read_field_parity(OlcSim* s, uint8_t* out, void* stream) {
+    if (!s || !out) return fail(s, OLC_ERR_ARG, "olc_read_field_parity: null argument");
+    if (!s->n_sims) return fail(s, OLC_ERR_STATE, "olc_read_field_parity: not a batch handle");
+    cudaStream_t st = as_stream(stream);
+    OLC_TRY(check(s, cudaStreamSynchronize(st), "sync"));
+    std::vector<unsigned char> par((size_t)s->n_sims * OLC_MAX_FIELDS);
+    OLC_TRY(check(s, cudaMemcpy(par.data(), s->fpar_dev, par.size(), cudaMemcpyDeviceToHost), "read field parity"));
+    const olc_u32 F = s->caps.n_fields;
+    for (olc_u32 k = 0; k < s->n_sims; ++k)
+        for (olc_u32 f = 0; f < F; ++f) out[(size_t)k * F + f] = par[(size_t)k * F + f];
+    return OLC_OK;
+}
+
+int olc_set_params_batch(OlcSim* s, const void* blob, size_t stride, void* stream) {
+    if (!s || !blob || stride == 0) return fail(s, OLC_ERR_ARG, "olc_set_params_batch: bad arguments");
+    if (!s->n_sims) return fail(s, OLC_ERR_STATE, "olc_set_params_batch: not a batch handle");
+    cudaStream_t st = as_stream(stream);
+    const size_t bytes = stride * s->n_sims;
+    if (bytes > s->params_cap || stride != s->params_stride) {
+        drop_graphs(s);
+        OLC_TRY(check(s, cudaStreamSynchronize(st), "sync before params upload"));
+        if (bytes > s->params_cap) {
+            cudaFree(s->params_dev);
+            if (s->params_host) cudaFreeHost(s->params_host);
+            s->params_dev = nullptr;
+            s->params_host = nullptr;
+            const size_t cap = (bytes + 255) & ~size_t(255);
+            OLC_TRY(dev_alloc(s, &s->params_dev, cap, "params"));
+            OLC_TRY(check(s, cudaMallocHost(reinterpret_cast<void**>(&s->params_host), cap), "pinned params"));
+            s->params_cap = cap;
+        }
+        s->params_stride = stride;
+        for (olc_u32 k = 0; k < s->n_sims; ++k) s->desc_host[k].params_off = (olc_u32)(k * stride);
+        OLC_TRY(upload_desc(s));
+    } else {
+        OLC_TRY(check(s, cudaStreamSynchronize(st), "sync before params upload"));
+    }
+    std::memcpy(s->params_host, blob, bytes);
+    return check(s, cudaMemcpyAsync(s->params_dev, s->params_host, bytes, cudaMemcpyHostToDevice, st),
+                 "params upload");
+}
+
+int olc_read_reductions_batch(OlcSim* s, OlcReductions* out, void* stream) {
+    if (!s || !out) return fail(s, OLC_ERR_ARG, "olc_read_reductions_batch: null argument");
+    if (!s->n_sims) return fail(s, OLC_ERR_STATE, "olc_read_reductions_batch: not a batch handle");
+    cudaStream_t st = as_stream(stream);
+    const size_t bytes = sizeof(OlcReductions) * s->n_sims;
+    OLC_TRY(check(s, cudaMemcpyAsync(s->red_batch_host, s->red_batch_dev, bytes, cudaMemcpyDeviceToHost, st),
+                  "reductions readback"));
+    OLC_TRY(check(s, cudaStreamSynchronize(st), "sync"));
+    std::memcpy(out, s->red_batch_host, bytes);
+    return OLC_OK;
+}
+
+int olc_read_user_metrics_batch(OlcSim* s, void* out, size_t bytes_per_sim, void* stream) {
+    if (!s || !out) return fail(s, OLC_ERR_ARG, "olc_read_user_metrics_batch: null argument");
+    if (!s->n_sims) return fail(s, OLC_ERR_STATE, "olc_read_user_metrics_batch: not a batch handle");
+    if (bytes_per_sim != s->metrics_bytes)
+        return fail(s, OLC_ERR_ARG, "olc_read_user_metrics_batch: bytes_per_sim must equal the metrics size");
+    if (!bytes_per_sim) return OLC_OK;
+    cudaStream_t st = as_stream(stream);
+    OLC_TRY(check(s, cudaMemcpyAsync(out, s->metrics_dev, bytes_per_sim * s->n_sims, cudaMemcpyDeviceToHost, st),
+                  "metrics readback"));
     return check(s, cudaStreamSynchronize(st), "sync");
 }
 

@@ -179,6 +179,15 @@ class Engine:
 
     # ---- model loading ----------------------------------------------------
     def load_model(self, sim_instance: Any) -> None:
+        self._prepare_model(sim_instance)
+        from oncolytica_b200.backend import CudaBackend
+
+        self._backend_impl = CudaBackend(self)
+        self._backend_impl.compile(sim_instance)
+
+    def _prepare_model(self, sim_instance: Any) -> None:
+        """Rule discovery and model checks of load_model, without a backend
+        (a BatchEngine drives many prepared engines through one handle)."""
         if not isinstance(sim_instance, Simulation):
             raise CompilationError(f"Expected an instance of 'ol.Simulation', got '{type(sim_instance).__name__}'.")
         self._sim = sim_instance
@@ -213,10 +222,6 @@ class Engine:
         for f in self._diffusion:
             if f not in self.chemistry._fields:
                 raise CompilationError(f"setup_diffusion: chemistry class has no field {f!r}")
-        from oncolytica_b200.backend import CudaBackend
-
-        self._backend_impl = CudaBackend(self)
-        self._backend_impl.compile(sim_instance)
 
     # ---- execution ---------------------------------------------------------
     def run_step(self, collect_metrics: bool = False) -> None:

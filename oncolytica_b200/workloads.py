@@ -16,6 +16,7 @@ exists for these; all inputs are generated here from numpy's default_rng(seed).
 from __future__ import annotations
 
 import math
+from typing import Any
 from dataclasses import dataclass, field, replace
 
 import numpy as np
@@ -221,6 +222,30 @@ SCALE = TumourSpec(name="scale", n_agents=1_000_000, domain=1000.0, ball_radius=
 CONFIGS = {s.name: s for s in (PLAIN_SMALL, SCALE)}
 
 
+def batched_specs(n_sims: int = 512, seed: int = 0, g_choices: tuple = (32, 48, 64, 96, 128),
+                  n_range: tuple = (1e3, 2e5), density: float = 3.73e-3) -> list:
+    """Members of a parameter sweep (the batched configuration): per member a
+    grid G from ``g_choices`` (domain G * 4 um, dx = 4 um, 10 um bins), an agent
+    count log-uniform in ``n_range`` capped so the ball of radius 0.4 * domain is
+    no denser than the scale workload (``density`` agents per um^3), D_O2 ~
+    U(1000, 3000), uptake ~ U(0.01, 0.04), drug decay ~ U(0.05, 0.2), and seed
+    ``seed + k``.  Drawn from numpy default_rng(seed)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_sims):
+        g = int(rng.choice(g_choices))
+        domain = 4.0 * g
+        ball = 0.4 * domain
+        n_max = max(100, int(density * (4.0 / 3.0) * math.pi * ball ** 3))
+        n = int(math.exp(rng.uniform(math.log(n_range[0]), math.log(n_range[1]))))
+        n = max(100, min(n, n_max))
+        out.append(TumourSpec(name=f"sweep_{k}", n_agents=n, domain=domain, ball_radius=ball, field_dims=(g, g, g),
+                              r_lo=4.0, r_hi=6.0, has_drug=True, D_o2=float(rng.uniform(1000.0, 3000.0)),
+                              uptake=float(rng.uniform(0.01, 0.04)), decay_drug=float(rng.uniform(0.05, 0.2)),
+                              death_k=0.02, seed=seed + k, capacity=2 * n + 1024))
+    return out
+
+
 def scaled(spec: TumourSpec, **kw) -> TumourSpec:
     """A copy with some numbers changed (smaller test cases)."""
     out = replace(spec, **kw)
@@ -267,6 +292,24 @@ def initial_fields(spec: TumourSpec) -> tuple[np.ndarray, np.ndarray | None]:
 
 def build_engine(spec: TumourSpec, state: dict | None = None) -> Engine:
     """An Engine loaded with the tumour model and the initial state of ``spec``."""
+    eng, sim = configure_engine(spec, state)
+    eng.load_model(sim)
+    return eng
+
+
+def build_batch(specs: list, states: list | None = None, max_agents: int | None = None):
+    """A BatchEngine running the tumour model for every spec (one member each)."""
+    from oncolytica_b200.batch import BatchEngine
+
+    states = states if states is not None else [None] * len(specs)
+    pairs = [configure_engine(sp, st) for sp, st in zip(specs, states)]
+    cap = max_agents if max_agents is not None else sum(sp.capacity for sp in specs)
+    return BatchEngine([e for e, _ in pairs], [s for _, s in pairs], max_agents=cap)
+
+
+def configure_engine(spec: TumourSpec, state: dict | None = None) -> tuple[Engine, Any]:
+    """An Engine set up for ``spec`` (geometry, fields, contact, agents) and the
+    model instance carrying its parameters, not yet loaded."""
     state = state if state is not None else initial_state(spec)
     eng = Engine(backend="cuda", max_agents=spec.capacity)
     eng.setup_geometry(tissue_shape=tuple(spec.tissue_dims), tissue_voxel_size=spec.bin_size)
@@ -290,5 +333,4 @@ def build_engine(spec: TumourSpec, state: dict | None = None) -> Engine:
     sim._params = TumourParams(dt=float(spec.dt), growth=float(spec.growth), v_div=float(spec.v_div),
                                o2_necrotic=float(spec.o2_necrotic), o2_quiescent=float(spec.o2_quiescent),
                                uptake=float(spec.uptake), death_k=float(spec.death_k))
-    eng.load_model(sim)
-    return eng
+    return eng, sim

@@ -186,3 +186,24 @@ def _err_sim(body):
 def test_unsupported_constructs_raise(body, msg):
     with pytest.raises(ol.CompilationError, match=msg):
         _translate(_err_sim(body))
+
+
+def test_batched_translation_compiles():
+    """Batched mode adds a `_sim` column after `_rng_state`, gives rule bodies
+    a per-simulation view and still compiles for sm_100a."""
+    for cls, radius in ((W.TumourDrugSim, "radius"), (GSim, None)):
+        sim = cls()
+        rules = {"cell": [], "metric": []}
+        for name in dir(sim):
+            m = getattr(sim, name, None)
+            kind = getattr(m, "_rule_type", None)
+            if kind in rules:
+                rules[kind].append(m)
+        sim._engine = SimpleNamespace(_cell_rules=rules["cell"], _metric_rules=rules["metric"])
+        layout = make_layout(sim._spec, radius, batched=True)
+        assert [c for c, _, _ in layout.cell_cols][-2:] == ["_rng_state", "_sim"]
+        assert layout.cell_cols[layout.rng_col][0] == "_rng_state"
+        prog = translate_model(sim, layout, radius)
+        assert "typedef OlcSimView OlcP;" in prog.source
+        assert "olc_sim_view(P, sim)" in prog.source
+        _nvrtc_ok(prog)
