@@ -29,6 +29,8 @@ import tempfile
 import time
 from dataclasses import replace
 
+import numpy as np
+
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
@@ -46,6 +48,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = as many as --steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graphs", action="store_true", help="eager launches instead of CUDA graphs of whole steps")
+    ap.add_argument("--sims", type=int, default=512, help="members of the batched workload (--workload batch)")
+    ap.add_argument("--solo-sample", type=int, default=0, help="members also timed one at a time (--workload batch)")
     return ap.parse_args()
 
 
@@ -372,10 +376,119 @@ def run_b200(args) -> None:
         dist.destroy_process_group()
 
 
+def measure_batch(n_sims: int, steps: int, warmup: int, graphs: bool = True, solo_sample: int = 0,
+                  seed: int = 0) -> dict:
+    """The batched workload: ``n_sims`` sweep members (uneven agent counts,
+    grids and diffusion) stepped by one BatchEngine.  Device time with CUDA
+    events over ``steps`` steps after ``warmup``; stage times from a second
+    batch replaying the same steps eagerly with events between stages.  With
+    ``solo_sample`` > 0 the same number of members (spread over the sweep) also
+    run one at a time through solo engines, for the batched-vs-solo ratio."""
+    import torch
+
+    from oncolytica_b200 import workloads as W
+
+    specs = W.batched_specs(n_sims, seed=seed)
+    states = [W.initial_state(sp) for sp in specs]
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    def timed(b):
+        b.run_steps(warmup)
+        torch.cuda.synchronize(dev)
+        c0 = b.counters()
+        st = torch.cuda.current_stream(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        b.run_steps(steps)
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1), b.counters()["agent_steps"] - c0["agent_steps"], b
+
+    batch = W.build_batch(specs, states)
+    batch.set_graphs(graphs)
+    ms, agent_steps, batch = timed(batch)
+    status = batch.counters()["status"]
+    del batch
+    torch.cuda.empty_cache()
+    prof_batch = W.build_batch(specs, states)
+    prof_batch.run_steps(warmup)
+    prof_batch.set_profiling(True)
+    prof_batch.run_steps(steps)
+    prof = prof_batch.profile()
+    prof_batch.set_profiling(False)
+    del prof_batch
+    torch.cuda.empty_cache()
+    vox = sum(int(np.prod(sp.field_dims)) * (sp.S_o2 + sp.S_drug) for sp in specs) * steps
+    out = {"n_sims": n_sims, "steps": steps, "warmup": warmup, "ms_per_step": ms / steps,
+           "agent_steps_per_s": agent_steps / (ms / 1e3), "voxel_updates_per_s": vox / (ms / 1e3),
+           "agents_start": int(sum(sp.n_agents for sp in specs)),
+           "voxels_per_field": int(sum(int(np.prod(sp.field_dims)) for sp in specs)),
+           "substeps_o2": [min(sp.S_o2 for sp in specs), max(sp.S_o2 for sp in specs)],
+           "stages_ms_per_step": {k[3:]: prof[k] / max(1, prof["steps"]) for k in
+                                  ("ms_sink", "ms_substeps", "ms_grid", "ms_rules", "ms_contact", "ms_collect")},
+           "gpu_launches_per_step": prof["kernel_launches"] / max(1, prof["steps"]),
+           "graphs": graphs, "status": status}
+    if solo_sample:
+        idx = np.linspace(0, n_sims - 1, solo_sample).astype(int)
+        sub = [specs[i] for i in idx]
+        sub_states = [states[i] for i in idx]
+        solo_ms, solo_as = 0.0, 0
+        for sp, st0 in zip(sub, sub_states):
+            e = W.build_engine(sp, st0)
+            e.set_graphs(graphs)
+            m, a, _ = timed(_SoloAsBatch(e))
+            solo_ms += m
+            solo_as += a
+            del e
+        bsub = W.build_batch(sub, sub_states)
+        bsub.set_graphs(graphs)
+        bm, ba, _ = timed(bsub)
+        del bsub
+        out["solo_vs_batch_sample"] = {"members": solo_sample, "solo_agent_steps_per_s": solo_as / (solo_ms / 1e3),
+                                      "batch_agent_steps_per_s": ba / (bm / 1e3),
+                                      "speedup": (ba / (bm / 1e3)) / (solo_as / (solo_ms / 1e3))}
+    return out
+
+
+class _SoloAsBatch:
+    """A solo Engine behind the two calls measure_batch's timer uses."""
+
+    def __init__(self, eng) -> None:
+        self.eng = eng
+
+    def run_steps(self, n: int) -> None:
+        self.eng.run_steps(n)
+
+    def counters(self) -> dict:
+        return self.eng._backend_impl.counters()
+
+
+def run_batch_workload(args) -> None:
+    import torch
+
+    rank, world, local = env_ranks()
+    torch.cuda.set_device(local)
+    r = measure_batch(args.sims, args.steps, args.warmup, graphs=not args.no_graphs, solo_sample=args.solo_sample,
+                      seed=rank)
+    peaks = measured_peaks()
+    line = {"metric": "agent-steps/s + voxel-updates/s, batched FP32 on 1 B200", "value": r["agent_steps_per_s"],
+            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (numpy default_rng, seed 0 + rank)",
+            "config": {"workload": f"batched sweep, {args.sims} members", "members": args.sims,
+                       "agents": r["agents_start"], "voxels_per_field": r["voxels_per_field"], "fields": "o2+drug",
+                       "substeps_o2": r["substeps_o2"], "parallelism": f"replicas x{world}"},
+            "voxel_updates_per_s": r["voxel_updates_per_s"], "batch": r, "peak_hbm_gbs": peaks["hbm_gbs"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch_workload(args)
     else:
         run_b200(args)
 

@@ -94,7 +94,18 @@ typedef struct {
     int32_t substeps;           /* S >= 1, D*dt/S/dx^2 <= 1/6 is checked;
                                    0 = static field (read by rules only)       */
     int32_t has_sink;           /* rules deposit uptake rates into this field */
+    int32_t storage;            /* OLC_FIELD_F32 (default), OLC_FIELD_BF16 or
+                                   OLC_FIELD_F16: element type of the buffers */
 } OlcDiffusion;
+
+/* Field storage types (OlcDiffusion.storage).  16-bit storage halves the
+ * stencil's bytes: each substep reads 16-bit values, updates in FP32 and
+ * rounds to nearest even; uptake and decay are applied once per step in FP32
+ * with the rounding residual kept in a caller-provided FP32 compensation
+ * buffer (olc_bind_field_ex).  No counterpart in the reference (FP32 textures). */
+#define OLC_FIELD_F32  0
+#define OLC_FIELD_BF16 1
+#define OLC_FIELD_F16  2
 
 /* Hertz-like contact repulsion (engine/assets/shaders/tumor_sim.wgsl:505-628):
  * for d < r_i + r_j, F += k * delta^(3/2) * (p_i - p_j)/d with
@@ -169,6 +180,14 @@ int olc_bind_agent_column(OlcSim* sim, int index, void* a_dev, void* b_dev);
  * Chem_In/Chem_Out (_device_manager.py:76-119). */
 int olc_bind_field(OlcSim* sim, int index, float* a_dev, float* b_dev, float* sink_dev,
                    const OlcDiffusion* spec);
+
+/* olc_bind_field for any storage type: a_dev, b_dev hold 4-byte (FP32) or
+ * 2-byte (BF16/FP16) elements; comp_dev is an FP32 buffer, one element per
+ * voxel, zeroed by the caller, that carries each voxel's rounding residual of
+ * the per-step reaction (required for 16-bit storage, ignored for FP32).  No
+ * counterpart in the reference. */
+int olc_bind_field_ex(OlcSim* sim, int index, void* a_dev, void* b_dev, float* sink_dev, float* comp_dev,
+                      const OlcDiffusion* spec);
 
 int olc_set_contact(OlcSim* sim, const OlcContact* spec);
 
@@ -328,6 +347,12 @@ int olc_stage_bin_ranges(const uint32_t* sorted_keys_dev, uint32_t n, uint32_t n
  * after use). */
 int olc_stage_diffuse(float* f_dev, float* tmp_dev, float* sink_dev, const int32_t dims[3],
                       float dx, float dt, const OlcDiffusion* spec, void* stream);
+
+/* One step of one 16-bit field (reaction with compensation, then S
+ * substeps), result in f_dev; f_dev, tmp_dev hold BF16/FP16 elements, comp_dev
+ * the FP32 residuals. */
+int olc_stage_diffuse16(void* f_dev, void* tmp_dev, float* sink_dev, float* comp_dev, const int32_t dims[3],
+                        float dx, float dt, const OlcDiffusion* spec, void* stream);
 
 /* Contact pass over n sorted agents: posr_dev holds (x, y, z, radius) with
  * radius < 0 marking a dead agent; writes the new positions. */

@@ -43,6 +43,7 @@ EXPORTS = (
     "olc_stage_bin_ranges", "olc_stage_diffuse", "olc_stage_contact",
     "olc_create_batch", "olc_batch_field_offsets", "olc_bind_field_batch", "olc_set_params_batch",
     "olc_read_field_parity", "olc_read_reductions_batch", "olc_read_user_metrics_batch",
+    "olc_bind_field_ex", "olc_stage_diffuse16",
 )
 
 
@@ -84,6 +85,7 @@ class OlcDiffusion(C.Structure):
         ("boundary", C.c_float),
         ("substeps", C.c_int32),
         ("has_sink", C.c_int32),
+        ("storage", C.c_int32),
     ]
 
 
@@ -163,6 +165,9 @@ _SIGS = {
     "olc_create_batch": (C.c_int, [C.POINTER(OlcGeom), C.c_int, C.POINTER(OlcCaps), C.POINTER(_VP)]),
     "olc_batch_field_offsets": (C.c_int, [_VP, C.POINTER(C.c_uint64)]),
     "olc_bind_field_batch": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, C.POINTER(OlcDiffusion)]),
+    "olc_bind_field_ex": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, _VP, C.POINTER(OlcDiffusion)]),
+    "olc_stage_diffuse16": (C.c_int, [_VP, _VP, _VP, _VP, C.POINTER(C.c_int32 * 3), C.c_float, C.c_float,
+                                      C.POINTER(OlcDiffusion), _VP]),
     "olc_set_params_batch": (C.c_int, [_VP, _VP, C.c_size_t, _VP]),
     "olc_read_field_parity": (C.c_int, [_VP, C.POINTER(C.c_uint8), _VP]),
     "olc_read_reductions_batch": (C.c_int, [_VP, C.POINTER(OlcReductions), _VP]),

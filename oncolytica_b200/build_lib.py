@@ -24,7 +24,7 @@ INCLUDE = os.path.join(REPO, "include")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
-SOURCES = ["olc_grid.cu", "olc_field.cu", "olc_contact.cu", "olc_reduce.cu", "olc_batch.cu", "olc_sim.cu",
+SOURCES = ["olc_grid.cu", "olc_field.cu", "olc_field16.cu", "olc_contact.cu", "olc_reduce.cu", "olc_batch.cu", "olc_sim.cu",
            "olc_noalloc.cu"]
 HEADERS = ["olc_device.cuh", "olc_rule_rt.cuh", "olc_internal.h"]
 

@@ -496,7 +496,7 @@ class Translator:
             lines.append(f"__device__ __forceinline__ void olc_copy_from(" f"{STRUCT_NAME[kind]}& a, "
                          f"const {STRUCT_NAME[kind]}& b) {{\n{assigns}\n}}")
         # chemistry / tissue lookups
-        chem_reads = "\n".join(f"    c.{n} = P.field[{i}] ? P.field[{i}][v] : 0.0f;"
+        chem_reads = "\n".join(f"    c.{n} = olc_field_at(P, {i}, v);"
                                for i, n in enumerate(L.chem_fields))
         lines.append("__device__ __forceinline__ Chem_t olc_chem_at(const OlcP& P, olc_vec3 p) {\n"
                      "    Chem_t c = olc_default_chemistry();\n    const olc_u32 v = olc_chem_index(P, p);\n" +

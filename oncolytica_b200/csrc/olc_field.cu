@@ -47,12 +47,28 @@ bool make_field_step(const OlcDiffusion& d, const int dims[3], float dx, float d
                " > 1/6; raise substeps";
         return false;
     }
+    if (d.storage < OLC_FIELD_F32 || d.storage > OLC_FIELD_F16) {
+        *err = "storage must be OLC_FIELD_F32, OLC_FIELD_BF16 or OLC_FIELD_F16";
+        return false;
+    }
+    if (d.storage != OLC_FIELD_F32 && dims[0] % 8 != 0) {
+        *err = "16-bit field storage needs an x extent that is a multiple of 8";
+        return false;
+    }
     for (int i = 0; i < 3; ++i) out->dims[i] = dims[i];
     out->r = r;
-    out->inv_decay = 1.0f / (1.0f + d.decay * dts);
     out->bval = d.boundary;
     out->sink_dt = dt;
     out->substeps = d.substeps;
+    out->storage = d.storage;
+    if (d.storage == OLC_FIELD_F32) {
+        out->inv_decay = 1.0f / (1.0f + d.decay * dts);
+        out->decay_step = 1.0f;
+    } else {
+        // decay leaves the substeps and is applied once per step by the reaction pass
+        out->inv_decay = 1.0f;
+        out->decay_step = (float)std::pow(1.0 + (double)d.decay * (double)dts, -(double)d.substeps);
+    }
     return true;
 }
 
@@ -798,6 +814,20 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 }  // namespace
+
+bool encode_map_elems(CUtensorMap* map, void* base, const int dims[3], const cuuint32_t box[3], int elem_bytes) {
+    if (elem_bytes != 2 && elem_bytes != 4) return false;
+    if (((size_t)dims[0] * elem_bytes) % 16 != 0 || (reinterpret_cast<uintptr_t>(base) & 15u) != 0) return false;
+    if (((size_t)box[0] * elem_bytes) % 16 != 0) return false;
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t gdim[3] = {(cuuint64_t)dims[0], (cuuint64_t)dims[1], (cuuint64_t)dims[2]};
+    cuuint64_t gstride[2] = {(cuuint64_t)dims[0] * elem_bytes, (cuuint64_t)dims[0] * dims[1] * elem_bytes};
+    cuuint32_t estride[3] = {1, 1, 1};
+    return fn(map, elem_bytes == 2 ? CU_TENSOR_MAP_DATA_TYPE_UINT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, gdim,
+              gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 static bool encode_map(CUtensorMap* map, float* base, const int dims[3], const cuuint32_t box[3]) {
     if ((dims[0] * 4) % 16 != 0 || (reinterpret_cast<uintptr_t>(base) & 15u) != 0) return false;

@@ -1,0 +1,343 @@
+// Diffusion-reaction of a field stored as BF16 or FP16 (the precision tier;
+// no counterpart in the reference, whose fields are FP32 textures).
+//
+// Per step:
+//   reaction  (once):  v = f + comp;  v /= 1 + K dt (uptake, if any);
+//                      v *= (1 + lambda dt/S)^-S (the step's decay);
+//                      f = round16(v);  comp = v - f          (FP32, RN-even)
+//   diffusion (S substeps): c' = round16(max(c + r (S6 - 6 c), 0)) with the
+//                      sum S6 = ((xm + xp) + (ym + yp)) + (zm + zp) in FP32;
+//                      outer faces pinned to round16(boundary).
+// comp carries each voxel's rounding residual of the reaction into the next
+// step (compensated summation), so small uptake and decay terms are not lost
+// to the 8- or 11-bit mantissa.  The substeps round every result; their
+// error is what the FP64 comparison reports.  Every operation is separately
+// rounded, so the CPU restatement reproduces the bits.
+#include "olc_internal.h"
+
+#include <cuda.h>
+
+namespace olc {
+
+namespace {
+
+__device__ __forceinline__ olc_u32 smem_addr(const void* p) {
+    return static_cast<olc_u32>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ bool mbar_wait_once(olc_u32 bar, olc_u32 parity) {
+    olc_u32 ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Storage type traits (the bits are handled as unsigned short).
+template <int ST>
+struct Store16;
+
+template <>
+struct Store16<OLC_FIELD_BF16> {
+    static __device__ __forceinline__ float to_f(unsigned short h) { return __uint_as_float((olc_u32)h << 16); }
+    // round to nearest even on the FP32 bit pattern (values here are finite)
+    static __device__ __forceinline__ unsigned short from_f(float f) {
+        unsigned short h;
+        asm("cvt.rn.bf16.f32 %0, %1;" : "=h"(h) : "f"(f));
+        return h;
+    }
+};
+
+template <>
+struct Store16<OLC_FIELD_F16> {
+    static __device__ __forceinline__ float to_f(unsigned short h) {
+        float f;
+        asm("{ .reg .b16 t; mov.b16 t, %1; cvt.f32.f16 %0, t; }" : "=f"(f) : "h"(h));
+        return f;
+    }
+    static __device__ __forceinline__ unsigned short from_f(float f) {
+        unsigned short h;
+        asm("{ .reg .b16 t; cvt.rn.f16.f32 t, %1; mov.b16 %0, t; }" : "=h"(h) : "f"(f));
+        return h;
+    }
+};
+
+template <int ST>
+__device__ __forceinline__ float4 load4(const unsigned short* p) {
+    const uint2 raw = *reinterpret_cast<const uint2*>(p);
+    return make_float4(Store16<ST>::to_f((unsigned short)(raw.x & 0xffffu)), Store16<ST>::to_f((unsigned short)(raw.x >> 16)),
+                       Store16<ST>::to_f((unsigned short)(raw.y & 0xffffu)), Store16<ST>::to_f((unsigned short)(raw.y >> 16)));
+}
+
+template <int ST>
+__device__ __forceinline__ void store4(unsigned short* p, float4 v) {
+    const olc_u32 lo = (olc_u32)Store16<ST>::from_f(v.x) | ((olc_u32)Store16<ST>::from_f(v.y) << 16);
+    const olc_u32 hi = (olc_u32)Store16<ST>::from_f(v.z) | ((olc_u32)Store16<ST>::from_f(v.w) << 16);
+    *reinterpret_cast<uint2*>(p) = make_uint2(lo, hi);
+}
+
+__device__ __forceinline__ float diffuse1(float xm, float xp, float ym, float yp, float zm, float zp, float c, float r) {
+    const float s = __fadd_rn(__fadd_rn(__fadd_rn(xm, xp), __fadd_rn(ym, yp)), __fadd_rn(zm, zp));
+    return fmaxf(__fadd_rn(c, __fmul_rn(r, __fsub_rn(s, __fmul_rn(6.0f, c)))), 0.0f);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ reaction
+template <int ST>
+__global__ void __launch_bounds__(256) k_react16(unsigned short* __restrict__ f, float* __restrict__ K,
+                                                 float* __restrict__ comp, int nx, int ny, int nz, float dt,
+                                                 float decay_step) {
+    const size_t nvox = (size_t)nx * ny * nz;
+    for (size_t v = blockIdx.x * (size_t)blockDim.x + threadIdx.x; v < nvox; v += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(v % (size_t)nx);
+        const size_t t = v / (size_t)nx;
+        const int y = (int)(t % (size_t)ny);
+        const int z = (int)(t / (size_t)ny);
+        const bool face = x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1;
+        float k = 0.0f;
+        if (K) {
+            k = K[v];
+            if (k != 0.0f) K[v] = 0.0f;
+        }
+        if (face) continue;
+        float val = __fadd_rn(Store16<ST>::to_f(f[v]), comp[v]);
+        if (k != 0.0f) val = __fdiv_rn(val, __fadd_rn(1.0f, __fmul_rn(k, dt)));
+        val = __fmul_rn(val, decay_step);
+        const unsigned short h = Store16<ST>::from_f(val);
+        f[v] = h;
+        comp[v] = __fsub_rn(val, Store16<ST>::to_f(h));
+    }
+}
+
+void launch_react16(void* f, float* sink, float* comp, const FieldStep& fs, cudaStream_t s) {
+    const size_t nvox = (size_t)fs.dims[0] * fs.dims[1] * fs.dims[2];
+    size_t blocks = (nvox + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    if (fs.storage == OLC_FIELD_BF16)
+        k_react16<OLC_FIELD_BF16><<<(unsigned)blocks, 256, 0, s>>>(static_cast<unsigned short*>(f), sink, comp,
+                                                                    fs.dims[0], fs.dims[1], fs.dims[2], fs.sink_dt,
+                                                                    fs.decay_step);
+    else
+        k_react16<OLC_FIELD_F16><<<(unsigned)blocks, 256, 0, s>>>(static_cast<unsigned short*>(f), sink, comp,
+                                                                   fs.dims[0], fs.dims[1], fs.dims[2], fs.sink_dt,
+                                                                   fs.decay_step);
+}
+
+// ------------------------------------------------------------------ diffusion substep
+// The 4-wide TMA tile of k_substep_x4 on 16-bit storage: a CTA of 16 x TYR
+// threads owns a 64 x TYR x TZ block; the TMA box is 80 x (TYR+2) x (TZ+2)
+// elements with x starting 8 columns early (16-byte alignment of 2-byte
+// elements).  Each thread handles four x voxels: 8-byte shared loads of the
+// centre, y and z rows, 2-byte loads of the x neighbours, an 8-byte store.
+namespace t16 {
+constexpr int TX = 64, HX = 8, WX = TX + 2 * HX;  // 80 elements, 160 bytes
+constexpr int TYR = 8, TZ = 8, WY = TYR + 2, WZ = TZ + 2;
+constexpr unsigned BYTES = WX * WY * WZ * 2;
+constexpr size_t SMEM = BYTES + 16 + 128;
+}  // namespace t16
+
+template <int ST>
+__global__ void __launch_bounds__(16 * t16::TYR) k_substep16(const __grid_constant__ CUtensorMap in_map,
+                                                            unsigned short* __restrict__ out, int nx, int ny, int nz,
+                                                            float r, float bval, olc_u32* status, int rev) {
+    using namespace t16;
+    extern __shared__ unsigned char t16_raw[];
+    const olc_u32 pad = (128u - (smem_addr(t16_raw) & 127u)) & 127u;
+    unsigned short* tile = reinterpret_cast<unsigned short*>(t16_raw + pad);
+    const olc_u32 bar = smem_addr(t16_raw + pad + BYTES);
+    const int bx = rev ? gridDim.x - 1 - blockIdx.x : blockIdx.x;
+    const int by = rev ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
+    const int bz = rev ? gridDim.z - 1 - blockIdx.z : blockIdx.z;
+    const int x0 = bx * TX, y0 = by * TYR, z0 = bz * TZ;
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(BYTES) : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+            "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(tile)),
+            "l"(reinterpret_cast<unsigned long long>(&in_map)), "r"(x0 - HX), "r"(y0 - 1), "r"(z0 - 1), "r"(bar)
+            : "memory");
+    }
+    bool ready = false;
+    for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it) {
+        if (mbar_wait_once(bar, 0)) {
+            ready = true;
+            break;
+        }
+    }
+    if (!ready) {
+        if (threadIdx.x == 0) atomicOr(status, OLC_ST_TIMEOUT);
+        for (olc_u32 it = 0; it < OLC_SPIN_LIMIT && !mbar_wait_once(bar, 0); ++it) {
+        }
+        return;
+    }
+    const int g = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int x = x0 + 4 * g, y = y0 + ty;
+    if (x >= nx || y >= ny) return;
+    const bool edge_y = y == 0 || y == ny - 1;
+    const bool ex0 = x == 0, ex3 = x + 3 == nx - 1;
+    constexpr int PS = WY * WX;
+    const unsigned short* col = tile + (ty + 1) * WX + HX + 4 * g;
+    float4 zm = load4<ST>(col);
+    float4 c = load4<ST>(col + PS);
+    const size_t sz = (size_t)nx * ny;
+    unsigned short* o = out + (size_t)z0 * sz + (size_t)y * nx + x;
+    const float bf = Store16<ST>::to_f(Store16<ST>::from_f(bval));  // the face value as stored
+#pragma unroll 4
+    for (int lz = 1; lz <= TZ; ++lz) {
+        const int z = z0 + lz - 1;
+        if (z >= nz) break;
+        const unsigned short* pc = col + lz * PS;
+        const float4 zp = load4<ST>(pc + PS);
+        const float4 ym = load4<ST>(pc - WX);
+        const float4 yp = load4<ST>(pc + WX);
+        const float xl = Store16<ST>::to_f(pc[-1]), xr = Store16<ST>::to_f(pc[4]);
+        float4 v;
+        v.x = diffuse1(xl, c.y, ym.x, yp.x, zm.x, zp.x, c.x, r);
+        v.y = diffuse1(c.x, c.z, ym.y, yp.y, zm.y, zp.y, c.y, r);
+        v.z = diffuse1(c.y, c.w, ym.z, yp.z, zm.z, zp.z, c.z, r);
+        v.w = diffuse1(c.z, xr, ym.w, yp.w, zm.w, zp.w, c.w, r);
+        if (edge_y || z == 0 || z == nz - 1) {
+            v = make_float4(bf, bf, bf, bf);
+        } else {
+            if (ex0) v.x = bf;
+            if (ex3) v.w = bf;
+        }
+        store4<ST>(o, v);
+        o += sz;
+        zm = c;
+        c = zp;
+    }
+}
+
+bool make_field_maps16(FieldMaps16* m, void* a, void* b, const int dims[3]) {
+    using namespace t16;
+    m->ok = false;
+    const cuuint32_t box[3] = {WX, WY, WZ};
+    if (!encode_map_elems(&m->map[0], a, dims, box, 2) || !encode_map_elems(&m->map[1], b, dims, box, 2)) return false;
+    m->ok = true;
+    return true;
+}
+
+template <int ST>
+static void launch_sub16(const CUtensorMap& map, void* out, const FieldStep& fs, olc_u32* status, int rev,
+                         cudaStream_t s) {
+    using namespace t16;
+    static int configured_mask = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 32 && !(configured_mask & (1 << dev))) {
+        cudaFuncSetAttribute(k_substep16<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+        configured_mask |= 1 << dev;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((fs.dims[0] + TX - 1) / TX, (fs.dims[1] + TYR - 1) / TYR, (fs.dims[2] + TZ - 1) / TZ);
+    cfg.blockDim = dim3(16 * TYR);
+    cfg.dynamicSmemBytes = SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_substep16<ST>, map, static_cast<unsigned short*>(out), fs.dims[0], fs.dims[1],
+                       fs.dims[2], fs.r, fs.bval, status, rev);
+}
+
+void* run_substeps16(void* a, void* b, const FieldMaps16& m, int a_index, const FieldStep& fs, olc_u32* status,
+                     cudaStream_t s) {
+    void* bufs[2];
+    bufs[a_index] = a;
+    bufs[1 - a_index] = b;
+    int cur = a_index;
+    for (int i = 0; i < fs.substeps; ++i) {
+        if (fs.storage == OLC_FIELD_BF16)
+            launch_sub16<OLC_FIELD_BF16>(m.map[cur], bufs[1 - cur], fs, status, i & 1, s);
+        else
+            launch_sub16<OLC_FIELD_F16>(m.map[cur], bufs[1 - cur], fs, status, i & 1, s);
+        cur = 1 - cur;
+    }
+    return bufs[cur];
+}
+
+// ------------------------------------------------------------------ reductions
+// Mass (FP64 sum of value + residual), minimum and maximum of a 16-bit field;
+// one block partial per block, summed in a fixed order by the last block (as
+// k_reduce_field).
+template <int ST>
+__global__ void __launch_bounds__(256) k_reduce_field16(const unsigned short* __restrict__ f,
+                                                        const float* __restrict__ comp, size_t nvox, int slot,
+                                                        OlcReductions* out, double* partials, olc_u32* ticket) {
+    __shared__ double s_v[3][8];
+    __shared__ bool s_last;
+    double sum = 0.0, mn = 1e300, mx = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nvox; i += (size_t)gridDim.x * blockDim.x) {
+        const double v = (double)__fadd_rn(Store16<ST>::to_f(f[i]), comp ? comp[i] : 0.0f);
+        sum += v;
+        mn = fmin(mn, v);
+        mx = fmax(mx, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_v[0][warp] = sum;
+        s_v[1][warp] = mn;
+        s_v[2][warp] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0, a = 1e300, b = 0.0;
+        for (int w = 0; w < 8; ++w) {
+            t += s_v[0][w];
+            a = fmin(a, s_v[1][w]);
+            b = fmax(b, s_v[2][w]);
+        }
+        atomicMin(reinterpret_cast<unsigned long long*>(&out->field_min[slot]), (unsigned long long)__double_as_longlong(a));
+        atomicMax(reinterpret_cast<unsigned long long*>(&out->field_max[slot]), (unsigned long long)__double_as_longlong(b));
+        partials[blockIdx.x] = t;
+        __threadfence();
+        s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (unsigned b = 0; b < gridDim.x; ++b) t += __ldcg(partials + b);
+        out->field_mass[slot] = t;
+        *ticket = 0u;
+    }
+}
+
+void launch_reduce_field16(const void* f, const float* comp, const FieldStep& fs, int slot, OlcReductions* out,
+                           const RedScratch& rs, cudaStream_t s) {
+    const size_t nvox = (size_t)fs.dims[0] * fs.dims[1] * fs.dims[2];
+    size_t blocks = (nvox + 255) / 256;
+    if (blocks == 0) blocks = 1;
+    if (blocks > RED_MAX_BLOCKS) blocks = RED_MAX_BLOCKS;
+    double* part = rs.partials + (size_t)(4 + slot) * RED_MAX_BLOCKS;
+    olc_u32* ticket = rs.tickets + 1 + slot;
+    const unsigned short* p = static_cast<const unsigned short*>(f);
+    if (fs.storage == OLC_FIELD_BF16)
+        k_reduce_field16<OLC_FIELD_BF16><<<(unsigned)blocks, 256, 0, s>>>(p, comp, nvox, slot, out, part, ticket);
+    else
+        k_reduce_field16<OLC_FIELD_F16><<<(unsigned)blocks, 256, 0, s>>>(p, comp, nvox, slot, out, part, ticket);
+}
+
+}  // namespace olc

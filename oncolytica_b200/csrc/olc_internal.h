@@ -98,11 +98,13 @@ void launch_permute(const olc_u32* idx, olc_u32* counters, olc_u32 n_cap, const 
 // ------------------------------------------------------------------ field
 struct FieldStep {
     int dims[3];
-    float r;          // D * dt_sub / dx^2
-    float inv_decay;  // 1 / (1 + lambda * dt_sub)
+    float r;           // D * dt_sub / dx^2
+    float inv_decay;   // 1 / (1 + lambda * dt_sub) (FP32 storage; 1 for 16-bit storage)
     float bval;
-    float sink_dt;    // dt of the implicit sink
+    float sink_dt;     // dt of the implicit sink
     int substeps;
+    int storage;       // OLC_FIELD_F32 / OLC_FIELD_BF16 / OLC_FIELD_F16
+    float decay_step;  // 16-bit storage: (1 + lambda dt/S)^-S, applied once per step by the reaction
 };
 bool make_field_step(const OlcDiffusion& d, const int dims[3], float dx, float dt, FieldStep* out,
                      std::string* err);
@@ -133,6 +135,23 @@ float* run_substeps_tma(float* a, float* b, const FieldMaps& m, int a_index, con
 int launches_for(const FieldMaps& m, int substeps);
 // OLC_STENCIL=plain in the environment selects the register-column kernel.
 bool stencil_tma_enabled();
+bool encode_map_elems(CUtensorMap* map, void* base, const int dims[3], const cuuint32_t box[3], int elem_bytes);
+
+// 16-bit field storage (olc_field16.cu): fields stored as BF16 or FP16,
+// every update computed in FP32.  Per step: one reaction pass (uptake and the
+// step's decay, with the FP32 rounding residual of each voxel kept in `comp`
+// and added back the next step, i.e. Kahan-compensated), then S diffusion
+// substeps that round each result to the storage type.
+struct FieldMaps16 {
+    bool ok = false;
+    CUtensorMap map[2];
+};
+bool make_field_maps16(FieldMaps16* m, void* a, void* b, const int dims[3]);
+void launch_react16(void* f, float* sink, float* comp, const FieldStep& fs, cudaStream_t s);
+// Runs fs.substeps substeps from buffer a_index of (a, b); returns the buffer holding the result.
+void* run_substeps16(void* a, void* b, const FieldMaps16& m, int a_index, const FieldStep& fs, olc_u32* status,
+                     cudaStream_t s);
+
 olc_u32* stage_status_word();
 
 // ------------------------------------------------------------------ contact
@@ -169,6 +188,8 @@ void launch_reduce_agents(const ReduceArgs& a, const olc_u32* counters, olc_u32 
 void launch_reduce_field(const float* f, size_t nvox, int slot, OlcReductions* out_dev, const RedScratch& rs,
                          cudaStream_t s);
 void launch_reset_reductions(OlcReductions* out_dev, int nfields, cudaStream_t s);
+void launch_reduce_field16(const void* f, const float* comp, const FieldStep& fs, int slot, OlcReductions* out,
+                           const RedScratch& rs, cudaStream_t s);
 
 void launch_rng(olc_u32* states, olc_u32 n, int draws, float* out, float* dirs, cudaStream_t s);
 

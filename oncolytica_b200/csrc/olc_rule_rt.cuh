@@ -56,7 +56,7 @@ struct OlcSimDesc {
 struct OlcRuleParams {
     const void* in[OLC_MAX_AGENT_COLS];
     void* out[OLC_MAX_AGENT_COLS];
-    const float* field[OLC_MAX_FIELD_COLS];
+    const void* field[OLC_MAX_FIELD_COLS];  // current grid of each field (storage per field_type)
     float* sink[OLC_MAX_FIELD_COLS];
     const olc_u32* ranges;        // bin table, 2 words per key
     unsigned char* life;          // 0 alive, 1 dead (removed at the next sort)
@@ -84,10 +84,11 @@ struct OlcRuleParams {
     const OlcSimDesc* sims;
     const void* const* cols_in;
     void* const* cols_out;
-    const float* field_alt[OLC_MAX_FIELD_COLS];
+    const void* field_alt[OLC_MAX_FIELD_COLS];
     const unsigned char* fpar;
     int n_fields;
     int sim_col;
+    int field_type[OLC_MAX_FIELD_COLS];  // 0 FP32, 1 BF16, 2 FP16 storage
 };
 
 // What a rule body sees of one simulation of a batch (batched mode).  Member
@@ -95,7 +96,8 @@ struct OlcRuleParams {
 struct OlcSimView {
     const void* const* in;
     void* const* out;
-    const float* field[OLC_MAX_FIELD_COLS];
+    const void* field[OLC_MAX_FIELD_COLS];
+    int field_type[OLC_MAX_FIELD_COLS];
     float* sink[OLC_MAX_FIELD_COLS];
     const olc_u32* ranges;
     float4* posr;
@@ -118,8 +120,9 @@ __device__ __forceinline__ OlcSimView olc_sim_view(const OlcRuleParams& P, olc_u
 #pragma unroll
     for (int f = 0; f < OLC_MAX_FIELD_COLS; ++f) {
         const bool alt = f < P.n_fields && P.fpar[sim * (olc_u32)P.n_fields + f] != 0;
-        const float* base = alt ? P.field_alt[f] : P.field[f];
-        V.field[f] = base ? base + d.field_off : nullptr;
+        const unsigned char* base = static_cast<const unsigned char*>(alt ? P.field_alt[f] : P.field[f]);
+        V.field_type[f] = P.field_type[f];
+        V.field[f] = base ? base + d.field_off * (P.field_type[f] ? 2u : 4u) : nullptr;
         V.sink[f] = P.sink[f] ? P.sink[f] + d.field_off : nullptr;
     }
     V.ranges = P.ranges + 2ull * d.ranges_base;
@@ -265,6 +268,25 @@ template <class PT>
 __device__ __forceinline__ olc_ivec3 olc_tissue_coord(const PT& P, olc_vec3 p) {
     return olc_iv3(olc_bin_coord(p.x, P.tvs, P.tdims[0]), olc_bin_coord(p.y, P.tvs, P.tdims[1]),
                    olc_bin_coord(p.z, P.tvs, P.tdims[2]));
+}
+
+// 16-bit field storage: BF16 is the top half of an FP32 pattern; FP16 is
+// widened with the exact PTX conversion.
+__device__ __forceinline__ float olc_bf16_to_float(unsigned short h) { return __uint_as_float((olc_u32)h << 16); }
+__device__ __forceinline__ float olc_f16_to_float(unsigned short h) {
+    float f;
+    asm("{ .reg .b16 t; mov.b16 t, %1; cvt.f32.f16 %0, t; }" : "=f"(f) : "h"(h));
+    return f;
+}
+
+// Field value at voxel v of field f, whatever its storage.
+template <class PT>
+__device__ __forceinline__ float olc_field_at(const PT& P, int f, olc_u32 v) {
+    const void* p = P.field[f];
+    if (!p) return 0.0f;
+    if (P.field_type[f] == 1) return olc_bf16_to_float(static_cast<const unsigned short*>(p)[v]);
+    if (P.field_type[f] == 2) return olc_f16_to_float(static_cast<const unsigned short*>(p)[v]);
+    return static_cast<const float*>(p)[v];
 }
 
 // Deposit into a field's sink (sum of first-order uptake rates of a voxel).

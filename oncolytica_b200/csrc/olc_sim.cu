@@ -64,6 +64,8 @@ struct OlcSim {
     int field_cur[OLC_MAX_FIELDS] = {};
     bool field_bound[OLC_MAX_FIELDS] = {};
     FieldMaps fmaps[OLC_MAX_FIELDS];           // TMA descriptors of both buffers
+    FieldMaps16 fmaps16[OLC_MAX_FIELDS];       // the same for 16-bit storage
+    float* comp[OLC_MAX_FIELDS] = {};          // 16-bit storage: reaction residual per voxel (FP32)
 
     OlcContact contact = {};
     ContactDev contact_dev = {};
@@ -195,6 +197,7 @@ OlcRuleParams make_rule_params(OlcSim* s, int rule_index, int in_buf) {
     }
     for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
         P.field[f] = s->field[s->field_cur[f]][f];
+        P.field_type[f] = s->fstep[f].storage;
         P.sink[f] = s->sink[f];
     }
     P.ranges = s->ranges;
@@ -269,7 +272,14 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
     mark(s, 0, st);
     // 1. fields: implicit sinks, then the substeps of every field
     for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
-        if (!s->field_bound[f] || s->fstep[f].substeps == 0 || !s->sink[f]) continue;
+        if (!s->field_bound[f] || s->fstep[f].substeps == 0) continue;
+        if (s->fstep[f].storage != OLC_FIELD_F32) {
+            // 16-bit storage: uptake and the step's decay, compensated, every step
+            launch_react16(s->field[s->field_cur[f]][f], s->sink[f], s->comp[f], s->fstep[f], st);
+            ++launches;
+            continue;
+        }
+        if (!s->sink[f]) continue;
         launch_sink(s->field[s->field_cur[f]][f], s->sink[f], s->fstep[f], st);
         ++launches;
     }
@@ -277,6 +287,14 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
     for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
         if (!s->field_bound[f] || s->fstep[f].substeps == 0) continue;  // unbound or static
         int cur = s->field_cur[f];
+        if (s->fstep[f].storage != OLC_FIELD_F32) {
+            void* res = run_substeps16(s->field[cur][f], s->field[1 - cur][f], s->fmaps16[f], cur, s->fstep[f],
+                                       s->counters + OLC_CTR_STATUS, st);
+            s->field_cur[f] = (res == s->field[cur][f]) ? cur : 1 - cur;
+            substeps += (uint32_t)s->fstep[f].substeps;
+            launches += (uint64_t)s->fstep[f].substeps;
+            continue;
+        }
         float* a = s->field[cur][f];
         float* b = s->field[1 - cur][f];
         const bool tma_path = s->fmaps[f].ok && stencil_tma_enabled();
@@ -356,7 +374,14 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
         for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
             if (!s->field_bound[f]) continue;
             const size_t nvox = (size_t)s->geom.chem_dims[0] * s->geom.chem_dims[1] * s->geom.chem_dims[2];
-            launch_reduce_field(s->field[s->field_cur[f]][f], nvox, (int)f, s->red_dev, s->red_scratch, st);
+            if (s->fstep[f].storage != OLC_FIELD_F32) {
+                FieldStep fsr = s->fstep[f];
+                for (int i = 0; i < 3; ++i) fsr.dims[i] = s->geom.chem_dims[i];
+                launch_reduce_field16(s->field[s->field_cur[f]][f], s->comp[f], fsr, (int)f, s->red_dev,
+                                      s->red_scratch, st);
+            } else {
+                launch_reduce_field(s->field[s->field_cur[f]][f], nvox, (int)f, s->red_dev, s->red_scratch, st);
+            }
             ++launches;
         }
         if (s->metrics_dev && s->metrics_bytes) {
@@ -843,6 +868,14 @@ int olc_bind_agent_column(OlcSim* s, int index, void* a, void* b) {
 }
 
 int olc_bind_field(OlcSim* s, int index, float* a, float* b, float* sink, const OlcDiffusion* spec) {
+    if (spec && spec->storage != OLC_FIELD_F32)
+        return fail(s, OLC_ERR_ARG, "olc_bind_field: 16-bit storage needs olc_bind_field_ex (compensation buffer)");
+    return olc_bind_field_ex(s, index, a, b, sink, nullptr, spec);
+}
+
+int olc_bind_field_ex(OlcSim* s, int index, void* a_, void* b_, float* sink, float* comp, const OlcDiffusion* spec) {
+    float* a = static_cast<float*>(a_);
+    float* b = static_cast<float*>(b_);
     if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
     if (index < 0 || index >= (int)s->caps.n_fields || !a || !b || !spec)
         return fail(s, OLC_ERR_ARG, "olc_bind_field: bad index or null argument");
@@ -852,12 +885,25 @@ int olc_bind_field(OlcSim* s, int index, float* a, float* b, float* sink, const 
     if (spec->substeps != 0 &&
         !make_field_step(*spec, s->geom.chem_dims, s->geom.chem_voxel_size, s->caps.dt, &fs, &err))
         return fail(s, OLC_ERR_ARG, "olc_bind_field: " + err);
+    if (spec->substeps == 0) {
+        if (spec->storage < OLC_FIELD_F32 || spec->storage > OLC_FIELD_F16)
+            return fail(s, OLC_ERR_ARG, "olc_bind_field: bad storage type");
+        fs.storage = spec->storage;
+    }
     if (spec->has_sink && !sink) return fail(s, OLC_ERR_ARG, "olc_bind_field: has_sink without a sink buffer");
+    const bool half = fs.storage != OLC_FIELD_F32;
+    if (half && spec->substeps != 0 && !comp)
+        return fail(s, OLC_ERR_ARG, "olc_bind_field_ex: 16-bit storage needs a compensation buffer");
     drop_graphs(s);
     s->field[0][index] = a;
     s->field[1][index] = b;
     s->fmaps[index].ok = false;
-    if (spec->substeps > 0) make_field_maps(&s->fmaps[index], a, b, s->geom.chem_dims);
+    s->fmaps16[index].ok = false;
+    if (spec->substeps > 0 && !half) make_field_maps(&s->fmaps[index], a, b, s->geom.chem_dims);
+    if (spec->substeps > 0 && half && !make_field_maps16(&s->fmaps16[index], a, b, s->geom.chem_dims))
+        return fail(s, OLC_ERR_ARG, "olc_bind_field_ex: TMA descriptors of the 16-bit field failed (16-byte aligned "
+                                    "buffers, x extent a multiple of 8)");
+    s->comp[index] = half ? comp : nullptr;
     s->sink[index] = spec->has_sink ? sink : nullptr;
     s->fspec[index] = *spec;
     s->fstep[index] = fs;
@@ -1357,6 +1403,8 @@ int olc_stage_bin_ranges(const uint32_t* keys, uint32_t n, uint32_t n_bins, uint
 int olc_stage_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], float dx, float dt,
                       const OlcDiffusion* spec, void* stream) {
     if (!f || !tmp || !dims || !spec) return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse: null argument");
+    if (spec->storage != OLC_FIELD_F32)
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse: FP32 storage only (olc_stage_diffuse16 for 16-bit)");
     std::string err;
     FieldStep fs;
     if (!make_field_step(*spec, dims, dx, dt, &fs, &err)) return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse: " + err);
@@ -1375,6 +1423,30 @@ int olc_stage_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], 
         cudaMemcpyAsync(f, res, bytes, cudaMemcpyDeviceToDevice, st);
     }
     return cuda_status(cudaGetLastError(), "olc_stage_diffuse");
+}
+
+int olc_stage_diffuse16(void* f, void* tmp, float* sink, float* comp, const int32_t dims[3], float dx, float dt,
+                        const OlcDiffusion* spec, void* stream) {
+    if (!f || !tmp || !comp || !dims || !spec)
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse16: null argument");
+    if (spec->storage != OLC_FIELD_BF16 && spec->storage != OLC_FIELD_F16)
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse16: storage must be BF16 or FP16");
+    std::string err;
+    FieldStep fs;
+    if (!make_field_step(*spec, dims, dx, dt, &fs, &err))
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse16: " + err);
+    cudaStream_t st = as_stream(stream);
+    olc_u32* status = stage_status_word();
+    FieldMaps16 maps;
+    if (!status || !make_field_maps16(&maps, f, tmp, dims))
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse16: TMA descriptors failed (16-byte aligned buffers)");
+    launch_react16(f, spec->has_sink ? sink : nullptr, comp, fs, st);
+    void* res = run_substeps16(f, tmp, maps, 0, fs, status, st);
+    if (res != f) {
+        const size_t bytes = (size_t)dims[0] * dims[1] * dims[2] * 2;
+        cudaMemcpyAsync(f, res, bytes, cudaMemcpyDeviceToDevice, st);
+    }
+    return cuda_status(cudaGetLastError(), "olc_stage_diffuse16");
 }
 
 int olc_stage_contact(const float* posr, const uint32_t* ranges, uint32_t n, const OlcGeom* geom,

@@ -228,6 +228,145 @@ int orc_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], float 
     return 0;
 }
 
+/* ------------------------------------------------------------------ 16-bit field storage */
+/* The precision tier of the CUDA path (olc_field16.cu), restated: fields stored
+ * as BF16 (storage 1) or FP16 (storage 2), every update in FP32 with
+ * round-to-nearest-even back to storage.  Per step: a reaction pass
+ * (value + residual, uptake, the step's decay (1 + lambda dt/S)^-S, residual
+ * kept in comp), then S substeps without decay; faces pinned. */
+static float bf16_to_f(uint16_t h) {
+    uint32_t u = (uint32_t)h << 16;
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+static uint16_t f_to_bf16(float f) { /* finite values: RN-even on the bit pattern */
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    return (uint16_t)((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
+}
+static float h16_to_f(uint16_t h, int storage) {
+    if (storage == 1) return bf16_to_f(h);
+    _Float16 x;
+    memcpy(&x, &h, 2);
+    return (float)x;
+}
+static uint16_t f_to_h16(float f, int storage) {
+    if (storage == 1) return f_to_bf16(f);
+    _Float16 x = (_Float16)f;
+    uint16_t h;
+    memcpy(&h, &x, 2);
+    return h;
+}
+
+int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const int32_t dims[3], float dx, float dt,
+                  float D, float decay, float boundary, int substeps, int storage, int nthreads) {
+    const int nx = dims[0], ny = dims[1], nz = dims[2];
+    const int nt = nthreads_or_all(nthreads);
+    if (substeps < 1 || (storage != 1 && storage != 2)) return -1;
+    const float dts = dt / (float)substeps;
+    const float r = D * dts / (dx * dx);
+    if (r > 1.0f / 6.0f + 1e-7f) return -1;
+    const float decay_step = (float)pow(1.0 + (double)decay * (double)dts, -(double)substeps);
+    const uint16_t bh = f_to_h16(boundary, storage);
+    const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
+#pragma omp parallel for num_threads(nt) schedule(static)
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                size_t v = (size_t)z * sz + (size_t)y * sy + x;
+                float k = sink ? sink[v] : 0.0f;
+                if (sink) sink[v] = 0.0f;
+                if (x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1) continue;
+                float val = h16_to_f(f[v], storage) + comp[v];
+                if (k != 0.0f) val = val / (1.0f + k * dt);
+                val = val * decay_step;
+                uint16_t h = f_to_h16(val, storage);
+                f[v] = h;
+                comp[v] = val - h16_to_f(h, storage);
+            }
+    uint16_t* cur = f;
+    uint16_t* nxt = tmp;
+    for (int s = 0; s < substeps; ++s) {
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int z = 0; z < nz; ++z)
+            for (int y = 0; y < ny; ++y) {
+                size_t row = (size_t)z * sz + (size_t)y * sy;
+                for (int x = 0; x < nx; ++x) {
+                    size_t v = row + x;
+                    if (x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1) {
+                        nxt[v] = bh;
+                        continue;
+                    }
+                    float c = h16_to_f(cur[v], storage);
+                    float s1 = (h16_to_f(cur[v - 1], storage) + h16_to_f(cur[v + 1], storage)) +
+                               (h16_to_f(cur[v - sy], storage) + h16_to_f(cur[v + sy], storage));
+                    float s2 = s1 + (h16_to_f(cur[v - sz], storage) + h16_to_f(cur[v + sz], storage));
+                    float u = c + r * (s2 - 6.0f * c);
+                    nxt[v] = f_to_h16(u > 0.0f ? u : 0.0f, storage);
+                }
+            }
+        uint16_t* t = cur;
+        cur = nxt;
+        nxt = t;
+    }
+    if (cur != f) memcpy(f, cur, (size_t)nx * ny * nz * 2);
+    return 0;
+}
+
+/* The field schemes evaluated in FP64, the reference against which each
+ * storage type's field error is measured.  split = 0: the FP32 scheme
+ * (orc_diffuse: decay in every substep); split = 1: the 16-bit scheme's
+ * arithmetic (uptake and the step's decay (1 + lambda dt/S)^-S once, then
+ * substeps without decay), so the difference of the two FP64 results is the
+ * splitting error alone. */
+int orc_diffuse_f64(double* f, double* tmp, const float* sink, const int32_t dims[3], double dx, double dt, double D,
+                    double decay, double boundary, int substeps, int split, int nthreads) {
+    const int nx = dims[0], ny = dims[1], nz = dims[2];
+    const int nt = nthreads_or_all(nthreads);
+    if (substeps < 1) return -1;
+    const double dts = dt / substeps;
+    const double r = D * dts / (dx * dx);
+    const double inv_decay = split ? 1.0 : 1.0 / (1.0 + decay * dts);
+    const double decay_step = split ? pow(1.0 + decay * dts, -(double)substeps) : 1.0;
+    const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
+    if (sink || split) {
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int z = 1; z < nz - 1; ++z)
+            for (int y = 1; y < ny - 1; ++y)
+                for (int x = 1; x < nx - 1; ++x) {
+                    size_t v = (size_t)z * sz + (size_t)y * sy + x;
+                    if (sink) f[v] = f[v] / (1.0 + (double)sink[v] * dt);
+                    f[v] *= decay_step;
+                }
+    }
+    double* cur = f;
+    double* nxt = tmp;
+    for (int s = 0; s < substeps; ++s) {
+#pragma omp parallel for num_threads(nt) schedule(static)
+        for (int z = 0; z < nz; ++z)
+            for (int y = 0; y < ny; ++y) {
+                size_t row = (size_t)z * sz + (size_t)y * sy;
+                for (int x = 0; x < nx; ++x) {
+                    size_t v = row + x;
+                    if (x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1) {
+                        nxt[v] = boundary;
+                        continue;
+                    }
+                    double c = cur[v];
+                    double s2 = ((cur[v - 1] + cur[v + 1]) + (cur[v - sy] + cur[v + sy])) + (cur[v - sz] + cur[v + sz]);
+                    double u = (c + r * (s2 - 6.0 * c)) * inv_decay;
+                    nxt[v] = u > 0.0 ? u : 0.0;
+                }
+            }
+        double* t = cur;
+        cur = nxt;
+        nxt = t;
+    }
+    if (cur != f) memcpy(f, cur, (size_t)nx * ny * nz * 8);
+    return 0;
+}
+
 /* ------------------------------------------------------------------ contact */
 
 /* engine/assets/shaders/tumor_sim.wgsl:505-628, overdamped (see olc_contact.cu) */

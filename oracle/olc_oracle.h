@@ -49,6 +49,10 @@ void orc_bin_ranges(const uint32_t* keys, uint32_t n, uint32_t n_bins, uint32_t*
 /* tumor_sim.wgsl:387-446: sink then S substeps; result in f. Returns 0 or -1 when unstable. */
 int orc_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], float dx, float dt, float D,
                 float decay, float boundary, int substeps, int nthreads);
+int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const int32_t dims[3], float dx, float dt,
+                  float D, float decay, float boundary, int substeps, int storage, int nthreads);
+int orc_diffuse_f64(double* f, double* tmp, const float* sink, const int32_t dims[3], double dx, double dt, double D,
+                    double decay, double boundary, int substeps, int split, int nthreads);
 
 /* tumor_sim.wgsl:505-628 force law, overdamped; see oncolytica_b200/csrc/olc_contact.cu */
 void orc_contact(const float* posr, const uint32_t* ranges, uint32_t n, const int32_t tdims[3], float tvs,

@@ -121,6 +121,53 @@ def diffuse(f: np.ndarray, sink: np.ndarray | None, dx: float, dt: float, D: flo
     return f
 
 
+def to_bits16(f: np.ndarray, storage: int) -> np.ndarray:
+    """float32 values -> BF16 (storage 1) or FP16 (storage 2) bit patterns,
+    rounded to nearest even (finite values)."""
+    f = np.ascontiguousarray(f, dtype=np.float32)
+    if storage == 2:
+        return f.astype(np.float16).view(np.uint16)
+    u = f.view(np.uint32).astype(np.uint64)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+
+
+def from_bits16(h: np.ndarray, storage: int) -> np.ndarray:
+    h = np.ascontiguousarray(h, dtype=np.uint16)
+    if storage == 2:
+        return h.view(np.float16).astype(np.float32)
+    return (h.astype(np.uint32) << 16).view(np.float32)
+
+
+def diffuse16(bits: np.ndarray, sink: np.ndarray | None, comp: np.ndarray, dx: float, dt: float, D: float,
+              decay: float, boundary: float, substeps: int, storage: int, nthreads: int = 0):
+    """One step of a 16-bit field (indexed [z, y, x]): returns (bits, comp)."""
+    f = np.ascontiguousarray(bits, dtype=np.uint16).copy()
+    tmp = np.zeros_like(f)
+    c = np.ascontiguousarray(comp, dtype=np.float32).copy()
+    s = None if sink is None else np.ascontiguousarray(sink, dtype=np.float32).copy()
+    dims = np.array([f.shape[2], f.shape[1], f.shape[0]], dtype=np.int32)
+    rc = lib().orc_diffuse16(_p(f), _p(tmp), _p(s), _p(c), _p(dims), C.c_float(dx), C.c_float(dt), C.c_float(D),
+                             C.c_float(decay), C.c_float(boundary), substeps, storage, nthreads)
+    if rc != 0:
+        raise ValueError("oracle diffuse16: unstable or bad arguments")
+    return f, c
+
+
+def diffuse_f64(f: np.ndarray, sink: np.ndarray | None, dx: float, dt: float, D: float, decay: float,
+                boundary: float, substeps: int, split: bool = False, nthreads: int = 0) -> np.ndarray:
+    """A field scheme evaluated in FP64: the FP32 scheme (decay in every
+    substep) or, with ``split``, the 16-bit scheme's (decay once per step)."""
+    f = np.ascontiguousarray(f, dtype=np.float64).copy()
+    tmp = np.zeros_like(f)
+    s = None if sink is None else np.ascontiguousarray(sink, dtype=np.float32)
+    dims = np.array([f.shape[2], f.shape[1], f.shape[0]], dtype=np.int32)
+    rc = lib().orc_diffuse_f64(_p(f), _p(tmp), _p(s), _p(dims), C.c_double(dx), C.c_double(dt), C.c_double(D),
+                               C.c_double(decay), C.c_double(boundary), substeps, int(bool(split)), nthreads)
+    if rc != 0:
+        raise ValueError("oracle diffuse_f64: bad arguments")
+    return f
+
+
 def contact(posr: np.ndarray, ranges: np.ndarray, tdims, tvs: float, stiffness: float, mobility: float,
             max_disp: float, dt: float, lo, hi, nthreads: int = 0):
     posr = np.ascontiguousarray(posr, dtype=np.float32)

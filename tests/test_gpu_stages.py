@@ -300,3 +300,46 @@ def test_contact_bit_exact(cuda, olc):
     np.testing.assert_array_equal(got, ref)
     moved = np.any(got != posr[:, :3], axis=1)
     assert moved.sum() > n // 2
+
+
+# ------------------------------------------------------------------ 16-bit field storage
+
+@pytest.mark.parametrize("storage", [1, 2])
+@pytest.mark.parametrize("dims,substeps,decay,with_sink", [((32, 24, 20), 5, 0.0, True),
+                                                          ((64, 41, 37), 7, 0.1, True),
+                                                          ((136, 17, 9), 3, 0.05, False)])
+def test_diffuse16_bit_exact(cuda, olc, storage, dims, substeps, decay, with_sink):
+    """BF16 / FP16 storage: three steps of reaction (uptake, decay, residual)
+    and substeps give the oracle's bits, residuals included."""
+    import torch
+
+    rng = np.random.default_rng(sum(dims) + storage)
+    nx, ny, nz = dims
+    f = (rng.random((nz, ny, nx), dtype=np.float32) * 0.8 + 0.1).astype(np.float32)
+    dx, dt, D = 4.0, 0.1, 2000.0
+    D = min(D, (1.0 / 6.0) * dx * dx * substeps / dt * 0.999)
+    bits = oracle.to_bits16(f, storage)
+    comp = np.zeros_like(f)
+    fd = torch.from_numpy(bits.view(np.int16).copy()).to(cuda)
+    tmp = torch.empty_like(fd)
+    cd = torch.zeros(f.size, dtype=torch.float32, device=cuda)
+    spec = _lib.OlcDiffusion(diffusion=D, decay=decay, boundary=0.7, substeps=substeps, has_sink=int(with_sink),
+                             storage=storage)
+    dims_c = (C.c_int32 * 3)(nx, ny, nz)
+    for step in range(3):
+        sink = None
+        sd = None
+        if with_sink:
+            sink = np.zeros_like(f)
+            m = rng.random(f.shape) < 0.2
+            sink[m] = rng.random(int(m.sum())).astype(np.float32) * 0.5
+            sd = to_dev(sink, cuda)
+        bits, comp = oracle.diffuse16(bits, sink, comp, dx, dt, D, decay, 0.7, substeps, storage)
+        _lib.check(olc.olc_stage_diffuse16(dptr(fd), dptr(tmp), dptr(sd) if sd is not None else None, dptr(cd),
+                                           C.byref(dims_c), dx, dt, C.byref(spec), None))
+        torch.cuda.synchronize()
+        got = fd.cpu().numpy().view(np.uint16).reshape(nz, ny, nx)
+        np.testing.assert_array_equal(got, bits, err_msg=f"field bits step {step}")
+        np.testing.assert_array_equal(cd.cpu().numpy().reshape(nz, ny, nx), comp, err_msg=f"residual step {step}")
+        if sd is not None:
+            assert float(to_host(sd).max()) == 0.0
