@@ -280,8 +280,11 @@ int olc_create_batch(const OlcGeom* geoms, int n_sims, const OlcCaps* caps, OlcS
 int olc_batch_field_offsets(const OlcSim* sim, uint64_t* offsets);
 
 /* Binds field `index` for every simulation; specs[k] is simulation k's
- * diffusion (its own substep count; 0 = static). */
-int olc_bind_field_batch(OlcSim* sim, int index, float* a, float* b, float* sink, const OlcDiffusion* specs);
+ * diffusion (its own substep count; 0 = static; one storage type for all
+ * members).  comp is the FP32 residual buffer of 16-bit storage (as in
+ * olc_bind_field_ex), NULL for FP32. */
+int olc_bind_field_batch(OlcSim* sim, int index, void* a, void* b, float* sink, float* comp,
+                         const OlcDiffusion* specs);
 
 /* n_sims Params blobs of `stride` bytes each, back to back. */
 int olc_set_params_batch(OlcSim* sim, const void* blob, size_t stride, void* stream);

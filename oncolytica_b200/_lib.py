@@ -164,7 +164,7 @@ _SIGS = {
     "olc_read_user_metrics": (C.c_int, [_VP, _VP, C.c_size_t, _VP]),
     "olc_create_batch": (C.c_int, [C.POINTER(OlcGeom), C.c_int, C.POINTER(OlcCaps), C.POINTER(_VP)]),
     "olc_batch_field_offsets": (C.c_int, [_VP, C.POINTER(C.c_uint64)]),
-    "olc_bind_field_batch": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, C.POINTER(OlcDiffusion)]),
+    "olc_bind_field_batch": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, _VP, C.POINTER(OlcDiffusion)]),
     "olc_bind_field_ex": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, _VP, C.POINTER(OlcDiffusion)]),
     "olc_stage_diffuse16": (C.c_int, [_VP, _VP, _VP, _VP, C.POINTER(C.c_int32 * 3), C.c_float, C.c_float,
                                       C.POINTER(OlcDiffusion), _VP]),

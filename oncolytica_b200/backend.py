@@ -18,6 +18,10 @@ import numpy as np
 from oncolytica_b200 import _lib
 from oncolytica_b200._types import metric_fields
 from oncolytica_b200.compiler.emit_cuda import make_layout, pack_params, translate_model
+from oncolytica_b200.engine import STORAGE_CODES
+
+# torch element type of each field storage code (OLC_FIELD_F32 / BF16 / F16)
+FIELD_DTYPES = {0: lambda t: t.float32, 1: lambda t: t.bfloat16, 2: lambda t: t.float16}
 
 
 def seed_rng(seed: int, idx: np.ndarray) -> np.ndarray:
@@ -110,13 +114,19 @@ class CudaBackend:
                                                        C.c_void_p(b.data_ptr())))
         nvox = int(np.prod(cdims))
         sinks = self.program.sink_fields if self.program else set()
+        self.comp_dev = []
         for i, name in enumerate(L.chem_fields):
-            a = torch.zeros(nvox, dtype=torch.float32, device=self.device)
-            b = torch.zeros(nvox, dtype=torch.float32, device=self.device)
-            s = torch.zeros(nvox, dtype=torch.float32, device=self.device) if name in sinks else None
-            self.fields_dev.append((a, b, s))
-            d = _lib.OlcDiffusion()
             spec_d = eng._diffusion.get(name)
+            storage = STORAGE_CODES[spec_d.storage] if spec_d is not None else 0
+            fdt = FIELD_DTYPES[storage](torch)
+            a = torch.zeros(nvox, dtype=fdt, device=self.device)
+            b = torch.zeros(nvox, dtype=fdt, device=self.device)
+            s = torch.zeros(nvox, dtype=torch.float32, device=self.device) if name in sinks else None
+            comp = torch.zeros(nvox, dtype=torch.float32, device=self.device) if storage else None
+            self.fields_dev.append((a, b, s))
+            self.comp_dev.append(comp)
+            d = _lib.OlcDiffusion()
+            d.storage = storage
             if spec_d is None:
                 if name in sinks:
                     raise ValueError(f"sink_at(...).{name} needs Engine.setup_diffusion({name!r}, ...)")
@@ -127,8 +137,11 @@ class CudaBackend:
                 d.boundary = spec_d.boundary
                 d.substeps = eng.substeps_for(name)
                 d.has_sink = int(s is not None)
-            self._check(self.lib.olc_bind_field(self.handle, i, C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()),
-                                                C.c_void_p(s.data_ptr()) if s is not None else None, C.byref(d)))
+            self._check(self.lib.olc_bind_field_ex(self.handle, i, C.c_void_p(a.data_ptr()),
+                                                   C.c_void_p(b.data_ptr()),
+                                                   C.c_void_p(s.data_ptr()) if s is not None else None,
+                                                   C.c_void_p(comp.data_ptr()) if comp is not None else None,
+                                                   C.byref(d)))
         ct = _lib.OlcContact()
         if contact is not None:
             ct.enabled = 1
@@ -254,9 +267,12 @@ class CudaBackend:
                 host[:, :, 0] = host[:, :, -1] = b
             flat = np.ascontiguousarray(host.ravel(order="F"))
             cur = (fb >> i) & 1
+            # 16-bit fields: torch rounds to nearest even on the copy
             self.fields_dev[i][cur].copy_(torch.from_numpy(flat))
             if self.fields_dev[i][2] is not None:
                 self.fields_dev[i][2].zero_()
+            if self.comp_dev[i] is not None:
+                self.comp_dev[i].zero_()
         self._upload_tissue()
         self.torch.cuda.synchronize(self.device)
         self._check(self.lib.olc_set_agent_count(self.handle, n, self._stream()))
@@ -302,9 +318,17 @@ class CudaBackend:
             cols[col] = a[keep].copy()
         eng.cells._set_columns(cols, L.cell_class)
         for i, name in enumerate(L.chem_fields):
-            cur = (fb >> i) & 1
-            flat = self.fields_dev[i][cur].cpu().numpy()
+            flat = self._field_values(i, fb)
             eng.chemistry.column(name)[...] = flat.reshape(eng.chemistry_shape, order="F")
+
+    def _field_values(self, i: int, fb: int) -> np.ndarray:
+        """Field i as float32 on the host; for 16-bit storage the stored value
+        plus its FP32 rounding residual (what the next reaction continues from)."""
+        cur = (fb >> i) & 1
+        t = self.fields_dev[i][cur]
+        if self.comp_dev[i] is None:
+            return t.cpu().numpy()
+        return (t.float() + self.comp_dev[i]).cpu().numpy()
 
     def _life(self, rows: int) -> np.ndarray:
         buf = (C.c_uint8 * max(rows, 1))()
@@ -323,9 +347,14 @@ class CudaBackend:
             a = self.cols_dev[i][ab][:rows].cpu().numpy()
             out["cols"][col] = a.view(np.uint32).copy() if dt == np.uint32 else a.copy()
         for i, name in enumerate(self.layout.chem_fields):
-            out["fields"][name] = self.fields_dev[i][(fb >> i) & 1].cpu().numpy().copy()
+            t = self.fields_dev[i][(fb >> i) & 1]
+            out["fields"][name] = t.cpu().numpy().copy() if t.dtype == self.torch.float32 else \
+                t.cpu().view(self.torch.int16).numpy().view(np.uint16).copy()
             s = self.fields_dev[i][2]
             out["sinks"][name] = s.cpu().numpy().copy() if s is not None else None
+            c = self.comp_dev[i]
+            if c is not None:
+                out.setdefault("residuals", {})[name] = c.cpu().numpy().copy()
         return out
 
     def field_tensor(self, name: str):

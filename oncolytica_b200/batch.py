@@ -18,7 +18,8 @@ from typing import Any, Sequence
 import numpy as np
 
 from oncolytica_b200 import _lib
-from oncolytica_b200.backend import seed_rng
+from oncolytica_b200.backend import FIELD_DTYPES, seed_rng
+from oncolytica_b200.engine import STORAGE_CODES
 from oncolytica_b200.compiler.emit_cuda import make_layout, pack_params, translate_model
 
 
@@ -110,15 +111,24 @@ class BatchEngine:
         nvox = int(self.field_off[-1])
         sinks = self.program.sink_fields if self.program else set()
         self.fields_dev = []
+        self.comp_dev = []
         for i, name in enumerate(L.chem_fields):
-            a = torch.zeros(max(nvox, 1), dtype=torch.float32, device=self.device)
-            b = torch.zeros(max(nvox, 1), dtype=torch.float32, device=self.device)
+            kinds = {e._diffusion[name].storage for e in self.engines if name in e._diffusion}
+            if len(kinds) > 1:
+                raise ValueError(f"every member of a batch stores field {name!r} with the same type")
+            storage = STORAGE_CODES[kinds.pop()] if kinds else 0
+            fdt = FIELD_DTYPES[storage](torch)
+            a = torch.zeros(max(nvox, 1), dtype=fdt, device=self.device)
+            b = torch.zeros(max(nvox, 1), dtype=fdt, device=self.device)
             s = torch.zeros(max(nvox, 1), dtype=torch.float32, device=self.device) if name in sinks else None
+            comp = torch.zeros(max(nvox, 1), dtype=torch.float32, device=self.device) if storage else None
             self.fields_dev.append((a, b, s))
+            self.comp_dev.append(comp)
             specs = (_lib.OlcDiffusion * n)()
             for k, eng in enumerate(self.engines):
                 spec_d = eng._diffusion.get(name)
                 d = specs[k]
+                d.storage = storage
                 if spec_d is None:
                     if name in sinks:
                         raise ValueError(f"sink_at(...).{name} needs Engine.setup_diffusion({name!r}, ...)")
@@ -129,7 +139,9 @@ class BatchEngine:
                     d.has_sink = int(s is not None)
             self._check(self.lib.olc_bind_field_batch(self.handle, i, C.c_void_p(a.data_ptr()),
                                                       C.c_void_p(b.data_ptr()),
-                                                      C.c_void_p(s.data_ptr()) if s is not None else None, specs))
+                                                      C.c_void_p(s.data_ptr()) if s is not None else None,
+                                                      C.c_void_p(comp.data_ptr()) if comp is not None else None,
+                                                      specs))
         ct = _lib.OlcContact()
         if contact is not None:
             ct.enabled = 1
@@ -286,6 +298,8 @@ class BatchEngine:
                 self.fields_dev[i][int(par[k, i])][lo:hi].copy_(torch.from_numpy(flat))
             if self.fields_dev[i][2] is not None:
                 self.fields_dev[i][2].zero_()
+            if self.comp_dev[i] is not None:
+                self.comp_dev[i].zero_()
         torch.cuda.synchronize(self.device)
         self._check(self.lib.olc_set_agent_count(self.handle, total, self._stream()))
 
@@ -312,7 +326,11 @@ class BatchEngine:
         par = self._field_parity()
         lo, hi = int(self.field_off[k]), int(self.field_off[k + 1])
         for i, name in enumerate(self.layout.chem_fields):
-            out["fields"][name] = self.fields_dev[i][int(par[k, i])][lo:hi].cpu().numpy().copy()
+            t = self.fields_dev[i][int(par[k, i])][lo:hi]
+            out["fields"][name] = t.cpu().numpy().copy() if t.dtype == self.torch.float32 else \
+                t.cpu().view(self.torch.int16).numpy().view(np.uint16).copy()
+            if self.comp_dev[i] is not None:
+                out.setdefault("residuals", {})[name] = self.comp_dev[i][lo:hi].cpu().numpy().copy()
         return out
 
     def sync_to_host(self) -> None:
@@ -331,7 +349,10 @@ class BatchEngine:
             eng.cells._set_columns(cols, L.cell_class)
             lo, hi = int(self.field_off[k]), int(self.field_off[k + 1])
             for i, name in enumerate(L.chem_fields):
-                flat = self.fields_dev[i][int(par[k, i])][lo:hi].cpu().numpy()
+                t = self.fields_dev[i][int(par[k, i])][lo:hi]
+                if self.comp_dev[i] is not None:
+                    t = t.float() + self.comp_dev[i][lo:hi]
+                flat = t.cpu().numpy()
                 eng.chemistry.column(name)[...] = flat.reshape(eng.chemistry_shape, order="F")
 
     def close(self) -> None:

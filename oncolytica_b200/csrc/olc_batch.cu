@@ -21,6 +21,7 @@
 // bit.  The FP64 sums of the per-simulation reductions are accumulated with
 // atomics and are exact only up to their order.
 #include "olc_internal.h"
+#include "olc_store16.cuh"
 
 namespace olc {
 
@@ -323,6 +324,187 @@ __global__ void k_flip_parity(const FieldStep* __restrict__ steps, int field, in
 void launch_flip_parity(const FieldStep* steps, int field, int n_fields, olc_u32 n_sims, unsigned char* fpar,
                         cudaStream_t s) {
     k_flip_parity<<<(n_sims + 255) / 256, 256, 0, s>>>(steps, field, n_fields, n_sims, fpar);
+}
+
+// ------------------------------------------------------------------ 16-bit fields
+// The same tiles on BF16 / FP16 storage (olc_field16.cu's arithmetic): the
+// reaction pass with its FP32 residual, then substeps without decay.
+template <int ST>
+__global__ void __launch_bounds__(128) k_substep_batch16(const uint4* __restrict__ tiles,
+                                                         const OlcSimDesc* __restrict__ sims,
+                                                         const FieldStep* __restrict__ steps, int field, int n_fields,
+                                                         const unsigned char* __restrict__ fpar, int sub,
+                                                         unsigned short* fa, unsigned short* fb) {
+    const uint4 t = tiles[blockIdx.x];
+    const olc_u32 k = t.x;
+    const OlcSimDesc& d = sims[k];
+    const FieldStep fs = steps[(size_t)k * n_fields + field];
+    const int nx = d.cdims[0], ny = d.cdims[1], nz = d.cdims[2];
+    const bool flip = ((fpar[(size_t)k * n_fields + field] ^ (unsigned)sub) & 1u) != 0u;
+    const unsigned short* in = (flip ? fb : fa) + d.field_off;
+    unsigned short* out = (flip ? fa : fb) + d.field_off;
+    const int x = (int)t.y * BT_X + 4 * (threadIdx.x & 7);
+    const int y = (int)t.z * BT_Y + (threadIdx.x >> 3);
+    const int z0 = (int)t.w * BT_Z;
+    if (x >= nx || y >= ny) return;
+    const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
+    const bool edge_y = y == 0 || y == ny - 1;
+    const bool ex0 = x == 0, ex3 = x + 3 == nx - 1;
+    const float bf = Store16<ST>::to_f(Store16<ST>::from_f(fs.bval));
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    size_t idx = (size_t)z0 * sz + (size_t)y * sy + x;
+    float4 zm = z0 > 0 ? load4<ST>(in + idx - sz) : zero;
+    float4 c = load4<ST>(in + idx);
+    const int z1 = min(z0 + BT_Z, nz);
+    for (int zz = z0; zz < z1; ++zz, idx += sz) {
+        const float4 zp = zz + 1 < nz ? load4<ST>(in + idx + sz) : zero;
+        const float4 ym = y > 0 ? load4<ST>(in + idx - sy) : zero;
+        const float4 yp = y + 1 < ny ? load4<ST>(in + idx + sy) : zero;
+        const float xl = x > 0 ? Store16<ST>::to_f(in[idx - 1]) : 0.0f;
+        const float xr = x + 4 < nx ? Store16<ST>::to_f(in[idx + 4]) : 0.0f;
+        float4 v = update4_b(xl, xr, c, ym, yp, zm, zp, fs.r, 1.0f);
+        if (edge_y || zz == 0 || zz == nz - 1) {
+            v = make_float4(bf, bf, bf, bf);
+        } else {
+            if (ex0) v.x = bf;
+            if (ex3) v.w = bf;
+        }
+        store4<ST>(out + idx, v);
+        zm = c;
+        c = zp;
+    }
+}
+
+template <int ST>
+__global__ void __launch_bounds__(128) k_react_batch16(const uint4* __restrict__ tiles,
+                                                       const OlcSimDesc* __restrict__ sims,
+                                                       const FieldStep* __restrict__ steps, int field, int n_fields,
+                                                       const unsigned char* __restrict__ fpar, unsigned short* fa,
+                                                       unsigned short* fb, float* sink, float* comp) {
+    const uint4 t = tiles[blockIdx.x];
+    const olc_u32 k = t.x;
+    const OlcSimDesc& d = sims[k];
+    const FieldStep fs = steps[(size_t)k * n_fields + field];
+    if (fs.substeps == 0) return;
+    const int nx = d.cdims[0], ny = d.cdims[1], nz = d.cdims[2];
+    unsigned short* f = ((fpar[(size_t)k * n_fields + field] & 1u) ? fb : fa) + d.field_off;
+    float* K = sink ? sink + d.field_off : nullptr;
+    float* cp = comp + d.field_off;
+    const int x0 = (int)t.y * BT_X + 4 * (threadIdx.x & 7);
+    const int y = (int)t.z * BT_Y + (threadIdx.x >> 3);
+    const int z0 = (int)t.w * BT_Z;
+    if (x0 >= nx || y >= ny) return;
+    const int z1 = min(z0 + BT_Z, nz);
+    for (int z = z0; z < z1; ++z) {
+        for (int x = x0; x < x0 + 4; ++x) {
+            const size_t v = ((size_t)z * ny + y) * nx + x;
+            float kv = 0.0f;
+            if (K) {
+                kv = K[v];
+                if (kv != 0.0f) K[v] = 0.0f;
+            }
+            if (x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1) continue;
+            float val = __fadd_rn(Store16<ST>::to_f(f[v]), cp[v]);
+            if (kv != 0.0f) val = __fdiv_rn(val, __fadd_rn(1.0f, __fmul_rn(kv, fs.sink_dt)));
+            val = __fmul_rn(val, fs.decay_step);
+            const unsigned short h = Store16<ST>::from_f(val);
+            f[v] = h;
+            cp[v] = __fsub_rn(val, Store16<ST>::to_f(h));
+        }
+    }
+}
+
+template <int ST>
+__global__ void __launch_bounds__(128) k_reduce_field_batch16(const uint4* __restrict__ tiles,
+                                                              const OlcSimDesc* __restrict__ sims, int field,
+                                                              int n_fields, const unsigned char* __restrict__ fpar,
+                                                              const unsigned short* fa, const unsigned short* fb,
+                                                              const float* comp, OlcReductions* out) {
+    __shared__ double s_v[3][4];
+    const uint4 t = tiles[blockIdx.x];
+    const olc_u32 k = t.x;
+    const OlcSimDesc& d = sims[k];
+    const int nx = d.cdims[0], ny = d.cdims[1], nz = d.cdims[2];
+    const unsigned short* f = ((fpar[(size_t)k * n_fields + field] & 1u) ? fb : fa) + d.field_off;
+    const float* cp = comp + d.field_off;
+    const int x0 = (int)t.y * BT_X + 4 * (threadIdx.x & 7);
+    const int y = (int)t.z * BT_Y + (threadIdx.x >> 3);
+    const int z0 = (int)t.w * BT_Z;
+    double sum = 0.0, mn = 1e300, mx = 0.0;
+    if (x0 < nx && y < ny) {
+        const int z1 = min(z0 + BT_Z, nz);
+        for (int z = z0; z < z1; ++z)
+            for (int x = x0; x < x0 + 4; ++x) {
+                const size_t v = ((size_t)z * ny + y) * nx + x;
+                const double val = (double)__fadd_rn(Store16<ST>::to_f(f[v]), cp[v]);
+                sum += val;
+                mn = fmin(mn, val);
+                mx = fmax(mx, val);
+            }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_v[0][warp] = sum;
+        s_v[1][warp] = mn;
+        s_v[2][warp] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, lo = 1e300, hi = 0.0;
+        for (int w = 0; w < 4; ++w) {
+            a += s_v[0][w];
+            lo = fmin(lo, s_v[1][w]);
+            hi = fmax(hi, s_v[2][w]);
+        }
+        atomicAdd(&out[k].field_mass[field], a);
+        atomicMin(reinterpret_cast<unsigned long long*>(&out[k].field_min[field]), (unsigned long long)__double_as_longlong(lo));
+        atomicMax(reinterpret_cast<unsigned long long*>(&out[k].field_max[field]), (unsigned long long)__double_as_longlong(hi));
+    }
+}
+
+void launch_substep_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
+                            const FieldStep* steps, int field, int n_fields, const unsigned char* fpar, int sub,
+                            void* fa, void* fb, cudaStream_t s) {
+    if (n_tiles == 0) return;
+    unsigned short* a = static_cast<unsigned short*>(fa);
+    unsigned short* c = static_cast<unsigned short*>(fb);
+    if (storage == OLC_FIELD_BF16)
+        k_substep_batch16<OLC_FIELD_BF16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a, c);
+    else
+        k_substep_batch16<OLC_FIELD_F16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a, c);
+}
+
+void launch_react_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
+                          const FieldStep* steps, int field, int n_fields, const unsigned char* fpar, void* fa,
+                          void* fb, float* sink, float* comp, cudaStream_t s) {
+    if (n_tiles == 0) return;
+    unsigned short* a = static_cast<unsigned short*>(fa);
+    unsigned short* c = static_cast<unsigned short*>(fb);
+    if (storage == OLC_FIELD_BF16)
+        k_react_batch16<OLC_FIELD_BF16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, a, c,
+                                                                 sink, comp);
+    else
+        k_react_batch16<OLC_FIELD_F16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, a, c,
+                                                                sink, comp);
+}
+
+void launch_reduce_field_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles, int field,
+                                 int n_fields, const unsigned char* fpar, const void* fa, const void* fb,
+                                 const float* comp, OlcReductions* out, cudaStream_t s) {
+    if (n_tiles == 0) return;
+    const unsigned short* a = static_cast<const unsigned short*>(fa);
+    const unsigned short* c = static_cast<const unsigned short*>(fb);
+    if (storage == OLC_FIELD_BF16)
+        k_reduce_field_batch16<OLC_FIELD_BF16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, field, n_fields, fpar, a, c,
+                                                                        comp, out);
+    else
+        k_reduce_field_batch16<OLC_FIELD_F16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, field, n_fields, fpar, a, c,
+                                                                       comp, out);
 }
 
 // ------------------------------------------------------------------ reductions

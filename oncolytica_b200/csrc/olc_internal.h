@@ -223,5 +223,14 @@ void launch_reduce_field_batch(const BatchArgs& b, const uint4* tiles, olc_u32 n
                                const unsigned char* fpar, const float* fa, const float* fb, OlcReductions* out,
                                cudaStream_t s);
 void launch_reset_reductions_batch(OlcReductions* out, olc_u32 n_sims, cudaStream_t s);
+void launch_substep_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
+                            const FieldStep* steps, int field, int n_fields, const unsigned char* fpar, int sub,
+                            void* fa, void* fb, cudaStream_t s);
+void launch_react_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
+                          const FieldStep* steps, int field, int n_fields, const unsigned char* fpar, void* fa,
+                          void* fb, float* sink, float* comp, cudaStream_t s);
+void launch_reduce_field_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles, int field,
+                                 int n_fields, const unsigned char* fpar, const void* fa, const void* fb,
+                                 const float* comp, OlcReductions* out, cudaStream_t s);
 
 }  // namespace olc

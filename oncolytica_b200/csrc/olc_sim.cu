@@ -228,6 +228,7 @@ OlcRuleParams make_rule_params(OlcSim* s, int rule_index, int in_buf) {
         for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
             P.field[f] = s->field[0][f];
             P.field_alt[f] = s->field[1][f];
+            P.field_type[f] = s->fstep[f].storage;
         }
         P.fpar = s->fpar_dev;
         P.n_fields = (int)s->caps.n_fields;
@@ -428,7 +429,15 @@ int step_once_batch(OlcSim* s, int collect, cudaStream_t st) {
     mark(s, 0, st);
     // 1. fields: sinks, then every field's substeps over the simulations that take them
     for (olc_u32 f = 0; f < F; ++f) {
-        if (!s->field_bound[f] || !s->sink[f]) continue;
+        if (!s->field_bound[f]) continue;
+        const int stor = s->fstep[f].storage;
+        if (stor != OLC_FIELD_F32) {
+            launch_react_batch16(B, stor, s->btiles_all, s->n_btiles, s->bsteps_dev, (int)f, (int)F, s->fpar_dev,
+                                 s->field[0][f], s->field[1][f], s->sink[f], s->comp[f], st);
+            ++launches;
+            continue;
+        }
+        if (!s->sink[f]) continue;
         launch_sink_batch(B, s->btiles_all, s->n_btiles, s->bsteps_dev, (int)f, (int)F, s->fpar_dev, s->field[0][f],
                           s->field[1][f], s->sink[f], st);
         ++launches;
@@ -437,9 +446,14 @@ int step_once_batch(OlcSim* s, int collect, cudaStream_t st) {
     for (olc_u32 f = 0; f < F; ++f) {
         if (!s->field_bound[f]) continue;
         const std::vector<olc_u32>& cnt = s->btile_count[f];
+        const int stor = s->fstep[f].storage;
         for (size_t sub = 0; sub < cnt.size(); ++sub) {
-            launch_substep_batch(B, s->btiles_field[f], cnt[sub], s->bsteps_dev, (int)f, (int)F, s->fpar_dev, (int)sub,
-                                 s->field[0][f], s->field[1][f], st);
+            if (stor != OLC_FIELD_F32)
+                launch_substep_batch16(B, stor, s->btiles_field[f], cnt[sub], s->bsteps_dev, (int)f, (int)F,
+                                       s->fpar_dev, (int)sub, s->field[0][f], s->field[1][f], st);
+            else
+                launch_substep_batch(B, s->btiles_field[f], cnt[sub], s->bsteps_dev, (int)f, (int)F, s->fpar_dev,
+                                     (int)sub, s->field[0][f], s->field[1][f], st);
             ++launches;
         }
         substeps += (uint32_t)cnt.size();
@@ -515,8 +529,13 @@ int step_once_batch(OlcSim* s, int collect, cudaStream_t st) {
         launches += 3;
         for (olc_u32 f = 0; f < F; ++f) {
             if (!s->field_bound[f]) continue;
-            launch_reduce_field_batch(B, s->btiles_all, s->n_btiles, (int)f, (int)F, s->fpar_dev, s->field[0][f],
-                                      s->field[1][f], s->red_batch_dev, st);
+            if (s->fstep[f].storage != OLC_FIELD_F32)
+                launch_reduce_field_batch16(B, s->fstep[f].storage, s->btiles_all, s->n_btiles, (int)f, (int)F,
+                                            s->fpar_dev, s->field[0][f], s->field[1][f], s->comp[f], s->red_batch_dev,
+                                            st);
+            else
+                launch_reduce_field_batch(B, s->btiles_all, s->n_btiles, (int)f, (int)F, s->fpar_dev, s->field[0][f],
+                                          s->field[1][f], s->red_batch_dev, st);
             ++launches;
         }
         if (s->metrics_dev && s->metrics_bytes) {
@@ -1208,20 +1227,29 @@ int olc_read_user_metrics(OlcSim* s, void* out, size_t bytes, void* stream) {
 
 // ------------------------------------------------------------------ batched mode
 
-int olc_bind_field_batch(OlcSim* s, int index, float* a, float* b, float* sink, const OlcDiffusion* specs) {
+int olc_bind_field_batch(OlcSim* s, int index, void* a_, void* b_, float* sink, float* comp,
+                         const OlcDiffusion* specs) {
+    float* a = static_cast<float*>(a_);
+    float* b = static_cast<float*>(b_);
     if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
     if (!s->n_sims) return fail(s, OLC_ERR_STATE, "olc_bind_field_batch: not a batch handle");
     if (index < 0 || index >= (int)s->caps.n_fields || !a || !b || !specs)
         return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: bad index or null argument");
     const olc_u32 F = s->caps.n_fields;
+    const int storage = specs[0].storage;
+    for (olc_u32 k = 0; k < s->n_sims; ++k)
+        if (specs[k].storage != storage)
+            return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: every member stores a field with the same type");
+    if (storage != OLC_FIELD_F32 && !comp)
+        return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: 16-bit storage needs a compensation buffer");
     bool any_sink = false;
     std::vector<std::pair<int, olc_u32>> order;  // (substeps, simulation)
     for (olc_u32 k = 0; k < s->n_sims; ++k) {
         const OlcDiffusion& spec = specs[k];
         const OlcGeom& g = s->geoms[k];
-        if (g.chem_dims[0] % 4 != 0)
+        if (g.chem_dims[0] % (storage == OLC_FIELD_F32 ? 4 : 8) != 0)
             return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: simulation " + std::to_string(k) +
-                                            ": field x extent must be a multiple of 4");
+                                            ": field x extent must be a multiple of 4 (8 for 16-bit storage)");
         FieldStep fs = {};
         std::string err;
         if (spec.substeps != 0 && !make_field_step(spec, g.chem_dims, g.chem_voxel_size, s->caps.dt, &fs, &err))
@@ -1229,6 +1257,7 @@ int olc_bind_field_batch(OlcSim* s, int index, float* a, float* b, float* sink, 
         if (spec.substeps == 0) {
             for (int i = 0; i < 3; ++i) fs.dims[i] = g.chem_dims[i];
             fs.substeps = 0;
+            fs.storage = storage;
         }
         any_sink = any_sink || (spec.has_sink && spec.substeps != 0);
         s->bsteps_host[(size_t)k * F + index] = fs;
@@ -1277,6 +1306,8 @@ int olc_bind_field_batch(OlcSim* s, int index, float* a, float* b, float* sink, 
     s->field[0][index] = a;
     s->field[1][index] = b;
     s->sink[index] = any_sink ? sink : nullptr;
+    s->comp[index] = storage != OLC_FIELD_F32 ? comp : nullptr;
+    s->fstep[index].storage = storage;
     s->fspec[index] = specs[0];
     s->field_cur[index] = 0;
     s->field_bound[index] = true;

@@ -30,6 +30,10 @@ class DiffusionSpec:
     decay: float = 0.0
     boundary: float = 0.0
     substeps: Optional[int] = None
+    storage: str = "f32"   # "f32", "bf16" or "f16": element type of the field buffers
+
+
+STORAGE_CODES = {"f32": 0, "bf16": 1, "f16": 2}
 
 
 @dataclass
@@ -150,12 +154,18 @@ class Engine:
         self.chemistry = Grid(chemistry_class, self.chemistry_shape, self)
 
     def setup_diffusion(self, field: str, diffusion: float, decay: float = 0.0, boundary: float = 0.0,
-                        substeps: Optional[int] = None) -> None:
+                        substeps: Optional[int] = None, storage: str = "f32") -> None:
         """Built-in diffusion of one chemistry field: per step an implicit sink
         (rates deposited with ``self.sink_at(pos).field += k``), then S explicit
         7-point substeps with the outer faces pinned to ``boundary``
-        (engine tumor_sim.wgsl:387-446; substeps as chemistry_rule(iterations=S))."""
-        self._diffusion[field] = DiffusionSpec(float(diffusion), float(decay), float(boundary), substeps)
+        (engine tumor_sim.wgsl:387-446; substeps as chemistry_rule(iterations=S)).
+        ``storage`` "bf16" or "f16" keeps the field in 16 bits: updates run in
+        FP32, and uptake and decay are applied once per step with a per-voxel
+        FP32 rounding residual carried to the next step (no counterpart in the
+        reference, whose fields are FP32)."""
+        if storage not in STORAGE_CODES:
+            raise ValueError(f"storage must be one of {sorted(STORAGE_CODES)}, got {storage!r}")
+        self._diffusion[field] = DiffusionSpec(float(diffusion), float(decay), float(boundary), substeps, storage)
 
     def setup_contact(self, radius: str | float = "radius", stiffness: float = 1.0, mobility: float = 10.0,
                       max_disp: float = 1.0, margin: float = 0.1) -> None:

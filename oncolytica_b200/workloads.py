@@ -184,6 +184,7 @@ class TumourSpec:
     seed: int = 0
     capacity: int = 0
     tissue_dims: tuple = field(default=())
+    storage: str = "f32"      # field storage: "f32", "bf16" or "f16"
 
     def __post_init__(self) -> None:
         if not self.tissue_dims:
@@ -319,11 +320,11 @@ def configure_engine(spec: TumourSpec, state: dict | None = None) -> tuple[Engin
     chem_cls = O2DrugChem if spec.has_drug else O2Chem
     eng.setup_chemistry(chem_cls, shape=tuple(spec.field_dims), voxel_size=spec.dx)
     eng.chemistry.column("o2")[...] = spec.init_o2
-    eng.setup_diffusion("o2", diffusion=spec.D_o2, boundary=spec.bnd_o2, substeps=spec.S_o2)
+    eng.setup_diffusion("o2", diffusion=spec.D_o2, boundary=spec.bnd_o2, substeps=spec.S_o2, storage=spec.storage)
     if spec.has_drug:
         eng.chemistry.column("drug")[...] = spec.init_drug
         eng.setup_diffusion("drug", diffusion=spec.D_drug, decay=spec.decay_drug, boundary=spec.bnd_drug,
-                            substeps=spec.S_drug)
+                            substeps=spec.S_drug, storage=spec.storage)
     eng.setup_contact(radius="radius", stiffness=spec.stiffness, mobility=spec.mobility, max_disp=spec.max_disp,
                       margin=spec.margin)
     eng.cells.add_arrays(TumourCell, **{"pos.x": state["x"], "pos.y": state["y"], "pos.z": state["z"],

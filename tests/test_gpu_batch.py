@@ -12,10 +12,10 @@ from oncolytica_b200._types import metric_fields
 pytestmark = pytest.mark.gpu
 
 
-def _members():
+def _members(storage="f32"):
     """Four uneven members: different grids, agent counts, diffusion, uptake,
     death rates and seeds (substep counts differ, odd and even)."""
-    base = dict(r_lo=4.0, r_hi=6.0, has_drug=True, v_lo=1.85, v_hi=2.0)
+    base = dict(r_lo=4.0, r_hi=6.0, has_drug=True, v_lo=1.85, v_hi=2.0, storage=storage)
     return [
         W.TumourSpec(name="m0", n_agents=1500, domain=128.0, ball_radius=45.0, field_dims=(32, 32, 32),
                      D_o2=1500.0, uptake=0.6, death_k=0.3, seed=11, init_drug=0.3, **base),
@@ -33,9 +33,9 @@ def _metrics(eng):
     return {k: getattr(m, k) for k in metric_fields(type(m))}
 
 
-@pytest.mark.parametrize("graphs", [False, True])
-def test_batch_members_match_solo_runs(cuda, graphs):
-    specs = _members()
+@pytest.mark.parametrize("graphs,storage", [(False, "f32"), (True, "f32"), (True, "bf16"), (False, "f16")])
+def test_batch_members_match_solo_runs(cuda, graphs, storage):
+    specs = _members(storage)
     assert len({s.S_o2 % 2 for s in specs}) == 2  # odd and even substep counts
     states = [W.initial_state(s) for s in specs]
     solos = [W.build_engine(s, st) for s, st in zip(specs, states)]
@@ -55,6 +55,9 @@ def test_batch_members_match_solo_runs(cuda, graphs):
                 np.testing.assert_array_equal(a["cols"][col], b["cols"][col], err_msg=f"{col} step {step} member {k}")
             for f in a["fields"]:
                 np.testing.assert_array_equal(a["fields"][f], b["fields"][f], err_msg=f"{f} step {step} member {k}")
+            for f in a.get("residuals", {}):
+                np.testing.assert_array_equal(a["residuals"][f], b["residuals"][f], err_msg=f"{f} residual {step} {k}")
+            assert ("residuals" in a) == (storage != "f32")
         if collect:
             reds = batch.get_reductions()
             for k, e in enumerate(solos):

@@ -384,3 +384,48 @@ def test_graph_steps_match_eager_steps(cuda):
             ma, mb = (e.get_metrics() for e in engines)
             assert {k: getattr(ma, k) for k in metric_fields(type(ma))} == \
                    {k: getattr(mb, k) for k in metric_fields(type(mb))}
+
+
+@pytest.mark.parametrize("storage,code", [("bf16", 1), ("f16", 2)])
+def test_tumour_step_parity_16bit_fields(cuda, storage, code):
+    """16-bit field storage through the engine: each step from an identical
+    state gives the oracle's field bits and residuals (reaction + substeps,
+    oracle.diffuse16), and the agent phase, run by the oracle on those field
+    values, gives the same agents, life flags and uptake sink."""
+    import oracle
+
+    spec = W.scaled(_parity_spec(), storage=storage)
+    eng = W.build_engine(spec)
+    x = (np.arange(spec.field_dims[0], dtype=np.float32) + 0.5) / spec.field_dims[0]
+    eng.chemistry.column("o2")[...] = np.clip(2.2 * x - 0.6, 0.0, 1.0)[:, None, None]
+    eng.sync_to_device()
+    be = eng._backend_impl
+    shp = tuple(spec.field_dims[::-1])
+    for step in range(4):
+        snap = be.snapshot()
+        o2_bits, o2_res = oracle.diffuse16(snap["fields"]["o2"].reshape(shp), snap["sinks"]["o2"].reshape(shp),
+                                           snap["residuals"]["o2"].reshape(shp), spec.dx, spec.dt, spec.D_o2, 0.0,
+                                           spec.bnd_o2, spec.S_o2, code)
+        dr_bits, dr_res = oracle.diffuse16(snap["fields"]["drug"].reshape(shp), None,
+                                           snap["residuals"]["drug"].reshape(shp), spec.dx, spec.dt, spec.D_drug,
+                                           spec.decay_drug, spec.bnd_drug, spec.S_drug, code)
+        fsnap = dict(snap)
+        fsnap["fields"] = {"o2": oracle.from_bits16(o2_bits, code).ravel(),
+                           "drug": oracle.from_bits16(dr_bits, code).ravel()}
+        fsnap["sinks"] = {"o2": np.zeros(int(np.prod(shp)), np.float32)}
+        orc = oracle.TumourOracle.from_snapshot(spec, fsnap, spec.capacity)
+        orc.agents_part(nthreads=4)
+        eng.run_step()
+        got = be.snapshot()
+        np.testing.assert_array_equal(got["fields"]["o2"], o2_bits.ravel(), err_msg=f"o2 bits step {step}")
+        np.testing.assert_array_equal(got["residuals"]["o2"], o2_res.ravel(), err_msg=f"o2 residual step {step}")
+        np.testing.assert_array_equal(got["fields"]["drug"], dr_bits.ravel(), err_msg=f"drug bits step {step}")
+        np.testing.assert_array_equal(got["residuals"]["drug"], dr_res.ravel())
+        n = got["rows"]
+        assert n == orc.rows, step
+        np.testing.assert_array_equal(got["life"], orc.dead[:n])
+        for col, key in (("state", "state"), ("_rng_state", "rng"), ("volume", "volume"), ("radius", "radius")):
+            np.testing.assert_array_equal(got["cols"][col], orc.bufs[key][:n], err_msg=f"{col} step {step}")
+        for a, key in (("pos.x", "x"), ("pos.y", "y"), ("pos.z", "z")):
+            np.testing.assert_allclose(got["cols"][a], orc.bufs[key][:n], rtol=0, atol=1e-4)
+        np.testing.assert_array_equal(got["sinks"]["o2"], orc.o2_sink.ravel())
