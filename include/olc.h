@@ -103,9 +103,16 @@ typedef struct {
  * rounds to nearest even; uptake and decay are applied once per step in FP32
  * with the rounding residual kept in a caller-provided FP32 compensation
  * buffer (olc_bind_field_ex).  No counterpart in the reference (FP32 textures). */
-#define OLC_FIELD_F32  0
-#define OLC_FIELD_BF16 1
-#define OLC_FIELD_F16  2
+#define OLC_FIELD_F32     0
+#define OLC_FIELD_BF16    1
+#define OLC_FIELD_F16     2
+/* BF16 whose substeps round stochastically instead of to nearest: a voxel's
+ * result rounds up with probability equal to the discarded fraction, using
+ * hash bits of (voxel, step, substep, field), so runs are reproducible.  With
+ * 8 mantissa bits, round-to-nearest loses the small per-substep diffusion
+ * increments (the field stalls); stochastic rounding keeps them in
+ * expectation. */
+#define OLC_FIELD_BF16_SR 3
 
 /* Hertz-like contact repulsion (engine/assets/shaders/tumor_sim.wgsl:505-628):
  * for d < r_i + r_j, F += k * delta^(3/2) * (p_i - p_j)/d with
@@ -353,9 +360,10 @@ int olc_stage_diffuse(float* f_dev, float* tmp_dev, float* sink_dev, const int32
 
 /* One step of one 16-bit field (reaction with compensation, then S
  * substeps), result in f_dev; f_dev, tmp_dev hold BF16/FP16 elements, comp_dev
- * the FP32 residuals. */
+ * the FP32 residuals; `step` and `field` salt stochastic rounding (the step
+ * loop of a handle uses its step count and the field's index). */
 int olc_stage_diffuse16(void* f_dev, void* tmp_dev, float* sink_dev, float* comp_dev, const int32_t dims[3],
-                        float dx, float dt, const OlcDiffusion* spec, void* stream);
+                        float dx, float dt, const OlcDiffusion* spec, uint32_t step, int field, void* stream);
 
 /* Contact pass over n sorted agents: posr_dev holds (x, y, z, radius) with
  * radius < 0 marking a dead agent; writes the new positions. */

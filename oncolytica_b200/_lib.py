@@ -167,7 +167,7 @@ _SIGS = {
     "olc_bind_field_batch": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, _VP, C.POINTER(OlcDiffusion)]),
     "olc_bind_field_ex": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, _VP, C.POINTER(OlcDiffusion)]),
     "olc_stage_diffuse16": (C.c_int, [_VP, _VP, _VP, _VP, C.POINTER(C.c_int32 * 3), C.c_float, C.c_float,
-                                      C.POINTER(OlcDiffusion), _VP]),
+                                      C.POINTER(OlcDiffusion), C.c_uint32, C.c_int, _VP]),
     "olc_set_params_batch": (C.c_int, [_VP, _VP, C.c_size_t, _VP]),
     "olc_read_field_parity": (C.c_int, [_VP, C.POINTER(C.c_uint8), _VP]),
     "olc_read_reductions_batch": (C.c_int, [_VP, C.POINTER(OlcReductions), _VP]),

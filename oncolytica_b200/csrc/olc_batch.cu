@@ -334,7 +334,8 @@ __global__ void __launch_bounds__(128) k_substep_batch16(const uint4* __restrict
                                                          const OlcSimDesc* __restrict__ sims,
                                                          const FieldStep* __restrict__ steps, int field, int n_fields,
                                                          const unsigned char* __restrict__ fpar, int sub,
-                                                         unsigned short* fa, unsigned short* fb) {
+                                                         unsigned short* fa, unsigned short* fb,
+                                                         const olc_u32* step_ctr) {
     const uint4 t = tiles[blockIdx.x];
     const olc_u32 k = t.x;
     const OlcSimDesc& d = sims[k];
@@ -351,6 +352,7 @@ __global__ void __launch_bounds__(128) k_substep_batch16(const uint4* __restrict
     const bool edge_y = y == 0 || y == ny - 1;
     const bool ex0 = x == 0, ex3 = x + 3 == nx - 1;
     const float bf = Store16<ST>::to_f(Store16<ST>::from_f(fs.bval));
+    const olc_u32 key = olc_sr_key(*step_ctr, sub, field);
     const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     size_t idx = (size_t)z0 * sz + (size_t)y * sy + x;
     float4 zm = z0 > 0 ? load4<ST>(in + idx - sz) : zero;
@@ -369,7 +371,7 @@ __global__ void __launch_bounds__(128) k_substep_batch16(const uint4* __restrict
             if (ex0) v.x = bf;
             if (ex3) v.w = bf;
         }
-        store4<ST>(out + idx, v);
+        store4_at<ST>(out + idx, v, idx, key);
         zm = c;
         c = zp;
     }
@@ -469,14 +471,19 @@ __global__ void __launch_bounds__(128) k_reduce_field_batch16(const uint4* __res
 
 void launch_substep_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
                             const FieldStep* steps, int field, int n_fields, const unsigned char* fpar, int sub,
-                            void* fa, void* fb, cudaStream_t s) {
+                            void* fa, void* fb, const olc_u32* step_ctr, cudaStream_t s) {
     if (n_tiles == 0) return;
     unsigned short* a = static_cast<unsigned short*>(fa);
     unsigned short* c = static_cast<unsigned short*>(fb);
     if (storage == OLC_FIELD_BF16)
-        k_substep_batch16<OLC_FIELD_BF16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a, c);
+        k_substep_batch16<OLC_FIELD_BF16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a, c,
+                                                                   step_ctr);
+    else if (storage == OLC_FIELD_BF16_SR)
+        k_substep_batch16<OLC_FIELD_BF16_SR><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a,
+                                                                      c, step_ctr);
     else
-        k_substep_batch16<OLC_FIELD_F16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a, c);
+        k_substep_batch16<OLC_FIELD_F16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a, c,
+                                                                  step_ctr);
 }
 
 void launch_react_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
@@ -485,7 +492,7 @@ void launch_react_batch16(const BatchArgs& b, int storage, const uint4* tiles, o
     if (n_tiles == 0) return;
     unsigned short* a = static_cast<unsigned short*>(fa);
     unsigned short* c = static_cast<unsigned short*>(fb);
-    if (storage == OLC_FIELD_BF16)
+    if (storage != OLC_FIELD_F16)
         k_react_batch16<OLC_FIELD_BF16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, a, c,
                                                                  sink, comp);
     else
@@ -499,7 +506,7 @@ void launch_reduce_field_batch16(const BatchArgs& b, int storage, const uint4* t
     if (n_tiles == 0) return;
     const unsigned short* a = static_cast<const unsigned short*>(fa);
     const unsigned short* c = static_cast<const unsigned short*>(fb);
-    if (storage == OLC_FIELD_BF16)
+    if (storage != OLC_FIELD_F16)
         k_reduce_field_batch16<OLC_FIELD_BF16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, field, n_fields, fpar, a, c,
                                                                         comp, out);
     else

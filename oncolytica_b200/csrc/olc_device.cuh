@@ -46,6 +46,14 @@ __device__ __forceinline__ float3 olc_rand_dir(olc_u32& s) {
     return make_float3(__fmul_rn(rxy, cosf(phi)), __fmul_rn(rxy, sinf(phi)), z);
 }
 
+// MurmurHash3's 32-bit finaliser (fmix32), a published integer mixer.
+__device__ __host__ __forceinline__ olc_u32 olc_fmix32(olc_u32 h) {
+    h ^= h >> 16; h *= 0x85EBCA6Bu;
+    h ^= h >> 13; h *= 0xC2B2AE35u;
+    h ^= h >> 16;
+    return h;
+}
+
 // Initial per-agent RNG state: MurmurHash3's 32-bit finaliser (fmix32, a
 // published integer mixer) of seed*golden + index, forced odd so it is never
 // the xorshift fixed point 0.

@@ -7,7 +7,9 @@
 //                      f = round16(v);  comp = v - f          (FP32, RN-even)
 //   diffusion (S substeps): c' = round16(max(c + r (S6 - 6 c), 0)) with the
 //                      sum S6 = ((xm + xp) + (ym + yp)) + (zm + zp) in FP32;
-//                      outer faces pinned to round16(boundary).
+//                      outer faces pinned to round16(boundary); round16 is to
+//                      nearest even, or stochastic for OLC_FIELD_BF16_SR
+//                      (hash bits of voxel, step, substep and field).
 // comp carries each voxel's rounding residual of the reaction into the next
 // step (compensated summation), so small uptake and decay terms are not lost
 // to the 8- or 11-bit mantissa.  The substeps round every result; their
@@ -76,7 +78,7 @@ void launch_react16(void* f, float* sink, float* comp, const FieldStep& fs, cuda
     const size_t nvox = (size_t)fs.dims[0] * fs.dims[1] * fs.dims[2];
     size_t blocks = (nvox + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    if (fs.storage == OLC_FIELD_BF16)
+    if (fs.storage != OLC_FIELD_F16)
         k_react16<OLC_FIELD_BF16><<<(unsigned)blocks, 256, 0, s>>>(static_cast<unsigned short*>(f), sink, comp,
                                                                     fs.dims[0], fs.dims[1], fs.dims[2], fs.sink_dt,
                                                                     fs.decay_step);
@@ -102,7 +104,9 @@ constexpr size_t SMEM = BYTES + 16 + 128;
 template <int ST>
 __global__ void __launch_bounds__(16 * t16::TYR) k_substep16(const __grid_constant__ CUtensorMap in_map,
                                                             unsigned short* __restrict__ out, int nx, int ny, int nz,
-                                                            float r, float bval, olc_u32* status, int rev) {
+                                                            float r, float bval, olc_u32* status, int rev,
+                                                            const olc_u32* step_ctr, olc_u32 step_host, int sub,
+                                                            int field) {
     using namespace t16;
     extern __shared__ unsigned char t16_raw[];
     const olc_u32 pad = (128u - (smem_addr(t16_raw) & 127u)) & 127u;
@@ -153,6 +157,8 @@ __global__ void __launch_bounds__(16 * t16::TYR) k_substep16(const __grid_consta
     const size_t sz = (size_t)nx * ny;
     unsigned short* o = out + (size_t)z0 * sz + (size_t)y * nx + x;
     const float bf = Store16<ST>::to_f(Store16<ST>::from_f(bval));  // the face value as stored
+    const olc_u32 key = olc_sr_key(step_ctr ? *step_ctr : step_host, sub, field);
+    unsigned long long vi = (unsigned long long)z0 * sz + (unsigned long long)y * nx + x;
 #pragma unroll 4
     for (int lz = 1; lz <= TZ; ++lz) {
         const int z = z0 + lz - 1;
@@ -173,8 +179,9 @@ __global__ void __launch_bounds__(16 * t16::TYR) k_substep16(const __grid_consta
             if (ex0) v.x = bf;
             if (ex3) v.w = bf;
         }
-        store4<ST>(o, v);
+        store4_at<ST>(o, v, vi, key);
         o += sz;
+        vi += sz;
         zm = c;
         c = zp;
     }
@@ -191,7 +198,7 @@ bool make_field_maps16(FieldMaps16* m, void* a, void* b, const int dims[3]) {
 
 template <int ST>
 static void launch_sub16(const CUtensorMap& map, void* out, const FieldStep& fs, olc_u32* status, int rev,
-                         cudaStream_t s) {
+                         const olc_u32* step_ctr, olc_u32 step_host, int sub, int field, cudaStream_t s) {
     using namespace t16;
     static int configured_mask = 0;
     int dev = 0;
@@ -211,20 +218,23 @@ static void launch_sub16(const CUtensorMap& map, void* out, const FieldStep& fs,
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cudaLaunchKernelEx(&cfg, k_substep16<ST>, map, static_cast<unsigned short*>(out), fs.dims[0], fs.dims[1],
-                       fs.dims[2], fs.r, fs.bval, status, rev);
+                       fs.dims[2], fs.r, fs.bval, status, rev, step_ctr, step_host, sub, field);
 }
 
 void* run_substeps16(void* a, void* b, const FieldMaps16& m, int a_index, const FieldStep& fs, olc_u32* status,
-                     cudaStream_t s) {
+                     const olc_u32* step_ctr, olc_u32 step_host, int field, cudaStream_t s) {
     void* bufs[2];
     bufs[a_index] = a;
     bufs[1 - a_index] = b;
     int cur = a_index;
     for (int i = 0; i < fs.substeps; ++i) {
         if (fs.storage == OLC_FIELD_BF16)
-            launch_sub16<OLC_FIELD_BF16>(m.map[cur], bufs[1 - cur], fs, status, i & 1, s);
+            launch_sub16<OLC_FIELD_BF16>(m.map[cur], bufs[1 - cur], fs, status, i & 1, step_ctr, step_host, i, field, s);
+        else if (fs.storage == OLC_FIELD_BF16_SR)
+            launch_sub16<OLC_FIELD_BF16_SR>(m.map[cur], bufs[1 - cur], fs, status, i & 1, step_ctr, step_host, i,
+                                            field, s);
         else
-            launch_sub16<OLC_FIELD_F16>(m.map[cur], bufs[1 - cur], fs, status, i & 1, s);
+            launch_sub16<OLC_FIELD_F16>(m.map[cur], bufs[1 - cur], fs, status, i & 1, step_ctr, step_host, i, field, s);
         cur = 1 - cur;
     }
     return bufs[cur];
@@ -292,7 +302,7 @@ void launch_reduce_field16(const void* f, const float* comp, const FieldStep& fs
     double* part = rs.partials + (size_t)(4 + slot) * RED_MAX_BLOCKS;
     olc_u32* ticket = rs.tickets + 1 + slot;
     const unsigned short* p = static_cast<const unsigned short*>(f);
-    if (fs.storage == OLC_FIELD_BF16)
+    if (fs.storage != OLC_FIELD_F16)
         k_reduce_field16<OLC_FIELD_BF16><<<(unsigned)blocks, 256, 0, s>>>(p, comp, nvox, slot, out, part, ticket);
     else
         k_reduce_field16<OLC_FIELD_F16><<<(unsigned)blocks, 256, 0, s>>>(p, comp, nvox, slot, out, part, ticket);

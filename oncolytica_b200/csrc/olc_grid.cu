@@ -151,6 +151,7 @@ __global__ void __launch_bounds__(256) k_scan_hist(const olc_u32* __restrict__ h
         *reinterpret_cast<unsigned long long*>(counters + OLC_CTR_AGENT_STEPS) += (unsigned long long)(rows - dead);
         counters[OLC_CTR_DEAD] = dead;
         counters[OLC_CTR_DEAD_TMP] = 0u;
+        counters[OLC_CTR_FIELD_STEP] += 1u;
         for (int j = 0; j < OLC_MAX_RULE_KERNELS; ++j) {
             counters[OLC_CTR_BIRTHS + j] = 0u;
             counters[OLC_CTR_RULE_TILE + j] = 0u;

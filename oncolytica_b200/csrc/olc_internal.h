@@ -149,8 +149,9 @@ struct FieldMaps16 {
 bool make_field_maps16(FieldMaps16* m, void* a, void* b, const int dims[3]);
 void launch_react16(void* f, float* sink, float* comp, const FieldStep& fs, cudaStream_t s);
 // Runs fs.substeps substeps from buffer a_index of (a, b); returns the buffer holding the result.
+// step_ctr (device, else step_host) and field salt stochastic rounding.
 void* run_substeps16(void* a, void* b, const FieldMaps16& m, int a_index, const FieldStep& fs, olc_u32* status,
-                     cudaStream_t s);
+                     const olc_u32* step_ctr, olc_u32 step_host, int field, cudaStream_t s);
 
 olc_u32* stage_status_word();
 
@@ -225,7 +226,7 @@ void launch_reduce_field_batch(const BatchArgs& b, const uint4* tiles, olc_u32 n
 void launch_reset_reductions_batch(OlcReductions* out, olc_u32 n_sims, cudaStream_t s);
 void launch_substep_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
                             const FieldStep* steps, int field, int n_fields, const unsigned char* fpar, int sub,
-                            void* fa, void* fb, cudaStream_t s);
+                            void* fa, void* fb, const olc_u32* step_ctr, cudaStream_t s);
 void launch_react_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
                           const FieldStep* steps, int field, int n_fields, const unsigned char* fpar, void* fa,
                           void* fb, float* sink, float* comp, cudaStream_t s);

@@ -26,6 +26,7 @@
 #define OLC_CTR_STATUS     2    // sticky OLC_ST_* bits
 #define OLC_CTR_DEAD_TMP   3    // dead rows counted by the key kernel
 #define OLC_CTR_ROWS       4    // rows entering this step's sort (live + dead)
+#define OLC_CTR_FIELD_STEP 5    // steps whose grid stage has run (salt of stochastic rounding)
 #define OLC_CTR_SORT_TILE  8    // 4 words: tile counters of the sort passes
 #define OLC_CTR_RULE_TILE  12   // OLC_MAX_RULE_KERNELS words: tile counters
 #define OLC_CTR_BIRTHS     28   // OLC_MAX_RULE_KERNELS words: births per rule

@@ -290,7 +290,7 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
         int cur = s->field_cur[f];
         if (s->fstep[f].storage != OLC_FIELD_F32) {
             void* res = run_substeps16(s->field[cur][f], s->field[1 - cur][f], s->fmaps16[f], cur, s->fstep[f],
-                                       s->counters + OLC_CTR_STATUS, st);
+                                       s->counters + OLC_CTR_STATUS, s->counters + OLC_CTR_FIELD_STEP, 0u, (int)f, st);
             s->field_cur[f] = (res == s->field[cur][f]) ? cur : 1 - cur;
             substeps += (uint32_t)s->fstep[f].substeps;
             launches += (uint64_t)s->fstep[f].substeps;
@@ -450,7 +450,8 @@ int step_once_batch(OlcSim* s, int collect, cudaStream_t st) {
         for (size_t sub = 0; sub < cnt.size(); ++sub) {
             if (stor != OLC_FIELD_F32)
                 launch_substep_batch16(B, stor, s->btiles_field[f], cnt[sub], s->bsteps_dev, (int)f, (int)F,
-                                       s->fpar_dev, (int)sub, s->field[0][f], s->field[1][f], st);
+                                       s->fpar_dev, (int)sub, s->field[0][f], s->field[1][f],
+                                       s->counters + OLC_CTR_FIELD_STEP, st);
             else
                 launch_substep_batch(B, s->btiles_field[f], cnt[sub], s->bsteps_dev, (int)f, (int)F, s->fpar_dev,
                                      (int)sub, s->field[0][f], s->field[1][f], st);
@@ -905,7 +906,7 @@ int olc_bind_field_ex(OlcSim* s, int index, void* a_, void* b_, float* sink, flo
         !make_field_step(*spec, s->geom.chem_dims, s->geom.chem_voxel_size, s->caps.dt, &fs, &err))
         return fail(s, OLC_ERR_ARG, "olc_bind_field: " + err);
     if (spec->substeps == 0) {
-        if (spec->storage < OLC_FIELD_F32 || spec->storage > OLC_FIELD_F16)
+        if (spec->storage < OLC_FIELD_F32 || spec->storage > OLC_FIELD_BF16_SR)
             return fail(s, OLC_ERR_ARG, "olc_bind_field: bad storage type");
         fs.storage = spec->storage;
     }
@@ -1101,7 +1102,9 @@ int olc_set_agent_count(OlcSim* s, uint32_t n, void* stream) {
     OLC_TRY(check(s, cudaMemcpy(words, s->counters, sizeof(words), cudaMemcpyDeviceToHost), "read counters"));
     const olc_u32 status = words[OLC_CTR_STATUS];
     const olc_u32 as_lo = words[OLC_CTR_AGENT_STEPS], as_hi = words[OLC_CTR_AGENT_STEPS + 1];
+    const olc_u32 fstep = words[OLC_CTR_FIELD_STEP];
     std::memset(words, 0, sizeof(words));
+    words[OLC_CTR_FIELD_STEP] = fstep;
     words[OLC_CTR_N] = n;
     words[OLC_CTR_ROWS] = n;
     words[OLC_CTR_STATUS] = status;
@@ -1457,11 +1460,11 @@ int olc_stage_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], 
 }
 
 int olc_stage_diffuse16(void* f, void* tmp, float* sink, float* comp, const int32_t dims[3], float dx, float dt,
-                        const OlcDiffusion* spec, void* stream) {
+                        const OlcDiffusion* spec, uint32_t step, int field, void* stream) {
     if (!f || !tmp || !comp || !dims || !spec)
         return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse16: null argument");
-    if (spec->storage != OLC_FIELD_BF16 && spec->storage != OLC_FIELD_F16)
-        return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse16: storage must be BF16 or FP16");
+    if (spec->storage != OLC_FIELD_BF16 && spec->storage != OLC_FIELD_F16 && spec->storage != OLC_FIELD_BF16_SR)
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse16: storage must be BF16, FP16 or BF16_SR");
     std::string err;
     FieldStep fs;
     if (!make_field_step(*spec, dims, dx, dt, &fs, &err))
@@ -1472,7 +1475,7 @@ int olc_stage_diffuse16(void* f, void* tmp, float* sink, float* comp, const int3
     if (!status || !make_field_maps16(&maps, f, tmp, dims))
         return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse16: TMA descriptors failed (16-byte aligned buffers)");
     launch_react16(f, spec->has_sink ? sink : nullptr, comp, fs, st);
-    void* res = run_substeps16(f, tmp, maps, 0, fs, status, st);
+    void* res = run_substeps16(f, tmp, maps, 0, fs, status, nullptr, step, field, st);
     if (res != f) {
         const size_t bytes = (size_t)dims[0] * dims[1] * dims[2] * 2;
         cudaMemcpyAsync(f, res, bytes, cudaMemcpyDeviceToDevice, st);

@@ -246,24 +246,43 @@ static uint16_t f_to_bf16(float f) { /* finite values: RN-even on the bit patter
     return (uint16_t)((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
 }
 static float h16_to_f(uint16_t h, int storage) {
-    if (storage == 1) return bf16_to_f(h);
+    if (storage == 1 || storage == 3) return bf16_to_f(h);
     _Float16 x;
     memcpy(&x, &h, 2);
     return (float)x;
 }
 static uint16_t f_to_h16(float f, int storage) {
-    if (storage == 1) return f_to_bf16(f);
+    if (storage == 1 || storage == 3) return f_to_bf16(f);
     _Float16 x = (_Float16)f;
     uint16_t h;
     memcpy(&h, &x, 2);
     return h;
 }
 
+/* Stochastic BF16 rounding of the substeps (storage 3): random bits of voxel
+ * v are fmix32(v * 0x9E3779B1 ^ key), key = fmix32((step << 8) ^ substep ^
+ * (field << 24)); the low 16 FP32 bits plus 16 random bits carry into the
+ * kept half with probability equal to the discarded fraction. */
+static uint32_t fmix32(uint32_t h) {
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= 0xC2B2AE35u;
+    h ^= h >> 16;
+    return h;
+}
+static uint16_t f_to_bf16_sr(float f, uint32_t rnd) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    return (uint16_t)((u + (rnd & 0xffffu)) >> 16);
+}
+
 int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const int32_t dims[3], float dx, float dt,
-                  float D, float decay, float boundary, int substeps, int storage, int nthreads) {
+                  float D, float decay, float boundary, int substeps, int storage, uint32_t step, int field,
+                  int nthreads) {
     const int nx = dims[0], ny = dims[1], nz = dims[2];
     const int nt = nthreads_or_all(nthreads);
-    if (substeps < 1 || (storage != 1 && storage != 2)) return -1;
+    if (substeps < 1 || storage < 1 || storage > 3) return -1;
     const float dts = dt / (float)substeps;
     const float r = D * dts / (dx * dx);
     if (r > 1.0f / 6.0f + 1e-7f) return -1;
@@ -288,6 +307,7 @@ int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const in
     uint16_t* cur = f;
     uint16_t* nxt = tmp;
     for (int s = 0; s < substeps; ++s) {
+        const uint32_t key = fmix32((step << 8) ^ (uint32_t)s ^ ((uint32_t)field << 24));
 #pragma omp parallel for num_threads(nt) schedule(static)
         for (int z = 0; z < nz; ++z)
             for (int y = 0; y < ny; ++y) {
@@ -303,7 +323,9 @@ int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const in
                                (h16_to_f(cur[v - sy], storage) + h16_to_f(cur[v + sy], storage));
                     float s2 = s1 + (h16_to_f(cur[v - sz], storage) + h16_to_f(cur[v + sz], storage));
                     float u = c + r * (s2 - 6.0f * c);
-                    nxt[v] = f_to_h16(u > 0.0f ? u : 0.0f, storage);
+                    u = u > 0.0f ? u : 0.0f;
+                    nxt[v] = storage == 3 ? f_to_bf16_sr(u, fmix32((uint32_t)v * 0x9E3779B1u ^ key))
+                                          : f_to_h16(u, storage);
                 }
             }
         uint16_t* t = cur;

@@ -50,7 +50,8 @@ void orc_bin_ranges(const uint32_t* keys, uint32_t n, uint32_t n_bins, uint32_t*
 int orc_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], float dx, float dt, float D,
                 float decay, float boundary, int substeps, int nthreads);
 int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const int32_t dims[3], float dx, float dt,
-                  float D, float decay, float boundary, int substeps, int storage, int nthreads);
+                  float D, float decay, float boundary, int substeps, int storage, uint32_t step, int field,
+                  int nthreads);
 int orc_diffuse_f64(double* f, double* tmp, const float* sink, const int32_t dims[3], double dx, double dt, double D,
                     double decay, double boundary, int substeps, int split, int nthreads);
 

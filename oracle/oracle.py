@@ -122,8 +122,8 @@ def diffuse(f: np.ndarray, sink: np.ndarray | None, dx: float, dt: float, D: flo
 
 
 def to_bits16(f: np.ndarray, storage: int) -> np.ndarray:
-    """float32 values -> BF16 (storage 1) or FP16 (storage 2) bit patterns,
-    rounded to nearest even (finite values)."""
+    """float32 values -> BF16 (storage 1 and 3) or FP16 (storage 2) bit
+    patterns, rounded to nearest even (finite values)."""
     f = np.ascontiguousarray(f, dtype=np.float32)
     if storage == 2:
         return f.astype(np.float16).view(np.uint16)
@@ -139,15 +139,18 @@ def from_bits16(h: np.ndarray, storage: int) -> np.ndarray:
 
 
 def diffuse16(bits: np.ndarray, sink: np.ndarray | None, comp: np.ndarray, dx: float, dt: float, D: float,
-              decay: float, boundary: float, substeps: int, storage: int, nthreads: int = 0):
-    """One step of a 16-bit field (indexed [z, y, x]): returns (bits, comp)."""
+              decay: float, boundary: float, substeps: int, storage: int, step: int = 0, field: int = 0,
+              nthreads: int = 0):
+    """One step of a 16-bit field (indexed [z, y, x]): returns (bits, comp).
+    ``step`` and ``field`` salt the stochastic rounding of storage 3."""
     f = np.ascontiguousarray(bits, dtype=np.uint16).copy()
     tmp = np.zeros_like(f)
     c = np.ascontiguousarray(comp, dtype=np.float32).copy()
     s = None if sink is None else np.ascontiguousarray(sink, dtype=np.float32).copy()
     dims = np.array([f.shape[2], f.shape[1], f.shape[0]], dtype=np.int32)
     rc = lib().orc_diffuse16(_p(f), _p(tmp), _p(s), _p(c), _p(dims), C.c_float(dx), C.c_float(dt), C.c_float(D),
-                             C.c_float(decay), C.c_float(boundary), substeps, storage, nthreads)
+                             C.c_float(decay), C.c_float(boundary), substeps, storage, C.c_uint32(step), field,
+                             nthreads)
     if rc != 0:
         raise ValueError("oracle diffuse16: unstable or bad arguments")
     return f, c

@@ -1,0 +1,86 @@
+"""Field precision tier: FP32, BF16 and FP16 storage of a diffusing field
+with a fixed uptake pattern and decay, against the FP64 oracle after many
+steps.  The bounds are the stated tolerances of each storage type (absolute,
+on fields in [0, 1]); they also pin that the compensated reaction keeps the
+uptake and the decay from being lost to rounding."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from oncolytica_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+# storage code -> (L-infinity bound, mean-absolute bound) against FP64 after 200
+# steps of a 32^3 field.  Measured on B200: FP32 1.9e-7 / 3.2e-8 (O2-like) and
+# 4.2e-6 / 1.8e-6 (drug-like); BF16 with round-to-nearest 0.19 / 0.024 (the
+# field stalls: per-substep increments fall below half an ulp); FP16 6.9e-3 /
+# 2.0e-3; BF16 with stochastic rounding 1.3e-2 / 3.5e-3.  The 16-bit figures
+# include the drug field's decay applied once per step instead of per substep.
+TOLERANCE = {0: (2e-5, 2e-6), 1: (3e-1, 5e-2), 2: (1e-2, 5e-3), 3: (2e-2, 5e-3)}
+
+
+def _problem(n=32, seed=5):
+    rng = np.random.default_rng(seed)
+    shape = (n, n, n)
+    z, y, x = np.indices(shape)
+    c = (n - 1) / 2.0
+    ball = ((x - c) ** 2 + (y - c) ** 2 + (z - c) ** 2) <= (0.3 * n) ** 2
+    K = np.where(ball, 0.5 * rng.poisson(2.0, size=shape), 0.0).astype(np.float32)
+    return shape, K
+
+
+def _run_gpu(olc, cuda, storage, shape, K, D, decay, bnd, init, S, dx, dt, steps):
+    import torch
+
+    nz, ny, nx = shape
+    f0 = np.full(shape, init, np.float32)
+    f0[0], f0[-1], f0[:, 0], f0[:, -1], f0[:, :, 0], f0[:, :, -1] = bnd, bnd, bnd, bnd, bnd, bnd
+    spec = _lib.OlcDiffusion(diffusion=D, decay=decay, boundary=bnd, substeps=S, has_sink=1, storage=storage)
+    dims = (C.c_int32 * 3)(nx, ny, nz)
+    sink = torch.empty(K.size, dtype=torch.float32, device=cuda)
+    Kd = torch.from_numpy(K.ravel()).to(cuda)
+    if storage == 0:
+        f = torch.from_numpy(f0.ravel()).to(cuda)
+        tmp = torch.empty_like(f)
+        for _ in range(steps):
+            sink.copy_(Kd)
+            _lib.check(olc.olc_stage_diffuse(C.c_void_p(f.data_ptr()), C.c_void_p(tmp.data_ptr()),
+                                             C.c_void_p(sink.data_ptr()), C.byref(dims), dx, dt, C.byref(spec), None))
+        return f.cpu().numpy().reshape(shape).astype(np.float64)
+    bits = oracle.to_bits16(f0, storage)
+    f = torch.from_numpy(bits.view(np.int16).ravel().copy()).to(cuda)
+    tmp = torch.empty_like(f)
+    comp = torch.zeros(K.size, dtype=torch.float32, device=cuda)
+    for step in range(steps):
+        sink.copy_(Kd)
+        _lib.check(olc.olc_stage_diffuse16(C.c_void_p(f.data_ptr()), C.c_void_p(tmp.data_ptr()),
+                                           C.c_void_p(sink.data_ptr()), C.c_void_p(comp.data_ptr()), C.byref(dims),
+                                           dx, dt, C.byref(spec), step, 0, None))
+    v = oracle.from_bits16(f.cpu().numpy().view(np.uint16), storage) + comp.cpu().numpy()
+    return v.reshape(shape).astype(np.float64)
+
+
+@pytest.mark.parametrize("storage", [0, 1, 2, 3])
+def test_field_error_against_fp64(cuda, olc, storage):
+    shape, K = _problem()
+    steps, dx, dt = 200, 4.0, 0.1
+    # an O2-like field (uptake, no decay) and a drug-like field (decay, boundary source)
+    for D, decay, bnd, init, K_used in ((2000.0, 0.0, 1.0, 1.0, K), (500.0, 0.1, 1.0, 0.0, K * 0.5)):
+        S = int(np.ceil(6.0 * D * dt / (dx * dx) * 1.05))
+        got = _run_gpu(olc, cuda, storage, shape, K_used, D, decay, bnd, init, S, dx, dt, steps)
+        ref = np.full(shape, init, np.float64)
+        ref[0], ref[-1], ref[:, 0], ref[:, -1], ref[:, :, 0], ref[:, :, -1] = bnd, bnd, bnd, bnd, bnd, bnd
+        for _ in range(steps):
+            ref = oracle.diffuse_f64(ref, K_used, dx, dt, D, decay, bnd, S)
+        err = np.abs(got - ref)
+        print(f"storage {storage} D {D}: max {err.max():.3e} mean {err.mean():.3e} moved {np.abs(ref - init).max():.3f}")
+        linf, mean = TOLERANCE[storage]
+        assert err.max() <= linf, (storage, D, err.max())
+        assert err.mean() <= mean, (storage, D, err.mean())
+        # the field moved: uptake and decay acted (not rounded away)
+        assert np.abs(ref - init).max() > 0.05

@@ -304,13 +304,14 @@ def test_contact_bit_exact(cuda, olc):
 
 # ------------------------------------------------------------------ 16-bit field storage
 
-@pytest.mark.parametrize("storage", [1, 2])
+@pytest.mark.parametrize("storage", [1, 2, 3])
 @pytest.mark.parametrize("dims,substeps,decay,with_sink", [((32, 24, 20), 5, 0.0, True),
                                                           ((64, 41, 37), 7, 0.1, True),
                                                           ((136, 17, 9), 3, 0.05, False)])
 def test_diffuse16_bit_exact(cuda, olc, storage, dims, substeps, decay, with_sink):
-    """BF16 / FP16 storage: three steps of reaction (uptake, decay, residual)
-    and substeps give the oracle's bits, residuals included."""
+    """BF16 / FP16 / BF16 with stochastic rounding: three steps of reaction
+    (uptake, decay, residual) and substeps give the oracle's bits, residuals
+    included."""
     import torch
 
     rng = np.random.default_rng(sum(dims) + storage)
@@ -334,9 +335,10 @@ def test_diffuse16_bit_exact(cuda, olc, storage, dims, substeps, decay, with_sin
             m = rng.random(f.shape) < 0.2
             sink[m] = rng.random(int(m.sum())).astype(np.float32) * 0.5
             sd = to_dev(sink, cuda)
-        bits, comp = oracle.diffuse16(bits, sink, comp, dx, dt, D, decay, 0.7, substeps, storage)
+        bits, comp = oracle.diffuse16(bits, sink, comp, dx, dt, D, decay, 0.7, substeps, storage, step=100 + step,
+                                      field=1)
         _lib.check(olc.olc_stage_diffuse16(dptr(fd), dptr(tmp), dptr(sd) if sd is not None else None, dptr(cd),
-                                           C.byref(dims_c), dx, dt, C.byref(spec), None))
+                                           C.byref(dims_c), dx, dt, C.byref(spec), 100 + step, 1, None))
         torch.cuda.synchronize()
         got = fd.cpu().numpy().view(np.uint16).reshape(nz, ny, nx)
         np.testing.assert_array_equal(got, bits, err_msg=f"field bits step {step}")
