@@ -34,7 +34,7 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
-METRIC = "agent-steps/s + voxel-updates/s, plain FP32 on 1 B200"
+METRIC = "agent-steps/s + voxel-updates/s, batched vs plain FP32 on 1 B200; p99 sim latency"
 UNIT = "agent-steps/s"
 
 
@@ -50,6 +50,11 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--no-graphs", action="store_true", help="eager launches instead of CUDA graphs of whole steps")
     ap.add_argument("--sims", type=int, default=512, help="members of the batched workload (--workload batch)")
     ap.add_argument("--solo-sample", type=int, default=0, help="members also timed one at a time (--workload batch)")
+    ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16", "bf16_sr"],
+                    help="field storage of --workload batch")
+    ap.add_argument("--extra-steps", type=int, default=10,
+                    help="timed steps of the batched and 16-bit measurements added to the default line")
+    ap.add_argument("--no-extras", action="store_true", help="leave the batched and 16-bit measurements out")
     return ap.parse_args()
 
 
@@ -369,6 +374,16 @@ def run_b200(args) -> None:
         "clocks": clk,
         "status": c1["status"],
     }
+    if world == 1 and not args.no_extras:
+        # the metric's other halves on the same GPU: the batched sweep (FP32
+        # and BF16 with stochastic rounding) and 16-bit field storage of the
+        # scale workload
+        torch.cuda.empty_cache()
+        line["batched"] = {st: measure_batch(args.sims, args.extra_steps, 3, graphs=not args.no_graphs,
+                                             solo_sample=8 if st == "f32" else 0, storage=st)
+                           for st in ("f32", "bf16_sr")}
+        line["precision"] = {st: measure_storage(spec, st, args.extra_steps * 5, 3, graphs=not args.no_graphs)
+                             for st in ("bf16_sr", "f16")}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(spec)
     print(json.dumps(line), flush=True)
@@ -376,8 +391,58 @@ def run_b200(args) -> None:
         dist.destroy_process_group()
 
 
+def measure_storage(spec, storage: str, steps: int, warmup: int, graphs: bool = True) -> dict:
+    """The scale workload with 16-bit field storage: whole-step device time
+    (graphs) and the substep kernel's live launch time from a profiled replay
+    of the same steps; roofline on 4 B per voxel-substep (2 B read + 2 B
+    written)."""
+    import torch
+
+    from oncolytica_b200 import workloads as W
+
+    sp = replace(spec, storage=storage)
+    state0 = W.initial_state(sp)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    eng = W.build_engine(sp, state0)
+    eng.set_graphs(graphs)
+    be = eng._backend_impl
+    eng.run_steps(warmup)
+    torch.cuda.synchronize(dev)
+    c0 = be.counters()
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    eng.run_steps(steps)
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    agent_steps = be.counters()["agent_steps"] - c0["agent_steps"]
+    del eng, be
+    torch.cuda.empty_cache()
+    eng = W.build_engine(sp, state0)
+    be = eng._backend_impl
+    eng.run_steps(warmup)
+    be.set_profiling(True)
+    eng.run_steps(steps)
+    prof = be.profile()
+    be.set_profiling(False)
+    del eng, be
+    torch.cuda.empty_cache()
+    nvox = int(np.prod(sp.field_dims))
+    sub_ms = prof["ms_substeps"] / max(1, prof["substep_launches"])
+    peaks = measured_peaks()
+    achieved = 4 * nvox / (sub_ms / 1e3) / 1e9
+    return {"storage": storage, "steps": steps, "ms_per_step": ms / steps,
+            "agent_steps_per_s": agent_steps / (ms / 1e3),
+            "voxel_updates_per_s": sp.voxel_updates_per_step() * steps / (ms / 1e3),
+            "substep_us": sub_ms * 1e3, "substep_alg_bytes": 4 * nvox, "substep_achieved_gbs": achieved,
+            "substep_frac_of_measured_hbm": achieved / peaks["hbm_gbs"],
+            "stages_ms_per_step": {k[3:]: prof[k] / max(1, prof["steps"]) for k in
+                                   ("ms_sink", "ms_substeps", "ms_grid", "ms_rules", "ms_contact", "ms_collect")}}
+
+
 def measure_batch(n_sims: int, steps: int, warmup: int, graphs: bool = True, solo_sample: int = 0,
-                  seed: int = 0) -> dict:
+                  seed: int = 0, storage: str = "f32") -> dict:
     """The batched workload: ``n_sims`` sweep members (uneven agent counts,
     grids and diffusion) stepped by one BatchEngine.  Device time with CUDA
     events over ``steps`` steps after ``warmup``; stage times from a second
@@ -388,7 +453,7 @@ def measure_batch(n_sims: int, steps: int, warmup: int, graphs: bool = True, sol
 
     from oncolytica_b200 import workloads as W
 
-    specs = W.batched_specs(n_sims, seed=seed)
+    specs = [replace(sp, storage=storage) for sp in W.batched_specs(n_sims, seed=seed)]
     states = [W.initial_state(sp) for sp in specs]
     dev = torch.device("cuda", torch.cuda.current_device())
 
@@ -427,7 +492,7 @@ def measure_batch(n_sims: int, steps: int, warmup: int, graphs: bool = True, sol
            "stages_ms_per_step": {k[3:]: prof[k] / max(1, prof["steps"]) for k in
                                   ("ms_sink", "ms_substeps", "ms_grid", "ms_rules", "ms_contact", "ms_collect")},
            "gpu_launches_per_step": prof["kernel_launches"] / max(1, prof["steps"]),
-           "graphs": graphs, "status": status}
+           "graphs": graphs, "status": status, "storage": storage}
     if solo_sample:
         idx = np.linspace(0, n_sims - 1, solo_sample).astype(int)
         sub = [specs[i] for i in idx]
@@ -469,12 +534,13 @@ def run_batch_workload(args) -> None:
     rank, world, local = env_ranks()
     torch.cuda.set_device(local)
     r = measure_batch(args.sims, args.steps, args.warmup, graphs=not args.no_graphs, solo_sample=args.solo_sample,
-                      seed=rank)
+                      seed=rank, storage=args.storage)
     peaks = measured_peaks()
-    line = {"metric": "agent-steps/s + voxel-updates/s, batched FP32 on 1 B200", "value": r["agent_steps_per_s"],
+    line = {"metric": METRIC, "value": r["agent_steps_per_s"],
             "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (numpy default_rng, seed 0 + rank)",
+            "dtype": "f32" if args.storage == "f32" else f"{args.storage} fields, f32 update",
+            "data": "synthetic (numpy default_rng, seed 0 + rank)",
             "config": {"workload": f"batched sweep, {args.sims} members", "members": args.sims,
                        "agents": r["agents_start"], "voxels_per_field": r["voxels_per_field"], "fields": "o2+drug",
                        "substeps_o2": r["substeps_o2"], "parallelism": f"replicas x{world}"},

@@ -89,7 +89,7 @@ struct OlcRuleParams {
     const unsigned char* fpar;
     int n_fields;
     int sim_col;
-    int field_type[OLC_MAX_FIELD_COLS];  // 0 FP32, 1 BF16, 2 FP16 storage
+    int field_type[OLC_MAX_FIELD_COLS];  // OLC_FIELD_* storage: 0 FP32, 1 BF16, 2 FP16, 3 BF16 (stochastic)
 };
 
 // What a rule body sees of one simulation of a batch (batched mode).  Member
@@ -285,9 +285,10 @@ template <class PT>
 __device__ __forceinline__ float olc_field_at(const PT& P, int f, olc_u32 v) {
     const void* p = P.field[f];
     if (!p) return 0.0f;
-    if (P.field_type[f] == 1) return olc_bf16_to_float(static_cast<const unsigned short*>(p)[v]);
-    if (P.field_type[f] == 2) return olc_f16_to_float(static_cast<const unsigned short*>(p)[v]);
-    return static_cast<const float*>(p)[v];
+    const int t = P.field_type[f];
+    if (t == 0) return static_cast<const float*>(p)[v];
+    const unsigned short h = static_cast<const unsigned short*>(p)[v];
+    return t == 2 ? olc_f16_to_float(h) : olc_bf16_to_float(h);  // 1 and 3 store BF16
 }
 
 // Deposit into a field's sink (sum of first-order uptake rates of a voxel).

@@ -33,7 +33,8 @@ def _metrics(eng):
     return {k: getattr(m, k) for k in metric_fields(type(m))}
 
 
-@pytest.mark.parametrize("graphs,storage", [(False, "f32"), (True, "f32"), (True, "bf16"), (False, "f16")])
+@pytest.mark.parametrize("graphs,storage", [(False, "f32"), (True, "f32"), (True, "bf16"), (False, "f16"),
+                                            (True, "bf16_sr")])
 def test_batch_members_match_solo_runs(cuda, graphs, storage):
     specs = _members(storage)
     assert len({s.S_o2 % 2 for s in specs}) == 2  # odd and even substep counts

@@ -386,7 +386,7 @@ def test_graph_steps_match_eager_steps(cuda):
                    {k: getattr(mb, k) for k in metric_fields(type(mb))}
 
 
-@pytest.mark.parametrize("storage,code", [("bf16", 1), ("f16", 2)])
+@pytest.mark.parametrize("storage,code", [("bf16", 1), ("f16", 2), ("bf16_sr", 3)])
 def test_tumour_step_parity_16bit_fields(cuda, storage, code):
     """16-bit field storage through the engine: each step from an identical
     state gives the oracle's field bits and residuals (reaction + substeps,
@@ -403,12 +403,13 @@ def test_tumour_step_parity_16bit_fields(cuda, storage, code):
     shp = tuple(spec.field_dims[::-1])
     for step in range(4):
         snap = be.snapshot()
+        k = be.counters()["steps"]  # the step count salts stochastic rounding, with the field's index
         o2_bits, o2_res = oracle.diffuse16(snap["fields"]["o2"].reshape(shp), snap["sinks"]["o2"].reshape(shp),
                                            snap["residuals"]["o2"].reshape(shp), spec.dx, spec.dt, spec.D_o2, 0.0,
-                                           spec.bnd_o2, spec.S_o2, code)
+                                           spec.bnd_o2, spec.S_o2, code, step=k, field=0)
         dr_bits, dr_res = oracle.diffuse16(snap["fields"]["drug"].reshape(shp), None,
                                            snap["residuals"]["drug"].reshape(shp), spec.dx, spec.dt, spec.D_drug,
-                                           spec.decay_drug, spec.bnd_drug, spec.S_drug, code)
+                                           spec.decay_drug, spec.bnd_drug, spec.S_drug, code, step=k, field=1)
         fsnap = dict(snap)
         fsnap["fields"] = {"o2": oracle.from_bits16(o2_bits, code).ravel(),
                            "drug": oracle.from_bits16(dr_bits, code).ravel()}
