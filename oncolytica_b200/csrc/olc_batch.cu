@@ -329,13 +329,14 @@ void launch_flip_parity(const FieldStep* steps, int field, int n_fields, olc_u32
 // ------------------------------------------------------------------ 16-bit fields
 // The same tiles on BF16 / FP16 storage (olc_field16.cu's arithmetic): the
 // reaction pass with its FP32 residual, then substeps without decay.
+// Eight voxels per thread (16-byte loads and stores), 64 threads per tile.
 template <int ST>
-__global__ void __launch_bounds__(128) k_substep_batch16(const uint4* __restrict__ tiles,
-                                                         const OlcSimDesc* __restrict__ sims,
-                                                         const FieldStep* __restrict__ steps, int field, int n_fields,
-                                                         const unsigned char* __restrict__ fpar, int sub,
-                                                         unsigned short* fa, unsigned short* fb,
-                                                         const olc_u32* step_ctr) {
+__global__ void __launch_bounds__(64) k_substep_batch16(const uint4* __restrict__ tiles,
+                                                        const OlcSimDesc* __restrict__ sims,
+                                                        const FieldStep* __restrict__ steps, int field, int n_fields,
+                                                        const unsigned char* __restrict__ fpar, int sub,
+                                                        unsigned short* fa, unsigned short* fb,
+                                                        const olc_u32* step_ctr) {
     const uint4 t = tiles[blockIdx.x];
     const olc_u32 k = t.x;
     const OlcSimDesc& d = sims[k];
@@ -344,36 +345,65 @@ __global__ void __launch_bounds__(128) k_substep_batch16(const uint4* __restrict
     const bool flip = ((fpar[(size_t)k * n_fields + field] ^ (unsigned)sub) & 1u) != 0u;
     const unsigned short* in = (flip ? fb : fa) + d.field_off;
     unsigned short* out = (flip ? fa : fb) + d.field_off;
-    const int x = (int)t.y * BT_X + 4 * (threadIdx.x & 7);
-    const int y = (int)t.z * BT_Y + (threadIdx.x >> 3);
+    const int x = (int)t.y * BT_X + 8 * (threadIdx.x & 3);
+    const int y = (int)t.z * BT_Y + (threadIdx.x >> 2);
     const int z0 = (int)t.w * BT_Z;
     if (x >= nx || y >= ny) return;
     const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
     const bool edge_y = y == 0 || y == ny - 1;
-    const bool ex0 = x == 0, ex3 = x + 3 == nx - 1;
+    const bool ex0 = x == 0, ex7 = x + 7 == nx - 1;
     const float bf = Store16<ST>::to_f(Store16<ST>::from_f(fs.bval));
     const olc_u32 key = olc_sr_key(*step_ctr, sub, field);
-    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     size_t idx = (size_t)z0 * sz + (size_t)y * sy + x;
-    float4 zm = z0 > 0 ? load4<ST>(in + idx - sz) : zero;
-    float4 c = load4<ST>(in + idx);
+    float zm[8], c[8], zp[8], ym[8], yp[8], v[8];
+    if (z0 > 0) {
+        load8<ST>(in + idx - sz, zm);
+    } else {
+#pragma unroll
+        for (int e = 0; e < 8; ++e) zm[e] = 0.0f;
+    }
+    load8<ST>(in + idx, c);
     const int z1 = min(z0 + BT_Z, nz);
     for (int zz = z0; zz < z1; ++zz, idx += sz) {
-        const float4 zp = zz + 1 < nz ? load4<ST>(in + idx + sz) : zero;
-        const float4 ym = y > 0 ? load4<ST>(in + idx - sy) : zero;
-        const float4 yp = y + 1 < ny ? load4<ST>(in + idx + sy) : zero;
-        const float xl = x > 0 ? Store16<ST>::to_f(in[idx - 1]) : 0.0f;
-        const float xr = x + 4 < nx ? Store16<ST>::to_f(in[idx + 4]) : 0.0f;
-        float4 v = update4_b(xl, xr, c, ym, yp, zm, zp, fs.r, 1.0f);
-        if (edge_y || zz == 0 || zz == nz - 1) {
-            v = make_float4(bf, bf, bf, bf);
+        if (zz + 1 < nz) {
+            load8<ST>(in + idx + sz, zp);
         } else {
-            if (ex0) v.x = bf;
-            if (ex3) v.w = bf;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) zp[e] = 0.0f;
         }
-        store4_at<ST>(out + idx, v, idx, key);
-        zm = c;
-        c = zp;
+        if (y > 0) {
+            load8<ST>(in + idx - sy, ym);
+        } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) ym[e] = 0.0f;
+        }
+        if (y + 1 < ny) {
+            load8<ST>(in + idx + sy, yp);
+        } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) yp[e] = 0.0f;
+        }
+        const float xl = x > 0 ? Store16<ST>::to_f(in[idx - 1]) : 0.0f;
+        const float xr = x + 8 < nx ? Store16<ST>::to_f(in[idx + 8]) : 0.0f;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const float xm = e == 0 ? xl : c[e - 1], xp = e == 7 ? xr : c[e + 1];
+            const float s6 = __fadd_rn(__fadd_rn(__fadd_rn(xm, xp), __fadd_rn(ym[e], yp[e])), __fadd_rn(zm[e], zp[e]));
+            v[e] = fmaxf(__fadd_rn(c[e], __fmul_rn(fs.r, __fsub_rn(s6, __fmul_rn(6.0f, c[e])))), 0.0f);
+        }
+        if (edge_y || zz == 0 || zz == nz - 1) {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) v[e] = bf;
+        } else {
+            if (ex0) v[0] = bf;
+            if (ex7) v[7] = bf;
+        }
+        store8_at<ST>(out + idx, v, idx, key);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            zm[e] = c[e];
+            c[e] = zp[e];
+        }
     }
 }
 
@@ -476,13 +506,13 @@ void launch_substep_batch16(const BatchArgs& b, int storage, const uint4* tiles,
     unsigned short* a = static_cast<unsigned short*>(fa);
     unsigned short* c = static_cast<unsigned short*>(fb);
     if (storage == OLC_FIELD_BF16)
-        k_substep_batch16<OLC_FIELD_BF16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a, c,
+        k_substep_batch16<OLC_FIELD_BF16><<<n_tiles, 64, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a, c,
                                                                    step_ctr);
     else if (storage == OLC_FIELD_BF16_SR)
-        k_substep_batch16<OLC_FIELD_BF16_SR><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a,
+        k_substep_batch16<OLC_FIELD_BF16_SR><<<n_tiles, 64, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a,
                                                                       c, step_ctr);
     else
-        k_substep_batch16<OLC_FIELD_F16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a, c,
+        k_substep_batch16<OLC_FIELD_F16><<<n_tiles, 64, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a, c,
                                                                   step_ctr);
 }
 

@@ -89,24 +89,27 @@ void launch_react16(void* f, float* sink, float* comp, const FieldStep& fs, cuda
 }
 
 // ------------------------------------------------------------------ diffusion substep
-// The 4-wide TMA tile of k_substep_x4 on 16-bit storage: a CTA of 16 x TYR
-// threads owns a 64 x TYR x TZ block; the TMA box is 80 x (TYR+2) x (TZ+2)
-// elements with x starting 8 columns early (16-byte alignment of 2-byte
-// elements).  Each thread handles four x voxels: 8-byte shared loads of the
-// centre, y and z rows, 2-byte loads of the x neighbours, an 8-byte store.
+// The TMA tile of k_substep_x4 on 16-bit storage, eight voxels per thread: a
+// CTA of 8 x TYR threads owns a 64 x TYR x TZ block; the TMA box is
+// 80 x (TYR+2) x (TZ+2) elements with x starting 8 columns early (16-byte
+// alignment of 2-byte elements).  Per eight voxels a thread issues 16-byte
+// shared loads of the centre, y and z rows, two 2-byte loads of the x
+// neighbours and one 16-byte store, as many instructions per byte as the
+// 4-wide FP32 kernel.
 namespace t16 {
 constexpr int TX = 64, HX = 8, WX = TX + 2 * HX;  // 80 elements, 160 bytes
-constexpr int TYR = 8, TZ = 8, WY = TYR + 2, WZ = TZ + 2;
+constexpr int TYR = 16, TZ = 8, WY = TYR + 2, WZ = TZ + 2;
+constexpr int THREADS = 8 * TYR;
 constexpr unsigned BYTES = WX * WY * WZ * 2;
 constexpr size_t SMEM = BYTES + 16 + 128;
 }  // namespace t16
 
 template <int ST>
-__global__ void __launch_bounds__(16 * t16::TYR) k_substep16(const __grid_constant__ CUtensorMap in_map,
-                                                            unsigned short* __restrict__ out, int nx, int ny, int nz,
-                                                            float r, float bval, olc_u32* status, int rev,
-                                                            const olc_u32* step_ctr, olc_u32 step_host, int sub,
-                                                            int field) {
+__global__ void __launch_bounds__(t16::THREADS) k_substep16(const __grid_constant__ CUtensorMap in_map,
+                                                           unsigned short* __restrict__ out, int nx, int ny, int nz,
+                                                           float r, float bval, olc_u32* status, int rev,
+                                                           const olc_u32* step_ctr, olc_u32 step_host, int sub,
+                                                           int field) {
     using namespace t16;
     extern __shared__ unsigned char t16_raw[];
     const olc_u32 pad = (128u - (smem_addr(t16_raw) & 127u)) & 127u;
@@ -145,45 +148,48 @@ __global__ void __launch_bounds__(16 * t16::TYR) k_substep16(const __grid_consta
         }
         return;
     }
-    const int g = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int x = x0 + 4 * g, y = y0 + ty;
+    const int g = threadIdx.x & 7, ty = threadIdx.x >> 3;
+    const int x = x0 + 8 * g, y = y0 + ty;
     if (x >= nx || y >= ny) return;
     const bool edge_y = y == 0 || y == ny - 1;
-    const bool ex0 = x == 0, ex3 = x + 3 == nx - 1;
+    const bool ex0 = x == 0, ex7 = x + 7 == nx - 1;
     constexpr int PS = WY * WX;
-    const unsigned short* col = tile + (ty + 1) * WX + HX + 4 * g;
-    float4 zm = load4<ST>(col);
-    float4 c = load4<ST>(col + PS);
+    const unsigned short* col = tile + (ty + 1) * WX + HX + 8 * g;
+    float zm[8], c[8], zp[8], ym[8], yp[8], v[8];
+    load8<ST>(col, zm);
+    load8<ST>(col + PS, c);
     const size_t sz = (size_t)nx * ny;
     unsigned short* o = out + (size_t)z0 * sz + (size_t)y * nx + x;
     const float bf = Store16<ST>::to_f(Store16<ST>::from_f(bval));  // the face value as stored
     const olc_u32 key = olc_sr_key(step_ctr ? *step_ctr : step_host, sub, field);
     unsigned long long vi = (unsigned long long)z0 * sz + (unsigned long long)y * nx + x;
-#pragma unroll 4
+#pragma unroll 2
     for (int lz = 1; lz <= TZ; ++lz) {
         const int z = z0 + lz - 1;
         if (z >= nz) break;
         const unsigned short* pc = col + lz * PS;
-        const float4 zp = load4<ST>(pc + PS);
-        const float4 ym = load4<ST>(pc - WX);
-        const float4 yp = load4<ST>(pc + WX);
-        const float xl = Store16<ST>::to_f(pc[-1]), xr = Store16<ST>::to_f(pc[4]);
-        float4 v;
-        v.x = diffuse1(xl, c.y, ym.x, yp.x, zm.x, zp.x, c.x, r);
-        v.y = diffuse1(c.x, c.z, ym.y, yp.y, zm.y, zp.y, c.y, r);
-        v.z = diffuse1(c.y, c.w, ym.z, yp.z, zm.z, zp.z, c.z, r);
-        v.w = diffuse1(c.z, xr, ym.w, yp.w, zm.w, zp.w, c.w, r);
+        load8<ST>(pc + PS, zp);
+        load8<ST>(pc - WX, ym);
+        load8<ST>(pc + WX, yp);
+        const float xl = Store16<ST>::to_f(pc[-1]), xr = Store16<ST>::to_f(pc[8]);
+#pragma unroll
+        for (int e = 0; e < 8; ++e)
+            v[e] = diffuse1(e == 0 ? xl : c[e - 1], e == 7 ? xr : c[e + 1], ym[e], yp[e], zm[e], zp[e], c[e], r);
         if (edge_y || z == 0 || z == nz - 1) {
-            v = make_float4(bf, bf, bf, bf);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) v[e] = bf;
         } else {
-            if (ex0) v.x = bf;
-            if (ex3) v.w = bf;
+            if (ex0) v[0] = bf;
+            if (ex7) v[7] = bf;
         }
-        store4_at<ST>(o, v, vi, key);
+        store8_at<ST>(o, v, vi, key);
         o += sz;
         vi += sz;
-        zm = c;
-        c = zp;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            zm[e] = c[e];
+            c[e] = zp[e];
+        }
     }
 }
 
@@ -209,7 +215,7 @@ static void launch_sub16(const CUtensorMap& map, void* out, const FieldStep& fs,
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((fs.dims[0] + TX - 1) / TX, (fs.dims[1] + TYR - 1) / TYR, (fs.dims[2] + TZ - 1) / TZ);
-    cfg.blockDim = dim3(16 * TYR);
+    cfg.blockDim = dim3(THREADS);
     cfg.dynamicSmemBytes = SMEM;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];

@@ -46,13 +46,16 @@ __device__ __forceinline__ unsigned short olc_bf16_sr(float f, olc_u32 rnd) {
     return (unsigned short)((__float_as_uint(f) + (rnd & 0xffffu)) >> 16);
 }
 
-// Random bits of voxel v (index within its grid) for one substep: `key` mixes
-// the step, substep and field (olc_sr_key).
+// Random bits for one substep: `key` mixes the step, substep and field
+// (fmix32, once per launch); voxels 2p and 2p+1 of a grid share one 32-bit
+// word x = ((p ^ key) * 0x9E3779B1) ^ (x >> 15) (a multiplicative hash with
+// one xorshift), voxel 2p taking its low and voxel 2p+1 its high 16 bits.
 __device__ __forceinline__ olc_u32 olc_sr_key(olc_u32 step, int sub, int field) {
     return olc_fmix32((step << 8) ^ (olc_u32)sub ^ ((olc_u32)field << 24));
 }
-__device__ __forceinline__ olc_u32 olc_sr_bits(unsigned long long v, olc_u32 key) {
-    return olc_fmix32((olc_u32)v * 0x9E3779B1u ^ key);
+__device__ __forceinline__ olc_u32 olc_sr_pair(unsigned long long pair, olc_u32 key) {
+    olc_u32 x = ((olc_u32)pair ^ key) * 0x9E3779B1u;
+    return x ^ (x >> 15);
 }
 
 template <int ST>
@@ -65,17 +68,44 @@ __device__ __forceinline__ float4 load4(const unsigned short* p) {
 // Stores four values at voxel index v (stochastic rounding for ST = BF16_SR).
 template <int ST>
 __device__ __forceinline__ void store4_at(unsigned short* p, float4 v, unsigned long long vi, olc_u32 key) {
-    if (ST == OLC_FIELD_BF16_SR) {
-        const olc_u32 lo = (olc_u32)olc_bf16_sr(v.x, olc_sr_bits(vi, key)) |
-                           ((olc_u32)olc_bf16_sr(v.y, olc_sr_bits(vi + 1, key)) << 16);
-        const olc_u32 hi = (olc_u32)olc_bf16_sr(v.z, olc_sr_bits(vi + 2, key)) |
-                           ((olc_u32)olc_bf16_sr(v.w, olc_sr_bits(vi + 3, key)) << 16);
+    if (ST == OLC_FIELD_BF16_SR) {  // vi is a multiple of 4
+        const olc_u32 r0 = olc_sr_pair(vi >> 1, key), r1 = olc_sr_pair((vi >> 1) + 1, key);
+        const olc_u32 lo = (olc_u32)olc_bf16_sr(v.x, r0) | ((olc_u32)olc_bf16_sr(v.y, r0 >> 16) << 16);
+        const olc_u32 hi = (olc_u32)olc_bf16_sr(v.z, r1) | ((olc_u32)olc_bf16_sr(v.w, r1 >> 16) << 16);
         *reinterpret_cast<uint2*>(p) = make_uint2(lo, hi);
         return;
     }
     const olc_u32 lo = (olc_u32)Store16<ST>::from_f(v.x) | ((olc_u32)Store16<ST>::from_f(v.y) << 16);
     const olc_u32 hi = (olc_u32)Store16<ST>::from_f(v.z) | ((olc_u32)Store16<ST>::from_f(v.w) << 16);
     *reinterpret_cast<uint2*>(p) = make_uint2(lo, hi);
+}
+
+// Eight consecutive values (16 bytes): load to FP32, store with rounding at
+// voxel index vi (a multiple of 8; stochastic for ST = BF16_SR).
+template <int ST>
+__device__ __forceinline__ void load8(const unsigned short* p, float (&f)[8]) {
+    const uint4 raw = *reinterpret_cast<const uint4*>(p);
+    const olc_u32 w[4] = {raw.x, raw.y, raw.z, raw.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        f[2 * k] = Store16<ST>::to_f((unsigned short)(w[k] & 0xffffu));
+        f[2 * k + 1] = Store16<ST>::to_f((unsigned short)(w[k] >> 16));
+    }
+}
+
+template <int ST>
+__device__ __forceinline__ void store8_at(unsigned short* p, const float (&v)[8], unsigned long long vi, olc_u32 key) {
+    olc_u32 w[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (ST == OLC_FIELD_BF16_SR) {
+            const olc_u32 r = olc_sr_pair((vi >> 1) + k, key);
+            w[k] = (olc_u32)olc_bf16_sr(v[2 * k], r) | ((olc_u32)olc_bf16_sr(v[2 * k + 1], r >> 16) << 16);
+        } else {
+            w[k] = (olc_u32)Store16<ST>::from_f(v[2 * k]) | ((olc_u32)Store16<ST>::from_f(v[2 * k + 1]) << 16);
+        }
+    }
+    *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
 }
 
 template <int ST>

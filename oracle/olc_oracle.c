@@ -259,10 +259,11 @@ static uint16_t f_to_h16(float f, int storage) {
     return h;
 }
 
-/* Stochastic BF16 rounding of the substeps (storage 3): random bits of voxel
- * v are fmix32(v * 0x9E3779B1 ^ key), key = fmix32((step << 8) ^ substep ^
- * (field << 24)); the low 16 FP32 bits plus 16 random bits carry into the
- * kept half with probability equal to the discarded fraction. */
+/* Stochastic BF16 rounding of the substeps (storage 3): key = fmix32((step <<
+ * 8) ^ substep ^ (field << 24)); voxels 2p, 2p+1 share x = (p ^ key) *
+ * 0x9E3779B1, x ^= x >> 15, voxel 2p taking the low and 2p+1 the high 16 bits;
+ * the low 16 FP32 bits plus those random bits carry into the kept half with
+ * probability equal to the discarded fraction. */
 static uint32_t fmix32(uint32_t h) {
     h ^= h >> 16;
     h *= 0x85EBCA6Bu;
@@ -324,8 +325,13 @@ int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const in
                     float s2 = s1 + (h16_to_f(cur[v - sz], storage) + h16_to_f(cur[v + sz], storage));
                     float u = c + r * (s2 - 6.0f * c);
                     u = u > 0.0f ? u : 0.0f;
-                    nxt[v] = storage == 3 ? f_to_bf16_sr(u, fmix32((uint32_t)v * 0x9E3779B1u ^ key))
-                                          : f_to_h16(u, storage);
+                    if (storage == 3) {
+                        uint32_t xr = ((uint32_t)(v >> 1) ^ key) * 0x9E3779B1u;
+                        xr ^= xr >> 15;
+                        nxt[v] = f_to_bf16_sr(u, (v & 1) ? (xr >> 16) : (xr & 0xffffu));
+                    } else {
+                        nxt[v] = f_to_h16(u, storage);
+                    }
                 }
             }
         uint16_t* t = cur;
