@@ -55,6 +55,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--extra-steps", type=int, default=10,
                     help="timed steps of the batched and 16-bit measurements added to the default line")
     ap.add_argument("--no-extras", action="store_true", help="leave the batched and 16-bit measurements out")
+    ap.add_argument("--rate", type=float, default=20.0, help="request arrivals per second (--workload serve)")
+    ap.add_argument("--duration", type=float, default=120.0, help="seconds of arrivals (--workload serve)")
     return ap.parse_args()
 
 
@@ -515,6 +517,99 @@ def measure_batch(n_sims: int, steps: int, warmup: int, graphs: bool = True, sol
     return out
 
 
+def measure_serving(rate: float, duration: float, seed: int = 0, storage: str = "f32", solo_sample: int = 0,
+                    hbm_fraction: float = 0.3, max_slots: int = 2048) -> dict:
+    """The serving mix: requests drawn like sweep members (steps U{100..1000})
+    arrive as a Poisson process at ``rate``/s for ``duration`` s and are served
+    by one pool (continuous batching, admission by free HBM: the arenas take
+    ``hbm_fraction`` of the free device memory, split as the mix uses them).
+    Wall-clock time to completion per request (arrival to result on the host)
+    and whole-run throughput (device agent-step counter / wall time from the
+    first arrival to the last result).  With ``solo_sample`` > 0 that many
+    requests (spread over the mix) also run alone on the plain FP32 path (solo
+    engine, CUDA graphs), for the throughput ratio."""
+    import torch
+
+    from oncolytica_b200 import workloads as W
+    from oncolytica_b200._geometry import voxel_table_size
+    from oncolytica_b200.serving import Footprint, PoolDevice, ServingPool, SimRequest, plan_arenas
+
+    sched = W.serving_schedule(rate=rate, duration=duration, seed=seed, storage=storage)
+    specs = [sp for _, sp, _ in sched]
+    mix = [Footprint(sp.capacity, voxel_table_size(sp.tissue_dims), int(np.prod(sp.field_dims))) for sp in specs]
+    tdims = tuple(max(sp.tissue_dims[i] for sp in specs) for i in range(3))
+    free, _ = torch.cuda.mem_get_info()
+    code = {"f32": 0, "bf16": 1, "f16": 2, "bf16_sr": 3}[storage]
+    plan = plan_arenas(int(hbm_fraction * free), mix, n_cols=8, storages=[code, code], sinks=[True, False])
+    proto = W.configure_engine(specs[0])
+    dev = PoolDevice(proto, max_slots=max_slots, max_tissue_dims=tdims, **plan)
+    # warm-up outside the timed run: one short request loads every kernel
+    warm = ServingPool(dev)
+    e, s = W.configure_engine(specs[0])
+    warm.submit(SimRequest(e, s, 3, return_state=True))
+    warm.drain()
+    pool = ServingPool(dev)
+
+    def factory(sp, n):
+        return lambda: SimRequest(*W.configure_engine(sp), n, return_state=True)
+
+    arrivals = [(t, factory(sp, n)) for t, sp, n in sched]
+    torch.cuda.synchronize()
+    c0 = dev.counters()
+    t0 = time.perf_counter()
+    results = pool.serve(arrivals)
+    t1 = time.perf_counter()
+    c1 = dev.counters()
+    done = [r for r in results if r.status == "done"]
+    ttc = np.array([r.ttc for r in done]) if done else np.zeros(1)
+    wait = np.array([r.admitted - r.arrival for r in done]) if done else np.zeros(1)
+    wall = t1 - t0
+    agent_steps = c1["agent_steps"] - c0["agent_steps"]
+    vox = sum(r.voxel_updates for r in done)
+    statuses = {}
+    for r in results:
+        statuses[r.status] = statuses.get(r.status, 0) + 1
+    out = {"rate_per_s": rate, "duration_s": duration, "requests": len(sched), "status": statuses,
+           "storage": storage, "wall_s": wall, "steps_run": pool.steps_run, "ms_per_batch_step": 1e3 * wall / max(1, pool.steps_run),
+           "ttc_p50_s": float(np.percentile(ttc, 50)), "ttc_p99_s": float(np.percentile(ttc, 99)),
+           "ttc_mean_s": float(ttc.mean()), "ttc_max_s": float(ttc.max()),
+           "queue_wait_p99_s": float(np.percentile(wait, 99)),
+           "agent_steps_per_s": agent_steps / wall, "voxel_updates_per_s": vox / wall,
+           "max_resident": pool.max_resident, "device_status": c1["status"],
+           "arenas": {k: int(v) for k, v in plan.items()},
+           "peak_usage": {k: int(v) for k, v in pool.peak_usage.items()},
+           "hbm_fraction": hbm_fraction}
+    dev.close()
+    del dev, pool, warm
+    torch.cuda.empty_cache()
+    if solo_sample:
+        order = np.argsort([int(np.prod(sp.field_dims)) * (sp.S_o2 + sp.S_drug) + sp.n_agents for sp in specs])
+        idx = order[np.linspace(0, len(order) - 1, solo_sample).astype(int)]
+        solo_ms, solo_as, served_as_est = 0.0, 0, 0
+        st = torch.cuda.current_stream()
+        for i in idx:
+            _, sp, n = sched[i]
+            sp32 = replace(sp, storage="f32")
+            eng = W.build_engine(sp32)
+            eng.set_graphs(True)
+            be = eng._backend_impl
+            a0 = be.counters()["agent_steps"]
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            eng.run_steps(n)
+            e1.record(st)
+            torch.cuda.synchronize()
+            solo_ms += e0.elapsed_time(e1)
+            solo_as += be.counters()["agent_steps"] - a0
+            del eng, be
+        out["solo_fp32_sample"] = {"requests": int(solo_sample), "agent_steps_per_s": solo_as / (solo_ms / 1e3),
+                                   "served_vs_solo": out["agent_steps_per_s"] / (solo_as / (solo_ms / 1e3)),
+                                   "sample": "requests spread over the mix by size, each run alone for its own "
+                                             "step count on a solo FP32 engine with CUDA graphs"}
+        torch.cuda.empty_cache()
+    return out
+
+
 class _SoloAsBatch:
     """A solo Engine behind the two calls measure_batch's timer uses."""
 
@@ -549,12 +644,31 @@ def run_batch_workload(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+def run_serving_workload(args) -> None:
+    import torch
+
+    rank, world, local = env_ranks()
+    torch.cuda.set_device(local)
+    r = measure_serving(args.rate, args.duration, seed=rank, storage=args.storage, solo_sample=args.solo_sample)
+    line = {"metric": METRIC, "value": r["agent_steps_per_s"], "unit": UNIT, "n_gpus": world, "steps": r["steps_run"],
+            "warmup": 1, "ms_per_step": r["ms_per_batch_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if args.storage == "f32" else f"{args.storage} fields, f32 update",
+            "data": "synthetic (numpy default_rng, seed 0 + rank)",
+            "config": {"workload": f"serving mix, Poisson {args.rate}/s for {args.duration} s",
+                       "parallelism": f"replicas x{world}"},
+            "serving": r}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "batch":
         run_batch_workload(args)
+    elif args.workload == "serve":
+        run_serving_workload(args)
     else:
         run_b200(args)
 

@@ -304,6 +304,83 @@ int olc_read_field_parity(OlcSim* sim, uint8_t* out, void* stream);
 int olc_read_reductions_batch(OlcSim* sim, OlcReductions* out, void* stream);
 int olc_read_user_metrics_batch(OlcSim* sim, void* out, size_t bytes_per_sim, void* stream);
 
+/* ------------------------------------------------------------- serving pool
+ * A batch handle whose members join and leave between steps (no counterpart
+ * in the reference).  Members occupy slots [0, max_slots); each holds one
+ * range of the bin-table arena and one range of the field arena (the same
+ * voxel range in every field buffer), taken at admission and returned at
+ * retirement, so admission is decided by free device memory.  A member
+ * reproduces its solo run bit for bit from the step it joins (its rows are
+ * appended where births go and sorted into place by the next step; its
+ * stochastic-rounding salt counts its own steps).  All calls on a pool are
+ * stream-ordered on the caller's stream: use one stream for every call.
+ * olc_bind_agent_column, olc_set_contact, olc_set_rule_source,
+ * olc_set_user_metrics_size (bytes per slot), olc_step, olc_read_counters,
+ * olc_set_graphs, olc_read_reductions_batch and olc_read_user_metrics_batch
+ * (max_slots records) work on pools; the batch calls that bind or upload all
+ * members at once do not. */
+typedef struct {
+    uint32_t max_slots;           /* members resident at once */
+    int32_t max_tissue_dims[3];   /* largest bin grid of any member (sets the sort-key split) */
+    uint64_t table_entries;       /* bin-table arena, 8-byte entries */
+    uint64_t field_voxels;        /* field arena: voxels of every field buffer */
+} OlcPoolConfig;
+
+typedef struct {
+    uint32_t slots_used, max_slots;
+    uint64_t table_used, table_entries, table_largest_free;
+    uint64_t field_used, field_voxels, field_largest_free;
+} OlcPoolUsage;
+
+int olc_create_pool(const OlcPoolConfig* cfg, const OlcCaps* caps, OlcSim** out);
+
+/* Field `index` of every member: a and b hold cfg.field_voxels elements of the
+ * storage type (OLC_FIELD_*), sink (FP32, or NULL when no rule deposits into
+ * the field) and comp (FP32, 16-bit storage only) as many. */
+int olc_bind_field_pool(OlcSim* sim, int index, void* a, void* b, float* sink, float* comp, int storage);
+
+/* Admits one simulation: geometry, specs[n_fields] (specs[f].storage must
+ * match the bound storage) and its Params blob (every member's blob has the
+ * same size).  On success *slot and *field_off (first voxel of its grids in
+ * every field buffer) are set; the caller then writes the initial grids into
+ * buffer a at field_off and adds the agents.  The member's sink, residual,
+ * field parity, metric and reduction records are cleared.  OLC_ERR_CAPACITY
+ * (nothing changed) when no slot, table range or field range is free. */
+int olc_pool_admit(OlcSim* sim, const OlcGeom* geom, const OlcDiffusion* specs, const void* params,
+                   size_t params_bytes, int32_t* slot, uint64_t* field_off, void* stream);
+
+/* Appends n agent rows of `slot`: cols_dev[c] holds n 4-byte elements of
+ * agent column c (the `_sim` column's pointer is ignored; it is written with
+ * the slot).  Rows past the handle's capacity are not written and set
+ * OLC_STATUS_CAPACITY. */
+int olc_pool_add_agents(OlcSim* sim, int32_t slot, void* const* cols_dev, uint32_t n, void* stream);
+
+/* Copies the live rows of `slot` in device order into dst_dev[c] (NULL
+ * columns skipped; at most max_rows rows) and writes the slot's live-row
+ * count to *count_dev (device word; a count above max_rows means rows were
+ * left out).  The result of a member is read this way before retiring it. */
+int olc_pool_gather(OlcSim* sim, int32_t slot, void* const* dst_dev, uint32_t max_rows, uint32_t* count_dev,
+                    void* stream);
+
+/* Async copies of the slot's last collected reductions and metric
+ * accumulators into host memory (pinned, for the copy to stay async). */
+int olc_pool_copy_results(OlcSim* sim, int32_t slot, OlcReductions* red_host, void* metrics_host, void* stream);
+
+/* Frees the slot: its rows are flagged dead (the next step's sort drops
+ * them) and its arena ranges are returned. */
+int olc_pool_retire(OlcSim* sim, int32_t slot, void* stream);
+
+int olc_pool_usage(const OlcSim* sim, OlcPoolUsage* out);
+
+/* The pool's range allocator on its own, for callers that plan admissions
+ * (and for tests): best fit over [0, capacity), merged on release. */
+typedef struct OlcArena OlcArena;
+int olc_arena_create(uint64_t capacity, OlcArena** out);
+int olc_arena_alloc(OlcArena* arena, uint64_t n, uint64_t align, uint64_t* offset);
+int olc_arena_release(OlcArena* arena, uint64_t offset, uint64_t n);
+int olc_arena_stats(const OlcArena* arena, uint64_t* used, uint64_t* largest_free, uint64_t* free_ranges);
+int olc_arena_destroy(OlcArena* arena);
+
 /* ---------------------------------------------------- stateless stages */
 /* These run one stage on caller buffers; the parity tests call them. */
 

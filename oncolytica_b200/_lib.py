@@ -44,6 +44,9 @@ EXPORTS = (
     "olc_create_batch", "olc_batch_field_offsets", "olc_bind_field_batch", "olc_set_params_batch",
     "olc_read_field_parity", "olc_read_reductions_batch", "olc_read_user_metrics_batch",
     "olc_bind_field_ex", "olc_stage_diffuse16",
+    "olc_create_pool", "olc_bind_field_pool", "olc_pool_admit", "olc_pool_add_agents", "olc_pool_gather",
+    "olc_pool_copy_results", "olc_pool_retire", "olc_pool_usage",
+    "olc_arena_create", "olc_arena_alloc", "olc_arena_release", "olc_arena_stats", "olc_arena_destroy",
 )
 
 
@@ -143,7 +146,30 @@ class OlcReductions(C.Structure):
     ]
 
 
+class OlcPoolConfig(C.Structure):
+    _fields_ = [
+        ("max_slots", C.c_uint32),
+        ("max_tissue_dims", C.c_int32 * 3),
+        ("table_entries", C.c_uint64),
+        ("field_voxels", C.c_uint64),
+    ]
+
+
+class OlcPoolUsage(C.Structure):
+    _fields_ = [
+        ("slots_used", C.c_uint32),
+        ("max_slots", C.c_uint32),
+        ("table_used", C.c_uint64),
+        ("table_entries", C.c_uint64),
+        ("table_largest_free", C.c_uint64),
+        ("field_used", C.c_uint64),
+        ("field_voxels", C.c_uint64),
+        ("field_largest_free", C.c_uint64),
+    ]
+
+
 _VP = C.c_void_p
+_U64P = C.POINTER(C.c_uint64)
 _SIGS = {
     "olc_create": (C.c_int, [C.POINTER(OlcGeom), C.POINTER(OlcCaps), C.POINTER(_VP)]),
     "olc_destroy": (C.c_int, [_VP]),
@@ -188,6 +214,20 @@ _SIGS = {
                                     C.POINTER(OlcDiffusion), _VP]),
     "olc_stage_contact": (C.c_int, [_VP, _VP, C.c_uint32, C.POINTER(OlcGeom), C.POINTER(OlcContact), C.c_float,
                                     _VP, _VP, _VP, _VP]),
+    "olc_create_pool": (C.c_int, [C.POINTER(OlcPoolConfig), C.POINTER(OlcCaps), C.POINTER(_VP)]),
+    "olc_bind_field_pool": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, _VP, C.c_int]),
+    "olc_pool_admit": (C.c_int, [_VP, C.POINTER(OlcGeom), C.POINTER(OlcDiffusion), _VP, C.c_size_t,
+                                 C.POINTER(C.c_int32), _U64P, _VP]),
+    "olc_pool_add_agents": (C.c_int, [_VP, C.c_int32, C.POINTER(_VP), C.c_uint32, _VP]),
+    "olc_pool_gather": (C.c_int, [_VP, C.c_int32, C.POINTER(_VP), C.c_uint32, _VP, _VP]),
+    "olc_pool_copy_results": (C.c_int, [_VP, C.c_int32, _VP, _VP, _VP]),
+    "olc_pool_retire": (C.c_int, [_VP, C.c_int32, _VP]),
+    "olc_pool_usage": (C.c_int, [_VP, C.POINTER(OlcPoolUsage)]),
+    "olc_arena_create": (C.c_int, [C.c_uint64, C.POINTER(_VP)]),
+    "olc_arena_alloc": (C.c_int, [_VP, C.c_uint64, C.c_uint64, _U64P]),
+    "olc_arena_release": (C.c_int, [_VP, C.c_uint64, C.c_uint64]),
+    "olc_arena_stats": (C.c_int, [_VP, _U64P, _U64P, _U64P]),
+    "olc_arena_destroy": (C.c_int, [_VP]),
 }
 
 _lock = threading.Lock()

@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(64) k_substep_batch16(const uint4* __restrict_
     const bool edge_y = y == 0 || y == ny - 1;
     const bool ex0 = x == 0, ex7 = x + 7 == nx - 1;
     const float bf = Store16<ST>::to_f(Store16<ST>::from_f(fs.bval));
-    const olc_u32 key = olc_sr_key(*step_ctr, sub, field);
+    const olc_u32 key = olc_sr_key(*step_ctr - d.step_base, sub, field);  // the simulation's own step
     size_t idx = (size_t)z0 * sz + (size_t)y * sy + x;
     float zm[8], c[8], zp[8], ym[8], yp[8], v[8];
     if (z0 > 0) {

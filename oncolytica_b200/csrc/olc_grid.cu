@@ -161,6 +161,9 @@ __global__ void __launch_bounds__(256) k_scan_hist(const olc_u32* __restrict__ h
 
 // One onesweep pass: stable partition of a tile of keys by one digit, tile
 // offsets by decoupled look-back, coalesced scatter through shared memory.
+// Blocks take tiles in order from a counter and loop until the rows are
+// covered, so the grid need not follow the capacity; a tile's predecessors are
+// always held by blocks that are already running.
 template <int IPT>
 __global__ void __launch_bounds__(SORT_THREADS) k_onesweep(const olc_u32* __restrict__ kin,
                                                            const olc_u32* __restrict__ vin,
@@ -183,79 +186,82 @@ __global__ void __launch_bounds__(SORT_THREADS) k_onesweep(const olc_u32* __rest
 
     const olc_u32 n = n_dev ? *n_dev : n_host;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
-    for (int i = tid; i < WARPS * RADIX; i += SORT_THREADS) (&s_whist[0][0])[i] = 0u;
-    __syncthreads();
-    const olc_u32 tile = s_tile;
-    const olc_u32 tile_start = tile * (olc_u32)TILE;
-    if (tile_start >= n) return;
-    const olc_u32 mask = (bits >= 32) ? 0xffffffffu : ((1u << bits) - 1u);
+    for (;;) {
+        if (tid == 0) s_tile = atomicAdd(tile_ctr, 1u);
+        for (int i = tid; i < WARPS * RADIX; i += SORT_THREADS) (&s_whist[0][0])[i] = 0u;
+        __syncthreads();
+        const olc_u32 tile = s_tile;
+        if ((olc_u64)tile * TILE >= n) return;
+        const olc_u32 tile_start = tile * (olc_u32)TILE;
+        const olc_u32 mask = (bits >= 32) ? 0xffffffffu : ((1u << bits) - 1u);
 
-    olc_u32 keys[IPT], vals[IPT], ranks[IPT];
-    const olc_u32 wbase = tile_start + (olc_u32)warp * (32u * IPT);
+        olc_u32 keys[IPT], vals[IPT], ranks[IPT];
+        const olc_u32 wbase = tile_start + (olc_u32)warp * (32u * IPT);
 #pragma unroll
-    for (int j = 0; j < IPT; ++j) {
-        olc_u32 idx = wbase + (olc_u32)j * 32u + (olc_u32)lane;
-        if (idx < n) {
-            keys[j] = kin[idx];
-            vals[j] = vin ? vin[idx] : idx;
-        } else {
-            keys[j] = 0xffffffffu;
-            vals[j] = 0u;
+        for (int j = 0; j < IPT; ++j) {
+            olc_u32 idx = wbase + (olc_u32)j * 32u + (olc_u32)lane;
+            if (idx < n) {
+                keys[j] = kin[idx];
+                vals[j] = vin ? vin[idx] : idx;
+            } else {
+                keys[j] = 0xffffffffu;
+                vals[j] = 0u;
+            }
         }
-    }
-    const olc_u32 lt_mask = (1u << lane) - 1u;
+        const olc_u32 lt_mask = (1u << lane) - 1u;
 #pragma unroll
-    for (int j = 0; j < IPT; ++j) {
-        olc_u32 idx = wbase + (olc_u32)j * 32u + (olc_u32)lane;
-        bool valid = idx < n;
-        olc_u32 d = valid ? ((keys[j] >> shift) & mask) : (0x100u + (olc_u32)lane);
-        olc_u32 peers = __match_any_sync(0xffffffffu, d);
-        olc_u32 before = __popc(peers & lt_mask);
-        olc_u32 b = valid ? s_whist[warp][d] : 0u;
-        __syncwarp();
-        if (valid && before == 0u) s_whist[warp][d] = b + (olc_u32)__popc(peers);
-        __syncwarp();
-        ranks[j] = b + before;
-    }
-    __syncthreads();
+        for (int j = 0; j < IPT; ++j) {
+            olc_u32 idx = wbase + (olc_u32)j * 32u + (olc_u32)lane;
+            bool valid = idx < n;
+            olc_u32 d = valid ? ((keys[j] >> shift) & mask) : (0x100u + (olc_u32)lane);
+            olc_u32 peers = __match_any_sync(0xffffffffu, d);
+            olc_u32 before = __popc(peers & lt_mask);
+            olc_u32 b = valid ? s_whist[warp][d] : 0u;
+            __syncwarp();
+            if (valid && before == 0u) s_whist[warp][d] = b + (olc_u32)__popc(peers);
+            __syncwarp();
+            ranks[j] = b + before;
+        }
+        __syncthreads();
 
-    // thread == digit: per-warp exclusive offsets and the tile's digit count
-    olc_u32 total = 0;
+        // thread == digit: per-warp exclusive offsets and the tile's digit count
+        olc_u32 total = 0;
 #pragma unroll
-    for (int w = 0; w < WARPS; ++w) {
-        olc_u32 c = s_whist[w][tid];
-        s_whist[w][tid] = total;
-        total += c;
-    }
-    olc_u32 excl = olc_lookback(lookback + tid, RADIX, tile, total, status);
-    olc_u32 local_off = block_excl_scan256(total, s_w);
-    s_off[tid] = local_off;
-    s_gbase[tid] = base[tid] + excl - local_off;
-    __syncthreads();
+        for (int w = 0; w < WARPS; ++w) {
+            olc_u32 c = s_whist[w][tid];
+            s_whist[w][tid] = total;
+            total += c;
+        }
+        olc_u32 excl = olc_lookback(lookback + tid, RADIX, tile, total, status);
+        olc_u32 local_off = block_excl_scan256(total, s_w);
+        s_off[tid] = local_off;
+        s_gbase[tid] = base[tid] + excl - local_off;
+        __syncthreads();
 
 #pragma unroll
-    for (int j = 0; j < IPT; ++j) {
-        olc_u32 idx = wbase + (olc_u32)j * 32u + (olc_u32)lane;
-        if (idx < n) {
-            olc_u32 d = (keys[j] >> shift) & mask;
-            olc_u32 pos = s_off[d] + s_whist[warp][d] + ranks[j];
-            s_keys[pos] = keys[j];
-            s_vals[pos] = vals[j];
+        for (int j = 0; j < IPT; ++j) {
+            olc_u32 idx = wbase + (olc_u32)j * 32u + (olc_u32)lane;
+            if (idx < n) {
+                olc_u32 d = (keys[j] >> shift) & mask;
+                olc_u32 pos = s_off[d] + s_whist[warp][d] + ranks[j];
+                s_keys[pos] = keys[j];
+                s_vals[pos] = vals[j];
+            }
         }
-    }
-    __syncthreads();
-    const olc_u32 tile_n = min((olc_u32)TILE, n - tile_start);
-    for (olc_u32 i = tid; i < tile_n; i += SORT_THREADS) {
-        olc_u32 k = s_keys[i];
-        olc_u32 d = (k >> shift) & mask;
-        olc_u32 o = s_gbase[d] + i;
-        // Offsets are exact unless a look-back wait gave up (status flagged);
-        // the bound keeps even that case inside the output.
-        if (o < n) {
-            kout[o] = k;
-            vout[o] = s_vals[i];
+        __syncthreads();
+        const olc_u32 tile_n = min((olc_u32)TILE, n - tile_start);
+        for (olc_u32 i = tid; i < tile_n; i += SORT_THREADS) {
+            olc_u32 k = s_keys[i];
+            olc_u32 d = (k >> shift) & mask;
+            olc_u32 o = s_gbase[d] + i;
+            // Offsets are exact unless a look-back wait gave up (status flagged);
+            // the bound keeps even that case inside the output.
+            if (o < n) {
+                kout[o] = k;
+                vout[o] = s_vals[i];
+            }
         }
+        __syncthreads();  // shared tiles are reused by the block's next tile
     }
 }
 
@@ -330,6 +336,7 @@ void launch_onesweep(const olc_u32* kin, const olc_u32* vin, olc_u32* kout, olc_
                      cudaStream_t s) {
     unsigned tiles = (n_cap + SORT_TILE - 1) / SORT_TILE;
     if (tiles == 0) tiles = 1;
+    if (tiles > sm_count() * 8) tiles = sm_count() * 8;
     k_onesweep<SORT_IPT><<<tiles, SORT_THREADS, 0, s>>>(kin, vin, kout, vout, n_dev, n_host, shift, bits,
                                                          base, lookback, tile_ctr, status);
 }
@@ -371,18 +378,34 @@ bool carve_sort_scratch(void* base, size_t bytes, olc_u32 n_cap, int key_bits, S
     return true;
 }
 
+// Zeroes the look-back words of the tiles rows [0, *n_dev) occupy in every
+// pass (the work follows the rows in use, not the capacity).
+__global__ void __launch_bounds__(256) k_clear_lookback(uint4* lookback, const olc_u32* n_dev, int passes,
+                                                        size_t tiles_cap) {
+    const size_t used = ((size_t)*n_dev + SORT_TILE - 1) / SORT_TILE;
+    const size_t vecs = used * (RADIX / 4), stride = tiles_cap * (RADIX / 4);
+    for (int p = 0; p < passes; ++p)
+        for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < vecs; i += (size_t)gridDim.x * blockDim.x)
+            lookback[p * stride + i] = make_uint4(0u, 0u, 0u, 0u);
+}
+
 void run_sort(const olc_u32* kin, const olc_u32* vin, olc_u32* kout, olc_u32* vout, const olc_u32* n_dev,
               olc_u32 n_host, olc_u32 n_cap, int key_bits, const SortScratch& sc, bool hist_ready,
               olc_u32* counters, olc_u32 capacity, cudaStream_t s) {
     const int passes = (key_bits + 7) / 8;
     const size_t tiles = (n_cap + SORT_TILE - 1) / SORT_TILE ? (n_cap + SORT_TILE - 1) / SORT_TILE : 1;
-    cudaMemsetAsync(sc.lookback, 0, (size_t)passes * tiles * RADIX * 4, s);
+    // with the row count on the device (committed by the scan below), only the
+    // tiles in use are cleared
+    const bool rows_on_device = counters && n_dev;
+    if (!rows_on_device) cudaMemsetAsync(sc.lookback, 0, (size_t)passes * tiles * RADIX * 4, s);
     if (!hist_ready) {
         cudaMemsetAsync(sc.hist, 0, MAX_PASSES * RADIX * 4, s);
         launch_digit_hist(kin, n_dev, n_host, n_cap, sc.hist, passes, s);
     }
     launch_scan_hist(sc.hist, sc.base, passes, counters ? counters + OLC_CTR_SORT_TILE : sc.tile_ctr,
                      counters, capacity, s);
+    if (rows_on_device)
+        k_clear_lookback<<<sm_count() * 4, 256, 0, s>>>(reinterpret_cast<uint4*>(sc.lookback), n_dev, passes, tiles);
     const olc_u32* ck = kin;
     const olc_u32* cv = vin;
     for (int p = 0; p < passes; ++p) {

@@ -234,4 +234,22 @@ void launch_reduce_field_batch16(const BatchArgs& b, int storage, const uint4* t
                                  int n_fields, const unsigned char* fpar, const void* fa, const void* fb,
                                  const float* comp, OlcReductions* out, cudaStream_t s);
 
+// ------------------------------------------------------------------ serving pool (olc_pool.cu)
+// Column pointer sets of the row kernels; every column holds 4-byte elements.
+struct PoolCols {
+    const void* src[OLC_MAX_AGENT_COLS];
+    void* dst[OLC_MAX_AGENT_COLS];  // gather: null columns are skipped
+    int ncols;
+    int sim_col;                    // append: this column is written with the slot
+};
+constexpr olc_u32 POOL_GATHER_BLOCKS = 592;  // 4 per SM; the scan takes <= 1024 block counts
+constexpr olc_u32 POOL_TABLE_CHUNK = 8192;    // bin-table entries cleared per block
+void launch_clear_table_chunks(const uint2* chunks, olc_u32 n_chunks, olc_u32* ranges, cudaStream_t s);
+void launch_pool_append(const PoolCols& cols, olc_u32 n, olc_u32 slot, unsigned char* life, olc_u32* counters,
+                        olc_u32 capacity, cudaStream_t s);
+void launch_pool_retire(const olc_u32* sim, unsigned char* life, const olc_u32* counters, olc_u32 n_cap,
+                        olc_u32 slot, cudaStream_t s);
+void launch_pool_gather(const PoolCols& cols, const olc_u32* sim, const unsigned char* life, const olc_u32* counters,
+                        olc_u32 slot, olc_u32* block_counts, olc_u32* count_out, olc_u32 max_rows, cudaStream_t s);
+
 }  // namespace olc

@@ -51,6 +51,7 @@ struct OlcSimDesc {
     olc_u32 params_off;            // bytes into the params blob
     olc_u32 metrics_off;           // bytes into the metric accumulators
     olc_u32 substeps_mask;         // bit f: field f takes an odd number of substeps
+    olc_u32 step_base;             // handle steps run before this simulation joined (serving pool)
     unsigned long long field_off;  // first voxel of this simulation in every field buffer
 };
 

@@ -12,6 +12,7 @@
 //   5. reductions and metric rules when collect != 0
 // Everything is enqueued on one stream; no host synchronisation.
 #include "olc_internal.h"
+#include "olc_arena.h"
 
 #include <nvrtc.h>
 
@@ -131,6 +132,26 @@ struct OlcSim {
     OlcReductions* red_batch_dev = nullptr;
     OlcReductions* red_batch_host = nullptr;          // pinned
     size_t params_stride = 0;
+
+    // serving pool (pool == true): a batch whose members join and leave
+    // between steps; n_sims is the slot count
+    bool pool = false;
+    RangeArena table_arena, field_arena;
+    std::vector<unsigned char> slot_used;
+    std::vector<olc_u64> slot_table_off, slot_table_n, slot_field_off, slot_field_n;
+    olc_u32 slots_used = 0;
+    bool pool_dirty = false;                          // records / tiles changed since the last upload
+    uint64_t pool_steps = 0;                          // steps run on the pool
+    std::vector<unsigned char> params_all;            // host copy of every slot's Params
+    unsigned char* stage_host[2] = {};                // pinned upload staging, alternating
+    size_t stage_cap[2] = {};
+    cudaEvent_t stage_ev[2] = {};
+    int stage_i = 0;
+    size_t tiles_cap = 0;                             // tiles held by btiles_all / btiles_field[f]
+    olc_u32* gather_counts = nullptr;                 // POOL_GATHER_BLOCKS words
+    uint2* table_chunks = nullptr;                    // bin-table ranges of the members, cleared each step
+    olc_u32 n_table_chunks = 0;
+    size_t table_chunks_cap = 0;
 
     // CUDA graphs of whole steps, keyed by the buffer parities at step start
     bool use_graphs = false;
@@ -472,7 +493,11 @@ int step_once_batch(OlcSim* s, int collect, cudaStream_t st) {
                       s->life, s->counters, cap, s->keys_in, s->sc.hist, passes, s->counters + OLC_CTR_DEAD_TMP, st);
     run_sort(s->keys_in, nullptr, s->keys, s->vals, s->counters + OLC_CTR_ROWS, 0, cap, s->key_bits, s->sc, true,
              s->counters, cap, st);
-    OLC_TRY(check(s, cudaMemsetAsync(s->ranges, 0, (size_t)s->n_table * 8, st), "memset ranges"));
+    if (s->pool) {
+        launch_clear_table_chunks(s->table_chunks, s->n_table_chunks, s->ranges, st);
+    } else {
+        OLC_TRY(check(s, cudaMemsetAsync(s->ranges, 0, (size_t)s->n_table * 8, st), "memset ranges"));
+    }
     launch_bin_ranges_batch(B, s->keys, s->counters + OLC_CTR_ROWS, cap, s->ranges, st);
     PermuteArgs pa;
     std::memset(&pa, 0, sizeof(pa));
@@ -589,6 +614,15 @@ void drop_graphs(OlcSim* s) {
     s->graph_seen.clear();
 }
 
+// Without the device synchronisation: an executable graph destroyed while in
+// flight is released when it completes.  For membership changes of a pool,
+// whose buffers stay allocated.
+void drop_graphs_nosync(OlcSim* s) {
+    for (auto& g : s->graphs) cudaGraphExecDestroy(g.exec);
+    s->graphs.clear();
+    s->graph_seen.clear();
+}
+
 // One step through a cached CUDA graph.  A step's launches depend only on the
 // bindings and on the buffer parities at its start (agent buffer, one bit per
 // field) plus `collect`, so graphs are cached by that state; the parity pattern
@@ -642,6 +676,134 @@ int step_graph(OlcSim* s, int collect, cudaStream_t st) {
     set_field_mask(s, g->field_after);
     s->total_launches += g->launches;
     s->steps++;
+    return OLC_OK;
+}
+
+// ------------------------------------------------------------------ serving pool
+// Field tiles of one member (slot, tile x, tile y, tile z), x fastest.
+void pool_tiles(const OlcGeom& g, olc_u32 slot, std::vector<uint4>* out) {
+    const int tx = (g.chem_dims[0] + BATCH_TILE_X - 1) / BATCH_TILE_X;
+    const int ty = (g.chem_dims[1] + BATCH_TILE_Y - 1) / BATCH_TILE_Y;
+    const int tz = (g.chem_dims[2] + BATCH_TILE_Z - 1) / BATCH_TILE_Z;
+    for (int z = 0; z < tz; ++z)
+        for (int y = 0; y < ty; ++y)
+            for (int x = 0; x < tx; ++x) out->push_back(make_uint4(slot, (unsigned)x, (unsigned)y, (unsigned)z));
+}
+
+int pool_grow_tiles(OlcSim* s, size_t need, cudaStream_t st) {
+    if (need <= s->tiles_cap) return OLC_OK;
+    OLC_TRY(check(s, cudaStreamSynchronize(st), "sync before tile-list growth"));
+    const size_t cap = std::max<size_t>(need + need / 2, 4096);
+    cudaFree(s->btiles_all);
+    s->btiles_all = nullptr;
+    OLC_TRY(dev_alloc(s, &s->btiles_all, cap * sizeof(uint4), "field tiles"));
+    for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
+        cudaFree(s->btiles_field[f]);
+        s->btiles_field[f] = nullptr;
+        OLC_TRY(dev_alloc(s, &s->btiles_field[f], cap * sizeof(uint4), "field tiles"));
+    }
+    s->tiles_cap = cap;
+    return OLC_OK;
+}
+
+// Uploads the member records, field steps, Params and tile lists of the
+// current membership (stream-ordered before the next step's kernels) through
+// one of two pinned staging buffers.
+int pool_commit(OlcSim* s, cudaStream_t st) {
+    const olc_u32 F = s->caps.n_fields;
+    std::vector<uint4> all;
+    std::vector<uint2> chunks;
+    std::vector<std::vector<uint4>> per_slot(s->n_sims);
+    for (olc_u32 k = 0; k < s->n_sims; ++k) {
+        if (!s->slot_used[k]) continue;
+        pool_tiles(s->geoms[k], k, &per_slot[k]);
+        all.insert(all.end(), per_slot[k].begin(), per_slot[k].end());
+        for (olc_u64 e = 0; e < s->slot_table_n[k]; e += POOL_TABLE_CHUNK)
+            chunks.push_back(make_uint2((unsigned)(s->slot_table_off[k] + e),
+                                        (unsigned)std::min<olc_u64>(POOL_TABLE_CHUNK, s->slot_table_n[k] - e)));
+    }
+    if (chunks.size() > s->table_chunks_cap) return fail(s, OLC_ERR_STATE, "pool: bin-table chunk list overflow");
+    std::vector<uint4> fl[OLC_MAX_FIELDS];
+    std::vector<olc_u32> counts[OLC_MAX_FIELDS];
+    for (olc_u32 f = 0; f < F; ++f) {
+        if (!s->field_bound[f]) continue;
+        std::vector<std::pair<int, olc_u32>> order;  // (substeps, slot), most substeps first, slots ascending
+        for (olc_u32 k = 0; k < s->n_sims; ++k)
+            if (s->slot_used[k]) order.push_back({s->bsteps_host[(size_t)k * F + f].substeps, k});
+        std::stable_sort(order.begin(), order.end(), [](const std::pair<int, olc_u32>& x,
+                                                        const std::pair<int, olc_u32>& y) { return x.first > y.first; });
+        std::vector<int> steps_of;
+        for (const auto& o : order)
+            for (const uint4& t : per_slot[o.second]) {
+                fl[f].push_back(t);
+                steps_of.push_back(o.first);
+            }
+        const int max_s = order.empty() ? 0 : order.front().first;
+        counts[f].assign(max_s, 0u);
+        olc_u32 c = (olc_u32)fl[f].size();
+        for (int sub = 0; sub < max_s; ++sub) {  // tiles of members taking more than `sub` substeps
+            while (c > 0 && steps_of[c - 1] <= sub) --c;
+            counts[f][sub] = c;
+        }
+    }
+    OLC_TRY(pool_grow_tiles(s, std::max<size_t>(all.size(), 1), st));
+    auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
+    const size_t n_desc = sizeof(OlcSimDesc) * s->n_sims;
+    const size_t n_steps = sizeof(FieldStep) * s->bsteps_host.size();
+    const size_t n_params = s->params_all.size();
+    size_t off = 0;
+    const size_t o_desc = off;
+    off = al(off + n_desc);
+    const size_t o_steps = off;
+    off = al(off + n_steps);
+    const size_t o_params = off;
+    off = al(off + n_params);
+    const size_t o_all = off;
+    off = al(off + all.size() * sizeof(uint4));
+    const size_t o_chunks = off;
+    off = al(off + chunks.size() * sizeof(uint2));
+    size_t o_f[OLC_MAX_FIELDS] = {};
+    for (olc_u32 f = 0; f < F; ++f) {
+        o_f[f] = off;
+        off = al(off + fl[f].size() * sizeof(uint4));
+    }
+    const int i = s->stage_i;
+    if (s->stage_ev[i]) OLC_TRY(check(s, cudaEventSynchronize(s->stage_ev[i]), "staging reuse"));
+    if (s->stage_cap[i] < off) {
+        if (s->stage_host[i]) cudaFreeHost(s->stage_host[i]);
+        s->stage_host[i] = nullptr;
+        s->stage_cap[i] = 0;
+        const size_t cap = off + off / 2;
+        OLC_TRY(check(s, cudaMallocHost(reinterpret_cast<void**>(&s->stage_host[i]), cap), "pinned staging"));
+        s->stage_cap[i] = cap;
+    }
+    unsigned char* h = s->stage_host[i];
+    std::memcpy(h + o_desc, s->desc_host.data(), n_desc);
+    std::memcpy(h + o_steps, s->bsteps_host.data(), n_steps);
+    if (n_params) std::memcpy(h + o_params, s->params_all.data(), n_params);
+    if (!all.empty()) std::memcpy(h + o_all, all.data(), all.size() * sizeof(uint4));
+    if (!chunks.empty()) std::memcpy(h + o_chunks, chunks.data(), chunks.size() * sizeof(uint2));
+    for (olc_u32 f = 0; f < F; ++f)
+        if (!fl[f].empty()) std::memcpy(h + o_f[f], fl[f].data(), fl[f].size() * sizeof(uint4));
+    auto up = [&](void* dst, size_t o, size_t n, const char* what) {
+        return n ? check(s, cudaMemcpyAsync(dst, h + o, n, cudaMemcpyHostToDevice, st), what) : OLC_OK;
+    };
+    OLC_TRY(up(s->desc_dev, o_desc, n_desc, "upload member records"));
+    OLC_TRY(up(s->bsteps_dev, o_steps, n_steps, "upload field steps"));
+    OLC_TRY(up(s->params_dev, o_params, n_params, "upload params"));
+    OLC_TRY(up(s->btiles_all, o_all, all.size() * sizeof(uint4), "upload field tiles"));
+    OLC_TRY(up(s->table_chunks, o_chunks, chunks.size() * sizeof(uint2), "upload bin-table chunks"));
+    for (olc_u32 f = 0; f < F; ++f)
+        if (s->field_bound[f]) OLC_TRY(up(s->btiles_field[f], o_f[f], fl[f].size() * sizeof(uint4), "upload tiles"));
+    if (!s->stage_ev[i])
+        OLC_TRY(check(s, cudaEventCreateWithFlags(&s->stage_ev[i], cudaEventDisableTiming), "staging event"));
+    OLC_TRY(check(s, cudaEventRecord(s->stage_ev[i], st), "staging event"));
+    s->stage_i ^= 1;
+    s->n_btiles = (olc_u32)all.size();
+    s->n_table_chunks = (olc_u32)chunks.size();
+    for (olc_u32 f = 0; f < F; ++f) s->btile_count[f] = counts[f];
+    drop_graphs_nosync(s);
+    s->pool_dirty = false;
     return OLC_OK;
 }
 
@@ -834,7 +996,8 @@ int olc_create_batch(const OlcGeom* geoms, int n_sims, const OlcCaps* caps, OlcS
 
 int olc_batch_field_offsets(const OlcSim* s, uint64_t* offsets) {
     if (!s || !offsets) return fail(nullptr, OLC_ERR_ARG, "olc_batch_field_offsets: null argument");
-    if (!s->n_sims) return fail(const_cast<OlcSim*>(s), OLC_ERR_STATE, "olc_batch_field_offsets: not a batch handle");
+    if (!s->n_sims || s->pool)
+        return fail(const_cast<OlcSim*>(s), OLC_ERR_STATE, "olc_batch_field_offsets: not a batch handle");
     for (olc_u32 k = 0; k <= s->n_sims; ++k) offsets[k] = s->field_off[k];
     return OLC_OK;
 }
@@ -868,6 +1031,12 @@ int olc_destroy(OlcSim* s) {
     for (int f = 0; f < OLC_MAX_FIELDS; ++f) cudaFree(s->btiles_field[f]);
     cudaFree(s->red_batch_dev);
     if (s->red_batch_host) cudaFreeHost(s->red_batch_host);
+    cudaFree(s->gather_counts);
+    cudaFree(s->table_chunks);
+    for (int i = 0; i < 2; ++i) {
+        if (s->stage_host[i]) cudaFreeHost(s->stage_host[i]);
+        if (s->stage_ev[i]) cudaEventDestroy(s->stage_ev[i]);
+    }
     cudaFree(s->metrics_dev);
     if (s->params_host) cudaFreeHost(s->params_host);
     if (s->red_host) cudaFreeHost(s->red_host);
@@ -967,6 +1136,10 @@ int olc_set_contact(OlcSim* s, const OlcContact* c) {
                 s->desc_host[k].lo[i] = s->geoms[k].domain_lo[i] + c->margin;
                 s->desc_host[k].hi[i] = s->geoms[k].domain_hi[i] - c->margin;
             }
+        if (s->pool) {
+            s->pool_dirty = true;
+            return OLC_OK;
+        }
         return upload_desc(s);
     }
     return OLC_OK;
@@ -1085,6 +1258,10 @@ int olc_set_user_metrics_size(OlcSim* s, size_t bytes) {
     }
     if (s->n_sims) {
         for (olc_u32 k = 0; k < s->n_sims; ++k) s->desc_host[k].metrics_off = (olc_u32)(k * bytes);
+        if (s->pool) {
+            s->pool_dirty = true;
+            return OLC_OK;
+        }
         return upload_desc(s);
     }
     return OLC_OK;
@@ -1092,6 +1269,7 @@ int olc_set_user_metrics_size(OlcSim* s, size_t bytes) {
 
 int olc_set_agent_count(OlcSim* s, uint32_t n, void* stream) {
     if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (s->pool) return fail(s, OLC_ERR_STATE, "olc_set_agent_count: pools add rows with olc_pool_add_agents");
     if (n > s->caps.max_agents) return fail(s, OLC_ERR_CAPACITY, "olc_set_agent_count: n exceeds max_agents");
     for (olc_u32 c = 0; c < s->caps.n_agent_fields; ++c)
         if (!s->col[0][c]) return fail(s, OLC_ERR_STATE, "olc_set_agent_count: agent column not bound");
@@ -1141,6 +1319,10 @@ int olc_step(OlcSim* s, int nsteps, int collect, void* stream) {
     cudaStream_t st = as_stream(stream);
     for (int i = 0; i < nsteps; ++i) {
         const int c = (collect && i == nsteps - 1) ? 1 : 0;
+        if (s->pool) {
+            if (s->pool_dirty) OLC_TRY(pool_commit(s, st));
+            s->pool_steps++;
+        }
         if (s->use_graphs && !s->profiling) {
             OLC_TRY(step_graph(s, c, st));
         } else {
@@ -1235,7 +1417,7 @@ int olc_bind_field_batch(OlcSim* s, int index, void* a_, void* b_, float* sink, 
     float* a = static_cast<float*>(a_);
     float* b = static_cast<float*>(b_);
     if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
-    if (!s->n_sims) return fail(s, OLC_ERR_STATE, "olc_bind_field_batch: not a batch handle");
+    if (!s->n_sims || s->pool) return fail(s, OLC_ERR_STATE, "olc_bind_field_batch: not a batch handle");
     if (index < 0 || index >= (int)s->caps.n_fields || !a || !b || !specs)
         return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: bad index or null argument");
     const olc_u32 F = s->caps.n_fields;
@@ -1332,7 +1514,7 @@ int olc_read_field_parity(OlcSim* s, uint8_t* out, void* stream) {
 
 int olc_set_params_batch(OlcSim* s, const void* blob, size_t stride, void* stream) {
     if (!s || !blob || stride == 0) return fail(s, OLC_ERR_ARG, "olc_set_params_batch: bad arguments");
-    if (!s->n_sims) return fail(s, OLC_ERR_STATE, "olc_set_params_batch: not a batch handle");
+    if (!s->n_sims || s->pool) return fail(s, OLC_ERR_STATE, "olc_set_params_batch: not a batch handle");
     cudaStream_t st = as_stream(stream);
     const size_t bytes = stride * s->n_sims;
     if (bytes > s->params_cap || stride != s->params_stride) {
@@ -1381,6 +1563,354 @@ int olc_read_user_metrics_batch(OlcSim* s, void* out, size_t bytes_per_sim, void
     OLC_TRY(check(s, cudaMemcpyAsync(out, s->metrics_dev, bytes_per_sim * s->n_sims, cudaMemcpyDeviceToHost, st),
                   "metrics readback"));
     return check(s, cudaStreamSynchronize(st), "sync");
+}
+
+// ------------------------------------------------------------------ serving pool
+
+int olc_create_pool(const OlcPoolConfig* cfg, const OlcCaps* caps, OlcSim** out) {
+    if (!cfg || !caps || !out) return fail(nullptr, OLC_ERR_ARG, "olc_create_pool: null argument");
+    std::string err;
+    if (!caps_ok(caps, "olc_create_pool", &err)) return fail(nullptr, OLC_ERR_ARG, err);
+    if (cfg->max_slots < 1 || cfg->max_slots > (1u << 20))
+        return fail(nullptr, OLC_ERR_ARG, "olc_create_pool: max_slots must be in [1, 2^20]");
+    OlcGeom gmax = {};
+    for (int i = 0; i < 3; ++i) gmax.tissue_dims[i] = cfg->max_tissue_dims[i];
+    gmax.tissue_voxel_size = 1.0f;
+    if (!geom_ok(gmax, &err)) return fail(nullptr, OLC_ERR_ARG, "olc_create_pool: max_tissue_dims: " + err);
+    const olc_u32 top = olc_tissue_key(gmax.tissue_dims[0], gmax.tissue_dims[1], gmax.tissue_dims[2]);
+    const int shift = std::max(1, key_bits_for(top));
+    if (shift + key_bits_for(cfg->max_slots) > 32)
+        return fail(nullptr, OLC_ERR_ARG, "olc_create_pool: slot index and bin key exceed 32 key bits");
+    if (cfg->table_entries == 0 || cfg->table_entries >= (1ull << 31))
+        return fail(nullptr, OLC_ERR_ARG, "olc_create_pool: table_entries must be in [1, 2^31)");
+    if (caps->n_fields && cfg->field_voxels == 0)
+        return fail(nullptr, OLC_ERR_ARG, "olc_create_pool: field_voxels must be > 0 with fields");
+    OlcSim* s = new OlcSim();
+    const olc_u32 n = cfg->max_slots;
+    s->pool = true;
+    s->caps = *caps;
+    s->geom = gmax;
+    s->n_sims = n;
+    s->geoms.assign(n, OlcGeom{});
+    s->bins = make_bin_grid(gmax);
+    s->bargs.shift = shift;
+    s->bargs.n_sims = n;
+    s->bargs.sentinel = n << shift;
+    s->key_bits = key_bits_for(s->bargs.sentinel);
+    s->n_table = (olc_u32)cfg->table_entries;
+    s->desc_host.assign(n, OlcSimDesc{});
+    s->bsteps_host.assign((size_t)n * std::max<olc_u32>(1u, caps->n_fields), FieldStep{});
+    s->slot_used.assign(n, 0);
+    s->slot_table_off.assign(n, 0);
+    s->slot_table_n.assign(n, 0);
+    s->slot_field_off.assign(n, 0);
+    s->slot_field_n.assign(n, 0);
+    s->table_arena.reset(cfg->table_entries);
+    s->field_arena.reset(cfg->field_voxels);
+    int rc = alloc_common(s);
+    auto A = [&](int r) {
+        if (rc == OLC_OK) rc = r;
+    };
+    A(dev_alloc(s, &s->desc_dev, sizeof(OlcSimDesc) * n, "member records"));
+    A(dev_alloc(s, &s->cols_dev, sizeof(void*) * 2 * OLC_MAX_AGENT_COLS, "column tables"));
+    A(dev_alloc(s, &s->fpar_dev, (size_t)n * OLC_MAX_FIELDS, "field parity"));
+    A(dev_alloc(s, &s->bsteps_dev, sizeof(FieldStep) * s->bsteps_host.size(), "field steps"));
+    A(dev_alloc(s, &s->red_batch_dev, sizeof(OlcReductions) * n, "pool reductions"));
+    A(dev_alloc(s, &s->gather_counts, POOL_GATHER_BLOCKS * sizeof(olc_u32), "gather counts"));
+    // each member's range splits into at most n / CHUNK + 1 chunks
+    s->table_chunks_cap = (size_t)(cfg->table_entries / POOL_TABLE_CHUNK) + n + 1;
+    A(dev_alloc(s, &s->table_chunks, s->table_chunks_cap * sizeof(uint2), "bin-table chunks"));
+    A(check(s, cudaMallocHost(reinterpret_cast<void**>(&s->red_batch_host), sizeof(OlcReductions) * n),
+            "pinned pool reductions"));
+    if (rc == OLC_OK) {
+        A(check(s, cudaMemset(s->desc_dev, 0, sizeof(OlcSimDesc) * n), "memset member records"));
+        A(check(s, cudaMemset(s->fpar_dev, 0, (size_t)n * OLC_MAX_FIELDS), "memset field parity"));
+        A(check(s, cudaMemset(s->bsteps_dev, 0, sizeof(FieldStep) * s->bsteps_host.size()), "memset field steps"));
+        A(check(s, cudaMemset(s->red_batch_dev, 0, sizeof(OlcReductions) * n), "memset pool reductions"));
+    }
+    s->bargs.sims = s->desc_dev;
+    s->pool_dirty = true;
+    if (rc != OLC_OK) {
+        std::string msg = s->err;
+        olc_destroy(s);
+        return fail(nullptr, rc, msg);
+    }
+    *out = s;
+    return OLC_OK;
+}
+
+int olc_bind_field_pool(OlcSim* s, int index, void* a, void* b, float* sink, float* comp, int storage) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (!s->pool) return fail(s, OLC_ERR_STATE, "olc_bind_field_pool: not a pool");
+    if (index < 0 || index >= (int)s->caps.n_fields || !a || !b)
+        return fail(s, OLC_ERR_ARG, "olc_bind_field_pool: bad index or null buffer");
+    if (storage < OLC_FIELD_F32 || storage > OLC_FIELD_BF16_SR)
+        return fail(s, OLC_ERR_ARG, "olc_bind_field_pool: bad storage type");
+    if (storage != OLC_FIELD_F32 && !comp)
+        return fail(s, OLC_ERR_ARG, "olc_bind_field_pool: 16-bit storage needs a compensation buffer");
+    if (s->slots_used) return fail(s, OLC_ERR_STATE, "olc_bind_field_pool: bind fields before admitting members");
+    drop_graphs(s);
+    s->field[0][index] = static_cast<float*>(a);
+    s->field[1][index] = static_cast<float*>(b);
+    s->sink[index] = sink;
+    s->comp[index] = storage != OLC_FIELD_F32 ? comp : nullptr;
+    s->fstep[index] = FieldStep{};
+    s->fstep[index].storage = storage;
+    s->field_cur[index] = 0;
+    s->field_bound[index] = true;
+    s->pool_dirty = true;
+    return OLC_OK;
+}
+
+int olc_pool_admit(OlcSim* s, const OlcGeom* geom, const OlcDiffusion* specs, const void* params,
+                   size_t params_bytes, int32_t* slot_out, uint64_t* field_off_out, void* stream) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (!s->pool) return fail(s, OLC_ERR_STATE, "olc_pool_admit: not a pool");
+    if (!geom || !slot_out || !field_off_out || (s->caps.n_fields && !specs) || (params_bytes && !params))
+        return fail(s, OLC_ERR_ARG, "olc_pool_admit: null argument");
+    std::string err;
+    if (!geom_ok(*geom, &err)) return fail(s, OLC_ERR_ARG, "olc_pool_admit: " + err);
+    const olc_u32 top = olc_tissue_key(geom->tissue_dims[0], geom->tissue_dims[1], geom->tissue_dims[2]);
+    if (top >> s->bargs.shift) return fail(s, OLC_ERR_ARG, "olc_pool_admit: bin grid larger than max_tissue_dims");
+    const olc_u32 F = s->caps.n_fields;
+    const olc_u64 nvox = (olc_u64)geom->chem_dims[0] * geom->chem_dims[1] * geom->chem_dims[2];
+    FieldStep fs[OLC_MAX_FIELDS] = {};
+    for (olc_u32 f = 0; f < F; ++f) {
+        if (!s->field_bound[f]) return fail(s, OLC_ERR_STATE, "olc_pool_admit: bind every field before admitting");
+        const int storage = s->fstep[f].storage;
+        if (specs[f].storage != storage)
+            return fail(s, OLC_ERR_ARG, "olc_pool_admit: field " + std::to_string(f) + " storage differs from the pool's");
+        if (nvox == 0 || geom->chem_dims[0] % (storage == OLC_FIELD_F32 ? 4 : 8) != 0)
+            return fail(s, OLC_ERR_ARG, "olc_pool_admit: field x extent must be a multiple of 4 (8 for 16-bit storage)");
+        if (specs[f].substeps != 0) {
+            if (!make_field_step(specs[f], geom->chem_dims, geom->chem_voxel_size, s->caps.dt, &fs[f], &err))
+                return fail(s, OLC_ERR_ARG, "olc_pool_admit: field " + std::to_string(f) + ": " + err);
+        } else {
+            for (int i = 0; i < 3; ++i) fs[f].dims[i] = geom->chem_dims[i];
+            fs[f].storage = storage;
+        }
+    }
+    if (params_bytes && s->params_stride && params_bytes != s->params_stride)
+        return fail(s, OLC_ERR_ARG, "olc_pool_admit: every member's Params blob has the same size");
+    cudaStream_t st = as_stream(stream);
+    if (params_bytes && !s->params_stride) {
+        const size_t bytes = params_bytes * s->n_sims;
+        const size_t cap = (bytes + 255) & ~size_t(255);
+        OLC_TRY(dev_alloc(s, &s->params_dev, cap, "params"));
+        s->params_cap = cap;
+        s->params_stride = params_bytes;
+        s->params_all.assign(bytes, 0);
+    }
+    olc_u32 slot = 0;
+    while (slot < s->n_sims && s->slot_used[slot]) ++slot;
+    if (slot == s->n_sims) return fail(s, OLC_ERR_CAPACITY, "olc_pool_admit: no free slot");
+    const olc_u64 t_off = s->table_arena.alloc((olc_u64)top + 1u);
+    if (t_off == RangeArena::NONE) return fail(s, OLC_ERR_CAPACITY, "olc_pool_admit: bin-table arena full");
+    olc_u64 f_off = 0;
+    if (F) {
+        f_off = s->field_arena.alloc(nvox, 32);  // 128-byte aligned grids
+        if (f_off == RangeArena::NONE) {
+            s->table_arena.release(t_off, (olc_u64)top + 1u);
+            return fail(s, OLC_ERR_CAPACITY, "olc_pool_admit: field arena full");
+        }
+    }
+    OlcSimDesc& d = s->desc_host[slot];
+    std::memset(&d, 0, sizeof(d));
+    for (int i = 0; i < 3; ++i) {
+        d.tdims[i] = geom->tissue_dims[i];
+        d.cdims[i] = geom->chem_dims[i];
+        d.lo[i] = geom->domain_lo[i] + s->contact.margin;
+        d.hi[i] = geom->domain_hi[i] - s->contact.margin;
+        d.center[i] = 0.5f * (geom->domain_lo[i] + geom->domain_hi[i]);
+    }
+    d.tvs = geom->tissue_voxel_size;
+    d.cvs = geom->chem_voxel_size;
+    d.bin_width = s->caps.radial_bin_width > 0.0f ? s->caps.radial_bin_width : 1.0f;
+    d.ranges_base = (olc_u32)t_off;
+    d.params_off = (olc_u32)(slot * s->params_stride);
+    d.metrics_off = (olc_u32)(slot * s->metrics_bytes);
+    d.step_base = (olc_u32)s->pool_steps;
+    d.field_off = f_off;
+    s->geoms[slot] = *geom;
+    for (olc_u32 f = 0; f < F; ++f) s->bsteps_host[(size_t)slot * F + f] = fs[f];
+    if (params_bytes) std::memcpy(s->params_all.data() + (size_t)slot * s->params_stride, params, params_bytes);
+    // clear the member's per-slot device records and field side buffers
+    int rc = OLC_OK;
+    auto A = [&](int r) {
+        if (rc == OLC_OK) rc = r;
+    };
+    if (F) A(check(s, cudaMemsetAsync(s->fpar_dev + (size_t)slot * F, 0, F, st), "clear field parity"));
+    if (s->metrics_dev && s->metrics_bytes)
+        A(check(s, cudaMemsetAsync(static_cast<unsigned char*>(s->metrics_dev) + (size_t)slot * s->metrics_bytes, 0,
+                                   s->metrics_bytes, st),
+                "clear metrics"));
+    launch_reset_reductions_batch(s->red_batch_dev + slot, 1u, st);
+    for (olc_u32 f = 0; f < F; ++f) {
+        if (s->sink[f]) A(check(s, cudaMemsetAsync(s->sink[f] + f_off, 0, nvox * 4, st), "clear sink"));
+        if (s->comp[f]) A(check(s, cudaMemsetAsync(s->comp[f] + f_off, 0, nvox * 4, st), "clear residuals"));
+    }
+    A(check(s, cudaGetLastError(), "olc_pool_admit"));
+    if (rc != OLC_OK) {
+        s->table_arena.release(t_off, (olc_u64)top + 1u);
+        if (F) s->field_arena.release(f_off, nvox);
+        return rc;
+    }
+    s->slot_used[slot] = 1;
+    s->slot_table_off[slot] = t_off;
+    s->slot_table_n[slot] = (olc_u64)top + 1u;
+    s->slot_field_off[slot] = f_off;
+    s->slot_field_n[slot] = F ? nvox : 0;
+    s->slots_used++;
+    s->pool_dirty = true;
+    *slot_out = (int32_t)slot;
+    *field_off_out = f_off;
+    return OLC_OK;
+}
+
+static bool pool_slot_ok(OlcSim* s, int32_t slot, const char* who) {
+    if (!s->pool) {
+        fail(s, OLC_ERR_STATE, std::string(who) + ": not a pool");
+        return false;
+    }
+    if (slot < 0 || (olc_u32)slot >= s->n_sims || !s->slot_used[slot]) {
+        fail(s, OLC_ERR_ARG, std::string(who) + ": slot not in use");
+        return false;
+    }
+    return true;
+}
+
+int olc_pool_add_agents(OlcSim* s, int32_t slot, void* const* cols_dev, uint32_t n, void* stream) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (!pool_slot_ok(s, slot, "olc_pool_add_agents")) return s->pool ? OLC_ERR_ARG : OLC_ERR_STATE;
+    if (n == 0) return OLC_OK;
+    const int sim_col = (int)s->caps.n_agent_fields - 1;
+    PoolCols pc;
+    std::memset(&pc, 0, sizeof(pc));
+    pc.ncols = (int)s->caps.n_agent_fields;
+    pc.sim_col = sim_col;
+    for (int c = 0; c < pc.ncols; ++c) {
+        if (!s->col[s->agent_cur][c]) return fail(s, OLC_ERR_STATE, "olc_pool_add_agents: agent column not bound");
+        if (c != sim_col && (!cols_dev || !cols_dev[c]))
+            return fail(s, OLC_ERR_ARG, "olc_pool_add_agents: null source column");
+        pc.src[c] = c == sim_col ? nullptr : cols_dev[c];
+        pc.dst[c] = s->col[s->agent_cur][c];
+    }
+    cudaStream_t st = as_stream(stream);
+    launch_pool_append(pc, n, (olc_u32)slot, s->life, s->counters, s->caps.max_agents, st);
+    return check(s, cudaGetLastError(), "olc_pool_add_agents");
+}
+
+int olc_pool_gather(OlcSim* s, int32_t slot, void* const* dst_dev, uint32_t max_rows, uint32_t* count_dev,
+                    void* stream) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (!pool_slot_ok(s, slot, "olc_pool_gather")) return s->pool ? OLC_ERR_ARG : OLC_ERR_STATE;
+    if (!dst_dev || !count_dev) return fail(s, OLC_ERR_ARG, "olc_pool_gather: null argument");
+    const int sim_col = (int)s->caps.n_agent_fields - 1;
+    PoolCols pc;
+    std::memset(&pc, 0, sizeof(pc));
+    pc.ncols = (int)s->caps.n_agent_fields;
+    pc.sim_col = sim_col;
+    for (int c = 0; c < pc.ncols; ++c) {
+        pc.src[c] = s->col[s->agent_cur][c];
+        pc.dst[c] = c == sim_col ? nullptr : dst_dev[c];
+    }
+    cudaStream_t st = as_stream(stream);
+    launch_pool_gather(pc, static_cast<const olc_u32*>(s->col[s->agent_cur][sim_col]), s->life, s->counters,
+                       (olc_u32)slot, s->gather_counts, count_dev, max_rows, st);
+    return check(s, cudaGetLastError(), "olc_pool_gather");
+}
+
+int olc_pool_copy_results(OlcSim* s, int32_t slot, OlcReductions* red_host, void* metrics_host, void* stream) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (!pool_slot_ok(s, slot, "olc_pool_copy_results")) return s->pool ? OLC_ERR_ARG : OLC_ERR_STATE;
+    cudaStream_t st = as_stream(stream);
+    if (red_host)
+        OLC_TRY(check(s, cudaMemcpyAsync(red_host, s->red_batch_dev + slot, sizeof(OlcReductions),
+                                         cudaMemcpyDeviceToHost, st),
+                      "reductions readback"));
+    if (metrics_host && s->metrics_dev && s->metrics_bytes)
+        OLC_TRY(check(s, cudaMemcpyAsync(metrics_host,
+                                         static_cast<unsigned char*>(s->metrics_dev) + (size_t)slot * s->metrics_bytes,
+                                         s->metrics_bytes, cudaMemcpyDeviceToHost, st),
+                      "metrics readback"));
+    return OLC_OK;
+}
+
+int olc_pool_retire(OlcSim* s, int32_t slot, void* stream) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (!pool_slot_ok(s, slot, "olc_pool_retire")) return s->pool ? OLC_ERR_ARG : OLC_ERR_STATE;
+    const int sim_col = (int)s->caps.n_agent_fields - 1;
+    const void* simc = s->col[s->agent_cur][sim_col];
+    if (simc)
+        launch_pool_retire(static_cast<const olc_u32*>(simc), s->life, s->counters, s->caps.max_agents,
+                           (olc_u32)slot, as_stream(stream));
+    s->table_arena.release(s->slot_table_off[slot], s->slot_table_n[slot]);
+    if (s->slot_field_n[slot]) s->field_arena.release(s->slot_field_off[slot], s->slot_field_n[slot]);
+    const olc_u32 F = s->caps.n_fields;
+    for (olc_u32 f = 0; f < F; ++f) s->bsteps_host[(size_t)slot * F + f] = FieldStep{};
+    std::memset(&s->desc_host[slot], 0, sizeof(OlcSimDesc));
+    s->slot_used[slot] = 0;
+    s->slot_table_n[slot] = s->slot_field_n[slot] = 0;
+    s->slots_used--;
+    s->pool_dirty = true;
+    return check(s, cudaGetLastError(), "olc_pool_retire");
+}
+
+int olc_pool_usage(const OlcSim* s, OlcPoolUsage* out) {
+    if (!s || !out) return fail(nullptr, OLC_ERR_ARG, "olc_pool_usage: null argument");
+    if (!s->pool) return fail(const_cast<OlcSim*>(s), OLC_ERR_STATE, "olc_pool_usage: not a pool");
+    out->slots_used = s->slots_used;
+    out->max_slots = s->n_sims;
+    out->table_used = s->table_arena.used();
+    out->table_entries = s->table_arena.capacity();
+    out->table_largest_free = s->table_arena.largest_free();
+    out->field_used = s->field_arena.used();
+    out->field_voxels = s->field_arena.capacity();
+    out->field_largest_free = s->field_arena.largest_free();
+    return OLC_OK;
+}
+
+}  // extern "C"
+
+struct OlcArena {
+    olc::RangeArena a;
+};
+
+extern "C" {
+
+int olc_arena_create(uint64_t capacity, OlcArena** out) {
+    if (!out || capacity == 0) return fail(nullptr, OLC_ERR_ARG, "olc_arena_create: bad arguments");
+    *out = new OlcArena();
+    (*out)->a.reset(capacity);
+    return OLC_OK;
+}
+
+int olc_arena_alloc(OlcArena* arena, uint64_t n, uint64_t align, uint64_t* offset) {
+    if (!arena || !offset || n == 0 || align == 0 || (align & (align - 1)))
+        return fail(nullptr, OLC_ERR_ARG, "olc_arena_alloc: bad arguments (n > 0, align a power of two)");
+    const uint64_t off = arena->a.alloc(n, align);
+    if (off == RangeArena::NONE) return fail(nullptr, OLC_ERR_CAPACITY, "olc_arena_alloc: no free range fits");
+    *offset = off;
+    return OLC_OK;
+}
+
+int olc_arena_release(OlcArena* arena, uint64_t offset, uint64_t n) {
+    if (!arena) return fail(nullptr, OLC_ERR_ARG, "olc_arena_release: null arena");
+    if (!arena->a.release(offset, n)) return fail(nullptr, OLC_ERR_ARG, "olc_arena_release: range not allocated");
+    return OLC_OK;
+}
+
+int olc_arena_stats(const OlcArena* arena, uint64_t* used, uint64_t* largest_free, uint64_t* free_ranges) {
+    if (!arena) return fail(nullptr, OLC_ERR_ARG, "olc_arena_stats: null arena");
+    if (used) *used = arena->a.used();
+    if (largest_free) *largest_free = arena->a.largest_free();
+    if (free_ranges) *free_ranges = arena->a.free_ranges();
+    return OLC_OK;
+}
+
+int olc_arena_destroy(OlcArena* arena) {
+    delete arena;
+    return OLC_OK;
 }
 
 // ------------------------------------------------------------------ stages

@@ -247,6 +247,27 @@ def batched_specs(n_sims: int = 512, seed: int = 0, g_choices: tuple = (32, 48, 
     return out
 
 
+def serving_schedule(rate: float = 20.0, duration: float = 120.0, seed: int = 0, steps_range: tuple = (100, 1000),
+                     storage: str = "f32") -> list:
+    """Requests of the serving mix: a Poisson process of ``rate`` requests/s
+    over ``duration`` s; each request is one simulation drawn like a member of
+    the batched sweep (``batched_specs``) with a step count uniform in
+    ``steps_range`` and an agent capacity of 4 n + 4096 (its solo run's
+    max_agents, reserved on admission).  Returns (arrival s, spec, steps)
+    triples in arrival order, from numpy default_rng(seed)."""
+    rng = np.random.default_rng(seed)
+    times, t = [], 0.0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t > duration:
+            break
+        times.append(t)
+    specs = batched_specs(len(times), seed=seed + 7919) if times else []
+    steps = rng.integers(steps_range[0], steps_range[1] + 1, size=len(times))
+    return [(tt, replace(sp, storage=storage, capacity=4 * sp.n_agents + 4096, name=f"request_{k}"), int(n))
+            for k, (tt, sp, n) in enumerate(zip(times, specs, steps))]
+
+
 def scaled(spec: TumourSpec, **kw) -> TumourSpec:
     """A copy with some numbers changed (smaller test cases)."""
     out = replace(spec, **kw)

@@ -35,6 +35,23 @@ def test_struct_sizes_match_header_layout():
     assert C.sizeof(_lib.OlcContact) == 28
     assert C.sizeof(_lib.OlcCounters) == 40
     assert C.sizeof(_lib.OlcProfile) == 16 + 6 * 8
+    assert C.sizeof(_lib.OlcPoolConfig) == 4 + 12 + 8 + 8
+    assert C.sizeof(_lib.OlcPoolUsage) == 8 + 6 * 8
+
+
+def test_create_pool_rejects_bad_configs_without_a_gpu(olc):
+    caps = _lib.OlcCaps(max_agents=1024, n_agent_fields=4, n_fields=1, state_field=-1)
+    h = C.c_void_p()
+    cfg = _lib.OlcPoolConfig(max_slots=0, table_entries=4096, field_voxels=4096)
+    cfg.max_tissue_dims[:] = (16, 16, 16)
+    assert olc.olc_create_pool(C.byref(cfg), C.byref(caps), C.byref(h)) == _lib.OLC_ERR_ARG
+    cfg.max_slots = 1 << 20                     # 20 slot bits + 12 bin-key bits of 16^3 overflow 32
+    cfg.max_tissue_dims[:] = (32, 32, 32)
+    assert olc.olc_create_pool(C.byref(cfg), C.byref(caps), C.byref(h)) == _lib.OLC_ERR_ARG
+    assert "32 key bits" in _lib.last_error()
+    cfg.max_slots, cfg.field_voxels = 64, 0
+    assert olc.olc_create_pool(C.byref(cfg), C.byref(caps), C.byref(h)) == _lib.OLC_ERR_ARG
+    assert olc.olc_pool_admit(None, None, None, None, 0, None, None, None) == _lib.OLC_ERR_ARG
 
 
 def test_version_string(olc):
