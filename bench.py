@@ -518,7 +518,7 @@ def measure_batch(n_sims: int, steps: int, warmup: int, graphs: bool = True, sol
 
 
 def measure_serving(rate: float, duration: float, seed: int = 0, storage: str = "f32", solo_sample: int = 0,
-                    hbm_fraction: float = 0.3, max_slots: int = 2048) -> dict:
+                    hbm_fraction: float = 0.3, max_slots: int = 2048, depth: int = 6, prefetch: float = 0.5) -> dict:
     """The serving mix: requests drawn like sweep members (steps U{100..1000})
     arrive as a Poisson process at ``rate``/s for ``duration`` s and are served
     by one pool (continuous batching, admission by free HBM: the arenas take
@@ -548,7 +548,8 @@ def measure_serving(rate: float, duration: float, seed: int = 0, storage: str = 
     e, s = W.configure_engine(specs[0])
     warm.submit(SimRequest(e, s, 3, return_state=True))
     warm.drain()
-    pool = ServingPool(dev)
+    pool = ServingPool(dev, depth=depth)
+    dev.time_steps = True
 
     def factory(sp, n):
         return lambda: SimRequest(*W.configure_engine(sp), n, return_state=True)
@@ -557,25 +558,31 @@ def measure_serving(rate: float, duration: float, seed: int = 0, storage: str = 
     torch.cuda.synchronize()
     c0 = dev.counters()
     t0 = time.perf_counter()
-    results = pool.serve(arrivals)
+    results = pool.serve(arrivals, prefetch=prefetch)
     t1 = time.perf_counter()
     c1 = dev.counters()
+    busy = dev.device_seconds()
     done = [r for r in results if r.status == "done"]
     ttc = np.array([r.ttc for r in done]) if done else np.zeros(1)
     wait = np.array([r.admitted - r.arrival for r in done]) if done else np.zeros(1)
     wall = t1 - t0
     agent_steps = c1["agent_steps"] - c0["agent_steps"]
     vox = sum(r.voxel_updates for r in done)
-    statuses = {}
+    statuses, failed = {}, []
     for r in results:
         statuses[r.status] = statuses.get(r.status, 0) + 1
+        if r.status != "done" and len(failed) < 5:
+            _, sp, n = sched[r.request_id]
+            failed.append({"request": r.request_id, "status": r.status, "error": (r.error or "")[:160],
+                           "agents": sp.n_agents, "capacity": sp.capacity, "grid": sp.field_dims[0], "steps": n})
     out = {"rate_per_s": rate, "duration_s": duration, "requests": len(sched), "status": statuses,
            "storage": storage, "wall_s": wall, "steps_run": pool.steps_run, "ms_per_batch_step": 1e3 * wall / max(1, pool.steps_run),
            "ttc_p50_s": float(np.percentile(ttc, 50)), "ttc_p99_s": float(np.percentile(ttc, 99)),
            "ttc_mean_s": float(ttc.mean()), "ttc_max_s": float(ttc.max()),
            "queue_wait_p99_s": float(np.percentile(wait, 99)),
            "agent_steps_per_s": agent_steps / wall, "voxel_updates_per_s": vox / wall,
-           "max_resident": pool.max_resident, "device_status": c1["status"],
+           "max_resident": pool.max_resident, "device_status": c1["status"], "not_done": failed,
+           "device_busy_s": busy, "device_busy_frac": busy / wall, "depth": depth, "prefetch_s": prefetch,
            "arenas": {k: int(v) for k, v in plan.items()},
            "peak_usage": {k: int(v) for k, v in pool.peak_usage.items()},
            "hbm_fraction": hbm_fraction}

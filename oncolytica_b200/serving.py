@@ -58,6 +58,7 @@ class SimRequest:
     return_state: bool = True
     request_id: int = -1
     arrival: float | None = None   # clock time of submission (set by submit when None)
+    _payload: Any = field(default=None, repr=False, compare=False)  # host half of the admission
 
 
 @dataclass
@@ -287,18 +288,41 @@ class ServingPool:
         return out
 
     def serve(self, arrivals: Sequence[tuple[float, Callable[[], SimRequest]]],
-              on_result: Callable[[SimResult], None] | None = None) -> list[SimResult]:
+              on_result: Callable[[SimResult], None] | None = None, prefetch: float = 0.0,
+              workers: int = 2) -> list[SimResult]:
         """Replays an arrival schedule in real time: ``arrivals`` holds
         (seconds after start, request factory) in time order; each request is
-        built and submitted when its time comes (its arrival is the scheduled
-        time).  Returns every result once all have finished."""
+        submitted when its time comes (its arrival is the scheduled time).
+        With ``prefetch`` > 0, worker threads build the requests (the factory
+        and the device's host-side ``prepare``) up to that many seconds ahead,
+        as clients would send them ready-made.  Returns every result once all
+        have finished."""
+        import concurrent.futures as cf
+
+        ex = cf.ThreadPoolExecutor(max(1, workers)) if prefetch > 0 else None
+        futures: dict[int, Any] = {}
+        prep = getattr(self.device, "prepare", None)
+
+        def build(j: int) -> SimRequest:
+            req = arrivals[j][1]()
+            if prep is not None:
+                try:
+                    prep(req)
+                except RequestError:
+                    pass  # rejected on admission with the same message
+            return req
+
         t0 = self.clock()
-        i, idle = 0, 0
+        i, idle, ahead = 0, 0, 0
         out: list[SimResult] = []
         while i < len(arrivals) or not self.idle:
             now = self.clock()
+            if ex is not None:
+                while ahead < len(arrivals) and t0 + arrivals[ahead][0] <= now + prefetch:
+                    futures[ahead] = ex.submit(build, ahead)
+                    ahead += 1
             while i < len(arrivals) and t0 + arrivals[i][0] <= now:
-                req = arrivals[i][1]()
+                req = futures.pop(i).result() if i in futures else arrivals[i][1]()
                 req.arrival = t0 + arrivals[i][0]
                 self.submit(req)
                 if req.request_id in self.results:
@@ -307,9 +331,11 @@ class ServingPool:
             got = self.step()
             idle = self._unstick(idle)
             if self.idle and i < len(arrivals):
-                time.sleep(max(0.0, t0 + arrivals[i][0] - self.clock()))
+                time.sleep(max(0.0, min(t0 + arrivals[i][0] - self.clock(), 0.05)))
             out += got
         out += self.poll(wait=True)
+        if ex is not None:
+            ex.shutdown(wait=True)
         if on_result is not None:
             for r in out:
                 on_result(r)
@@ -381,6 +407,8 @@ class PoolDevice:
         self.max_slots, self.max_rows = int(max_slots), int(max_rows)
         self.table_entries, self.field_voxels = int(table_entries), int(field_voxels)
         self.max_tissue_dims = tuple(int(v) for v in max_tissue_dims)
+        self.time_steps = False
+        self.step_events: list = []
         self._build(eng, sim)
         self.set_graphs(graphs)
 
@@ -505,7 +533,13 @@ class PoolDevice:
         if int(e.max_agents) < 1:
             raise RequestError("max_agents must be >= 1")
 
-    def admit(self, req: SimRequest) -> _Member:
+    def prepare(self, req: SimRequest) -> None:
+        """Host half of an admission, safe to run on another thread ahead of
+        time: model checks, agent columns (RNG states seeded as in a solo
+        run) and initial grids (faces pinned to the boundary, x fastest) in
+        pinned host memory, diffusion specs and the Params blob."""
+        if getattr(req, "_payload", None) is not None:
+            return
         torch = self.torch
         e, sim = req.engine, req.sim
         e._prepare_model(sim)
@@ -529,51 +563,69 @@ class PoolDevice:
                 sp.substeps = e.substeps_for(name)
                 sp.has_sink = int(name in self.sinks)
                 substeps.append(int(sp.substeps))
+        rng = cols.get("_rng_state", np.zeros(n, np.uint32)).astype(np.uint32)
+        zero = rng == 0
+        if zero.any():
+            rng = rng.copy()
+            rng[zero] = seed_rng(e.seed, np.nonzero(zero)[0].astype(np.uint32))
+        agents = {}
+        if n:
+            for i, (col, _, dt) in enumerate(L.cell_cols):
+                if col == "_sim":
+                    continue
+                host = rng if col == "_rng_state" else np.asarray(cols[col]).astype(dt)
+                arr = np.ascontiguousarray(host).view(np.int32 if dt != np.float32 else np.float32)
+                agents[i] = torch.from_numpy(arr).pin_memory()
+        fields = []
+        for i, name in enumerate(L.chem_fields):
+            host = np.asarray(e.chemistry.column(name), dtype=np.float32)
+            d = e._diffusion.get(name)
+            pin = torch.empty(host.size, dtype=torch.float32, pin_memory=True)
+            flat = pin.numpy()
+            out = flat.reshape(host.shape, order="F")  # x fastest, written in place
+            if not np.shares_memory(out, flat):
+                raise RuntimeError("pinned field staging is not a view")
+            out[...] = host
+            if d is not None:
+                b = np.float32(d.boundary)
+                out[0, :, :] = out[-1, :, :] = b
+                out[:, 0, :] = out[:, -1, :] = b
+                out[:, :, 0] = out[:, :, -1] = b
+            fields.append(pin)
         blob = pack_params(L, sim._params)
-        buf = C.create_string_buffer(blob, len(blob))
+        req._payload = {"n": n, "specs": specs, "substeps": tuple(substeps), "agents": agents, "fields": fields,
+                        "blob": blob, "geom": _geom_of(e), "nvox": int(np.prod(e.chemistry_shape)) if nf else 0}
+
+    def admit(self, req: SimRequest) -> _Member:
+        """Device half of an admission: a slot and arena ranges, then the
+        agents appended and the initial grids written, all on the pool's
+        stream.  CapacityError (nothing taken) when the pool is full."""
+        torch = self.torch
+        self.prepare(req)
+        P = req._payload
+        L = self.layout
+        buf = C.create_string_buffer(P["blob"], len(P["blob"]))
         slot, foff = C.c_int32(), C.c_uint64()
-        rc = self.lib.olc_pool_admit(self.handle, C.byref(_geom_of(e)), specs, C.cast(buf, C.c_void_p), len(blob),
-                                     C.byref(slot), C.byref(foff), self._s())
+        rc = self.lib.olc_pool_admit(self.handle, C.byref(P["geom"]), P["specs"], C.cast(buf, C.c_void_p),
+                                     len(P["blob"]), C.byref(slot), C.byref(foff), self._s())
         if rc == _lib.OLC_ERR_CAPACITY:
             raise CapacityError(_lib.last_error(self.handle))
         if rc == _lib.OLC_ERR_ARG:
             raise RequestError(_lib.last_error(self.handle))
         self._check(rc)
-        nvox = int(np.prod(e.chemistry_shape)) if nf else 0
-        m = _Member(int(slot.value), int(foff.value), nvox, tuple(substeps))
+        n, nvox = P["n"], P["nvox"]
+        m = _Member(int(slot.value), int(foff.value), nvox, P["substeps"])
         with torch.cuda.stream(self.stream):
-            # agents: host -> pinned -> device staging -> appended rows of the slot
-            rng = cols.get("_rng_state", np.zeros(n, np.uint32)).astype(np.uint32)
-            zero = rng == 0
-            if zero.any():
-                rng = rng.copy()
-                rng[zero] = seed_rng(e.seed, np.nonzero(zero)[0].astype(np.uint32))
-            ptrs = (C.c_void_p * len(L.cell_cols))()
             keep = []
             if n:
-                for i, (col, _, dt) in enumerate(L.cell_cols):
-                    if col == "_sim":
-                        continue
-                    host = rng if col == "_rng_state" else np.asarray(cols[col]).astype(dt)
-                    arr = np.ascontiguousarray(host).view(np.int32 if dt != np.float32 else np.float32)
-                    pin = torch.from_numpy(arr).pin_memory()
+                ptrs = (C.c_void_p * len(L.cell_cols))()
+                for i, pin in P["agents"].items():
                     dev = torch.empty(n, dtype=pin.dtype, device=self.device)
                     dev.copy_(pin, non_blocking=True)
                     keep.append(dev)
                     ptrs[i] = dev.data_ptr()
                 self._check(self.lib.olc_pool_add_agents(self.handle, m.slot, ptrs, n, self._s()))
-            # fields: initial grids into buffer a, faces pinned to the boundary
-            for i, name in enumerate(L.chem_fields):
-                host = np.asarray(e.chemistry.column(name), dtype=np.float32)
-                d = e._diffusion.get(name)
-                if d is not None:
-                    host = host.copy(order="F")
-                    b = np.float32(d.boundary)
-                    host[0, :, :] = host[-1, :, :] = b
-                    host[:, 0, :] = host[:, -1, :] = b
-                    host[:, :, 0] = host[:, :, -1] = b
-                flat = np.ascontiguousarray(host.ravel(order="F"))
-                pin = torch.from_numpy(flat).pin_memory()
+            for i, pin in enumerate(P["fields"]):
                 dst = self.fields_dev[i][0][m.field_off:m.field_off + nvox]
                 if dst.dtype == torch.float32:
                     dst.copy_(pin, non_blocking=True)
@@ -584,10 +636,24 @@ class PoolDevice:
                     keep.append(tmp)
             for t in keep:
                 t.record_stream(self.stream)
+        req._payload = None  # pinned buffers return to torch's cache once the copies are done
         return m
 
     def step(self, collect: bool) -> None:
-        self._check(self.lib.olc_step(self.handle, 1, int(collect), self._s()))
+        if self.time_steps:
+            a, b = self.torch.cuda.Event(enable_timing=True), self.torch.cuda.Event(enable_timing=True)
+            a.record(self.stream)
+            self._check(self.lib.olc_step(self.handle, 1, int(collect), self._s()))
+            b.record(self.stream)
+            self.step_events.append((a, b))
+        else:
+            self._check(self.lib.olc_step(self.handle, 1, int(collect), self._s()))
+
+    def device_seconds(self) -> float:
+        """Device time of the steps run since time_steps was set (each step
+        from its first to its last kernel; idle gaps between steps excluded)."""
+        self.stream.synchronize()
+        return sum(a.elapsed_time(b) for a, b in self.step_events) / 1e3
 
     def fence(self):
         ev = self.torch.cuda.Event()

@@ -270,3 +270,20 @@ def test_plan_arenas_follows_the_mix():
     from oncolytica_b200.serving import row_bytes, voxel_bytes
     used = rows * row_bytes(8) + vox * voxel_bytes([0, 0], [True, False]) + tab * 8
     assert used == pytest.approx(8 << 30, rel=1e-3)
+
+
+def test_serve_with_prefetching_workers():
+    pool, dev = _pool(slots=3)
+    built = []
+
+    def make(rid, steps):
+        def f():
+            built.append(rid)
+            return _req(rid, steps)
+        return f
+
+    arrivals = [(0.001 * k, make(k, 1 + k % 4)) for k in range(12)]
+    res = pool.serve(arrivals, prefetch=0.05, workers=2)
+    assert sorted(r.request_id for r in res) == list(range(12))
+    assert all(r.status == "done" for r in res)
+    assert sorted(built) == list(range(12))
