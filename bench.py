@@ -57,6 +57,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--no-extras", action="store_true", help="leave the batched and 16-bit measurements out")
     ap.add_argument("--rate", type=float, default=20.0, help="request arrivals per second (--workload serve)")
     ap.add_argument("--duration", type=float, default=120.0, help="seconds of arrivals (--workload serve)")
+    ap.add_argument("--serve-seconds", type=float, default=15.0,
+                    help="seconds of arrivals of the serving run added to the default line")
     return ap.parse_args()
 
 
@@ -386,6 +388,9 @@ def run_b200(args) -> None:
                            for st in ("f32", "bf16_sr")}
         line["precision"] = {st: measure_storage(spec, st, args.extra_steps * 5, 3, graphs=not args.no_graphs)
                              for st in ("bf16_sr", "f16")}
+        torch.cuda.empty_cache()
+        # the serving mix, shortened to args.serve_seconds of arrivals
+        line["serving"] = measure_serving(args.rate, args.serve_seconds, seed=0, storage="bf16_sr", solo_sample=4)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(spec)
     print(json.dumps(line), flush=True)

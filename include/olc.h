@@ -113,6 +113,11 @@ typedef struct {
  * increments (the field stalls); stochastic rounding keeps them in
  * expectation. */
 #define OLC_FIELD_BF16_SR 3
+/* OLC_FIELD_F16_SR: FP16 storage whose substeps round stochastically (13
+ * random bits added below the kept mantissa, then rounding toward zero; same
+ * hash bits as OLC_FIELD_BF16_SR).  Unbiased rounding with FP16's 11-bit
+ * significand keeps the accumulated field error near 1e-3 of FP64. */
+#define OLC_FIELD_F16_SR  4
 
 /* Hertz-like contact repulsion (engine/assets/shaders/tumor_sim.wgsl:505-628):
  * for d < r_i + r_j, F += k * delta^(3/2) * (p_i - p_j)/d with

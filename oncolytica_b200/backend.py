@@ -21,7 +21,8 @@ from oncolytica_b200.compiler.emit_cuda import make_layout, pack_params, transla
 from oncolytica_b200.engine import STORAGE_CODES
 
 # torch element type of each field storage code (OLC_FIELD_F32 / BF16 / F16)
-FIELD_DTYPES = {0: lambda t: t.float32, 1: lambda t: t.bfloat16, 2: lambda t: t.float16, 3: lambda t: t.bfloat16}
+FIELD_DTYPES = {0: lambda t: t.float32, 1: lambda t: t.bfloat16, 2: lambda t: t.float16, 3: lambda t: t.bfloat16,
+                4: lambda t: t.float16}
 
 
 def seed_rng(seed: int, idx: np.ndarray) -> np.ndarray:

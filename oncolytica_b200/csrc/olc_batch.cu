@@ -511,6 +511,9 @@ void launch_substep_batch16(const BatchArgs& b, int storage, const uint4* tiles,
     else if (storage == OLC_FIELD_BF16_SR)
         k_substep_batch16<OLC_FIELD_BF16_SR><<<n_tiles, 64, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a,
                                                                       c, step_ctr);
+    else if (storage == OLC_FIELD_F16_SR)
+        k_substep_batch16<OLC_FIELD_F16_SR><<<n_tiles, 64, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a,
+                                                                     c, step_ctr);
     else
         k_substep_batch16<OLC_FIELD_F16><<<n_tiles, 64, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a, c,
                                                                   step_ctr);
@@ -522,7 +525,7 @@ void launch_react_batch16(const BatchArgs& b, int storage, const uint4* tiles, o
     if (n_tiles == 0) return;
     unsigned short* a = static_cast<unsigned short*>(fa);
     unsigned short* c = static_cast<unsigned short*>(fb);
-    if (storage != OLC_FIELD_F16)
+    if (storage != OLC_FIELD_F16 && storage != OLC_FIELD_F16_SR)
         k_react_batch16<OLC_FIELD_BF16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, a, c,
                                                                  sink, comp);
     else
@@ -536,7 +539,7 @@ void launch_reduce_field_batch16(const BatchArgs& b, int storage, const uint4* t
     if (n_tiles == 0) return;
     const unsigned short* a = static_cast<const unsigned short*>(fa);
     const unsigned short* c = static_cast<const unsigned short*>(fb);
-    if (storage != OLC_FIELD_F16)
+    if (storage != OLC_FIELD_F16 && storage != OLC_FIELD_F16_SR)
         k_reduce_field_batch16<OLC_FIELD_BF16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, field, n_fields, fpar, a, c,
                                                                         comp, out);
     else

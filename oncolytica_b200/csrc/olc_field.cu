@@ -47,8 +47,8 @@ bool make_field_step(const OlcDiffusion& d, const int dims[3], float dx, float d
                " > 1/6; raise substeps";
         return false;
     }
-    if (d.storage < OLC_FIELD_F32 || d.storage > OLC_FIELD_BF16_SR) {
-        *err = "storage must be OLC_FIELD_F32, OLC_FIELD_BF16, OLC_FIELD_F16 or OLC_FIELD_BF16_SR";
+    if (d.storage < OLC_FIELD_F32 || d.storage > OLC_FIELD_F16_SR) {
+        *err = "storage must be OLC_FIELD_F32, OLC_FIELD_BF16, OLC_FIELD_F16, OLC_FIELD_BF16_SR or OLC_FIELD_F16_SR";
         return false;
     }
     if (d.storage != OLC_FIELD_F32 && dims[0] % 8 != 0) {

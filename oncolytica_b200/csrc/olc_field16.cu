@@ -8,7 +8,8 @@
 //   diffusion (S substeps): c' = round16(max(c + r (S6 - 6 c), 0)) with the
 //                      sum S6 = ((xm + xp) + (ym + yp)) + (zm + zp) in FP32;
 //                      outer faces pinned to round16(boundary); round16 is to
-//                      nearest even, or stochastic for OLC_FIELD_BF16_SR
+//                      nearest even, or stochastic for OLC_FIELD_BF16_SR and
+//                      OLC_FIELD_F16_SR
 //                      (hash bits of voxel, step, substep and field).
 // comp carries each voxel's rounding residual of the reaction into the next
 // step (compensated summation), so small uptake and decay terms are not lost
@@ -78,7 +79,7 @@ void launch_react16(void* f, float* sink, float* comp, const FieldStep& fs, cuda
     const size_t nvox = (size_t)fs.dims[0] * fs.dims[1] * fs.dims[2];
     size_t blocks = (nvox + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    if (fs.storage != OLC_FIELD_F16)
+    if (fs.storage != OLC_FIELD_F16 && fs.storage != OLC_FIELD_F16_SR)
         k_react16<OLC_FIELD_BF16><<<(unsigned)blocks, 256, 0, s>>>(static_cast<unsigned short*>(f), sink, comp,
                                                                     fs.dims[0], fs.dims[1], fs.dims[2], fs.sink_dt,
                                                                     fs.decay_step);
@@ -239,6 +240,9 @@ void* run_substeps16(void* a, void* b, const FieldMaps16& m, int a_index, const 
         else if (fs.storage == OLC_FIELD_BF16_SR)
             launch_sub16<OLC_FIELD_BF16_SR>(m.map[cur], bufs[1 - cur], fs, status, i & 1, step_ctr, step_host, i,
                                             field, s);
+        else if (fs.storage == OLC_FIELD_F16_SR)
+            launch_sub16<OLC_FIELD_F16_SR>(m.map[cur], bufs[1 - cur], fs, status, i & 1, step_ctr, step_host, i,
+                                           field, s);
         else
             launch_sub16<OLC_FIELD_F16>(m.map[cur], bufs[1 - cur], fs, status, i & 1, step_ctr, step_host, i, field, s);
         cur = 1 - cur;
@@ -308,7 +312,7 @@ void launch_reduce_field16(const void* f, const float* comp, const FieldStep& fs
     double* part = rs.partials + (size_t)(4 + slot) * RED_MAX_BLOCKS;
     olc_u32* ticket = rs.tickets + 1 + slot;
     const unsigned short* p = static_cast<const unsigned short*>(f);
-    if (fs.storage != OLC_FIELD_F16)
+    if (fs.storage != OLC_FIELD_F16 && fs.storage != OLC_FIELD_F16_SR)
         k_reduce_field16<OLC_FIELD_BF16><<<(unsigned)blocks, 256, 0, s>>>(p, comp, nvox, slot, out, part, ticket);
     else
         k_reduce_field16<OLC_FIELD_F16><<<(unsigned)blocks, 256, 0, s>>>(p, comp, nvox, slot, out, part, ticket);

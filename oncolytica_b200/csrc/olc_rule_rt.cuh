@@ -289,7 +289,7 @@ __device__ __forceinline__ float olc_field_at(const PT& P, int f, olc_u32 v) {
     const int t = P.field_type[f];
     if (t == 0) return static_cast<const float*>(p)[v];
     const unsigned short h = static_cast<const unsigned short*>(p)[v];
-    return t == 2 ? olc_f16_to_float(h) : olc_bf16_to_float(h);  // 1 and 3 store BF16
+    return (t == 2 || t == 4) ? olc_f16_to_float(h) : olc_bf16_to_float(h);  // 1 and 3 store BF16
 }
 
 // Deposit into a field's sink (sum of first-order uptake rates of a voxel).

@@ -1075,7 +1075,7 @@ int olc_bind_field_ex(OlcSim* s, int index, void* a_, void* b_, float* sink, flo
         !make_field_step(*spec, s->geom.chem_dims, s->geom.chem_voxel_size, s->caps.dt, &fs, &err))
         return fail(s, OLC_ERR_ARG, "olc_bind_field: " + err);
     if (spec->substeps == 0) {
-        if (spec->storage < OLC_FIELD_F32 || spec->storage > OLC_FIELD_BF16_SR)
+        if (spec->storage < OLC_FIELD_F32 || spec->storage > OLC_FIELD_F16_SR)
             return fail(s, OLC_ERR_ARG, "olc_bind_field: bad storage type");
         fs.storage = spec->storage;
     }
@@ -1644,7 +1644,7 @@ int olc_bind_field_pool(OlcSim* s, int index, void* a, void* b, float* sink, flo
     if (!s->pool) return fail(s, OLC_ERR_STATE, "olc_bind_field_pool: not a pool");
     if (index < 0 || index >= (int)s->caps.n_fields || !a || !b)
         return fail(s, OLC_ERR_ARG, "olc_bind_field_pool: bad index or null buffer");
-    if (storage < OLC_FIELD_F32 || storage > OLC_FIELD_BF16_SR)
+    if (storage < OLC_FIELD_F32 || storage > OLC_FIELD_F16_SR)
         return fail(s, OLC_ERR_ARG, "olc_bind_field_pool: bad storage type");
     if (storage != OLC_FIELD_F32 && !comp)
         return fail(s, OLC_ERR_ARG, "olc_bind_field_pool: 16-bit storage needs a compensation buffer");
@@ -1993,7 +1993,7 @@ int olc_stage_diffuse16(void* f, void* tmp, float* sink, float* comp, const int3
                         const OlcDiffusion* spec, uint32_t step, int field, void* stream) {
     if (!f || !tmp || !comp || !dims || !spec)
         return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse16: null argument");
-    if (spec->storage != OLC_FIELD_BF16 && spec->storage != OLC_FIELD_F16 && spec->storage != OLC_FIELD_BF16_SR)
+    if (spec->storage < OLC_FIELD_BF16 || spec->storage > OLC_FIELD_F16_SR)
         return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse16: storage must be BF16, FP16 or BF16_SR");
     std::string err;
     FieldStep fs;

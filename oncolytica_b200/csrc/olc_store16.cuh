@@ -35,15 +35,38 @@ struct Store16<OLC_FIELD_F16> {
     }
 };
 
-// BF16 with stochastic rounding in the substeps: same storage as BF16
+// BF16 / FP16 with stochastic rounding in the substeps: same storage
 template <>
 struct Store16<OLC_FIELD_BF16_SR> : Store16<OLC_FIELD_BF16> {};
+template <>
+struct Store16<OLC_FIELD_F16_SR> : Store16<OLC_FIELD_F16> {};
+
+template <int ST>
+struct IsSR {
+    static constexpr bool value = ST == OLC_FIELD_BF16_SR || ST == OLC_FIELD_F16_SR;
+};
 
 // Stochastic BF16 rounding of a finite non-negative value with 32 random bits:
 // the low 16 bits of the FP32 pattern plus 16 random bits carry into the kept
 // half with probability equal to the discarded fraction.
 __device__ __forceinline__ unsigned short olc_bf16_sr(float f, olc_u32 rnd) {
     return (unsigned short)((__float_as_uint(f) + (rnd & 0xffffu)) >> 16);
+}
+
+// Stochastic FP16 rounding of a finite value with 13 random bits: the 13 FP32
+// mantissa bits that FP16 drops (normal range) plus 13 random bits, then
+// conversion toward zero.  Below FP16's normal range (2^-14) more bits are
+// dropped and the sum is truncated (spacing there is 2^-24).
+__device__ __forceinline__ unsigned short olc_f16_sr(float f, olc_u32 rnd) {
+    const float g = __uint_as_float(__float_as_uint(f) + (rnd & 0x1fffu));
+    unsigned short h;
+    asm("{ .reg .b16 t; cvt.rz.f16.f32 t, %1; mov.b16 %0, t; }" : "=h"(h) : "f"(g));
+    return h;
+}
+
+template <int ST>
+__device__ __forceinline__ unsigned short olc_sr16(float f, olc_u32 rnd) {
+    return ST == OLC_FIELD_F16_SR ? olc_f16_sr(f, rnd) : olc_bf16_sr(f, rnd);
 }
 
 // Random bits for one substep: `key` mixes the step, substep and field
@@ -65,13 +88,13 @@ __device__ __forceinline__ float4 load4(const unsigned short* p) {
                        Store16<ST>::to_f((unsigned short)(raw.y & 0xffffu)), Store16<ST>::to_f((unsigned short)(raw.y >> 16)));
 }
 
-// Stores four values at voxel index v (stochastic rounding for ST = BF16_SR).
+// Stores four values at voxel index v (stochastic rounding for the _SR types).
 template <int ST>
 __device__ __forceinline__ void store4_at(unsigned short* p, float4 v, unsigned long long vi, olc_u32 key) {
-    if (ST == OLC_FIELD_BF16_SR) {  // vi is a multiple of 4
+    if (IsSR<ST>::value) {  // vi is a multiple of 4
         const olc_u32 r0 = olc_sr_pair(vi >> 1, key), r1 = olc_sr_pair((vi >> 1) + 1, key);
-        const olc_u32 lo = (olc_u32)olc_bf16_sr(v.x, r0) | ((olc_u32)olc_bf16_sr(v.y, r0 >> 16) << 16);
-        const olc_u32 hi = (olc_u32)olc_bf16_sr(v.z, r1) | ((olc_u32)olc_bf16_sr(v.w, r1 >> 16) << 16);
+        const olc_u32 lo = (olc_u32)olc_sr16<ST>(v.x, r0) | ((olc_u32)olc_sr16<ST>(v.y, r0 >> 16) << 16);
+        const olc_u32 hi = (olc_u32)olc_sr16<ST>(v.z, r1) | ((olc_u32)olc_sr16<ST>(v.w, r1 >> 16) << 16);
         *reinterpret_cast<uint2*>(p) = make_uint2(lo, hi);
         return;
     }
@@ -81,7 +104,7 @@ __device__ __forceinline__ void store4_at(unsigned short* p, float4 v, unsigned 
 }
 
 // Eight consecutive values (16 bytes): load to FP32, store with rounding at
-// voxel index vi (a multiple of 8; stochastic for ST = BF16_SR).
+// voxel index vi (a multiple of 8; stochastic for the _SR types).
 template <int ST>
 __device__ __forceinline__ void load8(const unsigned short* p, float (&f)[8]) {
     const uint4 raw = *reinterpret_cast<const uint4*>(p);
@@ -98,9 +121,9 @@ __device__ __forceinline__ void store8_at(unsigned short* p, const float (&v)[8]
     olc_u32 w[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        if (ST == OLC_FIELD_BF16_SR) {
+        if (IsSR<ST>::value) {
             const olc_u32 r = olc_sr_pair((vi >> 1) + k, key);
-            w[k] = (olc_u32)olc_bf16_sr(v[2 * k], r) | ((olc_u32)olc_bf16_sr(v[2 * k + 1], r >> 16) << 16);
+            w[k] = (olc_u32)olc_sr16<ST>(v[2 * k], r) | ((olc_u32)olc_sr16<ST>(v[2 * k + 1], r >> 16) << 16);
         } else {
             w[k] = (olc_u32)Store16<ST>::from_f(v[2 * k]) | ((olc_u32)Store16<ST>::from_f(v[2 * k + 1]) << 16);
         }

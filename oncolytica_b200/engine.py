@@ -30,10 +30,10 @@ class DiffusionSpec:
     decay: float = 0.0
     boundary: float = 0.0
     substeps: Optional[int] = None
-    storage: str = "f32"   # "f32", "bf16", "f16" or "bf16_sr": element type (and rounding) of the field
+    storage: str = "f32"   # "f32", "bf16", "f16", "bf16_sr" or "f16_sr": element type (and rounding) of the field
 
 
-STORAGE_CODES = {"f32": 0, "bf16": 1, "f16": 2, "bf16_sr": 3}
+STORAGE_CODES = {"f32": 0, "bf16": 1, "f16": 2, "bf16_sr": 3, "f16_sr": 4}
 
 
 @dataclass
@@ -161,10 +161,11 @@ class Engine:
         (engine tumor_sim.wgsl:387-446; substeps as chemistry_rule(iterations=S)).
         ``storage`` "bf16" or "f16" keeps the field in 16 bits: updates run in
         FP32, and uptake and decay are applied once per step with a per-voxel
-        FP32 rounding residual carried to the next step; "bf16_sr" rounds the
-        substeps stochastically (reproducible hash bits) so that small
-        diffusion increments are not lost to BF16's 8-bit mantissa (no
-        counterpart in the reference, whose fields are FP32)."""
+        FP32 rounding residual carried to the next step; "bf16_sr" and
+        "f16_sr" round the substeps stochastically (reproducible hash bits) so
+        that small diffusion increments are not lost to the short mantissa and
+        rounding errors do not accumulate a bias (no counterpart in the
+        reference, whose fields are FP32)."""
         if storage not in STORAGE_CODES:
             raise ValueError(f"storage must be one of {sorted(STORAGE_CODES)}, got {storage!r}")
         self._diffusion[field] = DiffusionSpec(float(diffusion), float(decay), float(boundary), substeps, storage)

@@ -252,9 +252,11 @@ def serving_schedule(rate: float = 20.0, duration: float = 120.0, seed: int = 0,
     """Requests of the serving mix: a Poisson process of ``rate`` requests/s
     over ``duration`` s; each request is one simulation drawn like a member of
     the batched sweep (``batched_specs``) with a step count uniform in
-    ``steps_range`` and an agent capacity of 4 n + 4096 (its solo run's
-    max_agents, reserved on admission).  Returns (arrival s, spec, steps)
-    triples in arrival order, from numpy default_rng(seed)."""
+    ``steps_range``.  Its agent capacity (its solo run's max_agents, reserved on
+    admission) allows the population to double every 300 steps with 50 %
+    headroom: the largest domains grew about 6x in 900 steps.  Returns
+    (arrival s, spec, steps) triples in arrival order, from numpy
+    default_rng(seed)."""
     rng = np.random.default_rng(seed)
     times, t = [], 0.0
     while True:
@@ -264,7 +266,8 @@ def serving_schedule(rate: float = 20.0, duration: float = 120.0, seed: int = 0,
         times.append(t)
     specs = batched_specs(len(times), seed=seed + 7919) if times else []
     steps = rng.integers(steps_range[0], steps_range[1] + 1, size=len(times))
-    return [(tt, replace(sp, storage=storage, capacity=4 * sp.n_agents + 4096, name=f"request_{k}"), int(n))
+    return [(tt, replace(sp, storage=storage, capacity=int(1.5 * sp.n_agents * 2.0 ** (n / 300.0)) + 8192,
+                         name=f"request_{k}"), int(n))
             for k, (tt, sp, n) in enumerate(zip(times, specs, steps))]
 
 

@@ -246,7 +246,7 @@ static uint16_t f_to_bf16(float f) { /* finite values: RN-even on the bit patter
     return (uint16_t)((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
 }
 static float h16_to_f(uint16_t h, int storage) {
-    if (storage == 1 || storage == 3) return bf16_to_f(h);
+    if (storage == 1 || storage == 3) return bf16_to_f(h);  /* 2 and 4: FP16 */
     _Float16 x;
     memcpy(&x, &h, 2);
     return (float)x;
@@ -278,12 +278,52 @@ static uint16_t f_to_bf16_sr(float f, uint32_t rnd) {
     return (uint16_t)((u + (rnd & 0xffffu)) >> 16);
 }
 
+/* FP32 -> FP16 rounded toward zero (IEEE binary16; finite inputs, results
+ * past the largest finite FP16 clamp to it), from the bit pattern. */
+static uint16_t f_to_f16_rz(float f) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    const uint16_t sign = (uint16_t)((u >> 16) & 0x8000u);
+    const int e = (int)((u >> 23) & 0xffu) - 127;
+    const uint32_t m = u & 0x7fffffu;
+    if (((u >> 23) & 0xffu) == 0u) return sign; /* zero and FP32 subnormals */
+    if (e > 15) return (uint16_t)(sign | 0x7bffu);
+    if (e >= -14) return (uint16_t)(sign | (uint16_t)((e + 15) << 10) | (uint16_t)(m >> 13));
+    if (e < -24) return sign;
+    return (uint16_t)(sign | (uint16_t)((0x800000u | m) >> (uint32_t)(-1 - e))); /* |f| * 2^24, truncated */
+}
+
+/* Stochastic FP16 rounding (storage 4): the 13 FP32 mantissa bits FP16 drops
+ * (normal range) plus 13 random bits, then rounding toward zero; the random
+ * bits come from the same pair hash as storage 3 (low / high 16 bits). */
+static uint16_t f_to_f16_sr(float f, uint32_t rnd) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    u += rnd & 0x1fffu;
+    float g;
+    memcpy(&g, &u, 4);
+    return f_to_f16_rz(g);
+}
+
+void orc_round16(const float* in, uint16_t* out, size_t n, int storage, const uint32_t* rnd) {
+    for (size_t i = 0; i < n; ++i) {
+        if (storage == 3)
+            out[i] = f_to_bf16_sr(in[i], rnd[i]);
+        else if (storage == 4)
+            out[i] = f_to_f16_sr(in[i], rnd[i]);
+        else if (storage == 5)
+            out[i] = f_to_f16_rz(in[i]);
+        else
+            out[i] = f_to_h16(in[i], storage);
+    }
+}
+
 int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const int32_t dims[3], float dx, float dt,
                   float D, float decay, float boundary, int substeps, int storage, uint32_t step, int field,
                   int nthreads) {
     const int nx = dims[0], ny = dims[1], nz = dims[2];
     const int nt = nthreads_or_all(nthreads);
-    if (substeps < 1 || storage < 1 || storage > 3) return -1;
+    if (substeps < 1 || storage < 1 || storage > 4) return -1;
     const float dts = dt / (float)substeps;
     const float r = D * dts / (dx * dx);
     if (r > 1.0f / 6.0f + 1e-7f) return -1;
@@ -325,10 +365,11 @@ int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const in
                     float s2 = s1 + (h16_to_f(cur[v - sz], storage) + h16_to_f(cur[v + sz], storage));
                     float u = c + r * (s2 - 6.0f * c);
                     u = u > 0.0f ? u : 0.0f;
-                    if (storage == 3) {
+                    if (storage == 3 || storage == 4) {
                         uint32_t xr = ((uint32_t)(v >> 1) ^ key) * 0x9E3779B1u;
                         xr ^= xr >> 15;
-                        nxt[v] = f_to_bf16_sr(u, (v & 1) ? (xr >> 16) : (xr & 0xffffu));
+                        const uint32_t rb = (v & 1) ? (xr >> 16) : (xr & 0xffffu);
+                        nxt[v] = storage == 3 ? f_to_bf16_sr(u, rb) : f_to_f16_sr(u, rb);
                     } else {
                         nxt[v] = f_to_h16(u, storage);
                     }

@@ -50,6 +50,7 @@ def lib() -> C.CDLL:
         L.orc_tumour_agents.restype = C.c_int
         L.orc_tumour_agents.argtypes = [P, C.c_int]
         L.orc_tumour_sizeof.restype = C.c_size_t
+        L.orc_round16.argtypes = [P, P, C.c_size_t, C.c_int, P]
         _lib = L
     return _lib
 
@@ -122,18 +123,29 @@ def diffuse(f: np.ndarray, sink: np.ndarray | None, dx: float, dt: float, D: flo
 
 
 def to_bits16(f: np.ndarray, storage: int) -> np.ndarray:
-    """float32 values -> BF16 (storage 1 and 3) or FP16 (storage 2) bit
+    """float32 values -> BF16 (storage 1 and 3) or FP16 (storage 2 and 4) bit
     patterns, rounded to nearest even (finite values)."""
     f = np.ascontiguousarray(f, dtype=np.float32)
-    if storage == 2:
+    if storage in (2, 4):
         return f.astype(np.float16).view(np.uint16)
     u = f.view(np.uint32).astype(np.uint64)
     return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
 
 
+def round16(f: np.ndarray, storage: int, rnd: np.ndarray | None = None) -> np.ndarray:
+    """The 16-bit storage roundings element-wise (``orc_round16``): 1/2 to
+    nearest even, 3/4 stochastic with ``rnd`` (uint32 per element), 5 FP16
+    toward zero."""
+    f = np.ascontiguousarray(f, dtype=np.float32)
+    out = np.zeros(f.shape, np.uint16)
+    r = None if rnd is None else np.ascontiguousarray(rnd, dtype=np.uint32)
+    lib().orc_round16(_p(f), _p(out), f.size, storage, _p(r))
+    return out
+
+
 def from_bits16(h: np.ndarray, storage: int) -> np.ndarray:
     h = np.ascontiguousarray(h, dtype=np.uint16)
-    if storage == 2:
+    if storage in (2, 4):
         return h.view(np.float16).astype(np.float32)
     return (h.astype(np.uint32) << 16).view(np.float32)
 
@@ -142,7 +154,7 @@ def diffuse16(bits: np.ndarray, sink: np.ndarray | None, comp: np.ndarray, dx: f
               decay: float, boundary: float, substeps: int, storage: int, step: int = 0, field: int = 0,
               nthreads: int = 0):
     """One step of a 16-bit field (indexed [z, y, x]): returns (bits, comp).
-    ``step`` and ``field`` salt the stochastic rounding of storage 3."""
+    ``step`` and ``field`` salt the stochastic rounding of storages 3 and 4."""
     f = np.ascontiguousarray(bits, dtype=np.uint16).copy()
     tmp = np.zeros_like(f)
     c = np.ascontiguousarray(comp, dtype=np.float32).copy()

@@ -34,7 +34,7 @@ def _metrics(eng):
 
 
 @pytest.mark.parametrize("graphs,storage", [(False, "f32"), (True, "f32"), (True, "bf16"), (False, "f16"),
-                                            (True, "bf16_sr")])
+                                            (True, "bf16_sr"), (True, "f16_sr")])
 def test_batch_members_match_solo_runs(cuda, graphs, storage):
     specs = _members(storage)
     assert len({s.S_o2 % 2 for s in specs}) == 2  # odd and even substep counts

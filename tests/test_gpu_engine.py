@@ -386,7 +386,7 @@ def test_graph_steps_match_eager_steps(cuda):
                    {k: getattr(mb, k) for k in metric_fields(type(mb))}
 
 
-@pytest.mark.parametrize("storage,code", [("bf16", 1), ("f16", 2), ("bf16_sr", 3)])
+@pytest.mark.parametrize("storage,code", [("bf16", 1), ("f16", 2), ("bf16_sr", 3), ("f16_sr", 4)])
 def test_tumour_step_parity_16bit_fields(cuda, storage, code):
     """16-bit field storage through the engine: each step from an identical
     state gives the oracle's field bits and residuals (reaction + substeps,

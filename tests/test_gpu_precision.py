@@ -21,7 +21,8 @@ pytestmark = pytest.mark.gpu
 # field stalls: per-substep increments fall below half an ulp); FP16 6.9e-3 /
 # 2.0e-3; BF16 with stochastic rounding 1.3e-2 / 3.5e-3.  The 16-bit figures
 # include the drug field's decay applied once per step instead of per substep.
-TOLERANCE = {0: (2e-5, 2e-6), 1: (3e-1, 5e-2), 2: (1e-2, 5e-3), 3: (2e-2, 5e-3)}
+# FP16 with stochastic rounding (storage 4) is held to 2e-3 / 1e-3.
+TOLERANCE = {0: (2e-5, 2e-6), 1: (3e-1, 5e-2), 2: (1e-2, 5e-3), 3: (2e-2, 5e-3), 4: (2e-3, 1e-3)}
 
 
 def _problem(n=32, seed=5):
@@ -65,7 +66,7 @@ def _run_gpu(olc, cuda, storage, shape, K, D, decay, bnd, init, S, dx, dt, steps
     return v.reshape(shape).astype(np.float64)
 
 
-@pytest.mark.parametrize("storage", [0, 1, 2, 3])
+@pytest.mark.parametrize("storage", [0, 1, 2, 3, 4])
 def test_field_error_against_fp64(cuda, olc, storage):
     shape, K = _problem()
     steps, dx, dt = 200, 4.0, 0.1

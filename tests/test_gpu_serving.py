@@ -73,7 +73,7 @@ def _check_same(spec, res, e):
         assert ra["field_min"][f] == rb["field_min"][f] and ra["field_max"][f] == rb["field_max"][f]
 
 
-@pytest.mark.parametrize("storage", ["f32", "bf16_sr"])
+@pytest.mark.parametrize("storage", ["f32", "bf16_sr", "f16_sr"])
 def test_each_request_in_the_mix_matches_its_solo_run(cuda, storage):
     specs = _specs(storage)
     steps = [6, 3, 7, 4, 5]

@@ -304,7 +304,7 @@ def test_contact_bit_exact(cuda, olc):
 
 # ------------------------------------------------------------------ 16-bit field storage
 
-@pytest.mark.parametrize("storage", [1, 2, 3])
+@pytest.mark.parametrize("storage", [1, 2, 3, 4])
 @pytest.mark.parametrize("dims,substeps,decay,with_sink", [((32, 24, 20), 5, 0.0, True),
                                                           ((64, 41, 37), 7, 0.1, True),
                                                           ((136, 17, 9), 3, 0.05, False)])
