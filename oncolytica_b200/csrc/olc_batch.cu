@@ -328,7 +328,8 @@ void launch_flip_parity(const FieldStep* steps, int field, int n_fields, olc_u32
 
 // ------------------------------------------------------------------ 16-bit fields
 // The same tiles on BF16 / FP16 storage (olc_field16.cu's arithmetic): the
-// reaction pass with its FP32 residual, then substeps without decay.
+// reaction pass with its FP32 residual, then the substeps (decaying in each
+// for the stochastically rounded storages).
 // Eight voxels per thread (16-byte loads and stores), 64 threads per tile.
 template <int ST>
 __global__ void __launch_bounds__(64) k_substep_batch16(const uint4* __restrict__ tiles,
@@ -389,7 +390,8 @@ __global__ void __launch_bounds__(64) k_substep_batch16(const uint4* __restrict_
         for (int e = 0; e < 8; ++e) {
             const float xm = e == 0 ? xl : c[e - 1], xp = e == 7 ? xr : c[e + 1];
             const float s6 = __fadd_rn(__fadd_rn(__fadd_rn(xm, xp), __fadd_rn(ym[e], yp[e])), __fadd_rn(zm[e], zp[e]));
-            v[e] = fmaxf(__fadd_rn(c[e], __fmul_rn(fs.r, __fsub_rn(s6, __fmul_rn(6.0f, c[e])))), 0.0f);
+            v[e] = fmaxf(__fmul_rn(__fadd_rn(c[e], __fmul_rn(fs.r, __fsub_rn(s6, __fmul_rn(6.0f, c[e])))), fs.inv_decay),
+                         0.0f);
         }
         if (edge_y || zz == 0 || zz == nz - 1) {
 #pragma unroll

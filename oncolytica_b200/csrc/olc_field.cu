@@ -61,11 +61,13 @@ bool make_field_step(const OlcDiffusion& d, const int dims[3], float dx, float d
     out->sink_dt = dt;
     out->substeps = d.substeps;
     out->storage = d.storage;
-    if (d.storage == OLC_FIELD_F32) {
+    if (d.storage == OLC_FIELD_F32 || d.storage == OLC_FIELD_BF16_SR || d.storage == OLC_FIELD_F16_SR) {
+        // every substep decays (stochastic rounding keeps the small decrements)
         out->inv_decay = 1.0f / (1.0f + d.decay * dts);
         out->decay_step = 1.0f;
     } else {
-        // decay leaves the substeps and is applied once per step by the reaction pass
+        // round to nearest would lose the small per-substep decrements: decay
+        // leaves the substeps and is applied once per step by the reaction pass
         out->inv_decay = 1.0f;
         out->decay_step = (float)std::pow(1.0 + (double)d.decay * (double)dts, -(double)d.substeps);
     }

@@ -41,9 +41,12 @@ __device__ __forceinline__ bool mbar_wait_once(olc_u32 bar, olc_u32 parity) {
     return ok != 0;
 }
 
-__device__ __forceinline__ float diffuse1(float xm, float xp, float ym, float yp, float zm, float zp, float c, float r) {
+// One voxel's substep in FP32: the FP32 kernels' arithmetic (inv_decay is 1
+// for the storages that decay once per step in the reaction pass).
+__device__ __forceinline__ float diffuse1(float xm, float xp, float ym, float yp, float zm, float zp, float c, float r,
+                                         float inv_decay) {
     const float s = __fadd_rn(__fadd_rn(__fadd_rn(xm, xp), __fadd_rn(ym, yp)), __fadd_rn(zm, zp));
-    return fmaxf(__fadd_rn(c, __fmul_rn(r, __fsub_rn(s, __fmul_rn(6.0f, c)))), 0.0f);
+    return fmaxf(__fmul_rn(__fadd_rn(c, __fmul_rn(r, __fsub_rn(s, __fmul_rn(6.0f, c)))), inv_decay), 0.0f);
 }
 
 }  // namespace
@@ -108,7 +111,8 @@ constexpr size_t SMEM = BYTES + 16 + 128;
 template <int ST>
 __global__ void __launch_bounds__(t16::THREADS) k_substep16(const __grid_constant__ CUtensorMap in_map,
                                                            unsigned short* __restrict__ out, int nx, int ny, int nz,
-                                                           float r, float bval, olc_u32* status, int rev,
+                                                           float r, float inv_decay, float bval, olc_u32* status,
+                                                           int rev,
                                                            const olc_u32* step_ctr, olc_u32 step_host, int sub,
                                                            int field) {
     using namespace t16;
@@ -175,7 +179,8 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep16(const __grid_constan
         const float xl = Store16<ST>::to_f(pc[-1]), xr = Store16<ST>::to_f(pc[8]);
 #pragma unroll
         for (int e = 0; e < 8; ++e)
-            v[e] = diffuse1(e == 0 ? xl : c[e - 1], e == 7 ? xr : c[e + 1], ym[e], yp[e], zm[e], zp[e], c[e], r);
+            v[e] = diffuse1(e == 0 ? xl : c[e - 1], e == 7 ? xr : c[e + 1], ym[e], yp[e], zm[e], zp[e], c[e], r,
+                            inv_decay);
         if (edge_y || z == 0 || z == nz - 1) {
 #pragma unroll
             for (int e = 0; e < 8; ++e) v[e] = bf;
@@ -225,7 +230,7 @@ static void launch_sub16(const CUtensorMap& map, void* out, const FieldStep& fs,
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cudaLaunchKernelEx(&cfg, k_substep16<ST>, map, static_cast<unsigned short*>(out), fs.dims[0], fs.dims[1],
-                       fs.dims[2], fs.r, fs.bval, status, rev, step_ctr, step_host, sub, field);
+                       fs.dims[2], fs.r, fs.inv_decay, fs.bval, status, rev, step_ctr, step_host, sub, field);
 }
 
 void* run_substeps16(void* a, void* b, const FieldMaps16& m, int a_index, const FieldStep& fs, olc_u32* status,

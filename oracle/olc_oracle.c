@@ -233,7 +233,9 @@ int orc_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], float 
  * as BF16 (storage 1) or FP16 (storage 2), every update in FP32 with
  * round-to-nearest-even back to storage.  Per step: a reaction pass
  * (value + residual, uptake, the step's decay (1 + lambda dt/S)^-S, residual
- * kept in comp), then S substeps without decay; faces pinned. */
+ * kept in comp), then S substeps without decay; faces pinned.  Storages 3 and
+ * 4 (stochastic rounding) keep the FP32 scheme's decay in every substep
+ * (u * 1/(1 + lambda dt/S)) and no decay in the reaction pass. */
 static float bf16_to_f(uint16_t h) {
     uint32_t u = (uint32_t)h << 16;
     float f;
@@ -327,7 +329,9 @@ int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const in
     const float dts = dt / (float)substeps;
     const float r = D * dts / (dx * dx);
     if (r > 1.0f / 6.0f + 1e-7f) return -1;
-    const float decay_step = (float)pow(1.0 + (double)decay * (double)dts, -(double)substeps);
+    const int sr = storage == 3 || storage == 4;
+    const float decay_step = sr ? 1.0f : (float)pow(1.0 + (double)decay * (double)dts, -(double)substeps);
+    const float inv_decay = sr ? 1.0f / (1.0f + decay * dts) : 1.0f;
     const uint16_t bh = f_to_h16(boundary, storage);
     const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
 #pragma omp parallel for num_threads(nt) schedule(static)
@@ -363,7 +367,7 @@ int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const in
                     float s1 = (h16_to_f(cur[v - 1], storage) + h16_to_f(cur[v + 1], storage)) +
                                (h16_to_f(cur[v - sy], storage) + h16_to_f(cur[v + sy], storage));
                     float s2 = s1 + (h16_to_f(cur[v - sz], storage) + h16_to_f(cur[v + sz], storage));
-                    float u = c + r * (s2 - 6.0f * c);
+                    float u = (c + r * (s2 - 6.0f * c)) * inv_decay;
                     u = u > 0.0f ? u : 0.0f;
                     if (storage == 3 || storage == 4) {
                         uint32_t xr = ((uint32_t)(v >> 1) ^ key) * 0x9E3779B1u;
