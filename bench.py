@@ -50,7 +50,7 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--no-graphs", action="store_true", help="eager launches instead of CUDA graphs of whole steps")
     ap.add_argument("--sims", type=int, default=512, help="members of the batched workload (--workload batch)")
     ap.add_argument("--solo-sample", type=int, default=0, help="members also timed one at a time (--workload batch)")
-    ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16", "bf16_sr"],
+    ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16", "bf16_sr", "f16_sr"],
                     help="field storage of --workload batch")
     ap.add_argument("--extra-steps", type=int, default=10,
                     help="timed steps of the batched and 16-bit measurements added to the default line")
@@ -385,12 +385,12 @@ def run_b200(args) -> None:
         torch.cuda.empty_cache()
         line["batched"] = {st: measure_batch(args.sims, args.extra_steps, 3, graphs=not args.no_graphs,
                                              solo_sample=8 if st == "f32" else 0, storage=st)
-                           for st in ("f32", "bf16_sr")}
+                           for st in ("f32", "f16_sr")}
         line["precision"] = {st: measure_storage(spec, st, args.extra_steps * 5, 3, graphs=not args.no_graphs)
-                             for st in ("bf16_sr", "f16")}
+                             for st in ("f16_sr", "bf16_sr", "f16")}
         torch.cuda.empty_cache()
         # the serving mix, shortened to args.serve_seconds of arrivals
-        line["serving"] = measure_serving(args.rate, args.serve_seconds, seed=0, storage="bf16_sr", solo_sample=4)
+        line["serving"] = measure_serving(args.rate, args.serve_seconds, seed=0, storage="f16_sr", solo_sample=4)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(spec)
     print(json.dumps(line), flush=True)
@@ -544,7 +544,7 @@ def measure_serving(rate: float, duration: float, seed: int = 0, storage: str = 
     mix = [Footprint(sp.capacity, voxel_table_size(sp.tissue_dims), int(np.prod(sp.field_dims))) for sp in specs]
     tdims = tuple(max(sp.tissue_dims[i] for sp in specs) for i in range(3))
     free, _ = torch.cuda.mem_get_info()
-    code = {"f32": 0, "bf16": 1, "f16": 2, "bf16_sr": 3}[storage]
+    code = {"f32": 0, "bf16": 1, "f16": 2, "bf16_sr": 3, "f16_sr": 4}[storage]
     plan = plan_arenas(int(hbm_fraction * free), mix, n_cols=8, storages=[code, code], sinks=[True, False])
     proto = W.configure_engine(specs[0])
     dev = PoolDevice(proto, max_slots=max_slots, max_tissue_dims=tdims, **plan)
