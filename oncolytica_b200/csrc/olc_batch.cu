@@ -21,6 +21,7 @@
 // bit.  The FP64 sums of the per-simulation reductions are accumulated with
 // atomics and are exact only up to their order.
 #include "olc_internal.h"
+#include "olc_stencil.cuh"
 #include "olc_store16.cuh"
 
 namespace olc {
@@ -386,13 +387,7 @@ __global__ void __launch_bounds__(64) k_substep_batch16(const uint4* __restrict_
         }
         const float xl = x > 0 ? Store16<ST>::to_f(in[idx - 1]) : 0.0f;
         const float xr = x + 8 < nx ? Store16<ST>::to_f(in[idx + 8]) : 0.0f;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            const float xm = e == 0 ? xl : c[e - 1], xp = e == 7 ? xr : c[e + 1];
-            const float s6 = __fadd_rn(__fadd_rn(__fadd_rn(xm, xp), __fadd_rn(ym[e], yp[e])), __fadd_rn(zm[e], zp[e]));
-            v[e] = fmaxf(__fmul_rn(__fadd_rn(c[e], __fmul_rn(fs.r, __fsub_rn(s6, __fmul_rn(6.0f, c[e])))), fs.inv_decay),
-                         0.0f);
-        }
+        stencil_update8(xl, xr, c, ym, yp, zm, zp, fs.r, fs.inv_decay, v);
         if (edge_y || zz == 0 || zz == nz - 1) {
 #pragma unroll
             for (int e = 0; e < 8; ++e) v[e] = bf;

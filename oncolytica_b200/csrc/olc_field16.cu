@@ -17,6 +17,7 @@
 // error is what the FP64 comparison reports.  Every operation is separately
 // rounded, so the CPU restatement reproduces the bits.
 #include "olc_internal.h"
+#include "olc_stencil.cuh"
 #include "olc_store16.cuh"
 
 #include <cuda.h>
@@ -39,14 +40,6 @@ __device__ __forceinline__ bool mbar_wait_once(olc_u32 bar, olc_u32 parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     return ok != 0;
-}
-
-// One voxel's substep in FP32: the FP32 kernels' arithmetic (inv_decay is 1
-// for the storages that decay once per step in the reaction pass).
-__device__ __forceinline__ float diffuse1(float xm, float xp, float ym, float yp, float zm, float zp, float c, float r,
-                                         float inv_decay) {
-    const float s = __fadd_rn(__fadd_rn(__fadd_rn(xm, xp), __fadd_rn(ym, yp)), __fadd_rn(zm, zp));
-    return fmaxf(__fmul_rn(__fadd_rn(c, __fmul_rn(r, __fsub_rn(s, __fmul_rn(6.0f, c)))), inv_decay), 0.0f);
 }
 
 }  // namespace
@@ -177,10 +170,7 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep16(const __grid_constan
         load8<ST>(pc - WX, ym);
         load8<ST>(pc + WX, yp);
         const float xl = Store16<ST>::to_f(pc[-1]), xr = Store16<ST>::to_f(pc[8]);
-#pragma unroll
-        for (int e = 0; e < 8; ++e)
-            v[e] = diffuse1(e == 0 ? xl : c[e - 1], e == 7 ? xr : c[e + 1], ym[e], yp[e], zm[e], zp[e], c[e], r,
-                            inv_decay);
+        stencil_update8(xl, xr, c, ym, yp, zm, zp, r, inv_decay, v);
         if (edge_y || z == 0 || z == nz - 1) {
 #pragma unroll
             for (int e = 0; e < 8; ++e) v[e] = bf;

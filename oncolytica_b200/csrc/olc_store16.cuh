@@ -1,6 +1,6 @@
 // BF16 / FP16 storage of fields: conversions to and from FP32 (round to
-// nearest even) and 4-element vector loads and stores.  Bits are handled as
-// unsigned short.
+// nearest even, or stochastic for the _SR types) and 8-element vector loads
+// and stores.  Bits are handled as unsigned short.
 #pragma once
 #include "olc_device.cuh"
 #include "../../include/olc.h"
@@ -81,28 +81,6 @@ __device__ __forceinline__ olc_u32 olc_sr_pair(unsigned long long pair, olc_u32 
     return x ^ (x >> 15);
 }
 
-template <int ST>
-__device__ __forceinline__ float4 load4(const unsigned short* p) {
-    const uint2 raw = *reinterpret_cast<const uint2*>(p);
-    return make_float4(Store16<ST>::to_f((unsigned short)(raw.x & 0xffffu)), Store16<ST>::to_f((unsigned short)(raw.x >> 16)),
-                       Store16<ST>::to_f((unsigned short)(raw.y & 0xffffu)), Store16<ST>::to_f((unsigned short)(raw.y >> 16)));
-}
-
-// Stores four values at voxel index v (stochastic rounding for the _SR types).
-template <int ST>
-__device__ __forceinline__ void store4_at(unsigned short* p, float4 v, unsigned long long vi, olc_u32 key) {
-    if (IsSR<ST>::value) {  // vi is a multiple of 4
-        const olc_u32 r0 = olc_sr_pair(vi >> 1, key), r1 = olc_sr_pair((vi >> 1) + 1, key);
-        const olc_u32 lo = (olc_u32)olc_sr16<ST>(v.x, r0) | ((olc_u32)olc_sr16<ST>(v.y, r0 >> 16) << 16);
-        const olc_u32 hi = (olc_u32)olc_sr16<ST>(v.z, r1) | ((olc_u32)olc_sr16<ST>(v.w, r1 >> 16) << 16);
-        *reinterpret_cast<uint2*>(p) = make_uint2(lo, hi);
-        return;
-    }
-    const olc_u32 lo = (olc_u32)Store16<ST>::from_f(v.x) | ((olc_u32)Store16<ST>::from_f(v.y) << 16);
-    const olc_u32 hi = (olc_u32)Store16<ST>::from_f(v.z) | ((olc_u32)Store16<ST>::from_f(v.w) << 16);
-    *reinterpret_cast<uint2*>(p) = make_uint2(lo, hi);
-}
-
 // Eight consecutive values (16 bytes): load to FP32, store with rounding at
 // voxel index vi (a multiple of 8; stochastic for the _SR types).
 template <int ST>
@@ -116,27 +94,43 @@ __device__ __forceinline__ void load8(const unsigned short* p, float (&f)[8]) {
     }
 }
 
+// Two FP32 values -> one word of two 16-bit values (a in the low half, b in
+// the high half).  cvt.*x2 converts its first source into the high half.
+template <int ST>
+__device__ __forceinline__ olc_u32 pack2(float a, float b) {
+    olc_u32 d;
+    if (ST == OLC_FIELD_BF16 || ST == OLC_FIELD_BF16_SR)
+        asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(b), "f"(a));
+    else
+        asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(b), "f"(a));
+    return d;
+}
+
+// The same with stochastic rounding: a takes the low 16 random bits of rnd, b
+// the high 16 (olc_bf16_sr / olc_f16_sr on each value).
+template <int ST>
+__device__ __forceinline__ olc_u32 pack2_sr(float a, float b, olc_u32 rnd) {
+    if (ST == OLC_FIELD_BF16_SR) {
+        const olc_u32 ua = __float_as_uint(a) + (rnd & 0xffffu), ub = __float_as_uint(b) + (rnd >> 16);
+        return __byte_perm(ua, ub, 0x7632);  // high halves: ua's in the low half, ub's in the high
+    }
+    const float ga = __uint_as_float(__float_as_uint(a) + (rnd & 0x1fffu));
+    const float gb = __uint_as_float(__float_as_uint(b) + ((rnd >> 16) & 0x1fffu));
+    olc_u32 d;
+    asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(gb), "f"(ga));
+    return d;
+}
+
+// Eight values (16 bytes) stored at voxel index vi (a multiple of 8), rounded
+// to nearest even or, for the _SR types, stochastically with the pair hash.
 template <int ST>
 __device__ __forceinline__ void store8_at(unsigned short* p, const float (&v)[8], unsigned long long vi, olc_u32 key) {
     olc_u32 w[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        if (IsSR<ST>::value) {
-            const olc_u32 r = olc_sr_pair((vi >> 1) + k, key);
-            w[k] = (olc_u32)olc_sr16<ST>(v[2 * k], r) | ((olc_u32)olc_sr16<ST>(v[2 * k + 1], r >> 16) << 16);
-        } else {
-            w[k] = (olc_u32)Store16<ST>::from_f(v[2 * k]) | ((olc_u32)Store16<ST>::from_f(v[2 * k + 1]) << 16);
-        }
-    }
+    for (int k = 0; k < 4; ++k)
+        w[k] = IsSR<ST>::value ? pack2_sr<ST>(v[2 * k], v[2 * k + 1], olc_sr_pair((vi >> 1) + k, key))
+                               : pack2<ST>(v[2 * k], v[2 * k + 1]);
     *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
 }
-
-template <int ST>
-__device__ __forceinline__ void store4(unsigned short* p, float4 v) {
-    const olc_u32 lo = (olc_u32)Store16<ST>::from_f(v.x) | ((olc_u32)Store16<ST>::from_f(v.y) << 16);
-    const olc_u32 hi = (olc_u32)Store16<ST>::from_f(v.z) | ((olc_u32)Store16<ST>::from_f(v.w) << 16);
-    *reinterpret_cast<uint2*>(p) = make_uint2(lo, hi);
-}
-
 
 }  // namespace olc
