@@ -331,33 +331,7 @@ void launch_flip_parity(const FieldStep* steps, int field, int n_fields, olc_u32
 // The same tiles on BF16 / FP16 storage (olc_field16.cu's arithmetic): the
 // reaction pass with its FP32 residual, then the substeps (decaying in each
 // for the stochastically rounded storages).
-//
-// Substep: 64 threads per tile, eight x voxels per thread (16-byte loads and
-// stores), marching in z.  Each plane is converted to FP32 once: every thread
-// writes its row of the plane into a shared plane (18 rows x 40 floats: the
-// tile, one halo row above and below, one halo column left and right), which
-// its y and x neighbours read; the z neighbours stay in registers.  The next
-// plane's own row and halo are loaded one iteration ahead, and the shared
-// planes alternate, so one barrier per plane suffices.  Outputs on the grid's
-// faces are replaced by the boundary value, so halo values outside the grid
-// (left at zero) never reach a stored result.
-namespace b16 {
-constexpr int PX = BT_X + 8;  // plane row: x0 - 4 .. x0 + BT_X + 3 (own voxels from column 4)
-constexpr int PY = BT_Y + 2;
-}  // namespace b16
-
-__device__ __forceinline__ uint4 ld16b(const unsigned short* p) { return *reinterpret_cast<const uint4*>(p); }
-
-template <int ST>
-__device__ __forceinline__ void unpack8(uint4 raw, float (&f)[8]) {
-    const olc_u32 w[4] = {raw.x, raw.y, raw.z, raw.w};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        f[2 * k] = Store16<ST>::to_f((unsigned short)(w[k] & 0xffffu));
-        f[2 * k + 1] = Store16<ST>::to_f((unsigned short)(w[k] >> 16));
-    }
-}
-
+// Eight voxels per thread (16-byte loads and stores), 64 threads per tile.
 template <int ST>
 __global__ void __launch_bounds__(64) k_substep_batch16(const uint4* __restrict__ tiles,
                                                         const OlcSimDesc* __restrict__ sims,
@@ -365,8 +339,6 @@ __global__ void __launch_bounds__(64) k_substep_batch16(const uint4* __restrict_
                                                         const unsigned char* __restrict__ fpar, int sub,
                                                         unsigned short* fa, unsigned short* fb,
                                                         const olc_u32* step_ctr) {
-    using namespace b16;
-    __shared__ __align__(16) float pl[2][PY][PX];
     const uint4 t = tiles[blockIdx.x];
     const olc_u32 k = t.x;
     const OlcSimDesc& d = sims[k];
@@ -375,106 +347,60 @@ __global__ void __launch_bounds__(64) k_substep_batch16(const uint4* __restrict_
     const bool flip = ((fpar[(size_t)k * n_fields + field] ^ (unsigned)sub) & 1u) != 0u;
     const unsigned short* in = (flip ? fb : fa) + d.field_off;
     unsigned short* out = (flip ? fa : fb) + d.field_off;
-    const int tid = threadIdx.x, g = tid & 3, ty = tid >> 2;
-    const int x0 = (int)t.y * BT_X, y0 = (int)t.z * BT_Y, z0 = (int)t.w * BT_Z;
-    const int x = x0 + 8 * g, y = y0 + ty;
-    const bool act = x < nx && y < ny;
+    const int x = (int)t.y * BT_X + 8 * (threadIdx.x & 3);
+    const int y = (int)t.z * BT_Y + (threadIdx.x >> 2);
+    const int z0 = (int)t.w * BT_Z;
+    if (x >= nx || y >= ny) return;
     const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
-    // halo duty: threads 0-7 load a row segment above / below the tile,
-    // threads 8-39 one voxel left / right of it
-    int h_kind = 0, h_r = 0, h_c = 0;
-    size_t h_off = 0;
-    if (tid < 8) {
-        const int hy = tid < 4 ? y0 - 1 : y0 + BT_Y, hx = x0 + 8 * (tid & 3);
-        if (hy >= 0 && hy < ny && hx < nx) {
-            h_kind = 1;
-            h_off = (size_t)hy * sy + hx;
-            h_r = tid < 4 ? 0 : BT_Y + 1;
-            h_c = 4 + 8 * (tid & 3);
-        }
-    } else if (tid < 40) {
-        const int j = tid - 8, hy = y0 + (j & 15), hx = (j >> 4) ? x0 + BT_X : x0 - 1;
-        if (hy < ny && hx >= 0 && hx < nx) {
-            h_kind = 2;
-            h_off = (size_t)hy * sy + hx;
-            h_r = (j & 15) + 1;
-            h_c = (j >> 4) ? 4 + BT_X : 3;
-        }
-    }
-    for (int i = tid; i < 2 * PY * PX / 4; i += 64) reinterpret_cast<float4*>(&pl[0][0][0])[i] = make_float4(0, 0, 0, 0);
     const bool edge_y = y == 0 || y == ny - 1;
     const bool ex0 = x == 0, ex7 = x + 7 == nx - 1;
     const float bf = Store16<ST>::to_f(Store16<ST>::from_f(fs.bval));
     const olc_u32 key = olc_sr_key(*step_ctr - d.step_base, sub, field);  // the simulation's own step
-    const size_t own = (size_t)y * sy + x;
+    size_t idx = (size_t)z0 * sz + (size_t)y * sy + x;
     float zm[8], c[8], zp[8], ym[8], yp[8], v[8];
-    const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
-    uint4 hraw = zero4;
-    unsigned short hs = 0;
-    if (act) {
-        unpack8<ST>(z0 > 0 ? ld16b(in + (size_t)(z0 - 1) * sz + own) : zero4, zm);
-        unpack8<ST>(ld16b(in + (size_t)z0 * sz + own), c);
+    if (z0 > 0) {
+        load8<ST>(in + idx - sz, zm);
+    } else {
+#pragma unroll
+        for (int e = 0; e < 8; ++e) zm[e] = 0.0f;
     }
-    if (h_kind == 1) hraw = ld16b(in + (size_t)z0 * sz + h_off);
-    if (h_kind == 2) hs = in[(size_t)z0 * sz + h_off];
+    load8<ST>(in + idx, c);
     const int z1 = min(z0 + BT_Z, nz);
-    __syncthreads();  // planes zeroed
-#pragma unroll 2
-    for (int zz = z0; zz < z1; ++zz) {
-        const int b = zz & 1;
-        // the next plane's own row and halo, one iteration ahead
-        const bool more = zz + 1 < nz;
-        const uint4 zraw = act && more ? ld16b(in + (size_t)(zz + 1) * sz + own) : zero4;
-        uint4 hraw_n = zero4;
-        unsigned short hs_n = 0;
-        if (zz + 1 < z1) {
-            if (h_kind == 1) hraw_n = ld16b(in + (size_t)(zz + 1) * sz + h_off);
-            if (h_kind == 2) hs_n = in[(size_t)(zz + 1) * sz + h_off];
-        }
-        // this plane into the shared plane b
-        if (act) {
-            float4* row = reinterpret_cast<float4*>(&pl[b][ty + 1][4 + 8 * g]);
-            row[0] = make_float4(c[0], c[1], c[2], c[3]);
-            row[1] = make_float4(c[4], c[5], c[6], c[7]);
-        }
-        if (h_kind == 1) {
-            float hv[8];
-            unpack8<ST>(hraw, hv);
-            float4* row = reinterpret_cast<float4*>(&pl[b][h_r][h_c]);
-            row[0] = make_float4(hv[0], hv[1], hv[2], hv[3]);
-            row[1] = make_float4(hv[4], hv[5], hv[6], hv[7]);
-        } else if (h_kind == 2) {
-            pl[b][h_r][h_c] = Store16<ST>::to_f(hs);
-        }
-        __syncthreads();
-        if (act) {
-            const float4* rm = reinterpret_cast<const float4*>(&pl[b][ty][4 + 8 * g]);
-            const float4* rp = reinterpret_cast<const float4*>(&pl[b][ty + 2][4 + 8 * g]);
-            const float4 a0 = rm[0], a1 = rm[1], p0 = rp[0], p1 = rp[1];
-            ym[0] = a0.x; ym[1] = a0.y; ym[2] = a0.z; ym[3] = a0.w;
-            ym[4] = a1.x; ym[5] = a1.y; ym[6] = a1.z; ym[7] = a1.w;
-            yp[0] = p0.x; yp[1] = p0.y; yp[2] = p0.z; yp[3] = p0.w;
-            yp[4] = p1.x; yp[5] = p1.y; yp[6] = p1.z; yp[7] = p1.w;
-            const float xl = pl[b][ty + 1][3 + 8 * g], xr = pl[b][ty + 1][12 + 8 * g];
-            unpack8<ST>(zraw, zp);
-            stencil_update8(xl, xr, c, ym, yp, zm, zp, fs.r, fs.inv_decay, v);
-            if (edge_y || zz == 0 || zz == nz - 1) {
+    for (int zz = z0; zz < z1; ++zz, idx += sz) {
+        if (zz + 1 < nz) {
+            load8<ST>(in + idx + sz, zp);
+        } else {
 #pragma unroll
-                for (int e = 0; e < 8; ++e) v[e] = bf;
-            } else {
-                if (ex0) v[0] = bf;
-                if (ex7) v[7] = bf;
-            }
-            const size_t idx = (size_t)zz * sz + own;
-            store8_at<ST>(out + idx, v, idx, key);
-#pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                zm[e] = c[e];
-                c[e] = zp[e];
-            }
+            for (int e = 0; e < 8; ++e) zp[e] = 0.0f;
         }
-        hraw = hraw_n;
-        hs = hs_n;
+        if (y > 0) {
+            load8<ST>(in + idx - sy, ym);
+        } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) ym[e] = 0.0f;
+        }
+        if (y + 1 < ny) {
+            load8<ST>(in + idx + sy, yp);
+        } else {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) yp[e] = 0.0f;
+        }
+        const float xl = x > 0 ? Store16<ST>::to_f(in[idx - 1]) : 0.0f;
+        const float xr = x + 8 < nx ? Store16<ST>::to_f(in[idx + 8]) : 0.0f;
+        stencil_update8(xl, xr, c, ym, yp, zm, zp, fs.r, fs.inv_decay, v);
+        if (edge_y || zz == 0 || zz == nz - 1) {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) v[e] = bf;
+        } else {
+            if (ex0) v[0] = bf;
+            if (ex7) v[7] = bf;
+        }
+        store8_at<ST>(out + idx, v, idx, key);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            zm[e] = c[e];
+            c[e] = zp[e];
+        }
     }
 }
 
