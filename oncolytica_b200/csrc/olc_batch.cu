@@ -21,7 +21,6 @@
 // bit.  The FP64 sums of the per-simulation reductions are accumulated with
 // atomics and are exact only up to their order.
 #include "olc_internal.h"
-#include "olc_stencil.cuh"
 #include "olc_store16.cuh"
 
 namespace olc {
@@ -201,78 +200,12 @@ void launch_contact_batch(const BatchArgs& b, const float4* posr, const olc_u32*
 }
 
 // ------------------------------------------------------------------ fields
-// A field tile: BT_X x BT_Y x BT_Z voxels of one simulation's grid.  128
-// threads, each owning four consecutive x voxels of one row and walking the
-// tile's planes with the z neighbours in registers.  Neighbours are read with
-// plain loads (grids of a batch are small and stay in L2); reads that would
-// leave the grid return 0 and only ever feed face voxels, which are pinned.
+// A field tile of the per-voxel passes (sink, reaction, reductions): BT_X x
+// BT_Y x BT_Z voxels of one simulation's grid, 128 threads.  The substeps run
+// on TMA tiles of their own geometry (k_substep_batch_x4, k_substep_batch_t16).
 constexpr int BT_X = BATCH_TILE_X, BT_Y = BATCH_TILE_Y, BT_Z = BATCH_TILE_Z;
 
 __device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
-
-__device__ __forceinline__ float4 update4_b(float xl, float xr, float4 c, float4 ym, float4 yp, float4 zm,
-                                            float4 zp, float r, float inv_decay) {
-    float4 v;
-    v.x = __fadd_rn(__fadd_rn(__fadd_rn(xl, c.y), __fadd_rn(ym.x, yp.x)), __fadd_rn(zm.x, zp.x));
-    v.y = __fadd_rn(__fadd_rn(__fadd_rn(c.x, c.z), __fadd_rn(ym.y, yp.y)), __fadd_rn(zm.y, zp.y));
-    v.z = __fadd_rn(__fadd_rn(__fadd_rn(c.y, c.w), __fadd_rn(ym.z, yp.z)), __fadd_rn(zm.z, zp.z));
-    v.w = __fadd_rn(__fadd_rn(__fadd_rn(c.z, xr), __fadd_rn(ym.w, yp.w)), __fadd_rn(zm.w, zp.w));
-    v.x = fmaxf(__fmul_rn(__fadd_rn(c.x, __fmul_rn(r, __fsub_rn(v.x, __fmul_rn(6.0f, c.x)))), inv_decay), 0.0f);
-    v.y = fmaxf(__fmul_rn(__fadd_rn(c.y, __fmul_rn(r, __fsub_rn(v.y, __fmul_rn(6.0f, c.y)))), inv_decay), 0.0f);
-    v.z = fmaxf(__fmul_rn(__fadd_rn(c.z, __fmul_rn(r, __fsub_rn(v.z, __fmul_rn(6.0f, c.z)))), inv_decay), 0.0f);
-    v.w = fmaxf(__fmul_rn(__fadd_rn(c.w, __fmul_rn(r, __fsub_rn(v.w, __fmul_rn(6.0f, c.w)))), inv_decay), 0.0f);
-    return v;
-}
-
-__global__ void __launch_bounds__(128) k_substep_batch(const uint4* __restrict__ tiles,
-                                                       const OlcSimDesc* __restrict__ sims,
-                                                       const FieldStep* __restrict__ steps, int field, int n_fields,
-                                                       const unsigned char* __restrict__ fpar, int sub,
-                                                       float* fa, float* fb) {
-    const uint4 t = tiles[blockIdx.x];
-    const olc_u32 k = t.x;
-    const OlcSimDesc& d = sims[k];
-    const FieldStep fs = steps[(size_t)k * n_fields + field];
-    const int nx = d.cdims[0], ny = d.cdims[1], nz = d.cdims[2];
-    const bool flip = ((fpar[(size_t)k * n_fields + field] ^ (unsigned)sub) & 1u) != 0u;
-    const float* in = (flip ? fb : fa) + d.field_off;
-    float* out = (flip ? fa : fb) + d.field_off;
-    const int x = (int)t.y * BT_X + 4 * (threadIdx.x & 7);
-    const int y = (int)t.z * BT_Y + (threadIdx.x >> 3);
-    const int z0 = (int)t.w * BT_Z;
-    if (x >= nx || y >= ny) return;
-    const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
-    const bool edge_y = y == 0 || y == ny - 1;
-    const bool ex0 = x == 0, ex3 = x + 3 == nx - 1;
-    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    size_t idx = (size_t)z0 * sz + (size_t)y * sy + x;
-    float4 zm = z0 > 0 ? ld4(in + idx - sz) : zero;
-    float4 c = ld4(in + idx);
-    const int z1 = min(z0 + BT_Z, nz);
-    for (int zz = z0; zz < z1; ++zz, idx += sz) {
-        const float4 zp = zz + 1 < nz ? ld4(in + idx + sz) : zero;
-        const float4 ym = y > 0 ? ld4(in + idx - sy) : zero;
-        const float4 yp = y + 1 < ny ? ld4(in + idx + sy) : zero;
-        const float xl = x > 0 ? __ldg(in + idx - 1) : 0.0f;
-        const float xr = x + 4 < nx ? __ldg(in + idx + 4) : 0.0f;
-        float4 v = update4_b(xl, xr, c, ym, yp, zm, zp, fs.r, fs.inv_decay);
-        if (edge_y || zz == 0 || zz == nz - 1) {
-            v = make_float4(fs.bval, fs.bval, fs.bval, fs.bval);
-        } else {
-            if (ex0) v.x = fs.bval;
-            if (ex3) v.w = fs.bval;
-        }
-        *reinterpret_cast<float4*>(out + idx) = v;
-        zm = c;
-        c = zp;
-    }
-}
-
-void launch_substep_batch(const BatchArgs& b, const uint4* tiles, olc_u32 n_tiles, const FieldStep* steps, int field,
-                          int n_fields, const unsigned char* fpar, int sub, float* fa, float* fb, cudaStream_t s) {
-    if (n_tiles == 0) return;
-    k_substep_batch<<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, fa, fb);
-}
 
 // f <- f / (1 + K dt) on interior voxels, K <- 0, per tile (as k_sink).
 __global__ void __launch_bounds__(128) k_sink_batch(const uint4* __restrict__ tiles,
@@ -328,82 +261,8 @@ void launch_flip_parity(const FieldStep* steps, int field, int n_fields, olc_u32
 }
 
 // ------------------------------------------------------------------ 16-bit fields
-// The same tiles on BF16 / FP16 storage (olc_field16.cu's arithmetic): the
-// reaction pass with its FP32 residual, then the substeps (decaying in each
-// for the stochastically rounded storages).
-// Eight voxels per thread (16-byte loads and stores), 64 threads per tile.
-template <int ST>
-__global__ void __launch_bounds__(64) k_substep_batch16(const uint4* __restrict__ tiles,
-                                                        const OlcSimDesc* __restrict__ sims,
-                                                        const FieldStep* __restrict__ steps, int field, int n_fields,
-                                                        const unsigned char* __restrict__ fpar, int sub,
-                                                        unsigned short* fa, unsigned short* fb,
-                                                        const olc_u32* step_ctr) {
-    const uint4 t = tiles[blockIdx.x];
-    const olc_u32 k = t.x;
-    const OlcSimDesc& d = sims[k];
-    const FieldStep fs = steps[(size_t)k * n_fields + field];
-    const int nx = d.cdims[0], ny = d.cdims[1], nz = d.cdims[2];
-    const bool flip = ((fpar[(size_t)k * n_fields + field] ^ (unsigned)sub) & 1u) != 0u;
-    const unsigned short* in = (flip ? fb : fa) + d.field_off;
-    unsigned short* out = (flip ? fa : fb) + d.field_off;
-    const int x = (int)t.y * BT_X + 8 * (threadIdx.x & 3);
-    const int y = (int)t.z * BT_Y + (threadIdx.x >> 2);
-    const int z0 = (int)t.w * BT_Z;
-    if (x >= nx || y >= ny) return;
-    const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
-    const bool edge_y = y == 0 || y == ny - 1;
-    const bool ex0 = x == 0, ex7 = x + 7 == nx - 1;
-    const float bf = Store16<ST>::to_f(Store16<ST>::from_f(fs.bval));
-    const olc_u32 key = olc_sr_key(*step_ctr - d.step_base, sub, field);  // the simulation's own step
-    size_t idx = (size_t)z0 * sz + (size_t)y * sy + x;
-    float zm[8], c[8], zp[8], ym[8], yp[8], v[8];
-    if (z0 > 0) {
-        load8<ST>(in + idx - sz, zm);
-    } else {
-#pragma unroll
-        for (int e = 0; e < 8; ++e) zm[e] = 0.0f;
-    }
-    load8<ST>(in + idx, c);
-    const int z1 = min(z0 + BT_Z, nz);
-    for (int zz = z0; zz < z1; ++zz, idx += sz) {
-        if (zz + 1 < nz) {
-            load8<ST>(in + idx + sz, zp);
-        } else {
-#pragma unroll
-            for (int e = 0; e < 8; ++e) zp[e] = 0.0f;
-        }
-        if (y > 0) {
-            load8<ST>(in + idx - sy, ym);
-        } else {
-#pragma unroll
-            for (int e = 0; e < 8; ++e) ym[e] = 0.0f;
-        }
-        if (y + 1 < ny) {
-            load8<ST>(in + idx + sy, yp);
-        } else {
-#pragma unroll
-            for (int e = 0; e < 8; ++e) yp[e] = 0.0f;
-        }
-        const float xl = x > 0 ? Store16<ST>::to_f(in[idx - 1]) : 0.0f;
-        const float xr = x + 8 < nx ? Store16<ST>::to_f(in[idx + 8]) : 0.0f;
-        stencil_update8(xl, xr, c, ym, yp, zm, zp, fs.r, fs.inv_decay, v);
-        if (edge_y || zz == 0 || zz == nz - 1) {
-#pragma unroll
-            for (int e = 0; e < 8; ++e) v[e] = bf;
-        } else {
-            if (ex0) v[0] = bf;
-            if (ex7) v[7] = bf;
-        }
-        store8_at<ST>(out + idx, v, idx, key);
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            zm[e] = c[e];
-            c[e] = zp[e];
-        }
-    }
-}
-
+// The reaction pass and the reductions on BF16 / FP16 storage
+// (olc_field16.cu's arithmetic).
 template <int ST>
 __global__ void __launch_bounds__(128) k_react_batch16(const uint4* __restrict__ tiles,
                                                        const OlcSimDesc* __restrict__ sims,
@@ -494,26 +353,6 @@ __global__ void __launch_bounds__(128) k_reduce_field_batch16(const uint4* __res
         atomicMin(reinterpret_cast<unsigned long long*>(&out[k].field_min[field]), (unsigned long long)__double_as_longlong(lo));
         atomicMax(reinterpret_cast<unsigned long long*>(&out[k].field_max[field]), (unsigned long long)__double_as_longlong(hi));
     }
-}
-
-void launch_substep_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
-                            const FieldStep* steps, int field, int n_fields, const unsigned char* fpar, int sub,
-                            void* fa, void* fb, const olc_u32* step_ctr, cudaStream_t s) {
-    if (n_tiles == 0) return;
-    unsigned short* a = static_cast<unsigned short*>(fa);
-    unsigned short* c = static_cast<unsigned short*>(fb);
-    if (storage == OLC_FIELD_BF16)
-        k_substep_batch16<OLC_FIELD_BF16><<<n_tiles, 64, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a, c,
-                                                                   step_ctr);
-    else if (storage == OLC_FIELD_BF16_SR)
-        k_substep_batch16<OLC_FIELD_BF16_SR><<<n_tiles, 64, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a,
-                                                                      c, step_ctr);
-    else if (storage == OLC_FIELD_F16_SR)
-        k_substep_batch16<OLC_FIELD_F16_SR><<<n_tiles, 64, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a,
-                                                                     c, step_ctr);
-    else
-        k_substep_batch16<OLC_FIELD_F16><<<n_tiles, 64, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, a, c,
-                                                                  step_ctr);
 }
 
 void launch_react_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,

@@ -101,6 +101,55 @@ constexpr unsigned BYTES = WX * WY * WZ * 2;
 constexpr size_t SMEM = BYTES + 16 + 128;
 }  // namespace t16
 
+// The 64 x TYR x TZ output block at (x0, y0, z0) from its staged 16-bit box
+// (stochastic-rounding key given).
+template <int ST>
+__device__ __forceinline__ void t16_tile(const unsigned short* tile, unsigned short* __restrict__ out, int x0, int y0,
+                                         int z0, int nx, int ny, int nz, float r, float inv_decay, float bval,
+                                         olc_u32 key) {
+    using namespace t16;
+    const int g = threadIdx.x & 7, ty = threadIdx.x >> 3;
+    const int x = x0 + 8 * g, y = y0 + ty;
+    if (x >= nx || y >= ny) return;
+    const bool edge_y = y == 0 || y == ny - 1;
+    const bool ex0 = x == 0, ex7 = x + 7 == nx - 1;
+    constexpr int PS = WY * WX;
+    const unsigned short* col = tile + (ty + 1) * WX + HX + 8 * g;
+    float zm[8], c[8], zp[8], ym[8], yp[8], v[8];
+    load8<ST>(col, zm);
+    load8<ST>(col + PS, c);
+    const size_t sz = (size_t)nx * ny;
+    unsigned short* o = out + (size_t)z0 * sz + (size_t)y * nx + x;
+    const float bf = Store16<ST>::to_f(Store16<ST>::from_f(bval));  // the face value as stored
+    unsigned long long vi = (unsigned long long)z0 * sz + (unsigned long long)y * nx + x;
+#pragma unroll 2
+    for (int lz = 1; lz <= TZ; ++lz) {
+        const int z = z0 + lz - 1;
+        if (z >= nz) break;
+        const unsigned short* pc = col + lz * PS;
+        load8<ST>(pc + PS, zp);
+        load8<ST>(pc - WX, ym);
+        load8<ST>(pc + WX, yp);
+        const float xl = Store16<ST>::to_f(pc[-1]), xr = Store16<ST>::to_f(pc[8]);
+        stencil_update8(xl, xr, c, ym, yp, zm, zp, r, inv_decay, v);
+        if (edge_y || z == 0 || z == nz - 1) {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) v[e] = bf;
+        } else {
+            if (ex0) v[0] = bf;
+            if (ex7) v[7] = bf;
+        }
+        store8_at<ST>(o, v, vi, key);
+        o += sz;
+        vi += sz;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            zm[e] = c[e];
+            c[e] = zp[e];
+        }
+    }
+}
+
 template <int ST>
 __global__ void __launch_bounds__(t16::THREADS) k_substep16(const __grid_constant__ CUtensorMap in_map,
                                                            unsigned short* __restrict__ out, int nx, int ny, int nz,
@@ -146,47 +195,101 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep16(const __grid_constan
         }
         return;
     }
-    const int g = threadIdx.x & 7, ty = threadIdx.x >> 3;
-    const int x = x0 + 8 * g, y = y0 + ty;
-    if (x >= nx || y >= ny) return;
-    const bool edge_y = y == 0 || y == ny - 1;
-    const bool ex0 = x == 0, ex7 = x + 7 == nx - 1;
-    constexpr int PS = WY * WX;
-    const unsigned short* col = tile + (ty + 1) * WX + HX + 8 * g;
-    float zm[8], c[8], zp[8], ym[8], yp[8], v[8];
-    load8<ST>(col, zm);
-    load8<ST>(col + PS, c);
-    const size_t sz = (size_t)nx * ny;
-    unsigned short* o = out + (size_t)z0 * sz + (size_t)y * nx + x;
-    const float bf = Store16<ST>::to_f(Store16<ST>::from_f(bval));  // the face value as stored
-    const olc_u32 key = olc_sr_key(step_ctr ? *step_ctr : step_host, sub, field);
-    unsigned long long vi = (unsigned long long)z0 * sz + (unsigned long long)y * nx + x;
-#pragma unroll 2
-    for (int lz = 1; lz <= TZ; ++lz) {
-        const int z = z0 + lz - 1;
-        if (z >= nz) break;
-        const unsigned short* pc = col + lz * PS;
-        load8<ST>(pc + PS, zp);
-        load8<ST>(pc - WX, ym);
-        load8<ST>(pc + WX, yp);
-        const float xl = Store16<ST>::to_f(pc[-1]), xr = Store16<ST>::to_f(pc[8]);
-        stencil_update8(xl, xr, c, ym, yp, zm, zp, r, inv_decay, v);
-        if (edge_y || z == 0 || z == nz - 1) {
-#pragma unroll
-            for (int e = 0; e < 8; ++e) v[e] = bf;
-        } else {
-            if (ex0) v[0] = bf;
-            if (ex7) v[7] = bf;
-        }
-        store8_at<ST>(o, v, vi, key);
-        o += sz;
-        vi += sz;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-            zm[e] = c[e];
-            c[e] = zp[e];
+    t16_tile<ST>(tile, out, x0, y0, z0, nx, ny, nz, r, inv_decay, bval,
+                 olc_sr_key(step_ctr ? *step_ctr : step_host, sub, field));
+}
+
+// ------------------------------------------------------------------ batched substep
+// k_substep16's tile on one member of a batch (as k_substep_batch_x4 does for
+// FP32): tile list entry blockIdx.x names the member and the tile, the
+// member's tensor maps come from a table in device memory, and the
+// stochastic-rounding key counts the member's own steps.
+static_assert(t16::TX == BATCH_T16_TX && t16::TYR == BATCH_T16_TY && t16::TZ == BATCH_T16_TZ, "batched 16-bit tile");
+
+template <int ST>
+__global__ void __launch_bounds__(t16::THREADS) k_substep_batch_t16(
+    const uint4* __restrict__ tiles, const OlcSimDesc* __restrict__ sims, const FieldStep* __restrict__ steps,
+    const CUtensorMap* __restrict__ maps, int field, int n_fields, const unsigned char* __restrict__ fpar, int sub,
+    unsigned short* fa, unsigned short* fb, const olc_u32* step_ctr, olc_u32* status) {
+    using namespace t16;
+    extern __shared__ unsigned char t16_raw[];
+    const olc_u32 pad = (128u - (smem_addr(t16_raw) & 127u)) & 127u;
+    unsigned short* tile = reinterpret_cast<unsigned short*>(t16_raw + pad);
+    const olc_u32 bar = smem_addr(t16_raw + pad + BYTES);
+    const uint4 t = tiles[blockIdx.x];
+    const OlcSimDesc& d = sims[t.x];
+    const size_t j = (size_t)t.x * n_fields + field;
+    const FieldStep fs = steps[j];
+    const bool flip = ((fpar[j] ^ (unsigned)sub) & 1u) != 0u;
+    const CUtensorMap* map = maps + 2 * j + (flip ? 1 : 0);
+    unsigned short* out = (flip ? fa : fb) + d.field_off;
+    const int x0 = (int)t.y * TX, y0 = (int)t.z * TYR, z0 = (int)t.w * TZ;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(BYTES) : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+            "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(tile)),
+            "l"(reinterpret_cast<unsigned long long>(map)), "r"(x0 - HX), "r"(y0 - 1), "r"(z0 - 1), "r"(bar)
+            : "memory");
+    }
+    bool ready = false;
+    for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it) {
+        if (mbar_wait_once(bar, 0)) {
+            ready = true;
+            break;
         }
     }
+    if (!ready) {
+        if (threadIdx.x == 0) atomicOr(status, OLC_ST_TIMEOUT);
+        for (olc_u32 it = 0; it < OLC_SPIN_LIMIT && !mbar_wait_once(bar, 0); ++it) {
+        }
+        return;
+    }
+    t16_tile<ST>(tile, out, x0, y0, z0, d.cdims[0], d.cdims[1], d.cdims[2], fs.r, fs.inv_decay, fs.bval,
+                 olc_sr_key(*step_ctr - d.step_base, sub, field));
+}
+
+template <int ST>
+static void launch_bt16(const uint4* tiles, olc_u32 n_tiles, const OlcSimDesc* sims, const FieldStep* steps,
+                        const CUtensorMap* maps, int field, int n_fields, const unsigned char* fpar, int sub,
+                        void* fa, void* fb, const olc_u32* step_ctr, olc_u32* status, cudaStream_t s) {
+    using namespace t16;
+    static int configured_mask = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 32 && !(configured_mask & (1 << dev))) {
+        cudaFuncSetAttribute(k_substep_batch_t16<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+        configured_mask |= 1 << dev;
+    }
+    k_substep_batch_t16<ST><<<n_tiles, THREADS, SMEM, s>>>(tiles, sims, steps, maps, field, n_fields, fpar, sub,
+                                                          static_cast<unsigned short*>(fa),
+                                                          static_cast<unsigned short*>(fb), step_ctr, status);
+}
+
+void launch_substep_batch_t16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
+                              const FieldStep* steps, const CUtensorMap* maps, int field, int n_fields,
+                              const unsigned char* fpar, int sub, void* fa, void* fb, const olc_u32* step_ctr,
+                              olc_u32* status, cudaStream_t s) {
+    if (n_tiles == 0) return;
+    if (storage == OLC_FIELD_BF16)
+        launch_bt16<OLC_FIELD_BF16>(tiles, n_tiles, b.sims, steps, maps, field, n_fields, fpar, sub, fa, fb, step_ctr,
+                                    status, s);
+    else if (storage == OLC_FIELD_BF16_SR)
+        launch_bt16<OLC_FIELD_BF16_SR>(tiles, n_tiles, b.sims, steps, maps, field, n_fields, fpar, sub, fa, fb,
+                                       step_ctr, status, s);
+    else if (storage == OLC_FIELD_F16_SR)
+        launch_bt16<OLC_FIELD_F16_SR>(tiles, n_tiles, b.sims, steps, maps, field, n_fields, fpar, sub, fa, fb,
+                                      step_ctr, status, s);
+    else
+        launch_bt16<OLC_FIELD_F16>(tiles, n_tiles, b.sims, steps, maps, field, n_fields, fpar, sub, fa, fb, step_ctr,
+                                   status, s);
 }
 
 bool make_field_maps16(FieldMaps16* m, void* a, void* b, const int dims[3]) {

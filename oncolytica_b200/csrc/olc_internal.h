@@ -212,8 +212,21 @@ void launch_contact_batch(const BatchArgs& b, const float4* posr, const olc_u32*
 // Field tiles: uint4 (simulation, tile x, tile y, tile z) of BATCH_TILE_X x
 // BATCH_TILE_Y x BATCH_TILE_Z voxels.
 constexpr int BATCH_TILE_X = 32, BATCH_TILE_Y = 16, BATCH_TILE_Z = 16;
-void launch_substep_batch(const BatchArgs& b, const uint4* tiles, olc_u32 n_tiles, const FieldStep* steps, int field,
-                          int n_fields, const unsigned char* fpar, int sub, float* fa, float* fb, cudaStream_t s);
+// Substeps of a batch on TMA tiles (olc_field.cu, olc_field16.cu): the
+// per-field substep tile lists use these geometries (FP32: k_substep_x4's
+// 64 x 8 x 8 tile; 16-bit: k_substep16's 64 x 16 x 8), and each member's grid
+// is read through its tensor maps (maps[2 * (member * n_fields + field) + buffer],
+// boxes from batch_substep_box).
+constexpr int BATCH_X4_TX = 64, BATCH_X4_TY = 8, BATCH_X4_TZ = 8;
+constexpr int BATCH_T16_TX = 64, BATCH_T16_TY = 16, BATCH_T16_TZ = 8;
+void batch_substep_box(int storage, cuuint32_t box[3]);
+void launch_substep_batch_x4(const BatchArgs& b, const uint4* tiles, olc_u32 n_tiles, const FieldStep* steps,
+                             const CUtensorMap* maps, int field, int n_fields, const unsigned char* fpar, int sub,
+                             float* fa, float* fb, olc_u32* status, cudaStream_t s);
+void launch_substep_batch_t16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
+                              const FieldStep* steps, const CUtensorMap* maps, int field, int n_fields,
+                              const unsigned char* fpar, int sub, void* fa, void* fb, const olc_u32* step_ctr,
+                              olc_u32* status, cudaStream_t s);
 void launch_sink_batch(const BatchArgs& b, const uint4* tiles, olc_u32 n_tiles, const FieldStep* steps, int field,
                        int n_fields, const unsigned char* fpar, float* fa, float* fb, float* sink, cudaStream_t s);
 void launch_flip_parity(const FieldStep* steps, int field, int n_fields, olc_u32 n_sims, unsigned char* fpar,
@@ -224,9 +237,6 @@ void launch_reduce_field_batch(const BatchArgs& b, const uint4* tiles, olc_u32 n
                                const unsigned char* fpar, const float* fa, const float* fb, OlcReductions* out,
                                cudaStream_t s);
 void launch_reset_reductions_batch(OlcReductions* out, olc_u32 n_sims, cudaStream_t s);
-void launch_substep_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
-                            const FieldStep* steps, int field, int n_fields, const unsigned char* fpar, int sub,
-                            void* fa, void* fb, const olc_u32* step_ctr, cudaStream_t s);
 void launch_react_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
                           const FieldStep* steps, int field, int n_fields, const unsigned char* fpar, void* fa,
                           void* fb, float* sink, float* comp, cudaStream_t s);

@@ -127,7 +127,9 @@ struct OlcSim {
     std::vector<FieldStep> bsteps_host;
     uint4* btiles_all = nullptr;                      // every field tile, simulation order
     olc_u32 n_btiles = 0;
-    uint4* btiles_field[OLC_MAX_FIELDS] = {};         // per field, by substep count (descending)
+    uint4* btiles_field[OLC_MAX_FIELDS] = {};         // per field, by substep count (descending), substep tiles
+    std::vector<CUtensorMap> bmaps_host;              // [(simulation * n_fields + field) * 2 + buffer]
+    CUtensorMap* bmaps_dev = nullptr;
     std::vector<olc_u32> btile_count[OLC_MAX_FIELDS];  // [s] = tiles of simulations taking > s substeps
     OlcReductions* red_batch_dev = nullptr;
     OlcReductions* red_batch_host = nullptr;          // pinned
@@ -470,12 +472,13 @@ int step_once_batch(OlcSim* s, int collect, cudaStream_t st) {
         const int stor = s->fstep[f].storage;
         for (size_t sub = 0; sub < cnt.size(); ++sub) {
             if (stor != OLC_FIELD_F32)
-                launch_substep_batch16(B, stor, s->btiles_field[f], cnt[sub], s->bsteps_dev, (int)f, (int)F,
-                                       s->fpar_dev, (int)sub, s->field[0][f], s->field[1][f],
-                                       s->counters + OLC_CTR_FIELD_STEP, st);
+                launch_substep_batch_t16(B, stor, s->btiles_field[f], cnt[sub], s->bsteps_dev, s->bmaps_dev, (int)f,
+                                         (int)F, s->fpar_dev, (int)sub, s->field[0][f], s->field[1][f],
+                                         s->counters + OLC_CTR_FIELD_STEP, s->counters + OLC_CTR_STATUS, st);
             else
-                launch_substep_batch(B, s->btiles_field[f], cnt[sub], s->bsteps_dev, (int)f, (int)F, s->fpar_dev,
-                                     (int)sub, s->field[0][f], s->field[1][f], st);
+                launch_substep_batch_x4(B, s->btiles_field[f], cnt[sub], s->bsteps_dev, s->bmaps_dev, (int)f, (int)F,
+                                        s->fpar_dev, (int)sub, s->field[0][f], s->field[1][f],
+                                        s->counters + OLC_CTR_STATUS, st);
             ++launches;
         }
         substeps += (uint32_t)cnt.size();
@@ -690,6 +693,29 @@ void pool_tiles(const OlcGeom& g, olc_u32 slot, std::vector<uint4>* out) {
             for (int x = 0; x < tx; ++x) out->push_back(make_uint4(slot, (unsigned)x, (unsigned)y, (unsigned)z));
 }
 
+// Substep tiles of one member for the TMA tile geometry of `storage`.
+void substep_tiles(const OlcGeom& g, olc_u32 k, int storage, std::vector<uint4>* out) {
+    const bool f32 = storage == OLC_FIELD_F32;
+    const int TX = f32 ? BATCH_X4_TX : BATCH_T16_TX, TY = f32 ? BATCH_X4_TY : BATCH_T16_TY;
+    const int TZ = f32 ? BATCH_X4_TZ : BATCH_T16_TZ;
+    const int tx = (g.chem_dims[0] + TX - 1) / TX, ty = (g.chem_dims[1] + TY - 1) / TY;
+    const int tz = (g.chem_dims[2] + TZ - 1) / TZ;
+    for (int z = 0; z < tz; ++z)
+        for (int y = 0; y < ty; ++y)
+            for (int x = 0; x < tx; ++x) out->push_back(make_uint4(k, (unsigned)x, (unsigned)y, (unsigned)z));
+}
+
+// Tensor maps of member k's grid of field f in buffers a and b (its voxels
+// from field_off on), for the batched substep kernels.
+bool member_maps(OlcSim* s, olc_u32 k, int f, void* a, void* b, olc_u64 field_off, const OlcGeom& g, int storage) {
+    const int elem = storage == OLC_FIELD_F32 ? 4 : 2;
+    cuuint32_t box[3];
+    batch_substep_box(storage, box);
+    CUtensorMap* m = &s->bmaps_host[((size_t)k * s->caps.n_fields + f) * 2];
+    return encode_map_elems(&m[0], static_cast<char*>(a) + field_off * elem, g.chem_dims, box, elem) &&
+           encode_map_elems(&m[1], static_cast<char*>(b) + field_off * elem, g.chem_dims, box, elem);
+}
+
 int pool_grow_tiles(OlcSim* s, size_t need, cudaStream_t st) {
     if (need <= s->tiles_cap) return OLC_OK;
     OLC_TRY(check(s, cudaStreamSynchronize(st), "sync before tile-list growth"));
@@ -733,11 +759,13 @@ int pool_commit(OlcSim* s, cudaStream_t st) {
         std::stable_sort(order.begin(), order.end(), [](const std::pair<int, olc_u32>& x,
                                                         const std::pair<int, olc_u32>& y) { return x.first > y.first; });
         std::vector<int> steps_of;
-        for (const auto& o : order)
-            for (const uint4& t : per_slot[o.second]) {
-                fl[f].push_back(t);
-                steps_of.push_back(o.first);
-            }
+        std::vector<uint4> mt;
+        for (const auto& o : order) {
+            mt.clear();
+            substep_tiles(s->geoms[o.second], o.second, s->fstep[f].storage, &mt);
+            fl[f].insert(fl[f].end(), mt.begin(), mt.end());
+            steps_of.insert(steps_of.end(), mt.size(), o.first);
+        }
         const int max_s = order.empty() ? 0 : order.front().first;
         counts[f].assign(max_s, 0u);
         olc_u32 c = (olc_u32)fl[f].size();
@@ -746,11 +774,14 @@ int pool_commit(OlcSim* s, cudaStream_t st) {
             counts[f][sub] = c;
         }
     }
-    OLC_TRY(pool_grow_tiles(s, std::max<size_t>(all.size(), 1), st));
+    size_t need = std::max<size_t>(all.size(), 1);
+    for (olc_u32 f = 0; f < F; ++f) need = std::max(need, fl[f].size());
+    OLC_TRY(pool_grow_tiles(s, need, st));
     auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
     const size_t n_desc = sizeof(OlcSimDesc) * s->n_sims;
     const size_t n_steps = sizeof(FieldStep) * s->bsteps_host.size();
     const size_t n_params = s->params_all.size();
+    const size_t n_maps = sizeof(CUtensorMap) * s->bmaps_host.size();
     size_t off = 0;
     const size_t o_desc = off;
     off = al(off + n_desc);
@@ -762,6 +793,8 @@ int pool_commit(OlcSim* s, cudaStream_t st) {
     off = al(off + all.size() * sizeof(uint4));
     const size_t o_chunks = off;
     off = al(off + chunks.size() * sizeof(uint2));
+    const size_t o_maps = off;
+    off = al(off + n_maps);
     size_t o_f[OLC_MAX_FIELDS] = {};
     for (olc_u32 f = 0; f < F; ++f) {
         o_f[f] = off;
@@ -783,6 +816,7 @@ int pool_commit(OlcSim* s, cudaStream_t st) {
     if (n_params) std::memcpy(h + o_params, s->params_all.data(), n_params);
     if (!all.empty()) std::memcpy(h + o_all, all.data(), all.size() * sizeof(uint4));
     if (!chunks.empty()) std::memcpy(h + o_chunks, chunks.data(), chunks.size() * sizeof(uint2));
+    if (n_maps) std::memcpy(h + o_maps, s->bmaps_host.data(), n_maps);
     for (olc_u32 f = 0; f < F; ++f)
         if (!fl[f].empty()) std::memcpy(h + o_f[f], fl[f].data(), fl[f].size() * sizeof(uint4));
     auto up = [&](void* dst, size_t o, size_t n, const char* what) {
@@ -793,6 +827,7 @@ int pool_commit(OlcSim* s, cudaStream_t st) {
     OLC_TRY(up(s->params_dev, o_params, n_params, "upload params"));
     OLC_TRY(up(s->btiles_all, o_all, all.size() * sizeof(uint4), "upload field tiles"));
     OLC_TRY(up(s->table_chunks, o_chunks, chunks.size() * sizeof(uint2), "upload bin-table chunks"));
+    OLC_TRY(up(s->bmaps_dev, o_maps, n_maps, "upload tensor maps"));
     for (olc_u32 f = 0; f < F; ++f)
         if (s->field_bound[f]) OLC_TRY(up(s->btiles_field[f], o_f[f], fl[f].size() * sizeof(uint4), "upload tiles"));
     if (!s->stage_ev[i])
@@ -973,6 +1008,8 @@ int olc_create_batch(const OlcGeom* geoms, int n_sims, const OlcCaps* caps, OlcS
     A(dev_alloc(s, &s->bsteps_dev, sizeof(FieldStep) * s->bsteps_host.size(), "field steps"));
     A(dev_alloc(s, &s->btiles_all, sizeof(uint4) * tiles.size(), "field tiles"));
     A(dev_alloc(s, &s->red_batch_dev, sizeof(OlcReductions) * n_sims, "batch reductions"));
+    s->bmaps_host.assign((size_t)n_sims * std::max<olc_u32>(1u, caps->n_fields) * 2, CUtensorMap{});
+    A(dev_alloc(s, &s->bmaps_dev, sizeof(CUtensorMap) * s->bmaps_host.size(), "tensor maps"));
     A(check(s, cudaMallocHost(reinterpret_cast<void**>(&s->red_batch_host), sizeof(OlcReductions) * n_sims),
             "pinned batch reductions"));
     if (rc == OLC_OK) {
@@ -1032,6 +1069,7 @@ int olc_destroy(OlcSim* s) {
     cudaFree(s->red_batch_dev);
     if (s->red_batch_host) cudaFreeHost(s->red_batch_host);
     cudaFree(s->gather_counts);
+    cudaFree(s->bmaps_dev);
     cudaFree(s->table_chunks);
     for (int i = 0; i < 2; ++i) {
         if (s->stage_host[i]) cudaFreeHost(s->stage_host[i]);
@@ -1453,18 +1491,22 @@ int olc_bind_field_batch(OlcSim* s, int index, void* a_, void* b_, float* sink, 
     // tiles of this field, simulations taking the most substeps first (stable)
     std::stable_sort(order.begin(), order.end(),
                      [](const std::pair<int, olc_u32>& x, const std::pair<int, olc_u32>& y) { return x.first > y.first; });
-    std::vector<uint4> all(s->n_btiles);
-    OLC_TRY(check(s, cudaMemcpy(all.data(), s->btiles_all, sizeof(uint4) * all.size(), cudaMemcpyDeviceToHost),
-                  "read field tiles"));
-    std::vector<std::vector<uint4>> per_sim(s->n_sims);
-    for (const uint4& t : all) per_sim[t.x].push_back(t);
-    std::vector<uint4> tiles;
+    // substep tiles of the TMA kernel's geometry, and each member's tensor maps
+    std::vector<uint4> tiles, mt;
     std::vector<int> tile_steps;
-    for (const auto& o : order)
-        for (const uint4& t : per_sim[o.second]) {
-            tiles.push_back(t);
-            tile_steps.push_back(o.first);
-        }
+    for (const auto& o : order) {
+        mt.clear();
+        substep_tiles(s->geoms[o.second], o.second, storage, &mt);
+        tiles.insert(tiles.end(), mt.begin(), mt.end());
+        tile_steps.insert(tile_steps.end(), mt.size(), o.first);
+    }
+    for (olc_u32 k = 0; k < s->n_sims; ++k)
+        if (specs[k].substeps != 0 && !member_maps(s, k, index, a, b, s->field_off[k], s->geoms[k], storage))
+            return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: simulation " + std::to_string(k) +
+                                            ": tensor maps of its grid failed (16-byte aligned grids)");
+    OLC_TRY(check(s, cudaMemcpy(s->bmaps_dev, s->bmaps_host.data(), sizeof(CUtensorMap) * s->bmaps_host.size(),
+                                cudaMemcpyHostToDevice),
+                  "upload tensor maps"));
     const int max_s = order.empty() ? 0 : order.front().first;
     std::vector<olc_u32> count(max_s, 0u);
     for (int sub = 0; sub < max_s; ++sub) {
@@ -1616,6 +1658,8 @@ int olc_create_pool(const OlcPoolConfig* cfg, const OlcCaps* caps, OlcSim** out)
     A(dev_alloc(s, &s->fpar_dev, (size_t)n * OLC_MAX_FIELDS, "field parity"));
     A(dev_alloc(s, &s->bsteps_dev, sizeof(FieldStep) * s->bsteps_host.size(), "field steps"));
     A(dev_alloc(s, &s->red_batch_dev, sizeof(OlcReductions) * n, "pool reductions"));
+    s->bmaps_host.assign((size_t)n * std::max<olc_u32>(1u, caps->n_fields) * 2, CUtensorMap{});
+    A(dev_alloc(s, &s->bmaps_dev, sizeof(CUtensorMap) * s->bmaps_host.size(), "tensor maps"));
     A(dev_alloc(s, &s->gather_counts, POOL_GATHER_BLOCKS * sizeof(olc_u32), "gather counts"));
     // each member's range splits into at most n / CHUNK + 1 chunks
     s->table_chunks_cap = (size_t)(cfg->table_entries / POOL_TABLE_CHUNK) + n + 1;
@@ -1714,6 +1758,13 @@ int olc_pool_admit(OlcSim* s, const OlcGeom* geom, const OlcDiffusion* specs, co
             return fail(s, OLC_ERR_CAPACITY, "olc_pool_admit: field arena full");
         }
     }
+    for (olc_u32 f = 0; f < F; ++f)
+        if (fs[f].substeps != 0 &&
+            !member_maps(s, slot, (int)f, s->field[0][f], s->field[1][f], f_off, *geom, fs[f].storage)) {
+            s->table_arena.release(t_off, (olc_u64)top + 1u);
+            s->field_arena.release(f_off, nvox);
+            return fail(s, OLC_ERR_ARG, "olc_pool_admit: tensor maps of the member's grid failed");
+        }
     OlcSimDesc& d = s->desc_host[slot];
     std::memset(&d, 0, sizeof(d));
     for (int i = 0; i < 3; ++i) {
