@@ -200,12 +200,79 @@ void launch_contact_batch(const BatchArgs& b, const float4* posr, const olc_u32*
 }
 
 // ------------------------------------------------------------------ fields
-// A field tile of the per-voxel passes (sink, reaction, reductions): BT_X x
-// BT_Y x BT_Z voxels of one simulation's grid, 128 threads.  The substeps run
-// on TMA tiles of their own geometry (k_substep_batch_x4, k_substep_batch_t16).
+// A field tile: BT_X x BT_Y x BT_Z voxels of one simulation's grid, 128
+// threads.  The FP32 substep gives each thread four consecutive x voxels of
+// one row, walking the tile's planes with the z neighbours in registers;
+// neighbours are read with plain loads (reads that would leave the grid
+// return 0 and only ever feed face voxels, which are pinned).  16-bit fields
+// take their substeps on TMA tiles (k_substep_batch_t16).
 constexpr int BT_X = BATCH_TILE_X, BT_Y = BATCH_TILE_Y, BT_Z = BATCH_TILE_Z;
 
 __device__ __forceinline__ float4 ld4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+__device__ __forceinline__ float4 update4_b(float xl, float xr, float4 c, float4 ym, float4 yp, float4 zm,
+                                            float4 zp, float r, float inv_decay) {
+    float4 v;
+    v.x = __fadd_rn(__fadd_rn(__fadd_rn(xl, c.y), __fadd_rn(ym.x, yp.x)), __fadd_rn(zm.x, zp.x));
+    v.y = __fadd_rn(__fadd_rn(__fadd_rn(c.x, c.z), __fadd_rn(ym.y, yp.y)), __fadd_rn(zm.y, zp.y));
+    v.z = __fadd_rn(__fadd_rn(__fadd_rn(c.y, c.w), __fadd_rn(ym.z, yp.z)), __fadd_rn(zm.z, zp.z));
+    v.w = __fadd_rn(__fadd_rn(__fadd_rn(c.z, xr), __fadd_rn(ym.w, yp.w)), __fadd_rn(zm.w, zp.w));
+    v.x = fmaxf(__fmul_rn(__fadd_rn(c.x, __fmul_rn(r, __fsub_rn(v.x, __fmul_rn(6.0f, c.x)))), inv_decay), 0.0f);
+    v.y = fmaxf(__fmul_rn(__fadd_rn(c.y, __fmul_rn(r, __fsub_rn(v.y, __fmul_rn(6.0f, c.y)))), inv_decay), 0.0f);
+    v.z = fmaxf(__fmul_rn(__fadd_rn(c.z, __fmul_rn(r, __fsub_rn(v.z, __fmul_rn(6.0f, c.z)))), inv_decay), 0.0f);
+    v.w = fmaxf(__fmul_rn(__fadd_rn(c.w, __fmul_rn(r, __fsub_rn(v.w, __fmul_rn(6.0f, c.w)))), inv_decay), 0.0f);
+    return v;
+}
+
+__global__ void __launch_bounds__(128) k_substep_batch(const uint4* __restrict__ tiles,
+                                                       const OlcSimDesc* __restrict__ sims,
+                                                       const FieldStep* __restrict__ steps, int field, int n_fields,
+                                                       const unsigned char* __restrict__ fpar, int sub,
+                                                       float* fa, float* fb) {
+    const uint4 t = tiles[blockIdx.x];
+    const olc_u32 k = t.x;
+    const OlcSimDesc& d = sims[k];
+    const FieldStep fs = steps[(size_t)k * n_fields + field];
+    const int nx = d.cdims[0], ny = d.cdims[1], nz = d.cdims[2];
+    const bool flip = ((fpar[(size_t)k * n_fields + field] ^ (unsigned)sub) & 1u) != 0u;
+    const float* in = (flip ? fb : fa) + d.field_off;
+    float* out = (flip ? fa : fb) + d.field_off;
+    const int x = (int)t.y * BT_X + 4 * (threadIdx.x & 7);
+    const int y = (int)t.z * BT_Y + (threadIdx.x >> 3);
+    const int z0 = (int)t.w * BT_Z;
+    if (x >= nx || y >= ny) return;
+    const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
+    const bool edge_y = y == 0 || y == ny - 1;
+    const bool ex0 = x == 0, ex3 = x + 3 == nx - 1;
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    size_t idx = (size_t)z0 * sz + (size_t)y * sy + x;
+    float4 zm = z0 > 0 ? ld4(in + idx - sz) : zero;
+    float4 c = ld4(in + idx);
+    const int z1 = min(z0 + BT_Z, nz);
+    for (int zz = z0; zz < z1; ++zz, idx += sz) {
+        const float4 zp = zz + 1 < nz ? ld4(in + idx + sz) : zero;
+        const float4 ym = y > 0 ? ld4(in + idx - sy) : zero;
+        const float4 yp = y + 1 < ny ? ld4(in + idx + sy) : zero;
+        const float xl = x > 0 ? __ldg(in + idx - 1) : 0.0f;
+        const float xr = x + 4 < nx ? __ldg(in + idx + 4) : 0.0f;
+        float4 v = update4_b(xl, xr, c, ym, yp, zm, zp, fs.r, fs.inv_decay);
+        if (edge_y || zz == 0 || zz == nz - 1) {
+            v = make_float4(fs.bval, fs.bval, fs.bval, fs.bval);
+        } else {
+            if (ex0) v.x = fs.bval;
+            if (ex3) v.w = fs.bval;
+        }
+        *reinterpret_cast<float4*>(out + idx) = v;
+        zm = c;
+        c = zp;
+    }
+}
+
+void launch_substep_batch(const BatchArgs& b, const uint4* tiles, olc_u32 n_tiles, const FieldStep* steps, int field,
+                          int n_fields, const unsigned char* fpar, int sub, float* fa, float* fb, cudaStream_t s) {
+    if (n_tiles == 0) return;
+    k_substep_batch<<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, sub, fa, fb);
+}
 
 // f <- f / (1 + K dt) on interior voxels, K <- 0, per tile (as k_sink).
 __global__ void __launch_bounds__(128) k_sink_batch(const uint4* __restrict__ tiles,

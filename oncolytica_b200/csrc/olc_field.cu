@@ -342,87 +342,12 @@ __global__ void __launch_bounds__(16 * TYR, 1) k_substep_x4(const __grid_constan
 }
 
 // ---------------------------------------------------------------- batched substep
-// k_substep_x4's tile on one member of a batch: block b takes tile list entry
-// b = (member, tile x, tile y, tile z); the member's grid is read through its
-// own tensor map, from a table in device memory with two maps (buffers a and
-// b) per member and field.  The acquire fence orders the map's bytes, copied
-// in by the host before the launch, before the tensor-map reads of the TMA.
-__global__ void __launch_bounds__(16 * BATCH_X4_TY, 1) k_substep_batch_x4(
-    const uint4* __restrict__ tiles, const OlcSimDesc* __restrict__ sims, const FieldStep* __restrict__ steps,
-    const CUtensorMap* __restrict__ maps, int field, int n_fields, const unsigned char* __restrict__ fpar, int sub,
-    float* fa, float* fb, olc_u32* status) {
-    using S = X4Shape<BATCH_X4_TY, BATCH_X4_TZ>;
-    extern __shared__ unsigned char x4_raw[];
-    const olc_u32 pad = (128u - (smem_u32(x4_raw) & 127u)) & 127u;
-    float* tile = reinterpret_cast<float*>(x4_raw + pad);
-    const olc_u32 bar_a = smem_u32(x4_raw + pad + S::BYTES);
-    const uint4 t = tiles[blockIdx.x];
-    const OlcSimDesc& d = sims[t.x];
-    const size_t j = (size_t)t.x * n_fields + field;
-    const FieldStep fs = steps[j];
-    const bool flip = ((fpar[j] ^ (unsigned)sub) & 1u) != 0u;
-    const CUtensorMap* map = maps + 2 * j + (flip ? 1 : 0);
-    float* out = (flip ? fa : fb) + d.field_off;
-    const int x0 = (int)t.y * S::TX, y0 = (int)t.z * BATCH_X4_TY, z0 = (int)t.w * BATCH_X4_TZ;
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(S::BYTES) : "memory");
-        asm volatile(
-            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
-            "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(tile)),
-            "l"(reinterpret_cast<unsigned long long>(map)), "r"(x0 - S::HX), "r"(y0 - 1), "r"(z0 - 1), "r"(bar_a)
-            : "memory");
-    }
-    bool ready = false;
-    for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it) {
-        if (mbar_try_wait(bar_a, 0)) {
-            ready = true;
-            break;
-        }
-    }
-    if (!ready) {
-        if (threadIdx.x == 0) atomicOr(status, OLC_ST_TIMEOUT);
-        for (olc_u32 it = 0; it < OLC_SPIN_LIMIT && !mbar_try_wait(bar_a, 0); ++it) {
-        }
-        return;
-    }
-    x4_tile<BATCH_X4_TY, BATCH_X4_TZ>(tile, out, x0, y0, z0, d.cdims[0], d.cdims[1], d.cdims[2], fs.r, fs.inv_decay,
-                                      fs.bval);
-}
-
-void launch_substep_batch_x4(const BatchArgs& b, const uint4* tiles, olc_u32 n_tiles, const FieldStep* steps,
-                             const CUtensorMap* maps, int field, int n_fields, const unsigned char* fpar, int sub,
-                             float* fa, float* fb, olc_u32* status, cudaStream_t s) {
-    using S = X4Shape<BATCH_X4_TY, BATCH_X4_TZ>;
-    if (n_tiles == 0) return;
-    static int configured_mask = 0;  // per device (up to 32)
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 32 && !(configured_mask & (1 << dev))) {
-        cudaFuncSetAttribute(k_substep_batch_x4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
-        configured_mask |= 1 << dev;
-    }
-    k_substep_batch_x4<<<n_tiles, S::THREADS, S::SMEM, s>>>(tiles, b.sims, steps, maps, field, n_fields, fpar, sub,
-                                                            fa, fb, status);
-}
-
+// TMA box of a member's tensor map for the batched 16-bit substep.
 void batch_substep_box(int storage, cuuint32_t box[3]) {
-    using S = X4Shape<BATCH_X4_TY, BATCH_X4_TZ>;
-    if (storage == OLC_FIELD_F32) {
-        box[0] = S::WX;
-        box[1] = S::WY;
-        box[2] = S::WZ;
-    } else {
-        box[0] = BATCH_T16_TX + 16;
-        box[1] = BATCH_T16_TY + 2;
-        box[2] = BATCH_T16_TZ + 2;
-    }
+    (void)storage;
+    box[0] = BATCH_T16_TX + 16;
+    box[1] = BATCH_T16_TY + 2;
+    box[2] = BATCH_T16_TZ + 2;
 }
 
 // ---------------------------------------------------------------- persistent pipeline

@@ -212,17 +212,14 @@ void launch_contact_batch(const BatchArgs& b, const float4* posr, const olc_u32*
 // Field tiles: uint4 (simulation, tile x, tile y, tile z) of BATCH_TILE_X x
 // BATCH_TILE_Y x BATCH_TILE_Z voxels.
 constexpr int BATCH_TILE_X = 32, BATCH_TILE_Y = 16, BATCH_TILE_Z = 16;
-// Substeps of a batch on TMA tiles (olc_field.cu, olc_field16.cu): the
-// per-field substep tile lists use these geometries (FP32: k_substep_x4's
-// 64 x 8 x 8 tile; 16-bit: k_substep16's 64 x 16 x 8), and each member's grid
-// is read through its tensor maps (maps[2 * (member * n_fields + field) + buffer],
-// boxes from batch_substep_box).
-constexpr int BATCH_X4_TX = 64, BATCH_X4_TY = 8, BATCH_X4_TZ = 8;
+// Substeps of a batch: FP32 fields on BATCH_TILE tiles with plain loads
+// (olc_batch.cu); 16-bit fields on TMA tiles of k_substep16's 64 x 16 x 8
+// geometry (olc_field16.cu), each member's grid read through its tensor maps
+// (maps[2 * (member * n_fields + field) + buffer], box from batch_substep_box).
 constexpr int BATCH_T16_TX = 64, BATCH_T16_TY = 16, BATCH_T16_TZ = 8;
 void batch_substep_box(int storage, cuuint32_t box[3]);
-void launch_substep_batch_x4(const BatchArgs& b, const uint4* tiles, olc_u32 n_tiles, const FieldStep* steps,
-                             const CUtensorMap* maps, int field, int n_fields, const unsigned char* fpar, int sub,
-                             float* fa, float* fb, olc_u32* status, cudaStream_t s);
+void launch_substep_batch(const BatchArgs& b, const uint4* tiles, olc_u32 n_tiles, const FieldStep* steps, int field,
+                          int n_fields, const unsigned char* fpar, int sub, float* fa, float* fb, cudaStream_t s);
 void launch_substep_batch_t16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
                               const FieldStep* steps, const CUtensorMap* maps, int field, int n_fields,
                               const unsigned char* fpar, int sub, void* fa, void* fb, const olc_u32* step_ctr,

@@ -476,9 +476,8 @@ int step_once_batch(OlcSim* s, int collect, cudaStream_t st) {
                                          (int)F, s->fpar_dev, (int)sub, s->field[0][f], s->field[1][f],
                                          s->counters + OLC_CTR_FIELD_STEP, s->counters + OLC_CTR_STATUS, st);
             else
-                launch_substep_batch_x4(B, s->btiles_field[f], cnt[sub], s->bsteps_dev, s->bmaps_dev, (int)f, (int)F,
-                                        s->fpar_dev, (int)sub, s->field[0][f], s->field[1][f],
-                                        s->counters + OLC_CTR_STATUS, st);
+                launch_substep_batch(B, s->btiles_field[f], cnt[sub], s->bsteps_dev, (int)f, (int)F, s->fpar_dev,
+                                     (int)sub, s->field[0][f], s->field[1][f], st);
             ++launches;
         }
         substeps += (uint32_t)cnt.size();
@@ -693,11 +692,11 @@ void pool_tiles(const OlcGeom& g, olc_u32 slot, std::vector<uint4>* out) {
             for (int x = 0; x < tx; ++x) out->push_back(make_uint4(slot, (unsigned)x, (unsigned)y, (unsigned)z));
 }
 
-// Substep tiles of one member for the TMA tile geometry of `storage`.
+// Substep tiles of one member for the substep kernel of `storage`.
 void substep_tiles(const OlcGeom& g, olc_u32 k, int storage, std::vector<uint4>* out) {
     const bool f32 = storage == OLC_FIELD_F32;
-    const int TX = f32 ? BATCH_X4_TX : BATCH_T16_TX, TY = f32 ? BATCH_X4_TY : BATCH_T16_TY;
-    const int TZ = f32 ? BATCH_X4_TZ : BATCH_T16_TZ;
+    const int TX = f32 ? BATCH_TILE_X : BATCH_T16_TX, TY = f32 ? BATCH_TILE_Y : BATCH_T16_TY;
+    const int TZ = f32 ? BATCH_TILE_Z : BATCH_T16_TZ;
     const int tx = (g.chem_dims[0] + TX - 1) / TX, ty = (g.chem_dims[1] + TY - 1) / TY;
     const int tz = (g.chem_dims[2] + TZ - 1) / TZ;
     for (int z = 0; z < tz; ++z)
@@ -1501,7 +1500,8 @@ int olc_bind_field_batch(OlcSim* s, int index, void* a_, void* b_, float* sink, 
         tile_steps.insert(tile_steps.end(), mt.size(), o.first);
     }
     for (olc_u32 k = 0; k < s->n_sims; ++k)
-        if (specs[k].substeps != 0 && !member_maps(s, k, index, a, b, s->field_off[k], s->geoms[k], storage))
+        if (storage != OLC_FIELD_F32 && specs[k].substeps != 0 &&
+            !member_maps(s, k, index, a, b, s->field_off[k], s->geoms[k], storage))
             return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: simulation " + std::to_string(k) +
                                             ": tensor maps of its grid failed (16-byte aligned grids)");
     OLC_TRY(check(s, cudaMemcpy(s->bmaps_dev, s->bmaps_host.data(), sizeof(CUtensorMap) * s->bmaps_host.size(),
@@ -1759,7 +1759,7 @@ int olc_pool_admit(OlcSim* s, const OlcGeom* geom, const OlcDiffusion* specs, co
         }
     }
     for (olc_u32 f = 0; f < F; ++f)
-        if (fs[f].substeps != 0 &&
+        if (fs[f].storage != OLC_FIELD_F32 && fs[f].substeps != 0 &&
             !member_maps(s, slot, (int)f, s->field[0][f], s->field[1][f], f_off, *geom, fs[f].storage)) {
             s->table_arena.release(t_off, (olc_u64)top + 1u);
             s->field_arena.release(f_off, nvox);
