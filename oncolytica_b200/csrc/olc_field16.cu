@@ -122,7 +122,7 @@ __device__ __forceinline__ void t16_tile(const unsigned short* tile, unsigned sh
     unsigned short* o = out + (size_t)z0 * sz + (size_t)y * nx + x;
     const float bf = Store16<ST>::to_f(Store16<ST>::from_f(bval));  // the face value as stored
     unsigned long long vi = (unsigned long long)z0 * sz + (unsigned long long)y * nx + x;
-#pragma unroll 2
+#pragma unroll
     for (int lz = 1; lz <= TZ; ++lz) {
         const int z = z0 + lz - 1;
         if (z >= nz) break;
@@ -131,7 +131,7 @@ __device__ __forceinline__ void t16_tile(const unsigned short* tile, unsigned sh
         load8<ST>(pc - WX, ym);
         load8<ST>(pc + WX, yp);
         const float xl = Store16<ST>::to_f(pc[-1]), xr = Store16<ST>::to_f(pc[8]);
-        stencil_update8(xl, xr, c, ym, yp, zm, zp, r, inv_decay, v);
+        stencil_update8_fma(xl, xr, c, ym, yp, zm, zp, r, inv_decay, v);
         if (edge_y || z == 0 || z == nz - 1) {
 #pragma unroll
             for (int e = 0; e < 8; ++e) v[e] = bf;

@@ -74,6 +74,34 @@ __device__ __forceinline__ float4 stencil_update4(float xl, float xr, float4 c, 
     return make_float4(a.x, a.y, b.x, b.y);
 }
 
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// The update of the 16-bit field storages: the same sums, with the two
+// products fused into their sums (one rounding each):
+//   u = fma(r, fma(-6, c, s), c),   out = max(u * inv_decay, 0)
+// on eight consecutive x voxels (four pairs); the oracle restates it with C's
+// correctly rounded fmaf.
+__device__ __forceinline__ void stencil_update8_fma(float xl, float xr, const float (&c)[8], const float (&ym)[8],
+                                                    const float (&yp)[8], const float (&zm)[8], const float (&zp)[8],
+                                                    float r, float inv_decay, float (&out)[8]) {
+    const f32x2 r2 = pk2(r, r), id2 = pk2(inv_decay, inv_decay), m6 = pk2(-6.0f, -6.0f);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int e = 2 * k;
+        const f32x2 cc = pk2(c[e], c[e + 1]);
+        const f32x2 s = add2(add2(add2(pk2(k == 0 ? xl : c[e - 1], c[e]), pk2(c[e + 1], k == 3 ? xr : c[e + 2])),
+                                  add2(pk2(ym[e], ym[e + 1]), pk2(yp[e], yp[e + 1]))),
+                             add2(pk2(zm[e], zm[e + 1]), pk2(zp[e], zp[e + 1])));
+        const float2 w = upk2(mul2(fma2(r2, fma2(m6, cc, s), cc), id2));
+        out[e] = fmaxf(w.x, 0.0f);
+        out[e + 1] = fmaxf(w.y, 0.0f);
+    }
+}
+
 // Eight consecutive x voxels (four pairs): centre row c, rows ym/yp, planes
 // zm/zp, and the neighbours xl/xr left and right of the group.
 __device__ __forceinline__ void stencil_update8(float xl, float xr, const float (&c)[8], const float (&ym)[8],

@@ -235,7 +235,9 @@ int orc_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], float 
  * (value + residual, uptake, the step's decay (1 + lambda dt/S)^-S, residual
  * kept in comp), then S substeps without decay; faces pinned.  Storages 3 and
  * 4 (stochastic rounding) keep the FP32 scheme's decay in every substep
- * (u * 1/(1 + lambda dt/S)) and no decay in the reaction pass. */
+ * (u * 1/(1 + lambda dt/S)) and no decay in the reaction pass.  The substep
+ * fuses its two products: u = fmaf(r, fmaf(-6, c, s), c) (C's fmaf rounds
+ * once, as the GPU's fused multiply-add). */
 static float bf16_to_f(uint16_t h) {
     uint32_t u = (uint32_t)h << 16;
     float f;
@@ -367,7 +369,7 @@ int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const in
                     float s1 = (h16_to_f(cur[v - 1], storage) + h16_to_f(cur[v + 1], storage)) +
                                (h16_to_f(cur[v - sy], storage) + h16_to_f(cur[v + sy], storage));
                     float s2 = s1 + (h16_to_f(cur[v - sz], storage) + h16_to_f(cur[v + sz], storage));
-                    float u = (c + r * (s2 - 6.0f * c)) * inv_decay;
+                    float u = fmaf(r, fmaf(-6.0f, c, s2), c) * inv_decay;
                     u = u > 0.0f ? u : 0.0f;
                     if (storage == 3 || storage == 4) {
                         uint32_t xr = ((uint32_t)(v >> 1) ^ key) * 0x9E3779B1u;
