@@ -53,21 +53,6 @@ __device__ __forceinline__ unsigned short olc_bf16_sr(float f, olc_u32 rnd) {
     return (unsigned short)((__float_as_uint(f) + (rnd & 0xffffu)) >> 16);
 }
 
-// Stochastic FP16 rounding of a finite value with 13 random bits: the 13 FP32
-// mantissa bits that FP16 drops (normal range) plus 13 random bits, then
-// conversion toward zero.  Below FP16's normal range (2^-14) more bits are
-// dropped and the sum is truncated (spacing there is 2^-24).
-__device__ __forceinline__ unsigned short olc_f16_sr(float f, olc_u32 rnd) {
-    const float g = __uint_as_float(__float_as_uint(f) + (rnd & 0x1fffu));
-    unsigned short h;
-    asm("{ .reg .b16 t; cvt.rz.f16.f32 t, %1; mov.b16 %0, t; }" : "=h"(h) : "f"(g));
-    return h;
-}
-
-template <int ST>
-__device__ __forceinline__ unsigned short olc_sr16(float f, olc_u32 rnd) {
-    return ST == OLC_FIELD_F16_SR ? olc_f16_sr(f, rnd) : olc_bf16_sr(f, rnd);
-}
 
 // Random bits for one substep: `key` mixes the step, substep and field
 // (fmix32, once per launch); voxels 2p and 2p+1 of a grid share one 32-bit
@@ -106,18 +91,17 @@ __device__ __forceinline__ olc_u32 pack2(float a, float b) {
     return d;
 }
 
-// The same with stochastic rounding: a takes the low 16 random bits of rnd, b
-// the high 16 (olc_bf16_sr / olc_f16_sr on each value).
+// The same with stochastic rounding, by the conversion's random-bits form:
+// the low half (a) takes bits 15..0 of rnd (BF16) or 12..0 (FP16), the high
+// half (b) bits 31..16 or 28..16; a value rounds away from zero when the top
+// of its discarded bits plus those random bits carries (olc_bf16_sr for BF16).
 template <int ST>
 __device__ __forceinline__ olc_u32 pack2_sr(float a, float b, olc_u32 rnd) {
-    if (ST == OLC_FIELD_BF16_SR) {
-        const olc_u32 ua = __float_as_uint(a) + (rnd & 0xffffu), ub = __float_as_uint(b) + (rnd >> 16);
-        return __byte_perm(ua, ub, 0x7632);  // high halves: ua's in the low half, ub's in the high
-    }
-    const float ga = __uint_as_float(__float_as_uint(a) + (rnd & 0x1fffu));
-    const float gb = __uint_as_float(__float_as_uint(b) + ((rnd >> 16) & 0x1fffu));
     olc_u32 d;
-    asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(gb), "f"(ga));
+    if (ST == OLC_FIELD_BF16_SR)
+        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(b), "f"(a), "r"(rnd));
+    else
+        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(b), "f"(a), "r"(rnd));
     return d;
 }
 

@@ -297,16 +297,29 @@ static uint16_t f_to_f16_rz(float f) {
     return (uint16_t)(sign | (uint16_t)((0x800000u | m) >> (uint32_t)(-1 - e))); /* |f| * 2^24, truncated */
 }
 
-/* Stochastic FP16 rounding (storage 4): the 13 FP32 mantissa bits FP16 drops
- * (normal range) plus 13 random bits, then rounding toward zero; the random
- * bits come from the same pair hash as storage 3 (low / high 16 bits). */
+/* Stochastic FP16 rounding (storage 4) of a finite value: the value rounded
+ * toward zero, plus one unit in the last place when the top 13 of the bits
+ * below that place plus 13 random bits carry (normal results drop 13 FP32
+ * mantissa bits; subnormal results drop more, and their top 13 are used).
+ * The random bits come from the same pair hash as storage 3 (voxel 2p: bits
+ * 12..0 of the pair word, voxel 2p+1: bits 28..16). */
 static uint16_t f_to_f16_sr(float f, uint32_t rnd) {
     uint32_t u;
     memcpy(&u, &f, 4);
-    u += rnd & 0x1fffu;
-    float g;
-    memcpy(&g, &u, 4);
-    return f_to_f16_rz(g);
+    const uint16_t h = f_to_f16_rz(f);
+    const int ebits = (int)((u >> 23) & 0xffu);
+    if (ebits == 0 || (h & 0x7fffu) == 0x7bffu) return h; /* zero / FP32 subnormal, or at the FP16 maximum */
+    const int e = ebits - 127;
+    const uint32_t m = (u & 0x7fffffu) | 0x800000u;
+    uint32_t top13;
+    if (e >= -14) {
+        top13 = m & 0x1fffu; /* 13 dropped mantissa bits */
+    } else {
+        const int sh = -1 - e; /* bits of m below the subnormal unit 2^-24 (>= 14) */
+        if (sh > 24 + 13) return h;
+        top13 = sh >= 13 ? (uint32_t)(((uint64_t)m & ((1ull << sh) - 1ull)) >> (sh - 13)) : 0u;
+    }
+    return (top13 + (rnd & 0x1fffu) >= 0x2000u) ? (uint16_t)(h + 1u) : h;
 }
 
 void orc_round16(const float* in, uint16_t* out, size_t n, int storage, const uint32_t* rnd) {

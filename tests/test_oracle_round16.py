@@ -54,3 +54,23 @@ def test_stochastic_roundings_are_unbiased():
         exact = to_f(oracle.round16(x, 2 if storage == 4 else 1))
         kept = oracle.round16(exact, storage, np.full(exact.size, 0xFFFFFFFF, np.uint32))
         np.testing.assert_array_equal(to_f(kept), exact)
+
+
+def test_stochastic_roundings_match_the_b200_conversions():
+    """The oracle's BF16 / FP16 stochastic rounding equals the B200's
+    cvt.rs.bf16x2.f32 / cvt.rs.f16x2.f32 on the recorded cases (single random
+    bits, random values, every subnormal FP16 result of 2^20 random draws);
+    tests/golden/make_rounding_fixture.cu made the file on a B200."""
+    import os
+
+    from conftest import GOLDEN
+
+    raw = open(os.path.join(GOLDEN, "rounding_sr.bin"), "rb").read()
+    n = int(np.frombuffer(raw[:4], np.int32)[0])
+    a, b, r, f16, bf16 = np.frombuffer(raw[4:], np.uint32).reshape(5, n)
+    a, b = a.view(np.float32), b.view(np.float32)
+    assert n > 16384 and (np.minimum(a, b) < 2.0 ** -14).sum() > 30
+    for storage, hw in ((4, f16), (3, bf16)):
+        lo = oracle.round16(b, storage, r & 0xFFFF).astype(np.uint32)
+        hi = oracle.round16(a, storage, r >> 16).astype(np.uint32)
+        np.testing.assert_array_equal((hi << 16) | lo, hw, err_msg=f"storage {storage}")
