@@ -21,9 +21,6 @@
 #include "olc_store16.cuh"
 
 #include <cuda.h>
-#include <algorithm>
-#include <cstdlib>
-#include <cstring>
 
 namespace olc {
 
@@ -259,141 +256,21 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep_batch_t16(
                  olc_sr_key(*step_ctr - d.step_base, sub, field));
 }
 
-// The same substep as a persistent kernel: each CTA walks the tile list with a
-// stride of the grid size and keeps two staging buffers, so thread 0 resolves
-// the next tile (list entry, member record, field step, parity, tensor map)
-// and starts its TMA box while the CTA computes the current one.  Buffer s is
-// refilled only after the barrier that ends the iteration which read it; each
-// buffer's mbarrier completes once per use (phase parity alternates).  A wait
-// that gives up flags OLC_ST_TIMEOUT, waits once more (bounded) and the CTA
-// still computes (on whatever the buffer holds, in bounds) so that every
-// thread reaches every barrier.
-struct T16Job {
-    unsigned short* out;
-    int x0, y0, z0, nx, ny, nz;
-    float r, inv_decay, bval;
-    olc_u32 key;
-};
-
-template <int ST>
-__global__ void __launch_bounds__(t16::THREADS) k_substep_batch_t16p(
-    const uint4* __restrict__ tiles, olc_u32 n_tiles, const OlcSimDesc* __restrict__ sims,
-    const FieldStep* __restrict__ steps, const CUtensorMap* __restrict__ maps, int field, int n_fields,
-    const unsigned char* __restrict__ fpar, int sub, unsigned short* fa, unsigned short* fb, const olc_u32* step_ctr,
-    olc_u32* status) {
-    using namespace t16;
-    extern __shared__ unsigned char t16_raw[];
-    __shared__ T16Job job[2];
-    const olc_u32 pad = (128u - (smem_addr(t16_raw) & 127u)) & 127u;
-    unsigned short* const buf0 = reinterpret_cast<unsigned short*>(t16_raw + pad);  // stage s at buf0 + s * BYTES / 2
-    const olc_u32 bar0 = smem_addr(t16_raw + pad + 2 * BYTES);                      // stage s's mbarrier at bar0 + 8 s
-    const olc_u32 step_now = *step_ctr;
-    // thread 0: tile i into stage st
-    auto prepare = [&](olc_u32 i, int st) {
-        const uint4 t = tiles[i];
-        const OlcSimDesc& d = sims[t.x];
-        const size_t j = (size_t)t.x * n_fields + field;
-        const FieldStep fs = steps[j];
-        const bool flip = ((fpar[j] ^ (unsigned)sub) & 1u) != 0u;
-        const CUtensorMap* map = maps + 2 * j + (flip ? 1 : 0);
-        T16Job& jb = job[st];
-        jb.out = (flip ? fa : fb) + d.field_off;
-        jb.x0 = (int)t.y * TX;
-        jb.y0 = (int)t.z * TYR;
-        jb.z0 = (int)t.w * TZ;
-        jb.nx = d.cdims[0];
-        jb.ny = d.cdims[1];
-        jb.nz = d.cdims[2];
-        jb.r = fs.r;
-        jb.inv_decay = fs.inv_decay;
-        jb.bval = fs.bval;
-        jb.key = olc_sr_key(step_now - d.step_base, sub, field);
-        asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
-        const olc_u32 bst = bar0 + 8u * (olc_u32)st;
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bst), "r"(BYTES) : "memory");
-        asm volatile(
-            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
-            "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(buf0 + (size_t)st * (BYTES / 2))),
-            "l"(reinterpret_cast<unsigned long long>(map)), "r"(jb.x0 - HX), "r"(jb.y0 - 1), "r"(jb.z0 - 1),
-            "r"(bst)
-            : "memory");
-    };
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0 + 8u) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (blockIdx.x < n_tiles) prepare(blockIdx.x, 0);
-    }
-    __syncthreads();
-    olc_u32 phase = 0;  // bit s: parity of stage s's next completion
-    int st = 0;
-    for (olc_u32 i = blockIdx.x; i < n_tiles; i += gridDim.x) {
-        const olc_u32 nxt = i + gridDim.x;
-        if (threadIdx.x == 0 && nxt < n_tiles) prepare(nxt, st ^ 1);
-        bool ready = false;
-        for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it) {
-            if (mbar_wait_once(bar0 + 8u * (olc_u32)st, (phase >> st) & 1u)) {
-                ready = true;
-                break;
-            }
-        }
-        if (!ready) {  // flag it, and give the copy a second bounded wait before the buffer is reused
-            if (threadIdx.x == 0) atomicOr(status, OLC_ST_TIMEOUT);
-            for (olc_u32 it = 0; it < OLC_SPIN_LIMIT && !mbar_wait_once(bar0 + 8u * (olc_u32)st, (phase >> st) & 1u);
-                 ++it) {
-            }
-        }
-        const T16Job jb = job[st];
-        t16_tile<ST>(buf0 + (size_t)st * (BYTES / 2), jb.out, jb.x0, jb.y0, jb.z0, jb.nx, jb.ny, jb.nz, jb.r,
-                     jb.inv_decay, jb.bval, jb.key);
-        phase ^= 1u << st;
-        st ^= 1;
-        __syncthreads();  // buffer st^1 (just read) may now be refilled
-    }
-    // a prepared tile is always consumed by the loop, so no copy is in flight here
-}
-
-// OLC_BATCH16=single selects one tile per CTA instead of the persistent kernel
-// (kept for measurement; both give the same bits).
-static bool batch16_single() {
-    static int v = -1;
-    if (v < 0) {
-        const char* e = std::getenv("OLC_BATCH16");
-        v = (e && std::strcmp(e, "single") == 0) ? 1 : 0;
-    }
-    return v == 1;
-}
-
 template <int ST>
 static void launch_bt16(const uint4* tiles, olc_u32 n_tiles, const OlcSimDesc* sims, const FieldStep* steps,
                         const CUtensorMap* maps, int field, int n_fields, const unsigned char* fpar, int sub,
                         void* fa, void* fb, const olc_u32* step_ctr, olc_u32* status, cudaStream_t s) {
     using namespace t16;
     static int configured_mask = 0;
-    static unsigned persistent_grid = 0;
     int dev = 0;
     cudaGetDevice(&dev);
-    constexpr size_t SMEM2 = 2 * (size_t)BYTES + 16 + 128;
     if (dev < 32 && !(configured_mask & (1 << dev))) {
         cudaFuncSetAttribute(k_substep_batch_t16<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-        cudaFuncSetAttribute(k_substep_batch_t16p<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM2);
-        int per_sm = 0, sms = 148;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_substep_batch_t16p<ST>, THREADS, SMEM2);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        persistent_grid = (unsigned)(std::max(1, per_sm) * sms);
         configured_mask |= 1 << dev;
     }
-    if (batch16_single()) {
-        k_substep_batch_t16<ST><<<n_tiles, THREADS, SMEM, s>>>(tiles, sims, steps, maps, field, n_fields, fpar, sub,
-                                                              static_cast<unsigned short*>(fa),
-                                                              static_cast<unsigned short*>(fb), step_ctr, status);
-        return;
-    }
-    const unsigned grid = n_tiles < persistent_grid ? n_tiles : persistent_grid;
-    k_substep_batch_t16p<ST><<<grid, THREADS, SMEM2, s>>>(tiles, n_tiles, sims, steps, maps, field, n_fields, fpar,
-                                                         sub, static_cast<unsigned short*>(fa),
-                                                         static_cast<unsigned short*>(fb), step_ctr, status);
+    k_substep_batch_t16<ST><<<n_tiles, THREADS, SMEM, s>>>(tiles, sims, steps, maps, field, n_fields, fpar, sub,
+                                                          static_cast<unsigned short*>(fa),
+                                                          static_cast<unsigned short*>(fb), step_ctr, status);
 }
 
 void launch_substep_batch_t16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
