@@ -258,6 +258,42 @@ int olc_read_counters(OlcSim* sim, OlcCounters* out, void* stream);
 int olc_set_profiling(OlcSim* sim, int enable);
 int olc_read_profile(OlcSim* sim, OlcProfile* out);
 
+/* The engine's metrics set: Kernel_ClearMetrics / Kernel_CollectMetrics /
+ * Kernel_FinalizeMetrics (engine/assets/shaders/tumor_sim.wgsl:248-361) and
+ * the 23 values of MetricIndex (engine/src/sim/readback.rs:25-50), in that
+ * order: total live, proliferating, quiescent, necrotic, their fractions, the
+ * hypoxic fraction, CSC count and fraction, centroid x/y/z, radius of
+ * gyration, invasive radius, necrotic radius, rim thickness, mean energy,
+ * mean O2, mean glucose (second field), mean speed, crowded fraction, step.
+ * Counts are exact integers and sums FP64 (the engine accumulates fixed-point
+ * i32: r*r, 10*delta, 1000*field, 100*r for the maximum); the last block sums
+ * the block partials in a fixed order, so repeated calls give the same bits.
+ * Fields are sampled at the agent's nearest voxel (chemistry_at's rule; the
+ * engine samples trilinearly through a texture unit).  A live agent is one
+ * whose life flag is 0 and whose state is not 0 (STATE_DELETED); state 3 is
+ * necrotic, 1 proliferating, any other quiescent; with state_field < 0 every
+ * live agent counts as proliferating. */
+#define OLC_ENGINE_METRICS 23
+typedef struct {
+    int32_t state_field;        /* i32 agent column, or -1                    */
+    int32_t energy_field;       /* f32 agent column, or -1 (mean energy 0)   */
+    int32_t speed_field;        /* first of three f32 columns (a vec3) whose
+                                   length is the speed, or -1                */
+    int32_t csc_field;          /* i32 column, nonzero marks a cancer stem
+                                   cell (the engine's species table: no
+                                   symmetric division), or -1                */
+    int32_t o2_field;           /* chemistry field sampled as O2, or -1      */
+    int32_t glucose_field;      /* chemistry field sampled as glucose, or -1 */
+    float   hypoxia_threshold;  /* HYPOXIA_METRIC_THR (0.1)                   */
+    int32_t crowd_threshold;    /* CROWD_THRESHOLD (12): agents in the bin    */
+    float   center[3];          /* DomainCenter                               */
+    float   pad;
+} OlcEngineMetricsSpec;
+
+/* Computes the engine metrics of the current state on `stream` (one kernel)
+ * and copies the 23 values to out[0..22] (synchronises the stream). */
+int olc_engine_metrics(OlcSim* sim, const OlcEngineMetricsSpec* spec, double* out, void* stream);
+
 /* Copies the last step's reductions / metric-rule accumulators to host memory
  * (replaces the MetricsBuffer readback, _gpu_backend.py:166-169). */
 int olc_read_reductions(OlcSim* sim, OlcReductions* out, void* stream);

@@ -47,6 +47,7 @@ EXPORTS = (
     "olc_create_pool", "olc_bind_field_pool", "olc_pool_admit", "olc_pool_add_agents", "olc_pool_gather",
     "olc_pool_copy_results", "olc_pool_retire", "olc_pool_usage",
     "olc_arena_create", "olc_arena_alloc", "olc_arena_release", "olc_arena_stats", "olc_arena_destroy",
+    "olc_engine_metrics",
 )
 
 
@@ -146,6 +147,30 @@ class OlcReductions(C.Structure):
     ]
 
 
+OLC_ENGINE_METRICS = 23
+# MetricIndex of engine/src/sim/readback.rs:25-50, in output order
+ENGINE_METRIC_NAMES = (
+    "total_live", "n_prolif", "n_quiesc", "n_necr", "frac_prolif", "frac_quiesc", "frac_necr", "frac_hypoxic",
+    "csc_count", "csc_frac", "centroid_x", "centroid_y", "centroid_z", "r_gyration", "r_invasive", "r_necrotic",
+    "rim_thickness", "mean_energy", "mean_o2", "mean_glu", "mean_speed", "crowd_frac", "step",
+)
+
+
+class OlcEngineMetricsSpec(C.Structure):
+    _fields_ = [
+        ("state_field", C.c_int32),
+        ("energy_field", C.c_int32),
+        ("speed_field", C.c_int32),
+        ("csc_field", C.c_int32),
+        ("o2_field", C.c_int32),
+        ("glucose_field", C.c_int32),
+        ("hypoxia_threshold", C.c_float),
+        ("crowd_threshold", C.c_int32),
+        ("center", C.c_float * 3),
+        ("pad", C.c_float),
+    ]
+
+
 class OlcPoolConfig(C.Structure):
     _fields_ = [
         ("max_slots", C.c_uint32),
@@ -228,6 +253,7 @@ _SIGS = {
     "olc_arena_release": (C.c_int, [_VP, C.c_uint64, C.c_uint64]),
     "olc_arena_stats": (C.c_int, [_VP, _U64P, _U64P, _U64P]),
     "olc_arena_destroy": (C.c_int, [_VP]),
+    "olc_engine_metrics": (C.c_int, [_VP, C.POINTER(OlcEngineMetricsSpec), C.POINTER(C.c_double), _VP]),
 }
 
 _lock = threading.Lock()

@@ -229,6 +229,43 @@ class CudaBackend:
                 "field_min": {f: r.field_min[i] for i, f in enumerate(self.layout.chem_fields[:n])},
                 "field_max": {f: r.field_max[i] for i, f in enumerate(self.layout.chem_fields[:n])}}
 
+    def engine_metrics(self, state: str | None = "state", energy: str | None = None, speed: str | None = None,
+                       csc: str | None = None, o2: str | None = None, glucose: str | None = None,
+                       hypoxia_threshold: float = 0.1, crowd_threshold: int = 12) -> dict:
+        """The engine's 23 metrics (engine/src/sim/readback.rs:25-50) of the
+        current state, computed on the device (olc_engine_metrics).  Column
+        and field names select what the engine reads from its fixed cell
+        struct; a name the model lacks reads as absent (zero).  By default O2
+        is the first chemistry field and glucose the second."""
+        L = self.layout
+
+        def col(name, dtype):
+            if name is None:
+                return -1
+            for i, (c, _, dt) in enumerate(L.cell_cols):
+                if c == name and dt == dtype:
+                    return i
+            return -1
+
+        def field(name, default):
+            if name is None:
+                return default if default < len(L.chem_fields) else -1
+            return L.chem_fields.index(name) if name in L.chem_fields else -1
+
+        sp = _lib.OlcEngineMetricsSpec()
+        sp.state_field = col(state, np.int32)
+        sp.energy_field = col(energy, np.float32)
+        sp.speed_field = col(None if speed is None else f"{speed}.x", np.float32)  # a vec3: x, y, z columns
+        sp.csc_field = col(csc, np.int32)
+        sp.o2_field = field(o2, 0)
+        sp.glucose_field = field(glucose, 1)
+        sp.hypoxia_threshold = hypoxia_threshold
+        sp.crowd_threshold = int(crowd_threshold)
+        sp.center[:] = tuple(self.caps.center)
+        out = (C.c_double * _lib.OLC_ENGINE_METRICS)()
+        self._check(self.lib.olc_engine_metrics(self.handle, C.byref(sp), out, self._stream()))
+        return dict(zip(_lib.ENGINE_METRIC_NAMES, list(out)))
+
     def _current(self) -> tuple[int, int]:
         a, f = C.c_int(), C.c_int()
         self._check(self.lib.olc_current_buffers(self.handle, C.byref(a), C.byref(f)))

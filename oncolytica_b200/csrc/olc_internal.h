@@ -192,6 +192,46 @@ void launch_reset_reductions(OlcReductions* out_dev, int nfields, cudaStream_t s
 void launch_reduce_field16(const void* f, const float* comp, const FieldStep& fs, int slot, OlcReductions* out,
                            const RedScratch& rs, cudaStream_t s);
 
+// ------------------------------------------------------------------ engine metrics
+// Inputs of k_engine_metrics (olc_metrics.cu): current agent columns (optional
+// ones null), the current buffers of the sampled fields, and the bin table.
+struct EngineMetricArgs {
+    const float* x;
+    const float* y;
+    const float* z;
+    const unsigned char* life;
+    const int* state;
+    const int* csc;
+    const float* energy;
+    const float* speed_x;
+    const float* speed_y;
+    const float* speed_z;
+    const void* f0;
+    const void* f1;
+    int f0_type, f1_type;
+    int cdims[3];
+    float cvs;
+    const uint2* ranges;
+    int tdims[3];
+    float tvs;
+    float cx, cy, cz;
+    float hypoxia;
+    int crowd;
+    double step;
+};
+// Device accumulators; `out` receives the 23 finalized values.
+struct EngineMetricAcc {
+    olc_u32 counts[6];
+    olc_u32 ticket;
+    olc_u32 pad;
+    double max_r;
+    double out[OLC_ENGINE_METRICS];
+};
+constexpr olc_u32 EM_MAX_BLOCKS = 148 * 4;
+constexpr size_t EM_PARTIALS = 8 * (size_t)EM_MAX_BLOCKS;  // doubles
+void launch_engine_metrics(const EngineMetricArgs& a, const olc_u32* counters, olc_u32 n_cap, EngineMetricAcc* acc,
+                           double* partials, cudaStream_t s);
+
 void launch_rng(olc_u32* states, olc_u32 n, int draws, float* out, float* dirs, cudaStream_t s);
 
 // ------------------------------------------------------------------ batched mode (olc_batch.cu)

@@ -96,6 +96,9 @@ struct OlcSim {
     void* metrics_dev = nullptr;
     size_t metrics_bytes = 0;
     olc_u32* ctr_host_words = nullptr;     // pinned copy of the counter block
+    EngineMetricAcc* em_acc = nullptr;     // engine metrics (allocated on first use)
+    double* em_partials = nullptr;
+    EngineMetricAcc* em_host = nullptr;    // pinned
 
     cudaLibrary_t module = nullptr;
     std::vector<cudaKernel_t> funcs;
@@ -1078,6 +1081,9 @@ int olc_destroy(OlcSim* s) {
     if (s->params_host) cudaFreeHost(s->params_host);
     if (s->red_host) cudaFreeHost(s->red_host);
     if (s->ctr_host_words) cudaFreeHost(s->ctr_host_words);
+    cudaFree(s->em_acc);
+    cudaFree(s->em_partials);
+    if (s->em_host) cudaFreeHost(s->em_host);
     delete s;
     return OLC_OK;
 }
@@ -1435,6 +1441,71 @@ int olc_read_reductions(OlcSim* s, OlcReductions* out, void* stream) {
                   "reductions readback"));
     OLC_TRY(check(s, cudaStreamSynchronize(st), "sync"));
     std::memcpy(out, s->red_host, sizeof(OlcReductions));
+    return OLC_OK;
+}
+
+int olc_engine_metrics(OlcSim* s, const OlcEngineMetricsSpec* spec, double* out, void* stream) {
+    if (!s || !spec || !out) return fail(s, OLC_ERR_ARG, "olc_engine_metrics: null argument");
+    if (s->n_sims) return fail(s, OLC_ERR_STATE, "olc_engine_metrics: batch handle");
+    const int ncol = (int)s->caps.n_agent_fields;
+    auto col_ok = [&](int c, int width) { return c < 0 || (c + width <= ncol); };
+    if (!col_ok(spec->state_field, 1) || !col_ok(spec->energy_field, 1) || !col_ok(spec->speed_field, 3) ||
+        !col_ok(spec->csc_field, 1))
+        return fail(s, OLC_ERR_ARG, "olc_engine_metrics: agent column out of range");
+    for (int f : {spec->o2_field, spec->glucose_field})
+        if (f >= (int)s->caps.n_fields || (f >= 0 && !s->field_bound[f]))
+            return fail(s, OLC_ERR_ARG, "olc_engine_metrics: field not bound");
+    if (!s->col[0][0]) return fail(s, OLC_ERR_STATE, "olc_engine_metrics: agent columns not bound");
+    cudaStream_t st = as_stream(stream);
+    if (!s->em_acc) {
+        OLC_TRY(dev_alloc(s, &s->em_acc, sizeof(EngineMetricAcc), "engine metrics"));
+        OLC_TRY(dev_alloc(s, &s->em_partials, sizeof(double) * EM_PARTIALS, "engine metric partials"));
+        OLC_TRY(check(s, cudaMallocHost(reinterpret_cast<void**>(&s->em_host), sizeof(EngineMetricAcc)),
+                      "pinned engine metrics"));
+    }
+    const int cc = s->agent_cur;
+    auto colp = [&](int c) { return c < 0 ? nullptr : s->col[cc][c]; };
+    EngineMetricArgs a = {};
+    a.x = static_cast<const float*>(s->col[cc][0]);
+    a.y = static_cast<const float*>(s->col[cc][1]);
+    a.z = static_cast<const float*>(s->col[cc][2]);
+    a.life = s->life;
+    a.state = static_cast<const int*>(colp(spec->state_field));
+    a.csc = static_cast<const int*>(colp(spec->csc_field));
+    a.energy = static_cast<const float*>(colp(spec->energy_field));
+    if (spec->speed_field >= 0) {
+        a.speed_x = static_cast<const float*>(colp(spec->speed_field));
+        a.speed_y = static_cast<const float*>(colp(spec->speed_field + 1));
+        a.speed_z = static_cast<const float*>(colp(spec->speed_field + 2));
+    }
+    if (spec->o2_field >= 0) {
+        a.f0 = s->field[s->field_cur[spec->o2_field]][spec->o2_field];
+        a.f0_type = s->fspec[spec->o2_field].storage;
+    }
+    if (spec->glucose_field >= 0) {
+        a.f1 = s->field[s->field_cur[spec->glucose_field]][spec->glucose_field];
+        a.f1_type = s->fspec[spec->glucose_field].storage;
+    }
+    for (int i = 0; i < 3; ++i) {
+        a.cdims[i] = s->geom.chem_dims[i];
+        a.tdims[i] = s->bins.dims[i];
+    }
+    a.cvs = s->geom.chem_voxel_size;
+    a.tvs = s->bins.vs;
+    // the bin table holds the ranges of the last sort; before any step it is empty
+    a.ranges = s->steps ? reinterpret_cast<const uint2*>(s->ranges) : nullptr;
+    a.cx = spec->center[0];
+    a.cy = spec->center[1];
+    a.cz = spec->center[2];
+    a.hypoxia = spec->hypoxia_threshold;
+    a.crowd = spec->crowd_threshold;
+    a.step = (double)s->steps;
+    launch_engine_metrics(a, s->counters, s->caps.max_agents, s->em_acc, s->em_partials, st);
+    OLC_TRY(check(s, cudaGetLastError(), "engine metrics launch"));
+    OLC_TRY(check(s, cudaMemcpyAsync(s->em_host, s->em_acc, sizeof(EngineMetricAcc), cudaMemcpyDeviceToHost, st),
+                  "engine metrics readback"));
+    OLC_TRY(check(s, cudaStreamSynchronize(st), "sync"));
+    std::memcpy(out, s->em_host->out, sizeof(double) * OLC_ENGINE_METRICS);
     return OLC_OK;
 }
 

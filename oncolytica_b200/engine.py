@@ -260,6 +260,15 @@ class Engine:
     def get_metrics(self) -> Any:
         return self._metrics
 
+    def get_engine_metrics(self, **kw: Any) -> dict:
+        """The engine's metrics set (engine/assets/shaders/tumor_sim.wgsl:248-361:
+        counts, fractions, centroid, radii, mean field values, crowding) of the
+        current state, computed on the device; keyword arguments name the
+        columns and fields to read (CudaBackend.engine_metrics)."""
+        if self._backend_impl is None:
+            raise RuntimeError("Engine.get_engine_metrics() called before load_model().")
+        return self._backend_impl.engine_metrics(**kw)
+
     def get_reductions(self) -> dict:
         return self._backend_impl.get_reductions()
 

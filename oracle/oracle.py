@@ -346,3 +346,89 @@ class TumourOracle:
         n = self.rows
         keep = self.dead[:n] == 0
         return {k: self.bufs[k][:n][keep].copy() for k in AGENT_COLS}
+
+
+# ------------------------------------------------------------------ engine metrics
+
+ENGINE_METRIC_NAMES = (
+    "total_live", "n_prolif", "n_quiesc", "n_necr", "frac_prolif", "frac_quiesc", "frac_necr", "frac_hypoxic",
+    "csc_count", "csc_frac", "centroid_x", "centroid_y", "centroid_z", "r_gyration", "r_invasive", "r_necrotic",
+    "rim_thickness", "mean_energy", "mean_o2", "mean_glu", "mean_speed", "crowd_frac", "step",
+)
+
+
+def _bin(p: np.ndarray, vs: float, dim: int) -> np.ndarray:
+    """trunc(p / vs) with an IEEE float32 divide, clamped to [0, dim - 1]."""
+    q = (np.asarray(p, dtype=np.float32) / np.float32(vs)).astype(np.float32)
+    c = np.trunc(q)
+    c = np.where(np.isnan(c), 0.0, c)
+    return np.clip(c, 0, dim - 1).astype(np.int64)
+
+
+def engine_metrics(x, y, z, life, state, center, step: int, o2=None, glu=None, cdims=None, cvs=None,
+                   bin_counts=None, tdims=None, tvs=None, energy=None, speed=None, csc=None,
+                   hypoxia: float = 0.1, crowd: int = 12) -> dict:
+    """Restates Kernel_CollectMetrics / Kernel_FinalizeMetrics
+    (engine/assets/shaders/tumor_sim.wgsl:255-361) in FP64 with exact counts.
+
+    x, y, z, life, state: the rows in use (life 0 = alive); o2 / glu: flat
+    float32 fields (x fastest) sampled at the agent's nearest voxel; bin_counts:
+    agents per bin key of the last sort (crowding: more than `crowd`).  Necrotic
+    agents (state 3) only count; state 0 (deleted) is skipped; state 1 is
+    proliferating and any other state quiescent."""
+    x = np.asarray(x, np.float32)
+    y = np.asarray(y, np.float32)
+    z = np.asarray(z, np.float32)
+    st = np.ones(len(x), np.int32) if state is None else np.asarray(state, np.int32)
+    alive = (np.asarray(life) == 0) & (st != 0)
+    necr = alive & (st == 3)
+    live = alive & (st != 3)
+    prolif = live & (st == 1)
+    n_prolif, n_live, n_necr = int(prolif.sum()), int(live.sum()), int(necr.sum())
+    n_quiesc = n_live - n_prolif
+    dx = x[live].astype(np.float64) - np.float64(np.float32(center[0]))
+    dy = y[live].astype(np.float64) - np.float64(np.float32(center[1]))
+    dz = z[live].astype(np.float64) - np.float64(np.float32(center[2]))
+    r2 = dx * dx + dy * dy + dz * dz
+    f_live = max(float(n_live), 1.0)
+    f_total = max(float(n_live + n_necr), 1.0)
+    n_csc = int((np.asarray(csc)[live] != 0).sum()) if csc is not None else 0
+    n_hyp, s_o2, s_glu = 0, 0.0, 0.0
+    if o2 is not None or glu is not None:
+        cx, cy, cz = (_bin(c[live], cvs, cdims[k]) for k, c in enumerate((x, y, z)))
+        v = (cz * cdims[1] + cy) * cdims[0] + cx
+        if o2 is not None:
+            s = np.asarray(o2, np.float32)[v]
+            s_o2 = float(s.astype(np.float64).sum())
+            n_hyp = int((s < np.float32(hypoxia)).sum())
+        if glu is not None:
+            s_glu = float(np.asarray(glu, np.float32)[v].astype(np.float64).sum())
+    n_crowd = 0
+    if bin_counts is not None:
+        tx, ty, tz = (_bin(c[live], tvs, tdims[k]) for k, c in enumerate((x, y, z)))
+        keys = np.array([tissue_key(int(a), int(b), int(c)) for a, b, c in zip(tx, ty, tz)], dtype=np.int64)
+        n_crowd = int((np.asarray(bin_counts)[keys] > crowd).sum())
+    s_energy = float(np.asarray(energy, np.float32)[live].astype(np.float64).sum()) if energy is not None else 0.0
+    s_speed = 0.0
+    if speed is not None:
+        sv = [np.asarray(c, np.float32)[live].astype(np.float64) for c in speed]
+        s_speed = float(np.sqrt(sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2]).sum())
+    r_inv = float(np.sqrt(r2).max()) if n_live else 0.0
+    r_necr = 0.5 * (n_necr / 0.65) ** 0.333333 if n_necr > 0 else 0.0
+    out = [n_live, n_prolif, n_quiesc, n_necr, n_prolif / f_live, n_quiesc / f_live, n_necr / f_total,
+           n_hyp / f_live, n_csc, n_csc / f_live,
+           float(np.float32(center[0])) + float(dx.sum()) / f_live,
+           float(np.float32(center[1])) + float(dy.sum()) / f_live,
+           float(np.float32(center[2])) + float(dz.sum()) / f_live,
+           float(np.sqrt(r2.sum() / f_live)), r_inv, r_necr, max(r_inv - r_necr, 0.0),
+           s_energy / f_live, s_o2 / f_live, s_glu / f_live, s_speed / f_live, n_crowd / f_live, float(step)]
+    return dict(zip(ENGINE_METRIC_NAMES, [float(v) for v in out]))
+
+
+def bin_counts_of(x, y, z, life, tdims, tvs, n_table: int) -> np.ndarray:
+    """Agents per bin key among rows with life 0 (the bin table's range
+    lengths after a sort of those rows)."""
+    keep = np.asarray(life) == 0
+    tx, ty, tz = (_bin(np.asarray(c)[keep], tvs, tdims[k]) for k, c in enumerate((x, y, z)))
+    keys = np.array([tissue_key(int(a), int(b), int(c)) for a, b, c in zip(tx, ty, tz)], dtype=np.int64)
+    return np.bincount(keys, minlength=n_table)
