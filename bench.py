@@ -384,8 +384,16 @@ def run_b200(args) -> None:
         # scale workload
         torch.cuda.empty_cache()
         line["batched"] = {st: measure_batch(args.sims, args.extra_steps, 3, graphs=not args.no_graphs,
-                                             solo_sample=8 if st == "f32" else 0, storage=st)
+                                             solo_sample=16 if st == "f32" else 0, storage=st)
                            for st in ("f32", "f16_sr")}
+        # the batched forms against the plain FP32 path on the same sweep:
+        # members sampled evenly over the sweep run one at a time on solo FP32
+        # engines (CUDA graphs); their agent-steps/s is the plain path's rate
+        solo = line["batched"]["f32"]["solo_vs_batch_sample"]
+        for st, r in line["batched"].items():
+            r["vs_plain_fp32"] = {"plain_fp32_agent_steps_per_s": solo["solo_agent_steps_per_s"],
+                                  "members_sampled": solo["members"],
+                                  "ratio": r["agent_steps_per_s"] / solo["solo_agent_steps_per_s"]}
         line["precision"] = {st: measure_storage(spec, st, args.extra_steps * 5, 3, graphs=not args.no_graphs)
                              for st in ("f16_sr", "bf16_sr", "f16")}
         torch.cuda.empty_cache()

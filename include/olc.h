@@ -231,6 +231,20 @@ int olc_set_params(OlcSim* sim, const void* blob, size_t bytes, void* stream);
  * buffer (replaces sync_to_device, _gpu_backend.py:353-371). */
 int olc_set_agent_count(OlcSim* sim, uint32_t n, void* stream);
 
+/* Step counters of a handle, for checkpoints: a state written back with
+ * olc_set_agent_count plus these counters continues bit for bit as the run it
+ * was taken from (the reference has no resume; its bundle export,
+ * framework/src/oncolytica/gpu/runtime/_gpu_backend.py:303-334, saves the
+ * buffers only). */
+typedef struct {
+    uint64_t steps;             /* steps run (the engine metrics' step)        */
+    uint64_t agent_steps;       /* sum over steps of live agents at the rule   */
+    uint32_t field_step;        /* grid stages run: salts stochastic rounding  */
+    uint32_t status;            /* OLC_STATUS_* bits                           */
+} OlcStepState;
+int olc_get_step_state(OlcSim* sim, OlcStepState* out, void* stream);
+int olc_set_step_state(OlcSim* sim, const OlcStepState* in, void* stream);
+
 /* Which of the pair (0 = a, 1 = b) currently holds agent / field state. */
 int olc_current_buffers(const OlcSim* sim, int* agent_buf, int* field_buf);
 

@@ -47,7 +47,7 @@ EXPORTS = (
     "olc_create_pool", "olc_bind_field_pool", "olc_pool_admit", "olc_pool_add_agents", "olc_pool_gather",
     "olc_pool_copy_results", "olc_pool_retire", "olc_pool_usage",
     "olc_arena_create", "olc_arena_alloc", "olc_arena_release", "olc_arena_stats", "olc_arena_destroy",
-    "olc_engine_metrics",
+    "olc_engine_metrics", "olc_get_step_state", "olc_set_step_state",
 )
 
 
@@ -171,6 +171,15 @@ class OlcEngineMetricsSpec(C.Structure):
     ]
 
 
+class OlcStepState(C.Structure):
+    _fields_ = [
+        ("steps", C.c_uint64),
+        ("agent_steps", C.c_uint64),
+        ("field_step", C.c_uint32),
+        ("status", C.c_uint32),
+    ]
+
+
 class OlcPoolConfig(C.Structure):
     _fields_ = [
         ("max_slots", C.c_uint32),
@@ -254,6 +263,8 @@ _SIGS = {
     "olc_arena_stats": (C.c_int, [_VP, _U64P, _U64P, _U64P]),
     "olc_arena_destroy": (C.c_int, [_VP]),
     "olc_engine_metrics": (C.c_int, [_VP, C.POINTER(OlcEngineMetricsSpec), C.POINTER(C.c_double), _VP]),
+    "olc_get_step_state": (C.c_int, [_VP, C.POINTER(OlcStepState), _VP]),
+    "olc_set_step_state": (C.c_int, [_VP, C.POINTER(OlcStepState), _VP]),
 }
 
 _lock = threading.Lock()

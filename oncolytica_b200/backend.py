@@ -395,6 +395,110 @@ class CudaBackend:
                 out.setdefault("residuals", {})[name] = c.cpu().numpy().copy()
         return out
 
+    # ---- checkpoints (no counterpart in the reference, which has no resume) ----
+    def _layout_signature(self) -> dict:
+        L = self.layout
+        storages = []
+        for i in range(len(L.chem_fields)):
+            t = self.fields_dev[i][0]
+            storages.append(str(t.dtype).replace("torch.", ""))
+        return {"cols": [[c, np.dtype(dt).name] for c, _, dt in L.cell_cols],
+                "fields": list(L.chem_fields), "field_dtypes": storages,
+                "sinks": [self.fields_dev[i][2] is not None for i in range(len(L.chem_fields))],
+                "chem_dims": [int(v) for v in self.geom.chem_dims], "tissue_dims": [int(v) for v in self.geom.tissue_dims],
+                "max_agents": int(self.caps.max_agents)}
+
+    def state_dict(self) -> dict:
+        """Everything the next step reads, as host arrays: the live agents (in
+        device order, every column including _rng_state), each field's current
+        buffer as stored (FP32 values or 16-bit bit patterns), its pending sink
+        and 16-bit residuals, the step counters and the parameters.
+        load_state_dict() of this on an engine built the same way continues
+        bit for bit as this one would: the next sort drops dead rows keeping
+        the survivors' order, so storing the survivors compacted changes
+        nothing."""
+        torch = self.torch
+        cnt = self.counters()
+        rows = cnt["n_agents"]
+        ab, fb = self._current()
+        torch.cuda.synchronize(self.device)
+        keep = self._life(rows) == 0
+        cols = {}
+        for i, (col, _, dt) in enumerate(self.layout.cell_cols):
+            a = self.cols_dev[i][ab][:rows].cpu().numpy()
+            cols[col] = (a.view(np.uint32) if dt == np.uint32 else a)[keep].copy()
+        fields, sinks, residuals = {}, {}, {}
+        for i, name in enumerate(self.layout.chem_fields):
+            t = self.fields_dev[i][(fb >> i) & 1]
+            fields[name] = t.cpu().numpy().copy() if t.dtype == torch.float32 else \
+                t.cpu().view(torch.int16).numpy().view(np.uint16).copy()
+            sk = self.fields_dev[i][2]
+            sinks[name] = sk.cpu().numpy().copy() if sk is not None else None
+            c = self.comp_dev[i]
+            residuals[name] = c.cpu().numpy().copy() if c is not None else None
+        ss = _lib.OlcStepState()
+        self._check(self.lib.olc_get_step_state(self.handle, C.byref(ss), self._stream()))
+        params = self.engine._sim._params
+        return {"format": "oncolytica_b200.state/1", "layout": self._layout_signature(), "cols": cols,
+                "fields": fields, "sinks": sinks, "residuals": residuals,
+                "step_state": {"steps": int(ss.steps), "agent_steps": int(ss.agent_steps),
+                               "field_step": int(ss.field_step), "status": int(ss.status)},
+                "engine_step": int(self.engine._step),
+                "params": {k: getattr(params, k) for k in params.__dataclass_fields__}}
+
+    def load_state_dict(self, sd: dict) -> None:
+        """Writes a state_dict() into this engine's current buffers (the model,
+        geometry, field storages and capacity must match)."""
+        torch = self.torch
+        if sd.get("format") != "oncolytica_b200.state/1":
+            raise ValueError(f"not a checkpoint state: format {sd.get('format')!r}")
+        mine = self._layout_signature()
+        theirs = sd["layout"]
+        for k in ("cols", "fields", "field_dtypes", "sinks", "chem_dims", "tissue_dims"):
+            if [list(x) if isinstance(x, (list, tuple)) else x for x in theirs[k]] != \
+                    [list(x) if isinstance(x, (list, tuple)) else x for x in mine[k]]:
+                raise ValueError(f"checkpoint does not match this engine: {k} {theirs[k]} != {mine[k]}")
+        L = self.layout
+        n = len(sd["cols"]["pos.x"])
+        if n > self.caps.max_agents:
+            raise _lib.OlcError(_lib.OLC_ERR_CAPACITY, f"{n} agents exceed max_agents={self.caps.max_agents}")
+        if sd.get("params"):
+            p = self.engine._sim._params
+            for k, v in sd["params"].items():
+                object.__setattr__(p, k, v)
+            self.upload_params()
+        ab, fb = self._current()
+        torch.cuda.synchronize(self.device)
+        for i, (col, _, dt) in enumerate(L.cell_cols):
+            a = np.ascontiguousarray(sd["cols"][col]).astype(dt, copy=False)
+            if dt == np.uint32:
+                a = a.view(np.int32)
+            if n:
+                self.cols_dev[i][ab][:n].copy_(torch.from_numpy(a))
+        for i, name in enumerate(L.chem_fields):
+            t = self.fields_dev[i][(fb >> i) & 1]
+            raw = np.ascontiguousarray(sd["fields"][name])
+            if t.dtype == torch.float32:
+                t.copy_(torch.from_numpy(raw.astype(np.float32, copy=False)))
+            else:
+                t.view(torch.int16).copy_(torch.from_numpy(raw.astype(np.uint16, copy=False).view(np.int16)))
+            sk = self.fields_dev[i][2]
+            if sk is not None:
+                v = sd["sinks"].get(name)
+                sk.copy_(torch.from_numpy(np.ascontiguousarray(v, dtype=np.float32))) if v is not None else sk.zero_()
+            c = self.comp_dev[i]
+            if c is not None:
+                v = sd["residuals"].get(name)
+                c.copy_(torch.from_numpy(np.ascontiguousarray(v, dtype=np.float32))) if v is not None else c.zero_()
+        torch.cuda.synchronize(self.device)
+        self._check(self.lib.olc_set_agent_count(self.handle, n, self._stream()))
+        ss = _lib.OlcStepState()
+        st = sd["step_state"]
+        ss.steps, ss.agent_steps = st["steps"], st["agent_steps"]
+        ss.field_step, ss.status = st["field_step"], st["status"]
+        self._check(self.lib.olc_set_step_state(self.handle, C.byref(ss), self._stream()))
+        self.engine._step = int(sd.get("engine_step", st["steps"]))
+
     def field_tensor(self, name: str):
         """The device tensor currently holding chemistry field ``name`` (x fastest)."""
         _, fb = self._current()

@@ -50,6 +50,51 @@ __global__ void __launch_bounds__(256) k_react16(unsigned short* __restrict__ f,
                                                  float* __restrict__ comp, int nx, int ny, int nz, float dt,
                                                  float decay_step) {
     const size_t nvox = (size_t)nx * ny * nz;
+    const bool aligned = ((reinterpret_cast<uintptr_t>(f) & 7u) | (reinterpret_cast<uintptr_t>(comp) & 15u) |
+                          (reinterpret_cast<uintptr_t>(K) & 15u)) == 0u;
+    if ((nx & 3) == 0 && aligned) {
+        // four voxels of one row per thread, 8- and 16-byte accesses; the
+        // arithmetic per voxel is the scalar loop's below
+        const size_t nq = nvox / 4;
+        for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nq; q += (size_t)gridDim.x * blockDim.x) {
+            const size_t v0 = 4 * q;
+            const int x0 = (int)(v0 % (size_t)nx);
+            const size_t t = v0 / (size_t)nx;
+            const int y = (int)(t % (size_t)ny);
+            const int z = (int)(t / (size_t)ny);
+            const bool face_yz = y == 0 || z == 0 || y == ny - 1 || z == nz - 1;
+            float kv[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            if (K) {
+                const float4 k4 = *reinterpret_cast<const float4*>(K + v0);
+                kv[0] = k4.x;
+                kv[1] = k4.y;
+                kv[2] = k4.z;
+                kv[3] = k4.w;
+                if (k4.x != 0.0f || k4.y != 0.0f || k4.z != 0.0f || k4.w != 0.0f)
+                    *reinterpret_cast<float4*>(K + v0) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
+            if (face_yz) continue;
+            const uint2 h2 = *reinterpret_cast<const uint2*>(f + v0);
+            const float4 c4 = *reinterpret_cast<const float4*>(comp + v0);
+            unsigned short h[4] = {(unsigned short)(h2.x & 0xffffu), (unsigned short)(h2.x >> 16),
+                                   (unsigned short)(h2.y & 0xffffu), (unsigned short)(h2.y >> 16)};
+            float c[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int x = x0 + e;
+                if (x == 0 || x == nx - 1) continue;
+                float val = __fadd_rn(Store16<ST>::to_f(h[e]), c[e]);
+                if (kv[e] != 0.0f) val = __fdiv_rn(val, __fadd_rn(1.0f, __fmul_rn(kv[e], dt)));
+                val = __fmul_rn(val, decay_step);
+                h[e] = Store16<ST>::from_f(val);
+                c[e] = __fsub_rn(val, Store16<ST>::to_f(h[e]));
+            }
+            *reinterpret_cast<uint2*>(f + v0) =
+                make_uint2((olc_u32)h[0] | ((olc_u32)h[1] << 16), (olc_u32)h[2] | ((olc_u32)h[3] << 16));
+            *reinterpret_cast<float4*>(comp + v0) = make_float4(c[0], c[1], c[2], c[3]);
+        }
+        return;
+    }
     for (size_t v = blockIdx.x * (size_t)blockDim.x + threadIdx.x; v < nvox; v += (size_t)gridDim.x * blockDim.x) {
         const int x = (int)(v % (size_t)nx);
         const size_t t = v / (size_t)nx;
@@ -224,12 +269,18 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep_batch_t16(
     const CUtensorMap* map = maps + 2 * j + (flip ? 1 : 0);
     unsigned short* out = (flip ? fa : fb) + d.field_off;
     const int x0 = (int)t.y * TX, y0 = (int)t.z * TYR, z0 = (int)t.w * TZ;
+    // programmatic dependent launch: the next substep's CTAs may start their
+    // prologue (tile entry, member record, parity, barrier set-up: nothing the
+    // previous launch writes) during this launch's last wave; every access to
+    // field data follows griddepcontrol.wait
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncthreads();
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     if (threadIdx.x == 0) {
         asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(BYTES) : "memory");
@@ -268,9 +319,18 @@ static void launch_bt16(const uint4* tiles, olc_u32 n_tiles, const OlcSimDesc* s
         cudaFuncSetAttribute(k_substep_batch_t16<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
         configured_mask |= 1 << dev;
     }
-    k_substep_batch_t16<ST><<<n_tiles, THREADS, SMEM, s>>>(tiles, sims, steps, maps, field, n_fields, fpar, sub,
-                                                          static_cast<unsigned short*>(fa),
-                                                          static_cast<unsigned short*>(fb), step_ctr, status);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(n_tiles);
+    cfg.blockDim = dim3(THREADS);
+    cfg.dynamicSmemBytes = SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_substep_batch_t16<ST>, tiles, sims, steps, maps, field, n_fields, fpar, sub,
+                       static_cast<unsigned short*>(fa), static_cast<unsigned short*>(fb), step_ctr, status);
 }
 
 void launch_substep_batch_t16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,

@@ -52,7 +52,10 @@ __global__ void __launch_bounds__(256) k_engine_metrics(EngineMetricArgs a, cons
             ++cnt[2];
             continue;
         }
-        ++cnt[st == 1 ? 0 : 1];
+        if (st == 1)
+            ++cnt[0];
+        else
+            ++cnt[1];
         if (a.csc && a.csc[i] != 0) ++cnt[3];
         const float px = a.x[i], py = a.y[i], pz = a.z[i];
         const double dx = (double)px - (double)a.cx, dy = (double)py - (double)a.cy, dz = (double)pz - (double)a.cz;

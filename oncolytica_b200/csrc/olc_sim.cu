@@ -1336,6 +1336,37 @@ int olc_set_agent_count(OlcSim* s, uint32_t n, void* stream) {
     return OLC_OK;
 }
 
+int olc_get_step_state(OlcSim* s, OlcStepState* out, void* stream) {
+    if (!s || !out) return fail(s, OLC_ERR_ARG, "olc_get_step_state: null argument");
+    if (s->n_sims) return fail(s, OLC_ERR_STATE, "olc_get_step_state: batch handle");
+    cudaStream_t st = as_stream(stream);
+    OLC_TRY(check(s, cudaMemcpyAsync(s->ctr_host_words, s->counters, OLC_CTR_WORDS * 4, cudaMemcpyDeviceToHost, st),
+                  "counters readback"));
+    OLC_TRY(check(s, cudaStreamSynchronize(st), "sync"));
+    const olc_u32* w = s->ctr_host_words;
+    out->steps = s->steps;
+    out->agent_steps = (uint64_t)w[OLC_CTR_AGENT_STEPS] | ((uint64_t)w[OLC_CTR_AGENT_STEPS + 1] << 32);
+    out->field_step = w[OLC_CTR_FIELD_STEP];
+    out->status = w[OLC_CTR_STATUS];
+    return OLC_OK;
+}
+
+int olc_set_step_state(OlcSim* s, const OlcStepState* in, void* stream) {
+    if (!s || !in) return fail(s, OLC_ERR_ARG, "olc_set_step_state: null argument");
+    if (s->n_sims) return fail(s, OLC_ERR_STATE, "olc_set_step_state: batch handle");
+    cudaStream_t st = as_stream(stream);
+    OLC_TRY(check(s, cudaStreamSynchronize(st), "sync"));
+    olc_u32 w[OLC_CTR_WORDS];
+    OLC_TRY(check(s, cudaMemcpy(w, s->counters, sizeof(w), cudaMemcpyDeviceToHost), "read counters"));
+    w[OLC_CTR_AGENT_STEPS] = (olc_u32)(in->agent_steps & 0xffffffffu);
+    w[OLC_CTR_AGENT_STEPS + 1] = (olc_u32)(in->agent_steps >> 32);
+    w[OLC_CTR_FIELD_STEP] = in->field_step;
+    w[OLC_CTR_STATUS] = in->status;
+    OLC_TRY(check(s, cudaMemcpy(s->counters, w, sizeof(w), cudaMemcpyHostToDevice), "write counters"));
+    s->steps = in->steps;  // host count only; kernels read the device counters
+    return OLC_OK;
+}
+
 int olc_current_buffers(const OlcSim* s, int* agent_buf, int* field_buf) {
     if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
     if (agent_buf) *agent_buf = s->agent_cur;

@@ -269,6 +269,34 @@ class Engine:
             raise RuntimeError("Engine.get_engine_metrics() called before load_model().")
         return self._backend_impl.engine_metrics(**kw)
 
+    # ---- checkpoints ----------------------------------------------------------
+    def state_dict(self) -> dict:
+        """The device state as host arrays (CudaBackend.state_dict); resuming
+        from it with load_state_dict continues bit for bit."""
+        if self._backend_impl is None:
+            raise RuntimeError("Engine.state_dict() called before load_model().")
+        return self._backend_impl.state_dict()
+
+    def load_state_dict(self, sd: dict) -> None:
+        if self._backend_impl is None:
+            raise RuntimeError("Engine.load_state_dict() called before load_model().")
+        self._backend_impl.load_state_dict(sd)
+
+    def export_bundle(self, export_dir: str, exact: bool = True) -> str:
+        """Writes the current state as a bundle (config.json + .bin files, the
+        reference's GpuBackend.export_bundle format) plus, with `exact`, a
+        resume record; returns the path of config.json."""
+        from oncolytica_b200.bundle import export_bundle
+
+        return export_bundle(self, export_dir, exact=exact)
+
+    def import_bundle(self, bundle_dir: str) -> None:
+        """Loads a bundle written by export_bundle (exactly) or by the
+        reference (through its recorded struct layout) into the loaded model."""
+        from oncolytica_b200.bundle import import_bundle
+
+        import_bundle(self, bundle_dir)
+
     def get_reductions(self) -> dict:
         return self._backend_impl.get_reductions()
 
