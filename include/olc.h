@@ -133,6 +133,31 @@ typedef struct {
     float   margin;
 } OlcContact;
 
+/* The rest of the engine's pair law and integrator (Kernel_Interaction,
+ * engine/assets/shaders/tumor_sim.wgsl:505-628), on top of OlcContact:
+ *   - repulsion scaled by necrotic_factor (engine: 0.3) when either agent is
+ *     necrotic (state 3 in state_field);
+ *   - adhesion between non-necrotic agents whose gap g = d - (r_i + r_j) is in
+ *     [0, adhesion_range): force adhesion_stiffness * 0.5 (1 + cos(3.14159 g /
+ *     adhesion_range)) towards the neighbour;
+ *   - with velocity_field >= 0 (three f32 columns holding a vec3), the
+ *     engine's damped velocity instead of the overdamped move:
+ *     v += (F - damping v) dt (damping doubled for a necrotic agent), |v|
+ *     capped at max_speed (engine: 0.8 x bin size), p += v dt, then the domain
+ *     clamp of OlcContact.margin.
+ * Summation order and coincident points are as OlcContact's.  Not used by the
+ * benchmark configurations; solo handles only. */
+typedef struct {
+    int32_t state_field;        /* i32 column, or -1 (nobody necrotic)        */
+    float   necrotic_factor;
+    float   adhesion_stiffness; /* 0: no adhesion                             */
+    float   adhesion_range;
+    int32_t velocity_field;     /* first of three f32 columns, or -1          */
+    float   damping;
+    float   max_speed;
+    int32_t enabled;            /* 0: plain OlcContact                        */
+} OlcMechanics;
+
 typedef struct {
     uint32_t n_agents;          /* agents entering the next step              */
     uint32_t n_total;           /* rows in use incl. this step's dead         */
@@ -202,6 +227,7 @@ int olc_bind_field_ex(OlcSim* sim, int index, void* a_dev, void* b_dev, float* s
                       const OlcDiffusion* spec);
 
 int olc_set_contact(OlcSim* sim, const OlcContact* spec);
+int olc_set_mechanics(OlcSim* sim, const OlcMechanics* spec);
 
 /* Binds the tissue grid for tissue_at(): `n_cols` 4-byte columns, each with
  * voxel_table_size entries indexed by the tissue (Morton) key, `stride_bytes`
@@ -502,6 +528,14 @@ int olc_stage_diffuse16(void* f_dev, void* tmp_dev, float* sink_dev, float* comp
 int olc_stage_contact(const float* posr_dev, const uint32_t* ranges_dev, uint32_t n,
                       const OlcGeom* geom, const OlcContact* spec, float dt,
                       float* x_dev, float* y_dev, float* z_dev, void* stream);
+
+/* The contact pass with OlcMechanics: state_dev (i32 per sorted row) may be
+ * NULL; vx/vy/vz_dev (f32 per sorted row, updated in place) are used when
+ * mech->velocity_field >= 0 and must then be non-NULL. */
+int olc_stage_contact_mech(const float* posr_dev, const uint32_t* ranges_dev, uint32_t n,
+                           const OlcGeom* geom, const OlcContact* spec, const OlcMechanics* mech,
+                           const int32_t* state_dev, float* vx_dev, float* vy_dev, float* vz_dev, float dt,
+                           float* x_dev, float* y_dev, float* z_dev, void* stream);
 
 #ifdef __cplusplus
 }

@@ -47,7 +47,8 @@ EXPORTS = (
     "olc_create_pool", "olc_bind_field_pool", "olc_pool_admit", "olc_pool_add_agents", "olc_pool_gather",
     "olc_pool_copy_results", "olc_pool_retire", "olc_pool_usage",
     "olc_arena_create", "olc_arena_alloc", "olc_arena_release", "olc_arena_stats", "olc_arena_destroy",
-    "olc_engine_metrics", "olc_get_step_state", "olc_set_step_state",
+    "olc_engine_metrics", "olc_get_step_state", "olc_set_step_state", "olc_set_mechanics",
+    "olc_stage_contact_mech",
 )
 
 
@@ -171,6 +172,19 @@ class OlcEngineMetricsSpec(C.Structure):
     ]
 
 
+class OlcMechanics(C.Structure):
+    _fields_ = [
+        ("state_field", C.c_int32),
+        ("necrotic_factor", C.c_float),
+        ("adhesion_stiffness", C.c_float),
+        ("adhesion_range", C.c_float),
+        ("velocity_field", C.c_int32),
+        ("damping", C.c_float),
+        ("max_speed", C.c_float),
+        ("enabled", C.c_int32),
+    ]
+
+
 class OlcStepState(C.Structure):
     _fields_ = [
         ("steps", C.c_uint64),
@@ -264,6 +278,10 @@ _SIGS = {
     "olc_arena_destroy": (C.c_int, [_VP]),
     "olc_engine_metrics": (C.c_int, [_VP, C.POINTER(OlcEngineMetricsSpec), C.POINTER(C.c_double), _VP]),
     "olc_get_step_state": (C.c_int, [_VP, C.POINTER(OlcStepState), _VP]),
+    "olc_set_mechanics": (C.c_int, [_VP, C.POINTER(OlcMechanics)]),
+    "olc_stage_contact_mech": (C.c_int, [_VP, _VP, C.c_uint32, C.POINTER(OlcGeom), C.POINTER(OlcContact),
+                                         C.POINTER(OlcMechanics), _VP, _VP, _VP, _VP, C.c_float, _VP, _VP, _VP,
+                                         _VP]),
     "olc_set_step_state": (C.c_int, [_VP, C.POINTER(OlcStepState), _VP]),
 }
 

@@ -155,6 +155,28 @@ class CudaBackend:
             ct.stiffness, ct.mobility = contact.stiffness, contact.mobility
             ct.max_disp, ct.margin = contact.max_disp, contact.margin
         self._check(self.lib.olc_set_contact(self.handle, C.byref(ct)))
+        if contact is not None and contact.mechanics:
+            m = _lib.OlcMechanics()
+            m.enabled = 1
+            m.state_field = -1
+            if contact.state is not None:
+                for i, (col, _, dt) in enumerate(L.cell_cols):
+                    if col == contact.state and dt == np.int32:
+                        m.state_field = i
+                if m.state_field < 0 and contact.necrotic_factor != 1.0:
+                    raise ValueError(f"setup_contact: no ol.i32 cell field {contact.state!r} for the necrotic test")
+            m.necrotic_factor = contact.necrotic_factor
+            m.adhesion_stiffness = contact.adhesion_stiffness
+            m.adhesion_range = contact.adhesion_range
+            m.velocity_field = -1
+            if contact.velocity is not None:
+                try:
+                    m.velocity_field = L.col_index(f"{contact.velocity}.x")
+                except KeyError:
+                    raise ValueError(f"setup_contact: velocity needs an ol.vec3 cell field {contact.velocity!r}")
+            m.damping = contact.damping
+            m.max_speed = contact.max_speed if contact.max_speed is not None else 0.8 * eng.tissue_voxel_size
+            self._check(self.lib.olc_set_mechanics(self.handle, C.byref(m)))
         if self.program is not None:
             names = (C.c_char_p * len(self.program.kernels))(*[k.encode() for k, _ in self.program.kernels])
             kinds = (C.c_int * len(self.program.kernels))(*[kind for _, kind in self.program.kernels])

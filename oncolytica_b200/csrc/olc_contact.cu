@@ -84,6 +84,133 @@ __global__ void __launch_bounds__(256) k_contact(const float4* __restrict__ posr
     }
 }
 
+// The engine's full pair law (tumor_sim.wgsl:505-628) over the same
+// neighbour walk and summation order as k_contact:
+//   repulsion  dist < r_i + r_j: k * ov^(3/2) along n_ij, k scaled by
+//              necrotic_factor when either agent is necrotic (state 3);
+//   adhesion   r_i + r_j <= dist < r_i + r_j + range, neither necrotic:
+//              -adh_k * 0.5 (1 + cos(3.14159 gap / range)) along n_ij;
+// then either the overdamped move of k_contact, or the engine's damped
+// velocity: v += (F - damping v) dt (damping doubled for a necrotic agent),
+// |v| capped at max_speed, p += v dt, clamped into the domain.  Coincident
+// points are pushed apart along x in index order, as in k_contact (the engine
+// draws a random direction instead).
+__global__ void __launch_bounds__(256) k_contact_mech(const float4* __restrict__ posr,
+                                                      const uint2* __restrict__ ranges, const olc_u32* n_dev,
+                                                      olc_u32 n_host, ContactDev c, MechDev m,
+                                                      float* __restrict__ xo, float* __restrict__ yo,
+                                                      float* __restrict__ zo) {
+    const olc_u32 n = n_dev ? *n_dev : n_host;
+    const bool adh = m.adh_k != 0.0f && m.adh_range > 0.0f;
+    const float k_nec = __fmul_rn(c.stiffness, m.necrotic_factor);
+    for (olc_u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 p = posr[i];
+        if (p.w < 0.0f) continue;
+        const bool nec_i = m.state && m.state[i] == 3;
+        const int cx = olc_bin_coord(p.x, c.tvs, c.tdims[0]);
+        const int cy = olc_bin_coord(p.y, c.tvs, c.tdims[1]);
+        const int cz = olc_bin_coord(p.z, c.tvs, c.tdims[2]);
+        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+        for (int dz = -1; dz <= 1; ++dz) {
+            const int nz = cz + dz;
+            if (nz < 0 || nz >= c.tdims[2]) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int ny = cy + dy;
+                if (ny < 0 || ny >= c.tdims[1]) continue;
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int nx = cx + dx;
+                    if (nx < 0 || nx >= c.tdims[0]) continue;
+                    const uint2 rg = __ldg(ranges + olc_tissue_key(nx, ny, nz));
+                    for (olc_u32 j = rg.x; j < rg.y; ++j) {
+                        if (j == i) continue;
+                        const float4 q = __ldg(posr + j);
+                        if (q.w < 0.0f) continue;
+                        const float ddx = __fsub_rn(p.x, q.x);
+                        const float ddy = __fsub_rn(p.y, q.y);
+                        const float ddz = __fsub_rn(p.z, q.z);
+                        const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)),
+                                                   __fmul_rn(ddz, ddz));
+                        const float rsum = __fadd_rn(p.w, q.w);
+                        const float reach = adh ? __fadd_rn(rsum, m.adh_range) : rsum;
+                        // as in k_contact: beyond reach^2 (1 + 2^-20) the exact tests below fail
+                        if (d2 > __fmul_rn(__fmul_rn(reach, reach), 1.00000095367431640625f)) continue;
+                        const float dist = sqrtf(d2);
+                        if (!(dist < reach)) continue;
+                        const bool nec = nec_i || (m.state && __ldg(m.state + j) == 3);
+                        if (dist < rsum) {
+                            const float ov = __fsub_rn(rsum, dist);
+                            const float f = __fmul_rn(__fmul_rn(nec ? k_nec : c.stiffness, ov), sqrtf(ov));
+                            if (dist < 1e-5f) {
+                                fx = __fadd_rn(fx, i < j ? -f : f);
+                            } else {
+                                const float s = __fdiv_rn(f, dist);
+                                fx = __fadd_rn(fx, __fmul_rn(ddx, s));
+                                fy = __fadd_rn(fy, __fmul_rn(ddy, s));
+                                fz = __fadd_rn(fz, __fmul_rn(ddz, s));
+                            }
+                        } else if (!nec) {
+                            const float gap = __fsub_rn(dist, rsum);
+                            const float fall =
+                                __fmul_rn(0.5f, __fadd_rn(1.0f, cosf(__fdiv_rn(__fmul_rn(3.14159f, gap), m.adh_range))));
+                            const float s = __fdiv_rn(__fmul_rn(m.adh_k, fall), dist);
+                            fx = __fsub_rn(fx, __fmul_rn(ddx, s));
+                            fy = __fsub_rn(fy, __fmul_rn(ddy, s));
+                            fz = __fsub_rn(fz, __fmul_rn(ddz, s));
+                        }
+                    }
+                }
+            }
+        }
+        float mx, my, mz;
+        if (!m.vx) {
+            const float md = __fmul_rn(c.mobility, c.dt);
+            mx = __fmul_rn(fx, md);
+            my = __fmul_rn(fy, md);
+            mz = __fmul_rn(fz, md);
+            const float len =
+                sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz)));
+            if (len > c.max_disp) {
+                const float sc = __fdiv_rn(c.max_disp, len);
+                mx = __fmul_rn(mx, sc);
+                my = __fmul_rn(my, sc);
+                mz = __fmul_rn(mz, sc);
+            }
+        } else {
+            const float damp = nec_i ? __fmul_rn(m.damping, 2.0f) : m.damping;
+            float vx = m.vx[i], vy = m.vy[i], vz = m.vz[i];
+            vx = __fadd_rn(vx, __fmul_rn(__fsub_rn(fx, __fmul_rn(vx, damp)), c.dt));
+            vy = __fadd_rn(vy, __fmul_rn(__fsub_rn(fy, __fmul_rn(vy, damp)), c.dt));
+            vz = __fadd_rn(vz, __fmul_rn(__fsub_rn(fz, __fmul_rn(vz, damp)), c.dt));
+            const float speed =
+                sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz)));
+            if (speed > m.max_speed) {
+                vx = __fmul_rn(__fdiv_rn(vx, speed), m.max_speed);
+                vy = __fmul_rn(__fdiv_rn(vy, speed), m.max_speed);
+                vz = __fmul_rn(__fdiv_rn(vz, speed), m.max_speed);
+            }
+            m.vx[i] = vx;
+            m.vy[i] = vy;
+            m.vz[i] = vz;
+            mx = __fmul_rn(vx, c.dt);
+            my = __fmul_rn(vy, c.dt);
+            mz = __fmul_rn(vz, c.dt);
+        }
+        xo[i] = fminf(fmaxf(__fadd_rn(p.x, mx), c.lo[0]), c.hi[0]);
+        yo[i] = fminf(fmaxf(__fadd_rn(p.y, my), c.lo[1]), c.hi[1]);
+        zo[i] = fminf(fmaxf(__fadd_rn(p.z, mz), c.lo[2]), c.hi[2]);
+    }
+}
+
+void launch_contact_mech(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
+                         olc_u32 n_cap, const ContactDev& c, const MechDev& m, float* x, float* y, float* z,
+                         cudaStream_t s) {
+    olc_u32 blocks = (n_cap + 255) / 256;
+    if (blocks == 0) blocks = 1;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    k_contact_mech<<<blocks, 256, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_dev, n_host, c, m, x, y,
+                                          z);
+}
+
 void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
                     olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s) {
     olc_u32 blocks = (n_cap + 255) / 256;

@@ -164,6 +164,20 @@ struct ContactDev {
 };
 void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
                     olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s);
+// The rest of the engine's force law (OlcMechanics): necrotic repulsion
+// factor, adhesion, damped velocity integration.
+struct MechDev {
+    const int* state;        // null: no agent is necrotic
+    float necrotic_factor;
+    float adh_k, adh_range;  // adh_k == 0: no adhesion
+    float* vx;               // null: overdamped (ContactDev.mobility, max_disp)
+    float* vy;
+    float* vz;
+    float damping, max_speed;
+};
+void launch_contact_mech(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
+                         olc_u32 n_cap, const ContactDev& c, const MechDev& m, float* x, float* y, float* z,
+                         cudaStream_t s);
 
 // ------------------------------------------------------------------ reductions
 struct ReduceArgs {

@@ -70,6 +70,7 @@ struct OlcSim {
 
     OlcContact contact = {};
     ContactDev contact_dev = {};
+    OlcMechanics mech = {};  // engine force-law extras (mech.enabled)
 
     const unsigned char* tissue = nullptr;  // borrowed tissue columns (Morton-indexed)
     int tissue_cols = 0;
@@ -376,7 +377,24 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
     mark(s, 4, st);
     // 4. contact
     const int cc = s->agent_cur;
-    if (s->contact.enabled) {
+    if (s->contact.enabled && s->mech.enabled) {
+        MechDev m = {};
+        m.state = s->mech.state_field >= 0 ? static_cast<const int*>(s->col[cc][s->mech.state_field]) : nullptr;
+        m.necrotic_factor = s->mech.necrotic_factor;
+        m.adh_k = s->mech.adhesion_stiffness;
+        m.adh_range = s->mech.adhesion_range;
+        if (s->mech.velocity_field >= 0) {
+            m.vx = static_cast<float*>(s->col[cc][s->mech.velocity_field]);
+            m.vy = static_cast<float*>(s->col[cc][s->mech.velocity_field + 1]);
+            m.vz = static_cast<float*>(s->col[cc][s->mech.velocity_field + 2]);
+        }
+        m.damping = s->mech.damping;
+        m.max_speed = s->mech.max_speed;
+        launch_contact_mech(s->posr, s->ranges, s->counters + OLC_CTR_N, 0, cap, s->contact_dev, m,
+                            static_cast<float*>(s->col[cc][0]), static_cast<float*>(s->col[cc][1]),
+                            static_cast<float*>(s->col[cc][2]), st);
+        ++launches;
+    } else if (s->contact.enabled) {
         launch_contact(s->posr, s->ranges, s->counters + OLC_CTR_N, 0, cap, s->contact_dev,
                        static_cast<float*>(s->col[cc][0]), static_cast<float*>(s->col[cc][1]),
                        static_cast<float*>(s->col[cc][2]), st);
@@ -1153,6 +1171,23 @@ int olc_bind_tissue(OlcSim* s, const void* cols, int n_cols, size_t stride_bytes
     s->tissue = static_cast<const unsigned char*>(cols);
     s->tissue_cols = n_cols;
     s->tissue_stride = stride_bytes;
+    return OLC_OK;
+}
+
+int olc_set_mechanics(OlcSim* s, const OlcMechanics* m) {
+    if (!s || !m) return fail(s, OLC_ERR_ARG, "olc_set_mechanics: null argument");
+    if (s->n_sims && m->enabled) return fail(s, OLC_ERR_STATE, "olc_set_mechanics: solo handles only");
+    const int nc = (int)s->caps.n_agent_fields;
+    if (m->enabled) {
+        if (m->state_field >= nc || m->velocity_field + 3 > nc)
+            return fail(s, OLC_ERR_ARG, "olc_set_mechanics: column out of range");
+        if (m->adhesion_stiffness != 0.0f && !(m->adhesion_range > 0.0f))
+            return fail(s, OLC_ERR_ARG, "olc_set_mechanics: adhesion needs adhesion_range > 0");
+        if (m->velocity_field >= 0 && !(m->max_speed > 0.0f))
+            return fail(s, OLC_ERR_ARG, "olc_set_mechanics: velocity integration needs max_speed > 0");
+    }
+    drop_graphs(s);
+    s->mech = *m;
     return OLC_OK;
 }
 
@@ -2186,6 +2221,46 @@ int olc_stage_contact(const float* posr, const uint32_t* ranges, uint32_t n, con
     d.dt = dt;
     launch_contact(reinterpret_cast<const float4*>(posr), ranges, nullptr, n, n, d, x, y, z, as_stream(stream));
     return cuda_status(cudaGetLastError(), "olc_stage_contact");
+}
+
+int olc_stage_contact_mech(const float* posr, const uint32_t* ranges, uint32_t n, const OlcGeom* geom,
+                           const OlcContact* spec, const OlcMechanics* mech, const int32_t* state, float* vx,
+                           float* vy, float* vz, float dt, float* x, float* y, float* z, void* stream) {
+    if (!geom || !spec || !mech || (n && (!posr || !ranges || !x || !y || !z)))
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_contact_mech: null argument");
+    if (mech->velocity_field >= 0 && n && (!vx || !vy || !vz))
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_contact_mech: velocity columns missing");
+    if (mech->adhesion_stiffness != 0.0f && !(mech->adhesion_range > 0.0f))
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_contact_mech: adhesion needs adhesion_range > 0");
+    std::string err;
+    if (!geom_ok(*geom, &err)) return fail(nullptr, OLC_ERR_ARG, "olc_stage_contact_mech: " + err);
+    if (n == 0) return OLC_OK;
+    ContactDev d;
+    for (int i = 0; i < 3; ++i) {
+        d.tdims[i] = geom->tissue_dims[i];
+        d.lo[i] = geom->domain_lo[i] + spec->margin;
+        d.hi[i] = geom->domain_hi[i] - spec->margin;
+    }
+    d.tvs = geom->tissue_voxel_size;
+    d.stiffness = spec->stiffness;
+    d.mobility = spec->mobility;
+    d.max_disp = spec->max_disp;
+    d.dt = dt;
+    MechDev m = {};
+    m.state = state;
+    m.necrotic_factor = mech->necrotic_factor;
+    m.adh_k = mech->adhesion_stiffness;
+    m.adh_range = mech->adhesion_range;
+    if (mech->velocity_field >= 0) {
+        m.vx = vx;
+        m.vy = vy;
+        m.vz = vz;
+    }
+    m.damping = mech->damping;
+    m.max_speed = mech->max_speed;
+    launch_contact_mech(reinterpret_cast<const float4*>(posr), ranges, nullptr, n, n, d, m, x, y, z,
+                        as_stream(stream));
+    return cuda_status(cudaGetLastError(), "olc_stage_contact_mech");
 }
 
 }  // extern "C"

@@ -43,6 +43,18 @@ class ContactSpec:
     mobility: float = 10.0
     max_disp: float = 1.0
     margin: float = 0.1
+    # the engine's extras (tumor_sim.wgsl:505-628); defaults leave them off
+    necrotic_factor: float = 1.0
+    adhesion_stiffness: float = 0.0
+    adhesion_range: float = 0.0
+    velocity: str | None = None
+    damping: float = 1.0
+    max_speed: float | None = None
+    state: str | None = "state"
+
+    @property
+    def mechanics(self) -> bool:
+        return self.necrotic_factor != 1.0 or self.adhesion_stiffness != 0.0 or self.velocity is not None
 
 
 def stable_substeps(D: float, dt: float, dx: float, margin: float = 1.05) -> int:
@@ -171,10 +183,23 @@ class Engine:
         self._diffusion[field] = DiffusionSpec(float(diffusion), float(decay), float(boundary), substeps, storage)
 
     def setup_contact(self, radius: str | float = "radius", stiffness: float = 1.0, mobility: float = 10.0,
-                      max_disp: float = 1.0, margin: float = 0.1) -> None:
+                      max_disp: float = 1.0, margin: float = 0.1, necrotic_factor: float = 1.0,
+                      adhesion_stiffness: float = 0.0, adhesion_range: float = 0.0, velocity: str | None = None,
+                      damping: float = 1.0, max_speed: float | None = None, state: str | None = "state") -> None:
         """Built-in Hertz-like contact repulsion over the 27 bins
-        (engine tumor_sim.wgsl:505-628), overdamped."""
-        self._contact = ContactSpec(radius, float(stiffness), float(mobility), float(max_disp), float(margin))
+        (engine tumor_sim.wgsl:505-628), overdamped.  The engine's other terms
+        are optional: `necrotic_factor` scales repulsion when either agent's
+        `state` is 3 (the engine uses 0.3); `adhesion_stiffness` and
+        `adhesion_range` add the cosine adhesion between non-necrotic agents;
+        `velocity` names an ol.vec3 cell field for the engine's damped velocity
+        integration (`damping`, speed cap `max_speed`, default 0.8 x bin size)
+        in place of the overdamped move."""
+        if adhesion_stiffness != 0.0 and not adhesion_range > 0.0:
+            raise ValueError("adhesion_stiffness needs adhesion_range > 0")
+        self._contact = ContactSpec(radius, float(stiffness), float(mobility), float(max_disp), float(margin),
+                                    float(necrotic_factor), float(adhesion_stiffness), float(adhesion_range),
+                                    velocity, float(damping), None if max_speed is None else float(max_speed),
+                                    state)
 
     def setup_domain(self, lo: tuple[float, float, float], hi: tuple[float, float, float]) -> None:
         self.domain_lo = tuple(float(v) for v in lo)

@@ -521,6 +521,111 @@ void orc_contact(const float* posr, const uint32_t* ranges, uint32_t n, const in
     }
 }
 
+/* Restates k_contact_mech: the walk, order and rounding of orc_contact, with
+ * the engine's necrotic factor and adhesion branch
+ * (engine/assets/shaders/tumor_sim.wgsl:552-569) and its damped velocity
+ * integration (:606-625). */
+void orc_contact_mech(const float* posr, const uint32_t* ranges, uint32_t n, const int32_t tdims[3], float tvs,
+                      float stiffness, float mobility, float max_disp, float dt, const float lo[3], const float hi[3],
+                      const int32_t* state, float necrotic_factor, float adh_k, float adh_range, float* vx,
+                      float* vy, float* vz, float damping, float max_speed, float* xo, float* yo, float* zo,
+                      int nthreads) {
+    const int nt = nthreads_or_all(nthreads);
+    const int adh = adh_k != 0.0f && adh_range > 0.0f;
+    const float k_nec = stiffness * necrotic_factor;
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 1024)
+    for (long long ii = 0; ii < (long long)n; ++ii) {
+        const uint32_t i = (uint32_t)ii;
+        const float* p = posr + 4 * (size_t)i;
+        if (p[3] < 0.0f) continue;
+        const int nec_i = state && state[i] == 3;
+        const int cx = orc_bin_coord(p[0], tvs, tdims[0]);
+        const int cy = orc_bin_coord(p[1], tvs, tdims[1]);
+        const int cz = orc_bin_coord(p[2], tvs, tdims[2]);
+        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+        for (int dz = -1; dz <= 1; ++dz) {
+            const int nz = cz + dz;
+            if (nz < 0 || nz >= tdims[2]) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int ny = cy + dy;
+                if (ny < 0 || ny >= tdims[1]) continue;
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int nx = cx + dx;
+                    if (nx < 0 || nx >= tdims[0]) continue;
+                    const uint32_t k = orc_tissue_key(nx, ny, nz);
+                    const uint32_t s = ranges[2 * (size_t)k], e = ranges[2 * (size_t)k + 1];
+                    for (uint32_t j = s; j < e; ++j) {
+                        if (j == i) continue;
+                        const float* q = posr + 4 * (size_t)j;
+                        if (q[3] < 0.0f) continue;
+                        const float ddx = p[0] - q[0], ddy = p[1] - q[1], ddz = p[2] - q[2];
+                        const float d2 = (ddx * ddx + ddy * ddy) + ddz * ddz;
+                        const float rsum = p[3] + q[3];
+                        const float reach = adh ? rsum + adh_range : rsum;
+                        const float dist = sqrtf(d2);
+                        if (!(dist < reach)) continue;
+                        const int nec = nec_i || (state && state[j] == 3);
+                        if (dist < rsum) {
+                            const float ov = rsum - dist;
+                            const float f = ((nec ? k_nec : stiffness) * ov) * sqrtf(ov);
+                            if (dist < 1e-5f) {
+                                fx = fx + (i < j ? -f : f);
+                            } else {
+                                const float sc = f / dist;
+                                fx = fx + ddx * sc;
+                                fy = fy + ddy * sc;
+                                fz = fz + ddz * sc;
+                            }
+                        } else if (!nec) {
+                            const float gap = dist - rsum;
+                            const float fall = 0.5f * (1.0f + cosf((3.14159f * gap) / adh_range));
+                            const float sc = (adh_k * fall) / dist;
+                            fx = fx - ddx * sc;
+                            fy = fy - ddy * sc;
+                            fz = fz - ddz * sc;
+                        }
+                    }
+                }
+            }
+        }
+        float mx, my, mz;
+        if (!vx) {
+            const float md = mobility * dt;
+            mx = fx * md;
+            my = fy * md;
+            mz = fz * md;
+            const float len = sqrtf((mx * mx + my * my) + mz * mz);
+            if (len > max_disp) {
+                const float sc = max_disp / len;
+                mx = mx * sc;
+                my = my * sc;
+                mz = mz * sc;
+            }
+        } else {
+            const float damp = nec_i ? damping * 2.0f : damping;
+            float ux = vx[i], uy = vy[i], uz = vz[i];
+            ux = ux + (fx - ux * damp) * dt;
+            uy = uy + (fy - uy * damp) * dt;
+            uz = uz + (fz - uz * damp) * dt;
+            const float speed = sqrtf((ux * ux + uy * uy) + uz * uz);
+            if (speed > max_speed) {
+                ux = (ux / speed) * max_speed;
+                uy = (uy / speed) * max_speed;
+                uz = (uz / speed) * max_speed;
+            }
+            vx[i] = ux;
+            vy[i] = uy;
+            vz[i] = uz;
+            mx = ux * dt;
+            my = uy * dt;
+            mz = uz * dt;
+        }
+        xo[i] = fminf(fmaxf(p[0] + mx, lo[0]), hi[0]);
+        yo[i] = fminf(fmaxf(p[1] + my, lo[1]), hi[1]);
+        zo[i] = fminf(fmaxf(p[2] + mz, lo[2]), hi[2]);
+    }
+}
+
 /* ------------------------------------------------------------------ tumour workload */
 
 size_t orc_tumour_sizeof(void) { return sizeof(OrcTumour); }

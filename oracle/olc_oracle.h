@@ -64,6 +64,15 @@ int orc_diffuse_f64(double* f, double* tmp, const float* sink, const int32_t dim
 void orc_contact(const float* posr, const uint32_t* ranges, uint32_t n, const int32_t tdims[3], float tvs,
                  float stiffness, float mobility, float max_disp, float dt, const float lo[3], const float hi[3],
                  float* x, float* y, float* z, int nthreads);
+/* Contact with the engine's extras (engine/assets/shaders/tumor_sim.wgsl:505-628,
+ * Kernel_Interaction): necrotic repulsion factor (state 3), cosine adhesion
+ * between non-necrotic agents, and, with vx != NULL, damped velocity
+ * integration with a speed cap; otherwise the overdamped move of orc_contact. */
+void orc_contact_mech(const float* posr, const uint32_t* ranges, uint32_t n, const int32_t tdims[3], float tvs,
+                      float stiffness, float mobility, float max_disp, float dt, const float lo[3], const float hi[3],
+                      const int32_t* state, float necrotic_factor, float adh_k, float adh_range, float* vx,
+                      float* vy, float* vz, float damping, float max_speed, float* xo, float* yo, float* zo,
+                      int nthreads);
 
 /* ---------------------------------------------------------------------------
  * Tumour-spheroid workload (the built-in benchmark model, restated from its

@@ -43,6 +43,9 @@ def lib() -> C.CDLL:
                                   C.c_int]
         L.orc_contact.argtypes = [P, P, C.c_uint32, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
                                   P, P, P, P, P, C.c_int]
+        L.orc_contact_mech.argtypes = [P, P, C.c_uint32, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                                       P, P, P, C.c_float, C.c_float, C.c_float, P, P, P, C.c_float, C.c_float,
+                                       P, P, P, C.c_int]
         L.orc_tumour_step.restype = C.c_int
         L.orc_tumour_step.argtypes = [P, C.c_int]
         L.orc_tumour_fields.restype = C.c_int
@@ -197,6 +200,29 @@ def contact(posr: np.ndarray, ranges: np.ndarray, tdims, tvs: float, stiffness: 
     lib().orc_contact(_p(posr), _p(r), n, _p(td), C.c_float(tvs), C.c_float(stiffness), C.c_float(mobility),
                       C.c_float(max_disp), C.c_float(dt), _p(lo_a), _p(hi_a), _p(x), _p(y), _p(z), nthreads)
     return np.stack([x, y, z], axis=1)
+
+
+def contact_mech(posr: np.ndarray, ranges: np.ndarray, tdims, tvs: float, stiffness: float, mobility: float,
+                 max_disp: float, dt: float, lo, hi, state=None, necrotic_factor: float = 1.0, adh_k: float = 0.0,
+                 adh_range: float = 0.0, vel: np.ndarray | None = None, damping: float = 0.0,
+                 max_speed: float = 0.0, nthreads: int = 0):
+    """orc_contact_mech; returns positions (n, 3) and, with `vel`, the new velocities."""
+    posr = np.ascontiguousarray(posr, dtype=np.float32)
+    n = len(posr)
+    x, y, z = (posr[:, k].copy() for k in range(3))
+    td = np.array(tdims, dtype=np.int32)
+    lo_a = np.array(lo, dtype=np.float32)
+    hi_a = np.array(hi, dtype=np.float32)
+    r = np.ascontiguousarray(ranges, dtype=np.uint32)
+    st = None if state is None else np.ascontiguousarray(state, dtype=np.int32)
+    v = None if vel is None else [np.ascontiguousarray(vel[:, k], dtype=np.float32).copy() for k in range(3)]
+    lib().orc_contact_mech(_p(posr), _p(r), n, _p(td), C.c_float(tvs), C.c_float(stiffness), C.c_float(mobility),
+                           C.c_float(max_disp), C.c_float(dt), _p(lo_a), _p(hi_a), _p(st), C.c_float(necrotic_factor),
+                           C.c_float(adh_k), C.c_float(adh_range), _p(v[0]) if v else None,
+                           _p(v[1]) if v else None, _p(v[2]) if v else None, C.c_float(damping),
+                           C.c_float(max_speed), _p(x), _p(y), _p(z), nthreads)
+    pos = np.stack([x, y, z], axis=1)
+    return (pos, np.stack(v, axis=1)) if v else (pos, None)
 
 
 # ------------------------------------------------------------------ tumour workload

@@ -320,6 +320,50 @@ def test_tumour_step_parity_with_oracle(cuda):
     assert all(v > 0 for v in seen.values()), seen
 
 
+def test_engine_mechanics_path_in_the_step(cuda):
+    """The step's contact stage through k_contact_mech (OlcMechanics enabled
+    with the plain law's parameters: necrotic factor 1, no adhesion,
+    overdamped) reproduces the oracle's plain step, so the state and column
+    plumbing of the extended kernel is the plain kernel's; a necrotic factor
+    of 0.3 then changes the positions of agents touching necrotic ones."""
+    import ctypes as C
+
+    import oracle
+    from oncolytica_b200 import _lib
+
+    spec = _parity_spec()
+    eng = W.build_engine(spec)
+    x = (np.arange(spec.field_dims[0], dtype=np.float32) + 0.5) / spec.field_dims[0]
+    eng.chemistry.column("o2")[...] = np.clip(2.2 * x - 0.6, 0.0, 1.0)[:, None, None]
+    eng.sync_to_device()
+    be = eng._backend_impl
+    m = _lib.OlcMechanics(state_field=be.layout.col_index("state"), necrotic_factor=1.0, adhesion_stiffness=0.0,
+                          adhesion_range=0.0, velocity_field=-1, damping=1.0, max_speed=8.0, enabled=1)
+    be._check(be.lib.olc_set_mechanics(be.handle, C.byref(m)))
+    for step in range(3):
+        snap = be.snapshot()
+        orc = oracle.TumourOracle.from_snapshot(spec, snap, spec.capacity)
+        eng.run_step()
+        orc.step(nthreads=4)
+        got = be.snapshot()
+        n = got["rows"]
+        assert n == orc.rows
+        for a, key in (("pos.x", "x"), ("pos.y", "y"), ("pos.z", "z")):
+            np.testing.assert_allclose(got["cols"][a], orc.bufs[key][:n], rtol=0, atol=1e-4)
+    assert (got["cols"]["state"] == 3).any()
+    snap = be.snapshot()
+    orc = oracle.TumourOracle.from_snapshot(spec, snap, spec.capacity)
+    m.necrotic_factor = 0.3
+    be._check(be.lib.olc_set_mechanics(be.handle, C.byref(m)))
+    eng.run_step()
+    orc.step(nthreads=4)
+    got = be.snapshot()
+    n = got["rows"]
+    np.testing.assert_array_equal(got["cols"]["state"], orc.bufs["state"][:n])
+    moved = np.abs(got["cols"]["pos.x"] - orc.bufs["x"][:n]) > 1e-3
+    assert moved.any(), "a necrotic factor of 0.3 must change some contacts"
+
+
 def test_tumour_long_run_statistics(cuda):
     """Independent 60-step runs (GPU vs oracle, same seed): population counts
     within 1 % and radial profiles within 3 % of the live count."""

@@ -302,6 +302,64 @@ def test_contact_bit_exact(cuda, olc):
     assert moved.sum() > n // 2
 
 
+@pytest.mark.parametrize("adhesion,velocity", [(False, True), (True, False), (True, True)])
+def test_contact_mechanics_matches_the_oracle(cuda, olc, adhesion, velocity):
+    """The engine's force-law extras (necrotic factor, adhesion, damped
+    velocity; tumor_sim.wgsl:505-628) against orc_contact_mech.  Without
+    adhesion every operation is + - * / sqrt and the bits agree; the
+    adhesion falloff calls cosf, which CUDA and the host C library may round
+    differently by an ulp, so those cases agree to 1e-5 um."""
+    rng = np.random.default_rng(21)
+    dims, vs = (16, 16, 16), 10.0
+    n = 20000
+    pos = np.clip(rng.normal(80.0, 22.0, size=(n, 3)), 0.0, 159.0).astype(np.float32)
+    pos[7] = pos[8]  # a coincident pair
+    radius = rng.uniform(4.0, 6.0, size=n).astype(np.float32)
+    k = oracle.keys(pos, dims, vs)
+    ks, perm = oracle.sort_pairs(k)
+    ranges = oracle.bin_ranges(ks, oracle.tissue_key(*dims))
+    posr = np.concatenate([pos[perm], radius[perm, None]], axis=1).astype(np.float32)
+    posr[rng.random(n) < 0.02, 3] = -1.0
+    state = rng.choice(np.array([1, 2, 3], np.int32), size=n, p=[0.5, 0.3, 0.2]).astype(np.int32)
+    vel = rng.normal(0.0, 2.0, size=(n, 3)).astype(np.float32) if velocity else None
+    prm = dict(stiffness=1.0, mobility=10.0, max_disp=1.0, dt=0.1)
+    mech = dict(necrotic_factor=0.3, adh_k=0.4 if adhesion else 0.0, adh_range=2.5 if adhesion else 0.0,
+                damping=1.5, max_speed=8.0)
+    lo, hi = (0.1, 0.1, 0.1), (159.9, 159.9, 159.9)
+    ref, ref_v = oracle.contact_mech(posr, ranges, dims, vs, prm["stiffness"], prm["mobility"], prm["max_disp"],
+                                     prm["dt"], lo, hi, state=state, vel=vel, **mech)
+    pr, rg = to_dev(posr, cuda), to_dev(ranges, cuda)
+    x, y, z = (to_dev(np.ascontiguousarray(posr[:, c]), cuda) for c in range(3))
+    st = to_dev(state, cuda)
+    vd = [to_dev(np.ascontiguousarray(vel[:, c]), cuda) for c in range(3)] if velocity else [None] * 3
+    g = geom(dims, vs, lo=(0, 0, 0), hi=(160, 160, 160))
+    spec = _lib.OlcContact(enabled=1, radius_field=-1, radius_const=0.0, stiffness=prm["stiffness"],
+                           mobility=prm["mobility"], max_disp=prm["max_disp"], margin=0.1)
+    m = _lib.OlcMechanics(state_field=0, necrotic_factor=mech["necrotic_factor"], adhesion_stiffness=mech["adh_k"],
+                          adhesion_range=mech["adh_range"], velocity_field=0 if velocity else -1,
+                          damping=mech["damping"], max_speed=mech["max_speed"], enabled=1)
+    _lib.check(olc.olc_stage_contact_mech(dptr(pr), dptr(rg), n, C.byref(g), C.byref(spec), C.byref(m), dptr(st),
+                                          *(dptr(v) if v is not None else None for v in vd), prm["dt"], dptr(x),
+                                          dptr(y), dptr(z), None))
+    got = np.stack([to_host(x), to_host(y), to_host(z)], axis=1)
+    if adhesion:
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-5)
+        assert np.mean(got == ref) > 0.9
+    else:
+        np.testing.assert_array_equal(got, ref)
+    if velocity:
+        got_v = np.stack([to_host(v) for v in vd], axis=1)
+        if adhesion:
+            np.testing.assert_allclose(got_v, ref_v, rtol=0, atol=1e-4)
+        else:
+            np.testing.assert_array_equal(got_v, ref_v)
+        assert np.abs(got_v).max() <= mech["max_speed"] * (1 + 1e-6)
+    # the extras change the result: necrotic pairs repel less, adhesion pulls
+    plain = oracle.contact(posr, ranges, dims, vs, prm["stiffness"], prm["mobility"], prm["max_disp"], prm["dt"],
+                           lo, hi)
+    assert np.any(got != plain)
+
+
 # ------------------------------------------------------------------ 16-bit field storage
 
 @pytest.mark.parametrize("storage", [1, 2, 3, 4])
