@@ -384,7 +384,7 @@ def run_b200(args) -> None:
         # scale workload
         torch.cuda.empty_cache()
         line["batched"] = {st: measure_batch(args.sims, args.extra_steps, 3, graphs=not args.no_graphs,
-                                             solo_sample=16 if st == "f32" else 0, storage=st)
+                                             solo_sample=64 if st == "f32" else 0, storage=st)
                            for st in ("f32", "f16_sr")}
         # the batched forms against the plain FP32 path on the same sweep:
         # members sampled evenly over the sweep run one at a time on solo FP32

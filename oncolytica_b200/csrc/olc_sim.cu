@@ -16,6 +16,9 @@
 
 #include <nvrtc.h>
 
+#include <map>
+#include <mutex>
+
 #include <algorithm>
 #include <array>
 #include <cstdio>
@@ -1275,9 +1278,25 @@ int olc_set_rule_source(OlcSim* s, const char* src, const char* const* kernels, 
         ncell += kinds[i] == 0;
     }
     OLC_TRY(ensure_context(s));
+    // Compiled modules are cached in the process by their source and include
+    // directory (the runtime headers there do not change while it runs), so
+    // engines of one model compile once; each handle still loads its own copy.
+    static std::mutex cache_mu;
+    static std::map<std::string, std::vector<char>> cache;
+    std::string key = std::string(include_dir ? include_dir : "") + '\n' + src;
     std::vector<char> cubin;
-    std::string log;
-    if (nvrtc_compile(src, include_dir, &cubin, &log) != OLC_OK) return fail(s, OLC_ERR_NVRTC, log);
+    {
+        std::lock_guard<std::mutex> lk(cache_mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) cubin = it->second;
+    }
+    if (cubin.empty()) {
+        std::string log;
+        if (nvrtc_compile(src, include_dir, &cubin, &log) != OLC_OK) return fail(s, OLC_ERR_NVRTC, log);
+        std::lock_guard<std::mutex> lk(cache_mu);
+        if (cache.size() >= 64) cache.clear();
+        cache.emplace(std::move(key), cubin);
+    }
     drop_graphs(s);
     if (s->module) {
         cudaDeviceSynchronize();
