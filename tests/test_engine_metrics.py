@@ -49,13 +49,13 @@ def test_engine_metrics_match_the_oracle(cuda, storage, crowd):
                     capacity=20_000, seed=5, uptake=2.0, death_k=0.3, init_drug=0.2, v_lo=1.9, v_hi=2.0,
                     storage=storage)
     eng = W.build_engine(spec)
-    # an O2 ramp along x: no oxygen in the lower half of the domain (the
-    # agents there turn necrotic in the first step), full oxygen at the top
+    # an O2 ramp along x: no oxygen in the lower half of the domain, so the
+    # first step holds necrotic, quiescent and proliferating agents (the
+    # oracle's run of this case: 50 / 1874 / 993 after one step)
     x = (np.arange(spec.field_dims[0], dtype=np.float32) + 0.5) / spec.field_dims[0]
     eng.chemistry.column("o2")[...] = np.clip(2.0 * x - 1.0, 0.0, 1.0)[:, None, None]
     eng.sync_to_device()
     be = eng._backend_impl
-    eng.run_steps(3)
     before = be.snapshot()
     eng.run_step(collect_metrics=True)
     after = be.snapshot()
