@@ -14,6 +14,8 @@
 // order with separately rounded operations.
 #include "olc_internal.h"
 
+#include <cstdlib>
+
 namespace olc {
 
 // One thread per agent, grid-stride.  The force sum runs over the Moore bins
@@ -211,8 +213,120 @@ void launch_contact_mech(const float4* posr, const olc_u32* ranges, const olc_u3
                                           z);
 }
 
+// The same sum as k_contact with one flat loop over each agent's candidates:
+// a thread first lists its non-empty Moore bins (in order) in its own column
+// of shared memory, then walks rows bin after bin, so the lanes of a warp stay
+// converged until each has run out of candidates (the nested loops run every
+// bin as long as the fullest lane's).  Same candidates, order and arithmetic.
+constexpr int CF_THREADS = 128;
+__global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __restrict__ posr,
+                                                            const uint2* __restrict__ ranges, const olc_u32* n_dev,
+                                                            olc_u32 n_host, ContactDev c, float* __restrict__ xo,
+                                                            float* __restrict__ yo, float* __restrict__ zo) {
+    __shared__ uint2 s_bins[27][CF_THREADS];
+    const olc_u32 n = n_dev ? *n_dev : n_host;
+    const float md = __fmul_rn(c.mobility, c.dt);
+    const int t = threadIdx.x;
+    for (olc_u32 base = blockIdx.x * CF_THREADS; base < n; base += gridDim.x * CF_THREADS) {
+        const olc_u32 i = base + t;
+        if (i >= n) continue;
+        const float4 p = posr[i];
+        if (p.w < 0.0f) continue;  // dead this step: no move, no force
+        const int cx = olc_bin_coord(p.x, c.tvs, c.tdims[0]);
+        const int cy = olc_bin_coord(p.y, c.tvs, c.tdims[1]);
+        const int cz = olc_bin_coord(p.z, c.tvs, c.tdims[2]);
+        int nb = 0;
+        for (int dz = -1; dz <= 1; ++dz) {
+            const int nz = cz + dz;
+            if (nz < 0 || nz >= c.tdims[2]) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int ny = cy + dy;
+                if (ny < 0 || ny >= c.tdims[1]) continue;
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int nx = cx + dx;
+                    if (nx < 0 || nx >= c.tdims[0]) continue;
+                    const uint2 rg = __ldg(ranges + olc_tissue_key(nx, ny, nz));
+                    if (rg.y > rg.x) s_bins[nb++][t] = rg;
+                }
+            }
+        }
+        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+        int b = 0;
+        olc_u32 j = 0, end = 0;
+        if (nb > 0) {
+            const uint2 r = s_bins[0][t];
+            j = r.x;
+            end = r.y;
+        }
+        while (b < nb) {
+            if (j != i) {
+                const float4 q = __ldg(posr + j);
+                if (!(q.w < 0.0f)) {
+                    const float ddx = __fsub_rn(p.x, q.x);
+                    const float ddy = __fsub_rn(p.y, q.y);
+                    const float ddz = __fsub_rn(p.z, q.z);
+                    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)),
+                                               __fmul_rn(ddz, ddz));
+                    const float rsum = __fadd_rn(p.w, q.w);
+                    if (!(d2 > __fmul_rn(__fmul_rn(rsum, rsum), 1.00000095367431640625f))) {
+                        const float dist = sqrtf(d2);
+                        if (dist < rsum) {
+                            const float ov = __fsub_rn(rsum, dist);
+                            const float f = __fmul_rn(__fmul_rn(c.stiffness, ov), sqrtf(ov));
+                            if (dist < 1e-5f) {
+                                fx = __fadd_rn(fx, i < j ? -f : f);
+                            } else {
+                                const float sc = __fdiv_rn(f, dist);
+                                fx = __fadd_rn(fx, __fmul_rn(ddx, sc));
+                                fy = __fadd_rn(fy, __fmul_rn(ddy, sc));
+                                fz = __fadd_rn(fz, __fmul_rn(ddz, sc));
+                            }
+                        }
+                    }
+                }
+            }
+            if (++j == end) {
+                if (++b < nb) {
+                    const uint2 r = s_bins[b][t];
+                    j = r.x;
+                    end = r.y;
+                }
+            }
+        }
+        float mx = __fmul_rn(fx, md), my = __fmul_rn(fy, md), mz = __fmul_rn(fz, md);
+        const float len = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz)));
+        if (len > c.max_disp) {
+            const float sc = __fdiv_rn(c.max_disp, len);
+            mx = __fmul_rn(mx, sc);
+            my = __fmul_rn(my, sc);
+            mz = __fmul_rn(mz, sc);
+        }
+        xo[i] = fminf(fmaxf(__fadd_rn(p.x, mx), c.lo[0]), c.hi[0]);
+        yo[i] = fminf(fmaxf(__fadd_rn(p.y, my), c.lo[1]), c.hi[1]);
+        zo[i] = fminf(fmaxf(__fadd_rn(p.z, mz), c.lo[2]), c.hi[2]);
+    }
+}
+
+// OLC_CONTACT=flat selects k_contact_flat (same bits as k_contact).
+static bool contact_flat() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("OLC_CONTACT");
+        v = (e && e[0] == 'f') ? 1 : 0;
+    }
+    return v == 1;
+}
+
 void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
                     olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s) {
+    if (contact_flat()) {
+        olc_u32 blocks = (n_cap + CF_THREADS - 1) / CF_THREADS;
+        if (blocks == 0) blocks = 1;
+        if (blocks > 148 * 16) blocks = 148 * 16;
+        k_contact_flat<<<blocks, CF_THREADS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_dev, n_host, c,
+                                                     x, y, z);
+        return;
+    }
     olc_u32 blocks = (n_cap + 255) / 256;
     if (blocks == 0) blocks = 1;
     if (blocks > 148 * 8) blocks = 148 * 8;
