@@ -504,12 +504,25 @@ def metric_fields(cls: type) -> dict[str, Any]:
     return {k: v for k, v in get_type_hints(cls).items() if not k.startswith("_")}
 
 
+_PARAM_HINTS: dict = {}
+
+
+def _param_hints(cls: type) -> dict:
+    """get_type_hints of a Params class, resolved once per class (resolving
+    string annotations costs tens of microseconds, and update_params
+    validates every field on every call)."""
+    h = _PARAM_HINTS.get(cls)
+    if h is None:
+        h = _PARAM_HINTS[cls] = get_type_hints(cls)
+    return h
+
+
 @dataclass(frozen=True, init=False)
 class Params:
     """Frozen typed parameters (reference _types.py:638-698)."""
 
     def __init__(self, **kwargs: Any) -> None:
-        hints = get_type_hints(type(self))
+        hints = _param_hints(type(self))
         for k in kwargs:
             if k not in hints:
                 raise TypeError(f"Missing field '{k}' in {type(self).__name__}")
@@ -535,7 +548,7 @@ class Params:
         cls()._validate()
 
     def _validate_field(self, name: str, val: Any) -> None:
-        hints = get_type_hints(type(self))
+        hints = _param_hints(type(self))
         if name not in hints:
             raise TypeError(f"Missing field '{name}' in {type(self).__name__}")
         t = hints[name]
@@ -548,7 +561,7 @@ class Params:
                             f"got {type(val).__name__} ({val!r})")
 
     def _validate(self) -> None:
-        hints = get_type_hints(type(self))
+        hints = _param_hints(type(self))
         for name, t in hints.items():
             if t not in PRIMITIVE_TYPES:
                 raise TypeError(f"Unsupported type '{t}' for '{name}' in {type(self).__name__}")
@@ -557,7 +570,7 @@ class Params:
 
 
 def param_fields(cls: type) -> dict[str, Any]:
-    return dict(get_type_hints(cls))
+    return dict(_param_hints(cls))
 
 
 BASE_CLASSES = [Tissue, Chemistry, Cell, Metrics, Params]
