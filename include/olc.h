@@ -237,10 +237,27 @@ int olc_set_mechanics(OlcSim* sim, const OlcMechanics* spec);
  * _gpu_backend.py:365-367 — here the host packs it by key). */
 int olc_bind_tissue(OlcSim* sim, const void* cols_dev, int n_cols, size_t stride_bytes);
 
+/* Tissue grid that tissue rules update: two buffers laid out as in
+ * olc_bind_tissue; a tissue rule reads the current one and writes the other
+ * (the reference's Tissue_In / Tissue_Out,
+ * framework/src/oncolytica/gpu/runtime/_gpu_backend.py:130-133).
+ * olc_current_tissue tells which holds the state (0 = a, 1 = b). */
+int olc_bind_tissue_pair(OlcSim* sim, void* a_dev, void* b_dev, int n_cols, size_t stride_bytes);
+int olc_current_tissue(const OlcSim* sim, int* tissue_buf);
+
+/* Iterations of each kernel of the last olc_set_rule_source (chemistry rules'
+ * @chemistry_rule(iterations=k); 1 for the others). */
+int olc_set_rule_iterations(OlcSim* sim, const int* iterations, int n);
+
 /* Compiles CUDA C emitted by the rule translator with NVRTC for sm_100a
  * (replaces WGSLCompiler.compile + create_shader_module,
  * framework/src/oncolytica/gpu/compiler/_compiler.py:233-352).  `kinds[i]` is
- * 0 for a cell rule, 1 for a metric rule.  `include_dir` holds
+ * 0 for a cell rule, 1 for a metric rule, 2 for a tissue rule (one thread per
+ * tissue voxel, tissue buffers flipped after it) and 3 for a chemistry rule
+ * (one thread per chemistry voxel, FP32 fields only, every field's buffers
+ * flipped after each iteration).  Per step, tissue rules and then chemistry
+ * rules run after the sort (their .cells loops see the sorted agents) and
+ * before the cell rules.  `include_dir` holds
  * olc_device.cuh and olc_rule_rt.cuh. */
 int olc_set_rule_source(OlcSim* sim, const char* cuda_src, const char* const* kernels,
                         const int* kinds, int n, const char* include_dir);

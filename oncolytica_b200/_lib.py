@@ -48,7 +48,7 @@ EXPORTS = (
     "olc_pool_copy_results", "olc_pool_retire", "olc_pool_usage",
     "olc_arena_create", "olc_arena_alloc", "olc_arena_release", "olc_arena_stats", "olc_arena_destroy",
     "olc_engine_metrics", "olc_get_step_state", "olc_set_step_state", "olc_set_mechanics",
-    "olc_stage_contact_mech",
+    "olc_stage_contact_mech", "olc_bind_tissue_pair", "olc_current_tissue", "olc_set_rule_iterations",
 )
 
 
@@ -279,6 +279,9 @@ _SIGS = {
     "olc_engine_metrics": (C.c_int, [_VP, C.POINTER(OlcEngineMetricsSpec), C.POINTER(C.c_double), _VP]),
     "olc_get_step_state": (C.c_int, [_VP, C.POINTER(OlcStepState), _VP]),
     "olc_set_mechanics": (C.c_int, [_VP, C.POINTER(OlcMechanics)]),
+    "olc_bind_tissue_pair": (C.c_int, [_VP, _VP, _VP, C.c_int, C.c_size_t]),
+    "olc_current_tissue": (C.c_int, [_VP, C.POINTER(C.c_int)]),
+    "olc_set_rule_iterations": (C.c_int, [_VP, C.POINTER(C.c_int), C.c_int]),
     "olc_stage_contact_mech": (C.c_int, [_VP, _VP, C.c_uint32, C.POINTER(OlcGeom), C.POINTER(OlcContact),
                                          C.POINTER(OlcMechanics), _VP, _VP, _VP, _VP, C.c_float, _VP, _VP, _VP,
                                          _VP]),

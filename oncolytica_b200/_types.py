@@ -266,6 +266,15 @@ class RuleHooks:
     def sink_at(self, pos: vec3) -> Any:  # pragma: no cover - interface
         raise NotImplementedError
 
+    def voxel_neighbors(self, voxel: Any):  # pragma: no cover - interface
+        raise NotImplementedError
+
+    def voxel_cells(self, voxel: Any):  # pragma: no cover - interface
+        raise NotImplementedError
+
+    def voxel_tissues(self, voxel: Any):  # pragma: no cover - interface
+        raise NotImplementedError
+
 
 _hooks: contextvars.ContextVar[RuleHooks | None] = contextvars.ContextVar("oncolytica_b200_rule_hooks",
                                                                          default=None)
@@ -447,9 +456,34 @@ def _class_dicts(cls: type) -> set[str]:
 class Tissue(BaseData, Generic[S, T, C, A, M, P]):
     """Tissue voxel (reference _types.py:456-483)."""
 
+    @property
+    def neighbors(self):
+        """The 26 Moore-neighbour tissue voxels inside the grid."""
+        return _need_hooks("neighbors").voxel_neighbors(self)
+
+    @property
+    def cells(self):
+        """The agents in this voxel (its bin of the spatial sort)."""
+        return _need_hooks("cells").voxel_cells(self)
+
 
 class Chemistry(BaseData, Generic[S, T, C, A, M, P]):
     """Chemistry voxel (reference _types.py:486-530)."""
+
+    @property
+    def neighbors(self):
+        """The 26 Moore-neighbour chemistry voxels inside the grid."""
+        return _need_hooks("neighbors").voxel_neighbors(self)
+
+    @property
+    def tissues(self):
+        """The 2 x 2 x 2 tissue voxels this chemistry voxel covers."""
+        return _need_hooks("tissues").voxel_tissues(self)
+
+    @property
+    def cells(self):
+        """The agents of those tissue voxels."""
+        return _need_hooks("cells").voxel_cells(self)
 
 
 class Cell(BaseData, Generic[S, T, C, A, M, P]):

@@ -16,6 +16,7 @@ from typing import Any
 import numpy as np
 
 from oncolytica_b200 import _lib
+from oncolytica_b200._errors import CompilationError
 from oncolytica_b200._types import metric_fields
 from oncolytica_b200.compiler.emit_cuda import make_layout, pack_params, translate_model
 from oncolytica_b200.engine import STORAGE_CODES
@@ -182,6 +183,12 @@ class CudaBackend:
             kinds = (C.c_int * len(self.program.kernels))(*[kind for _, kind in self.program.kernels])
             self._check(self.lib.olc_set_rule_source(self.handle, self.program.source.encode(), names, kinds,
                                                      len(self.program.kernels), _lib.CSRC_DIR.encode()))
+            if any(kind >= 2 for _, kind in self.program.kernels):
+                if any(kind == 3 for _, kind in self.program.kernels) and any(
+                        d.storage != "f32" for d in eng._diffusion.values()):
+                    raise CompilationError("chemistry rules need FP32 chemistry fields (setup_diffusion storage='f32')")
+                its = (C.c_int * len(self.program.kernels))(*self.program.iterations)
+                self._check(self.lib.olc_set_rule_iterations(self.handle, its, len(self.program.kernels)))
         self._check(self.lib.olc_set_user_metrics_size(self.handle, 4 * max(1, len(L.metrics))))
         self.upload_params()
         self.sync_to_device()
@@ -337,8 +344,38 @@ class CudaBackend:
         self.torch.cuda.synchronize(self.device)
         self._check(self.lib.olc_set_agent_count(self.handle, n, self._stream()))
 
+    @property
+    def _tissue_rules(self) -> bool:
+        return self.program is not None and any(kind == 2 for _, kind in self.program.kernels)
+
+    def _tissue_keys(self):
+        from oncolytica_b200._geometry import get_tissue_voxel_key, voxel_table_size
+
+        dims = self.engine.tissue_shape
+        ix, iy, iz = np.meshgrid(*(np.arange(d) for d in dims), indexing="ij")
+        keys = np.asarray(get_tissue_voxel_key(ix.ravel(), iy.ravel(), iz.ravel()), dtype=np.int64)
+        return keys, voxel_table_size(dims)
+
+    def _read_tissue(self) -> None:
+        """Tissue rules' results back into the host Tissue grid."""
+        eng = self.engine
+        L = self.layout
+        cur = C.c_int()
+        self._check(self.lib.olc_current_tissue(self.handle, C.byref(cur)))
+        packed = self.tissue_pair[cur.value].cpu().numpy()
+        keys, _ = self._tissue_keys()
+        shape = tuple(eng.tissue_shape)
+        for i, (name, t) in enumerate(L.tissue_fields.items()):
+            col = eng.tissue.column(name)
+            raw = packed[i, keys]
+            if col.dtype == np.float32:
+                col[...] = raw.reshape(shape)
+            else:
+                col[...] = raw.view(np.int32).reshape(shape).astype(col.dtype)
+
     def _upload_tissue(self) -> None:
-        """Tissue grid columns packed by tissue (Morton) key for tissue_at()."""
+        """Tissue grid columns packed by tissue (Morton) key for tissue_at();
+        with tissue rules, two such buffers (the rules write the other one)."""
         eng = self.engine
         L = self.layout
         if eng.tissue is None or not L.tissue_fields:
@@ -357,6 +394,12 @@ class CudaBackend:
             else:
                 packed[i].view(np.int32)[keys] = col.astype(np.int32).ravel(order="C")
         self.tissue_dev = self.torch.from_numpy(packed).to(self.device)
+        if self._tissue_rules:
+            self.tissue_pair = (self.tissue_dev, self.tissue_dev.clone())
+            self._check(self.lib.olc_bind_tissue_pair(self.handle, C.c_void_p(self.tissue_pair[0].data_ptr()),
+                                                      C.c_void_p(self.tissue_pair[1].data_ptr()),
+                                                      len(L.tissue_fields), v * 4))
+            return
         self._check(self.lib.olc_bind_tissue(self.handle, C.c_void_p(self.tissue_dev.data_ptr()),
                                              len(L.tissue_fields), v * 4))
 
@@ -380,6 +423,8 @@ class CudaBackend:
         for i, name in enumerate(L.chem_fields):
             flat = self._field_values(i, fb)
             eng.chemistry.column(name)[...] = flat.reshape(eng.chemistry_shape, order="F")
+        if self._tissue_rules and eng.tissue is not None and L.tissue_fields:
+            self._read_tissue()
 
     def _field_values(self, i: int, fb: int) -> np.ndarray:
         """Field i as float32 on the host; for 16-bit storage the stored value
@@ -415,6 +460,18 @@ class CudaBackend:
             c = self.comp_dev[i]
             if c is not None:
                 out.setdefault("residuals", {})[name] = c.cpu().numpy().copy()
+        if self._tissue_rules and self.engine.tissue is not None and self.layout.tissue_fields:
+            # the tissue grid the rules update, as (X, Y, Z) arrays per field
+            cur = C.c_int()
+            self._check(self.lib.olc_current_tissue(self.handle, C.byref(cur)))
+            packed = self.tissue_pair[cur.value].cpu().numpy()
+            keys, _ = self._tissue_keys()
+            shape = tuple(self.engine.tissue_shape)
+            out["tissue"] = {}
+            for i, (name, t) in enumerate(self.layout.tissue_fields.items()):
+                raw = packed[i, keys]
+                out["tissue"][name] = (raw if self.engine.tissue.column(name).dtype == np.float32
+                                       else raw.view(np.int32)).reshape(shape).copy()
         return out
 
     # ---- checkpoints (no counterpart in the reference, which has no resume) ----
@@ -461,8 +518,13 @@ class CudaBackend:
         ss = _lib.OlcStepState()
         self._check(self.lib.olc_get_step_state(self.handle, C.byref(ss), self._stream()))
         params = self.engine._sim._params
+        tissue = None
+        if self._tissue_rules and getattr(self, "tissue_pair", None) is not None:
+            cur = C.c_int()
+            self._check(self.lib.olc_current_tissue(self.handle, C.byref(cur)))
+            tissue = self.tissue_pair[cur.value].cpu().numpy().copy()  # packed by tissue key
         return {"format": "oncolytica_b200.state/1", "layout": self._layout_signature(), "cols": cols,
-                "fields": fields, "sinks": sinks, "residuals": residuals,
+                "fields": fields, "sinks": sinks, "residuals": residuals, "tissue": tissue,
                 "step_state": {"steps": int(ss.steps), "agent_steps": int(ss.agent_steps),
                                "field_step": int(ss.field_step), "status": int(ss.status)},
                 "engine_step": int(self.engine._step),
@@ -512,6 +574,10 @@ class CudaBackend:
             if c is not None:
                 v = sd["residuals"].get(name)
                 c.copy_(torch.from_numpy(np.ascontiguousarray(v, dtype=np.float32))) if v is not None else c.zero_()
+        if sd.get("tissue") is not None and getattr(self, "tissue_pair", None) is not None:
+            cur = C.c_int()
+            self._check(self.lib.olc_current_tissue(self.handle, C.byref(cur)))
+            self.tissue_pair[cur.value].copy_(torch.from_numpy(np.ascontiguousarray(sd["tissue"])))
         torch.cuda.synchronize(self.device)
         self._check(self.lib.olc_set_agent_count(self.handle, n, self._stream()))
         ss = _lib.OlcStepState()

@@ -197,6 +197,8 @@ def export_bundle(engine: Any, directory: str, exact: bool = True) -> str:
         fh.write(_pack_records(chem_layout, chem_stride, nvox, chem_cols, nvox))
     files["Chem_In"] = "chem_in.bin"
     tissue_fields = T.data_fields(L.tissue_class)
+    if engine.tissue is not None and tissue_fields and be._tissue_rules:
+        be._read_tissue()  # the host grid follows the device's tissue rules
     if engine.tissue is not None and tissue_fields:
         tshape = tuple(int(v) for v in engine.tissue_shape)
         tcols = {k: np.asarray(engine.tissue.column(k)).ravel(order="C") for k in tissue_fields}
@@ -218,6 +220,8 @@ def export_bundle(engine: Any, directory: str, exact: bool = True) -> str:
             for k, v in sd[group].items():
                 if v is not None:
                     flat[f"{group}/{k}"] = v
+        if sd.get("tissue") is not None:
+            flat["tissue"] = sd["tissue"]
         np.savez(os.path.join(directory, "resume.npz"), **flat)
         files["resume"] = "resume.npz"
 
@@ -284,6 +288,7 @@ def import_bundle(engine: Any, directory: str) -> None:
         sd["cols"] = {k[4:]: z[k] for k in z.files if k.startswith("col/")}
         for group in ("fields", "sinks", "residuals"):
             sd[group] = {f: (z[f"{group}/{f}"] if f"{group}/{f}" in z.files else None) for f in be.layout.chem_fields}
+        sd["tissue"] = z["tissue"] if "tissue" in z.files else None
         sd["params"] = _params_from_json(engine, config.get("params", {}))
         be.load_state_dict(sd)
         return

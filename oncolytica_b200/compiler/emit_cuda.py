@@ -155,10 +155,11 @@ class ModelLayout:
 @dataclass
 class Program:
     source: str
-    kernels: list                   # (name, kind) kind 0 = cell rule, 1 = metric rule
+    kernels: list                   # (name, kind): 0 cell rule, 1 metric rule, 2 tissue rule, 3 chemistry rule
     layout: ModelLayout
     sink_fields: set = field(default_factory=set)
     digest: str = ""
+    iterations: list = field(default_factory=list)  # per kernel (chemistry rules' iterations, else 1)
 
 
 def make_layout(spec, radius_field: str | None = None, batched: bool = False) -> ModelLayout:
@@ -386,7 +387,23 @@ class Translator:
             info.metrics_name = args[2].arg
             metric_infos.append(info)
 
-        for info in rule_infos + metric_infos:
+        voxel_infos = []  # (info, kind, iterations)
+        eng = self.sim._engine
+        for kind, rules in (("Tissue", list(getattr(eng, "_tissue_rules", []))),
+                            ("Chemistry", list(getattr(eng, "_chemistry_rules", [])))):
+            for i, rule in enumerate(rules):
+                node, src, filename, line0 = func_ast(rule)
+                args = node.args.args
+                if len(args) != 2:
+                    raise CompilationError(f"a {kind.lower()} rule takes (self, voxel)", node, src, filename, line0)
+                info = FuncInfo(f"rule_{kind.lower()}_{i}", rule, "rule", [[args[1].arg, ("struct", kind), True]],
+                                None, node, src, filename, line0)
+                info.self_by_ref = False
+                info.voxel_rule = True
+                iters = int(getattr(rule, "_iterations", 1)) if kind == "Chemistry" else 1
+                voxel_infos.append((info, kind, iters))
+
+        for info in rule_infos + metric_infos + [v[0] for v in voxel_infos]:
             bodies.append(self.emit_function(info))
         # helpers reachable from rules (emission may discover more)
         helper_bodies = []
@@ -407,6 +424,15 @@ class Translator:
             kname = f"Kernel_MetricRule_{i}"
             kernels.append((kname, 1))
             bodies.append(self.metric_kernel(kname, info.cname))
+        iterations = [1] * len(kernels)
+        counters = {"Tissue": 0, "Chemistry": 0}
+        for info, kind, iters in voxel_infos:
+            i = counters[kind]
+            counters[kind] += 1
+            kname = f"Kernel_{'Tissue' if kind == 'Tissue' else 'Chem'}Rule_{i}"
+            kernels.append((kname, 2 if kind == "Tissue" else 3))
+            iterations.append(iters)
+            bodies.append(self.voxel_kernel(kname, info.cname, kind))
 
         src = "\n".join([
             "// Generated by oncolytica_b200.compiler from the model's Python rules.",
@@ -424,7 +450,7 @@ class Translator:
             "",
         ])
         digest = hashlib.sha256(src.encode()).hexdigest()[:16]
-        return Program(src, kernels, self.L, set(self.sink_fields), digest)
+        return Program(src, kernels, self.L, set(self.sink_fields), digest, iterations)
 
     def emit_constants(self) -> str:
         return "\n".join(f"#define {k} {v}" for k, v in sorted(self.constants.items()))
@@ -435,12 +461,13 @@ class Translator:
         out.append("struct Cell_t {\n" + "".join(f"    {ctype(ty_of_py(t))} {n};\n" for n, t in cf.items()) +
                    "    olc_u32 _rng_state;\n" + ("    olc_u32 _sim;\n" if self.L.batched else "") + "};")
         chem = self.L.chem_fields
+        # voxels carry their grid coordinates (for .neighbors / .cells / .tissues)
         out.append("struct Chem_t {\n" + ("".join(f"    float {n};\n" for n in chem) or "    int _unused;\n") +
-                   "};")
+                   "    int _x, _y, _z;\n};")
         tf = self.L.tissue_fields
         out.append("struct Tissue_t {\n" +
                    ("".join(f"    {ctype(ty_of_py(t))} {n};\n" for n, t in tf.items()) or "    int _unused;\n") +
-                   "};")
+                   "    int _x, _y, _z;\n};")
         for elems in sorted(self.tuples, key=str):
             out.append(f"struct {tuple_struct_name(elems)} {{ " +
                        " ".join(f"{ctype(e)} v{i};" for i, e in enumerate(elems)) + " };")
@@ -489,6 +516,8 @@ class Translator:
                 body.append("    c._rng_state = 0u;")
                 if self.L.batched:
                     body.append("    c._sim = 0u;")
+            else:
+                body.append("    c._x = 0;\n    c._y = 0;\n    c._z = 0;")
             lines.append(f"__device__ __forceinline__ {STRUCT_NAME[kind]} olc_default_{kind.lower()}() {{\n" +
                          "\n".join(body) + "\n    return c;\n}")
             # copy_from keeps the receiver's private state
@@ -500,7 +529,14 @@ class Translator:
                                for i, n in enumerate(L.chem_fields))
         lines.append("__device__ __forceinline__ Chem_t olc_chem_at(const OlcP& P, olc_vec3 p) {\n"
                      "    Chem_t c = olc_default_chemistry();\n    const olc_u32 v = olc_chem_index(P, p);\n" +
-                     chem_reads + "\n    return c;\n}")
+                     chem_reads + "\n    c._x = olc_bin_coord(p.x, P.cvs, P.cdims[0]);\n"
+                     "    c._y = olc_bin_coord(p.y, P.cvs, P.cdims[1]);\n"
+                     "    c._z = olc_bin_coord(p.z, P.cvs, P.cdims[2]);\n    return c;\n}")
+        # chemistry voxel (x, y, z) as rules read it (any storage)
+        lines.append("__device__ __forceinline__ Chem_t olc_chem_voxel(const OlcP& P, int x, int y, int z) {\n"
+                     "    Chem_t c = olc_default_chemistry();\n"
+                     "    const olc_u32 v = ((olc_u32)z * (olc_u32)P.cdims[1] + (olc_u32)y) * (olc_u32)P.cdims[0] + "
+                     "(olc_u32)x;\n" + chem_reads + "\n    c._x = x;\n    c._y = y;\n    c._z = z;\n    return c;\n}")
         tis_reads = []
         for i, (n, t) in enumerate(L.tissue_fields.items()):
             ty = ty_of_py(t)
@@ -512,10 +548,32 @@ class Translator:
                 tis_reads.append(f"    c.{n} = olc_tissue_col<olc_u32>(P, {i}, k);")
             else:
                 tis_reads.append(f"    c.{n} = olc_tissue_col<int>(P, {i}, k);")
-        lines.append("__device__ __forceinline__ Tissue_t olc_tissue_at(const OlcP& P, olc_vec3 p) {\n"
-                     "    Tissue_t c = olc_default_tissue();\n    if (!P.tissue) return c;\n"
-                     "    const olc_u32 k = olc_tissue_index(P, p);\n" + "\n".join(tis_reads) +
+        lines.append("__device__ __forceinline__ Tissue_t olc_tissue_voxel(const OlcP& P, int x, int y, int z) {\n"
+                     "    Tissue_t c = olc_default_tissue();\n    c._x = x;\n    c._y = y;\n    c._z = z;\n"
+                     "    if (!P.tissue) return c;\n"
+                     "    const olc_u32 k = olc_tissue_key(x, y, z);\n" + "\n".join(tis_reads) +
                      "\n    return c;\n}")
+        lines.append("__device__ __forceinline__ Tissue_t olc_tissue_at(const OlcP& P, olc_vec3 p) {\n"
+                     "    const olc_ivec3 t = olc_tissue_coord(P, p);\n"
+                     "    return olc_tissue_voxel(P, t.x, t.y, t.z);\n}")
+        if not L.batched:
+            # voxel-rule stores: the other buffer of the tissue grid / of every field
+            tis_writes = []
+            for i, (n, t) in enumerate(L.tissue_fields.items()):
+                ty = ty_of_py(t)
+                if ty == F32:
+                    tis_writes.append(f"    olc_tissue_col_out<float>(P, {i}, k, c.{n});")
+                elif ty == BOOL:
+                    tis_writes.append(f"    olc_tissue_col_out<int>(P, {i}, k, c.{n} ? 1 : 0);")
+                elif ty == U32:
+                    tis_writes.append(f"    olc_tissue_col_out<olc_u32>(P, {i}, k, c.{n});")
+                else:
+                    tis_writes.append(f"    olc_tissue_col_out<int>(P, {i}, k, c.{n});")
+            lines.append("__device__ __forceinline__ void olc_store_tissue(const OlcP& P, olc_u32 k, "
+                         "const Tissue_t& c) {\n" + "\n".join(tis_writes) + "\n}")
+            chem_writes = "\n".join(f"    olc_field_out(P, {i}, v, c.{n});" for i, n in enumerate(L.chem_fields))
+            lines.append("__device__ __forceinline__ void olc_store_chem(const OlcP& P, olc_u32 v, "
+                         "const Chem_t& c) {\n" + chem_writes + "\n}")
         lines.append("__device__ __forceinline__ olc_vec3 olc_rand_dir3(olc_u32& s) {\n"
                      "    float3 d = olc_rand_dir(s);\n    return olc_v3(d.x, d.y, d.z);\n}")
         lines.append("__device__ __forceinline__ void olc_divide(OlcCtx& ctx, olc_u32 rng, const Cell_t& child) {\n"
@@ -613,6 +671,32 @@ class Translator:
     def child_sim(self) -> str:
         return "\n            ctx.child._sim = c._sim;  // a child belongs to its parent's simulation" \
             if self.L.batched else ""
+
+    def voxel_kernel(self, kname: str, fn: str, kind: str) -> str:
+        """One thread per voxel of the tissue (bin) grid or the chemistry grid:
+        load the voxel from the current buffer, run the rule, store it to the
+        other buffer (the host flips the buffers after the launch)."""
+        if self.L.batched:
+            raise CompilationError("tissue/chemistry rules are not compiled in batched mode")
+        dims = "P.tdims" if kind == "Tissue" else "P.cdims"
+        load = "olc_tissue_voxel(P, x, y, z)" if kind == "Tissue" else "olc_chem_voxel(P, x, y, z)"
+        store = "olc_store_tissue(P, olc_tissue_key(x, y, z), v)" if kind == "Tissue" else "olc_store_chem(P, w, v)"
+        return f"""extern "C" __global__ void __launch_bounds__(OLC_RULE_THREADS) {kname}(OlcRuleParams P) {{
+    const olc_u32 nx = (olc_u32){dims}[0], ny = (olc_u32){dims}[1], nz = (olc_u32){dims}[2];
+    const olc_u32 nv = nx * ny * nz;
+    for (olc_u32 w = blockIdx.x * blockDim.x + threadIdx.x; w < nv; w += gridDim.x * blockDim.x) {{
+        const int x = (int)(w % nx), y = (int)((w / nx) % ny), z = (int)(w / (nx * ny));
+        {STRUCT_NAME[kind]} v = {load};
+        olc_u32 rng = 0u;  // voxels have no RNG state
+        OlcCtx ctx;
+        ctx.i = 0xffffffffu;
+        ctx.dead = false;
+        ctx.born = false;
+        ctx.multi = false;
+        {fn}(P, rng, ctx, v);
+        {store};
+    }}
+}}"""
 
     def metric_kernel(self, kname: str, fn: str) -> str:
         return f"""extern "C" __global__ void __launch_bounds__(OLC_RULE_THREADS) {kname}(OlcRuleParams P) {{
@@ -994,9 +1078,11 @@ class FuncEmitter:
             return
         if isinstance(it, ast.Attribute) and it.attr == "neighbors":
             recv, rt = self.expr(it.value)
+            if rt in (("struct", "Tissue"), ("struct", "Chemistry")):
+                self.voxel_loop(n, "neighbors", recv, rt[1])
+                return
             if rt != ("struct", "Cell"):
-                raise self.err("only cell.neighbors is supported by this backend (tissue/chemistry "
-                               "neighbourhoods are not)", it)
+                raise self.err(".neighbors belongs to cells, tissue voxels and chemistry voxels", it)
             if not isinstance(n.target, ast.Name):
                 raise self.err("loop target must be a name", n.target)
             nb = n.target.id
@@ -1034,10 +1120,92 @@ class FuncEmitter:
             self.indent -= 1
             self.emit(f"}} {lab}:;")
             return
-        if isinstance(it, ast.Attribute) and it.attr in ("cells", "tissues"):
-            raise self.err(f".{it.attr} loops belong to tissue/chemistry rules, which this backend does not "
-                           f"compile", it)
-        raise self.err("for loops iterate over range(...) or cell.neighbors", n)
+        if isinstance(it, ast.Attribute) and it.attr in ("neighbors", "cells", "tissues"):
+            recv, rt = self.expr(it.value)
+            if rt in (("struct", "Tissue"), ("struct", "Chemistry")):
+                self.voxel_loop(n, it.attr, recv, rt[1])
+                return
+            raise self.err(f".{it.attr} loops run over tissue or chemistry voxels (cells: .neighbors only)", it)
+        raise self.err("for loops iterate over range(...), .neighbors, .cells or .tissues", n)
+
+    def tied_geometry(self, node) -> None:
+        """chem.cells / chem.tissues need the reference's tied grids: one
+        chemistry voxel covers 2 x 2 x 2 tissue voxels."""
+        eng = self.tr.sim._engine
+        ts, cs = tuple(eng.tissue_shape), tuple(eng.chemistry_shape)
+        if cs != tuple(t // 2 for t in ts) or abs(eng.chemistry_voxel_size - 2.0 * eng.tissue_voxel_size) > \
+                1e-6 * eng.chemistry_voxel_size:
+            raise self.err("chemistry .cells / .tissues need the chemistry grid tied to the tissue grid "
+                           "(setup_geometry; chemistry voxel = 2 x 2 x 2 tissue voxels)", node)
+
+    def voxel_loop(self, n: ast.For, attr: str, recv: str, kind: str) -> None:
+        """Loops over a voxel's 26 Moore neighbours (same grid, in bounds,
+        MooreOffsets order), its agents (tissue: the bin's rows in sorted
+        order; chemistry: those of its 8 tissue voxels in key order) or, for
+        a chemistry voxel, its 8 tissue voxels.  Loop values are copies of
+        the state before the rule."""
+        if not isinstance(n.target, ast.Name):
+            raise self.err("loop target must be a name", n.target)
+        nb = n.target.id
+        if self.var_type(nb) is not None:
+            raise self.err(f"loop variable {nb!r} shadows a variable", n.target)
+        if attr == "tissues" and kind != "Chemistry":
+            raise self.err(".tissues is a chemistry voxel's loop", n.iter)
+        if attr in ("cells", "tissues") and kind == "Chemistry":
+            self.tied_geometry(n.iter)
+        lab = self.fresh("_vx_done")
+        b, d = self.fresh("_b"), self.fresh("_d")
+        self.emit("{")
+        self.indent += 1
+        self.emit(f"const int {b}x = {recv}._x, {b}y = {recv}._y, {b}z = {recv}._z;")
+        if attr == "neighbors":
+            dims = "P.tdims" if kind == "Tissue" else "P.cdims"
+            self.emit(f"for (int {d}z = -1; {d}z <= 1; ++{d}z)")
+            self.emit(f"for (int {d}y = -1; {d}y <= 1; ++{d}y)")
+            self.emit(f"for (int {d}x = -1; {d}x <= 1; ++{d}x) {{")
+            self.indent += 1
+            self.emit(f"if ({d}x == 0 && {d}y == 0 && {d}z == 0) continue;")
+            self.emit(f"const int {d}nx = {b}x + {d}x, {d}ny = {b}y + {d}y, {d}nz = {b}z + {d}z;")
+            self.emit(f"if ({d}nx < 0 || {d}ny < 0 || {d}nz < 0 || {d}nx >= {dims}[0] || {d}ny >= {dims}[1] "
+                      f"|| {d}nz >= {dims}[2]) continue;")
+            load = "olc_tissue_voxel" if kind == "Tissue" else "olc_chem_voxel"
+            self.emit(f"const {STRUCT_NAME[kind]} {nb} = {load}(P, {d}nx, {d}ny, {d}nz);")
+            self.params[nb] = ("struct", kind)
+            closes = 1
+        else:
+            if kind == "Tissue":
+                self.emit(f"for (int {d}i = 0; {d}i < 1; ++{d}i) {{")
+                self.indent += 1
+                self.emit(f"const int {d}nx = {b}x, {d}ny = {b}y, {d}nz = {b}z;")
+            else:
+                self.emit(f"for (int {d}i = 0; {d}i < 8; ++{d}i) {{")
+                self.indent += 1
+                self.emit(f"const int {d}nx = 2 * {b}x + ({d}i & 1), {d}ny = 2 * {b}y + (({d}i >> 1) & 1), "
+                          f"{d}nz = 2 * {b}z + (({d}i >> 2) & 1);")
+                self.emit(f"if ({d}nx >= P.tdims[0] || {d}ny >= P.tdims[1] || {d}nz >= P.tdims[2]) continue;")
+            if attr == "tissues":
+                self.emit(f"const Tissue_t {nb} = olc_tissue_voxel(P, {d}nx, {d}ny, {d}nz);")
+                self.params[nb] = ("struct", "Tissue")
+                closes = 1
+            else:
+                k, j, s0, e0 = self.fresh("_k"), self.fresh("_j"), self.fresh("_s"), self.fresh("_e")
+                self.emit(f"const olc_u32 {k} = olc_tissue_key({d}nx, {d}ny, {d}nz);")
+                self.emit(f"const olc_u32 {s0} = P.ranges[2u * {k}], {e0} = P.ranges[2u * {k} + 1u];")
+                self.emit(f"for (olc_u32 {j} = {s0}; {j} < {e0}; ++{j}) {{")
+                self.indent += 1
+                self.emit(f"const Cell_t {nb} = olc_load_cell(P, {j});")
+                self.params[nb] = ("struct", "Cell")
+                closes = 2
+        self.loop_labels.append(lab)
+        for st in n.body:
+            self.stmt(st)
+        self.loop_labels.pop()
+        del self.params[nb]
+        for _ in range(closes):
+            self.indent -= 1
+            self.emit("}")
+        self.indent -= 1
+        self.emit(f"}} {lab}:;")
 
     # ---- expressions -------------------------------------------------------
     def cond(self, node) -> str:
@@ -1307,6 +1475,9 @@ class FuncEmitter:
 
     def call_static(self, g, n: ast.Call):
         args = [self.expr(a) for a in n.args]
+        if (g is T.random or g is _pkg.random or g is T.random_dir or g is _pkg.random_dir) and \
+                getattr(self.info, "voxel_rule", False):
+            raise self.err("tissue and chemistry voxels have no RNG state; random() is for cell rules", n)
         if g is T.random or g is _pkg.random:
             return "olc_next_rand(_rng)", F32
         if g is T.random_dir or g is _pkg.random_dir:

@@ -91,6 +91,11 @@ struct OlcRuleParams {
     int n_fields;
     int sim_col;
     int field_type[OLC_MAX_FIELD_COLS];  // OLC_FIELD_* storage: 0 FP32, 1 BF16, 2 FP16, 3 BF16 (stochastic)
+    // tissue / chemistry rules: the buffers a voxel rule writes; it reads
+    // `tissue` and `field` (the state before the rule: every voxel sees its
+    // neighbours' previous values)
+    unsigned char* tissue_out;
+    void* field_out[OLC_MAX_FIELD_COLS];
 };
 
 // What a rule body sees of one simulation of a batch (batched mode).  Member
@@ -317,6 +322,17 @@ __device__ __forceinline__ void olc_col_out(const PT& P, int col, olc_u32 i, T v
 template <typename T, class PT>
 __device__ __forceinline__ T olc_tissue_col(const PT& P, int col, olc_u32 key) {
     return reinterpret_cast<const T*>(P.tissue + (size_t)col * P.tissue_stride)[key];
+}
+template <typename T>
+__device__ __forceinline__ void olc_tissue_col_out(const OlcRuleParams& P, int col, olc_u32 key, T v) {
+    reinterpret_cast<T*>(P.tissue_out + (size_t)col * P.tissue_stride)[key] = v;
+}
+// Chemistry rules: FP32 fields only (the host checks the storage).
+__device__ __forceinline__ float olc_field_in(const OlcRuleParams& P, int f, olc_u32 v) {
+    return static_cast<const float*>(P.field[f])[v];
+}
+__device__ __forceinline__ void olc_field_out(const OlcRuleParams& P, int f, olc_u32 v, float x) {
+    static_cast<float*>(P.field_out[f])[v] = x;
 }
 
 // Metric accumulators: one 4-byte word per metric field.  Integer adds are

@@ -44,9 +44,10 @@ using namespace olc;
 #define OLC_PROF_EVENTS 7
 
 struct StepGraph {
-    int key = 0;  // (agent buffer << 16) | (field parity mask << 1) | collect
+    int key = 0;  // (agent buffer << 16) | (tissue buffer << 12) | (field parity mask << 1) | collect
     int agent_after = 0;
     int field_after = 0;
+    int tissue_after = 0;
     uint64_t launches = 0;
     cudaGraphExec_t exec = nullptr;
 };
@@ -75,7 +76,9 @@ struct OlcSim {
     ContactDev contact_dev = {};
     OlcMechanics mech = {};  // engine force-law extras (mech.enabled)
 
-    const unsigned char* tissue = nullptr;  // borrowed tissue columns (Morton-indexed)
+    const unsigned char* tissue = nullptr;  // borrowed tissue columns (Morton-indexed), the current buffer
+    unsigned char* tissue_buf[2] = {};      // tissue rules: both buffers (olc_bind_tissue_pair)
+    int tissue_cur = 0;
     int tissue_cols = 0;
     size_t tissue_stride = 0;
 
@@ -107,6 +110,7 @@ struct OlcSim {
     cudaLibrary_t module = nullptr;
     std::vector<cudaKernel_t> funcs;
     std::vector<int> kinds;
+    std::vector<int> iters;  // per kernel: chemistry-rule iterations (1 otherwise)
     int n_cell_rules = 0;
 
     uint64_t steps = 0;
@@ -269,11 +273,12 @@ OlcRuleParams make_rule_params(OlcSim* s, int rule_index, int in_buf) {
     return P;
 }
 
-int launch_rule(OlcSim* s, int k, const OlcRuleParams& P, cudaStream_t st) {
+int launch_rule(OlcSim* s, int k, const OlcRuleParams& P, cudaStream_t st, olc_u32 units = 0) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    olc_u32 blocks = (s->caps.max_agents + OLC_RULE_THREADS - 1) / OLC_RULE_THREADS;
+    if (units == 0) units = s->caps.max_agents;
+    olc_u32 blocks = (units + OLC_RULE_THREADS - 1) / OLC_RULE_THREADS;
     if (blocks == 0) blocks = 1;
     const olc_u32 cap_blocks = (olc_u32)sms * 8u;
     if (blocks > cap_blocks) blocks = cap_blocks;
@@ -362,6 +367,35 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
     launch_permute(s->vals, s->counters, cap, pa, st);
     s->agent_cur = 1 - ac;
     launches += 4 + (uint64_t)passes;  // keys, scan, passes, bin table, permute
+    // 3a. tissue rules, then chemistry rules (one thread per voxel; each reads
+    // the state before it and writes the other buffer)
+    for (size_t k = 0; k < s->funcs.size(); ++k) {
+        if (s->kinds[k] != 2) continue;
+        if (!s->tissue_buf[0] || !s->tissue_buf[1])
+            return fail(s, OLC_ERR_STATE, "tissue rule: bind the tissue grid with olc_bind_tissue_pair");
+        OlcRuleParams P = make_rule_params(s, 0, s->agent_cur);
+        P.tissue = s->tissue_buf[s->tissue_cur];
+        P.tissue_out = s->tissue_buf[1 - s->tissue_cur];
+        const olc_u32 nv = (olc_u32)s->geom.tissue_dims[0] * s->geom.tissue_dims[1] * s->geom.tissue_dims[2];
+        OLC_TRY(launch_rule(s, (int)k, P, st, nv));
+        s->tissue_cur = 1 - s->tissue_cur;
+        s->tissue = s->tissue_buf[s->tissue_cur];
+        ++launches;
+    }
+    for (size_t k = 0; k < s->funcs.size(); ++k) {
+        if (s->kinds[k] != 3) continue;
+        for (olc_u32 f = 0; f < s->caps.n_fields; ++f)
+            if (!s->field_bound[f] || s->fstep[f].storage != OLC_FIELD_F32)
+                return fail(s, OLC_ERR_STATE, "chemistry rule: every chemistry field must be bound with FP32 storage");
+        const olc_u32 nv = (olc_u32)s->geom.chem_dims[0] * s->geom.chem_dims[1] * s->geom.chem_dims[2];
+        for (int it = 0; it < s->iters[k]; ++it) {
+            OlcRuleParams P = make_rule_params(s, 0, s->agent_cur);
+            for (olc_u32 f = 0; f < s->caps.n_fields; ++f) P.field_out[f] = s->field[1 - s->field_cur[f]][f];
+            OLC_TRY(launch_rule(s, (int)k, P, st, nv));
+            for (olc_u32 f = 0; f < s->caps.n_fields; ++f) s->field_cur[f] = 1 - s->field_cur[f];
+            ++launches;
+        }
+    }
     mark(s, 3, st);
     // 3. cell rules
     if (s->n_cell_rules > 0) {
@@ -657,8 +691,8 @@ void drop_graphs_nosync(OlcSim* s) {
 // second captures it.  Capture runs on the handle's own stream (the legacy
 // default stream cannot be captured); the graph is launched on the caller's.
 int step_graph(OlcSim* s, int collect, cudaStream_t st) {
-    const int ac = s->agent_cur, fm = field_mask(s);
-    const int key = (ac << 16) | (fm << 1) | collect;
+    const int ac = s->agent_cur, fm = field_mask(s), tc = s->tissue_cur;
+    const int key = (ac << 16) | (tc << 12) | (fm << 1) | collect;
     StepGraph* g = nullptr;
     for (auto& e : s->graphs)
         if (e.key == key) g = &e;
@@ -680,12 +714,15 @@ int step_graph(OlcSim* s, int collect, cudaStream_t st) {
         ng.key = key;
         ng.agent_after = s->agent_cur;
         ng.field_after = field_mask(s);
+        ng.tissue_after = s->tissue_cur;
         ng.launches = s->total_launches - launches0;
         // nothing ran yet: restore the state the graph starts from
         s->steps = steps0;
         s->total_launches = launches0;
         s->agent_cur = ac;
         set_field_mask(s, fm);
+        s->tissue_cur = tc;
+        if (s->tissue_buf[tc]) s->tissue = s->tissue_buf[tc];
         if (rc != OLC_OK || e != cudaSuccess) {
             if (graph) cudaGraphDestroy(graph);
             cudaGetLastError();
@@ -700,6 +737,8 @@ int step_graph(OlcSim* s, int collect, cudaStream_t st) {
     OLC_TRY(check(s, cudaGraphLaunch(g->exec, st), "graph launch"));
     s->agent_cur = g->agent_after;
     set_field_mask(s, g->field_after);
+    s->tissue_cur = g->tissue_after;
+    if (s->tissue_buf[s->tissue_cur]) s->tissue = s->tissue_buf[s->tissue_cur];
     s->total_launches += g->launches;
     s->steps++;
     return OLC_OK;
@@ -1172,8 +1211,41 @@ int olc_bind_tissue(OlcSim* s, const void* cols, int n_cols, size_t stride_bytes
     if (s->n_sims && n_cols > 0) return fail(s, OLC_ERR_STATE, "olc_bind_tissue: tissue grids are not bound in batched mode");
     drop_graphs(s);
     s->tissue = static_cast<const unsigned char*>(cols);
+    s->tissue_buf[0] = s->tissue_buf[1] = nullptr;
+    s->tissue_cur = 0;
     s->tissue_cols = n_cols;
     s->tissue_stride = stride_bytes;
+    return OLC_OK;
+}
+
+int olc_bind_tissue_pair(OlcSim* s, void* a, void* b, int n_cols, size_t stride_bytes) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (n_cols <= 0 || !a || !b || stride_bytes < (size_t)s->n_table * 4)
+        return fail(s, OLC_ERR_ARG, "olc_bind_tissue_pair: two buffers of columns with voxel_table_size entries");
+    if (s->n_sims) return fail(s, OLC_ERR_STATE, "olc_bind_tissue_pair: tissue grids are not bound in batched mode");
+    drop_graphs(s);
+    s->tissue_buf[0] = static_cast<unsigned char*>(a);
+    s->tissue_buf[1] = static_cast<unsigned char*>(b);
+    s->tissue_cur = 0;
+    s->tissue = s->tissue_buf[0];
+    s->tissue_cols = n_cols;
+    s->tissue_stride = stride_bytes;
+    return OLC_OK;
+}
+
+int olc_current_tissue(const OlcSim* s, int* tissue_buf) {
+    if (!s || !tissue_buf) return fail(nullptr, OLC_ERR_ARG, "olc_current_tissue: null argument");
+    *tissue_buf = s->tissue_cur;
+    return OLC_OK;
+}
+
+int olc_set_rule_iterations(OlcSim* s, const int* iters, int n) {
+    if (!s || (n > 0 && !iters)) return fail(s, OLC_ERR_ARG, "olc_set_rule_iterations: null argument");
+    if (n != (int)s->funcs.size()) return fail(s, OLC_ERR_ARG, "olc_set_rule_iterations: one count per kernel");
+    for (int i = 0; i < n; ++i)
+        if (iters[i] < 0) return fail(s, OLC_ERR_ARG, "olc_set_rule_iterations: negative count");
+    drop_graphs(s);
+    s->iters.assign(iters, iters + n);
     return OLC_OK;
 }
 
@@ -1274,7 +1346,9 @@ int olc_set_rule_source(OlcSim* s, const char* src, const char* const* kernels, 
         return fail(s, OLC_ERR_ARG, "olc_set_rule_source: bad arguments");
     int ncell = 0;
     for (int i = 0; i < n; ++i) {
-        if (kinds[i] != 0 && kinds[i] != 1) return fail(s, OLC_ERR_ARG, "olc_set_rule_source: kind must be 0 or 1");
+        if (kinds[i] < 0 || kinds[i] > 3) return fail(s, OLC_ERR_ARG, "olc_set_rule_source: kind must be 0..3");
+        if (kinds[i] >= 2 && s->n_sims)
+            return fail(s, OLC_ERR_STATE, "olc_set_rule_source: tissue/chemistry rules need a solo handle");
         ncell += kinds[i] == 0;
     }
     OLC_TRY(ensure_context(s));
@@ -1305,6 +1379,7 @@ int olc_set_rule_source(OlcSim* s, const char* src, const char* const* kernels, 
     }
     s->funcs.clear();
     s->kinds.clear();
+    s->iters.clear();
     OLC_TRY(check(s, cudaLibraryLoadData(&s->module, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0),
                   "cudaLibraryLoadData"));
     for (int i = 0; i < n; ++i) {
@@ -1312,6 +1387,7 @@ int olc_set_rule_source(OlcSim* s, const char* src, const char* const* kernels, 
         OLC_TRY(check(s, cudaLibraryGetKernel(&fn, s->module, kernels[i]), kernels[i]));
         s->funcs.push_back(fn);
         s->kinds.push_back(kinds[i]);
+        s->iters.push_back(1);
     }
     s->n_cell_rules = ncell;
     return OLC_OK;

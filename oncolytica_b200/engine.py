@@ -248,11 +248,6 @@ class Engine:
             kind = getattr(method, "_rule_type", None)
             {"tissue": self._tissue_rules, "chemistry": self._chemistry_rules, "cell": self._cell_rules,
              "metric": self._metric_rules}.get(kind, []).append(method)
-        if self._tissue_rules or self._chemistry_rules:
-            names = [m.__name__ for m in self._tissue_rules + self._chemistry_rules]
-            raise CompilationError(
-                f"tissue/chemistry rules {names} are not compiled by this backend; declare diffusing chemistry "
-                f"fields with Engine.setup_diffusion (built-in 7-point stencil) instead")
         if self.tissue is None and self._tissue_class is None:
             self._tissue_class = sim_instance._spec.tissue_class
         if self.chemistry is None:

@@ -13,7 +13,13 @@ semantics the CUDA kernels implement, restated from the reference:
   * divide() appends one child in parent order (:442-453);
   * neighbors: 27 bins in MooreOffsets order (template.wgsl:11-21), bins
     outside the grid skipped, self skipped (_stmt_translator.py:459-491);
-  * chemistry_at / tissue_at: clamped nearest voxel (_types.py:314-346).
+  * chemistry_at / tissue_at: clamped nearest voxel (_types.py:314-346);
+  * tissue and chemistry rules (_stmt_translator.py:493-605, with the
+    reference's undefined symbols resolved): one call per voxel, reading the
+    state before the rule (Tissue_In / Chem_In) and writing a new grid;
+    .neighbors are the 26 in-grid Moore voxels in MooreOffsets order,
+    tissue .cells the voxel's bin in sorted order, chemistry .cells and
+    .tissues its 2 x 2 x 2 tissue voxels in tissue-key order.
 Arithmetic is float32 (numpy scalars), matching the kernels' separately
 rounded operations except for library functions (cos, sin, log, ...).
 Suitable for small cases only (a Python call per agent).
@@ -84,7 +90,9 @@ class Interpreter(T.RuleHooks):
         self.life = np.array(snap["life"][: self.rows], dtype=np.uint8)
         self.fields = {k: np.array(v, dtype=np.float32) for k, v in snap["fields"].items()}
         self.sinks = {k: (np.array(v, dtype=np.float32) if v is not None else None) for k, v in snap["sinks"].items()}
-        self.tissue = engine_cfg.get("tissue_cols")
+        self.tissue = snap.get("tissue") or engine_cfg.get("tissue_cols")  # the device's, when rules update it
+        if self.tissue is not None:
+            self.tissue = {k: np.array(v) for k, v in self.tissue.items()}
 
     # ---- hooks -----------------------------------------------------------
     def random(self) -> np.float32:
@@ -135,24 +143,111 @@ class Interpreter(T.RuleHooks):
         return (cz * cd[1] + cy) * cd[0] + cx
 
     def chemistry_at(self, pos):
-        c = self.spec.chemistry_class()
-        v = self._chem_index(pos)
-        for name in self.fields:
-            setattr(c, name, self.fields[name][v])
-        return c
+        cd, vs = self.cfg["chem_dims"], self.cfg["chem_voxel_size"]
+        return self._chem_voxel(*(_bin_coord(getattr(pos, a), vs, cd[k]) for k, a in enumerate("xyz")))
 
     def tissue_at(self, pos):
-        t = self.spec.tissue_class()
-        if self.tissue is None:
-            return t
         td, vs = self.cfg["tissue_dims"], self.cfg["tissue_voxel_size"]
-        x, y, z = (_bin_coord(getattr(pos, a), vs, td[k]) for k, a in enumerate("xyz"))
-        for name, arr in self.tissue.items():
-            setattr(t, name, arr[x, y, z])
-        return t
+        return self._tissue_voxel(*(_bin_coord(getattr(pos, a), vs, td[k]) for k, a in enumerate("xyz")))
 
     def sink_at(self, pos):
         return _Sink(self, self._chem_index(pos))
+
+    # ---- voxels (tissue / chemistry rules) -------------------------------
+    def _tissue_voxel(self, x: int, y: int, z: int):
+        t = self.spec.tissue_class()
+        if self.tissue is not None:
+            for name, arr in self.tissue.items():
+                v = arr[x, y, z]
+                ft = T.data_fields(self.spec.tissue_class).get(name)
+                setattr(t, name, F(v) if ft in T._FLOAT_TYPES else (bool(v) if ft is bool else int(v)))
+        object.__setattr__(t, "_vox", (x, y, z))
+        return t
+
+    def _chem_voxel(self, x: int, y: int, z: int):
+        cd = self.cfg["chem_dims"]
+        c = self.spec.chemistry_class()
+        v = (z * cd[1] + y) * cd[0] + x
+        for name in self.fields:
+            setattr(c, name, self.fields[name][v])
+        object.__setattr__(c, "_vox", (x, y, z))
+        return c
+
+    def _sub_tissue(self, chem):
+        x, y, z = chem._vox
+        td = self.cfg["tissue_dims"]
+        for i in range(8):
+            tx, ty, tz = 2 * x + (i & 1), 2 * y + ((i >> 1) & 1), 2 * z + ((i >> 2) & 1)
+            if tx < td[0] and ty < td[1] and tz < td[2]:
+                yield tx, ty, tz
+
+    def _bin_rows(self, x, y, z):
+        k = oracle.tissue_key(x, y, z)
+        s, e = int(self.ranges[2 * k]), int(self.ranges[2 * k + 1])
+        for j in range(s, e):
+            yield self._load(self.data, j)
+
+    def voxel_neighbors(self, voxel):
+        tissue = isinstance(voxel, T.Tissue)
+        dims = self.cfg["tissue_dims"] if tissue else self.cfg["chem_dims"]
+        x, y, z = voxel._vox
+        for dz in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    if dx == 0 and dy == 0 and dz == 0:
+                        continue
+                    nx, ny, nz = x + dx, y + dy, z + dz
+                    if not (0 <= nx < dims[0] and 0 <= ny < dims[1] and 0 <= nz < dims[2]):
+                        continue
+                    yield self._tissue_voxel(nx, ny, nz) if tissue else self._chem_voxel(nx, ny, nz)
+
+    def voxel_cells(self, voxel):
+        if isinstance(voxel, T.Tissue):
+            yield from self._bin_rows(*voxel._vox)
+            return
+        for tx, ty, tz in self._sub_tissue(voxel):
+            yield from self._bin_rows(tx, ty, tz)
+
+    def voxel_tissues(self, chem):
+        for tx, ty, tz in self._sub_tissue(chem):
+            yield self._tissue_voxel(tx, ty, tz)
+
+    def run_tissue_rules(self, rules) -> None:
+        td = self.cfg["tissue_dims"]
+        names = list(T.data_fields(self.spec.tissue_class))
+        for rule in rules:
+            out = {k: v.copy() for k, v in self.tissue.items()}
+            for z in range(td[2]):
+                for y in range(td[1]):
+                    for x in range(td[0]):
+                        t = self._tissue_voxel(x, y, z)
+                        tok = T.install_rule_hooks(self)
+                        try:
+                            rule(t)
+                        finally:
+                            T.reset_rule_hooks(tok)
+                        for name in names:
+                            out[name][x, y, z] = getattr(t, name)
+            self.tissue = out
+
+    def run_chemistry_rules(self, rules) -> None:
+        cd = self.cfg["chem_dims"]
+        for rule in rules:
+            for _ in range(int(getattr(rule, "_iterations", 1))):
+                out = {k: v.copy() for k, v in self.fields.items()}
+                for z in range(cd[2]):
+                    for y in range(cd[1]):
+                        for x in range(cd[0]):
+                            c = self._chem_voxel(x, y, z)
+                            tok = T.install_rule_hooks(self)
+                            try:
+                                rule(c)
+                            finally:
+                                T.reset_rule_hooks(tok)
+                            v = (z * cd[1] + y) * cd[0] + x
+                            for name in out:
+                                out[name][v] = F(getattr(c, name))
+                self.fields = out
 
     # ---- state -----------------------------------------------------------
     def _load(self, src: dict, i: int):
@@ -265,6 +360,7 @@ class Interpreter(T.RuleHooks):
     def snapshot(self) -> dict:
         return {"rows": self.rows, "life": self.life.copy(), "cols": {k: v.copy() for k, v in self.data.items()},
                 "fields": {k: v.copy() for k, v in self.fields.items()},
+                "tissue": {k: v.copy() for k, v in self.tissue.items()} if self.tissue is not None else None,
                 "sinks": {k: (v.copy() if v is not None else None) for k, v in self.sinks.items()}}
 
 
@@ -285,6 +381,10 @@ def step(interp: Interpreter, engine, collect: bool = False) -> dict:
         interp.diffuse(name, {"diffusion": d.diffusion, "decay": d.decay, "boundary": d.boundary,
                               "substeps": engine.substeps_for(name)})
     interp.sort()
+    if engine._tissue_rules:
+        interp.run_tissue_rules(engine._tissue_rules)
+    if engine._chemistry_rules:
+        interp.run_chemistry_rules(engine._chemistry_rules)
     out = interp.run_cell_rules(engine._cell_rules)
     if collect:
         out["metrics"] = interp.run_metric_rules(engine._metric_rules, engine._sim._spec.metrics_class)

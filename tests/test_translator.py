@@ -207,3 +207,55 @@ def test_batched_translation_compiles():
         assert "typedef OlcSimView OlcP;" in prog.source
         assert "olc_sim_view(P, sim)" in prog.source
         _nvrtc_ok(prog)
+
+
+# ---- tissue and chemistry rules ---------------------------------------------
+
+def _translate_all(sim_cls, tissue_shape=(12, 12, 12), vs=10.0, chem_shape=None, chem_vs=None):
+    sim = sim_cls()
+    rules = {"cell": [], "metric": [], "tissue": [], "chemistry": []}
+    for name in dir(sim):
+        m = getattr(sim, name, None)
+        kind = getattr(m, "_rule_type", None)
+        if kind in rules:
+            rules[kind].append(m)
+    sim._engine = SimpleNamespace(_cell_rules=rules["cell"], _metric_rules=rules["metric"],
+                                  _tissue_rules=rules["tissue"], _chemistry_rules=rules["chemistry"],
+                                  tissue_shape=tissue_shape, tissue_voxel_size=vs,
+                                  chemistry_shape=chem_shape or tuple(t // 2 for t in tissue_shape),
+                                  chemistry_voxel_size=chem_vs or 2.0 * vs)
+    return translate_model(sim, make_layout(sim._spec, None), None)
+
+
+def test_voxel_rules_compile():
+    import voxel_model as VM
+
+    prog = _translate_all(VM.VoxelSim)
+    kinds = dict(prog.kernels)
+    assert kinds["Kernel_TissueRule_0"] == 2 and kinds["Kernel_ChemRule_0"] == 3
+    assert prog.iterations[[k for k, _ in prog.kernels].index("Kernel_ChemRule_0")] == 2
+    src = prog.source
+    assert "olc_store_tissue" in src and "olc_store_chem" in src and "olc_chem_voxel" in src
+    _nvrtc_ok(prog)
+
+
+def test_chemistry_cells_need_the_tied_grids():
+    import voxel_model as VM
+
+    with pytest.raises(ol.CompilationError, match="tied"):
+        _translate_all(VM.VoxelSim, chem_shape=(8, 8, 8), chem_vs=15.0)
+
+
+class RTissue(ol.Tissue):
+    a: ol.f32 = 0.0
+
+
+class RandSim(ol.Simulation[RTissue, GChem, GCell, GMetrics, GParams]):
+    @ol.tissue_rule
+    def noisy(self, t: RTissue):
+        t.a = ol.random()
+
+
+def test_voxel_rules_have_no_rng():
+    with pytest.raises(ol.CompilationError, match="no RNG state"):
+        _translate_all(RandSim, tissue_shape=(20, 20, 20), vs=2.0)
