@@ -57,6 +57,9 @@ class CudaBackend:
         self.program = None
         self.cols_dev: list[tuple[Any, Any]] = []
         self.fields_dev: list[tuple[Any, Any, Any]] = []
+        self.comp_dev: list[Any] = []
+        self.tissue_dev = None
+        self.tissue_pair = None
         self._params_dirty = True
         self._last_reductions: dict | None = None
 
@@ -598,9 +601,13 @@ class CudaBackend:
         return self.cols_dev[self.layout.col_index(col)][ab]
 
     def close(self) -> None:
+        """Destroys the library handle and drops the device tensors (their
+        memory returns to torch's allocator)."""
         if self.handle:
             self.lib.olc_destroy(self.handle)
             self.handle = C.c_void_p()
+        self.cols_dev, self.fields_dev, self.comp_dev = [], [], []
+        self.tissue_dev = self.tissue_pair = None
 
     def __del__(self) -> None:
         try:

@@ -289,6 +289,14 @@ class Engine:
             raise RuntimeError("Engine.get_engine_metrics() called before load_model().")
         return self._backend_impl.engine_metrics(**kw)
 
+    def close(self) -> None:
+        """Releases the device state now (the engine, its model instance and its
+        backend refer to each other, so without this the memory is freed only
+        when Python's cycle collector runs)."""
+        if self._backend_impl is not None:
+            self._backend_impl.close()
+            self._backend_impl = None
+
     # ---- checkpoints ----------------------------------------------------------
     def state_dict(self) -> dict:
         """The device state as host arrays (CudaBackend.state_dict); resuming
