@@ -253,14 +253,27 @@ __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __res
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
         int b = 0;
         olc_u32 j = 0, end = 0;
+        float4 q = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
         if (nb > 0) {
             const uint2 r = s_bins[0][t];
             j = r.x;
             end = r.y;
+            q = __ldg(posr + j);
         }
         while (b < nb) {
+            // the next candidate's record is requested before this one is used,
+            // so two loads are in flight per thread
+            olc_u32 jn = j + 1, en = end;
+            int bn = b;
+            if (jn == en) {
+                if (++bn < nb) {
+                    const uint2 r = s_bins[bn][t];
+                    jn = r.x;
+                    en = r.y;
+                }
+            }
+            const float4 qn = bn < nb ? __ldg(posr + jn) : q;
             if (j != i) {
-                const float4 q = __ldg(posr + j);
                 if (!(q.w < 0.0f)) {
                     const float ddx = __fsub_rn(p.x, q.x);
                     const float ddy = __fsub_rn(p.y, q.y);
@@ -285,13 +298,10 @@ __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __res
                     }
                 }
             }
-            if (++j == end) {
-                if (++b < nb) {
-                    const uint2 r = s_bins[b][t];
-                    j = r.x;
-                    end = r.y;
-                }
-            }
+            j = jn;
+            end = en;
+            b = bn;
+            q = qn;
         }
         float mx = __fmul_rn(fx, md), my = __fmul_rn(fy, md), mz = __fmul_rn(fz, md);
         const float len = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz)));
@@ -319,9 +329,24 @@ static bool contact_flat() {
     return v == 1;
 }
 
+// OLC_CONTACT_CARVEOUT=<percent> sets the shared-memory carveout preference of
+// k_contact_flat (its bin lists take shared memory that neighbour loads would
+// otherwise find in L1); unset leaves the driver's choice.
+static void contact_flat_carveout() {
+    static int done = 0;
+    if (done) return;
+    done = 1;
+    const char* e = getenv("OLC_CONTACT_CARVEOUT");
+    if (!e) return;
+    const int pct = atoi(e);
+    if (pct >= 0 && pct <= 100)
+        cudaFuncSetAttribute(k_contact_flat, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+}
+
 void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
                     olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s) {
     if (contact_flat()) {
+        contact_flat_carveout();
         olc_u32 blocks = (n_cap + CF_THREADS - 1) / CF_THREADS;
         if (blocks == 0) blocks = 1;
         if (blocks > 148 * 16) blocks = 148 * 16;
