@@ -217,7 +217,9 @@ void launch_contact_mech(const float4* posr, const olc_u32* ranges, const olc_u3
 // a thread first lists its non-empty Moore bins (in order) in its own column
 // of shared memory, then walks rows bin after bin, so the lanes of a warp stay
 // converged until each has run out of candidates (the nested loops run every
-// bin as long as the fullest lane's).  Same candidates, order and arithmetic.
+// bin as long as the fullest lane's), and it requests the next candidate's
+// record before using the current one (the pass waits on L2 latency).  Same
+// candidates, order and arithmetic.
 constexpr int CF_THREADS = 128;
 __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __restrict__ posr,
                                                             const uint2* __restrict__ ranges, const olc_u32* n_dev,
@@ -318,8 +320,8 @@ __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __res
 }
 
 // k_contact_flat is the default; OLC_CONTACT=nested selects k_contact (same
-// bits; 0.72 ms vs 0.69 ms per step over steps 5-105 of the 1 M-agent scale
-// workload).
+// bits; over the 200 benchmark steps of the 1 M-agent scale workload 0.92 ms
+// vs 1.04 ms per step).
 static bool contact_flat() {
     static int v = -1;
     if (v < 0) {
