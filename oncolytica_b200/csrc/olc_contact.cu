@@ -220,7 +220,32 @@ void launch_contact_mech(const float4* posr, const olc_u32* ranges, const olc_u3
 // bin as long as the fullest lane's), and it requests the next candidate's
 // record before using the current one (the pass waits on L2 latency).  Same
 // candidates, order and arithmetic.
+// One candidate of the flat walk: the pair law of k_contact, summed into f.
+__device__ __forceinline__ void contact_pair(const float4& p, const float4& q, olc_u32 i, olc_u32 j,
+                                             const ContactDev& c, float& fx, float& fy, float& fz) {
+    if (j == i || q.w < 0.0f) return;
+    const float ddx = __fsub_rn(p.x, q.x);
+    const float ddy = __fsub_rn(p.y, q.y);
+    const float ddz = __fsub_rn(p.z, q.z);
+    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), __fmul_rn(ddz, ddz));
+    const float rsum = __fadd_rn(p.w, q.w);
+    if (d2 > __fmul_rn(__fmul_rn(rsum, rsum), 1.00000095367431640625f)) return;
+    const float dist = sqrtf(d2);
+    if (!(dist < rsum)) return;
+    const float ov = __fsub_rn(rsum, dist);
+    const float f = __fmul_rn(__fmul_rn(c.stiffness, ov), sqrtf(ov));
+    if (dist < 1e-5f) {
+        fx = __fadd_rn(fx, i < j ? -f : f);
+    } else {
+        const float sc = __fdiv_rn(f, dist);
+        fx = __fadd_rn(fx, __fmul_rn(ddx, sc));
+        fy = __fadd_rn(fy, __fmul_rn(ddy, sc));
+        fz = __fadd_rn(fz, __fmul_rn(ddz, sc));
+    }
+}
+
 constexpr int CF_THREADS = 128;
+template <int DEPTH>
 __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __restrict__ posr,
                                                             const uint2* __restrict__ ranges, const olc_u32* n_dev,
                                                             olc_u32 n_host, ContactDev c, float* __restrict__ xo,
@@ -253,57 +278,69 @@ __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __res
             }
         }
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-        int b = 0;
-        olc_u32 j = 0, end = 0;
-        float4 q = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
-        if (nb > 0) {
-            const uint2 r = s_bins[0][t];
-            j = r.x;
-            end = r.y;
-            q = __ldg(posr + j);
-        }
-        while (b < nb) {
-            // the next candidate's record is requested before this one is used,
-            // so two loads are in flight per thread
-            olc_u32 jn = j + 1, en = end;
-            int bn = b;
-            if (jn == en) {
-                if (++bn < nb) {
-                    const uint2 r = s_bins[bn][t];
-                    jn = r.x;
-                    en = r.y;
-                }
+        if (DEPTH == 1) {
+            // the next candidate's record is requested before this one is used
+            int b = 0;
+            olc_u32 j = 0, end = 0;
+            float4 q = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+            if (nb > 0) {
+                const uint2 r = s_bins[0][t];
+                j = r.x;
+                end = r.y;
+                q = __ldg(posr + j);
             }
-            const float4 qn = bn < nb ? __ldg(posr + jn) : q;
-            if (j != i) {
-                if (!(q.w < 0.0f)) {
-                    const float ddx = __fsub_rn(p.x, q.x);
-                    const float ddy = __fsub_rn(p.y, q.y);
-                    const float ddz = __fsub_rn(p.z, q.z);
-                    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)),
-                                               __fmul_rn(ddz, ddz));
-                    const float rsum = __fadd_rn(p.w, q.w);
-                    if (!(d2 > __fmul_rn(__fmul_rn(rsum, rsum), 1.00000095367431640625f))) {
-                        const float dist = sqrtf(d2);
-                        if (dist < rsum) {
-                            const float ov = __fsub_rn(rsum, dist);
-                            const float f = __fmul_rn(__fmul_rn(c.stiffness, ov), sqrtf(ov));
-                            if (dist < 1e-5f) {
-                                fx = __fadd_rn(fx, i < j ? -f : f);
-                            } else {
-                                const float sc = __fdiv_rn(f, dist);
-                                fx = __fadd_rn(fx, __fmul_rn(ddx, sc));
-                                fy = __fadd_rn(fy, __fmul_rn(ddy, sc));
-                                fz = __fadd_rn(fz, __fmul_rn(ddz, sc));
-                            }
-                        }
+            while (b < nb) {
+                olc_u32 jn = j + 1, en = end;
+                int bn = b;
+                if (jn == en) {
+                    if (++bn < nb) {
+                        const uint2 r = s_bins[bn][t];
+                        jn = r.x;
+                        en = r.y;
                     }
                 }
+                const float4 qn = bn < nb ? __ldg(posr + jn) : q;
+                contact_pair(p, q, i, j, c, fx, fy, fz);
+                j = jn;
+                end = en;
+                b = bn;
+                q = qn;
             }
-            j = jn;
-            end = en;
-            b = bn;
-            q = qn;
+        } else if (nb > 0) {
+            // two records ahead: slots 0 (in use), 1 and 2 (requested); the
+            // cursor (bc, jc, ec) is slot 2's position
+            int bc = 0;
+            uint2 r = s_bins[0][t];
+            olc_u32 jc = r.x, ec = r.y;
+            auto advance = [&]() -> bool {
+                if (++jc == ec && ++bc < nb) {
+                    const uint2 rn = s_bins[bc][t];
+                    jc = rn.x;
+                    ec = rn.y;
+                }
+                return bc < nb;
+            };
+            olc_u32 j0 = jc;
+            float4 q0 = __ldg(posr + j0);
+            bool v1 = advance();
+            olc_u32 j1 = jc;
+            float4 q1 = v1 ? __ldg(posr + j1) : q0;
+            bool v2 = advance();
+            olc_u32 j2 = jc;
+            float4 q2 = v2 ? __ldg(posr + j2) : q0;
+            bool v0 = true;
+            while (v0) {
+                contact_pair(p, q0, i, j0, c, fx, fy, fz);
+                j0 = j1;
+                q0 = q1;
+                v0 = v1;
+                j1 = j2;
+                q1 = q2;
+                v1 = v2;
+                v2 = v2 && advance();
+                j2 = jc;
+                if (v2) q2 = __ldg(posr + j2);
+            }
         }
         float mx = __fmul_rn(fx, md), my = __fmul_rn(fy, md), mz = __fmul_rn(fz, md);
         const float len = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz)));
@@ -331,6 +368,17 @@ static bool contact_flat() {
     return v == 1;
 }
 
+// OLC_CONTACT_PREFETCH=2 keeps two neighbour records in flight per thread
+// instead of one (same bits).
+static bool contact_prefetch2() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("OLC_CONTACT_PREFETCH");
+        v = (e && e[0] == '2') ? 1 : 0;
+    }
+    return v == 1;
+}
+
 // OLC_CONTACT_CARVEOUT=<percent> sets the shared-memory carveout preference of
 // k_contact_flat (its bin lists take shared memory that neighbour loads would
 // otherwise find in L1); unset leaves the driver's choice.
@@ -342,7 +390,10 @@ static void contact_flat_carveout() {
     if (!e) return;
     const int pct = atoi(e);
     if (pct >= 0 && pct <= 100)
-        cudaFuncSetAttribute(k_contact_flat, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+        {
+        cudaFuncSetAttribute(k_contact_flat<1>, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+        cudaFuncSetAttribute(k_contact_flat<2>, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+    }
 }
 
 void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
@@ -352,8 +403,12 @@ void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_
         olc_u32 blocks = (n_cap + CF_THREADS - 1) / CF_THREADS;
         if (blocks == 0) blocks = 1;
         if (blocks > 148 * 16) blocks = 148 * 16;
-        k_contact_flat<<<blocks, CF_THREADS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_dev, n_host, c,
-                                                     x, y, z);
+        if (contact_prefetch2())
+            k_contact_flat<2><<<blocks, CF_THREADS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_dev,
+                                                            n_host, c, x, y, z);
+        else
+            k_contact_flat<1><<<blocks, CF_THREADS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_dev,
+                                                            n_host, c, x, y, z);
         return;
     }
     olc_u32 blocks = (n_cap + 255) / 256;
