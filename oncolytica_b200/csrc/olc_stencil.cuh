@@ -93,8 +93,11 @@ __device__ __forceinline__ void stencil_update8_fma(float xl, float xr, const fl
     for (int k = 0; k < 4; ++k) {
         const int e = 2 * k;
         const f32x2 cc = pk2(c[e], c[e + 1]);
-        const f32x2 s = add2(add2(add2(pk2(k == 0 ? xl : c[e - 1], c[e]), pk2(c[e + 1], k == 3 ? xr : c[e + 2])),
-                                  add2(pk2(ym[e], ym[e + 1]), pk2(yp[e], yp[e + 1]))),
+        // the x sums as two scalar adds: their operands are shifted by one
+        // voxel, so as a pair they would straddle register pairs
+        const float sx0 = __fadd_rn(k == 0 ? xl : c[e - 1], c[e + 1]);
+        const float sx1 = __fadd_rn(c[e], k == 3 ? xr : c[e + 2]);
+        const f32x2 s = add2(add2(pk2(sx0, sx1), add2(pk2(ym[e], ym[e + 1]), pk2(yp[e], yp[e + 1]))),
                              add2(pk2(zm[e], zm[e + 1]), pk2(zp[e], zp[e + 1])));
         const float2 w = upk2(mul2(fma2(r2, fma2(m6, cc, s), cc), id2));
         out[e] = fmaxf(w.x, 0.0f);
