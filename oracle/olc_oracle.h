@@ -12,7 +12,8 @@
  * against a restatement of template.wgsl:75-82 in tests.  Diffusion, reaction,
  * contact force and the tumour rule have no reference test or golden output:
  * for those, parity is pinned only by this restatement of
- * engine/assets/shaders/tumor_sim.wgsl ("parity unpinned" in DESIGN.md).
+ * engine/assets/shaders/tumor_sim.wgsl: their parity is unpinned by the
+ * reference itself.
  *
  * Floating point: compile with -ffp-contract=off so a*b+c rounds twice, as the
  * CUDA kernels do (they use __fmul_rn/__fadd_rn and --fmad=false).
