@@ -147,6 +147,17 @@ typedef struct {
  *     clamp of OlcContact.margin.
  * Summation order and coincident points are as OlcContact's.  Not used by the
  * benchmark configurations; solo handles only. */
+#define OLC_MAX_SPECIES 8  /* records of the species table (the engine's MAX_SPECIES) */
+
+/* Per-species active motion (the engine's SpeciesParam chemoTaxisO2,
+ * chemoTaxisGlu, baseMoveProb). */
+typedef struct {
+    float chemotaxis_o2;
+    float chemotaxis_glucose;
+    float move_prob;
+    float pad;
+} OlcSpecies;
+
 typedef struct {
     int32_t state_field;        /* i32 column, or -1 (nobody necrotic)        */
     float   necrotic_factor;
@@ -156,6 +167,21 @@ typedef struct {
     float   damping;
     float   max_speed;
     int32_t enabled;            /* 0: plain OlcContact                        */
+    /* Active motion of non-necrotic agents (tumor_sim.wgsl:584-604), added to
+     * the contact force: chemotaxis (chemo_force x the species' coefficients
+     * x the central-difference gradient of the O2 and glucose fields at the
+     * agent's voxel, neighbours clamped to the grid) and random motility
+     * (move_prob x motility_impulse x a random direction drawn from the
+     * agent's RNG column, two draws per agent and step). */
+    int32_t species_field;      /* i32 column selecting the record (clamped), or -1: record 0 */
+    int32_t rng_field;          /* u32 RNG column for motility, or -1: none   */
+    int32_t o2_field;           /* chemistry field for chemotaxis, or -1      */
+    int32_t glucose_field;      /* second chemotactic field, or -1            */
+    float   chemo_force;        /* engine CHEMO_FORCE: 2.0                    */
+    float   motility_impulse;   /* engine VELOCITY_IMPULSE: 0.4               */
+    int32_t n_species;          /* records used; 0 turns active motion off    */
+    int32_t pad2;
+    OlcSpecies species[OLC_MAX_SPECIES];
 } OlcMechanics;
 
 typedef struct {
@@ -553,6 +579,17 @@ int olc_stage_contact_mech(const float* posr_dev, const uint32_t* ranges_dev, ui
                            const OlcGeom* geom, const OlcContact* spec, const OlcMechanics* mech,
                            const int32_t* state_dev, float* vx_dev, float* vy_dev, float* vz_dev, float dt,
                            float* x_dev, float* y_dev, float* z_dev, void* stream);
+
+/* The same with active motion: species_dev (i32 per row) and rng_dev (u32 per
+ * row, advanced in place) may be NULL; o2_dev / glucose_dev are FP32 fields of
+ * geom->chem_dims (x fastest), or NULL.  mech's column indices are ignored
+ * here: presence of a pointer turns the term on. */
+int olc_stage_contact_motion(const float* posr_dev, const uint32_t* ranges_dev, uint32_t n,
+                             const OlcGeom* geom, const OlcContact* spec, const OlcMechanics* mech,
+                             const int32_t* state_dev, float* vx_dev, float* vy_dev, float* vz_dev,
+                             const int32_t* species_dev, uint32_t* rng_dev, const float* o2_dev,
+                             const float* glucose_dev, float dt, float* x_dev, float* y_dev, float* z_dev,
+                             void* stream);
 
 #ifdef __cplusplus
 }

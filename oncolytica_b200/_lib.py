@@ -48,7 +48,7 @@ EXPORTS = (
     "olc_pool_copy_results", "olc_pool_retire", "olc_pool_usage",
     "olc_arena_create", "olc_arena_alloc", "olc_arena_release", "olc_arena_stats", "olc_arena_destroy",
     "olc_engine_metrics", "olc_get_step_state", "olc_set_step_state", "olc_set_mechanics",
-    "olc_stage_contact_mech", "olc_bind_tissue_pair", "olc_current_tissue", "olc_set_rule_iterations",
+    "olc_stage_contact_mech", "olc_stage_contact_motion", "olc_bind_tissue_pair", "olc_current_tissue", "olc_set_rule_iterations",
 )
 
 
@@ -172,6 +172,14 @@ class OlcEngineMetricsSpec(C.Structure):
     ]
 
 
+OLC_MAX_SPECIES = 8
+
+
+class OlcSpecies(C.Structure):
+    _fields_ = [("chemotaxis_o2", C.c_float), ("chemotaxis_glucose", C.c_float), ("move_prob", C.c_float),
+                ("pad", C.c_float)]
+
+
 class OlcMechanics(C.Structure):
     _fields_ = [
         ("state_field", C.c_int32),
@@ -182,6 +190,15 @@ class OlcMechanics(C.Structure):
         ("damping", C.c_float),
         ("max_speed", C.c_float),
         ("enabled", C.c_int32),
+        ("species_field", C.c_int32),
+        ("rng_field", C.c_int32),
+        ("o2_field", C.c_int32),
+        ("glucose_field", C.c_int32),
+        ("chemo_force", C.c_float),
+        ("motility_impulse", C.c_float),
+        ("n_species", C.c_int32),
+        ("pad2", C.c_int32),
+        ("species", OlcSpecies * OLC_MAX_SPECIES),
     ]
 
 
@@ -280,6 +297,9 @@ _SIGS = {
     "olc_get_step_state": (C.c_int, [_VP, C.POINTER(OlcStepState), _VP]),
     "olc_set_mechanics": (C.c_int, [_VP, C.POINTER(OlcMechanics)]),
     "olc_bind_tissue_pair": (C.c_int, [_VP, _VP, _VP, C.c_int, C.c_size_t]),
+    "olc_stage_contact_motion": (C.c_int, [_VP, _VP, C.c_uint32, C.POINTER(OlcGeom), C.POINTER(OlcContact),
+                                           C.POINTER(OlcMechanics), _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
+                                           C.c_float, _VP, _VP, _VP, _VP]),
     "olc_current_tissue": (C.c_int, [_VP, C.POINTER(C.c_int)]),
     "olc_set_rule_iterations": (C.c_int, [_VP, C.POINTER(C.c_int), C.c_int]),
     "olc_stage_contact_mech": (C.c_int, [_VP, _VP, C.c_uint32, C.POINTER(OlcGeom), C.POINTER(OlcContact),

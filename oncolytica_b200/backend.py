@@ -180,6 +180,29 @@ class CudaBackend:
                     raise ValueError(f"setup_contact: velocity needs an ol.vec3 cell field {contact.velocity!r}")
             m.damping = contact.damping
             m.max_speed = contact.max_speed if contact.max_speed is not None else 0.8 * eng.tissue_voxel_size
+            m.species_field = m.rng_field = m.o2_field = m.glucose_field = -1
+            if contact.motion:
+                m.n_species = len(contact.species)
+                for i, (a, b, c) in enumerate(contact.species):
+                    m.species[i].chemotaxis_o2, m.species[i].chemotaxis_glucose, m.species[i].move_prob = a, b, c
+                m.chemo_force = contact.chemo_force
+                m.motility_impulse = contact.motility_impulse
+                if contact.species_field is not None:
+                    try:
+                        m.species_field = L.col_index(contact.species_field)
+                    except KeyError:
+                        raise ValueError(f"setup_contact: no cell field {contact.species_field!r} for the species")
+                if any(rec[2] != 0.0 for rec in contact.species):
+                    m.rng_field = L.col_index("_rng_state")
+                if any(rec[0] != 0.0 or rec[1] != 0.0 for rec in contact.species):
+                    names = list(contact.chemo_fields)
+                    if names == [None, None]:
+                        names = (list(L.chem_fields) + [None, None])[:2]
+                    for attr, name in zip(("o2_field", "glucose_field"), names):
+                        if name is not None:
+                            if name not in L.chem_fields:
+                                raise ValueError(f"setup_contact: no chemistry field {name!r} for chemotaxis")
+                            setattr(m, attr, L.chem_fields.index(name))
             self._check(self.lib.olc_set_mechanics(self.handle, C.byref(m)))
         if self.program is not None:
             names = (C.c_char_p * len(self.program.kernels))(*[k.encode() for k, _ in self.program.kernels])

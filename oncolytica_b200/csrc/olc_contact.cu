@@ -86,6 +86,26 @@ __global__ void __launch_bounds__(256) k_contact(const float4* __restrict__ posr
     }
 }
 
+// Field value at (x, y, z) of a chemistry grid in any storage.
+__device__ __forceinline__ float motion_field(const void* f, int type, const int* dims, int x, int y, int z) {
+    const olc_u32 v = ((olc_u32)z * (olc_u32)dims[1] + (olc_u32)y) * (olc_u32)dims[0] + (olc_u32)x;
+    if (type == OLC_FIELD_F32) return static_cast<const float*>(f)[v];
+    const unsigned short h = static_cast<const unsigned short*>(f)[v];
+    return (type == OLC_FIELD_F16 || type == OLC_FIELD_F16_SR) ? olc_f16_to_float(h) : olc_bf16_to_float(h);
+}
+
+// Central-difference gradient 0.5 (f(v + e) - f(v - e)) per axis, the
+// neighbours clamped into the grid.
+__device__ __forceinline__ float3 motion_grad(const void* f, int type, const int* d, int x, int y, int z) {
+    const int xm = x > 0 ? x - 1 : 0, xp = x < d[0] - 1 ? x + 1 : d[0] - 1;
+    const int ym = y > 0 ? y - 1 : 0, yp = y < d[1] - 1 ? y + 1 : d[1] - 1;
+    const int zm = z > 0 ? z - 1 : 0, zp = z < d[2] - 1 ? z + 1 : d[2] - 1;
+    return make_float3(
+        __fmul_rn(0.5f, __fsub_rn(motion_field(f, type, d, xp, y, z), motion_field(f, type, d, xm, y, z))),
+        __fmul_rn(0.5f, __fsub_rn(motion_field(f, type, d, x, yp, z), motion_field(f, type, d, x, ym, z))),
+        __fmul_rn(0.5f, __fsub_rn(motion_field(f, type, d, x, y, zp), motion_field(f, type, d, x, y, zm))));
+}
+
 // The engine's full pair law (tumor_sim.wgsl:505-628) over the same
 // neighbour walk and summation order as k_contact:
 //   repulsion  dist < r_i + r_j: k * ov^(3/2) along n_ij, k scaled by
@@ -161,6 +181,34 @@ __global__ void __launch_bounds__(256) k_contact_mech(const float4* __restrict__
                         }
                     }
                 }
+            }
+        }
+        // active motion of a non-necrotic agent (tumor_sim.wgsl:584-604):
+        // F += chemo_force (grad O2 chemo_o2 + grad glucose chemo_glu), then
+        // F += rand_dir move_prob impulse
+        if (!nec_i && (m.f0 || m.f1 || m.rng)) {
+            int sp = m.species ? m.species[i] : 0;
+            sp = sp < 0 ? 0 : (sp >= m.n_species ? m.n_species - 1 : sp);
+            if (m.f0 || m.f1) {
+                const int vx = olc_bin_coord(p.x, m.cvs, m.cdims[0]);
+                const int vy = olc_bin_coord(p.y, m.cvs, m.cdims[1]);
+                const int vz = olc_bin_coord(p.z, m.cvs, m.cdims[2]);
+                float3 g0 = make_float3(0.0f, 0.0f, 0.0f), g1 = g0;
+                if (m.f0) g0 = motion_grad(m.f0, m.f0_type, m.cdims, vx, vy, vz);
+                if (m.f1) g1 = motion_grad(m.f1, m.f1_type, m.cdims, vx, vy, vz);
+                const float co2 = m.sp_o2[sp], cglu = m.sp_glu[sp];
+                fx = __fadd_rn(fx, __fmul_rn(__fadd_rn(__fmul_rn(g0.x, co2), __fmul_rn(g1.x, cglu)), m.chemo_force));
+                fy = __fadd_rn(fy, __fmul_rn(__fadd_rn(__fmul_rn(g0.y, co2), __fmul_rn(g1.y, cglu)), m.chemo_force));
+                fz = __fadd_rn(fz, __fmul_rn(__fadd_rn(__fmul_rn(g0.z, co2), __fmul_rn(g1.z, cglu)), m.chemo_force));
+            }
+            if (m.rng) {
+                olc_u32 st = m.rng[i];
+                const float3 r = olc_rand_dir(st);
+                m.rng[i] = st;
+                const float mv = m.sp_move[sp];
+                fx = __fadd_rn(fx, __fmul_rn(__fmul_rn(r.x, mv), m.impulse));
+                fy = __fadd_rn(fy, __fmul_rn(__fmul_rn(r.y, mv), m.impulse));
+                fz = __fadd_rn(fz, __fmul_rn(__fmul_rn(r.z, mv), m.impulse));
             }
         }
         float mx, my, mz;

@@ -174,6 +174,18 @@ struct MechDev {
     float* vy;
     float* vz;
     float damping, max_speed;
+    // active motion (non-necrotic agents): chemotaxis up the field gradients
+    // and random motility from the agent's RNG
+    const int* species;      // null: record 0
+    olc_u32* rng;            // null: no motility
+    const void* f0;          // O2 (current buffer), or null
+    const void* f1;          // glucose, or null
+    int f0_type, f1_type;
+    int cdims[3];
+    float cvs;
+    float chemo_force, impulse;
+    int n_species;
+    float sp_o2[OLC_MAX_SPECIES], sp_glu[OLC_MAX_SPECIES], sp_move[OLC_MAX_SPECIES];
 };
 void launch_contact_mech(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
                          olc_u32 n_cap, const ContactDev& c, const MechDev& m, float* x, float* y, float* z,

@@ -273,6 +273,27 @@ OlcRuleParams make_rule_params(OlcSim* s, int rule_index, int in_buf) {
     return P;
 }
 
+// Active-motion inputs of the engine's force law from a handle's current buffers.
+void fill_motion(OlcSim* s, const OlcMechanics& mech, int cc, MechDev* m) {
+    if (mech.n_species < 1) return;  // no species table: no active motion
+    m->species = mech.species_field >= 0 ? static_cast<const int*>(s->col[cc][mech.species_field]) : nullptr;
+    m->rng = mech.rng_field >= 0 ? static_cast<olc_u32*>(s->col[cc][mech.rng_field]) : nullptr;
+    m->f0 = mech.o2_field >= 0 ? s->field[s->field_cur[mech.o2_field]][mech.o2_field] : nullptr;
+    m->f1 = mech.glucose_field >= 0 ? s->field[s->field_cur[mech.glucose_field]][mech.glucose_field] : nullptr;
+    m->f0_type = mech.o2_field >= 0 ? s->fstep[mech.o2_field].storage : 0;
+    m->f1_type = mech.glucose_field >= 0 ? s->fstep[mech.glucose_field].storage : 0;
+    for (int i = 0; i < 3; ++i) m->cdims[i] = s->geom.chem_dims[i];
+    m->cvs = s->geom.chem_voxel_size;
+    m->chemo_force = mech.chemo_force;
+    m->impulse = mech.motility_impulse;
+    m->n_species = mech.n_species < 1 ? 1 : (mech.n_species > OLC_MAX_SPECIES ? OLC_MAX_SPECIES : mech.n_species);
+    for (int k = 0; k < OLC_MAX_SPECIES; ++k) {
+        m->sp_o2[k] = mech.species[k].chemotaxis_o2;
+        m->sp_glu[k] = mech.species[k].chemotaxis_glucose;
+        m->sp_move[k] = mech.species[k].move_prob;
+    }
+}
+
 int launch_rule(OlcSim* s, int k, const OlcRuleParams& P, cudaStream_t st, olc_u32 units = 0) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -427,6 +448,7 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
         }
         m.damping = s->mech.damping;
         m.max_speed = s->mech.max_speed;
+        fill_motion(s, s->mech, cc, &m);
         launch_contact_mech(s->posr, s->ranges, s->counters + OLC_CTR_N, 0, cap, s->contact_dev, m,
                             static_cast<float*>(s->col[cc][0]), static_cast<float*>(s->col[cc][1]),
                             static_cast<float*>(s->col[cc][2]), st);
@@ -1260,6 +1282,15 @@ int olc_set_mechanics(OlcSim* s, const OlcMechanics* m) {
             return fail(s, OLC_ERR_ARG, "olc_set_mechanics: adhesion needs adhesion_range > 0");
         if (m->velocity_field >= 0 && !(m->max_speed > 0.0f))
             return fail(s, OLC_ERR_ARG, "olc_set_mechanics: velocity integration needs max_speed > 0");
+        if (m->n_species < 0 || m->n_species > OLC_MAX_SPECIES)
+            return fail(s, OLC_ERR_ARG, "olc_set_mechanics: n_species must be in [0, OLC_MAX_SPECIES]");
+        if (m->n_species > 0) {
+            if (m->species_field >= nc || m->rng_field >= nc)
+                return fail(s, OLC_ERR_ARG, "olc_set_mechanics: species or RNG column out of range");
+            for (int f : {m->o2_field, m->glucose_field})
+                if (f >= (int)s->caps.n_fields || (f >= 0 && !s->field_bound[f]))
+                    return fail(s, OLC_ERR_ARG, "olc_set_mechanics: chemotactic field not bound");
+        }
     }
     drop_graphs(s);
     s->mech = *m;
@@ -2356,6 +2387,65 @@ int olc_stage_contact_mech(const float* posr, const uint32_t* ranges, uint32_t n
     launch_contact_mech(reinterpret_cast<const float4*>(posr), ranges, nullptr, n, n, d, m, x, y, z,
                         as_stream(stream));
     return cuda_status(cudaGetLastError(), "olc_stage_contact_mech");
+}
+
+int olc_stage_contact_motion(const float* posr, const uint32_t* ranges, uint32_t n, const OlcGeom* geom,
+                             const OlcContact* spec, const OlcMechanics* mech, const int32_t* state, float* vx,
+                             float* vy, float* vz, const int32_t* species, uint32_t* rng, const float* o2,
+                             const float* glucose, float dt, float* x, float* y, float* z, void* stream) {
+    if (!geom || !spec || !mech || (n && (!posr || !ranges || !x || !y || !z)))
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_contact_motion: null argument");
+    if (mech->velocity_field >= 0 && n && (!vx || !vy || !vz))
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_contact_motion: velocity columns missing");
+    if (mech->adhesion_stiffness != 0.0f && !(mech->adhesion_range > 0.0f))
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_contact_motion: adhesion needs adhesion_range > 0");
+    if (mech->n_species < 0 || mech->n_species > OLC_MAX_SPECIES)
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_contact_motion: n_species out of range");
+    std::string err;
+    if (!geom_ok(*geom, &err)) return fail(nullptr, OLC_ERR_ARG, "olc_stage_contact_motion: " + err);
+    if ((o2 || glucose) && (geom->chem_dims[0] < 1 || geom->chem_dims[1] < 1 || geom->chem_dims[2] < 1))
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_contact_motion: chemotaxis needs chem_dims");
+    if (n == 0) return OLC_OK;
+    ContactDev d;
+    for (int i = 0; i < 3; ++i) {
+        d.tdims[i] = geom->tissue_dims[i];
+        d.lo[i] = geom->domain_lo[i] + spec->margin;
+        d.hi[i] = geom->domain_hi[i] - spec->margin;
+    }
+    d.tvs = geom->tissue_voxel_size;
+    d.stiffness = spec->stiffness;
+    d.mobility = spec->mobility;
+    d.max_disp = spec->max_disp;
+    d.dt = dt;
+    MechDev m = {};
+    m.state = state;
+    m.necrotic_factor = mech->necrotic_factor;
+    m.adh_k = mech->adhesion_stiffness;
+    m.adh_range = mech->adhesion_range;
+    if (mech->velocity_field >= 0) {
+        m.vx = vx;
+        m.vy = vy;
+        m.vz = vz;
+    }
+    m.damping = mech->damping;
+    m.max_speed = mech->max_speed;
+    m.species = species;
+    m.rng = rng;
+    m.f0 = o2;
+    m.f1 = glucose;
+    for (int i = 0; i < 3; ++i) m.cdims[i] = geom->chem_dims[i];
+    m.cvs = geom->chem_voxel_size;
+    m.chemo_force = mech->chemo_force;
+    m.impulse = mech->motility_impulse;
+    m.n_species = mech->n_species < 1 ? 1 : mech->n_species;
+    for (int k = 0; k < OLC_MAX_SPECIES; ++k) {
+        m.sp_o2[k] = mech->species[k].chemotaxis_o2;
+        m.sp_glu[k] = mech->species[k].chemotaxis_glucose;
+        m.sp_move[k] = mech->species[k].move_prob;
+    }
+    launch_contact_mech(reinterpret_cast<const float4*>(posr), ranges, nullptr, n, n, d, m, x, y, z,
+                        as_stream(stream));
+    return cuda_status(cudaGetLastError(), "olc_stage_contact_motion");
 }
 
 }  // extern "C"

@@ -51,10 +51,22 @@ class ContactSpec:
     damping: float = 1.0
     max_speed: float | None = None
     state: str | None = "state"
+    # active motion: one (chemotaxis_o2, chemotaxis_glucose, move_prob) record,
+    # or a species table selected by an i32 cell field
+    species: tuple = ()
+    species_field: str | None = None
+    chemo_fields: tuple = (None, None)
+    chemo_force: float = 2.0
+    motility_impulse: float = 0.4
+
+    @property
+    def motion(self) -> bool:
+        return any(any(v != 0.0 for v in rec) for rec in self.species)
 
     @property
     def mechanics(self) -> bool:
-        return self.necrotic_factor != 1.0 or self.adhesion_stiffness != 0.0 or self.velocity is not None
+        return self.necrotic_factor != 1.0 or self.adhesion_stiffness != 0.0 or self.velocity is not None or \
+            self.motion
 
 
 def stable_substeps(D: float, dt: float, dx: float, margin: float = 1.05) -> int:
@@ -185,7 +197,10 @@ class Engine:
     def setup_contact(self, radius: str | float = "radius", stiffness: float = 1.0, mobility: float = 10.0,
                       max_disp: float = 1.0, margin: float = 0.1, necrotic_factor: float = 1.0,
                       adhesion_stiffness: float = 0.0, adhesion_range: float = 0.0, velocity: str | None = None,
-                      damping: float = 1.0, max_speed: float | None = None, state: str | None = "state") -> None:
+                      damping: float = 1.0, max_speed: float | None = None, state: str | None = "state",
+                      chemotaxis: tuple = (0.0, 0.0), motility: float = 0.0, species: list | None = None,
+                      species_field: str | None = None, chemotactic_fields: tuple | None = None,
+                      chemo_force: float = 2.0, motility_impulse: float = 0.4) -> None:
         """Built-in Hertz-like contact repulsion over the 27 bins
         (engine tumor_sim.wgsl:505-628), overdamped.  The engine's other terms
         are optional: `necrotic_factor` scales repulsion when either agent's
@@ -193,13 +208,27 @@ class Engine:
         `adhesion_range` add the cosine adhesion between non-necrotic agents;
         `velocity` names an ol.vec3 cell field for the engine's damped velocity
         integration (`damping`, speed cap `max_speed`, default 0.8 x bin size)
-        in place of the overdamped move."""
+        in place of the overdamped move.  Active motion of non-necrotic agents
+        (tumor_sim.wgsl:584-604): `chemotaxis` = (O2, glucose) coefficients on
+        the gradients of `chemotactic_fields` (default: the first two chemistry
+        fields) times `chemo_force`, and random motility `motility` times
+        `motility_impulse` along a direction drawn from the agent's RNG; or a
+        `species` table of (chemotaxis_o2, chemotaxis_glucose, move_prob)
+        records selected by the i32 cell field `species_field`."""
         if adhesion_stiffness != 0.0 and not adhesion_range > 0.0:
             raise ValueError("adhesion_stiffness needs adhesion_range > 0")
+        if species is None:
+            table = (tuple(float(v) for v in (*chemotaxis, motility)),)
+        else:
+            table = tuple(tuple(float(v) for v in rec) for rec in species)
+            if not 1 <= len(table) <= 8 or any(len(rec) != 3 for rec in table):
+                raise ValueError("species: 1 to 8 records of (chemotaxis_o2, chemotaxis_glucose, move_prob)")
         self._contact = ContactSpec(radius, float(stiffness), float(mobility), float(max_disp), float(margin),
                                     float(necrotic_factor), float(adhesion_stiffness), float(adhesion_range),
                                     velocity, float(damping), None if max_speed is None else float(max_speed),
-                                    state)
+                                    state, table, species_field,
+                                    tuple(chemotactic_fields) if chemotactic_fields is not None else (None, None),
+                                    float(chemo_force), float(motility_impulse))
 
     def setup_domain(self, lo: tuple[float, float, float], hi: tuple[float, float, float]) -> None:
         self.domain_lo = tuple(float(v) for v in lo)

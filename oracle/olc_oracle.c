@@ -525,11 +525,38 @@ void orc_contact(const float* posr, const uint32_t* ranges, uint32_t n, const in
  * the engine's necrotic factor and adhesion branch
  * (engine/assets/shaders/tumor_sim.wgsl:552-569) and its damped velocity
  * integration (:606-625). */
+static float orc_field_at(const float* f, const int32_t d[3], int x, int y, int z) {
+    return f[((size_t)z * d[1] + y) * d[0] + x];
+}
+
+/* Central difference 0.5 (f(v + e) - f(v - e)), neighbours clamped to the grid. */
+static void orc_grad(const float* f, const int32_t d[3], int x, int y, int z, float g[3]) {
+    const int xm = x > 0 ? x - 1 : 0, xp = x < d[0] - 1 ? x + 1 : d[0] - 1;
+    const int ym = y > 0 ? y - 1 : 0, yp = y < d[1] - 1 ? y + 1 : d[1] - 1;
+    const int zm = z > 0 ? z - 1 : 0, zp = z < d[2] - 1 ? z + 1 : d[2] - 1;
+    g[0] = 0.5f * (orc_field_at(f, d, xp, y, z) - orc_field_at(f, d, xm, y, z));
+    g[1] = 0.5f * (orc_field_at(f, d, x, yp, z) - orc_field_at(f, d, x, ym, z));
+    g[2] = 0.5f * (orc_field_at(f, d, x, y, zp) - orc_field_at(f, d, x, y, zm));
+}
+
 void orc_contact_mech(const float* posr, const uint32_t* ranges, uint32_t n, const int32_t tdims[3], float tvs,
                       float stiffness, float mobility, float max_disp, float dt, const float lo[3], const float hi[3],
                       const int32_t* state, float necrotic_factor, float adh_k, float adh_range, float* vx,
                       float* vy, float* vz, float damping, float max_speed, float* xo, float* yo, float* zo,
                       int nthreads) {
+    orc_contact_motion(posr, ranges, n, tdims, tvs, stiffness, mobility, max_disp, dt, lo, hi, state,
+                       necrotic_factor, adh_k, adh_range, vx, vy, vz, damping, max_speed, NULL, NULL, NULL, NULL,
+                       NULL, 0.0f, 0.0f, 0.0f, 0, NULL, NULL, NULL, xo, yo, zo, nthreads);
+}
+
+void orc_contact_motion(const float* posr, const uint32_t* ranges, uint32_t n, const int32_t tdims[3], float tvs,
+                        float stiffness, float mobility, float max_disp, float dt, const float lo[3],
+                        const float hi[3], const int32_t* state, float necrotic_factor, float adh_k,
+                        float adh_range, float* vx, float* vy, float* vz, float damping, float max_speed,
+                        const int32_t* species, uint32_t* rng, const float* o2, const float* glu,
+                        const int32_t* cdims, float cvs, float chemo_force, float impulse, int n_species,
+                        const float* sp_o2, const float* sp_glu, const float* sp_move, float* xo, float* yo,
+                        float* zo, int nthreads) {
     const int nt = nthreads_or_all(nthreads);
     const int adh = adh_k != 0.0f && adh_range > 0.0f;
     const float k_nec = stiffness * necrotic_factor;
@@ -586,6 +613,29 @@ void orc_contact_mech(const float* posr, const uint32_t* ranges, uint32_t n, con
                         }
                     }
                 }
+            }
+        }
+        /* active motion of a non-necrotic agent (tumor_sim.wgsl:584-604) */
+        if (!nec_i && n_species > 0 && (o2 || glu || rng)) {
+            int sp = species ? species[i] : 0;
+            sp = sp < 0 ? 0 : (sp >= n_species ? n_species - 1 : sp);
+            if (o2 || glu) {
+                const int gx = orc_bin_coord(p[0], cvs, cdims[0]);
+                const int gy = orc_bin_coord(p[1], cvs, cdims[1]);
+                const int gz = orc_bin_coord(p[2], cvs, cdims[2]);
+                float g0[3] = {0.0f, 0.0f, 0.0f}, g1[3] = {0.0f, 0.0f, 0.0f};
+                if (o2) orc_grad(o2, cdims, gx, gy, gz, g0);
+                if (glu) orc_grad(glu, cdims, gx, gy, gz, g1);
+                fx = fx + (g0[0] * sp_o2[sp] + g1[0] * sp_glu[sp]) * chemo_force;
+                fy = fy + (g0[1] * sp_o2[sp] + g1[1] * sp_glu[sp]) * chemo_force;
+                fz = fz + (g0[2] * sp_o2[sp] + g1[2] * sp_glu[sp]) * chemo_force;
+            }
+            if (rng) {
+                float r[3];
+                orc_rand_dir(&rng[i], r);
+                fx = fx + (r[0] * sp_move[sp]) * impulse;
+                fy = fy + (r[1] * sp_move[sp]) * impulse;
+                fz = fz + (r[2] * sp_move[sp]) * impulse;
             }
         }
         float mx, my, mz;

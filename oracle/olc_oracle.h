@@ -75,6 +75,20 @@ void orc_contact_mech(const float* posr, const uint32_t* ranges, uint32_t n, con
                       float* vy, float* vz, float damping, float max_speed, float* xo, float* yo, float* zo,
                       int nthreads);
 
+/* orc_contact_mech plus the engine's active motion of non-necrotic agents
+ * (tumor_sim.wgsl:584-604): chemotaxis up the clamped central-difference
+ * gradients of o2 / glu (x-fastest grids of cdims, voxel cvs) and random
+ * motility from rng (advanced in place); per-species coefficients selected by
+ * species (clamped; NULL = record 0).  n_species = 0 turns both off. */
+void orc_contact_motion(const float* posr, const uint32_t* ranges, uint32_t n, const int32_t tdims[3], float tvs,
+                        float stiffness, float mobility, float max_disp, float dt, const float lo[3],
+                        const float hi[3], const int32_t* state, float necrotic_factor, float adh_k,
+                        float adh_range, float* vx, float* vy, float* vz, float damping, float max_speed,
+                        const int32_t* species, uint32_t* rng, const float* o2, const float* glu,
+                        const int32_t* cdims, float cvs, float chemo_force, float impulse, int n_species,
+                        const float* sp_o2, const float* sp_glu, const float* sp_move, float* xo, float* yo,
+                        float* zo, int nthreads);
+
 /* ---------------------------------------------------------------------------
  * Tumour-spheroid workload (the built-in benchmark model, restated from its
  * DSL source in oncolytica_b200/workloads.py).  Columns: x y z radius volume

@@ -46,6 +46,10 @@ def lib() -> C.CDLL:
         L.orc_contact_mech.argtypes = [P, P, C.c_uint32, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
                                        P, P, P, C.c_float, C.c_float, C.c_float, P, P, P, C.c_float, C.c_float,
                                        P, P, P, C.c_int]
+        L.orc_contact_motion.argtypes = [P, P, C.c_uint32, P, C.c_float, C.c_float, C.c_float, C.c_float,
+                                         C.c_float, P, P, P, C.c_float, C.c_float, C.c_float, P, P, P, C.c_float,
+                                         C.c_float, P, P, P, P, P, C.c_float, C.c_float, C.c_float, C.c_int, P, P,
+                                         P, P, P, P, C.c_int]
         L.orc_tumour_step.restype = C.c_int
         L.orc_tumour_step.argtypes = [P, C.c_int]
         L.orc_tumour_fields.restype = C.c_int
@@ -223,6 +227,41 @@ def contact_mech(posr: np.ndarray, ranges: np.ndarray, tdims, tvs: float, stiffn
                            C.c_float(max_speed), _p(x), _p(y), _p(z), nthreads)
     pos = np.stack([x, y, z], axis=1)
     return (pos, np.stack(v, axis=1)) if v else (pos, None)
+
+
+def contact_motion(posr, ranges, tdims, tvs, stiffness, mobility, max_disp, dt, lo, hi, state=None,
+                   necrotic_factor=1.0, adh_k=0.0, adh_range=0.0, vel=None, damping=0.0, max_speed=0.0,
+                   species=None, rng=None, o2=None, glu=None, cdims=(1, 1, 1), cvs=1.0, chemo_force=2.0,
+                   impulse=0.4, table=((0.0, 0.0, 0.0),), nthreads: int = 0):
+    """orc_contact_motion; `table` rows are (chemotaxis_o2, chemotaxis_glucose,
+    move_prob).  Returns positions, velocities (or None) and the advanced RNG
+    states (or None)."""
+    posr = np.ascontiguousarray(posr, dtype=np.float32)
+    n = len(posr)
+    x, y, z = (posr[:, k].copy() for k in range(3))
+    td = np.array(tdims, dtype=np.int32)
+    cd = np.array(cdims, dtype=np.int32)
+    lo_a = np.array(lo, dtype=np.float32)
+    hi_a = np.array(hi, dtype=np.float32)
+    r = np.ascontiguousarray(ranges, dtype=np.uint32)
+    st = None if state is None else np.ascontiguousarray(state, dtype=np.int32)
+    v = None if vel is None else [np.ascontiguousarray(vel[:, k], dtype=np.float32).copy() for k in range(3)]
+    spc = None if species is None else np.ascontiguousarray(species, dtype=np.int32)
+    rg = None if rng is None else np.ascontiguousarray(rng, dtype=np.uint32).copy()
+    f0 = None if o2 is None else np.ascontiguousarray(o2, dtype=np.float32)
+    f1 = None if glu is None else np.ascontiguousarray(glu, dtype=np.float32)
+    tab = np.zeros((8, 3), np.float32)
+    if len(table):
+        tab[: len(table)] = np.asarray(table, np.float32).reshape(len(table), 3)
+    so2, sglu, smv = (np.ascontiguousarray(tab[:, k]) for k in range(3))
+    lib().orc_contact_motion(_p(posr), _p(r), n, _p(td), C.c_float(tvs), C.c_float(stiffness),
+                             C.c_float(mobility), C.c_float(max_disp), C.c_float(dt), _p(lo_a), _p(hi_a), _p(st),
+                             C.c_float(necrotic_factor), C.c_float(adh_k), C.c_float(adh_range),
+                             _p(v[0]) if v else None, _p(v[1]) if v else None, _p(v[2]) if v else None,
+                             C.c_float(damping), C.c_float(max_speed), _p(spc), _p(rg), _p(f0), _p(f1), _p(cd),
+                             C.c_float(cvs), C.c_float(chemo_force), C.c_float(impulse), len(table), _p(so2),
+                             _p(sglu), _p(smv), _p(x), _p(y), _p(z), nthreads)
+    return np.stack([x, y, z], axis=1), (np.stack(v, axis=1) if v else None), rg
 
 
 # ------------------------------------------------------------------ tumour workload

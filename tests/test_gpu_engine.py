@@ -364,6 +364,47 @@ def test_engine_mechanics_path_in_the_step(cuda):
     assert moved.any(), "a necrotic factor of 0.3 must change some contacts"
 
 
+def test_engine_active_motion_in_the_step(cuda):
+    """Chemotaxis and random motility through Engine.setup_contact: one step
+    from the same state with and without them keeps rows, states and life
+    flags; every live non-necrotic agent's RNG is two xorshift32 draws further
+    (the random direction), necrotic ones draw nothing, and positions move."""
+    spec = _parity_spec()
+
+    def run(**kw):
+        eng, sim = W.configure_engine(spec)
+        eng.setup_contact(radius="radius", stiffness=spec.stiffness, mobility=spec.mobility,
+                          max_disp=spec.max_disp, margin=spec.margin, **kw)
+        eng.load_model(sim)
+        x = (np.arange(spec.field_dims[0], dtype=np.float32) + 0.5) / spec.field_dims[0]
+        eng.chemistry.column("o2")[...] = np.clip(2.0 * x - 1.0, 0.0, 1.0)[:, None, None]  # no O2 below mid-x
+        eng.sync_to_device()
+        eng.run_step()
+        return eng._backend_impl.snapshot()
+
+    plain = run()
+    moved = run(chemotaxis=(2.0, 0.5), motility=0.3)
+    assert plain["rows"] == moved["rows"]
+    np.testing.assert_array_equal(plain["life"], moved["life"])
+    np.testing.assert_array_equal(plain["cols"]["state"], moved["cols"]["state"])
+
+    def two_draws(s):
+        s = s.astype(np.uint64)
+        for _ in range(2):
+            s ^= (s << 13) & 0xFFFFFFFF
+            s ^= s >> 17
+            s ^= (s << 5) & 0xFFFFFFFF
+        return s.astype(np.uint32)
+
+    live = plain["life"] == 0
+    active = live & (plain["cols"]["state"] != 3)
+    np.testing.assert_array_equal(moved["cols"]["_rng_state"][active], two_draws(plain["cols"]["_rng_state"][active]))
+    nec = live & (plain["cols"]["state"] == 3)
+    assert nec.any()
+    np.testing.assert_array_equal(moved["cols"]["_rng_state"][nec], plain["cols"]["_rng_state"][nec])
+    assert np.abs(moved["cols"]["pos.x"][active] - plain["cols"]["pos.x"][active]).max() > 1e-3
+
+
 def test_tumour_long_run_statistics(cuda):
     """Independent 60-step runs (GPU vs oracle, same seed): population counts
     within 1 % and radial profiles within 3 % of the live count."""

@@ -360,6 +360,66 @@ def test_contact_mechanics_matches_the_oracle(cuda, olc, adhesion, velocity):
     assert np.any(got != plain)
 
 
+def test_contact_active_motion_matches_the_oracle(cuda, olc):
+    """The engine's chemotaxis and random motility (tumor_sim.wgsl:584-604)
+    on top of the force law, per species: RNG states exact; positions and
+    velocities to 1e-4 (the random direction calls cosf/sinf)."""
+    rng = np.random.default_rng(33)
+    dims, vs = (16, 16, 16), 10.0
+    cd, cvs = (32, 32, 32), 5.0
+    n = 20000
+    pos = np.clip(rng.normal(80.0, 22.0, size=(n, 3)), 0.0, 159.0).astype(np.float32)
+    radius = rng.uniform(4.0, 6.0, size=n).astype(np.float32)
+    k = oracle.keys(pos, dims, vs)
+    ks, perm = oracle.sort_pairs(k)
+    ranges = oracle.bin_ranges(ks, oracle.tissue_key(*dims))
+    posr = np.concatenate([pos[perm], radius[perm, None]], axis=1).astype(np.float32)
+    state = rng.choice(np.array([1, 2, 3], np.int32), size=n, p=[0.6, 0.3, 0.1]).astype(np.int32)
+    species = rng.integers(-1, 5, size=n).astype(np.int32)  # out-of-range ids clamp
+    states = (rng.integers(1, 2 ** 32, size=n, dtype=np.uint64)).astype(np.uint32)
+    vel = rng.normal(0.0, 1.0, size=(n, 3)).astype(np.float32)
+    zz, yy, xx = np.meshgrid(*(np.arange(d, dtype=np.float32) for d in cd[::-1]), indexing="ij")
+    o2 = (0.5 + 0.4 * np.sin(xx / 5.0) * np.cos(yy / 7.0)).astype(np.float32).ravel()
+    glu = (zz / cd[2]).astype(np.float32).ravel()
+    table = ((1.5, 0.0, 0.3), (0.0, 2.0, 0.8), (-1.0, 0.5, 0.0))
+    prm = dict(stiffness=1.0, mobility=10.0, max_disp=1.0, dt=0.1)
+    lo, hi = (0.1, 0.1, 0.1), (159.9, 159.9, 159.9)
+    ref, ref_v, ref_rng = oracle.contact_motion(posr, ranges, dims, vs, prm["stiffness"], prm["mobility"],
+                                                prm["max_disp"], prm["dt"], lo, hi, state=state,
+                                                necrotic_factor=0.3, vel=vel, damping=1.5, max_speed=8.0,
+                                                species=species, rng=states, o2=o2, glu=glu, cdims=cd, cvs=cvs,
+                                                chemo_force=2.0, impulse=0.4, table=table)
+    pr, rg = to_dev(posr, cuda), to_dev(ranges, cuda)
+    x, y, z = (to_dev(np.ascontiguousarray(posr[:, c]), cuda) for c in range(3))
+    vd = [to_dev(np.ascontiguousarray(vel[:, c]), cuda) for c in range(3)]
+    st, spd, rgd = to_dev(state, cuda), to_dev(species, cuda), to_dev(states, cuda)
+    o2d, glud = to_dev(o2, cuda), to_dev(glu, cuda)
+    g = geom(dims, vs, lo=(0, 0, 0), hi=(160, 160, 160))
+    g.chem_dims[:] = cd
+    g.chem_voxel_size = cvs
+    spec = _lib.OlcContact(enabled=1, radius_field=-1, radius_const=0.0, stiffness=prm["stiffness"],
+                           mobility=prm["mobility"], max_disp=prm["max_disp"], margin=0.1)
+    m = _lib.OlcMechanics(state_field=0, necrotic_factor=0.3, adhesion_stiffness=0.0, adhesion_range=0.0,
+                          velocity_field=0, damping=1.5, max_speed=8.0, enabled=1, chemo_force=2.0,
+                          motility_impulse=0.4, n_species=len(table))
+    for i, (a, b, c) in enumerate(table):
+        m.species[i].chemotaxis_o2, m.species[i].chemotaxis_glucose, m.species[i].move_prob = a, b, c
+    _lib.check(olc.olc_stage_contact_motion(dptr(pr), dptr(rg), n, C.byref(g), C.byref(spec), C.byref(m), dptr(st),
+                                            *(dptr(v) for v in vd), dptr(spd), dptr(rgd), dptr(o2d), dptr(glud),
+                                            prm["dt"], dptr(x), dptr(y), dptr(z), None))
+    got = np.stack([to_host(x), to_host(y), to_host(z)], axis=1)
+    np.testing.assert_array_equal(to_host(rgd, np.uint32), ref_rng)
+    np.testing.assert_allclose(got, ref, rtol=0, atol=1e-4)
+    np.testing.assert_allclose(np.stack([to_host(v) for v in vd], axis=1), ref_v, rtol=0, atol=1e-4)
+    # necrotic agents draw nothing; the others advance their RNG by two draws
+    assert np.array_equal(ref_rng[state == 3], states[state == 3])
+    assert np.all(ref_rng[state != 3] != states[state != 3])
+    still, _, _ = oracle.contact_motion(posr, ranges, dims, vs, prm["stiffness"], prm["mobility"], prm["max_disp"],
+                                        prm["dt"], lo, hi, state=state, necrotic_factor=0.3, vel=vel, damping=1.5,
+                                        max_speed=8.0, table=())
+    assert np.abs(got - still).max() > 1e-3
+
+
 # ------------------------------------------------------------------ 16-bit field storage
 
 @pytest.mark.parametrize("storage", [1, 2, 3, 4])
