@@ -380,10 +380,13 @@ def test_engine_active_motion_in_the_step(cuda):
         eng.chemistry.column("o2")[...] = np.clip(2.0 * x - 1.0, 0.0, 1.0)[:, None, None]  # no O2 below mid-x
         eng.sync_to_device()
         eng.run_step()
-        return eng._backend_impl.snapshot()
+        snap = eng._backend_impl.snapshot()
+        snap["births"] = eng._backend_impl.counters()["births"]
+        return snap
 
     plain = run()
     moved = run(chemotaxis=(2.0, 0.5), motility=0.3)
+    assert plain["births"] == moved["births"] > 0
     assert plain["rows"] == moved["rows"]
     np.testing.assert_array_equal(plain["life"], moved["life"])
     np.testing.assert_array_equal(plain["cols"]["state"], moved["cols"]["state"])
@@ -396,9 +399,13 @@ def test_engine_active_motion_in_the_step(cuda):
             s ^= (s << 5) & 0xFFFFFFFF
         return s.astype(np.uint32)
 
-    live = plain["life"] == 0
+    # the contact stage moves the rows that entered the step; this step's
+    # children (appended after them) keep the RNG their parents gave them
+    entered = np.arange(plain["rows"]) < plain["rows"] - plain["births"]
+    live = (plain["life"] == 0) & entered
     active = live & (plain["cols"]["state"] != 3)
     np.testing.assert_array_equal(moved["cols"]["_rng_state"][active], two_draws(plain["cols"]["_rng_state"][active]))
+    np.testing.assert_array_equal(moved["cols"]["_rng_state"][~entered], plain["cols"]["_rng_state"][~entered])
     nec = live & (plain["cols"]["state"] == 3)
     assert nec.any()
     np.testing.assert_array_equal(moved["cols"]["_rng_state"][nec], plain["cols"]["_rng_state"][nec])
