@@ -263,6 +263,13 @@ int olc_set_mechanics(OlcSim* sim, const OlcMechanics* spec);
  * _gpu_backend.py:365-367 — here the host packs it by key). */
 int olc_bind_tissue(OlcSim* sim, const void* cols_dev, int n_cols, size_t stride_bytes);
 
+/* Pinned voxels of an FP32 field: after every substep the voxels idx_dev[0..n)
+ * (x-fastest indices, a caller-owned device array) hold `value` — the engine's
+ * vessel mask (engine/assets/shaders/tumor_sim.wgsl:366-380 marks voxels inside
+ * the vessel cylinder, and every diffusion pass stores them as 1.0, :430-433).
+ * n = 0 removes the pins.  Solo handles. */
+int olc_set_pinned(OlcSim* sim, int index, const uint32_t* idx_dev, uint32_t n, float value);
+
 /* Tissue grid that tissue rules update: two buffers laid out as in
  * olc_bind_tissue; a tissue rule reads the current one and writes the other
  * (the reference's Tissue_In / Tissue_Out,
@@ -558,6 +565,11 @@ int olc_stage_bin_ranges(const uint32_t* sorted_keys_dev, uint32_t n, uint32_t n
  * after use). */
 int olc_stage_diffuse(float* f_dev, float* tmp_dev, float* sink_dev, const int32_t dims[3],
                       float dx, float dt, const OlcDiffusion* spec, void* stream);
+
+/* olc_stage_diffuse with pinned voxels (olc_set_pinned's rule). */
+int olc_stage_diffuse_pinned(float* f_dev, float* tmp_dev, float* sink_dev, const int32_t dims[3], float dx,
+                             float dt, const OlcDiffusion* spec, const uint32_t* idx_dev, uint32_t n, float value,
+                             void* stream);
 
 /* One step of one 16-bit field (reaction with compensation, then S
  * substeps), result in f_dev; f_dev, tmp_dev hold BF16/FP16 elements, comp_dev

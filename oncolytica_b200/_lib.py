@@ -49,6 +49,7 @@ EXPORTS = (
     "olc_arena_create", "olc_arena_alloc", "olc_arena_release", "olc_arena_stats", "olc_arena_destroy",
     "olc_engine_metrics", "olc_get_step_state", "olc_set_step_state", "olc_set_mechanics",
     "olc_stage_contact_mech", "olc_stage_contact_motion", "olc_bind_tissue_pair", "olc_current_tissue", "olc_set_rule_iterations",
+    "olc_set_pinned", "olc_stage_diffuse_pinned",
 )
 
 
@@ -297,6 +298,9 @@ _SIGS = {
     "olc_get_step_state": (C.c_int, [_VP, C.POINTER(OlcStepState), _VP]),
     "olc_set_mechanics": (C.c_int, [_VP, C.POINTER(OlcMechanics)]),
     "olc_bind_tissue_pair": (C.c_int, [_VP, _VP, _VP, C.c_int, C.c_size_t]),
+    "olc_set_pinned": (C.c_int, [_VP, C.c_int, _VP, C.c_uint32, C.c_float]),
+    "olc_stage_diffuse_pinned": (C.c_int, [_VP, _VP, _VP, C.POINTER(C.c_int32 * 3), C.c_float, C.c_float,
+                                           C.POINTER(OlcDiffusion), _VP, C.c_uint32, C.c_float, _VP]),
     "olc_stage_contact_motion": (C.c_int, [_VP, _VP, C.c_uint32, C.POINTER(OlcGeom), C.POINTER(OlcContact),
                                            C.POINTER(OlcMechanics), _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP,
                                            C.c_float, _VP, _VP, _VP, _VP]),

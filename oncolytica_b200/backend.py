@@ -159,6 +159,19 @@ class CudaBackend:
             ct.stiffness, ct.mobility = contact.stiffness, contact.mobility
             ct.max_disp, ct.margin = contact.max_disp, contact.margin
         self._check(self.lib.olc_set_contact(self.handle, C.byref(ct)))
+        self.pins_dev = None
+        if eng._vessel is not None:
+            _, _, _, value, names = eng._vessel
+            if names is None:
+                names = [n for n in L.chem_fields
+                         if n in eng._diffusion and STORAGE_CODES[eng._diffusion[n].storage] == 0]
+            idx = eng.vessel_voxels()
+            self.pins_dev = self.torch.from_numpy(idx.view(np.int32).copy()).to(self.device)
+            for name in names:
+                if name not in L.chem_fields:
+                    raise ValueError(f"setup_vessel: no chemistry field {name!r}")
+                self._check(self.lib.olc_set_pinned(self.handle, L.chem_fields.index(name),
+                                                    C.c_void_p(self.pins_dev.data_ptr()), len(idx), value))
         if contact is not None and contact.mechanics:
             m = _lib.OlcMechanics()
             m.enabled = 1
@@ -359,6 +372,10 @@ class CudaBackend:
                 host[:, 0, :] = host[:, -1, :] = b
                 host[:, :, 0] = host[:, :, -1] = b
             flat = np.ascontiguousarray(host.ravel(order="F"))
+            if eng._vessel is not None and spec_d is not None and (eng._vessel[4] is None or name in eng._vessel[4]) \
+                    and STORAGE_CODES[spec_d.storage] == 0:
+                flat = flat.copy()
+                flat[eng.vessel_voxels()] = np.float32(eng._vessel[3])
             cur = (fb >> i) & 1
             # 16-bit fields: torch rounds to nearest even on the copy
             self.fields_dev[i][cur].copy_(torch.from_numpy(flat))

@@ -1083,8 +1083,22 @@ static bool launch_pair(const FieldMaps& m, int cur, float* out, const FieldStep
     return false;
 }
 
+// Pinned voxels (the engine's vessel mask): after a substep, the listed
+// voxels of its output hold the pin value.
+__global__ void __launch_bounds__(256) k_pin(float* __restrict__ f, const olc_u32* __restrict__ idx, olc_u32 n,
+                                             float value) {
+    for (olc_u32 k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) f[idx[k]] = value;
+}
+
+void launch_pins(float* f, const Pins* pins, cudaStream_t s) {
+    if (!pins || pins->n == 0) return;
+    olc_u32 blocks = (pins->n + 255) / 256;
+    if (blocks > 148 * 4) blocks = 148 * 4;
+    k_pin<<<blocks, 256, 0, s>>>(f, pins->idx, pins->n, pins->value);
+}
+
 float* run_substeps_tma(float* a, float* b, const FieldMaps& m, int a_index, const FieldStep& fs, olc_u32* status,
-                        cudaStream_t s) {
+                        cudaStream_t s, const Pins* pins) {
     float* bufs[2];
     bufs[a_index] = a;
     bufs[1 - a_index] = b;
@@ -1094,15 +1108,17 @@ float* run_substeps_tma(float* a, float* b, const FieldMaps& m, int a_index, con
     const char* order = getenv("OLC_STENCIL_ORDER");
     const bool alternate = !(order && std::string(order) == "forward");
     int launch = 0;
+    const bool pinned = pins && pins->n > 0;  // pins go between substeps: one substep per launch
     while (left > 0) {
         const int rev = alternate ? (launch & 1) : 0;
-        if (m.T2Y > 0 && left >= 2 && launch_pair(m, cur, bufs[1 - cur], fs, status, rev, s)) {
+        if (!pinned && m.T2Y > 0 && left >= 2 && launch_pair(m, cur, bufs[1 - cur], fs, status, rev, s)) {
             left -= 2;
-        } else if (m.T > 1 && left >= m.T) {
+        } else if (!pinned && m.T > 1 && left >= m.T) {
             launch_block(m, m.block[cur], bufs[1 - cur], fs, status, s);
             left -= m.T;
         } else {
             launch_single(m, cur, bufs[1 - cur], fs, status, rev, s);
+            launch_pins(bufs[1 - cur], pins, s);
             left -= 1;
         }
         cur = 1 - cur;
@@ -1146,11 +1162,12 @@ void launch_substep(const float* in, float* out, const FieldStep& fs, cudaStream
                                                        fs.inv_decay, fs.bval);
 }
 
-float* run_substeps(float* a, float* b, const FieldStep& fs, cudaStream_t s) {
+float* run_substeps(float* a, float* b, const FieldStep& fs, cudaStream_t s, const Pins* pins) {
     float* cur = a;
     float* nxt = b;
     for (int i = 0; i < fs.substeps; ++i) {
         launch_substep(cur, nxt, fs, s);
+        launch_pins(nxt, pins, s);
         float* t = cur;
         cur = nxt;
         nxt = t;
@@ -1158,12 +1175,13 @@ float* run_substeps(float* a, float* b, const FieldStep& fs, cudaStream_t s) {
     return cur;
 }
 
-float* run_field_step(float* a, float* b, float* sink, const FieldStep& fs, cudaStream_t s) {
+float* run_field_step(float* a, float* b, float* sink, const FieldStep& fs, cudaStream_t s, const Pins* pins) {
     launch_sink(a, sink, fs, s);
     float* cur = a;
     float* nxt = b;
     for (int i = 0; i < fs.substeps; ++i) {
         launch_substep(cur, nxt, fs, s);
+        launch_pins(nxt, pins, s);
         float* t = cur;
         cur = nxt;
         nxt = t;

@@ -109,11 +109,19 @@ struct FieldStep {
 bool make_field_step(const OlcDiffusion& d, const int dims[3], float dx, float dt, FieldStep* out,
                      std::string* err);
 void launch_sink(float* f, float* sink, const FieldStep& fs, cudaStream_t s);
+// Voxels held at a value after every substep (x-fastest indices, device memory).
+struct Pins {
+    const olc_u32* idx;
+    olc_u32 n;
+    float value;
+};
+void launch_pins(float* f, const Pins* pins, cudaStream_t s);
 void launch_substep(const float* in, float* out, const FieldStep& fs, cudaStream_t s);
 // Runs sink + S substeps starting from a; returns the buffer holding the result.
-float* run_field_step(float* a, float* b, float* sink, const FieldStep& fs, cudaStream_t s);
+float* run_field_step(float* a, float* b, float* sink, const FieldStep& fs, cudaStream_t s,
+                      const Pins* pins = nullptr);
 // The S substeps alone.
-float* run_substeps(float* a, float* b, const FieldStep& fs, cudaStream_t s);
+float* run_substeps(float* a, float* b, const FieldStep& fs, cudaStream_t s, const Pins* pins = nullptr);
 // TMA tile path (x extent must be a multiple of 4): tensor maps of both
 // buffers for the single-substep kernel and for the T-substep temporal block.
 struct FieldMaps {
@@ -131,7 +139,7 @@ struct FieldMaps {
 bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3]);
 // Runs fs.substeps substeps starting from a (buffer index a_index of m).
 float* run_substeps_tma(float* a, float* b, const FieldMaps& m, int a_index, const FieldStep& fs, olc_u32* status,
-                        cudaStream_t s);
+                        cudaStream_t s, const Pins* pins = nullptr);
 int launches_for(const FieldMaps& m, int substeps);
 // OLC_STENCIL=plain in the environment selects the register-column kernel.
 bool stencil_tma_enabled();

@@ -71,6 +71,7 @@ struct OlcSim {
     FieldMaps fmaps[OLC_MAX_FIELDS];           // TMA descriptors of both buffers
     FieldMaps16 fmaps16[OLC_MAX_FIELDS];       // the same for 16-bit storage
     float* comp[OLC_MAX_FIELDS] = {};          // 16-bit storage: reaction residual per voxel (FP32)
+    Pins pins[OLC_MAX_FIELDS] = {};            // voxels held at a value after every substep
 
     OlcContact contact = {};
     ContactDev contact_dev = {};
@@ -355,11 +356,15 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
         float* a = s->field[cur][f];
         float* b = s->field[1 - cur][f];
         const bool tma_path = s->fmaps[f].ok && stencil_tma_enabled();
-        float* res = tma_path ? run_substeps_tma(a, b, s->fmaps[f], cur, s->fstep[f], s->counters + OLC_CTR_STATUS, st)
-                              : run_substeps(a, b, s->fstep[f], st);
+        const Pins* pins = s->pins[f].n ? &s->pins[f] : nullptr;
+        float* res = tma_path ? run_substeps_tma(a, b, s->fmaps[f], cur, s->fstep[f], s->counters + OLC_CTR_STATUS, st,
+                                                 pins)
+                              : run_substeps(a, b, s->fstep[f], st, pins);
         s->field_cur[f] = (res == a) ? cur : 1 - cur;
         substeps += (uint32_t)s->fstep[f].substeps;
-        launches += (uint64_t)(tma_path ? launches_for(s->fmaps[f], s->fstep[f].substeps) : s->fstep[f].substeps);
+        launches += (uint64_t)(pins ? 2 * s->fstep[f].substeps
+                                    : (tma_path ? launches_for(s->fmaps[f], s->fstep[f].substeps)
+                                                : s->fstep[f].substeps));
     }
     mark(s, 2, st);
     // 2. grid + compaction
@@ -1237,6 +1242,21 @@ int olc_bind_tissue(OlcSim* s, const void* cols, int n_cols, size_t stride_bytes
     s->tissue_cur = 0;
     s->tissue_cols = n_cols;
     s->tissue_stride = stride_bytes;
+    return OLC_OK;
+}
+
+int olc_set_pinned(OlcSim* s, int index, const uint32_t* idx_dev, uint32_t n, float value) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (s->n_sims) return fail(s, OLC_ERR_STATE, "olc_set_pinned: solo handles only");
+    if (index < 0 || index >= (int)s->caps.n_fields || !s->field_bound[index])
+        return fail(s, OLC_ERR_ARG, "olc_set_pinned: field not bound");
+    if (n && !idx_dev) return fail(s, OLC_ERR_ARG, "olc_set_pinned: null index list");
+    if (n && s->fstep[index].storage != OLC_FIELD_F32)
+        return fail(s, OLC_ERR_ARG, "olc_set_pinned: FP32 fields only");
+    drop_graphs(s);
+    s->pins[index].idx = idx_dev;
+    s->pins[index].n = n;
+    s->pins[index].value = value;
     return OLC_OK;
 }
 
@@ -2301,6 +2321,33 @@ int olc_stage_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], 
         cudaMemcpyAsync(f, res, bytes, cudaMemcpyDeviceToDevice, st);
     }
     return cuda_status(cudaGetLastError(), "olc_stage_diffuse");
+}
+
+int olc_stage_diffuse_pinned(float* f, float* tmp, float* sink, const int32_t dims[3], float dx, float dt,
+                             const OlcDiffusion* spec, const uint32_t* idx, uint32_t n, float value, void* stream) {
+    if (!f || !tmp || !dims || !spec || (n && !idx))
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse_pinned: null argument");
+    if (spec->storage != OLC_FIELD_F32) return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse_pinned: FP32 only");
+    std::string err;
+    FieldStep fs;
+    if (!make_field_step(*spec, dims, dx, dt, &fs, &err))
+        return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse_pinned: " + err);
+    cudaStream_t st = as_stream(stream);
+    Pins pins = {idx, n, value};
+    FieldMaps maps;
+    olc_u32* status = stage_status_word();
+    float* res;
+    if (stencil_tma_enabled() && status && make_field_maps(&maps, f, tmp, dims)) {
+        launch_sink(f, spec->has_sink ? sink : nullptr, fs, st);
+        res = run_substeps_tma(f, tmp, maps, 0, fs, status, st, &pins);
+    } else {
+        res = run_field_step(f, tmp, spec->has_sink ? sink : nullptr, fs, st, &pins);
+    }
+    if (res != f) {
+        const size_t bytes = (size_t)dims[0] * dims[1] * dims[2] * 4;
+        cudaMemcpyAsync(f, res, bytes, cudaMemcpyDeviceToDevice, st);
+    }
+    return cuda_status(cudaGetLastError(), "olc_stage_diffuse_pinned");
 }
 
 int olc_stage_diffuse16(void* f, void* tmp, float* sink, float* comp, const int32_t dims[3], float dx, float dt,

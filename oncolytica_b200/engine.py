@@ -16,6 +16,8 @@ from __future__ import annotations
 
 import inspect
 import math
+
+import numpy as np
 from dataclasses import dataclass
 from typing import Any, Optional, Type
 
@@ -110,6 +112,7 @@ class Engine:
         self._cell_rules: list = []
         self._metric_rules: list = []
         self._diffusion: dict[str, DiffusionSpec] = {}
+        self._vessel: tuple | None = None
         self._contact: Optional[ContactSpec] = None
         self._tissue_class = None
         self._chem_class = None
@@ -229,6 +232,32 @@ class Engine:
                                     state, table, species_field,
                                     tuple(chemotactic_fields) if chemotactic_fields is not None else (None, None),
                                     float(chemo_force), float(motility_impulse))
+
+    def setup_vessel(self, center: tuple[float, float], radius: float, value: float = 1.0,
+                     fields: tuple | None = None) -> None:
+        """The engine's vessel (engine/assets/shaders/tumor_sim.wgsl:366-380,
+        430-433): chemistry voxels whose centre lies within `radius` of the
+        axis parallel to y through (x, z) = `center` are held at `value` after
+        every diffusion substep of `fields` (default: every FP32 diffusing
+        field)."""
+        if radius <= 0.0:
+            raise ValueError("setup_vessel: radius must be positive")
+        self._vessel = (float(center[0]), float(center[1]), float(radius), float(value),
+                        tuple(fields) if fields is not None else None)
+
+    def vessel_voxels(self) -> np.ndarray:
+        """x-fastest indices of the chemistry voxels inside the vessel."""
+        cx, cz, r, _, _ = self._vessel
+        nx, ny, nz = (int(v) for v in self.chemistry_shape)
+        dx = float(self.chemistry_voxel_size)
+        lo = self.domain_lo or (0.0, 0.0, 0.0)
+        xs = lo[0] + (np.arange(nx) + 0.5) * dx
+        zs = lo[2] + (np.arange(nz) + 0.5) * dx
+        inside = (xs[None, :] - cx) ** 2 + (zs[:, None] - cz) ** 2 <= r * r  # [z][x]
+        z, x = np.nonzero(inside)
+        y = np.arange(ny)
+        idx = (z[:, None] * ny + y[None, :]) * nx + x[:, None]
+        return np.sort(idx.ravel()).astype(np.uint32)
 
     def setup_domain(self, lo: tuple[float, float, float], hi: tuple[float, float, float]) -> None:
         self.domain_lo = tuple(float(v) for v in lo)

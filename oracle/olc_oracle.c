@@ -177,6 +177,16 @@ void orc_bin_ranges(const uint32_t* keys, uint32_t n, uint32_t n_bins, uint32_t*
  * (7-point Laplacian, Dirichlet faces), substeps as chemistry_rule(iterations=S). */
 int orc_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], float dx, float dt, float D,
                 float decay, float boundary, int substeps, int nthreads) {
+    return orc_diffuse_pinned(f, tmp, sink, dims, dx, dt, D, decay, boundary, substeps, NULL, 0, 0.0f, nthreads);
+}
+
+/* orc_diffuse with pinned voxels: after every substep the voxels listed in
+ * `pins` (x-fastest indices) hold `pin_value` — the engine's vessel mask
+ * (engine/assets/shaders/tumor_sim.wgsl:366-380, 430-433: voxels inside the
+ * vessel cylinder are stored as 1.0 by every diffusion pass). */
+int orc_diffuse_pinned(float* f, float* tmp, float* sink, const int32_t dims[3], float dx, float dt, float D,
+                       float decay, float boundary, int substeps, const uint32_t* pins, uint32_t n_pins,
+                       float pin_value, int nthreads) {
     const int nx = dims[0], ny = dims[1], nz = dims[2];
     const int nt = nthreads_or_all(nthreads);
     if (substeps < 1) return -1;
@@ -220,6 +230,7 @@ int orc_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], float 
                     nxt[v] = o > 0.0f ? o : 0.0f;
                 }
             }
+        for (uint32_t k = 0; k < n_pins; ++k) nxt[pins[k]] = pin_value;
         float* t = cur;
         cur = nxt;
         nxt = t;

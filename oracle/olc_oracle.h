@@ -50,6 +50,9 @@ void orc_bin_ranges(const uint32_t* keys, uint32_t n, uint32_t n_bins, uint32_t*
 /* tumor_sim.wgsl:387-446: sink then S substeps; result in f. Returns 0 or -1 when unstable. */
 int orc_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], float dx, float dt, float D,
                 float decay, float boundary, int substeps, int nthreads);
+int orc_diffuse_pinned(float* f, float* tmp, float* sink, const int32_t dims[3], float dx, float dt, float D,
+                       float decay, float boundary, int substeps, const uint32_t* pins, uint32_t n_pins,
+                       float pin_value, int nthreads);
 /* The storage roundings of the 16-bit fields, element-wise: storage 1/2
  * round to nearest even (BF16 / FP16), 3/4 stochastically with rnd[i]'s bits
  * (BF16: low 16, FP16: low 13), 5 = FP16 toward zero.  For tests. */

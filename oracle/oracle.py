@@ -41,6 +41,9 @@ def lib() -> C.CDLL:
         L.orc_diffuse.restype = C.c_int
         L.orc_diffuse.argtypes = [P, P, P, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
                                   C.c_int]
+        L.orc_diffuse_pinned.restype = C.c_int
+        L.orc_diffuse_pinned.argtypes = [P, P, P, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
+                                         P, C.c_uint32, C.c_float, C.c_int]
         L.orc_contact.argtypes = [P, P, C.c_uint32, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
                                   P, P, P, P, P, C.c_int]
         L.orc_contact_mech.argtypes = [P, P, C.c_uint32, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
@@ -126,6 +129,22 @@ def diffuse(f: np.ndarray, sink: np.ndarray | None, dx: float, dt: float, D: flo
                            C.c_float(decay), C.c_float(boundary), substeps, nthreads)
     if rc != 0:
         raise ValueError("oracle diffuse: unstable or bad arguments")
+    return f
+
+
+def diffuse_pinned(f: np.ndarray, sink, dx, dt, D, decay, boundary, substeps, pins, pin_value,
+                   nthreads: int = 0) -> np.ndarray:
+    """orc_diffuse_pinned on a (nz, ny, nx) float32 grid; returns the new grid."""
+    f = np.ascontiguousarray(f, dtype=np.float32).copy()
+    tmp = np.zeros_like(f)
+    s = None if sink is None else np.ascontiguousarray(sink, dtype=np.float32).copy()
+    dims = np.array(f.shape[::-1], dtype=np.int32)
+    pv = np.ascontiguousarray(pins, dtype=np.uint32)
+    rc = lib().orc_diffuse_pinned(_p(f), _p(tmp), _p(s), _p(dims), C.c_float(dx), C.c_float(dt), C.c_float(D),
+                                  C.c_float(decay), C.c_float(boundary), substeps, _p(pv), len(pv),
+                                  C.c_float(pin_value), nthreads)
+    if rc != 0:
+        raise ValueError("orc_diffuse_pinned: unstable or bad arguments")
     return f
 
 

@@ -264,6 +264,33 @@ def test_diffuse_plain_and_tma_paths_agree(cuda, olc, monkeypatch, dims):
         np.testing.assert_array_equal(out, ref, err_msg=str(mode))
 
 
+def test_diffuse_pinned_voxels_bit_exact(cuda, olc):
+    """Pinned voxels (the engine's vessel mask): a cylinder of voxels held at
+    1.0 after every substep, on the TMA path, against orc_diffuse_pinned."""
+    import torch
+
+    rng = np.random.default_rng(12)
+    nx, ny, nz = 64, 40, 48
+    f = rng.random((nz, ny, nx), dtype=np.float32) * np.float32(0.5)
+    zz, xx = np.meshgrid(np.arange(nz), np.arange(nx), indexing="ij")
+    inside = (xx + 0.5 - 30.0) ** 2 + (zz + 0.5 - 20.0) ** 2 <= 6.0 ** 2
+    z, x = np.nonzero(inside)
+    pins = np.sort(((z[:, None] * ny + np.arange(ny)[None, :]) * nx + x[:, None]).ravel()).astype(np.uint32)
+    spec = _lib.OlcDiffusion(diffusion=1.0, decay=0.02, boundary=0.4, substeps=7, has_sink=0, storage=0)
+    fd = to_dev(f.ravel(), cuda)
+    tmp = torch.zeros_like(fd)
+    pd = to_dev(pins, cuda)
+    dims_c = (C.c_int32 * 3)(nx, ny, nz)
+    _lib.check(olc.olc_stage_diffuse_pinned(dptr(fd), dptr(tmp), None, C.byref(dims_c), 1.0, 0.5, C.byref(spec),
+                                            dptr(pd), len(pins), 1.0, None))
+    ref = oracle.diffuse_pinned(f, None, 1.0, 0.5, 1.0, 0.02, 0.4, 7, pins, 1.0)
+    got = to_host(fd).reshape(nz, ny, nx)
+    np.testing.assert_array_equal(got, ref)
+    assert np.all(got.ravel()[pins] == 1.0)
+    plain = oracle.diffuse(f, None, dx=1.0, dt=0.5, D=1.0, decay=0.02, boundary=0.4, substeps=7)
+    assert np.abs(got - plain).max() > 0.1  # the vessel feeds its neighbourhood
+
+
 # ------------------------------------------------------------------ contact
 
 def test_contact_bit_exact(cuda, olc):

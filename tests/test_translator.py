@@ -259,3 +259,17 @@ class RandSim(ol.Simulation[RTissue, GChem, GCell, GMetrics, GParams]):
 def test_voxel_rules_have_no_rng():
     with pytest.raises(ol.CompilationError, match="no RNG state"):
         _translate_all(RandSim, tissue_shape=(20, 20, 20), vs=2.0)
+
+
+def test_vessel_voxels_are_the_cylinder():
+    import numpy as np
+
+    eng = ol.Engine(backend="cuda", max_agents=16)
+    eng.setup_geometry((20, 20, 20), 5.0)  # chemistry 10^3 voxels of 10 um
+    eng.setup_vessel(center=(42.0, 57.0), radius=12.0)
+    idx = eng.vessel_voxels()
+    nx, ny, nz = eng.chemistry_shape
+    want = [(z * ny + y) * nx + x for z in range(nz) for y in range(ny) for x in range(nx)
+            if (x * 10.0 + 5.0 - 42.0) ** 2 + (z * 10.0 + 5.0 - 57.0) ** 2 <= 144.0]
+    assert idx.tolist() == sorted(want) and len(want) > 0
+    assert idx.dtype == np.uint32
