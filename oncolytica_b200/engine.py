@@ -235,18 +235,19 @@ class Engine:
 
     def setup_vessel(self, center: tuple[float, float], radius: float, value: float = 1.0,
                      fields: tuple | None = None) -> None:
-        """The engine's vessel (engine/assets/shaders/tumor_sim.wgsl:366-380,
-        430-433): chemistry voxels whose centre lies within `radius` of the
-        axis parallel to y through (x, z) = `center` are held at `value` after
-        every diffusion substep of `fields` (default: every FP32 diffusing
-        field)."""
+        """The engine's vessel (engine/assets/shaders/tumor_sim.wgsl:375-385,
+        425-428): interior chemistry voxels whose centre lies within `radius`
+        of the axis parallel to y through (x, z) = `center` are held at
+        `value` after every diffusion substep of `fields` (default: every FP32
+        diffusing field).  Face voxels keep the Dirichlet boundary value, as
+        the engine tests the faces before the vessel."""
         if radius <= 0.0:
             raise ValueError("setup_vessel: radius must be positive")
         self._vessel = (float(center[0]), float(center[1]), float(radius), float(value),
                         tuple(fields) if fields is not None else None)
 
     def vessel_voxels(self) -> np.ndarray:
-        """x-fastest indices of the chemistry voxels inside the vessel."""
+        """x-fastest indices of the interior chemistry voxels inside the vessel."""
         cx, cz, r, _, _ = self._vessel
         nx, ny, nz = (int(v) for v in self.chemistry_shape)
         dx = float(self.chemistry_voxel_size)
@@ -254,8 +255,10 @@ class Engine:
         xs = lo[0] + (np.arange(nx) + 0.5) * dx
         zs = lo[2] + (np.arange(nz) + 0.5) * dx
         inside = (xs[None, :] - cx) ** 2 + (zs[:, None] - cz) ** 2 <= r * r  # [z][x]
+        inside[[0, -1], :] = False
+        inside[:, [0, -1]] = False
         z, x = np.nonzero(inside)
-        y = np.arange(ny)
+        y = np.arange(1, ny - 1)
         idx = (z[:, None] * ny + y[None, :]) * nx + x[:, None]
         return np.sort(idx.ravel()).astype(np.uint32)
 

@@ -269,7 +269,12 @@ def test_vessel_voxels_are_the_cylinder():
     eng.setup_vessel(center=(42.0, 57.0), radius=12.0)
     idx = eng.vessel_voxels()
     nx, ny, nz = eng.chemistry_shape
-    want = [(z * ny + y) * nx + x for z in range(nz) for y in range(ny) for x in range(nx)
+    want = [(z * ny + y) * nx + x for z in range(1, nz - 1) for y in range(1, ny - 1) for x in range(1, nx - 1)
             if (x * 10.0 + 5.0 - 42.0) ** 2 + (z * 10.0 + 5.0 - 57.0) ** 2 <= 144.0]
     assert idx.tolist() == sorted(want) and len(want) > 0
     assert idx.dtype == np.uint32
+    # a vessel across a corner of the grid: its face voxels stay Dirichlet
+    eng.setup_vessel(center=(5.0, 5.0), radius=25.0)
+    v = eng.vessel_voxels().astype(np.int64)
+    x, y, z = v % nx, v // nx % ny, v // (nx * ny)
+    assert len(v) > 0 and x.min() == 1 and z.min() == 1 and y.min() == 1 and y.max() == ny - 2
