@@ -278,3 +278,42 @@ def test_vessel_voxels_are_the_cylinder():
     v = eng.vessel_voxels().astype(np.int64)
     x, y, z = v % nx, v // nx % ny, v // (nx * ny)
     assert len(v) > 0 and x.min() == 1 and z.min() == 1 and y.min() == 1 and y.max() == ny - 2
+
+
+_REFERENCE_GBM = "/root/reference/framework/examples/gbm_model.py"
+
+
+@pytest.mark.skipif(not __import__("os").path.exists(_REFERENCE_GBM), reason="no reference checkout here")
+def test_reference_gbm_example_translates(tmp_path, monkeypatch):
+    """The reference's own example model (framework/examples/gbm_model.py),
+    with only its import line pointed at this package: its set-up runs through
+    this Engine's API (setup_geometry keywords, tissue/chemistry sample(),
+    cells.add), and its chemistry rule (helper methods looping over .cells and
+    .neighbors, tuple returns), cell rule (neighbours, divide with keyword
+    constructor, die, log/atan2/cos/sin) and metric rule translate to kernels
+    that NVRTC compiles.  Read from the reference checkout when it is present;
+    the model is not part of this repository."""
+    import importlib
+    import random
+    import sys
+
+    src = open(_REFERENCE_GBM, encoding="utf-8").read()
+    assert "import oncolytica as ol" in src
+    (tmp_path / "ref_gbm_model.py").write_text(src.replace("import oncolytica as ol", "import oncolytica_b200 as ol"))
+    monkeypatch.syspath_prepend(str(tmp_path))
+    G = importlib.import_module("ref_gbm_model")
+    try:
+        random.seed(42)
+        eng = ol.Engine(backend="cuda")
+        eng.setup_geometry(tissue_shape=(40, 40, 2), tissue_voxel_size=15.0, cell_diameter=10.0)
+        eng.setup_tissue(G.BrainTissue)
+        eng.setup_chemistry(G.BrainChem)
+        G._init_tissue(eng)
+        G._init_chemistry(eng)
+        G._init_cells(eng)
+        assert len(eng.cells) == 100 and tuple(eng.chemistry_shape) == (20, 20, 1)
+        prog = _translate_all(G.MultiscaleGBM, tissue_shape=(40, 40, 2), vs=15.0)
+        assert sorted(k for k, _ in prog.kernels) == ["Kernel_CellRule_0", "Kernel_ChemRule_0", "Kernel_MetricRule_0"]
+        _nvrtc_ok(prog)
+    finally:
+        sys.modules.pop("ref_gbm_model", None)
