@@ -320,6 +320,37 @@ def test_tumour_step_parity_with_oracle(cuda):
     assert all(v > 0 for v in seen.values()), seen
 
 
+def test_empty_and_extinct_populations(cuda):
+    """No agents at all, and a population that the drug kills within one step
+    (death_k * drug far above 1): steps run eagerly and from CUDA graphs, rows,
+    life flags and both fields follow the oracle's steps bit for bit, the dead
+    leave at the next sort, and the step status stays clean with zero rows."""
+    import oracle
+
+    base = _parity_spec()
+    for spec in (W.scaled(base, n_agents=0), W.scaled(base, n_agents=2000, death_k=1.0e6)):
+        eng = W.build_engine(spec)
+        be = eng._backend_impl
+        for step in range(4):
+            eng.set_graphs(step >= 2)
+            snap = be.snapshot()
+            orc = oracle.TumourOracle.from_snapshot(spec, snap, spec.capacity)
+            eng.run_step(collect_metrics=True)
+            orc.step(nthreads=4)
+            got = be.snapshot()
+            n = got["rows"]
+            assert n == orc.rows, (spec.n_agents, step)
+            np.testing.assert_array_equal(got["life"], orc.dead[:n])
+            np.testing.assert_array_equal(got["fields"]["o2"], orc.o2.ravel())
+            np.testing.assert_array_equal(got["fields"]["drug"], orc.drug.ravel())
+            if spec.n_agents and step == 0:
+                assert n == spec.n_agents and got["life"].all()  # every agent died in the first step
+        c = be.counters()
+        assert got["rows"] == 0 and c["status"] == 0 and c["births"] == 0
+        assert eng.get_engine_metrics()["total_live"] == 0
+        eng.close()
+
+
 def test_engine_mechanics_path_in_the_step(cuda):
     """The step's contact stage through k_contact_mech (OlcMechanics enabled
     with the plain law's parameters: necrotic factor 1, no adhesion,
@@ -436,6 +467,37 @@ def test_vessel_holds_its_voxels(cuda):
     np.testing.assert_array_equal(o2_graphs, o2)
     _, o2_plain = run(False, False)
     assert o2.sum() > o2_plain.sum()
+
+
+def test_plain_small_full_size_step_parity(cuda):
+    """The plain workload at its own size (10,000 agents in a 256 um domain,
+    one 64^3 O2 field with 79 substeps, 10 um bins decoupled from the field
+    grid): five steps, each from the device state, against the oracle: rows,
+    life flags and the integer and volume columns bit-exact, the field and the
+    pending sink bit-exact, positions to 1e-4 um."""
+    import oracle
+
+    spec = W.PLAIN_SMALL
+    eng = W.build_engine(spec)
+    be = eng._backend_impl
+    births = 0
+    for step in range(5):
+        snap = be.snapshot()
+        orc = oracle.TumourOracle.from_snapshot(spec, snap, spec.capacity)
+        eng.run_step()
+        orc.step(nthreads=4)
+        got = be.snapshot()
+        n = got["rows"]
+        assert n == orc.rows, step
+        np.testing.assert_array_equal(got["life"], orc.dead[:n])
+        for col, key in (("state", "state"), ("_rng_state", "rng"), ("volume", "volume"), ("radius", "radius")):
+            np.testing.assert_array_equal(got["cols"][col], orc.bufs[key][:n], err_msg=f"{col} step {step}")
+        for a, key in (("pos.x", "x"), ("pos.y", "y"), ("pos.z", "z")):
+            np.testing.assert_allclose(got["cols"][a], orc.bufs[key][:n], rtol=0, atol=1e-4)
+        np.testing.assert_array_equal(got["fields"]["o2"], orc.o2.ravel())
+        np.testing.assert_array_equal(got["sinks"]["o2"], orc.o2_sink.ravel())
+        births += int(orc.t.births)
+    assert spec.n_agents == 10_000 and tuple(spec.field_dims) == (64, 64, 64) and births > 0
 
 
 def test_tumour_long_run_statistics(cuda):
