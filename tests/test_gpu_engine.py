@@ -500,6 +500,40 @@ def test_plain_small_full_size_step_parity(cuda):
     assert spec.n_agents == 10_000 and tuple(spec.field_dims) == (64, 64, 64) and births > 0
 
 
+def test_scale_workload_full_size_step_parity(cuda):
+    """The scale workload at its own size (1,000,000 agents in a 400 um ball,
+    two 256^3 fields with 83 + 21 substeps, 100^3 bins and 21-bit keys): two
+    steps, each from the device state, against the oracle on every host
+    thread: rows, life flags, integer and volume columns, both fields and the
+    pending sink bit-exact, positions to 1e-4 um."""
+    import os
+
+    import oracle
+
+    spec = W.SCALE
+    eng = W.build_engine(spec)
+    be = eng._backend_impl
+    threads = max(1, os.cpu_count() or 1)
+    for step in range(2):
+        snap = be.snapshot()
+        orc = oracle.TumourOracle.from_snapshot(spec, snap, spec.capacity)
+        eng.run_step()
+        orc.step(nthreads=threads)
+        got = be.snapshot()
+        n = got["rows"]
+        assert n == orc.rows, step
+        np.testing.assert_array_equal(got["life"], orc.dead[:n])
+        for col, key in (("state", "state"), ("_rng_state", "rng"), ("volume", "volume"), ("radius", "radius")):
+            np.testing.assert_array_equal(got["cols"][col], orc.bufs[key][:n], err_msg=f"{col} step {step}")
+        for a, key in (("pos.x", "x"), ("pos.y", "y"), ("pos.z", "z")):
+            np.testing.assert_allclose(got["cols"][a], orc.bufs[key][:n], rtol=0, atol=1e-4)
+        np.testing.assert_array_equal(got["fields"]["o2"], orc.o2.ravel())
+        np.testing.assert_array_equal(got["fields"]["drug"], orc.drug.ravel())
+        np.testing.assert_array_equal(got["sinks"]["o2"], orc.o2_sink.ravel())
+    assert n >= spec.n_agents * 0.9 and tuple(spec.field_dims) == (256, 256, 256)
+    eng.close()
+
+
 def test_tumour_long_run_statistics(cuda):
     """Independent 60-step runs (GPU vs oracle, same seed): population counts
     within 1 % and radial profiles within 3 % of the live count."""
