@@ -91,3 +91,39 @@ def test_field_error_against_fp64(cuda, olc, storage):
             assert rel_l2 <= REL_L2[storage], (storage, D, rel_l2)
         # the field moved: uptake and decay acted (not rounded away)
         assert np.abs(ref - init).max() > 0.05
+
+
+# storage code -> (relative L2, L-infinity) bounds after 1,000 steps of a 64^3
+# field (the length of the scale workload's run).  Measured on B200 (relative
+# L2 / max / mean absolute): FP32 1.6e-7 / 1.2e-6 / 8.1e-8; BF16-SR 2.0e-3 /
+# 8.6e-3 / 1.4e-3; FP16-SR 2.5e-4 / 9.8e-4 / 1.8e-4.
+LONG_BOUNDS = {0: (1e-6, 1e-5), 3: (5e-3, 2e-2), 4: (1e-3, 2e-3)}
+_LONG_REF: dict = {}
+
+
+@pytest.mark.parametrize("storage", [0, 3, 4])
+def test_field_error_after_1000_steps(cuda, olc, storage):
+    """The precision claim over a full run: 1,000 steps of a 64^3 O2-like
+    field (uptake in a ball, Dirichlet faces, 79 substeps) against the FP64
+    oracle; FP16 with stochastic rounding holds the relative L2 error to 1e-3."""
+    import os
+
+    shape, K = _problem(n=64, seed=9)
+    steps, dx, dt, D = 1000, 4.0, 0.1, 2000.0
+    S = int(np.ceil(6.0 * D * dt / (dx * dx)))
+    got = _run_gpu(olc, cuda, storage, shape, K, D, 0.0, 1.0, 1.0, S, dx, dt, steps)
+    if "ref" not in _LONG_REF:  # the FP64 run is the same for every storage
+        ref = np.ones(shape, np.float64)
+        threads = max(1, os.cpu_count() or 1)
+        for _ in range(steps):
+            ref = oracle.diffuse_f64(ref, K, dx, dt, D, 0.0, 1.0, S, nthreads=threads)
+        _LONG_REF["ref"] = ref
+    ref = _LONG_REF["ref"]
+    err = np.abs(got - ref)
+    rel_l2 = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    print(f"storage {storage} 1000 steps 64^3: rel-L2 {rel_l2:.3e} max {err.max():.3e} mean {err.mean():.3e} "
+          f"moved {np.abs(ref - 1.0).max():.3f}")
+    l2_bound, linf = LONG_BOUNDS[storage]
+    assert rel_l2 <= l2_bound, (storage, rel_l2)
+    assert err.max() <= linf, (storage, err.max())
+    assert np.abs(ref - 1.0).max() > 0.05
