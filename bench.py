@@ -226,6 +226,22 @@ def run_reference(args) -> None:
 
 # ------------------------------------------------------------------ GPU arm
 
+def reduce_over_ranks(dist, t):
+    """Combine one rank's ``[seconds_or_ms, units...]`` float64 tensor over all ranks.
+
+    Returns ``(slowest time, t)`` where the time is the MAX of ``t[0]`` over ranks and ``t``
+    now holds the SUM over ranks of every entry (its units are the whole job's). Every rank
+    makes the same two collectives in the same order; with ``dist`` None (one rank) ``t`` is
+    returned unchanged.
+    """
+    if dist is None:
+        return float(t[0]), t
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(mx[0]), t
+
+
 def run_b200(args) -> None:
     import torch
 
@@ -295,13 +311,7 @@ def run_b200(args) -> None:
     agent_steps = c1["agent_steps"] - c0["agent_steps"]
     vox = spec.voxel_updates_per_step() * args.steps
     tot = torch.tensor([ms, float(agent_steps), float(vox)], dtype=torch.float64, device=dev)
-    if dist:
-        mx = tot.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-        ms_max = float(mx[0])
-    else:
-        ms_max = float(tot[0])
+    ms_max, tot = reduce_over_ranks(dist, tot)
     total_agent_steps, total_vox = float(tot[1]), float(tot[2])
     value = total_agent_steps / (ms_max / 1e3)
 
@@ -332,11 +342,7 @@ def run_b200(args) -> None:
     c3 = be.counters()
     e2e_agents = c3["agent_steps"] - c2["agent_steps"]
     t2 = torch.tensor([e2e_s, float(e2e_agents)], dtype=torch.float64, device=dev)
-    if dist:
-        m2 = t2.clone()
-        dist.all_reduce(m2, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t2, op=dist.ReduceOp.SUM)
-        e2e_s = float(m2[0])
+    e2e_s, t2 = reduce_over_ranks(dist, t2)
     e2e_value = float(t2[1]) / e2e_s
     h2d = len(pack_params(be.layout, params))
     d2h = 4 * max(1, len(be.layout.metrics))
