@@ -150,19 +150,24 @@ def read_traffic(kernel: str, nvox: int) -> int | None:
 
 # ------------------------------------------------------------------ CPU (oracle) timing
 
-def time_oracle_step(spec, orc, nthreads: int = 0, field_sample: int = 2) -> dict:
-    """One bounded sample of a step on the host: the full agent phase, and
-    `field_sample` substeps per field scaled to the full substep count."""
-    t0 = time.perf_counter()
-    orc.agents_part(nthreads)
-    t_agents = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    orc.fields_sample(field_sample, nthreads)
-    t_fields_sample = time.perf_counter() - t0
-    full = spec.S_o2 + (spec.S_drug if spec.has_drug else 0)
-    sample = field_sample * (2 if spec.has_drug else 1)
-    t_fields = t_fields_sample * full / sample
-    return {"t_agents": t_agents, "t_fields": t_fields, "agents": int(orc.rows)}
+def time_oracle_steps(orc, steps: int, nthreads: int = 0) -> dict:
+    """``steps`` whole steps of the C oracle, each timed on the host clock:
+    the field phase with every substep of every field, then the agent phase
+    (sort, rule, contact).  Agent-steps count the live agents at each step's
+    start, as the device counter does."""
+    t_fields = t_agents = 0.0
+    agents = 0
+    for _ in range(steps):
+        n = orc.rows
+        agents += int((orc.dead[:n] == 0).sum())
+        t0 = time.perf_counter()
+        orc.fields(nthreads)
+        t1 = time.perf_counter()
+        orc.agents_part(nthreads)
+        t2 = time.perf_counter()
+        t_fields += t1 - t0
+        t_agents += t2 - t1
+    return {"t_fields": t_fields, "t_agents": t_agents, "agents": agents, "steps": steps}
 
 
 def make_oracle(spec):
@@ -176,18 +181,47 @@ def make_oracle(spec):
     return oracle.TumourOracle(spec, st, o2, drug, spec.capacity)
 
 
-def cpu_baseline(spec, samples: int = 1) -> dict:
+def reference_cpu_backend_record() -> dict | None:
+    """The reference's own CPU backend (pure Python, one core) timed on a
+    small configuration of the plain workload, as recorded by
+    oracle/time_reference_cpu.py where the reference checkout exists (it does
+    not travel with this repository)."""
+    p = os.path.join(REPO, "oracle", "reference_cpu_backend.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        return json.load(fh)
+
+
+def workload_config(spec, world: int = 1) -> dict:
+    """The ``config`` object of a scale/plain_small line; the GPU arm and the
+    reference arm print the same one."""
+    nvox = int(np.prod(spec.field_dims))
+    return {"workload": spec.name, "agents": spec.n_agents, "fields": "o2+drug" if spec.has_drug else "o2",
+            "field_dims": list(spec.field_dims), "substeps": [spec.S_o2, spec.S_drug],
+            "bins": list(spec.tissue_dims), "l2": "inputs larger than L2 (field state "
+            f"{(5 if spec.has_drug else 3) * 4 * nvox / 1e6:.0f} MB)", "parallelism": f"replicas x{world}"}
+
+
+def cpu_baseline(spec, steps: int = 3, warmup: int = 1) -> dict:
+    """The C oracle on every host thread: ``warmup`` untimed then ``steps``
+    timed whole steps of the workload from its initial state (the same
+    procedure as the reference arm, shorter)."""
     orc = make_oracle(spec)
     cores = os.cpu_count() or 1
-    tot_t, tot_a = 0.0, 0
-    for _ in range(samples):
-        r = time_oracle_step(spec, orc)
-        tot_t += r["t_agents"] + r["t_fields"]
-        tot_a += r["agents"]
-    return {"value": tot_a / tot_t, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{samples} step(s) of {spec.name}: full agent phase ({spec.n_agents} agents, sort + rule + "
-                      f"contact) plus 2 substeps per field scaled to {spec.S_o2}+{spec.S_drug} substeps; "
-                      f"C oracle, OpenMP on {cores} threads"}
+    time_oracle_steps(orc, warmup)
+    r = time_oracle_steps(orc, steps)
+    tot = r["t_fields"] + r["t_agents"]
+    out = {"value": r["agents"] / tot, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"{steps} whole step(s) of {spec.name} after {warmup} warm-up step(s): every substep of every "
+                     f"field ({spec.S_o2}+{spec.S_drug}) and the full agent phase ({spec.n_agents} agents at the "
+                     f"start: sort, rule, contact); C oracle, OpenMP on {cores} threads",
+           "seconds": tot, "fields_s_per_step": r["t_fields"] / steps, "agents_s_per_step": r["t_agents"] / steps,
+           "voxel_updates_per_s": spec.voxel_updates_per_step() * steps / r["t_fields"]}
+    rec = reference_cpu_backend_record()
+    if rec is not None:
+        out["reference_cpu_backend"] = rec
+    return out
 
 
 def run_reference(args) -> None:
@@ -199,27 +233,22 @@ def run_reference(args) -> None:
     spec = W.CONFIGS[args.workload]
     orc = make_oracle(spec)
     cores = os.cpu_count() or 1
-    for _ in range(max(0, min(args.warmup, 1))):
-        time_oracle_step(spec, orc)
-    tot_t, tot_a = 0.0, 0
-    for _ in range(args.steps):
-        r = time_oracle_step(spec, orc)
-        tot_t += r["t_agents"] + r["t_fields"]
-        tot_a += r["agents"]
-    value = tot_a / tot_t
-    vox = spec.voxel_updates_per_step() * args.steps / tot_t
+    time_oracle_steps(orc, args.warmup)
+    r = time_oracle_steps(orc, args.steps)
+    tot = r["t_fields"] + r["t_agents"]
+    value = r["agents"] / tot
+    vox = spec.voxel_updates_per_step() * args.steps / tot
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (numpy default_rng, seed 0)",
-            "config": {"workload": spec.name, "agents": spec.n_agents,
-                       "fields": "o2+drug" if spec.has_drug else "o2", "field_dims": list(spec.field_dims),
-                       "substeps": [spec.S_o2, spec.S_drug]},
+            "data": "synthetic (numpy default_rng, seed 0 + rank)", "config": workload_config(spec, world),
             "voxel_updates_per_s": vox,
+            "phases_s_per_step": {"fields": r["t_fields"] / args.steps, "agents": r["t_agents"] / args.steps},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": "each step: the full agent phase plus 2 substeps per field scaled to the "
-                                       "full substep count; C oracle (the reference's algorithm restated; the "
-                                       "reference's own GPU path needs a graphics adapter, unavailable here)"},
+                             "sample": f"{args.steps} whole steps after {args.warmup} warm-up steps, every substep "
+                                       "of every field and the full agent phase, host clock; the C oracle (the "
+                                       "reference's algorithm restated: its own GPU path needs a graphics adapter, "
+                                       "unavailable on this box)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -371,11 +400,7 @@ def run_b200(args) -> None:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (numpy default_rng, seed 0 + rank)",
-        "config": {"workload": spec.name, "agents": spec.n_agents, "fields": "o2+drug" if spec.has_drug else "o2",
-                   "field_dims": list(spec.field_dims), "substeps": [spec.S_o2, spec.S_drug],
-                   "bins": list(spec.tissue_dims), "l2": "inputs larger than L2 (field state "
-                   f"{(5 if spec.has_drug else 3) * 4 * nvox / 1e6:.0f} MB)",
-                   "parallelism": f"replicas x{world}"},
+"config": workload_config(spec, world),
         "voxel_updates_per_s": total_vox / (ms_max / 1e3),
         "agents_end": c1["n_agents"],
         "roofline": {"bound": "hbm", "kernel": "k_substep_x4 (7-point FTCS, FP32, 4-wide rows, TMA tiles)", "achieved": achieved,
@@ -415,9 +440,51 @@ def run_b200(args) -> None:
         line["serving"] = measure_serving(args.rate, args.serve_seconds, seed=0, storage="f16_sr", solo_sample=4)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(spec)
+    line["summary"] = summarise(line)
+    assert_clean(line)
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def assert_clean(line: dict) -> None:
+    """Every device status word a line reports must be 0 (no dropped child,
+    no look-back or TMA wait that gave up, no capacity overflow)."""
+    from oncolytica_b200._lib import status_names
+
+    bad = []
+    if line.get("status"):
+        bad.append(("step", line["status"]))
+    for st, r in (line.get("batched") or {}).items():
+        if r.get("status"):
+            bad.append((f"batched {st}", r["status"]))
+    for st, r in (line.get("precision") or {}).items():
+        if r.get("status"):
+            bad.append((f"precision {st}", r["status"]))
+    if line.get("serving") and line["serving"].get("device_status"):
+        bad.append(("serving", line["serving"]["device_status"]))
+    if bad:
+        raise RuntimeError("device status set: " + "; ".join(f"{w}: {s:#x} {status_names(s)}" for w, s in bad))
+
+
+def summarise(line: dict) -> dict:
+    """The headline figures of a line's nested measurements, short, printed
+    last so that a log that keeps only the end of the line still shows them."""
+    out = {"agent_steps_per_s": line["value"], "e2e": line["e2e"]["value"], "roofline_frac": line["roofline"]["frac"]}
+    if line.get("cpu_baseline"):
+        out["cpu_port"] = line["cpu_baseline"]["value"]
+    for st, r in (line.get("batched") or {}).items():
+        out[f"batched_{st}_vs_plain_fp32"] = round(r["vs_plain_fp32"]["ratio"], 3)
+    for st, r in (line.get("precision") or {}).items():
+        out[f"{st}_ms_per_step"] = round(r["ms_per_step"], 4)
+        if "field_error" in r:
+            out[f"{st}_rel_l2"] = {f: round(e["rel_l2"], 7) for f, e in r["field_error"].items()}
+    if line.get("serving"):
+        sv = line["serving"]
+        out["serving_p50_p99_s"] = [round(sv["ttc_p50_s"], 3), round(sv["ttc_p99_s"], 3)]
+        if "p99_target_s" in sv:
+            out["serving_p99_target_s"] = sv["p99_target_s"]
+    return out
 
 
 def measure_storage(spec, storage: str, steps: int, warmup: int, graphs: bool = True) -> dict:

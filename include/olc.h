@@ -10,7 +10,7 @@
  * drives wgpu directly.  Here the Python backend class
  * oncolytica_b200.backend.CudaBackend implements that protocol and calls the
  * entry points below through ctypes; any other host language binds the same
- * symbols.
+ * symbols (ctypes here; cgo, JNI or any C FFI elsewhere).
  *
  * Conventions
  *   - Every entry point returns an int status: OLC_OK (0) or an OLC_ERR_* code.
@@ -535,8 +535,12 @@ int olc_stage_keys(const float* x_dev, const float* y_dev, const float* z_dev,
  * (onesweep: one upfront digit histogram, then one decoupled-look-back pass
  * per 8-bit digit).  Replaces the counting sort of template.wgsl:165-343.
  * vals_in_dev == NULL means values 0..n-1.  Scratch is caller memory of at
- * least olc_sort_scratch_bytes(n, key_bits) bytes, 256-byte aligned. */
+ * least olc_sort_scratch_bytes(n, key_bits) bytes, 256-byte aligned.  The
+ * sort's status word is the uint32 at byte olc_sort_status_offset() of the
+ * scratch (cleared by each call): OLC_STATUS_TIMEOUT there means a bounded
+ * look-back wait gave up and that call's output is unreliable. */
 size_t olc_sort_scratch_bytes(uint32_t n, int key_bits);
+size_t olc_sort_status_offset(void);
 int olc_stage_sort_pairs(const uint32_t* keys_in_dev, const uint32_t* vals_in_dev,
                          uint32_t* keys_out_dev, uint32_t* vals_out_dev, uint32_t n,
                          int key_bits, void* scratch_dev, size_t scratch_bytes, void* stream);
@@ -547,12 +551,30 @@ int olc_stage_sort_pairs(const uint32_t* keys_in_dev, const uint32_t* vals_in_de
  * argument.  The temporary memory is a file-scope device array of this library
  * (about 9.4 MB, held by every GPU that loads it until exit), so n is limited
  * to 1,048,576 keys (larger n: OLC_ERR_CAPACITY).  All calls share the array:
- * calls whose work overlaps on the GPU race and must be serialised.  The first
- * call on a device looks up the array's address; make it before any stream
- * capture.  Has no counterpart in the reference. */
+ * calls whose work overlaps on the GPU race and must be serialised.  Each
+ * call outside stream capture looks up the array's address on the current
+ * device (a device reset between calls is followed); a call on a capturing
+ * stream reuses the address the last uncaptured call found, so make one call
+ * on a device before capturing.  Has no counterpart in the reference. */
 int olc_stage_sort_pairs_noalloc(const uint32_t* keys_in_dev, const uint32_t* vals_in_dev,
                                  uint32_t* keys_out_dev, uint32_t* vals_out_dev, uint32_t n,
                                  int key_bits, void* stream);
+/* The status word of the last olc_stage_sort_pairs_noalloc call on the
+ * current device, read after `stream` finishes (the call waits for it):
+ * OLC_STATUS_TIMEOUT means a bounded look-back wait gave up and that sort's
+ * output is unreliable (possibly unsorted or with gaps).  Allocates nothing. */
+int olc_sort_noalloc_status(uint32_t* status_out, void* stream);
+
+/* Self-test of the bounded device waits: runs one look-back walk whose
+ * predecessor tile is never published (olc_lookback, as in the sort and the
+ * births) and one TMA-style mbarrier wait whose transaction is never issued
+ * (the wait of the stencil kernels), each with `limit` polls (1..65536), and
+ * returns out[0] = the look-back's status bits, out[1] = the mbarrier wait's
+ * status bits (both OLC_STATUS_TIMEOUT when the waits gave up as designed),
+ * out[2] = the prefix the walk returned (0).  Waits for `stream`; uses a
+ * file-scope device array (allocates nothing).  No counterpart in the
+ * reference. */
+int olc_selftest_bounded_waits(uint32_t limit, uint32_t out[3], void* stream);
 
 /* Bin table from sorted keys: ranges_dev[2k] = first index of key k,
  * ranges_dev[2k+1] = one past the last (both 0 when empty); keys >= n_bins are

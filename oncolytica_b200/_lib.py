@@ -49,7 +49,8 @@ EXPORTS = (
     "olc_arena_create", "olc_arena_alloc", "olc_arena_release", "olc_arena_stats", "olc_arena_destroy",
     "olc_engine_metrics", "olc_get_step_state", "olc_set_step_state", "olc_set_mechanics",
     "olc_stage_contact_mech", "olc_stage_contact_motion", "olc_bind_tissue_pair", "olc_current_tissue", "olc_set_rule_iterations",
-    "olc_set_pinned", "olc_stage_diffuse_pinned",
+    "olc_set_pinned", "olc_stage_diffuse_pinned", "olc_sort_noalloc_status", "olc_sort_status_offset",
+    "olc_selftest_bounded_waits",
 )
 
 
@@ -59,6 +60,83 @@ class OlcError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"libolc error {code}: {message}")
         self.code = code
+
+
+_STATUS_NAMES = ((OLC_STATUS_CAPACITY, "capacity (children dropped: max_agents reached)"),
+                 (OLC_STATUS_TIMEOUT, "timeout (a bounded device wait gave up: results of that step are unreliable)"),
+                 (OLC_STATUS_MULTI_DIVIDE, "multi_divide (a rule called divide() twice in one call)"))
+
+
+def status_names(bits: int) -> str:
+    """The OLC_STATUS_* bits of a device status word, by name."""
+    names = [n for b, n in _STATUS_NAMES if bits & b]
+    rest = bits & ~sum(b for b, _ in _STATUS_NAMES)
+    if rest:
+        names.append(f"unknown bits {rest:#x}")
+    return ", ".join(names) or "clean"
+
+
+class DeviceStatusError(OlcError):
+    """The device status word of a handle gained bits: a capacity overflow
+    (children dropped), a bounded wait that gave up, or a second divide() in
+    one rule call.  Raised by the host after the steps that set them; the
+    error code follows the first bit (OLC_ERR_CAPACITY, OLC_ERR_TIMEOUT,
+    OLC_ERR_STATE)."""
+
+    def __init__(self, bits: int, new_bits: int, where: str):
+        code = (OLC_ERR_TIMEOUT if new_bits & OLC_STATUS_TIMEOUT else
+                OLC_ERR_CAPACITY if new_bits & OLC_STATUS_CAPACITY else OLC_ERR_STATE)
+        super().__init__(code, f"{where}: device status {bits:#x}: {status_names(new_bits)}")
+        self.status = bits
+        self.new_bits = new_bits
+
+
+class StatusWatch:
+    """Checks a handle's sticky device status word every ``every`` steps
+    (one counter read, which waits for the stream) and after every step that
+    already waited for the device (metric collection).  ``policy`` "raise"
+    raises DeviceStatusError when bits appear that were not reported before,
+    "warn" issues a RuntimeWarning instead, "ignore" reads nothing.  Each bit
+    is reported once; the word itself stays sticky (olc_read_counters)."""
+
+    DEFAULT_EVERY = 64
+
+    def __init__(self, read_status, where: str, every: int = DEFAULT_EVERY, policy: str = "raise"):
+        self.read_status = read_status
+        self.where = where
+        self.every = max(1, int(every))
+        self.policy = policy
+        self.seen = 0
+        self.since = 0
+
+    def chunks(self, n: int):
+        """Step counts to enqueue so that no chunk passes a check point."""
+        n = int(n)
+        while n > 0:
+            k = min(n, self.every - self.since) if self.policy != "ignore" else n
+            yield k
+            n -= k
+
+    def after(self, steps: int, synced: bool = False) -> None:
+        self.since += int(steps)
+        if self.policy == "ignore" or (self.since < self.every and not synced):
+            return
+        self.since = 0
+        self.check()
+
+    def check(self) -> int:
+        bits = int(self.read_status())
+        new = bits & ~self.seen
+        self.seen |= bits
+        if new:
+            err = DeviceStatusError(bits, new, self.where)
+            if self.policy == "raise":
+                raise err
+            if self.policy == "warn":
+                import warnings
+
+                warnings.warn(str(err), RuntimeWarning, stacklevel=3)
+        return bits
 
 
 class OlcGeom(C.Structure):
@@ -310,6 +388,9 @@ _SIGS = {
                                          C.POINTER(OlcMechanics), _VP, _VP, _VP, _VP, C.c_float, _VP, _VP, _VP,
                                          _VP]),
     "olc_set_step_state": (C.c_int, [_VP, C.POINTER(OlcStepState), _VP]),
+    "olc_sort_noalloc_status": (C.c_int, [C.POINTER(C.c_uint32), _VP]),
+    "olc_sort_status_offset": (C.c_size_t, []),
+    "olc_selftest_bounded_waits": (C.c_int, [C.c_uint32, C.POINTER(C.c_uint32 * 3), _VP]),
 }
 
 _lock = threading.Lock()

@@ -62,6 +62,8 @@ class CudaBackend:
         self.tissue_pair = None
         self._params_dirty = True
         self._last_reductions: dict | None = None
+        self.status = _lib.StatusWatch(lambda: self.counters()["status"], "CudaBackend.run_steps",
+                                       every=engine.status_check_every, policy=engine.on_device_status)
 
     # ---- helpers -------------------------------------------------------------
     def _check(self, rc: int) -> None:
@@ -243,9 +245,18 @@ class CudaBackend:
         self.run_steps(1, collect_metrics)
 
     def run_steps(self, n: int, collect_metrics: bool = False) -> None:
-        self._check(self.lib.olc_step(self.handle, int(n), int(bool(collect_metrics)), self._stream()))
-        if collect_metrics:
-            self._read_metrics()
+        """n steps; the device status word is checked every
+        ``Engine.status_check_every`` steps and after every collected step
+        (StatusWatch: DeviceStatusError on new bits)."""
+        self.status.every = max(1, int(self.engine.status_check_every))
+        self.status.policy = self.engine.on_device_status
+        chunks = list(self.status.chunks(n))
+        for i, k in enumerate(chunks):
+            last = i == len(chunks) - 1
+            self._check(self.lib.olc_step(self.handle, int(k), int(bool(collect_metrics and last)), self._stream()))
+            if collect_metrics and last:
+                self._read_metrics()
+            self.status.after(k, synced=collect_metrics and last)
 
     def _read_metrics(self) -> None:
         L = self.layout

@@ -53,6 +53,8 @@ class BatchEngine:
         self.max_agents = int(max_agents or sum(e.max_agents for e in self.engines))
         self.use_graphs = False
         self._step = 0
+        self.status = _lib.StatusWatch(lambda: self.counters()["status"], "BatchEngine.run_steps",
+                                       every=e0.status_check_every, policy=e0.on_device_status)
         self._compile()
 
     # ---- set-up ----------------------------------------------------------------
@@ -186,9 +188,13 @@ class BatchEngine:
         self._step += n
         for eng in self.engines:
             eng._step += n
-        self._check(self.lib.olc_step(self.handle, int(n), int(bool(collect_metrics)), self._stream()))
-        if collect_metrics:
-            self._read_metrics()
+        chunks = list(self.status.chunks(n))
+        for i, k in enumerate(chunks):
+            last = i == len(chunks) - 1
+            self._check(self.lib.olc_step(self.handle, int(k), int(bool(collect_metrics and last)), self._stream()))
+            if collect_metrics and last:
+                self._read_metrics()
+            self.status.after(k, synced=collect_metrics and last)
 
     def run_step(self, collect_metrics: bool = False) -> None:
         self.run_steps(1, collect_metrics)

@@ -25,7 +25,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
 SOURCES = ["olc_grid.cu", "olc_field.cu", "olc_field16.cu", "olc_contact.cu", "olc_reduce.cu", "olc_batch.cu", "olc_sim.cu",
-           "olc_noalloc.cu", "olc_pool.cu", "olc_metrics.cu"]
+           "olc_noalloc.cu", "olc_pool.cu", "olc_metrics.cu", "olc_selftest.cu"]
 HEADERS = ["olc_device.cuh", "olc_rule_rt.cuh", "olc_internal.h", "olc_store16.cuh", "olc_arena.h", "olc_stencil.cuh"]
 
 # -fmad=false keeps a*b+c as two roundings everywhere, so the CPU oracle

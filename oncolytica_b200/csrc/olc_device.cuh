@@ -118,12 +118,14 @@ __device__ __forceinline__ void olc_st_relaxed(olc_u32* p, olc_u32 v) {
 #define OLC_LB_PREFIX 0x80000000u
 #define OLC_LB_MASK   0x3fffffffu
 
-// Waits (bounded) for the tile-`t` word to carry a flag, then returns it.
-__device__ __forceinline__ olc_u32 olc_lb_wait(const olc_u32* word, olc_u32* status) {
+// Waits (bounded: `limit` polls) for the tile-`t` word to carry a flag, then
+// returns it; on expiry it records OLC_ST_TIMEOUT and returns an empty prefix.
+__device__ __forceinline__ olc_u32 olc_lb_wait(const olc_u32* word, olc_u32* status,
+                                               olc_u32 limit = OLC_SPIN_LIMIT) {
     olc_u32 v = olc_ld_relaxed(word);
     olc_u32 spins = 0;
     while ((v & (OLC_LB_AGG | OLC_LB_PREFIX)) == 0u) {
-        if (++spins > OLC_SPIN_LIMIT) {
+        if (++spins > limit) {
             atomicOr(status, OLC_ST_TIMEOUT);
             return OLC_LB_PREFIX;  // count 0, treated as a prefix so the walk ends
         }
@@ -138,7 +140,8 @@ __device__ __forceinline__ olc_u32 olc_lb_wait(const olc_u32* word, olc_u32* sta
 // tiles is `stride` words).  Publishes this tile's aggregate first and its
 // inclusive prefix afterwards.
 __device__ __forceinline__ olc_u32 olc_lookback(olc_u32* words, olc_u32 stride, olc_u32 tile,
-                                                olc_u32 count, olc_u32* status) {
+                                                olc_u32 count, olc_u32* status,
+                                                olc_u32 limit = OLC_SPIN_LIMIT) {
     if (tile == 0) {
         olc_st_relaxed(words, OLC_LB_PREFIX | count);
         return 0;
@@ -147,11 +150,39 @@ __device__ __forceinline__ olc_u32 olc_lookback(olc_u32* words, olc_u32 stride, 
     olc_u32 excl = 0;
     int t = (int)tile - 1;
     while (t >= 0) {
-        olc_u32 v = olc_lb_wait(words + (olc_u64)t * stride, status);
+        olc_u32 v = olc_lb_wait(words + (olc_u64)t * stride, status, limit);
         excl += v & OLC_LB_MASK;
         if (v & OLC_LB_PREFIX) break;
         --t;
     }
     olc_st_relaxed(words + (olc_u64)tile * stride, OLC_LB_PREFIX | (excl + count));
     return excl;
+}
+
+// ---------------------------------------------------------------- mbarrier waits
+// One poll of phase `parity` of the shared-memory mbarrier at `bar`.
+__device__ __forceinline__ bool olc_mbar_try_wait(olc_u32 bar, olc_u32 parity) {
+    olc_u32 ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for a TMA tile's mbarrier phase: true once the phase
+// completed.  After `limit` polls the thread records OLC_ST_TIMEOUT, polls up
+// to `limit` more times so that a copy still in flight can land before the
+// block's shared memory is released, and returns false (the caller returns).
+__device__ __forceinline__ bool olc_mbar_wait_bounded(olc_u32 bar, olc_u32 parity, olc_u32* status,
+                                                      olc_u32 limit = OLC_SPIN_LIMIT) {
+    for (olc_u32 it = 0; it < limit; ++it)
+        if (olc_mbar_try_wait(bar, parity)) return true;
+    atomicOr(status, OLC_ST_TIMEOUT);
+    for (olc_u32 it = 0; it < limit && !olc_mbar_try_wait(bar, parity); ++it) {
+    }
+    return false;
 }

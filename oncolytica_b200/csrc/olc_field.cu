@@ -147,17 +147,6 @@ __device__ __forceinline__ olc_u32 smem_u32(const void* p) {
     return static_cast<olc_u32>(__cvta_generic_to_shared(p));
 }
 
-__device__ __forceinline__ bool mbar_try_wait(olc_u32 bar, olc_u32 parity) {
-    olc_u32 ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
 
 __global__ void __launch_bounds__(256) k_substep_tma(const __grid_constant__ CUtensorMap in_map,
                                                      float* __restrict__ out, int nx, int ny, int nz, float r,
@@ -188,22 +177,8 @@ __global__ void __launch_bounds__(256) k_substep_tma(const __grid_constant__ CUt
             "l"(reinterpret_cast<unsigned long long>(&in_map)), "r"(x0 - HX), "r"(y0 - 1), "r"(z0 - 1), "r"(bar_a)
             : "memory");
     }
-    // bounded wait for the tile
-    bool ready = false;
-    for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it) {
-        if (mbar_try_wait(bar_a, 0)) {
-            ready = true;
-            break;
-        }
-    }
-    if (!ready) {
-        if (threadIdx.x == 0) atomicOr(status, OLC_ST_TIMEOUT);
-        // give the copy in flight a second bounded chance to land before the
-        // block's shared memory is released
-        for (olc_u32 it = 0; it < OLC_SPIN_LIMIT && !mbar_try_wait(bar_a, 0); ++it) {
-        }
-        return;
-    }
+    // bounded wait for the tile (olc_mbar_wait_bounded records a timeout)
+    if (!olc_mbar_wait_bounded(bar_a, 0, status)) return;
     const int x = x0 + tx, y = y0 + ty;
     if (x >= nx || y >= ny) return;
     const bool edge_xy = x == 0 || y == 0 || x == nx - 1 || y == ny - 1;
@@ -325,19 +300,8 @@ __global__ void __launch_bounds__(16 * TYR, 1) k_substep_x4(const __grid_constan
             "r"(bar_a)
             : "memory");
     }
-    bool ready = false;
-    for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it) {
-        if (mbar_try_wait(bar_a, 0)) {
-            ready = true;
-            break;
-        }
-    }
-    if (!ready) {
-        if (threadIdx.x == 0) atomicOr(status, OLC_ST_TIMEOUT);
-        for (olc_u32 it = 0; it < OLC_SPIN_LIMIT && !mbar_try_wait(bar_a, 0); ++it) {
-        }
-        return;
-    }
+    // bounded wait for the tile (olc_mbar_wait_bounded records a timeout)
+    if (!olc_mbar_wait_bounded(bar_a, 0, status)) return;
     x4_tile<TYR, TZ>(tile, out, x0, y0, z0, nx, ny, nz, r, inv_decay, bval);
 }
 
@@ -413,7 +377,7 @@ __global__ void __launch_bounds__(16 * TYR, 1) k_substep_pipe(const __grid_const
         const olc_u32 bar = bar0 + 8 * (k % NS), parity = (olc_u32)((k / NS) & 1);
         bool ok = false;
         for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it) {
-            if (mbar_try_wait(bar, parity)) {
+            if (olc_mbar_try_wait(bar, parity)) {
                 ok = true;
                 break;
             }
@@ -426,7 +390,7 @@ __global__ void __launch_bounds__(16 * TYR, 1) k_substep_pipe(const __grid_const
                 const int last = min(mine - 1, k == 0 ? NS - 1 : k + NS - 2);
                 for (int j = k; j <= last; ++j)
                     for (olc_u32 it = 0;
-                         it < OLC_SPIN_LIMIT && !mbar_try_wait(bar0 + 8 * (j % NS), (olc_u32)((j / NS) & 1)); ++it) {
+                         it < OLC_SPIN_LIMIT && !olc_mbar_try_wait(bar0 + 8 * (j % NS), (olc_u32)((j / NS) & 1)); ++it) {
                     }
             }
             return;
@@ -528,7 +492,7 @@ __global__ void __launch_bounds__(T2Shape<TYR, ZC, NS>::THREADS, 1) k_substep_t2
     auto wait_plane = [&](int sidx) -> bool {
         const olc_u32 bar = bar0 + 8 * (sidx % NS), parity = (olc_u32)((sidx / NS) & 1);
         for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it)
-            if (mbar_try_wait(bar, parity)) return true;
+            if (olc_mbar_try_wait(bar, parity)) return true;
         return false;
     };
     if (threadIdx.x == 0)
@@ -644,19 +608,8 @@ __global__ void __launch_bounds__(256) k_substep_tb(const __grid_constant__ CUte
             "r"(bar_a)
             : "memory");
     }
-    bool ready = false;
-    for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it) {
-        if (mbar_try_wait(bar_a, 0)) {
-            ready = true;
-            break;
-        }
-    }
-    if (!ready) {
-        if (threadIdx.x == 0) atomicOr(status, OLC_ST_TIMEOUT);
-        for (olc_u32 it = 0; it < OLC_SPIN_LIMIT && !mbar_try_wait(bar_a, 0); ++it) {
-        }
-        return;
-    }
+    // bounded wait for the tile (olc_mbar_wait_bounded records a timeout)
+    if (!olc_mbar_wait_bounded(bar_a, 0, status)) return;
 
     // levels 1 .. T-1 in shared memory
     const float* src = bufA;

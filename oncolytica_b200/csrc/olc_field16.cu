@@ -30,17 +30,6 @@ __device__ __forceinline__ olc_u32 smem_addr(const void* p) {
     return static_cast<olc_u32>(__cvta_generic_to_shared(p));
 }
 
-__device__ __forceinline__ bool mbar_wait_once(olc_u32 bar, olc_u32 parity) {
-    olc_u32 ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
 
 }  // namespace
 
@@ -227,19 +216,8 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep16(const __grid_constan
             "l"(reinterpret_cast<unsigned long long>(&in_map)), "r"(x0 - HX), "r"(y0 - 1), "r"(z0 - 1), "r"(bar)
             : "memory");
     }
-    bool ready = false;
-    for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it) {
-        if (mbar_wait_once(bar, 0)) {
-            ready = true;
-            break;
-        }
-    }
-    if (!ready) {
-        if (threadIdx.x == 0) atomicOr(status, OLC_ST_TIMEOUT);
-        for (olc_u32 it = 0; it < OLC_SPIN_LIMIT && !mbar_wait_once(bar, 0); ++it) {
-        }
-        return;
-    }
+    // bounded wait for the tile (olc_mbar_wait_bounded records a timeout)
+    if (!olc_mbar_wait_bounded(bar, 0, status)) return;
     t16_tile<ST>(tile, out, x0, y0, z0, nx, ny, nz, r, inv_decay, bval,
                  olc_sr_key(step_ctr ? *step_ctr : step_host, sub, field));
 }
@@ -290,19 +268,8 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep_batch_t16(
             "l"(reinterpret_cast<unsigned long long>(map)), "r"(x0 - HX), "r"(y0 - 1), "r"(z0 - 1), "r"(bar)
             : "memory");
     }
-    bool ready = false;
-    for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it) {
-        if (mbar_wait_once(bar, 0)) {
-            ready = true;
-            break;
-        }
-    }
-    if (!ready) {
-        if (threadIdx.x == 0) atomicOr(status, OLC_ST_TIMEOUT);
-        for (olc_u32 it = 0; it < OLC_SPIN_LIMIT && !mbar_wait_once(bar, 0); ++it) {
-        }
-        return;
-    }
+    // bounded wait for the tile (olc_mbar_wait_bounded records a timeout)
+    if (!olc_mbar_wait_bounded(bar, 0, status)) return;
     t16_tile<ST>(tile, out, x0, y0, z0, d.cdims[0], d.cdims[1], d.cdims[2], fs.r, fs.inv_decay, fs.bval,
                  olc_sr_key(*step_ctr - d.step_base, sub, field));
 }

@@ -19,9 +19,14 @@
 //     words, status word) on the call's stream before using it.  Calls whose
 //     work overlaps on the GPU (other streams, other host threads) race on the
 //     array and must be serialised by the caller;
-//   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current and caches it; make that
-//     first call before any stream capture.
+//   * every call outside stream capture looks up the array's device address
+//     (cudaGetSymbolAddress) with the caller's device current, so a device
+//     reset between calls is followed; a call on a capturing stream uses the
+//     address the last uncaptured call on that device found, so make one
+//     call on a device before capturing any;
+//   * the sort's bounded look-back waits report a timeout in the array's
+//     status word, which olc_sort_noalloc_status reads back: a set
+//     OLC_STATUS_TIMEOUT bit means that call's output is unreliable.
 // No cudaMalloc, cudaFree or allocating library routine is called here.
 #include "olc_internal.h"
 
@@ -50,6 +55,31 @@ static __device__ __align__(256) unsigned char g_noalloc_sort_scratch[kNoAllocBy
 namespace {
 std::mutex g_noalloc_mu;
 void* g_noalloc_addr[kMaxDevices] = {};
+
+// The array's device address on device `dev` (current): looked up afresh
+// unless `st` is capturing, when the address the last uncaptured call found
+// is used (a capture records the address into its graph).
+int noalloc_base(int dev, cudaStream_t st, void** out) {
+    using namespace olc;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+        cudaGetLastError();
+        cs = cudaStreamCaptureStatusActive;  // unknown: do not call into the runtime's symbol table
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (cs == cudaStreamCaptureStatusNone) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_sort_scratch);
+        if (e != cudaSuccess) return cuda_status(e, "olc_stage_sort_pairs_noalloc: cudaGetSymbolAddress");
+        g_noalloc_addr[dev] = p;
+    } else if (!g_noalloc_addr[dev]) {
+        set_error("olc_stage_sort_pairs_noalloc: first call on this device is inside a stream capture; "
+                  "make one call outside capture first");
+        return OLC_ERR_STATE;
+    }
+    *out = g_noalloc_addr[dev];
+    return OLC_OK;
+}
 }  // namespace
 
 extern "C" int olc_stage_sort_pairs_noalloc(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
@@ -76,26 +106,49 @@ extern "C" int olc_stage_sort_pairs_noalloc(const uint32_t* keys_in, const uint3
         set_error("olc_stage_sort_pairs_noalloc: device index out of range");
         return OLC_ERR_ARG;
     }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     void* base = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_addr[dev]) {
-            void* p = nullptr;
-            e = cudaGetSymbolAddress(&p, g_noalloc_sort_scratch);
-            if (e != cudaSuccess) return cuda_status(e, "olc_stage_sort_pairs_noalloc: cudaGetSymbolAddress");
-            g_noalloc_addr[dev] = p;
-        }
-        base = g_noalloc_addr[dev];
-    }
+    const int rc = noalloc_base(dev, st, &base);
+    if (rc != OLC_OK) return rc;
     SortScratch sc;
     if (!carve_sort_scratch(base, kNoAllocBytes, n, key_bits, &sc)) {
         set_error("olc_stage_sort_pairs_noalloc: static scratch layout does not fit");
         return OLC_ERR_STATE;
     }
-    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     e = cudaMemsetAsync(sc.status, 0, 4, st);
     if (e != cudaSuccess) return cuda_status(e, "olc_stage_sort_pairs_noalloc: clear status");
     // run_sort clears the histograms and look-back words before the passes
     run_sort(keys_in, vals_in, keys_out, vals_out, nullptr, n, n, key_bits, sc, false, nullptr, 0, st);
     return cuda_status(cudaGetLastError(), "olc_stage_sort_pairs_noalloc");
+}
+
+extern "C" int olc_sort_noalloc_status(uint32_t* status_out, void* stream) {
+    using namespace olc;
+    if (!status_out) {
+        set_error("olc_sort_noalloc_status: null status_out");
+        return OLC_ERR_ARG;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e, "olc_sort_noalloc_status: cudaGetDevice");
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error("olc_sort_noalloc_status: device index out of range");
+        return OLC_ERR_ARG;
+    }
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    void* base = nullptr;
+    const int rc = noalloc_base(dev, st, &base);
+    if (rc != OLC_OK) return rc;
+    SortScratch sc;
+    if (!carve_sort_scratch(base, kNoAllocBytes, 1, 32, &sc)) {
+        set_error("olc_sort_noalloc_status: static scratch layout does not fit");
+        return OLC_ERR_STATE;
+    }
+    olc_u32 w = 0;
+    e = cudaMemcpyAsync(&w, sc.status, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_status(e, "olc_sort_noalloc_status: read status");
+    // the sort's status bits are the device's OLC_ST_* values (OLC_STATUS_* in olc.h)
+    *status_out = w;
+    return OLC_OK;
 }

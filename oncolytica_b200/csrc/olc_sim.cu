@@ -2272,6 +2272,15 @@ size_t olc_sort_scratch_bytes(uint32_t n, int key_bits) {
     return sort_scratch_bytes(n, key_bits);
 }
 
+size_t olc_sort_status_offset(void) {
+    // carve_sort_scratch's layout: the status word follows the histograms,
+    // the scanned bases and the tile counters, whatever n and key_bits are
+    SortScratch sc;
+    alignas(256) static unsigned char probe[16384];
+    carve_sort_scratch(probe, sizeof(probe), 1, 8, &sc);
+    return (size_t)(reinterpret_cast<unsigned char*>(sc.status) - probe);
+}
+
 int olc_stage_sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, uint32_t n,
                          int key_bits, void* scratch, size_t bytes, void* stream) {
     if (key_bits < 1 || key_bits > 32) return fail(nullptr, OLC_ERR_ARG, "olc_stage_sort_pairs: key_bits in [1, 32]");

@@ -101,6 +101,12 @@ class Engine:
         self.seed: int = 0
         # replay each step as one CUDA graph (same results; fewer launch gaps)
         self.use_graphs: bool = False
+        # device status word (capacity overflow, a bounded wait that gave up,
+        # a second divide() in one call): checked every this many steps and
+        # after every collected step; "raise" (DeviceStatusError), "warn" or
+        # "ignore".  The reference drops overflowing children silently.
+        self.status_check_every: int = 64
+        self.on_device_status: str = "raise"
         self._step = 0
         self.cells = AgentList(self)
         self.tissue: Optional[Grid] = None

@@ -144,6 +144,12 @@ class ServingPool:
         self.steps_run = 0
         self._next_id = 0
         self._inflight: collections.deque = collections.deque()
+        # the device status word (capacity overflow, a bounded wait that gave
+        # up) is read every status_every steps; new bits fail the requests on
+        # the device then (they cannot be attributed to one member)
+        self.status_every = _lib.StatusWatch.DEFAULT_EVERY
+        self._status_seen = 0
+        self._since_status = 0
 
     # ---- requests ---------------------------------------------------------
     def submit(self, req: SimRequest) -> int:
@@ -247,7 +253,34 @@ class ServingPool:
             self._inflight.append(self.device.fence())
             while len(self._inflight) > self.depth:
                 self._inflight.popleft().synchronize()
+            self._since_status += 1
+            if self._since_status >= self.status_every:
+                self._since_status = 0
+                self._check_status()
         return self.poll()
+
+    def _check_status(self) -> None:
+        """Reads the device status word; bits not seen before fail every
+        request whose steps ran since the last check: the residents and the
+        results still being copied out."""
+        read = getattr(self.device, "status", None)
+        if read is None:
+            return
+        bits = int(read())
+        new = bits & ~self._status_seen
+        self._status_seen |= bits
+        if not new:
+            return
+        msg = f"device status {bits:#x} during this request's steps: {_lib.status_names(new)}"
+        for rid, r in list(self.residents.items()):
+            self.device.retire(r.member)
+            self.rows_reserved -= self.device.footprint(r.req).rows
+            del self.residents[rid]
+            self._finish(r.req, "failed", error=msg, admitted=r.admitted, steps=r.done)
+        for r, pending in self.draining:
+            pending.wait()
+            self._finish(r.req, "failed", error=msg, admitted=r.admitted, steps=r.done)
+        self.draining = []
 
     def poll(self, wait: bool = False) -> list[SimResult]:
         out, keep = [], []
@@ -376,6 +409,9 @@ class _PendingResult:
 
     def ready(self) -> bool:
         return self.event.query()
+
+    def wait(self) -> None:
+        self.event.synchronize()
 
     def fill(self, res: SimResult) -> None:
         self.event.synchronize()
@@ -762,6 +798,9 @@ class PoolDevice:
         self._check(self.lib.olc_read_counters(self.handle, C.byref(c), self._s()))
         return {"n_agents": c.n_agents, "status": c.status, "steps": c.steps, "agent_steps": c.agent_steps}
 
+    def status(self) -> int:
+        return self.counters()["status"]
+
     def close(self) -> None:
         if self.handle:
             self.stream.synchronize()
@@ -828,6 +867,10 @@ class FakePoolDevice:
         self.slots: dict[int, tuple] = {}
         self.log: list[tuple] = []
         self.steps = 0
+        self.status_bits = 0  # the device status word a test sets
+
+    def status(self) -> int:
+        return self.status_bits
 
     def capacity(self) -> Footprint:
         return self.cap
@@ -871,6 +914,9 @@ class FakePoolDevice:
         class P:
             def ready(self) -> bool:
                 return True
+
+            def wait(self) -> None:
+                pass
 
             def fill(self, res: SimResult) -> None:
                 res.metrics = {"slot": slot, "steps_at_finish": outer.steps}

@@ -20,6 +20,11 @@ for p in (REPO, os.path.join(REPO, "oracle")):
 
 GOLDEN = os.path.join(REPO, "tests", "golden")
 
+# A checkout of the reference (yankokirill/Oncolytica), used only by the few
+# CPU tests that read its example model: $OLC_REFERENCE, else a directory named
+# "reference" beside this repository; those tests skip when neither exists.
+REFERENCE = os.environ.get("OLC_REFERENCE") or os.path.join(os.path.dirname(REPO), "reference")
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); parity tests through libolc.so")

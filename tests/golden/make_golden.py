@@ -24,7 +24,10 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+# the reference checkout: the first argument, else $OLC_REFERENCE, else a
+# directory named "reference" beside this repository
+REF = (sys.argv[1] if len(sys.argv) > 1 else os.environ.get("OLC_REFERENCE")
+       or os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(HERE))), "reference"))
 REF_SRC = os.path.join(REF, "framework", "src")
 
 

@@ -76,3 +76,49 @@ def test_voxel_rules_with_graphs_match_eager(cuda):
         np.testing.assert_array_equal(sa["fields"][k], sb["fields"][k], err_msg=k)
     for k in sa["tissue"]:
         np.testing.assert_array_equal(sa["tissue"][k], sb["tissue"][k], err_msg=k)
+
+
+class ItTissue(ol.Tissue):
+    pass
+
+
+class ItChem(ol.Chemistry):
+    drug_conc: ol.f32 = 0.0
+
+
+class ItCell(ol.Cell):
+    pos: ol.vec3
+
+
+class ItMetrics(ol.Metrics):
+    pass
+
+
+class ItParams(ol.Params):
+    pass
+
+
+class ItChemSim(ol.Simulation[ItTissue, ItChem, ItCell, ItMetrics, ItParams]):
+    @ol.chemistry_rule(iterations=3)
+    def diffuse(self, chem: ItChem):
+        chem.drug_conc += 1.0  # runs 3 times per step
+
+
+@pytest.mark.parametrize("tissue_shape", [(2, 2, 2), (16, 12, 8)])
+def test_chemistry_rule_iterations_add_three_per_step(cuda, tissue_shape):
+    """The reference's framework/tests/test_oncolytica.py:407-435 on the CUDA
+    path: @chemistry_rule(iterations=3) adding 1.0 runs three times per step,
+    so every chemistry voxel holds 3.0 after one step (and 6.0 after two)."""
+    eng = ol.Engine(backend="cuda", max_agents=64)
+    eng.setup_geometry(tissue_shape=tissue_shape)
+    eng.load_model(ItChemSim())
+    eng.chemistry.column("drug_conc")[...] = 0.0
+    eng.sync_to_device()
+    eng.run_step()
+    eng.sync_to_host()
+    vals = np.asarray(eng.chemistry.column("drug_conc"))
+    assert vals.size == int(np.prod(eng.chemistry_shape)) and vals.size >= 1
+    np.testing.assert_array_equal(vals, np.full(vals.shape, 3.0, np.float32))
+    eng.run_step()
+    eng.sync_to_host()
+    np.testing.assert_array_equal(np.asarray(eng.chemistry.column("drug_conc")), 6.0)

@@ -280,7 +280,9 @@ def test_vessel_voxels_are_the_cylinder():
     assert len(v) > 0 and x.min() == 1 and z.min() == 1 and y.min() == 1 and y.max() == ny - 2
 
 
-_REFERENCE_GBM = "/root/reference/framework/examples/gbm_model.py"
+from conftest import REFERENCE  # noqa: E402
+
+_REFERENCE_GBM = __import__("os").path.join(REFERENCE, "framework", "examples", "gbm_model.py")
 
 
 @pytest.mark.skipif(not __import__("os").path.exists(_REFERENCE_GBM), reason="no reference checkout here")
