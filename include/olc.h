@@ -96,6 +96,8 @@ typedef struct {
     int32_t has_sink;           /* rules deposit uptake rates into this field */
     int32_t storage;            /* OLC_FIELD_F32 (default), OLC_FIELD_BF16 or
                                    OLC_FIELD_F16: element type of the buffers */
+    int32_t encoding;           /* OLC_ENC_*: what a 16-bit element holds
+                                   (0 for FP32 storage)                       */
 } OlcDiffusion;
 
 /* Field storage types (OlcDiffusion.storage).  16-bit storage halves the
@@ -118,6 +120,29 @@ typedef struct {
  * hash bits as OLC_FIELD_BF16_SR).  Unbiased rounding with FP16's 11-bit
  * significand keeps the accumulated field error near 1e-3 of FP64. */
 #define OLC_FIELD_F16_SR  4
+
+/* Encodings of 16-bit field elements (OlcDiffusion.encoding).  Values of an
+ * encoded field stay within [0, boundary] (substep results are clamped to it;
+ * the reference's engine clamps its fields to [0, 1]).  With b = boundary:
+ *   OLC_ENC_VALUE    the element is the value f (any range; results >= 0).
+ *   OLC_ENC_DEFICIT  the element is b - f.  Near the boundary value, where a
+ *                    field like O2 spends its run, the short mantissa then
+ *                    resolves the small deficit instead of a number near b.
+ *                    The 7-point update is linear and the faces hold b, so the
+ *                    substeps run on the deficits unchanged (decay adds the
+ *                    constant b (1 - 1/(1 + lambda dt_sub))).
+ *   OLC_ENC_OFFSET3  the element is f - o, o in {0, b/2, b} the offset nearest
+ *                    f, with o and the sign in the two top bits (bit 15 the
+ *                    sign, bit 14, free in both formats for magnitudes below
+ *                    2, set for o = b/2 with f >= b/2 and for o = b): every
+ *                    value is held to within b/4 of an offset, four times the
+ *                    resolution of OLC_ENC_VALUE near b; for fields spread
+ *                    over [0, b] (a decaying drug).  Needs 0 < b <= 4.
+ * The FP32 residual of 16-bit storage is kept in the encoded domain (the
+ * deficit for OLC_ENC_DEFICIT, the value otherwise). */
+#define OLC_ENC_VALUE     0
+#define OLC_ENC_DEFICIT   1
+#define OLC_ENC_OFFSET3   2
 
 /* Hertz-like contact repulsion (engine/assets/shaders/tumor_sim.wgsl:505-628):
  * for d < r_i + r_j, F += k * delta^(3/2) * (p_i - p_j)/d with
@@ -467,8 +492,11 @@ int olc_create_pool(const OlcPoolConfig* cfg, const OlcCaps* caps, OlcSim** out)
 
 /* Field `index` of every member: a and b hold cfg.field_voxels elements of the
  * storage type (OLC_FIELD_*), sink (FP32, or NULL when no rule deposits into
- * the field) and comp (FP32, 16-bit storage only) as many. */
-int olc_bind_field_pool(OlcSim* sim, int index, void* a, void* b, float* sink, float* comp, int storage);
+ * the field) and comp (FP32, 16-bit storage only) as many.  encoding
+ * (OLC_ENC_*, 16-bit storage only) and, for an encoded field, its boundary
+ * value are the same for every member (olc_pool_admit checks them). */
+int olc_bind_field_pool(OlcSim* sim, int index, void* a, void* b, float* sink, float* comp, int storage,
+                        int encoding, float boundary);
 
 /* Admits one simulation: geometry, specs[n_fields] (specs[f].storage must
  * match the bound storage) and its Params blob (every member's blob has the

@@ -25,6 +25,10 @@ OLC_STATUS_CAPACITY = 0x1
 OLC_STATUS_TIMEOUT = 0x2
 OLC_STATUS_MULTI_DIVIDE = 0x4
 
+OLC_ENC_VALUE = 0
+OLC_ENC_DEFICIT = 1
+OLC_ENC_OFFSET3 = 2
+
 OLC_MAX_AGENT_FIELDS = 64
 OLC_MAX_FIELDS = 8
 OLC_MAX_RULES = 16
@@ -170,6 +174,7 @@ class OlcDiffusion(C.Structure):
         ("substeps", C.c_int32),
         ("has_sink", C.c_int32),
         ("storage", C.c_int32),
+        ("encoding", C.c_int32),
     ]
 
 
@@ -359,7 +364,7 @@ _SIGS = {
     "olc_stage_contact": (C.c_int, [_VP, _VP, C.c_uint32, C.POINTER(OlcGeom), C.POINTER(OlcContact), C.c_float,
                                     _VP, _VP, _VP, _VP]),
     "olc_create_pool": (C.c_int, [C.POINTER(OlcPoolConfig), C.POINTER(OlcCaps), C.POINTER(_VP)]),
-    "olc_bind_field_pool": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, _VP, C.c_int]),
+    "olc_bind_field_pool": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, _VP, C.c_int, C.c_int, C.c_float]),
     "olc_pool_admit": (C.c_int, [_VP, C.POINTER(OlcGeom), C.POINTER(OlcDiffusion), _VP, C.c_size_t,
                                  C.POINTER(C.c_int32), _U64P, _VP]),
     "olc_pool_add_agents": (C.c_int, [_VP, C.c_int32, C.POINTER(_VP), C.c_uint32, _VP]),

@@ -20,6 +20,7 @@ from oncolytica_b200._errors import CompilationError
 from oncolytica_b200._types import metric_fields
 from oncolytica_b200.compiler.emit_cuda import make_layout, pack_params, translate_model
 from oncolytica_b200.engine import STORAGE_CODES
+from oncolytica_b200 import _fieldcodec
 
 # torch element type of each field storage code (OLC_FIELD_F32 / BF16 / F16)
 FIELD_DTYPES = {0: lambda t: t.float32, 1: lambda t: t.bfloat16, 2: lambda t: t.float16, 3: lambda t: t.bfloat16,
@@ -84,7 +85,7 @@ class CudaBackend:
         contact = eng._contact
         radius_field = contact.radius if (contact and isinstance(contact.radius, str)) else None
         self.layout = L = make_layout(spec, radius_field)
-        if eng._cell_rules or eng._metric_rules:
+        if eng._cell_rules or eng._metric_rules or eng._tissue_rules or eng._chemistry_rules:
             self.program = translate_model(sim, L, radius_field)
         cap = eng.max_agents
         tdims = tuple(int(v) for v in eng.tissue_shape)
@@ -122,6 +123,8 @@ class CudaBackend:
         nvox = int(np.prod(cdims))
         sinks = self.program.sink_fields if self.program else set()
         self.comp_dev = []
+        # what each field's 16-bit elements hold (OLC_ENC_*), fixed at load
+        self.field_enc = [eng.field_encoding(name) for name in L.chem_fields]
         for i, name in enumerate(L.chem_fields):
             spec_d = eng._diffusion.get(name)
             storage = STORAGE_CODES[spec_d.storage] if spec_d is not None else 0
@@ -134,6 +137,7 @@ class CudaBackend:
             self.comp_dev.append(comp)
             d = _lib.OlcDiffusion()
             d.storage = storage
+            d.encoding = self.field_enc[i]
             if spec_d is None:
                 if name in sinks:
                     raise ValueError(f"sink_at(...).{name} needs Engine.setup_diffusion({name!r}, ...)")
@@ -388,8 +392,12 @@ class CudaBackend:
                 flat = flat.copy()
                 flat[eng.vessel_voxels()] = np.float32(eng._vessel[3])
             cur = (fb >> i) & 1
-            # 16-bit fields: torch rounds to nearest even on the copy
-            self.fields_dev[i][cur].copy_(torch.from_numpy(flat))
+            dst = self.fields_dev[i][cur]
+            if dst.dtype == torch.float32:
+                dst.copy_(torch.from_numpy(flat))
+            else:  # 16-bit elements of the field's encoding, rounded to nearest even
+                bits = _fieldcodec.encode(flat, self._storage_code(i), self.field_enc[i], self._boundary(i))
+                dst.view(torch.int16).copy_(torch.from_numpy(bits.view(np.int16)))
             if self.fields_dev[i][2] is not None:
                 self.fields_dev[i][2].zero_()
             if self.comp_dev[i] is not None:
@@ -480,14 +488,30 @@ class CudaBackend:
         if self._tissue_rules and eng.tissue is not None and L.tissue_fields:
             self._read_tissue()
 
+    def _storage_code(self, i: int) -> int:
+        spec_d = self.engine._diffusion.get(self.layout.chem_fields[i])
+        return STORAGE_CODES[spec_d.storage] if spec_d is not None else 0
+
+    def _boundary(self, i: int) -> float:
+        spec_d = self.engine._diffusion.get(self.layout.chem_fields[i])
+        return float(spec_d.boundary) if spec_d is not None else 0.0
+
+    def field_codec(self, name: str) -> tuple[int, int, float]:
+        """(storage code, encoding code, boundary value) of a field's elements."""
+        i = self.layout.chem_fields.index(name)
+        return self._storage_code(i), self.field_enc[i], self._boundary(i)
+
     def _field_values(self, i: int, fb: int) -> np.ndarray:
         """Field i as float32 on the host; for 16-bit storage the stored value
-        plus its FP32 rounding residual (what the next reaction continues from)."""
+        plus its FP32 rounding residual (what the next reaction continues from),
+        decoded from the field's encoding."""
         cur = (fb >> i) & 1
         t = self.fields_dev[i][cur]
         if self.comp_dev[i] is None:
             return t.cpu().numpy()
-        return (t.float() + self.comp_dev[i]).cpu().numpy()
+        bits = t.cpu().view(self.torch.int16).numpy().view(np.uint16)
+        return _fieldcodec.decode(bits, self._storage_code(i), self.field_enc[i], self._boundary(i),
+                                  self.comp_dev[i].cpu().numpy())
 
     def _life(self, rows: int) -> np.ndarray:
         buf = (C.c_uint8 * max(rows, 1))()
@@ -537,6 +561,7 @@ class CudaBackend:
             storages.append(str(t.dtype).replace("torch.", ""))
         return {"cols": [[c, np.dtype(dt).name] for c, _, dt in L.cell_cols],
                 "fields": list(L.chem_fields), "field_dtypes": storages,
+                "field_encodings": [int(e) for e in self.field_enc],
                 "sinks": [self.fields_dev[i][2] is not None for i in range(len(L.chem_fields))],
                 "chem_dims": [int(v) for v in self.geom.chem_dims], "tissue_dims": [int(v) for v in self.geom.tissue_dims],
                 "max_agents": int(self.caps.max_agents)}
@@ -592,7 +617,9 @@ class CudaBackend:
             raise ValueError(f"not a checkpoint state: format {sd.get('format')!r}")
         mine = self._layout_signature()
         theirs = sd["layout"]
-        for k in ("cols", "fields", "field_dtypes", "sinks", "chem_dims", "tissue_dims"):
+        theirs = dict(theirs)
+        theirs.setdefault("field_encodings", [0] * len(theirs["fields"]))
+        for k in ("cols", "fields", "field_dtypes", "field_encodings", "sinks", "chem_dims", "tissue_dims"):
             if [list(x) if isinstance(x, (list, tuple)) else x for x in theirs[k]] != \
                     [list(x) if isinstance(x, (list, tuple)) else x for x in mine[k]]:
                 raise ValueError(f"checkpoint does not match this engine: {k} {theirs[k]} != {mine[k]}")

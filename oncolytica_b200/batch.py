@@ -20,6 +20,7 @@ import numpy as np
 from oncolytica_b200 import _lib
 from oncolytica_b200.backend import FIELD_DTYPES, seed_rng
 from oncolytica_b200.engine import STORAGE_CODES
+from oncolytica_b200 import _fieldcodec
 from oncolytica_b200.compiler.emit_cuda import make_layout, pack_params, translate_model
 
 
@@ -114,11 +115,25 @@ class BatchEngine:
         sinks = self.program.sink_fields if self.program else set()
         self.fields_dev = []
         self.comp_dev = []
+        self.field_enc = []
+        self.field_bval = []
         for i, name in enumerate(L.chem_fields):
             kinds = {e._diffusion[name].storage for e in self.engines if name in e._diffusion}
             if len(kinds) > 1:
                 raise ValueError(f"every member of a batch stores field {name!r} with the same type")
             storage = STORAGE_CODES[kinds.pop()] if kinds else 0
+            # what the 16-bit elements hold: one encoding (and, when encoded,
+            # one boundary value) for every member
+            encs = {e.field_encoding(name) for e in self.engines}
+            if len(encs) > 1:
+                raise ValueError(f"members resolve different encodings for field {name!r}; pass "
+                                 "setup_diffusion(encoding=...) explicitly")
+            enc = encs.pop()
+            bvals = {float(e._diffusion[name].boundary) for e in self.engines if name in e._diffusion}
+            if enc and len(bvals) > 1:
+                raise ValueError(f"encoded field {name!r} needs one boundary value for every member")
+            self.field_enc.append(enc)
+            self.field_bval.append(bvals.pop() if bvals else 0.0)
             fdt = FIELD_DTYPES[storage](torch)
             a = torch.zeros(max(nvox, 1), dtype=fdt, device=self.device)
             b = torch.zeros(max(nvox, 1), dtype=fdt, device=self.device)
@@ -131,6 +146,7 @@ class BatchEngine:
                 spec_d = eng._diffusion.get(name)
                 d = specs[k]
                 d.storage = storage
+                d.encoding = enc
                 if spec_d is None:
                     if name in sinks:
                         raise ValueError(f"sink_at(...).{name} needs Engine.setup_diffusion({name!r}, ...)")
@@ -301,7 +317,12 @@ class BatchEngine:
                     host[:, :, 0] = host[:, :, -1] = b
                 flat = np.ascontiguousarray(host.ravel(order="F"))
                 lo, hi = int(self.field_off[k]), int(self.field_off[k + 1])
-                self.fields_dev[i][int(par[k, i])][lo:hi].copy_(torch.from_numpy(flat))
+                dst = self.fields_dev[i][int(par[k, i])][lo:hi]
+                if dst.dtype == torch.float32:
+                    dst.copy_(torch.from_numpy(flat))
+                else:
+                    bits = _fieldcodec.encode(flat, self._storage_code(name), self.field_enc[i], self.field_bval[i])
+                    dst.view(torch.int16).copy_(torch.from_numpy(bits.view(np.int16)))
             if self.fields_dev[i][2] is not None:
                 self.fields_dev[i][2].zero_()
             if self.comp_dev[i] is not None:
@@ -357,9 +378,18 @@ class BatchEngine:
             for i, name in enumerate(L.chem_fields):
                 t = self.fields_dev[i][int(par[k, i])][lo:hi]
                 if self.comp_dev[i] is not None:
-                    t = t.float() + self.comp_dev[i][lo:hi]
-                flat = t.cpu().numpy()
+                    bits = t.cpu().view(self.torch.int16).numpy().view(np.uint16)
+                    flat = _fieldcodec.decode(bits, self._storage_code(name), self.field_enc[i], self.field_bval[i],
+                                              self.comp_dev[i][lo:hi].cpu().numpy())
+                else:
+                    flat = t.cpu().numpy()
                 eng.chemistry.column(name)[...] = flat.reshape(eng.chemistry_shape, order="F")
+
+    def _storage_code(self, name: str) -> int:
+        for e in self.engines:
+            if name in e._diffusion:
+                return STORAGE_CODES[e._diffusion[name].storage]
+        return 0
 
     def close(self) -> None:
         if self.handle:

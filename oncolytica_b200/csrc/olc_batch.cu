@@ -330,7 +330,7 @@ void launch_flip_parity(const FieldStep* steps, int field, int n_fields, olc_u32
 // ------------------------------------------------------------------ 16-bit fields
 // The reaction pass and the reductions on BF16 / FP16 storage
 // (olc_field16.cu's arithmetic).
-template <int ST>
+template <int ST, int EN>
 __global__ void __launch_bounds__(128) k_react_batch16(const uint4* __restrict__ tiles,
                                                        const OlcSimDesc* __restrict__ sims,
                                                        const FieldStep* __restrict__ steps, int field, int n_fields,
@@ -341,6 +341,7 @@ __global__ void __launch_bounds__(128) k_react_batch16(const uint4* __restrict__
     const OlcSimDesc& d = sims[k];
     const FieldStep fs = steps[(size_t)k * n_fields + field];
     if (fs.substeps == 0) return;
+    const EncConst ek = {fs.bval, fs.half_b, fs.quarter_b, fs.upper_q};
     const int nx = d.cdims[0], ny = d.cdims[1], nz = d.cdims[2];
     unsigned short* f = ((fpar[(size_t)k * n_fields + field] & 1u) ? fb : fa) + d.field_off;
     float* K = sink ? sink + d.field_off : nullptr;
@@ -378,11 +379,7 @@ __global__ void __launch_bounds__(128) k_react_batch16(const uint4* __restrict__
             for (int e = 0; e < 4; ++e) {
                 const int x = x0 + e;
                 if (x == 0 || x == nx - 1) continue;
-                float val = __fadd_rn(Store16<ST>::to_f(h[e]), c[e]);
-                if (kv[e] != 0.0f) val = __fdiv_rn(val, __fadd_rn(1.0f, __fmul_rn(kv[e], fs.sink_dt)));
-                val = __fmul_rn(val, fs.decay_step);
-                h[e] = Store16<ST>::from_f(val);
-                c[e] = __fsub_rn(val, Store16<ST>::to_f(h[e]));
+                react_voxel<ST, EN>(h[e], c[e], kv[e], fs, ek);
             }
             *reinterpret_cast<uint2*>(f + v0) =
                 make_uint2((olc_u32)h[0] | ((olc_u32)h[1] << 16), (olc_u32)h[2] | ((olc_u32)h[3] << 16));
@@ -397,19 +394,19 @@ __global__ void __launch_bounds__(128) k_react_batch16(const uint4* __restrict__
                 if (kv != 0.0f) K[v] = 0.0f;
             }
             if (x == 0 || x == nx - 1 || face_yz) continue;
-            float val = __fadd_rn(Store16<ST>::to_f(f[v]), cp[v]);
-            if (kv != 0.0f) val = __fdiv_rn(val, __fadd_rn(1.0f, __fmul_rn(kv, fs.sink_dt)));
-            val = __fmul_rn(val, fs.decay_step);
-            const unsigned short h = Store16<ST>::from_f(val);
+            unsigned short h = f[v];
+            float c = cp[v];
+            react_voxel<ST, EN>(h, c, kv, fs, ek);
             f[v] = h;
-            cp[v] = __fsub_rn(val, Store16<ST>::to_f(h));
+            cp[v] = c;
         }
     }
 }
 
-template <int ST>
+template <int ST, int EN>
 __global__ void __launch_bounds__(128) k_reduce_field_batch16(const uint4* __restrict__ tiles,
-                                                              const OlcSimDesc* __restrict__ sims, int field,
+                                                              const OlcSimDesc* __restrict__ sims,
+                                                              const FieldStep* __restrict__ steps, int field,
                                                               int n_fields, const unsigned char* __restrict__ fpar,
                                                               const unsigned short* fa, const unsigned short* fb,
                                                               const float* comp, OlcReductions* out) {
@@ -420,6 +417,8 @@ __global__ void __launch_bounds__(128) k_reduce_field_batch16(const uint4* __res
     const int nx = d.cdims[0], ny = d.cdims[1], nz = d.cdims[2];
     const unsigned short* f = ((fpar[(size_t)k * n_fields + field] & 1u) ? fb : fa) + d.field_off;
     const float* cp = comp + d.field_off;
+    const FieldStep& fs = steps[(size_t)k * n_fields + field];
+    const EncConst ek = {fs.bval, fs.half_b, fs.quarter_b, fs.upper_q};
     const int x0 = (int)t.y * BT_X + 4 * (threadIdx.x & 7);
     const int y = (int)t.z * BT_Y + (threadIdx.x >> 3);
     const int z0 = (int)t.w * BT_Z;
@@ -429,7 +428,7 @@ __global__ void __launch_bounds__(128) k_reduce_field_batch16(const uint4* __res
         for (int z = z0; z < z1; ++z)
             for (int x = x0; x < x0 + 4; ++x) {
                 const size_t v = ((size_t)z * ny + y) * nx + x;
-                const double val = (double)__fadd_rn(Store16<ST>::to_f(f[v]), cp[v]);
+                const double val = (double)phys_with_residual<ST, EN>(f[v], cp[v], ek);
                 sum += val;
                 mn = fmin(mn, val);
                 mx = fmax(mx, val);
@@ -460,32 +459,29 @@ __global__ void __launch_bounds__(128) k_reduce_field_batch16(const uint4* __res
     }
 }
 
-void launch_react_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
+void launch_react_batch16(const BatchArgs& b, int storage, int encoding, const uint4* tiles, olc_u32 n_tiles,
                           const FieldStep* steps, int field, int n_fields, const unsigned char* fpar, void* fa,
                           void* fb, float* sink, float* comp, cudaStream_t s) {
     if (n_tiles == 0) return;
     unsigned short* a = static_cast<unsigned short*>(fa);
     unsigned short* c = static_cast<unsigned short*>(fb);
-    if (storage != OLC_FIELD_F16 && storage != OLC_FIELD_F16_SR)
-        k_react_batch16<OLC_FIELD_BF16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, a, c,
-                                                                 sink, comp);
-    else
-        k_react_batch16<OLC_FIELD_F16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, a, c,
-                                                                sink, comp);
+    with_storage16(storage, encoding, [&](auto st, auto en) {
+        k_react_batch16<BaseOf<decltype(st)::value>::value, decltype(en)::value>
+            <<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, a, c, sink, comp);
+    });
 }
 
-void launch_reduce_field_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles, int field,
-                                 int n_fields, const unsigned char* fpar, const void* fa, const void* fb,
-                                 const float* comp, OlcReductions* out, cudaStream_t s) {
+void launch_reduce_field_batch16(const BatchArgs& b, int storage, int encoding, const uint4* tiles, olc_u32 n_tiles,
+                                 const FieldStep* steps, int field, int n_fields, const unsigned char* fpar,
+                                 const void* fa, const void* fb, const float* comp, OlcReductions* out,
+                                 cudaStream_t s) {
     if (n_tiles == 0) return;
     const unsigned short* a = static_cast<const unsigned short*>(fa);
     const unsigned short* c = static_cast<const unsigned short*>(fb);
-    if (storage != OLC_FIELD_F16 && storage != OLC_FIELD_F16_SR)
-        k_reduce_field_batch16<OLC_FIELD_BF16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, field, n_fields, fpar, a, c,
-                                                                        comp, out);
-    else
-        k_reduce_field_batch16<OLC_FIELD_F16><<<n_tiles, 128, 0, s>>>(tiles, b.sims, field, n_fields, fpar, a, c,
-                                                                       comp, out);
+    with_storage16(storage, encoding, [&](auto st, auto en) {
+        k_reduce_field_batch16<BaseOf<decltype(st)::value>::value, decltype(en)::value>
+            <<<n_tiles, 128, 0, s>>>(tiles, b.sims, steps, field, n_fields, fpar, a, c, comp, out);
+    });
 }
 
 // ------------------------------------------------------------------ reductions

@@ -87,24 +87,24 @@ __global__ void __launch_bounds__(256) k_contact(const float4* __restrict__ posr
     }
 }
 
-// Field value at (x, y, z) of a chemistry grid in any storage.
-__device__ __forceinline__ float motion_field(const void* f, int type, const int* dims, int x, int y, int z) {
+// Field value at (x, y, z) of a chemistry grid in any storage (type word and
+// boundary value as olc_field_value takes them).
+__device__ __forceinline__ float motion_field(const void* f, int type, float b, const int* dims, int x, int y,
+                                              int z) {
     const olc_u32 v = ((olc_u32)z * (olc_u32)dims[1] + (olc_u32)y) * (olc_u32)dims[0] + (olc_u32)x;
-    if (type == OLC_FIELD_F32) return static_cast<const float*>(f)[v];
-    const unsigned short h = static_cast<const unsigned short*>(f)[v];
-    return (type == OLC_FIELD_F16 || type == OLC_FIELD_F16_SR) ? olc_f16_to_float(h) : olc_bf16_to_float(h);
+    return olc_field_value(f, type, b, v);
 }
 
 // Central-difference gradient 0.5 (f(v + e) - f(v - e)) per axis, the
 // neighbours clamped into the grid.
-__device__ __forceinline__ float3 motion_grad(const void* f, int type, const int* d, int x, int y, int z) {
+__device__ __forceinline__ float3 motion_grad(const void* f, int type, float b, const int* d, int x, int y, int z) {
     const int xm = x > 0 ? x - 1 : 0, xp = x < d[0] - 1 ? x + 1 : d[0] - 1;
     const int ym = y > 0 ? y - 1 : 0, yp = y < d[1] - 1 ? y + 1 : d[1] - 1;
     const int zm = z > 0 ? z - 1 : 0, zp = z < d[2] - 1 ? z + 1 : d[2] - 1;
     return make_float3(
-        __fmul_rn(0.5f, __fsub_rn(motion_field(f, type, d, xp, y, z), motion_field(f, type, d, xm, y, z))),
-        __fmul_rn(0.5f, __fsub_rn(motion_field(f, type, d, x, yp, z), motion_field(f, type, d, x, ym, z))),
-        __fmul_rn(0.5f, __fsub_rn(motion_field(f, type, d, x, y, zp), motion_field(f, type, d, x, y, zm))));
+        __fmul_rn(0.5f, __fsub_rn(motion_field(f, type, b, d, xp, y, z), motion_field(f, type, b, d, xm, y, z))),
+        __fmul_rn(0.5f, __fsub_rn(motion_field(f, type, b, d, x, yp, z), motion_field(f, type, b, d, x, ym, z))),
+        __fmul_rn(0.5f, __fsub_rn(motion_field(f, type, b, d, x, y, zp), motion_field(f, type, b, d, x, y, zm))));
 }
 
 // The engine's full pair law (tumor_sim.wgsl:505-628) over the same
@@ -195,8 +195,8 @@ __global__ void __launch_bounds__(256) k_contact_mech(const float4* __restrict__
                 const int vy = olc_bin_coord(p.y, m.cvs, m.cdims[1]);
                 const int vz = olc_bin_coord(p.z, m.cvs, m.cdims[2]);
                 float3 g0 = make_float3(0.0f, 0.0f, 0.0f), g1 = g0;
-                if (m.f0) g0 = motion_grad(m.f0, m.f0_type, m.cdims, vx, vy, vz);
-                if (m.f1) g1 = motion_grad(m.f1, m.f1_type, m.cdims, vx, vy, vz);
+                if (m.f0) g0 = motion_grad(m.f0, m.f0_type, m.f0_b, m.cdims, vx, vy, vz);
+                if (m.f1) g1 = motion_grad(m.f1, m.f1_type, m.f1_b, m.cdims, vx, vy, vz);
                 const float co2 = m.sp_o2[sp], cglu = m.sp_glu[sp];
                 fx = __fadd_rn(fx, __fmul_rn(__fadd_rn(__fmul_rn(g0.x, co2), __fmul_rn(g1.x, cglu)), m.chemo_force));
                 fy = __fadd_rn(fy, __fmul_rn(__fadd_rn(__fmul_rn(g0.y, co2), __fmul_rn(g1.y, cglu)), m.chemo_force));

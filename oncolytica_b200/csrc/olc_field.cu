@@ -56,6 +56,22 @@ bool make_field_step(const OlcDiffusion& d, const int dims[3], float dx, float d
         *err = "16-bit field storage needs an x extent that is a multiple of 8";
         return false;
     }
+    if (d.encoding < OLC_ENC_VALUE || d.encoding > OLC_ENC_OFFSET3) {
+        *err = "encoding must be OLC_ENC_VALUE, OLC_ENC_DEFICIT or OLC_ENC_OFFSET3";
+        return false;
+    }
+    if (d.encoding != OLC_ENC_VALUE && d.storage == OLC_FIELD_F32) {
+        *err = "encodings apply to 16-bit storage only (FP32 fields use OLC_ENC_VALUE)";
+        return false;
+    }
+    if (d.encoding == OLC_ENC_DEFICIT && !(d.boundary > 0.0f && d.boundary <= 65504.0f)) {
+        *err = "OLC_ENC_DEFICIT needs 0 < boundary <= 65504";
+        return false;
+    }
+    if (d.encoding == OLC_ENC_OFFSET3 && !(d.boundary > 0.0f && d.boundary <= 4.0f)) {
+        *err = "OLC_ENC_OFFSET3 needs 0 < boundary <= 4 (the offset flags use the top two bits)";
+        return false;
+    }
     for (int i = 0; i < 3; ++i) out->dims[i] = dims[i];
     out->r = r;
     out->bval = d.boundary;
@@ -72,6 +88,14 @@ bool make_field_step(const OlcDiffusion& d, const int dims[3], float dx, float d
         out->inv_decay = 1.0f;
         out->decay_step = (float)std::pow(1.0 + (double)d.decay * (double)dts, -(double)d.substeps);
     }
+    // the encodings' constants, each one FP32 operation (the oracle repeats them)
+    const float b = d.boundary;
+    out->encoding = d.encoding;
+    out->dec_sub = b * (1.0f - out->inv_decay);
+    out->dec_step = b * (1.0f - out->decay_step);
+    out->half_b = 0.5f * b;
+    out->quarter_b = 0.25f * b;
+    out->upper_q = b - out->quarter_b;
     return true;
 }
 

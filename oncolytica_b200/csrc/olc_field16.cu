@@ -33,12 +33,23 @@ __device__ __forceinline__ olc_u32 smem_addr(const void* p) {
 
 }  // namespace
 
+// The encoding constants of a field step.
+__host__ __device__ __forceinline__ EncConst enc_const(const FieldStep& fs) {
+    EncConst k;
+    k.b = fs.bval;
+    k.half_b = fs.half_b;
+    k.quarter_b = fs.quarter_b;
+    k.upper_q = fs.upper_q;
+    return k;
+}
+
 // ------------------------------------------------------------------ reaction
-template <int ST>
+template <int ST, int EN>
 __global__ void __launch_bounds__(256) k_react16(unsigned short* __restrict__ f, float* __restrict__ K,
-                                                 float* __restrict__ comp, int nx, int ny, int nz, float dt,
-                                                 float decay_step) {
+                                                 float* __restrict__ comp, const FieldStep fs) {
+    const int nx = fs.dims[0], ny = fs.dims[1], nz = fs.dims[2];
     const size_t nvox = (size_t)nx * ny * nz;
+    const EncConst ek = enc_const(fs);
     const bool aligned = ((reinterpret_cast<uintptr_t>(f) & 7u) | (reinterpret_cast<uintptr_t>(comp) & 15u) |
                           (reinterpret_cast<uintptr_t>(K) & 15u)) == 0u;
     if ((nx & 3) == 0 && aligned) {
@@ -72,11 +83,7 @@ __global__ void __launch_bounds__(256) k_react16(unsigned short* __restrict__ f,
             for (int e = 0; e < 4; ++e) {
                 const int x = x0 + e;
                 if (x == 0 || x == nx - 1) continue;
-                float val = __fadd_rn(Store16<ST>::to_f(h[e]), c[e]);
-                if (kv[e] != 0.0f) val = __fdiv_rn(val, __fadd_rn(1.0f, __fmul_rn(kv[e], dt)));
-                val = __fmul_rn(val, decay_step);
-                h[e] = Store16<ST>::from_f(val);
-                c[e] = __fsub_rn(val, Store16<ST>::to_f(h[e]));
+                react_voxel<ST, EN>(h[e], c[e], kv[e], fs, ek);
             }
             *reinterpret_cast<uint2*>(f + v0) =
                 make_uint2((olc_u32)h[0] | ((olc_u32)h[1] << 16), (olc_u32)h[2] | ((olc_u32)h[3] << 16));
@@ -96,12 +103,11 @@ __global__ void __launch_bounds__(256) k_react16(unsigned short* __restrict__ f,
             if (k != 0.0f) K[v] = 0.0f;
         }
         if (face) continue;
-        float val = __fadd_rn(Store16<ST>::to_f(f[v]), comp[v]);
-        if (k != 0.0f) val = __fdiv_rn(val, __fadd_rn(1.0f, __fmul_rn(k, dt)));
-        val = __fmul_rn(val, decay_step);
-        const unsigned short h = Store16<ST>::from_f(val);
+        unsigned short h = f[v];
+        float c = comp[v];
+        react_voxel<ST, EN>(h, c, k, fs, ek);
         f[v] = h;
-        comp[v] = __fsub_rn(val, Store16<ST>::to_f(h));
+        comp[v] = c;
     }
 }
 
@@ -109,14 +115,10 @@ void launch_react16(void* f, float* sink, float* comp, const FieldStep& fs, cuda
     const size_t nvox = (size_t)fs.dims[0] * fs.dims[1] * fs.dims[2];
     size_t blocks = (nvox + 255) / 256;
     if (blocks > 148 * 16) blocks = 148 * 16;
-    if (fs.storage != OLC_FIELD_F16 && fs.storage != OLC_FIELD_F16_SR)
-        k_react16<OLC_FIELD_BF16><<<(unsigned)blocks, 256, 0, s>>>(static_cast<unsigned short*>(f), sink, comp,
-                                                                    fs.dims[0], fs.dims[1], fs.dims[2], fs.sink_dt,
-                                                                    fs.decay_step);
-    else
-        k_react16<OLC_FIELD_F16><<<(unsigned)blocks, 256, 0, s>>>(static_cast<unsigned short*>(f), sink, comp,
-                                                                   fs.dims[0], fs.dims[1], fs.dims[2], fs.sink_dt,
-                                                                   fs.decay_step);
+    with_storage16(fs.storage, fs.encoding, [&](auto st, auto en) {
+        k_react16<BaseOf<decltype(st)::value>::value, decltype(en)::value>
+            <<<(unsigned)blocks, 256, 0, s>>>(static_cast<unsigned short*>(f), sink, comp, fs);
+    });
 }
 
 // ------------------------------------------------------------------ diffusion substep
@@ -135,37 +137,47 @@ constexpr unsigned BYTES = WX * WY * WZ * 2;
 constexpr size_t SMEM = BYTES + 16 + 128;
 }  // namespace t16
 
+// The working value the Dirichlet faces hold (OLC_ENC_*): the boundary as
+// stored, its deficit 0, or b itself (OLC_ENC_OFFSET3 stores it exactly).
+template <int ST, int EN>
+__device__ __forceinline__ float face_work(float bval) {
+    if (EN == OLC_ENC_DEFICIT) return 0.0f;
+    if (EN == OLC_ENC_OFFSET3) return bval;
+    return Store16<ST>::to_f(Store16<ST>::from_f(bval));
+}
+
 // The 64 x TYR x TZ output block at (x0, y0, z0) from its staged 16-bit box
-// (stochastic-rounding key given).
-template <int ST>
+// (stochastic-rounding key given), on the working values of encoding EN.
+template <int ST, int EN>
 __device__ __forceinline__ void t16_tile(const unsigned short* tile, unsigned short* __restrict__ out, int x0, int y0,
-                                         int z0, int nx, int ny, int nz, float r, float inv_decay, float bval,
-                                         olc_u32 key) {
+                                         int z0, int nx, int ny, int nz, const FieldStep& fs, olc_u32 key) {
     using namespace t16;
     const int g = threadIdx.x & 7, ty = threadIdx.x >> 3;
     const int x = x0 + 8 * g, y = y0 + ty;
     if (x >= nx || y >= ny) return;
+    const EncConst k = enc_const(fs);
+    const float r = fs.r, inv_decay = fs.inv_decay, dec_sub = fs.dec_sub;
     const bool edge_y = y == 0 || y == ny - 1;
     const bool ex0 = x == 0, ex7 = x + 7 == nx - 1;
     constexpr int PS = WY * WX;
     const unsigned short* col = tile + (ty + 1) * WX + HX + 8 * g;
     float zm[8], c[8], zp[8], ym[8], yp[8], v[8];
-    load8<ST>(col, zm);
-    load8<ST>(col + PS, c);
+    load8w<ST, EN>(col, zm, k);
+    load8w<ST, EN>(col + PS, c, k);
     const size_t sz = (size_t)nx * ny;
     unsigned short* o = out + (size_t)z0 * sz + (size_t)y * nx + x;
-    const float bf = Store16<ST>::to_f(Store16<ST>::from_f(bval));  // the face value as stored
+    const float bf = face_work<ST, EN>(fs.bval);
     unsigned long long vi = (unsigned long long)z0 * sz + (unsigned long long)y * nx + x;
 #pragma unroll
     for (int lz = 1; lz <= TZ; ++lz) {
         const int z = z0 + lz - 1;
         if (z >= nz) break;
         const unsigned short* pc = col + lz * PS;
-        load8<ST>(pc + PS, zp);
-        load8<ST>(pc - WX, ym);
-        load8<ST>(pc + WX, yp);
-        const float xl = Store16<ST>::to_f(pc[-1]), xr = Store16<ST>::to_f(pc[8]);
-        stencil_update8_fma(xl, xr, c, ym, yp, zm, zp, r, inv_decay, v);
+        load8w<ST, EN>(pc + PS, zp, k);
+        load8w<ST, EN>(pc - WX, ym, k);
+        load8w<ST, EN>(pc + WX, yp, k);
+        const float xl = Codec<ST, EN>::work(pc[-1], k), xr = Codec<ST, EN>::work(pc[8], k);
+        stencil_update8_enc<EN>(xl, xr, c, ym, yp, zm, zp, r, inv_decay, dec_sub, k.b, v);
         if (edge_y || z == 0 || z == nz - 1) {
 #pragma unroll
             for (int e = 0; e < 8; ++e) v[e] = bf;
@@ -173,7 +185,7 @@ __device__ __forceinline__ void t16_tile(const unsigned short* tile, unsigned sh
             if (ex0) v[0] = bf;
             if (ex7) v[7] = bf;
         }
-        store8_at<ST>(o, v, vi, key);
+        store8w_at<ST, EN>(o, v, vi, key, k);
         o += sz;
         vi += sz;
 #pragma unroll
@@ -184,13 +196,11 @@ __device__ __forceinline__ void t16_tile(const unsigned short* tile, unsigned sh
     }
 }
 
-template <int ST>
+template <int ST, int EN>
 __global__ void __launch_bounds__(t16::THREADS) k_substep16(const __grid_constant__ CUtensorMap in_map,
-                                                           unsigned short* __restrict__ out, int nx, int ny, int nz,
-                                                           float r, float inv_decay, float bval, olc_u32* status,
-                                                           int rev,
-                                                           const olc_u32* step_ctr, olc_u32 step_host, int sub,
-                                                           int field) {
+                                                           unsigned short* __restrict__ out, const FieldStep fs,
+                                                           olc_u32* status, int rev, const olc_u32* step_ctr,
+                                                           olc_u32 step_host, int sub, int field) {
     using namespace t16;
     extern __shared__ unsigned char t16_raw[];
     const olc_u32 pad = (128u - (smem_addr(t16_raw) & 127u)) & 127u;
@@ -218,8 +228,8 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep16(const __grid_constan
     }
     // bounded wait for the tile (olc_mbar_wait_bounded records a timeout)
     if (!olc_mbar_wait_bounded(bar, 0, status)) return;
-    t16_tile<ST>(tile, out, x0, y0, z0, nx, ny, nz, r, inv_decay, bval,
-                 olc_sr_key(step_ctr ? *step_ctr : step_host, sub, field));
+    t16_tile<ST, EN>(tile, out, x0, y0, z0, fs.dims[0], fs.dims[1], fs.dims[2], fs,
+                     olc_sr_key(step_ctr ? *step_ctr : step_host, sub, field));
 }
 
 // ------------------------------------------------------------------ batched substep
@@ -229,7 +239,7 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep16(const __grid_constan
 // stochastic-rounding key counts the member's own steps.
 static_assert(t16::TX == BATCH_T16_TX && t16::TYR == BATCH_T16_TY && t16::TZ == BATCH_T16_TZ, "batched 16-bit tile");
 
-template <int ST>
+template <int ST, int EN>
 __global__ void __launch_bounds__(t16::THREADS) k_substep_batch_t16(
     const uint4* __restrict__ tiles, const OlcSimDesc* __restrict__ sims, const FieldStep* __restrict__ steps,
     const CUtensorMap* __restrict__ maps, int field, int n_fields, const unsigned char* __restrict__ fpar, int sub,
@@ -270,11 +280,11 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep_batch_t16(
     }
     // bounded wait for the tile (olc_mbar_wait_bounded records a timeout)
     if (!olc_mbar_wait_bounded(bar, 0, status)) return;
-    t16_tile<ST>(tile, out, x0, y0, z0, d.cdims[0], d.cdims[1], d.cdims[2], fs.r, fs.inv_decay, fs.bval,
-                 olc_sr_key(*step_ctr - d.step_base, sub, field));
+    t16_tile<ST, EN>(tile, out, x0, y0, z0, d.cdims[0], d.cdims[1], d.cdims[2], fs,
+                     olc_sr_key(*step_ctr - d.step_base, sub, field));
 }
 
-template <int ST>
+template <int ST, int EN>
 static void launch_bt16(const uint4* tiles, olc_u32 n_tiles, const OlcSimDesc* sims, const FieldStep* steps,
                         const CUtensorMap* maps, int field, int n_fields, const unsigned char* fpar, int sub,
                         void* fa, void* fb, const olc_u32* step_ctr, olc_u32* status, cudaStream_t s) {
@@ -283,7 +293,7 @@ static void launch_bt16(const uint4* tiles, olc_u32 n_tiles, const OlcSimDesc* s
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 32 && !(configured_mask & (1 << dev))) {
-        cudaFuncSetAttribute(k_substep_batch_t16<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+        cudaFuncSetAttribute(k_substep_batch_t16<ST, EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
         configured_mask |= 1 << dev;
     }
     cudaLaunchConfig_t cfg = {};
@@ -296,27 +306,19 @@ static void launch_bt16(const uint4* tiles, olc_u32 n_tiles, const OlcSimDesc* s
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_substep_batch_t16<ST>, tiles, sims, steps, maps, field, n_fields, fpar, sub,
+    cudaLaunchKernelEx(&cfg, k_substep_batch_t16<ST, EN>, tiles, sims, steps, maps, field, n_fields, fpar, sub,
                        static_cast<unsigned short*>(fa), static_cast<unsigned short*>(fb), step_ctr, status);
 }
 
-void launch_substep_batch_t16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
+void launch_substep_batch_t16(const BatchArgs& b, int storage, int encoding, const uint4* tiles, olc_u32 n_tiles,
                               const FieldStep* steps, const CUtensorMap* maps, int field, int n_fields,
                               const unsigned char* fpar, int sub, void* fa, void* fb, const olc_u32* step_ctr,
                               olc_u32* status, cudaStream_t s) {
     if (n_tiles == 0) return;
-    if (storage == OLC_FIELD_BF16)
-        launch_bt16<OLC_FIELD_BF16>(tiles, n_tiles, b.sims, steps, maps, field, n_fields, fpar, sub, fa, fb, step_ctr,
-                                    status, s);
-    else if (storage == OLC_FIELD_BF16_SR)
-        launch_bt16<OLC_FIELD_BF16_SR>(tiles, n_tiles, b.sims, steps, maps, field, n_fields, fpar, sub, fa, fb,
-                                       step_ctr, status, s);
-    else if (storage == OLC_FIELD_F16_SR)
-        launch_bt16<OLC_FIELD_F16_SR>(tiles, n_tiles, b.sims, steps, maps, field, n_fields, fpar, sub, fa, fb,
-                                      step_ctr, status, s);
-    else
-        launch_bt16<OLC_FIELD_F16>(tiles, n_tiles, b.sims, steps, maps, field, n_fields, fpar, sub, fa, fb, step_ctr,
-                                   status, s);
+    with_storage16(storage, encoding, [&](auto st, auto en) {
+        launch_bt16<decltype(st)::value, decltype(en)::value>(tiles, n_tiles, b.sims, steps, maps, field, n_fields,
+                                                              fpar, sub, fa, fb, step_ctr, status, s);
+    });
 }
 
 bool make_field_maps16(FieldMaps16* m, void* a, void* b, const int dims[3]) {
@@ -328,7 +330,7 @@ bool make_field_maps16(FieldMaps16* m, void* a, void* b, const int dims[3]) {
     return true;
 }
 
-template <int ST>
+template <int ST, int EN>
 static void launch_sub16(const CUtensorMap& map, void* out, const FieldStep& fs, olc_u32* status, int rev,
                          const olc_u32* step_ctr, olc_u32 step_host, int sub, int field, cudaStream_t s) {
     using namespace t16;
@@ -336,7 +338,7 @@ static void launch_sub16(const CUtensorMap& map, void* out, const FieldStep& fs,
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 32 && !(configured_mask & (1 << dev))) {
-        cudaFuncSetAttribute(k_substep16<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+        cudaFuncSetAttribute(k_substep16<ST, EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
         configured_mask |= 1 << dev;
     }
     cudaLaunchConfig_t cfg = {};
@@ -349,8 +351,8 @@ static void launch_sub16(const CUtensorMap& map, void* out, const FieldStep& fs,
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_substep16<ST>, map, static_cast<unsigned short*>(out), fs.dims[0], fs.dims[1],
-                       fs.dims[2], fs.r, fs.inv_decay, fs.bval, status, rev, step_ctr, step_host, sub, field);
+    cudaLaunchKernelEx(&cfg, k_substep16<ST, EN>, map, static_cast<unsigned short*>(out), fs, status, rev, step_ctr,
+                       step_host, sub, field);
 }
 
 void* run_substeps16(void* a, void* b, const FieldMaps16& m, int a_index, const FieldStep& fs, olc_u32* status,
@@ -360,16 +362,10 @@ void* run_substeps16(void* a, void* b, const FieldMaps16& m, int a_index, const 
     bufs[1 - a_index] = b;
     int cur = a_index;
     for (int i = 0; i < fs.substeps; ++i) {
-        if (fs.storage == OLC_FIELD_BF16)
-            launch_sub16<OLC_FIELD_BF16>(m.map[cur], bufs[1 - cur], fs, status, i & 1, step_ctr, step_host, i, field, s);
-        else if (fs.storage == OLC_FIELD_BF16_SR)
-            launch_sub16<OLC_FIELD_BF16_SR>(m.map[cur], bufs[1 - cur], fs, status, i & 1, step_ctr, step_host, i,
-                                            field, s);
-        else if (fs.storage == OLC_FIELD_F16_SR)
-            launch_sub16<OLC_FIELD_F16_SR>(m.map[cur], bufs[1 - cur], fs, status, i & 1, step_ctr, step_host, i,
-                                           field, s);
-        else
-            launch_sub16<OLC_FIELD_F16>(m.map[cur], bufs[1 - cur], fs, status, i & 1, step_ctr, step_host, i, field, s);
+        with_storage16(fs.storage, fs.encoding, [&](auto st, auto en) {
+            launch_sub16<decltype(st)::value, decltype(en)::value>(m.map[cur], bufs[1 - cur], fs, status, i & 1,
+                                                                   step_ctr, step_host, i, field, s);
+        });
         cur = 1 - cur;
     }
     return bufs[cur];
@@ -379,15 +375,16 @@ void* run_substeps16(void* a, void* b, const FieldMaps16& m, int a_index, const 
 // Mass (FP64 sum of value + residual), minimum and maximum of a 16-bit field;
 // one block partial per block, summed in a fixed order by the last block (as
 // k_reduce_field).
-template <int ST>
+template <int ST, int EN>
 __global__ void __launch_bounds__(256) k_reduce_field16(const unsigned short* __restrict__ f,
                                                         const float* __restrict__ comp, size_t nvox, int slot,
-                                                        OlcReductions* out, double* partials, olc_u32* ticket) {
+                                                        OlcReductions* out, double* partials, olc_u32* ticket,
+                                                        const EncConst ek) {
     __shared__ double s_v[3][8];
     __shared__ bool s_last;
     double sum = 0.0, mn = 1e300, mx = 0.0;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nvox; i += (size_t)gridDim.x * blockDim.x) {
-        const double v = (double)__fadd_rn(Store16<ST>::to_f(f[i]), comp ? comp[i] : 0.0f);
+        const double v = (double)phys_with_residual<ST, EN>(f[i], comp ? comp[i] : 0.0f, ek);
         sum += v;
         mn = fmin(mn, v);
         mx = fmax(mx, v);
@@ -437,10 +434,11 @@ void launch_reduce_field16(const void* f, const float* comp, const FieldStep& fs
     double* part = rs.partials + (size_t)(4 + slot) * RED_MAX_BLOCKS;
     olc_u32* ticket = rs.tickets + 1 + slot;
     const unsigned short* p = static_cast<const unsigned short*>(f);
-    if (fs.storage != OLC_FIELD_F16 && fs.storage != OLC_FIELD_F16_SR)
-        k_reduce_field16<OLC_FIELD_BF16><<<(unsigned)blocks, 256, 0, s>>>(p, comp, nvox, slot, out, part, ticket);
-    else
-        k_reduce_field16<OLC_FIELD_F16><<<(unsigned)blocks, 256, 0, s>>>(p, comp, nvox, slot, out, part, ticket);
+    const EncConst ek = enc_const(fs);
+    with_storage16(fs.storage, fs.encoding, [&](auto st, auto en) {
+        k_reduce_field16<BaseOf<decltype(st)::value>::value, decltype(en)::value>
+            <<<(unsigned)blocks, 256, 0, s>>>(p, comp, nvox, slot, out, part, ticket, ek);
+    });
 }
 
 }  // namespace olc

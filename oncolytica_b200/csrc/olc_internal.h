@@ -105,9 +105,18 @@ struct FieldStep {
     int substeps;
     int storage;       // OLC_FIELD_F32 / OLC_FIELD_BF16 / OLC_FIELD_F16
     float decay_step;  // 16-bit storage: (1 + lambda dt/S)^-S, applied once per step by the reaction
+    // 16-bit encodings (OLC_ENC_*): constants in FP32, computed once on the host
+    int encoding;
+    float dec_sub;     // b * (1 - inv_decay): a deficit substep adds it after the decay factor
+    float dec_step;    // b * (1 - decay_step): a deficit reaction adds it after decay_step
+    float half_b;      // b / 2: the middle offset of OLC_ENC_OFFSET3
+    float quarter_b;   // b / 4: below it OLC_ENC_OFFSET3 uses offset 0
+    float upper_q;     // b - b / 4: above it OLC_ENC_OFFSET3 uses offset b
 };
 bool make_field_step(const OlcDiffusion& d, const int dims[3], float dx, float dt, FieldStep* out,
                      std::string* err);
+// The type word device code reads a field by: storage | (encoding << 8).
+inline int field_type_word(const FieldStep& fs) { return fs.storage | (fs.encoding << 8); }
 void launch_sink(float* f, float* sink, const FieldStep& fs, cudaStream_t s);
 // Voxels held at a value after every substep (x-fastest indices, device memory).
 struct Pins {
@@ -188,7 +197,8 @@ struct MechDev {
     olc_u32* rng;            // null: no motility
     const void* f0;          // O2 (current buffer), or null
     const void* f1;          // glucose, or null
-    int f0_type, f1_type;
+    int f0_type, f1_type;    // field type words (field_type_word)
+    float f0_b, f1_b;        // their boundary values (the encodings' b)
     int cdims[3];
     float cvs;
     float chemo_force, impulse;
@@ -242,7 +252,8 @@ struct EngineMetricArgs {
     const float* speed_z;
     const void* f0;
     const void* f1;
-    int f0_type, f1_type;
+    int f0_type, f1_type;  // field type words (field_type_word)
+    float f0_b, f1_b;
     int cdims[3];
     float cvs;
     const uint2* ranges;
@@ -294,7 +305,7 @@ constexpr int BATCH_T16_TX = 64, BATCH_T16_TY = 16, BATCH_T16_TZ = 8;
 void batch_substep_box(int storage, cuuint32_t box[3]);
 void launch_substep_batch(const BatchArgs& b, const uint4* tiles, olc_u32 n_tiles, const FieldStep* steps, int field,
                           int n_fields, const unsigned char* fpar, int sub, float* fa, float* fb, cudaStream_t s);
-void launch_substep_batch_t16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
+void launch_substep_batch_t16(const BatchArgs& b, int storage, int encoding, const uint4* tiles, olc_u32 n_tiles,
                               const FieldStep* steps, const CUtensorMap* maps, int field, int n_fields,
                               const unsigned char* fpar, int sub, void* fa, void* fb, const olc_u32* step_ctr,
                               olc_u32* status, cudaStream_t s);
@@ -308,12 +319,13 @@ void launch_reduce_field_batch(const BatchArgs& b, const uint4* tiles, olc_u32 n
                                const unsigned char* fpar, const float* fa, const float* fb, OlcReductions* out,
                                cudaStream_t s);
 void launch_reset_reductions_batch(OlcReductions* out, olc_u32 n_sims, cudaStream_t s);
-void launch_react_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles,
+void launch_react_batch16(const BatchArgs& b, int storage, int encoding, const uint4* tiles, olc_u32 n_tiles,
                           const FieldStep* steps, int field, int n_fields, const unsigned char* fpar, void* fa,
                           void* fb, float* sink, float* comp, cudaStream_t s);
-void launch_reduce_field_batch16(const BatchArgs& b, int storage, const uint4* tiles, olc_u32 n_tiles, int field,
-                                 int n_fields, const unsigned char* fpar, const void* fa, const void* fb,
-                                 const float* comp, OlcReductions* out, cudaStream_t s);
+void launch_reduce_field_batch16(const BatchArgs& b, int storage, int encoding, const uint4* tiles, olc_u32 n_tiles,
+                                 const FieldStep* steps, int field, int n_fields, const unsigned char* fpar,
+                                 const void* fa, const void* fb, const float* comp, OlcReductions* out,
+                                 cudaStream_t s);
 
 // ------------------------------------------------------------------ serving pool (olc_pool.cu)
 // Column pointer sets of the row kernels; every column holds 4-byte elements.

@@ -27,10 +27,8 @@ __device__ __forceinline__ olc_u32 em_warp_sum_u(olc_u32 v) {
     return v;
 }
 
-__device__ __forceinline__ float em_sample(const void* f, int type, olc_u32 v) {
-    if (type == OLC_FIELD_F32) return static_cast<const float*>(f)[v];
-    const unsigned short h = static_cast<const unsigned short*>(f)[v];
-    return (type == OLC_FIELD_F16 || type == OLC_FIELD_F16_SR) ? olc_f16_to_float(h) : olc_bf16_to_float(h);
+__device__ __forceinline__ float em_sample(const void* f, int type, float b, olc_u32 v) {
+    return olc_field_value(f, type, b, v);
 }
 
 __global__ void __launch_bounds__(256) k_engine_metrics(EngineMetricArgs a, const olc_u32* counters,
@@ -72,11 +70,11 @@ __global__ void __launch_bounds__(256) k_engine_metrics(EngineMetricArgs a, cons
             const int cz = olc_bin_coord(pz, a.cvs, a.cdims[2]);
             const olc_u32 v = ((olc_u32)cz * (olc_u32)a.cdims[1] + (olc_u32)cy) * (olc_u32)a.cdims[0] + (olc_u32)cx;
             if (a.f0) {
-                const float o2 = em_sample(a.f0, a.f0_type, v);
+                const float o2 = em_sample(a.f0, a.f0_type, a.f0_b, v);
                 sum[5] += (double)o2;
                 if (o2 < a.hypoxia) ++cnt[4];
             }
-            if (a.f1) sum[6] += (double)em_sample(a.f1, a.f1_type, v);
+            if (a.f1) sum[6] += (double)em_sample(a.f1, a.f1_type, a.f1_b, v);
         }
         if (a.speed_x) {
             const double vx = a.speed_x[i], vy = a.speed_y[i], vz = a.speed_z[i];

@@ -90,7 +90,8 @@ struct OlcRuleParams {
     const unsigned char* fpar;
     int n_fields;
     int sim_col;
-    int field_type[OLC_MAX_FIELD_COLS];  // OLC_FIELD_* storage: 0 FP32, 1 BF16, 2 FP16, 3 BF16 (stochastic)
+    int field_type[OLC_MAX_FIELD_COLS];  // OLC_FIELD_* storage | (OLC_ENC_* << 8)
+    float field_bval[OLC_MAX_FIELD_COLS];  // boundary value (the encodings' b)
     // tissue / chemistry rules: the buffers a voxel rule writes; it reads
     // `tissue` and `field` (the state before the rule: every voxel sees its
     // neighbours' previous values)
@@ -105,6 +106,7 @@ struct OlcSimView {
     void* const* out;
     const void* field[OLC_MAX_FIELD_COLS];
     int field_type[OLC_MAX_FIELD_COLS];
+    float field_bval[OLC_MAX_FIELD_COLS];
     float* sink[OLC_MAX_FIELD_COLS];
     const olc_u32* ranges;
     float4* posr;
@@ -129,6 +131,7 @@ __device__ __forceinline__ OlcSimView olc_sim_view(const OlcRuleParams& P, olc_u
         const bool alt = f < P.n_fields && P.fpar[sim * (olc_u32)P.n_fields + f] != 0;
         const unsigned char* base = static_cast<const unsigned char*>(alt ? P.field_alt[f] : P.field[f]);
         V.field_type[f] = P.field_type[f];
+        V.field_bval[f] = P.field_bval[f];
         V.field[f] = base ? base + d.field_off * (P.field_type[f] ? 2u : 4u) : nullptr;
         V.sink[f] = P.sink[f] ? P.sink[f] + d.field_off : nullptr;
     }
@@ -286,15 +289,35 @@ __device__ __forceinline__ float olc_f16_to_float(unsigned short h) {
     return f;
 }
 
+// Value of one 16-bit element of a field with type word t = storage |
+// (encoding << 8) and boundary value b.  Storage 2 and 4 are FP16, 1 and 3
+// BF16; encodings (olc.h OLC_ENC_*): 0 the value, 1 the deficit b - value,
+// 2 the value minus an offset in {0, b/2, b} named by bits 15 and 14.
+__device__ __forceinline__ float olc_field16_value(unsigned short h, int t, float b) {
+    const int st = t & 0xff, en = t >> 8;
+    const bool f16 = st == 2 || st == 4;
+    if (en == 2) {
+        const unsigned short mh = (unsigned short)(h & 0xBFFFu);
+        const float m = f16 ? olc_f16_to_float(mh) : olc_bf16_to_float(mh);
+        const olc_u32 units = (olc_u32)(h >> 15) + (olc_u32)((h >> 14) & 1u);
+        return __fadd_rn(m, __fmul_rn((float)units, __fmul_rn(0.5f, b)));
+    }
+    const float v = f16 ? olc_f16_to_float(h) : olc_bf16_to_float(h);
+    return en == 1 ? __fsub_rn(b, v) : v;
+}
+
+// Value at voxel v of a field in any storage (type word and boundary as above).
+__device__ __forceinline__ float olc_field_value(const void* p, int t, float b, olc_u32 v) {
+    if (t == 0) return static_cast<const float*>(p)[v];
+    return olc_field16_value(static_cast<const unsigned short*>(p)[v], t, b);
+}
+
 // Field value at voxel v of field f, whatever its storage.
 template <class PT>
 __device__ __forceinline__ float olc_field_at(const PT& P, int f, olc_u32 v) {
     const void* p = P.field[f];
     if (!p) return 0.0f;
-    const int t = P.field_type[f];
-    if (t == 0) return static_cast<const float*>(p)[v];
-    const unsigned short h = static_cast<const unsigned short*>(p)[v];
-    return (t == 2 || t == 4) ? olc_f16_to_float(h) : olc_bf16_to_float(h);  // 1 and 3 store BF16
+    return olc_field_value(p, P.field_type[f], P.field_bval[f], v);
 }
 
 // Deposit into a field's sink (sum of first-order uptake rates of a voxel).

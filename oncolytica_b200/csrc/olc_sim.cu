@@ -232,7 +232,8 @@ OlcRuleParams make_rule_params(OlcSim* s, int rule_index, int in_buf) {
     }
     for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
         P.field[f] = s->field[s->field_cur[f]][f];
-        P.field_type[f] = s->fstep[f].storage;
+        P.field_type[f] = field_type_word(s->fstep[f]);
+        P.field_bval[f] = s->fstep[f].bval;
         P.sink[f] = s->sink[f];
     }
     P.ranges = s->ranges;
@@ -263,7 +264,8 @@ OlcRuleParams make_rule_params(OlcSim* s, int rule_index, int in_buf) {
         for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
             P.field[f] = s->field[0][f];
             P.field_alt[f] = s->field[1][f];
-            P.field_type[f] = s->fstep[f].storage;
+            P.field_type[f] = field_type_word(s->fstep[f]);
+            P.field_bval[f] = s->fstep[f].bval;
         }
         P.fpar = s->fpar_dev;
         P.n_fields = (int)s->caps.n_fields;
@@ -281,8 +283,10 @@ void fill_motion(OlcSim* s, const OlcMechanics& mech, int cc, MechDev* m) {
     m->rng = mech.rng_field >= 0 ? static_cast<olc_u32*>(s->col[cc][mech.rng_field]) : nullptr;
     m->f0 = mech.o2_field >= 0 ? s->field[s->field_cur[mech.o2_field]][mech.o2_field] : nullptr;
     m->f1 = mech.glucose_field >= 0 ? s->field[s->field_cur[mech.glucose_field]][mech.glucose_field] : nullptr;
-    m->f0_type = mech.o2_field >= 0 ? s->fstep[mech.o2_field].storage : 0;
-    m->f1_type = mech.glucose_field >= 0 ? s->fstep[mech.glucose_field].storage : 0;
+    m->f0_type = mech.o2_field >= 0 ? field_type_word(s->fstep[mech.o2_field]) : 0;
+    m->f1_type = mech.glucose_field >= 0 ? field_type_word(s->fstep[mech.glucose_field]) : 0;
+    m->f0_b = mech.o2_field >= 0 ? s->fstep[mech.o2_field].bval : 0.0f;
+    m->f1_b = mech.glucose_field >= 0 ? s->fstep[mech.glucose_field].bval : 0.0f;
     for (int i = 0; i < 3; ++i) m->cdims[i] = s->geom.chem_dims[i];
     m->cvs = s->geom.chem_voxel_size;
     m->chemo_force = mech.chemo_force;
@@ -540,8 +544,8 @@ int step_once_batch(OlcSim* s, int collect, cudaStream_t st) {
         if (!s->field_bound[f]) continue;
         const int stor = s->fstep[f].storage;
         if (stor != OLC_FIELD_F32) {
-            launch_react_batch16(B, stor, s->btiles_all, s->n_btiles, s->bsteps_dev, (int)f, (int)F, s->fpar_dev,
-                                 s->field[0][f], s->field[1][f], s->sink[f], s->comp[f], st);
+            launch_react_batch16(B, stor, s->fstep[f].encoding, s->btiles_all, s->n_btiles, s->bsteps_dev, (int)f,
+                                 (int)F, s->fpar_dev, s->field[0][f], s->field[1][f], s->sink[f], s->comp[f], st);
             ++launches;
             continue;
         }
@@ -557,7 +561,8 @@ int step_once_batch(OlcSim* s, int collect, cudaStream_t st) {
         const int stor = s->fstep[f].storage;
         for (size_t sub = 0; sub < cnt.size(); ++sub) {
             if (stor != OLC_FIELD_F32)
-                launch_substep_batch_t16(B, stor, s->btiles_field[f], cnt[sub], s->bsteps_dev, s->bmaps_dev, (int)f,
+                launch_substep_batch_t16(B, stor, s->fstep[f].encoding, s->btiles_field[f], cnt[sub], s->bsteps_dev,
+                                         s->bmaps_dev, (int)f,
                                          (int)F, s->fpar_dev, (int)sub, s->field[0][f], s->field[1][f],
                                          s->counters + OLC_CTR_FIELD_STEP, s->counters + OLC_CTR_STATUS, st);
             else
@@ -643,9 +648,9 @@ int step_once_batch(OlcSim* s, int collect, cudaStream_t st) {
         for (olc_u32 f = 0; f < F; ++f) {
             if (!s->field_bound[f]) continue;
             if (s->fstep[f].storage != OLC_FIELD_F32)
-                launch_reduce_field_batch16(B, s->fstep[f].storage, s->btiles_all, s->n_btiles, (int)f, (int)F,
-                                            s->fpar_dev, s->field[0][f], s->field[1][f], s->comp[f], s->red_batch_dev,
-                                            st);
+                launch_reduce_field_batch16(B, s->fstep[f].storage, s->fstep[f].encoding, s->btiles_all,
+                                            s->n_btiles, s->bsteps_dev, (int)f, (int)F, s->fpar_dev, s->field[0][f],
+                                            s->field[1][f], s->comp[f], s->red_batch_dev, st);
             else
                 launch_reduce_field_batch(B, s->btiles_all, s->n_btiles, (int)f, (int)F, s->fpar_dev, s->field[0][f],
                                           s->field[1][f], s->red_batch_dev, st);
@@ -1207,7 +1212,12 @@ int olc_bind_field_ex(OlcSim* s, int index, void* a_, void* b_, float* sink, flo
     if (spec->substeps == 0) {
         if (spec->storage < OLC_FIELD_F32 || spec->storage > OLC_FIELD_F16_SR)
             return fail(s, OLC_ERR_ARG, "olc_bind_field: bad storage type");
+        if (spec->encoding < OLC_ENC_VALUE || spec->encoding > OLC_ENC_OFFSET3 ||
+            (spec->encoding != OLC_ENC_VALUE && spec->storage == OLC_FIELD_F32))
+            return fail(s, OLC_ERR_ARG, "olc_bind_field: bad encoding (encodings apply to 16-bit storage only)");
         fs.storage = spec->storage;
+        fs.encoding = spec->encoding;
+        fs.bval = spec->boundary;
     }
     if (spec->has_sink && !sink) return fail(s, OLC_ERR_ARG, "olc_bind_field: has_sink without a sink buffer");
     const bool half = fs.storage != OLC_FIELD_F32;
@@ -1692,11 +1702,13 @@ int olc_engine_metrics(OlcSim* s, const OlcEngineMetricsSpec* spec, double* out,
     }
     if (spec->o2_field >= 0) {
         a.f0 = s->field[s->field_cur[spec->o2_field]][spec->o2_field];
-        a.f0_type = s->fspec[spec->o2_field].storage;
+        a.f0_type = field_type_word(s->fstep[spec->o2_field]);
+        a.f0_b = s->fstep[spec->o2_field].bval;
     }
     if (spec->glucose_field >= 0) {
         a.f1 = s->field[s->field_cur[spec->glucose_field]][spec->glucose_field];
-        a.f1_type = s->fspec[spec->glucose_field].storage;
+        a.f1_type = field_type_word(s->fstep[spec->glucose_field]);
+        a.f1_b = s->fstep[spec->glucose_field].bval;
     }
     for (int i = 0; i < 3; ++i) {
         a.cdims[i] = s->geom.chem_dims[i];
@@ -1742,9 +1754,17 @@ int olc_bind_field_batch(OlcSim* s, int index, void* a_, void* b_, float* sink, 
         return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: bad index or null argument");
     const olc_u32 F = s->caps.n_fields;
     const int storage = specs[0].storage;
-    for (olc_u32 k = 0; k < s->n_sims; ++k)
+    const int encoding = specs[0].encoding;
+    for (olc_u32 k = 0; k < s->n_sims; ++k) {
         if (specs[k].storage != storage)
             return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: every member stores a field with the same type");
+        // rules read an encoded field through one boundary value per handle
+        if (specs[k].encoding != encoding ||
+            (encoding != OLC_ENC_VALUE && specs[k].boundary != specs[0].boundary))
+            return fail(s, OLC_ERR_ARG,
+                        "olc_bind_field_batch: every member encodes a field the same way (encoding and, when "
+                        "encoded, boundary value)");
+    }
     if (storage != OLC_FIELD_F32 && !comp)
         return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: 16-bit storage needs a compensation buffer");
     bool any_sink = false;
@@ -1763,6 +1783,8 @@ int olc_bind_field_batch(OlcSim* s, int index, void* a_, void* b_, float* sink, 
             for (int i = 0; i < 3; ++i) fs.dims[i] = g.chem_dims[i];
             fs.substeps = 0;
             fs.storage = storage;
+            fs.encoding = encoding;
+            fs.bval = spec.boundary;
         }
         any_sink = any_sink || (spec.has_sink && spec.substeps != 0);
         s->bsteps_host[(size_t)k * F + index] = fs;
@@ -1818,6 +1840,8 @@ int olc_bind_field_batch(OlcSim* s, int index, void* a_, void* b_, float* sink, 
     s->sink[index] = any_sink ? sink : nullptr;
     s->comp[index] = storage != OLC_FIELD_F32 ? comp : nullptr;
     s->fstep[index].storage = storage;
+    s->fstep[index].encoding = encoding;
+    s->fstep[index].bval = specs[0].boundary;
     s->fspec[index] = specs[0];
     s->field_cur[index] = 0;
     s->field_bound[index] = true;
@@ -1966,7 +1990,8 @@ int olc_create_pool(const OlcPoolConfig* cfg, const OlcCaps* caps, OlcSim** out)
     return OLC_OK;
 }
 
-int olc_bind_field_pool(OlcSim* s, int index, void* a, void* b, float* sink, float* comp, int storage) {
+int olc_bind_field_pool(OlcSim* s, int index, void* a, void* b, float* sink, float* comp, int storage, int encoding,
+                        float boundary) {
     if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
     if (!s->pool) return fail(s, OLC_ERR_STATE, "olc_bind_field_pool: not a pool");
     if (index < 0 || index >= (int)s->caps.n_fields || !a || !b)
@@ -1975,6 +2000,8 @@ int olc_bind_field_pool(OlcSim* s, int index, void* a, void* b, float* sink, flo
         return fail(s, OLC_ERR_ARG, "olc_bind_field_pool: bad storage type");
     if (storage != OLC_FIELD_F32 && !comp)
         return fail(s, OLC_ERR_ARG, "olc_bind_field_pool: 16-bit storage needs a compensation buffer");
+    if (encoding < OLC_ENC_VALUE || encoding > OLC_ENC_OFFSET3 || (encoding != OLC_ENC_VALUE && storage == OLC_FIELD_F32))
+        return fail(s, OLC_ERR_ARG, "olc_bind_field_pool: bad encoding (encodings apply to 16-bit storage only)");
     if (s->slots_used) return fail(s, OLC_ERR_STATE, "olc_bind_field_pool: bind fields before admitting members");
     drop_graphs(s);
     s->field[0][index] = static_cast<float*>(a);
@@ -1983,6 +2010,8 @@ int olc_bind_field_pool(OlcSim* s, int index, void* a, void* b, float* sink, flo
     s->comp[index] = storage != OLC_FIELD_F32 ? comp : nullptr;
     s->fstep[index] = FieldStep{};
     s->fstep[index].storage = storage;
+    s->fstep[index].encoding = encoding;
+    s->fstep[index].bval = boundary;
     s->field_cur[index] = 0;
     s->field_bound[index] = true;
     s->pool_dirty = true;
@@ -2007,6 +2036,10 @@ int olc_pool_admit(OlcSim* s, const OlcGeom* geom, const OlcDiffusion* specs, co
         const int storage = s->fstep[f].storage;
         if (specs[f].storage != storage)
             return fail(s, OLC_ERR_ARG, "olc_pool_admit: field " + std::to_string(f) + " storage differs from the pool's");
+        if (specs[f].encoding != s->fstep[f].encoding ||
+            (specs[f].encoding != OLC_ENC_VALUE && specs[f].boundary != s->fstep[f].bval))
+            return fail(s, OLC_ERR_ARG, "olc_pool_admit: field " + std::to_string(f) +
+                                            " encoding (or an encoded field's boundary value) differs from the pool's");
         if (nvox == 0 || geom->chem_dims[0] % (storage == OLC_FIELD_F32 ? 4 : 8) != 0)
             return fail(s, OLC_ERR_ARG, "olc_pool_admit: field x extent must be a multiple of 4 (8 for 16-bit storage)");
         if (specs[f].substeps != 0) {
@@ -2015,6 +2048,8 @@ int olc_pool_admit(OlcSim* s, const OlcGeom* geom, const OlcDiffusion* specs, co
         } else {
             for (int i = 0; i < 3; ++i) fs[f].dims[i] = geom->chem_dims[i];
             fs[f].storage = storage;
+            fs[f].encoding = s->fstep[f].encoding;
+            fs[f].bval = specs[f].boundary;
         }
     }
     if (params_bytes && s->params_stride && params_bytes != s->params_stride)

@@ -6,6 +6,7 @@
 // compiled without contraction).
 #pragma once
 #include "olc_device.cuh"
+#include "../../include/olc.h"
 
 namespace olc {
 
@@ -102,6 +103,37 @@ __device__ __forceinline__ void stencil_update8_fma(float xl, float xr, const fl
         const float2 w = upk2(mul2(fma2(r2, fma2(m6, cc, s), cc), id2));
         out[e] = fmaxf(w.x, 0.0f);
         out[e + 1] = fmaxf(w.y, 0.0f);
+    }
+}
+
+// stencil_update8_fma on the working values of an encoded 16-bit field
+// (OLC_ENC_*): OLC_ENC_DEFICIT updates deficits s = b - f, whose decay adds
+// dec_sub = b (1 - inv_decay) and whose clamp [0, b] is the image of f in
+// [0, b]:  out = min(max(fma(u, inv_decay, dec_sub), 0), b);  the other
+// encodings update values as stencil_update8_fma does (OLC_ENC_OFFSET3
+// clamps to [0, b] when it encodes).
+template <int EN>
+__device__ __forceinline__ void stencil_update8_enc(float xl, float xr, const float (&c)[8], const float (&ym)[8],
+                                                    const float (&yp)[8], const float (&zm)[8],
+                                                    const float (&zp)[8], float r, float inv_decay, float dec_sub,
+                                                    float b, float (&out)[8]) {
+    if (EN != OLC_ENC_DEFICIT) {
+        stencil_update8_fma(xl, xr, c, ym, yp, zm, zp, r, inv_decay, out);
+        return;
+    }
+    const f32x2 r2 = pk2(r, r), id2 = pk2(inv_decay, inv_decay), m6 = pk2(-6.0f, -6.0f),
+                ds2 = pk2(dec_sub, dec_sub);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int e = 2 * k;
+        const f32x2 cc = pk2(c[e], c[e + 1]);
+        const float sx0 = __fadd_rn(k == 0 ? xl : c[e - 1], c[e + 1]);
+        const float sx1 = __fadd_rn(c[e], k == 3 ? xr : c[e + 2]);
+        const f32x2 s = add2(add2(pk2(sx0, sx1), add2(pk2(ym[e], ym[e + 1]), pk2(yp[e], yp[e + 1]))),
+                             add2(pk2(zm[e], zm[e + 1]), pk2(zp[e], zp[e + 1])));
+        const float2 w = upk2(fma2(fma2(r2, fma2(m6, cc, s), cc), id2, ds2));
+        out[e] = fminf(fmaxf(w.x, 0.0f), b);
+        out[e + 1] = fminf(fmaxf(w.y, 0.0f), b);
     }
 }
 

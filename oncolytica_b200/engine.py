@@ -33,6 +33,7 @@ class DiffusionSpec:
     boundary: float = 0.0
     substeps: Optional[int] = None
     storage: str = "f32"   # "f32", "bf16", "f16", "bf16_sr" or "f16_sr": element type (and rounding) of the field
+    encoding: str = "auto"  # 16-bit elements: "value", "deficit", "offset3" or "auto" (_fieldcodec.resolve)
 
 
 STORAGE_CODES = {"f32": 0, "bf16": 1, "f16": 2, "bf16_sr": 3, "f16_sr": 4}
@@ -187,7 +188,7 @@ class Engine:
         self.chemistry = Grid(chemistry_class, self.chemistry_shape, self)
 
     def setup_diffusion(self, field: str, diffusion: float, decay: float = 0.0, boundary: float = 0.0,
-                        substeps: Optional[int] = None, storage: str = "f32") -> None:
+                        substeps: Optional[int] = None, storage: str = "f32", encoding: str = "auto") -> None:
         """Built-in diffusion of one chemistry field: per step an implicit sink
         (rates deposited with ``self.sink_at(pos).field += k``), then S explicit
         7-point substeps with the outer faces pinned to ``boundary``
@@ -198,10 +199,35 @@ class Engine:
         "f16_sr" round the substeps stochastically (reproducible hash bits) so
         that small diffusion increments are not lost to the short mantissa and
         rounding errors do not accumulate a bias (no counterpart in the
-        reference, whose fields are FP32)."""
+        reference, whose fields are FP32).  ``encoding`` says what a 16-bit
+        element holds: "value"; "deficit" (boundary - value, for fields that
+        stay near their boundary value, like O2); "offset3" (the value minus
+        the nearest of 0, b/2 and b, for fields spread over [0, b], like a
+        decaying drug); "auto" picks by storage, decay and the initial values
+        (_fieldcodec.resolve).  Encoded fields stay within [0, boundary]."""
+        from oncolytica_b200._fieldcodec import ENCODINGS
+
         if storage not in STORAGE_CODES:
             raise ValueError(f"storage must be one of {sorted(STORAGE_CODES)}, got {storage!r}")
-        self._diffusion[field] = DiffusionSpec(float(diffusion), float(decay), float(boundary), substeps, storage)
+        if encoding != "auto" and encoding not in ENCODINGS:
+            raise ValueError(f"encoding must be 'auto' or one of {sorted(ENCODINGS)}, got {encoding!r}")
+        self._diffusion[field] = DiffusionSpec(float(diffusion), float(decay), float(boundary), substeps, storage,
+                                               encoding)
+
+    def field_encoding(self, field: str) -> int:
+        """The OLC_ENC_* code a diffusing field's 16-bit elements use (0 for
+        FP32 fields and static fields), resolving "auto" from the field's
+        storage, decay, boundary and current host values."""
+        from oncolytica_b200._fieldcodec import resolve
+
+        spec = self._diffusion.get(field)
+        if spec is None:
+            return 0
+        mean = None
+        if self.chemistry is not None and field in self.chemistry._fields:
+            vals = np.asarray(self.chemistry.column(field), dtype=np.float64)
+            mean = float(vals.mean()) if vals.size else None
+        return resolve(spec.encoding, STORAGE_CODES[spec.storage], spec.decay, spec.boundary, mean)
 
     def setup_contact(self, radius: str | float = "radius", stiffness: float = 1.0, mobility: float = 10.0,
                       max_disp: float = 1.0, margin: float = 0.1, necrotic_factor: float = 1.0,

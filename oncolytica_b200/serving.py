@@ -34,7 +34,7 @@ from typing import Any, Callable, Iterable, Sequence
 
 import numpy as np
 
-from oncolytica_b200 import _lib
+from oncolytica_b200 import _fieldcodec, _lib
 from oncolytica_b200.backend import FIELD_DTYPES, seed_rng
 from oncolytica_b200.engine import STORAGE_CODES
 from oncolytica_b200.compiler.emit_cuda import make_layout, pack_params, translate_model
@@ -464,10 +464,13 @@ class PoolDevice:
         self.layout = L = make_layout(sim._spec, radius_field, batched=True)
         self.program = translate_model(sim, L, radius_field) if (eng._cell_rules or eng._metric_rules) else None
         self.sinks = self.program.sink_fields if self.program else set()
-        self.storage = {}
+        self.storage, self.encoding, self.bval = {}, {}, {}
         for name in L.chem_fields:
             d = eng._diffusion.get(name)
             self.storage[name] = STORAGE_CODES[d.storage] if d is not None else 0
+            # what the 16-bit elements hold; every request must resolve the same
+            self.encoding[name] = eng.field_encoding(name)
+            self.bval[name] = float(d.boundary) if d is not None else 0.0
         caps = _lib.OlcCaps()
         caps.max_agents = self.max_rows
         caps.n_agent_fields = len(L.cell_cols)
@@ -508,7 +511,8 @@ class PoolDevice:
                 self._check(self.lib.olc_bind_field_pool(
                     self.handle, i, C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()),
                     C.c_void_p(s.data_ptr()) if s is not None else None,
-                    C.c_void_p(comp.data_ptr()) if comp is not None else None, st))
+                    C.c_void_p(comp.data_ptr()) if comp is not None else None, st, self.encoding[name],
+                    C.c_float(self.bval[name])))
         self.stream.synchronize()
         ct = _lib.OlcContact()
         if contact is not None:
@@ -562,6 +566,9 @@ class PoolDevice:
             st = STORAGE_CODES[d.storage] if d is not None else 0
             if st != self.storage[name]:
                 raise RequestError(f"field {name!r} storage differs from the pool's")
+            if e.field_encoding(name) != self.encoding[name] or (
+                    self.encoding[name] and d is not None and float(d.boundary) != self.bval[name]):
+                raise RequestError(f"field {name!r} encoding (or encoded boundary value) differs from the pool's")
             if name in self.sinks and d is None:
                 raise RequestError(f"sink_at(...).{name} needs Engine.setup_diffusion({name!r}, ...)")
         if e.chemistry is not None and int(e.chemistry_shape[0]) % (8 if any(self.storage.values()) else 4):
@@ -591,6 +598,7 @@ class PoolDevice:
             d = e._diffusion.get(name)
             sp = specs[i]
             sp.storage = self.storage[name]
+            sp.encoding = self.encoding[name]
             if d is None:
                 sp.substeps = 0
                 substeps.append(0)
@@ -627,6 +635,9 @@ class PoolDevice:
                 out[0, :, :] = out[-1, :, :] = b
                 out[:, 0, :] = out[:, -1, :] = b
                 out[:, :, 0] = out[:, :, -1] = b
+            if self.storage[name]:  # 16-bit elements of the field's encoding, rounded to nearest even
+                bits = _fieldcodec.encode(flat, self.storage[name], self.encoding[name], self.bval[name])
+                pin = torch.from_numpy(bits.view(np.int16)).pin_memory()
             fields.append(pin)
         blob = pack_params(L, sim._params)
         req._payload = {"n": n, "specs": specs, "substeps": tuple(substeps), "agents": agents, "fields": fields,
@@ -665,11 +676,8 @@ class PoolDevice:
                 dst = self.fields_dev[i][0][m.field_off:m.field_off + nvox]
                 if dst.dtype == torch.float32:
                     dst.copy_(pin, non_blocking=True)
-                else:
-                    tmp = torch.empty(nvox, dtype=torch.float32, device=self.device)
-                    tmp.copy_(pin, non_blocking=True)
-                    dst.copy_(tmp)  # round to nearest even, as a solo run's upload
-                    keep.append(tmp)
+                else:  # encoded on the host (prepare), as a solo run's upload
+                    dst.view(torch.int16).copy_(pin, non_blocking=True)
             for t in keep:
                 t.record_stream(self.stream)
         req._payload = None  # pinned buffers return to torch's cache once the copies are done
@@ -780,7 +788,8 @@ class PoolDevice:
                     bits = h.view(torch.int16).numpy().view(np.uint16).copy()
                     res.field_bits[name] = bits
                     res.residuals[name] = c.numpy().copy()
-                    v = h.float().numpy() + res.residuals[name]
+                    v = _fieldcodec.decode(bits, self.storage[name], self.encoding[name], self.bval[name],
+                                           res.residuals[name])
                 res.fields[name] = v.reshape(shape, order="F")
 
         return _PendingResult(ev, fill)

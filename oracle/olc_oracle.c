@@ -346,34 +346,114 @@ void orc_round16(const float* in, uint16_t* out, size_t n, int storage, const ui
     }
 }
 
-int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const int32_t dims[3], float dx, float dt,
-                  float D, float decay, float boundary, int substeps, int storage, uint32_t step, int field,
-                  int nthreads) {
+/* Encodings of 16-bit elements (olc.h OLC_ENC_*): 0 the value, 1 the deficit
+ * b - f (the kernels' working value is then the deficit), 2 f minus the
+ * offset o in {0, b/2, b} nearest f, o and the sign in bits 15 and 14
+ * (oncolytica_b200/csrc/olc_store16.cuh: Codec). */
+typedef struct {
+    float b, hb, qb, uq;
+} Enc16;
+static Enc16 enc16_consts(float b) {
+    Enc16 k;
+    k.b = b;
+    k.hb = 0.5f * b;
+    k.qb = 0.25f * b;
+    k.uq = b - k.qb;
+    return k;
+}
+static float work16(uint16_t h, int storage, int enc, const Enc16* k) {
+    if (enc != 2) return h16_to_f(h, storage);
+    const float m = h16_to_f((uint16_t)(h & 0xBFFFu), storage);
+    const uint32_t units = (uint32_t)(h >> 15) + (uint32_t)((h >> 14) & 1u);
+    return m + (float)units * k->hb;
+}
+static float phys_of_work16(float w, int enc, const Enc16* k) { return enc == 1 ? k->b - w : w; }
+static float split3(float f, const Enc16* k, uint16_t* code) {
+    f = f > 0.0f ? f : 0.0f;
+    f = f < k->b ? f : k->b;
+    if (f < k->qb) {
+        *code = 0;
+        return fabsf(f);
+    }
+    if (f > k->uq) {
+        *code = 0xC000u;
+        return k->b - f;
+    }
+    const float d = f - k->hb;
+    *code = d < 0.0f ? 0x8000u : 0x4000u;
+    return fabsf(d);
+}
+static uint16_t enc16_rn(float w, int storage, int enc, const Enc16* k) {
+    if (enc != 2) return f_to_h16(w, storage);
+    uint16_t c;
+    const float m = split3(w, k, &c);
+    return (uint16_t)(f_to_h16(m, storage) | c);
+}
+static uint16_t enc16_sr(float w, int storage, int enc, const Enc16* k, uint32_t rb) {
+    uint16_t c = 0;
+    const float m = enc == 2 ? split3(w, k, &c) : w;
+    return (uint16_t)((storage == 3 ? f_to_bf16_sr(m, rb) : f_to_f16_sr(m, rb)) | c);
+}
+
+void orc_encode16(const float* f, uint16_t* out, size_t n, int storage, int encoding, float boundary) {
+    const Enc16 k = enc16_consts(boundary);
+    for (size_t i = 0; i < n; ++i) out[i] = enc16_rn(encoding == 1 ? boundary - f[i] : f[i], storage, encoding, &k);
+}
+
+void orc_decode16(const uint16_t* h, const float* comp, float* out, size_t n, int storage, int encoding,
+                  float boundary) {
+    const Enc16 k = enc16_consts(boundary);
+    for (size_t i = 0; i < n; ++i) {
+        float w = work16(h[i], storage, encoding, &k);
+        if (comp) w = w + comp[i];
+        out[i] = phys_of_work16(w, encoding, &k);
+    }
+}
+
+int orc_diffuse16e(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const int32_t dims[3], float dx, float dt,
+                   float D, float decay, float boundary, int substeps, int storage, int encoding, uint32_t step,
+                   int field, int nthreads) {
     const int nx = dims[0], ny = dims[1], nz = dims[2];
     const int nt = nthreads_or_all(nthreads);
-    if (substeps < 1 || storage < 1 || storage > 4) return -1;
+    if (substeps < 1 || storage < 1 || storage > 4 || encoding < 0 || encoding > 2) return -1;
+    if (encoding != 0 && !(boundary > 0.0f)) return -1;
+    if (encoding == 2 && boundary > 4.0f) return -1;
     const float dts = dt / (float)substeps;
     const float r = D * dts / (dx * dx);
     if (r > 1.0f / 6.0f + 1e-7f) return -1;
     const int sr = storage == 3 || storage == 4;
     const float decay_step = sr ? 1.0f : (float)pow(1.0 + (double)decay * (double)dts, -(double)substeps);
     const float inv_decay = sr ? 1.0f / (1.0f + decay * dts) : 1.0f;
-    const uint16_t bh = f_to_h16(boundary, storage);
+    const Enc16 k = enc16_consts(boundary);
+    const float dec_sub = boundary * (1.0f - inv_decay);
+    const float dec_step = boundary * (1.0f - decay_step);
+    /* the faces hold the boundary: value as stored, deficit 0, or b exactly */
+    const float face_w =
+        encoding == 1 ? 0.0f : (encoding == 2 ? boundary : h16_to_f(f_to_h16(boundary, storage), storage));
+    const uint16_t bh = enc16_rn(face_w, storage, encoding, &k);
     const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
 #pragma omp parallel for num_threads(nt) schedule(static)
     for (int z = 0; z < nz; ++z)
         for (int y = 0; y < ny; ++y)
             for (int x = 0; x < nx; ++x) {
                 size_t v = (size_t)z * sz + (size_t)y * sy + x;
-                float k = sink ? sink[v] : 0.0f;
+                float kv = sink ? sink[v] : 0.0f;
                 if (sink) sink[v] = 0.0f;
                 if (x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1) continue;
-                float val = h16_to_f(f[v], storage) + comp[v];
-                if (k != 0.0f) val = val / (1.0f + k * dt);
-                val = val * decay_step;
-                uint16_t h = f_to_h16(val, storage);
+                float val = work16(f[v], storage, encoding, &k) + comp[v];
+                if (encoding == 1) {
+                    if (kv != 0.0f) {
+                        const float kd = kv * dt;
+                        val = (val + boundary * kd) / (1.0f + kd);
+                    }
+                    val = fmaf(val, decay_step, dec_step);
+                } else {
+                    if (kv != 0.0f) val = val / (1.0f + kv * dt);
+                    val = val * decay_step;
+                }
+                uint16_t h = enc16_rn(val, storage, encoding, &k);
                 f[v] = h;
-                comp[v] = val - h16_to_f(h, storage);
+                comp[v] = val - work16(h, storage, encoding, &k);
             }
     uint16_t* cur = f;
     uint16_t* nxt = tmp;
@@ -389,19 +469,28 @@ int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const in
                         nxt[v] = bh;
                         continue;
                     }
-                    float c = h16_to_f(cur[v], storage);
-                    float s1 = (h16_to_f(cur[v - 1], storage) + h16_to_f(cur[v + 1], storage)) +
-                               (h16_to_f(cur[v - sy], storage) + h16_to_f(cur[v + sy], storage));
-                    float s2 = s1 + (h16_to_f(cur[v - sz], storage) + h16_to_f(cur[v + sz], storage));
-                    float u = fmaf(r, fmaf(-6.0f, c, s2), c) * inv_decay;
-                    u = u > 0.0f ? u : 0.0f;
-                    if (storage == 3 || storage == 4) {
+                    float c = work16(cur[v], storage, encoding, &k);
+                    float s1 = (work16(cur[v - 1], storage, encoding, &k) + work16(cur[v + 1], storage, encoding, &k)) +
+                               (work16(cur[v - sy], storage, encoding, &k) +
+                                work16(cur[v + sy], storage, encoding, &k));
+                    float s2 = s1 + (work16(cur[v - sz], storage, encoding, &k) +
+                                     work16(cur[v + sz], storage, encoding, &k));
+                    float u = fmaf(r, fmaf(-6.0f, c, s2), c);
+                    if (encoding == 1) {
+                        u = fmaf(u, inv_decay, dec_sub);
+                        u = u > 0.0f ? u : 0.0f;
+                        u = u < boundary ? u : boundary;
+                    } else {
+                        u = u * inv_decay;
+                        u = u > 0.0f ? u : 0.0f;
+                    }
+                    if (sr) {
                         uint32_t xr = ((uint32_t)(v >> 1) ^ key) * 0x9E3779B1u;
                         xr ^= xr >> 15;
                         const uint32_t rb = (v & 1) ? (xr >> 16) : (xr & 0xffffu);
-                        nxt[v] = storage == 3 ? f_to_bf16_sr(u, rb) : f_to_f16_sr(u, rb);
+                        nxt[v] = enc16_sr(u, storage, encoding, &k, rb);
                     } else {
-                        nxt[v] = f_to_h16(u, storage);
+                        nxt[v] = enc16_rn(u, storage, encoding, &k);
                     }
                 }
             }
@@ -411,6 +500,13 @@ int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const in
     }
     if (cur != f) memcpy(f, cur, (size_t)nx * ny * nz * 2);
     return 0;
+}
+
+int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const int32_t dims[3], float dx, float dt,
+                  float D, float decay, float boundary, int substeps, int storage, uint32_t step, int field,
+                  int nthreads) {
+    return orc_diffuse16e(f, tmp, sink, comp, dims, dx, dt, D, decay, boundary, substeps, storage, 0, step, field,
+                          nthreads);
 }
 
 /* The field schemes evaluated in FP64, the reference against which each

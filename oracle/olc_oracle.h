@@ -61,6 +61,16 @@ void orc_round16(const float* in, uint16_t* out, size_t n, int storage, const ui
 int orc_diffuse16(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const int32_t dims[3], float dx, float dt,
                   float D, float decay, float boundary, int substeps, int storage, uint32_t step, int field,
                   int nthreads);
+/* The same with an element encoding (0 value, 1 deficit, 2 three offsets;
+ * olc.h OLC_ENC_*), and the encodings' conversions: orc_encode16 rounds field
+ * values to nearest into encoded elements, orc_decode16 returns field values
+ * (plus the residuals, in the encoded domain, when comp is not NULL). */
+int orc_diffuse16e(uint16_t* f, uint16_t* tmp, float* sink, float* comp, const int32_t dims[3], float dx, float dt,
+                   float D, float decay, float boundary, int substeps, int storage, int encoding, uint32_t step,
+                   int field, int nthreads);
+void orc_encode16(const float* f, uint16_t* out, size_t n, int storage, int encoding, float boundary);
+void orc_decode16(const uint16_t* h, const float* comp, float* out, size_t n, int storage, int encoding,
+                  float boundary);
 int orc_diffuse_f64(double* f, double* tmp, const float* sink, const int32_t dims[3], double dx, double dt, double D,
                     double decay, double boundary, int substeps, int split, int nthreads);
 

@@ -61,6 +61,11 @@ def lib() -> C.CDLL:
         L.orc_tumour_agents.argtypes = [P, C.c_int]
         L.orc_tumour_sizeof.restype = C.c_size_t
         L.orc_round16.argtypes = [P, P, C.c_size_t, C.c_int, P]
+        L.orc_diffuse16e.restype = C.c_int
+        L.orc_diffuse16e.argtypes = [P, P, P, P, P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
+                                     C.c_int, C.c_int, C.c_uint32, C.c_int, C.c_int]
+        L.orc_encode16.argtypes = [P, P, C.c_size_t, C.c_int, C.c_int, C.c_float]
+        L.orc_decode16.argtypes = [P, P, P, C.c_size_t, C.c_int, C.c_int, C.c_float]
         _lib = L
     return _lib
 
@@ -148,10 +153,16 @@ def diffuse_pinned(f: np.ndarray, sink, dx, dt, D, decay, boundary, substeps, pi
     return f
 
 
-def to_bits16(f: np.ndarray, storage: int) -> np.ndarray:
+def to_bits16(f: np.ndarray, storage: int, encoding: int = 0, boundary: float = 0.0) -> np.ndarray:
     """float32 values -> BF16 (storage 1 and 3) or FP16 (storage 2 and 4) bit
-    patterns, rounded to nearest even (finite values)."""
+    patterns, rounded to nearest even (finite values); with an encoding (1
+    deficit, 2 three offsets) the encoded elements of a field whose boundary
+    value is ``boundary`` (``orc_encode16``)."""
     f = np.ascontiguousarray(f, dtype=np.float32)
+    if encoding:
+        out = np.zeros(f.shape, np.uint16)
+        lib().orc_encode16(_p(f), _p(out), f.size, storage, encoding, C.c_float(boundary))
+        return out
     if storage in (2, 4):
         return f.astype(np.float16).view(np.uint16)
     u = f.view(np.uint32).astype(np.uint64)
@@ -169,8 +180,16 @@ def round16(f: np.ndarray, storage: int, rnd: np.ndarray | None = None) -> np.nd
     return out
 
 
-def from_bits16(h: np.ndarray, storage: int) -> np.ndarray:
+def from_bits16(h: np.ndarray, storage: int, encoding: int = 0, boundary: float = 0.0,
+                comp: np.ndarray | None = None) -> np.ndarray:
+    """Field values of 16-bit elements (``orc_decode16`` for an encoding, or
+    when the residuals ``comp`` are to be added in the encoded domain)."""
     h = np.ascontiguousarray(h, dtype=np.uint16)
+    if encoding or comp is not None:
+        out = np.zeros(h.shape, np.float32)
+        c = None if comp is None else np.ascontiguousarray(comp, dtype=np.float32).reshape(h.shape)
+        lib().orc_decode16(_p(h), _p(c), _p(out), h.size, storage, encoding, C.c_float(boundary))
+        return out
     if storage in (2, 4):
         return h.view(np.float16).astype(np.float32)
     return (h.astype(np.uint32) << 16).view(np.float32)
@@ -178,17 +197,18 @@ def from_bits16(h: np.ndarray, storage: int) -> np.ndarray:
 
 def diffuse16(bits: np.ndarray, sink: np.ndarray | None, comp: np.ndarray, dx: float, dt: float, D: float,
               decay: float, boundary: float, substeps: int, storage: int, step: int = 0, field: int = 0,
-              nthreads: int = 0):
+              nthreads: int = 0, encoding: int = 0):
     """One step of a 16-bit field (indexed [z, y, x]): returns (bits, comp).
-    ``step`` and ``field`` salt the stochastic rounding of storages 3 and 4."""
+    ``step`` and ``field`` salt the stochastic rounding of storages 3 and 4;
+    ``encoding`` is the elements' (0 value, 1 deficit, 2 three offsets)."""
     f = np.ascontiguousarray(bits, dtype=np.uint16).copy()
     tmp = np.zeros_like(f)
     c = np.ascontiguousarray(comp, dtype=np.float32).copy()
     s = None if sink is None else np.ascontiguousarray(sink, dtype=np.float32).copy()
     dims = np.array([f.shape[2], f.shape[1], f.shape[0]], dtype=np.int32)
-    rc = lib().orc_diffuse16(_p(f), _p(tmp), _p(s), _p(c), _p(dims), C.c_float(dx), C.c_float(dt), C.c_float(D),
-                             C.c_float(decay), C.c_float(boundary), substeps, storage, C.c_uint32(step), field,
-                             nthreads)
+    rc = lib().orc_diffuse16e(_p(f), _p(tmp), _p(s), _p(c), _p(dims), C.c_float(dx), C.c_float(dt), C.c_float(D),
+                              C.c_float(decay), C.c_float(boundary), substeps, storage, encoding, C.c_uint32(step),
+                              field, nthreads)
     if rc != 0:
         raise ValueError("oracle diffuse16: unstable or bad arguments")
     return f, c

@@ -615,18 +615,23 @@ def test_tumour_step_parity_16bit_fields(cuda, storage, code):
     eng.sync_to_device()
     be = eng._backend_impl
     shp = tuple(spec.field_dims[::-1])
+    # what the elements hold: BF16 fields default to the deficit (O2, no
+    # decay, starts at its boundary value) and three offsets (the decaying drug)
+    e_o2, e_dr = be.field_codec("o2")[1], be.field_codec("drug")[1]
+    assert (e_o2, e_dr) == ((1, 2) if code in (1, 3) else (0, 0))
     for step in range(4):
         snap = be.snapshot()
         k = be.counters()["steps"]  # the step count salts stochastic rounding, with the field's index
         o2_bits, o2_res = oracle.diffuse16(snap["fields"]["o2"].reshape(shp), snap["sinks"]["o2"].reshape(shp),
                                            snap["residuals"]["o2"].reshape(shp), spec.dx, spec.dt, spec.D_o2, 0.0,
-                                           spec.bnd_o2, spec.S_o2, code, step=k, field=0)
+                                           spec.bnd_o2, spec.S_o2, code, step=k, field=0, encoding=e_o2)
         dr_bits, dr_res = oracle.diffuse16(snap["fields"]["drug"].reshape(shp), None,
                                            snap["residuals"]["drug"].reshape(shp), spec.dx, spec.dt, spec.D_drug,
-                                           spec.decay_drug, spec.bnd_drug, spec.S_drug, code, step=k, field=1)
+                                           spec.decay_drug, spec.bnd_drug, spec.S_drug, code, step=k, field=1,
+                                           encoding=e_dr)
         fsnap = dict(snap)
-        fsnap["fields"] = {"o2": oracle.from_bits16(o2_bits, code).ravel(),
-                           "drug": oracle.from_bits16(dr_bits, code).ravel()}
+        fsnap["fields"] = {"o2": oracle.from_bits16(o2_bits, code, e_o2, spec.bnd_o2).ravel(),
+                           "drug": oracle.from_bits16(dr_bits, code, e_dr, spec.bnd_drug).ravel()}
         fsnap["sinks"] = {"o2": np.zeros(int(np.prod(shp)), np.float32)}
         orc = oracle.TumourOracle.from_snapshot(spec, fsnap, spec.capacity)
         orc.agents_part(nthreads=4)

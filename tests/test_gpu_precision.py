@@ -37,13 +37,14 @@ def _problem(n=32, seed=5):
     return shape, K
 
 
-def _run_gpu(olc, cuda, storage, shape, K, D, decay, bnd, init, S, dx, dt, steps):
+def _run_gpu(olc, cuda, storage, shape, K, D, decay, bnd, init, S, dx, dt, steps, encoding=0):
     import torch
 
     nz, ny, nx = shape
     f0 = np.full(shape, init, np.float32)
     f0[0], f0[-1], f0[:, 0], f0[:, -1], f0[:, :, 0], f0[:, :, -1] = bnd, bnd, bnd, bnd, bnd, bnd
-    spec = _lib.OlcDiffusion(diffusion=D, decay=decay, boundary=bnd, substeps=S, has_sink=1, storage=storage)
+    spec = _lib.OlcDiffusion(diffusion=D, decay=decay, boundary=bnd, substeps=S, has_sink=1, storage=storage,
+                             encoding=encoding)
     dims = (C.c_int32 * 3)(nx, ny, nz)
     sink = torch.empty(K.size, dtype=torch.float32, device=cuda)
     Kd = torch.from_numpy(K.ravel()).to(cuda)
@@ -55,7 +56,7 @@ def _run_gpu(olc, cuda, storage, shape, K, D, decay, bnd, init, S, dx, dt, steps
             _lib.check(olc.olc_stage_diffuse(C.c_void_p(f.data_ptr()), C.c_void_p(tmp.data_ptr()),
                                              C.c_void_p(sink.data_ptr()), C.byref(dims), dx, dt, C.byref(spec), None))
         return f.cpu().numpy().reshape(shape).astype(np.float64)
-    bits = oracle.to_bits16(f0, storage)
+    bits = oracle.to_bits16(f0, storage, encoding, bnd)
     f = torch.from_numpy(bits.view(np.int16).ravel().copy()).to(cuda)
     tmp = torch.empty_like(f)
     comp = torch.zeros(K.size, dtype=torch.float32, device=cuda)
@@ -64,7 +65,7 @@ def _run_gpu(olc, cuda, storage, shape, K, D, decay, bnd, init, S, dx, dt, steps
         _lib.check(olc.olc_stage_diffuse16(C.c_void_p(f.data_ptr()), C.c_void_p(tmp.data_ptr()),
                                            C.c_void_p(sink.data_ptr()), C.c_void_p(comp.data_ptr()), C.byref(dims),
                                            dx, dt, C.byref(spec), step, 0, None))
-    v = oracle.from_bits16(f.cpu().numpy().view(np.uint16), storage) + comp.cpu().numpy()
+    v = oracle.from_bits16(f.cpu().numpy().view(np.uint16), storage, encoding, bnd, comp=comp.cpu().numpy())
     return v.reshape(shape).astype(np.float64)
 
 
@@ -127,3 +128,53 @@ def test_field_error_after_1000_steps(cuda, olc, storage):
     assert rel_l2 <= l2_bound, (storage, rel_l2)
     assert err.max() <= linf, (storage, err.max())
     assert np.abs(ref - 1.0).max() > 0.05
+
+
+# BF16 with stochastic rounding and the field encodings (olc.h OLC_ENC_*): the
+# O2-like field (no decay, starts at its boundary value) stores its deficit
+# from the boundary, the drug-like field (decay, spread over [0, 1]) the value
+# less the nearest of 0, 1/2 and 1.  Both reach the FP16 figures' bar:
+# relative L2 error below 1e-3 against FP64.
+ENC_REL_L2 = 1e-3
+
+
+def test_bf16_encodings_meet_the_error_bar(cuda, olc):
+    shape, K = _problem()
+    steps, dx, dt = 200, 4.0, 0.1
+    for D, decay, bnd, init, K_used, enc in ((2000.0, 0.0, 1.0, 1.0, K, 1), (500.0, 0.1, 1.0, 0.0, K * 0.5, 2)):
+        S = int(np.ceil(6.0 * D * dt / (dx * dx) * 1.05))
+        got = _run_gpu(olc, cuda, 3, shape, K_used, D, decay, bnd, init, S, dx, dt, steps, encoding=enc)
+        plain = _run_gpu(olc, cuda, 3, shape, K_used, D, decay, bnd, init, S, dx, dt, steps)
+        ref = np.full(shape, init, np.float64)
+        ref[0], ref[-1], ref[:, 0], ref[:, -1], ref[:, :, 0], ref[:, :, -1] = bnd, bnd, bnd, bnd, bnd, bnd
+        for _ in range(steps):
+            ref = oracle.diffuse_f64(ref, K_used, dx, dt, D, decay, bnd, S)
+        rel = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+        rel_plain = float(np.linalg.norm(plain - ref) / np.linalg.norm(ref))
+        print(f"BF16-SR encoding {enc} D {D}: rel-L2 {rel:.3e} (values: {rel_plain:.3e}) "
+              f"max {np.abs(got - ref).max():.3e}")
+        assert rel <= ENC_REL_L2, (enc, rel)
+        assert rel < rel_plain, (enc, rel, rel_plain)
+        assert got.min() >= 0.0 and got.max() <= bnd + 1e-6
+
+
+def test_bf16_deficit_after_1000_steps(cuda, olc):
+    """The 1,000-step O2-like run of test_field_error_after_1000_steps in
+    BF16 with stochastic rounding, storing deficits: relative L2 below 1e-3
+    (BF16 storing values: 2.0e-3)."""
+    import os
+
+    shape, K = _problem(n=64, seed=9)
+    steps, dx, dt, D = 1000, 4.0, 0.1, 2000.0
+    S = int(np.ceil(6.0 * D * dt / (dx * dx)))
+    got = _run_gpu(olc, cuda, 3, shape, K, D, 0.0, 1.0, 1.0, S, dx, dt, steps, encoding=1)
+    if "ref" not in _LONG_REF:
+        ref = np.ones(shape, np.float64)
+        threads = max(1, os.cpu_count() or 1)
+        for _ in range(steps):
+            ref = oracle.diffuse_f64(ref, K, dx, dt, D, 0.0, 1.0, S, nthreads=threads)
+        _LONG_REF["ref"] = ref
+    ref = _LONG_REF["ref"]
+    rel = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+    print(f"BF16-SR deficit 1000 steps 64^3: rel-L2 {rel:.3e} max {np.abs(got - ref).max():.3e}")
+    assert rel <= ENC_REL_L2, rel

@@ -449,28 +449,31 @@ def test_contact_active_motion_matches_the_oracle(cuda, olc):
 
 # ------------------------------------------------------------------ 16-bit field storage
 
+@pytest.mark.parametrize("encoding", [0, 1, 2])
 @pytest.mark.parametrize("storage", [1, 2, 3, 4])
 @pytest.mark.parametrize("dims,substeps,decay,with_sink", [((32, 24, 20), 5, 0.0, True),
                                                           ((64, 41, 37), 7, 0.1, True),
                                                           ((136, 17, 9), 3, 0.05, False)])
-def test_diffuse16_bit_exact(cuda, olc, storage, dims, substeps, decay, with_sink):
-    """BF16 / FP16 / BF16 with stochastic rounding: three steps of reaction
-    (uptake, decay, residual) and substeps give the oracle's bits, residuals
-    included."""
+def test_diffuse16_bit_exact(cuda, olc, storage, encoding, dims, substeps, decay, with_sink):
+    """BF16 / FP16 / BF16 with stochastic rounding, each element holding the
+    value, the deficit from the boundary value or the value less one of three
+    offsets: three steps of reaction (uptake, decay, residual) and substeps
+    give the oracle's bits, residuals included."""
     import torch
 
-    rng = np.random.default_rng(sum(dims) + storage)
+    rng = np.random.default_rng(sum(dims) + storage + 7 * encoding)
     nx, ny, nz = dims
-    f = (rng.random((nz, ny, nx), dtype=np.float32) * 0.8 + 0.1).astype(np.float32)
+    lo, span = (0.05, 0.6) if encoding else (0.1, 0.8)  # encoded fields live in [0, boundary = 0.7]
+    f = (rng.random((nz, ny, nx), dtype=np.float32) * span + lo).astype(np.float32)
     dx, dt, D = 4.0, 0.1, 2000.0
     D = min(D, (1.0 / 6.0) * dx * dx * substeps / dt * 0.999)
-    bits = oracle.to_bits16(f, storage)
+    bits = oracle.to_bits16(f, storage, encoding, 0.7)
     comp = np.zeros_like(f)
     fd = torch.from_numpy(bits.view(np.int16).copy()).to(cuda)
     tmp = torch.empty_like(fd)
     cd = torch.zeros(f.size, dtype=torch.float32, device=cuda)
     spec = _lib.OlcDiffusion(diffusion=D, decay=decay, boundary=0.7, substeps=substeps, has_sink=int(with_sink),
-                             storage=storage)
+                             storage=storage, encoding=encoding)
     dims_c = (C.c_int32 * 3)(nx, ny, nz)
     for step in range(3):
         sink = None
@@ -481,7 +484,7 @@ def test_diffuse16_bit_exact(cuda, olc, storage, dims, substeps, decay, with_sin
             sink[m] = rng.random(int(m.sum())).astype(np.float32) * 0.5
             sd = to_dev(sink, cuda)
         bits, comp = oracle.diffuse16(bits, sink, comp, dx, dt, D, decay, 0.7, substeps, storage, step=100 + step,
-                                      field=1)
+                                      field=1, encoding=encoding)
         _lib.check(olc.olc_stage_diffuse16(dptr(fd), dptr(tmp), dptr(sd) if sd is not None else None, dptr(cd),
                                            C.byref(dims_c), dx, dt, C.byref(spec), 100 + step, 1, None))
         torch.cuda.synchronize()

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol(olc):
 def test_struct_sizes_match_header_layout():
     assert C.sizeof(_lib.OlcGeom) == 4 * (3 + 1 + 3 + 1 + 3 + 3)
     assert C.sizeof(_lib.OlcCaps) == 4 * 9
-    assert C.sizeof(_lib.OlcDiffusion) == 24
+    assert C.sizeof(_lib.OlcDiffusion) == 28
     assert C.sizeof(_lib.OlcContact) == 28
     assert C.sizeof(_lib.OlcCounters) == 40
     assert C.sizeof(_lib.OlcProfile) == 16 + 6 * 8
