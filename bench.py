@@ -60,6 +60,10 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--duration", type=float, default=120.0, help="seconds of arrivals (--workload serve)")
     ap.add_argument("--serve-seconds", type=float, default=15.0,
                     help="seconds of arrivals of the serving run added to the default line")
+    ap.add_argument("--storages", default="bf16_sr,f16_sr", help="field storages of --workload precision")
+    ap.add_argument("--workload-base", default="scale", help="the workload --workload precision runs")
+    ap.add_argument("--error-steps", type=int, default=10,
+                    help="steps of the field-error measurement added to the default line")
     return ap.parse_args()
 
 
@@ -435,6 +439,11 @@ def run_b200(args) -> None:
                                   "ratio": r["agent_steps_per_s"] / solo["solo_agent_steps_per_s"]}
         line["precision"] = {st: measure_storage(spec, st, args.extra_steps * 5, 3, graphs=not args.no_graphs)
                              for st in ("f16_sr", "bf16_sr", "f16")}
+        # the precision tier's field error against FP64 on this workload (a
+        # short run; --workload precision --steps 1000 runs the full length)
+        if args.error_steps > 0:
+            torch.cuda.empty_cache()
+            line["field_error"] = measure_field_error(spec, ("bf16_sr", "f16_sr"), args.error_steps)
         torch.cuda.empty_cache()
         # the serving mix, shortened to args.serve_seconds of arrivals
         line["serving"] = measure_serving(args.rate, args.serve_seconds, seed=0, storage="f16_sr", solo_sample=4)
@@ -461,6 +470,9 @@ def assert_clean(line: dict) -> None:
     for st, r in (line.get("precision") or {}).items():
         if r.get("status"):
             bad.append((f"precision {st}", r["status"]))
+    for st, v in ((line.get("field_error") or {}).get("status") or {}).items():
+        if v:
+            bad.append((f"field error {st}", v))
     if line.get("serving") and line["serving"].get("device_status"):
         bad.append(("serving", line["serving"]["device_status"]))
     if bad:
@@ -477,8 +489,10 @@ def summarise(line: dict) -> dict:
         out[f"batched_{st}_vs_plain_fp32"] = round(r["vs_plain_fp32"]["ratio"], 3)
     for st, r in (line.get("precision") or {}).items():
         out[f"{st}_ms_per_step"] = round(r["ms_per_step"], 4)
-        if "field_error" in r:
-            out[f"{st}_rel_l2"] = {f: round(e["rel_l2"], 7) for f, e in r["field_error"].items()}
+    fe = line.get("field_error")
+    if fe:
+        out[f"rel_l2_vs_fp64_after_{fe['steps']}_steps"] = {
+            st: {f: float(f"{e['rel_l2']:.3g}") for f, e in r.items()} for st, r in fe["final"].items()}
     if line.get("serving"):
         sv = line["serving"]
         out["serving_p50_p99_s"] = [round(sv["ttc_p50_s"], 3), round(sv["ttc_p99_s"], 3)]
@@ -535,6 +549,105 @@ def measure_storage(spec, storage: str, steps: int, warmup: int, graphs: bool = 
             "substep_frac_of_measured_hbm": achieved / peaks["hbm_gbs"],
             "stages_ms_per_step": {k[3:]: prof[k] / max(1, prof["steps"]) for k in
                                    ("ms_sink", "ms_substeps", "ms_grid", "ms_rules", "ms_contact", "ms_collect")}}
+
+
+def measure_field_error(spec, storages: tuple, steps: int, checkpoints: tuple = (), nthreads: int = 0) -> dict:
+    """Field error of 16-bit storage against FP64 on the workload at its own
+    size.  Every storage runs its own simulation from the same initial state;
+    before each step its O2 sink (the uptake the agents deposited, which the
+    step's reaction consumes) is copied to the host, and an FP64 evaluation of
+    the field scheme (the oracle's orc_diffuse_f64: implicit sink, then S
+    substeps with decay in every substep) advances with it, so the comparison
+    isolates the storage's rounding from the agents' trajectory.  The drug
+    field takes no sinks, so one FP64 run serves every storage.  Relative L2,
+    maximum and mean absolute error of each field after ``steps`` steps (and
+    at ``checkpoints``)."""
+    import torch
+
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle  # the FP64 evaluation (checker only)
+
+    from oncolytica_b200 import workloads as W
+
+    state0 = W.initial_state(spec)
+    o2_0, drug_0 = W.initial_fields(spec)
+    shp = tuple(spec.field_dims[::-1])
+    engines = {st: W.build_engine(replace(spec, storage=st), state0) for st in storages}
+    ref = {st: np.ascontiguousarray(o2_0, dtype=np.float64) for st in storages}
+    tmp = np.zeros(shp, np.float64)
+    drug = np.ascontiguousarray(drug_0, dtype=np.float64) if spec.has_drug else None
+    enc = {st: {f: eng._backend_impl.field_codec(f)[1] for f in eng._backend_impl.layout.chem_fields}
+           for st, eng in engines.items()}
+    t_cpu = 0.0
+    out = {"steps": steps, "workload": spec.name, "field_dims": list(spec.field_dims),
+           "reference": "oracle orc_diffuse_f64 (FP64) with each run's per-step O2 sinks replayed", "by_step": {}}
+
+    def errors(step: int) -> None:
+        rec = {}
+        for st, eng in engines.items():
+            be = eng._backend_impl
+            fb = be._current()[1]
+            rec[st] = {}
+            for name, r in (("o2", ref[st]), ("drug", drug)):
+                if r is None:
+                    continue
+                got = be._field_values(be.layout.chem_fields.index(name), fb).reshape(shp).astype(np.float64)
+                d = got - r
+                rec[st][name] = {"rel_l2": float(np.linalg.norm(d) / np.linalg.norm(r)),
+                                 "max_abs": float(np.abs(d).max()), "mean_abs": float(np.abs(d).mean()),
+                                 "encoding": int(enc[st][name])}
+        out["by_step"][str(step)] = rec
+
+    for step in range(steps):
+        sinks = {}
+        for st, eng in engines.items():
+            be = eng._backend_impl
+            sinks[st] = be.fields_dev[be.layout.chem_fields.index("o2")][2].cpu().numpy().reshape(shp)
+            eng.run_step()
+        t0 = time.perf_counter()
+        for st in storages:
+            ref[st] = oracle.diffuse_f64(ref[st], sinks[st], spec.dx, spec.dt, spec.D_o2, 0.0, spec.bnd_o2,
+                                         spec.S_o2, nthreads=nthreads, tmp=tmp)
+        if drug is not None:
+            drug = oracle.diffuse_f64(drug, None, spec.dx, spec.dt, spec.D_drug, spec.decay_drug, spec.bnd_drug,
+                                      spec.S_drug, nthreads=nthreads, tmp=tmp)
+        t_cpu += time.perf_counter() - t0
+        if step + 1 in checkpoints and step + 1 != steps:
+            torch.cuda.synchronize()
+            errors(step + 1)
+    torch.cuda.synchronize()
+    errors(steps)
+    out["final"] = out["by_step"][str(steps)]
+    out["status"] = {st: eng._backend_impl.counters()["status"] for st, eng in engines.items()}
+    out["fp64_host_seconds"] = t_cpu
+    for eng in engines.values():
+        eng.close()
+    return out
+
+
+def run_precision_workload(args) -> None:
+    """Field error of the scale workload with 16-bit fields against FP64
+    (``--storages``, ``--steps`` steps; checkpoints every quarter)."""
+    import torch
+
+    rank, world, local = env_ranks()
+    torch.cuda.set_device(local)
+    from oncolytica_b200 import workloads as W
+
+    spec = replace(W.CONFIGS[args.workload_base], seed=W.CONFIGS[args.workload_base].seed + rank)
+    storages = tuple(s for s in args.storages.split(",") if s)
+    cps = tuple(sorted({max(1, args.steps * k // 4) for k in (1, 2, 3)}))
+    r = measure_field_error(spec, storages, args.steps, checkpoints=cps)
+    worst = max(e["rel_l2"] for st in r["final"].values() for e in st.values())
+    line = {"metric": METRIC, "value": worst, "unit": "relative L2 field error vs FP64 (worst field and storage)",
+            "n_gpus": world, "steps": args.steps, "warmup": 0, "ms_per_step": None, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "/".join(storages) + " fields, f32 update",
+            "data": "synthetic (numpy default_rng, seed 0 + rank)",
+            "config": {"workload": f"{spec.name} with 16-bit fields (field error against FP64)",
+                       "field_dims": list(spec.field_dims), "storages": list(storages)},
+            "precision": r}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def measure_batch(n_sims: int, steps: int, warmup: int, graphs: bool = True, solo_sample: int = 0,
@@ -770,6 +883,8 @@ def main() -> None:
         run_batch_workload(args)
     elif args.workload == "serve":
         run_serving_workload(args)
+    elif args.workload == "precision":
+        run_precision_workload(args)
     else:
         run_b200(args)
 

@@ -215,11 +215,17 @@ def diffuse16(bits: np.ndarray, sink: np.ndarray | None, comp: np.ndarray, dx: f
 
 
 def diffuse_f64(f: np.ndarray, sink: np.ndarray | None, dx: float, dt: float, D: float, decay: float,
-                boundary: float, substeps: int, split: bool = False, nthreads: int = 0) -> np.ndarray:
+                boundary: float, substeps: int, split: bool = False, nthreads: int = 0,
+                tmp: np.ndarray | None = None) -> np.ndarray:
     """A field scheme evaluated in FP64: the FP32 scheme (decay in every
-    substep) or, with ``split``, the 16-bit scheme's (decay once per step)."""
-    f = np.ascontiguousarray(f, dtype=np.float64).copy()
-    tmp = np.zeros_like(f)
+    substep) or, with ``split``, the 16-bit scheme's (decay once per step).
+    With ``tmp`` (a float64 array of f's shape) a C-contiguous float64 ``f``
+    is advanced in place and returned (long runs at full size)."""
+    if tmp is not None and f.dtype == np.float64 and f.flags.c_contiguous:
+        assert tmp.shape == f.shape and tmp.dtype == np.float64
+    else:
+        f = np.ascontiguousarray(f, dtype=np.float64).copy()
+        tmp = np.zeros_like(f)
     s = None if sink is None else np.ascontiguousarray(sink, dtype=np.float32)
     dims = np.array([f.shape[2], f.shape[1], f.shape[0]], dtype=np.int32)
     rc = lib().orc_diffuse_f64(_p(f), _p(tmp), _p(s), _p(dims), C.c_double(dx), C.c_double(dt), C.c_double(D),
