@@ -49,6 +49,7 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = as many as --steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graphs", action="store_true", help="eager launches instead of CUDA graphs of whole steps")
+    ap.add_argument("--no-tune", action="store_true", help="default kernel shapes instead of measured ones")
     ap.add_argument("--sims", type=int, default=512, help="members of the batched workload (--workload batch)")
     ap.add_argument("--solo-sample", type=int, default=0, help="members also timed one at a time (--workload batch)")
     ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16", "bf16_sr", "f16_sr"],
@@ -296,9 +297,20 @@ def run_b200(args) -> None:
     spec = replace(base, seed=base.seed + rank)
     state0 = W.initial_state(spec)
     eng = W.build_engine(spec, state0)
+    # kernel shapes and variants measured on this workload (state restored)
+    from oncolytica_b200 import autotune
+
+    tuning = autotune.tune_engine(eng) if not args.no_tune else {"tuning": None}
     eng.set_graphs(not args.no_graphs)
     be = eng._backend_impl
     dev = torch.device("cuda", local)
+
+    def tuned(e):
+        if tuning["tuning"]:
+            t = tuning["tuning"]
+            e._backend_impl.set_tuning(stencil_tile=tuple(t["stencil_tile"]), contact_variant=t["contact_variant"],
+                                       batch_tile_depth=t["batch_tile_depth"])
+        return e
     props = torch.cuda.get_device_properties(dev)
     gpu_id = None
     try:
@@ -333,7 +345,7 @@ def run_b200(args) -> None:
     # dominant kernel's launch time comes from here
     eng.close()
     del eng, be
-    eng = W.build_engine(spec, state0)
+    eng = tuned(W.build_engine(spec, state0))
     be = eng._backend_impl
     eng.run_steps(args.warmup)
     be.set_profiling(True)
@@ -355,7 +367,7 @@ def run_b200(args) -> None:
     eng.close()
     del eng, be
     gc.collect()
-    eng = W.build_engine(spec, state0)
+    eng = tuned(W.build_engine(spec, state0))
     eng.set_graphs(not args.no_graphs)
     be = eng._backend_impl
     eng.run_steps(args.warmup)
@@ -420,6 +432,7 @@ def run_b200(args) -> None:
                 "steps": e2e_steps, "api": "Engine.update_params + Engine.run_step(collect_metrics=True)"},
         "clocks": clk,
         "status": c1["status"],
+        "tuning": autotune.summary(tuning) if tuning["tuning"] else "defaults (--no-tune)",
     }
     if world == 1 and not args.no_extras:
         # the metric's other halves on the same GPU: the batched sweep (FP32
@@ -678,13 +691,25 @@ def measure_batch(n_sims: int, steps: int, warmup: int, graphs: bool = True, sol
         torch.cuda.synchronize(dev)
         return e0.elapsed_time(e1), b.counters()["agent_steps"] - c0["agent_steps"], b
 
-    batch = W.build_batch(specs, states)
+    tune = None
+    if storage == "f32":  # the batched FP32 substep's tile depth per member grid size
+        from oncolytica_b200 import autotune
+
+        tune = autotune.tune_batch(lambda: W.build_batch(specs, states), steps=2)
+
+    def build():
+        b = W.build_batch(specs, states)
+        if tune is not None:
+            autotune.apply_batch(b, tune["depths"])
+        return b
+
+    batch = build()
     batch.set_graphs(graphs)
     ms, agent_steps, batch = timed(batch)
     status = batch.counters()["status"]
     del batch
     torch.cuda.empty_cache()
-    prof_batch = W.build_batch(specs, states)
+    prof_batch = build()
     prof_batch.run_steps(warmup)
     prof_batch.set_profiling(True)
     prof_batch.run_steps(steps)
@@ -701,7 +726,8 @@ def measure_batch(n_sims: int, steps: int, warmup: int, graphs: bool = True, sol
            "stages_ms_per_step": {k[3:]: prof[k] / max(1, prof["steps"]) for k in
                                   ("ms_sink", "ms_substeps", "ms_grid", "ms_rules", "ms_contact", "ms_collect")},
            "gpu_launches_per_step": prof["kernel_launches"] / max(1, prof["steps"]),
-           "graphs": graphs, "status": status, "storage": storage}
+           "graphs": graphs, "status": status, "storage": storage,
+           "tile_depths": tune["depths"] if tune is not None else None}
     if solo_sample:
         idx = np.linspace(0, n_sims - 1, solo_sample).astype(int)
         sub = [specs[i] for i in idx]
@@ -715,6 +741,8 @@ def measure_batch(n_sims: int, steps: int, warmup: int, graphs: bool = True, sol
             solo_as += a
             del e
         bsub = W.build_batch(sub, sub_states)
+        if tune is not None:
+            autotune.apply_batch(bsub, tune["depths"])
         bsub.set_graphs(graphs)
         bm, ba, _ = timed(bsub)
         del bsub

@@ -144,6 +144,31 @@ typedef struct {
 #define OLC_ENC_DEFICIT   1
 #define OLC_ENC_OFFSET3   2
 
+/* Kernel shapes and variants of a handle (olc_set_tuning).  Every choice
+ * gives the same bits; oncolytica_b200.autotune measures them on the
+ * caller's workload and sets the fastest.  No counterpart in the reference
+ * (its dispatches are fixed 256-wide: _gpu_backend.py:134-136). */
+#define OLC_CONTACT_FLAT   0  /* one flat walk over each agent's listed non-empty Moore bins */
+#define OLC_CONTACT_NESTED 1  /* nested loops over the 27 Moore bins                       */
+typedef struct {
+    int32_t stencil_tile_y;   /* FP32 TMA substep tile: rows (8 or 16) ...             */
+    int32_t stencil_tile_z;   /* ... and planes; (y, z) in {(8,8), (16,8), (8,16), (16,4)} */
+    int32_t contact_variant;  /* OLC_CONTACT_FLAT or OLC_CONTACT_NESTED                */
+    int32_t batch_tile_depth; /* planes per tile of the batched FP32 substep: 8, 16 or
+                                 32 (members without their own, olc_set_batch_tile_depths) */
+} OlcTuning;
+
+/* Sets / reads a handle's kernel shapes and variants (OlcTuning; defaults
+ * (8, 8), OLC_CONTACT_FLAT, 16).  Every choice gives the same bits.  Rebuilds
+ * what depends on them (tensor maps, tile lists) and drops captured graphs;
+ * waits for the device. */
+int olc_set_tuning(OlcSim* sim, const OlcTuning* tuning);
+int olc_get_tuning(const OlcSim* sim, OlcTuning* out);
+/* Batch handles: the batched FP32 substep tile depth of each member (n =
+ * members; 0 = the handle's batch_tile_depth), so each grid size can take the
+ * depth measured fastest for it. */
+int olc_set_batch_tile_depths(OlcSim* sim, const int32_t* depths, uint32_t n);
+
 /* Hertz-like contact repulsion (engine/assets/shaders/tumor_sim.wgsl:505-628):
  * for d < r_i + r_j, F += k * delta^(3/2) * (p_i - p_j)/d with
  * delta = r_i + r_j - d; overdamped displacement mobility * F * dt, capped at

@@ -54,7 +54,7 @@ EXPORTS = (
     "olc_engine_metrics", "olc_get_step_state", "olc_set_step_state", "olc_set_mechanics",
     "olc_stage_contact_mech", "olc_stage_contact_motion", "olc_bind_tissue_pair", "olc_current_tissue", "olc_set_rule_iterations",
     "olc_set_pinned", "olc_stage_diffuse_pinned", "olc_sort_noalloc_status", "olc_sort_status_offset",
-    "olc_selftest_bounded_waits",
+    "olc_selftest_bounded_waits", "olc_set_tuning", "olc_get_tuning", "olc_set_batch_tile_depths",
 )
 
 
@@ -175,6 +175,19 @@ class OlcDiffusion(C.Structure):
         ("has_sink", C.c_int32),
         ("storage", C.c_int32),
         ("encoding", C.c_int32),
+    ]
+
+
+OLC_CONTACT_FLAT = 0
+OLC_CONTACT_NESTED = 1
+
+
+class OlcTuning(C.Structure):
+    _fields_ = [
+        ("stencil_tile_y", C.c_int32),
+        ("stencil_tile_z", C.c_int32),
+        ("contact_variant", C.c_int32),
+        ("batch_tile_depth", C.c_int32),
     ]
 
 
@@ -396,6 +409,9 @@ _SIGS = {
     "olc_sort_noalloc_status": (C.c_int, [C.POINTER(C.c_uint32), _VP]),
     "olc_sort_status_offset": (C.c_size_t, []),
     "olc_selftest_bounded_waits": (C.c_int, [C.c_uint32, C.POINTER(C.c_uint32 * 3), _VP]),
+    "olc_set_tuning": (C.c_int, [_VP, C.POINTER(OlcTuning)]),
+    "olc_get_tuning": (C.c_int, [_VP, C.POINTER(OlcTuning)]),
+    "olc_set_batch_tile_depths": (C.c_int, [_VP, C.POINTER(C.c_int32), C.c_uint32]),
 }
 
 _lock = threading.Lock()

@@ -294,6 +294,27 @@ class CudaBackend:
     def set_graphs(self, enable: bool) -> None:
         self._check(self.lib.olc_set_graphs(self.handle, int(bool(enable))))
 
+    # ---- tuning (olc.h OlcTuning; oncolytica_b200.autotune measures it) -------
+    def set_tuning(self, stencil_tile=(8, 8), contact_variant: int = _lib.OLC_CONTACT_FLAT,
+                   batch_tile_depth: int = 16) -> None:
+        t = _lib.OlcTuning(int(stencil_tile[0]), int(stencil_tile[1]), int(contact_variant), int(batch_tile_depth))
+        self._check(self.lib.olc_set_tuning(self.handle, C.byref(t)))
+
+    def get_tuning(self) -> dict:
+        t = _lib.OlcTuning()
+        self._check(self.lib.olc_get_tuning(self.handle, C.byref(t)))
+        return {"stencil_tile": (t.stencil_tile_y, t.stencil_tile_z), "contact_variant": t.contact_variant,
+                "batch_tile_depth": t.batch_tile_depth}
+
+    def has_tma_fields(self) -> bool:
+        """Whether a diffusing FP32 field takes the TMA substep (the tuned tile)."""
+        eng = self.engine
+        return any(STORAGE_CODES[d.storage] == 0 and eng.substeps_for(n) > 0 for n, d in eng._diffusion.items())
+
+    def mech_enabled(self) -> bool:
+        c = self.engine._contact
+        return bool(c is not None and c.mechanics)
+
     def set_profiling(self, enable: bool) -> None:
         self._check(self.lib.olc_set_profiling(self.handle, int(bool(enable))))
 

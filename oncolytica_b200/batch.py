@@ -191,6 +191,19 @@ class BatchEngine:
         self.use_graphs = bool(enable)
         self._check(self.lib.olc_set_graphs(self.handle, int(self.use_graphs)))
 
+    def set_tuning(self, stencil_tile=(8, 8), contact_variant: int = _lib.OLC_CONTACT_FLAT,
+                   batch_tile_depth: int = 16) -> None:
+        """Kernel shapes and variants of the batch handle (olc_set_tuning)."""
+        t = _lib.OlcTuning(int(stencil_tile[0]), int(stencil_tile[1]), int(contact_variant), int(batch_tile_depth))
+        self._check(self.lib.olc_set_tuning(self.handle, C.byref(t)))
+
+    def set_tile_depths(self, depths) -> None:
+        """The batched FP32 substep tile depth of each member (8, 16, 32; 0 =
+        the handle's); oncolytica_b200.autotune.tune_batch measures them."""
+        arr = (C.c_int32 * len(self.engines))(*[int(d) for d in depths])
+        self._check(self.lib.olc_set_batch_tile_depths(self.handle, arr, len(self.engines)))
+        self.tile_depths = [int(d) for d in depths]
+
     def set_profiling(self, enable: bool) -> None:
         self._check(self.lib.olc_set_profiling(self.handle, int(bool(enable))))
 

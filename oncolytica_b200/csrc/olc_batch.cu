@@ -239,7 +239,8 @@ __global__ void __launch_bounds__(128) k_substep_batch(const uint4* __restrict__
     float* out = (flip ? fa : fb) + d.field_off;
     const int x = (int)t.y * BT_X + 4 * (threadIdx.x & 7);
     const int y = (int)t.z * BT_Y + (threadIdx.x >> 3);
-    const int z0 = (int)t.w * BT_Z;
+    const int depth = (int)(t.w >> 16);  // the member's tile depth (8, 16 or 32 planes)
+    const int z0 = (int)(t.w & 0xffffu) * depth;
     if (x >= nx || y >= ny) return;
     const size_t sy = (size_t)nx, sz = (size_t)nx * ny;
     const bool edge_y = y == 0 || y == ny - 1;
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(128) k_substep_batch(const uint4* __restrict__
     size_t idx = (size_t)z0 * sz + (size_t)y * sy + x;
     float4 zm = z0 > 0 ? ld4(in + idx - sz) : zero;
     float4 c = ld4(in + idx);
-    const int z1 = min(z0 + BT_Z, nz);
+    const int z1 = min(z0 + depth, nz);
     for (int zz = z0; zz < z1; ++zz, idx += sz) {
         const float4 zp = zz + 1 < nz ? ld4(in + idx + sz) : zero;
         const float4 ym = y > 0 ? ld4(in + idx - sy) : zero;

@@ -14,8 +14,6 @@
 // order with separately rounded operations.
 #include "olc_internal.h"
 
-#include <cstdlib>
-#include <cstring>
 
 namespace olc {
 
@@ -294,7 +292,6 @@ __device__ __forceinline__ void contact_pair(const float4& p, const float4& q, o
 }
 
 constexpr int CF_THREADS = 128;
-template <int DEPTH>
 __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __restrict__ posr,
                                                             const uint2* __restrict__ ranges, const olc_u32* n_dev,
                                                             olc_u32 n_host, ContactDev c, float* __restrict__ xo,
@@ -327,69 +324,32 @@ __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __res
             }
         }
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-        if (DEPTH == 1) {
-            // the next candidate's record is requested before this one is used
-            int b = 0;
-            olc_u32 j = 0, end = 0;
-            float4 q = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
-            if (nb > 0) {
-                const uint2 r = s_bins[0][t];
-                j = r.x;
-                end = r.y;
-                q = __ldg(posr + j);
-            }
-            while (b < nb) {
-                olc_u32 jn = j + 1, en = end;
-                int bn = b;
-                if (jn == en) {
-                    if (++bn < nb) {
-                        const uint2 r = s_bins[bn][t];
-                        jn = r.x;
-                        en = r.y;
-                    }
+        // the next candidate's record is requested before this one is used
+        int b = 0;
+        olc_u32 j = 0, end = 0;
+        float4 q = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+        if (nb > 0) {
+            const uint2 r = s_bins[0][t];
+            j = r.x;
+            end = r.y;
+            q = __ldg(posr + j);
+        }
+        while (b < nb) {
+            olc_u32 jn = j + 1, en = end;
+            int bn = b;
+            if (jn == en) {
+                if (++bn < nb) {
+                    const uint2 r = s_bins[bn][t];
+                    jn = r.x;
+                    en = r.y;
                 }
-                const float4 qn = bn < nb ? __ldg(posr + jn) : q;
-                contact_pair(p, q, i, j, c, fx, fy, fz);
-                j = jn;
-                end = en;
-                b = bn;
-                q = qn;
             }
-        } else if (nb > 0) {
-            // two records ahead: slots 0 (in use), 1 and 2 (requested); the
-            // cursor (bc, jc, ec) is slot 2's position
-            int bc = 0;
-            uint2 r = s_bins[0][t];
-            olc_u32 jc = r.x, ec = r.y;
-            auto advance = [&]() -> bool {
-                if (++jc == ec && ++bc < nb) {
-                    const uint2 rn = s_bins[bc][t];
-                    jc = rn.x;
-                    ec = rn.y;
-                }
-                return bc < nb;
-            };
-            olc_u32 j0 = jc;
-            float4 q0 = __ldg(posr + j0);
-            bool v1 = advance();
-            olc_u32 j1 = jc;
-            float4 q1 = v1 ? __ldg(posr + j1) : q0;
-            bool v2 = advance();
-            olc_u32 j2 = jc;
-            float4 q2 = v2 ? __ldg(posr + j2) : q0;
-            bool v0 = true;
-            while (v0) {
-                contact_pair(p, q0, i, j0, c, fx, fy, fz);
-                j0 = j1;
-                q0 = q1;
-                v0 = v1;
-                j1 = j2;
-                q1 = q2;
-                v1 = v2;
-                v2 = v2 && advance();
-                j2 = jc;
-                if (v2) q2 = __ldg(posr + j2);
-            }
+            const float4 qn = bn < nb ? __ldg(posr + jn) : q;
+            contact_pair(p, q, i, j, c, fx, fy, fz);
+            j = jn;
+            end = en;
+            b = bn;
+            q = qn;
         }
         float mx = __fmul_rn(fx, md), my = __fmul_rn(fy, md), mz = __fmul_rn(fz, md);
         const float len = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz)));
@@ -405,150 +365,18 @@ __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __res
     }
 }
 
-// The flat walk with the bin list in a register instead of shared memory: bit
-// b of `todo` marks Moore bin b (dz, dy, dx order, x fastest) as in the grid
-// and non-empty.  A bin's row range is loaded again when the walk reaches it
-// (the listing pass brought it into L1), and the next bin's range is requested
-// when the walk enters a bin, so it is ready at the switch.  No shared memory:
-// the SM's L1 holds neighbour records instead, and occupancy is set by
-// registers alone.  Same candidates, order and arithmetic as k_contact_flat.
-__device__ __forceinline__ uint2 moore_range(const uint2* __restrict__ ranges, int cx, int cy, int cz, int b) {
-    const int dz = b / 9 - 1, dy = (b / 3) % 3 - 1, dx = b % 3 - 1;
-    return __ldg(ranges + olc_tissue_key(cx + dx, cy + dy, cz + dz));
-}
-
-template <int MINB>
-__global__ void __launch_bounds__(CF_THREADS, MINB) k_contact_bits(const float4* __restrict__ posr,
-                                                             const uint2* __restrict__ ranges, const olc_u32* n_dev,
-                                                             olc_u32 n_host, ContactDev c, float* __restrict__ xo,
-                                                             float* __restrict__ yo, float* __restrict__ zo) {
-    const olc_u32 n = n_dev ? *n_dev : n_host;
-    const float md = __fmul_rn(c.mobility, c.dt);
-    for (olc_u32 i = blockIdx.x * CF_THREADS + threadIdx.x; i < n; i += gridDim.x * CF_THREADS) {
-        const float4 p = posr[i];
-        if (p.w < 0.0f) continue;  // dead this step: no move, no force
-        const int cx = olc_bin_coord(p.x, c.tvs, c.tdims[0]);
-        const int cy = olc_bin_coord(p.y, c.tvs, c.tdims[1]);
-        const int cz = olc_bin_coord(p.z, c.tvs, c.tdims[2]);
-        olc_u32 todo = 0;
-        for (int dz = -1; dz <= 1; ++dz) {
-            const int nz = cz + dz;
-            if (nz < 0 || nz >= c.tdims[2]) continue;
-            for (int dy = -1; dy <= 1; ++dy) {
-                const int ny = cy + dy;
-                if (ny < 0 || ny >= c.tdims[1]) continue;
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const int nx = cx + dx;
-                    if (nx < 0 || nx >= c.tdims[0]) continue;
-                    const uint2 rg = __ldg(ranges + olc_tissue_key(nx, ny, nz));
-                    if (rg.y > rg.x) todo |= 1u << ((dz + 1) * 9 + (dy + 1) * 3 + (dx + 1));
-                }
-            }
-        }
-        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-        if (todo) {
-            // (j, end): the current bin; nxt: the range of the lowest bin left in todo
-            uint2 r = moore_range(ranges, cx, cy, cz, __ffs(todo) - 1);
-            todo &= todo - 1;
-            uint2 nxt = todo ? moore_range(ranges, cx, cy, cz, __ffs(todo) - 1) : make_uint2(0u, 0u);
-            olc_u32 j = r.x, end = r.y;
-            float4 q = __ldg(posr + j);
-            bool live = true;
-            while (live) {
-                olc_u32 jn = j + 1, en = end;
-                if (jn == en) {
-                    if (todo) {
-                        jn = nxt.x;
-                        en = nxt.y;
-                        todo &= todo - 1;
-                        if (todo) nxt = moore_range(ranges, cx, cy, cz, __ffs(todo) - 1);
-                    } else {
-                        live = false;
-                    }
-                }
-                const float4 qn = live ? __ldg(posr + jn) : q;
-                contact_pair(p, q, i, j, c, fx, fy, fz);
-                j = jn;
-                end = en;
-                q = qn;
-            }
-        }
-        float mx = __fmul_rn(fx, md), my = __fmul_rn(fy, md), mz = __fmul_rn(fz, md);
-        const float len = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz)));
-        if (len > c.max_disp) {
-            const float sc = __fdiv_rn(c.max_disp, len);
-            mx = __fmul_rn(mx, sc);
-            my = __fmul_rn(my, sc);
-            mz = __fmul_rn(mz, sc);
-        }
-        xo[i] = fminf(fmaxf(__fadd_rn(p.x, mx), c.lo[0]), c.hi[0]);
-        yo[i] = fminf(fmaxf(__fadd_rn(p.y, my), c.lo[1]), c.hi[1]);
-        zo[i] = fminf(fmaxf(__fadd_rn(p.z, mz), c.lo[2]), c.hi[2]);
-    }
-}
-
-// k_contact_flat is the default; OLC_CONTACT=nested selects k_contact (same
-// bits; over the 200 benchmark steps of the 1 M-agent scale workload 0.92 ms
-// vs 1.04 ms per step).
-// OLC_CONTACT=bits selects k_contact_bits (registers as the compiler
-// chooses), OLC_CONTACT=bits12 the build capped for 12 CTAs per SM.
-static int contact_kind() {
-    static int v = -1;
-    if (v < 0) {
-        const char* e = getenv("OLC_CONTACT");
-        v = (e && e[0] == 'n') ? 0 : (e && e[0] == 'b') ? (strcmp(e, "bits12") == 0 ? 3 : 2) : 1;
-    }
-    return v;
-}
-static bool contact_flat() { return contact_kind() != 0; }
-
-// OLC_CONTACT_PREFETCH=2 keeps two neighbour records in flight per thread
-// instead of one (same bits).
-static bool contact_prefetch2() {
-    static int v = -1;
-    if (v < 0) {
-        const char* e = getenv("OLC_CONTACT_PREFETCH");
-        v = (e && e[0] == '2') ? 1 : 0;
-    }
-    return v == 1;
-}
-
-// OLC_CONTACT_CARVEOUT=<percent> sets the shared-memory carveout preference of
-// k_contact_flat (its bin lists take shared memory that neighbour loads would
-// otherwise find in L1); unset leaves the driver's choice.
-static void contact_flat_carveout() {
-    static int done = 0;
-    if (done) return;
-    done = 1;
-    const char* e = getenv("OLC_CONTACT_CARVEOUT");
-    if (!e) return;
-    const int pct = atoi(e);
-    if (pct >= 0 && pct <= 100)
-        {
-        cudaFuncSetAttribute(k_contact_flat<1>, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
-        cudaFuncSetAttribute(k_contact_flat<2>, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
-    }
-}
-
+// The two walks (olc.h OLC_CONTACT_*): bit-identical, chosen per handle by
+// measurement (OlcTuning.contact_variant).  On the 1 M-agent scale workload
+// the flat walk took 0.92 ms per step over 200 steps against 1.04 for the
+// nested loops; sparser or denser populations can order them the other way.
 void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
-                    olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s) {
-    if (contact_flat()) {
-        contact_flat_carveout();
+                    olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s, int variant) {
+    if (variant != OLC_CONTACT_NESTED) {
         olc_u32 blocks = (n_cap + CF_THREADS - 1) / CF_THREADS;
         if (blocks == 0) blocks = 1;
         if (blocks > 148 * 16) blocks = 148 * 16;
-        if (contact_kind() == 2)
-            k_contact_bits<1><<<blocks, CF_THREADS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_dev,
-                                                            n_host, c, x, y, z);
-        else if (contact_kind() == 3)
-            k_contact_bits<12><<<blocks, CF_THREADS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_dev,
-                                                             n_host, c, x, y, z);
-        else if (contact_prefetch2())
-            k_contact_flat<2><<<blocks, CF_THREADS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_dev,
-                                                            n_host, c, x, y, z);
-        else
-            k_contact_flat<1><<<blocks, CF_THREADS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_dev,
-                                                            n_host, c, x, y, z);
+        k_contact_flat<<<blocks, CF_THREADS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_dev, n_host, c,
+                                                      x, y, z);
         return;
     }
     olc_u32 blocks = (n_cap + 255) / 256;

@@ -135,23 +135,17 @@ float* run_substeps(float* a, float* b, const FieldStep& fs, cudaStream_t s, con
 // buffers for the single-substep kernel and for the T-substep temporal block.
 struct FieldMaps {
     bool ok = false;
-    int T = 1, TY = 8, TZ = 16;
-    int VY = 0, VZ = 0;          // 4-wide single-substep kernel shape (0 = scalar k_substep_tma)
-    int PY = 0, PZ = 0, PN = 0;  // persistent pipelined shape (0 = one tile per CTA)
-    int T2Y = 0, T2Z = 0, T2N = 0;  // two-substeps-per-pass shape (0 = one substep per pass)
-    CUtensorMap single[2];
-    CUtensorMap block[2];
+    int VY = 8, VZ = 8;  // tile of k_substep_x4: rows and planes (a compiled shape)
     CUtensorMap vec[2];
-    CUtensorMap pipe[2];
-    CUtensorMap t2[2];
 };
-bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3]);
+// The TMA tensor maps of a FP32 field's two buffers for the (tile_y, tile_z)
+// tile; false when the tile is not compiled in or the field cannot be mapped
+// (the plain kernel runs then).
+bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3], int tile_y = 8, int tile_z = 8);
+bool stencil_tile_known(int tile_y, int tile_z);
 // Runs fs.substeps substeps starting from a (buffer index a_index of m).
 float* run_substeps_tma(float* a, float* b, const FieldMaps& m, int a_index, const FieldStep& fs, olc_u32* status,
                         cudaStream_t s, const Pins* pins = nullptr);
-int launches_for(const FieldMaps& m, int substeps);
-// OLC_STENCIL=plain in the environment selects the register-column kernel.
-bool stencil_tma_enabled();
 bool encode_map_elems(CUtensorMap* map, void* base, const int dims[3], const cuuint32_t box[3], int elem_bytes);
 
 // 16-bit field storage (olc_field16.cu): fields stored as BF16 or FP16,
@@ -180,7 +174,8 @@ struct ContactDev {
     float lo[3], hi[3];
 };
 void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
-                    olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s);
+                    olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s,
+                    int variant = OLC_CONTACT_FLAT);
 // The rest of the engine's force law (OlcMechanics): necrotic repulsion
 // factor, adhesion, damped velocity integration.
 struct MechDev {

@@ -69,6 +69,8 @@ struct OlcSim {
     int field_cur[OLC_MAX_FIELDS] = {};
     bool field_bound[OLC_MAX_FIELDS] = {};
     FieldMaps fmaps[OLC_MAX_FIELDS];           // TMA descriptors of both buffers
+    OlcTuning tuning = {8, 8, OLC_CONTACT_FLAT, 16};  // kernel shapes and variants (olc_set_tuning)
+    std::vector<int> member_depth;                    // batched FP32 tile depth per member (0: tuning's)
     FieldMaps16 fmaps16[OLC_MAX_FIELDS];       // the same for 16-bit storage
     float* comp[OLC_MAX_FIELDS] = {};          // 16-bit storage: reaction residual per voxel (FP32)
     Pins pins[OLC_MAX_FIELDS] = {};            // voxels held at a value after every substep
@@ -359,16 +361,14 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
         }
         float* a = s->field[cur][f];
         float* b = s->field[1 - cur][f];
-        const bool tma_path = s->fmaps[f].ok && stencil_tma_enabled();
+        const bool tma_path = s->fmaps[f].ok;
         const Pins* pins = s->pins[f].n ? &s->pins[f] : nullptr;
         float* res = tma_path ? run_substeps_tma(a, b, s->fmaps[f], cur, s->fstep[f], s->counters + OLC_CTR_STATUS, st,
                                                  pins)
                               : run_substeps(a, b, s->fstep[f], st, pins);
         s->field_cur[f] = (res == a) ? cur : 1 - cur;
         substeps += (uint32_t)s->fstep[f].substeps;
-        launches += (uint64_t)(pins ? 2 * s->fstep[f].substeps
-                                    : (tma_path ? launches_for(s->fmaps[f], s->fstep[f].substeps)
-                                                : s->fstep[f].substeps));
+        launches += (uint64_t)(pins ? 2 * s->fstep[f].substeps : s->fstep[f].substeps);
     }
     mark(s, 2, st);
     // 2. grid + compaction
@@ -465,7 +465,7 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
     } else if (s->contact.enabled) {
         launch_contact(s->posr, s->ranges, s->counters + OLC_CTR_N, 0, cap, s->contact_dev,
                        static_cast<float*>(s->col[cc][0]), static_cast<float*>(s->col[cc][1]),
-                       static_cast<float*>(s->col[cc][2]), st);
+                       static_cast<float*>(s->col[cc][2]), st, s->tuning.contact_variant);
         ++launches;
     }
     mark(s, 5, st);
@@ -787,16 +787,27 @@ void pool_tiles(const OlcGeom& g, olc_u32 slot, std::vector<uint4>* out) {
             for (int x = 0; x < tx; ++x) out->push_back(make_uint4(slot, (unsigned)x, (unsigned)y, (unsigned)z));
 }
 
-// Substep tiles of one member for the substep kernel of `storage`.
-void substep_tiles(const OlcGeom& g, olc_u32 k, int storage, std::vector<uint4>* out) {
+// Substep tiles of one member for the substep kernel of `storage`.  FP32
+// tiles are 32 x 16 x depth (depth 8, 16 or 32: the member's tile depth); the
+// entry's w word holds the z-tile index in its low half and the depth in its
+// high half.
+void substep_tiles(const OlcGeom& g, olc_u32 k, int storage, int depth, std::vector<uint4>* out) {
     const bool f32 = storage == OLC_FIELD_F32;
     const int TX = f32 ? BATCH_TILE_X : BATCH_T16_TX, TY = f32 ? BATCH_TILE_Y : BATCH_T16_TY;
-    const int TZ = f32 ? BATCH_TILE_Z : BATCH_T16_TZ;
+    const int TZ = f32 ? depth : BATCH_T16_TZ;
     const int tx = (g.chem_dims[0] + TX - 1) / TX, ty = (g.chem_dims[1] + TY - 1) / TY;
     const int tz = (g.chem_dims[2] + TZ - 1) / TZ;
     for (int z = 0; z < tz; ++z)
         for (int y = 0; y < ty; ++y)
-            for (int x = 0; x < tx; ++x) out->push_back(make_uint4(k, (unsigned)x, (unsigned)y, (unsigned)z));
+            for (int x = 0; x < tx; ++x)
+                out->push_back(make_uint4(k, (unsigned)x, (unsigned)y, f32 ? ((unsigned)z | ((unsigned)depth << 16))
+                                                                           : (unsigned)z));
+}
+
+// The batched FP32 substep tile depth of member k.
+int member_tile_depth(const OlcSim* s, olc_u32 k) {
+    const int d = k < s->member_depth.size() ? s->member_depth[k] : 0;
+    return d > 0 ? d : s->tuning.batch_tile_depth;
 }
 
 // Tensor maps of member k's grid of field f in buffers a and b (its voxels
@@ -856,7 +867,7 @@ int pool_commit(OlcSim* s, cudaStream_t st) {
         std::vector<uint4> mt;
         for (const auto& o : order) {
             mt.clear();
-            substep_tiles(s->geoms[o.second], o.second, s->fstep[f].storage, &mt);
+            substep_tiles(s->geoms[o.second], o.second, s->fstep[f].storage, member_tile_depth(s, o.second), &mt);
             fl[f].insert(fl[f].end(), mt.begin(), mt.end());
             steps_of.insert(steps_of.end(), mt.size(), o.first);
         }
@@ -1228,7 +1239,8 @@ int olc_bind_field_ex(OlcSim* s, int index, void* a_, void* b_, float* sink, flo
     s->field[1][index] = b;
     s->fmaps[index].ok = false;
     s->fmaps16[index].ok = false;
-    if (spec->substeps > 0 && !half) make_field_maps(&s->fmaps[index], a, b, s->geom.chem_dims);
+    if (spec->substeps > 0 && !half)
+        make_field_maps(&s->fmaps[index], a, b, s->geom.chem_dims, s->tuning.stencil_tile_y, s->tuning.stencil_tile_z);
     if (spec->substeps > 0 && half && !make_field_maps16(&s->fmaps16[index], a, b, s->geom.chem_dims))
         return fail(s, OLC_ERR_ARG, "olc_bind_field_ex: TMA descriptors of the 16-bit field failed (16-byte aligned "
                                     "buffers, x extent a multiple of 8)");
@@ -1744,6 +1756,41 @@ int olc_read_user_metrics(OlcSim* s, void* out, size_t bytes, void* stream) {
 
 // ------------------------------------------------------------------ batched mode
 
+// The substep tile list of field `index` of a batch handle: members taking the
+// most substeps first (stable), so substep s launches a prefix of the list;
+// btile_count[index][s] is that prefix's length.
+static int build_batch_field_tiles(OlcSim* s, int index) {
+    const olc_u32 F = s->caps.n_fields;
+    std::vector<std::pair<int, olc_u32>> order;  // (substeps, simulation)
+    for (olc_u32 k = 0; k < s->n_sims; ++k) order.push_back({s->bsteps_host[(size_t)k * F + index].substeps, k});
+    std::stable_sort(order.begin(), order.end(),
+                     [](const std::pair<int, olc_u32>& x, const std::pair<int, olc_u32>& y) { return x.first > y.first; });
+    std::vector<uint4> tiles, mt;
+    std::vector<int> tile_steps;
+    for (const auto& o : order) {
+        mt.clear();
+        substep_tiles(s->geoms[o.second], o.second, s->fstep[index].storage, member_tile_depth(s, o.second), &mt);
+        tiles.insert(tiles.end(), mt.begin(), mt.end());
+        tile_steps.insert(tile_steps.end(), mt.size(), o.first);
+    }
+    const int max_s = order.empty() ? 0 : order.front().first;
+    std::vector<olc_u32> count(max_s, 0u);
+    for (int sub = 0; sub < max_s; ++sub) {
+        olc_u32 c = 0;
+        while (c < tiles.size() && tile_steps[c] > sub) ++c;
+        count[sub] = c;
+    }
+    cudaFree(s->btiles_field[index]);
+    s->btiles_field[index] = nullptr;
+    OLC_TRY(dev_alloc(s, &s->btiles_field[index], sizeof(uint4) * std::max<size_t>(1, tiles.size()), "field tiles"));
+    if (!tiles.empty())
+        OLC_TRY(check(s, cudaMemcpy(s->btiles_field[index], tiles.data(), sizeof(uint4) * tiles.size(),
+                                    cudaMemcpyHostToDevice),
+                      "upload field tiles"));
+    s->btile_count[index] = count;
+    return OLC_OK;
+}
+
 int olc_bind_field_batch(OlcSim* s, int index, void* a_, void* b_, float* sink, float* comp,
                          const OlcDiffusion* specs) {
     float* a = static_cast<float*>(a_);
@@ -1768,7 +1815,6 @@ int olc_bind_field_batch(OlcSim* s, int index, void* a_, void* b_, float* sink, 
     if (storage != OLC_FIELD_F32 && !comp)
         return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: 16-bit storage needs a compensation buffer");
     bool any_sink = false;
-    std::vector<std::pair<int, olc_u32>> order;  // (substeps, simulation)
     for (olc_u32 k = 0; k < s->n_sims; ++k) {
         const OlcDiffusion& spec = specs[k];
         const OlcGeom& g = s->geoms[k];
@@ -1788,22 +1834,10 @@ int olc_bind_field_batch(OlcSim* s, int index, void* a_, void* b_, float* sink, 
         }
         any_sink = any_sink || (spec.has_sink && spec.substeps != 0);
         s->bsteps_host[(size_t)k * F + index] = fs;
-        order.push_back({fs.substeps, k});
     }
     if (any_sink && !sink) return fail(s, OLC_ERR_ARG, "olc_bind_field_batch: has_sink without a sink buffer");
     drop_graphs(s);
-    // tiles of this field, simulations taking the most substeps first (stable)
-    std::stable_sort(order.begin(), order.end(),
-                     [](const std::pair<int, olc_u32>& x, const std::pair<int, olc_u32>& y) { return x.first > y.first; });
-    // substep tiles of the TMA kernel's geometry, and each member's tensor maps
-    std::vector<uint4> tiles, mt;
-    std::vector<int> tile_steps;
-    for (const auto& o : order) {
-        mt.clear();
-        substep_tiles(s->geoms[o.second], o.second, storage, &mt);
-        tiles.insert(tiles.end(), mt.begin(), mt.end());
-        tile_steps.insert(tile_steps.end(), mt.size(), o.first);
-    }
+    // each member's tensor maps (16-bit storage)
     for (olc_u32 k = 0; k < s->n_sims; ++k)
         if (storage != OLC_FIELD_F32 && specs[k].substeps != 0 &&
             !member_maps(s, k, index, a, b, s->field_off[k], s->geoms[k], storage))
@@ -1812,21 +1846,8 @@ int olc_bind_field_batch(OlcSim* s, int index, void* a_, void* b_, float* sink, 
     OLC_TRY(check(s, cudaMemcpy(s->bmaps_dev, s->bmaps_host.data(), sizeof(CUtensorMap) * s->bmaps_host.size(),
                                 cudaMemcpyHostToDevice),
                   "upload tensor maps"));
-    const int max_s = order.empty() ? 0 : order.front().first;
-    std::vector<olc_u32> count(max_s, 0u);
-    for (int sub = 0; sub < max_s; ++sub) {
-        olc_u32 c = 0;
-        while (c < tiles.size() && tile_steps[c] > sub) ++c;
-        count[sub] = c;
-    }
-    cudaFree(s->btiles_field[index]);
-    s->btiles_field[index] = nullptr;
-    OLC_TRY(dev_alloc(s, &s->btiles_field[index], sizeof(uint4) * std::max<size_t>(1, tiles.size()), "field tiles"));
-    if (!tiles.empty())
-        OLC_TRY(check(s, cudaMemcpy(s->btiles_field[index], tiles.data(), sizeof(uint4) * tiles.size(),
-                                    cudaMemcpyHostToDevice),
-                      "upload field tiles"));
-    s->btile_count[index] = count;
+    s->fstep[index].storage = storage;
+    OLC_TRY(build_batch_field_tiles(s, index));
     OLC_TRY(check(s, cudaMemcpy(s->bsteps_dev, s->bsteps_host.data(), sizeof(FieldStep) * s->bsteps_host.size(),
                                 cudaMemcpyHostToDevice),
                   "upload field steps"));
@@ -2354,7 +2375,7 @@ int olc_stage_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], 
     FieldMaps maps;
     olc_u32* status = stage_status_word();
     float* res;
-    if (stencil_tma_enabled() && status && make_field_maps(&maps, f, tmp, dims)) {
+    if (status && make_field_maps(&maps, f, tmp, dims)) {
         launch_sink(f, spec->has_sink ? sink : nullptr, fs, st);
         res = run_substeps_tma(f, tmp, maps, 0, fs, status, st);
     } else {
@@ -2381,7 +2402,7 @@ int olc_stage_diffuse_pinned(float* f, float* tmp, float* sink, const int32_t di
     FieldMaps maps;
     olc_u32* status = stage_status_word();
     float* res;
-    if (stencil_tma_enabled() && status && make_field_maps(&maps, f, tmp, dims)) {
+    if (status && make_field_maps(&maps, f, tmp, dims)) {
         launch_sink(f, spec->has_sink ? sink : nullptr, fs, st);
         res = run_substeps_tma(f, tmp, maps, 0, fs, status, st, &pins);
     } else {
@@ -2540,3 +2561,55 @@ int olc_stage_contact_motion(const float* posr, const uint32_t* ranges, uint32_t
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ tuning
+int olc_set_tuning(OlcSim* s, const OlcTuning* t) {
+    if (!s || !t) return fail(s, OLC_ERR_ARG, "olc_set_tuning: null argument");
+    if (!stencil_tile_known(t->stencil_tile_y, t->stencil_tile_z))
+        return fail(s, OLC_ERR_ARG, "olc_set_tuning: stencil tile (" + std::to_string(t->stencil_tile_y) + ", " +
+                                        std::to_string(t->stencil_tile_z) +
+                                        ") is not one of (8,8), (16,8), (8,16), (16,4)");
+    if (t->contact_variant != OLC_CONTACT_FLAT && t->contact_variant != OLC_CONTACT_NESTED)
+        return fail(s, OLC_ERR_ARG, "olc_set_tuning: contact_variant must be OLC_CONTACT_FLAT or OLC_CONTACT_NESTED");
+    if (t->batch_tile_depth != 8 && t->batch_tile_depth != 16 && t->batch_tile_depth != 32)
+        return fail(s, OLC_ERR_ARG, "olc_set_tuning: batch_tile_depth must be 8, 16 or 32");
+    OLC_TRY(check(s, cudaDeviceSynchronize(), "sync"));
+    drop_graphs(s);
+    const bool depth_changed = t->batch_tile_depth != s->tuning.batch_tile_depth;
+    s->tuning = *t;
+    // solo handles: the FP32 fields' tensor maps for the new tile
+    if (!s->n_sims) {
+        for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
+            if (!s->field_bound[f] || s->fstep[f].storage != OLC_FIELD_F32 || s->fstep[f].substeps == 0) continue;
+            make_field_maps(&s->fmaps[f], s->field[0][f], s->field[1][f], s->geom.chem_dims, t->stencil_tile_y,
+                            t->stencil_tile_z);
+        }
+    } else if (depth_changed && !s->pool) {
+        for (olc_u32 f = 0; f < s->caps.n_fields; ++f)
+            if (s->field_bound[f] && s->fstep[f].storage == OLC_FIELD_F32) OLC_TRY(build_batch_field_tiles(s, (int)f));
+    } else if (depth_changed) {
+        s->pool_dirty = true;
+    }
+    return OLC_OK;
+}
+
+int olc_get_tuning(const OlcSim* s, OlcTuning* out) {
+    if (!s || !out) return fail(nullptr, OLC_ERR_ARG, "olc_get_tuning: null argument");
+    *out = s->tuning;
+    return OLC_OK;
+}
+
+int olc_set_batch_tile_depths(OlcSim* s, const int32_t* depths, uint32_t n) {
+    if (!s) return fail(nullptr, OLC_ERR_ARG, "null handle");
+    if (!s->n_sims || s->pool) return fail(s, OLC_ERR_STATE, "olc_set_batch_tile_depths: not a batch handle");
+    if (n != s->n_sims || !depths) return fail(s, OLC_ERR_ARG, "olc_set_batch_tile_depths: one depth per member");
+    for (uint32_t k = 0; k < n; ++k)
+        if (depths[k] != 0 && depths[k] != 8 && depths[k] != 16 && depths[k] != 32)
+            return fail(s, OLC_ERR_ARG, "olc_set_batch_tile_depths: depths must be 0 (the handle's), 8, 16 or 32");
+    OLC_TRY(check(s, cudaDeviceSynchronize(), "sync"));
+    drop_graphs(s);
+    s->member_depth.assign(depths, depths + n);
+    for (olc_u32 f = 0; f < s->caps.n_fields; ++f)
+        if (s->field_bound[f] && s->fstep[f].storage == OLC_FIELD_F32) OLC_TRY(build_batch_field_tiles(s, (int)f));
+    return OLC_OK;
+}
