@@ -27,7 +27,8 @@ import threading
 from oncolytica_b200 import _lib
 
 STENCIL_TILES = ((8, 8), (16, 8), (8, 16), (16, 4))
-CONTACT_VARIANTS = (_lib.OLC_CONTACT_FLAT, _lib.OLC_CONTACT_NESTED)
+CONTACT_VARIANTS = (_lib.OLC_CONTACT_FLAT, _lib.OLC_CONTACT_NESTED, _lib.OLC_CONTACT_BRICK)
+CONTACT_NAMES = {_lib.OLC_CONTACT_FLAT: "flat", _lib.OLC_CONTACT_NESTED: "nested", _lib.OLC_CONTACT_BRICK: "brick"}
 BATCH_DEPTHS = (8, 16, 32)
 DEFAULT = {"stencil_tile": (8, 8), "contact_variant": _lib.OLC_CONTACT_FLAT, "batch_tile_depth": 16}
 
@@ -122,7 +123,7 @@ def tune_engine(eng, steps: int = 4, cache: bool = True) -> dict:
             for v in CONTACT_VARIANTS:
                 times[v] = _measure(eng, sd, dict(best, contact_variant=v), "ms_contact", steps)
             best["contact_variant"] = min(times, key=times.get)
-            measured["contact"] = {("flat" if v == _lib.OLC_CONTACT_FLAT else "nested"): t for v, t in times.items()}
+            measured["contact"] = {CONTACT_NAMES[v]: t for v, t in times.items()}
     finally:
         be.set_tuning(**best)
         be.load_state_dict(sd)

@@ -365,12 +365,160 @@ __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __res
     }
 }
 
+// ---------------------------------------------------------------- bin bricks
+// k_contact_brick: one CTA per 2 x 2 x 2 brick of bins.  The hierarchical
+// Morton key of a bin is its brick's Morton code followed by three parity
+// bits, so the 8 bins of brick B are keys 8B .. 8B+7 and their agents are
+// consecutive sorted rows.  The CTA stages the records of the 4 x 4 x 4 bins
+// around the brick (the Moore neighbourhoods of all its bins) in shared
+// memory, with each bin's first row, once; then every home agent walks its 27
+// bins there in the same order as k_contact (dz, dy, dx, x fastest; rows
+// ascending) with the same pair law, so the sums are identical.  An agent
+// whose current position left the brick since the sort (a division offset),
+// and every agent of a brick whose halo holds more records than the staging
+// buffer, take k_contact's walk over global memory instead.
+constexpr int CB_THREADS = 64;
+constexpr int CB_CAP = 768;  // staged records per brick (12 KB)
+
+__device__ __forceinline__ olc_u32 olc_compact9(olc_u32 x) {
+    x &= 0x09249249u;
+    x = (x | (x >> 2)) & 0x030c30c3u;
+    x = (x | (x >> 4)) & 0x0300f00fu;
+    x = (x | (x >> 8)) & 0x030000ffu;
+    x = (x | (x >> 16)) & 0x000001ffu;
+    return x;
+}
+
+// k_contact's walk for agent i at p (global memory), summed into f.
+__device__ __forceinline__ void contact_walk_global(const float4* __restrict__ posr, const uint2* __restrict__ ranges,
+                                                    const float4& p, olc_u32 i, const ContactDev& c, float& fx,
+                                                    float& fy, float& fz) {
+    const int cx = olc_bin_coord(p.x, c.tvs, c.tdims[0]);
+    const int cy = olc_bin_coord(p.y, c.tvs, c.tdims[1]);
+    const int cz = olc_bin_coord(p.z, c.tvs, c.tdims[2]);
+    for (int dz = -1; dz <= 1; ++dz) {
+        const int nz = cz + dz;
+        if (nz < 0 || nz >= c.tdims[2]) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int ny = cy + dy;
+            if (ny < 0 || ny >= c.tdims[1]) continue;
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int nx = cx + dx;
+                if (nx < 0 || nx >= c.tdims[0]) continue;
+                const uint2 rg = __ldg(ranges + olc_tissue_key(nx, ny, nz));
+                for (olc_u32 j = rg.x; j < rg.y; ++j) contact_pair(p, __ldg(posr + j), i, j, c, fx, fy, fz);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(CB_THREADS) k_contact_brick(const float4* __restrict__ posr,
+                                                             const uint2* __restrict__ ranges, olc_u32 n_bricks,
+                                                             olc_u32 n_table, ContactDev c, float* __restrict__ xo,
+                                                             float* __restrict__ yo, float* __restrict__ zo) {
+    __shared__ float4 s_rec[CB_CAP];
+    __shared__ olc_u32 s_off[65];  // first staged record of halo bin b (x fastest), s_off[64] = total
+    __shared__ olc_u32 s_row[64];  // first row of halo bin b
+    __shared__ olc_u32 s_warp[2];
+    __shared__ olc_u32 s_home[2];  // the brick's rows [begin, end)
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const float md = __fmul_rn(c.mobility, c.dt);
+    for (olc_u32 B = blockIdx.x; B < n_bricks; B += gridDim.x) {
+        if (t == 0) {
+            olc_u32 begin = 0xffffffffu, end = 0u;
+            for (olc_u32 q = 0; q < 8u; ++q) {
+                const olc_u32 k = 8u * B + q;
+                if (k >= n_table) break;
+                const uint2 r = __ldg(ranges + k);
+                if (r.y > r.x) {
+                    begin = min(begin, r.x);
+                    end = max(end, r.y);
+                }
+            }
+            s_home[0] = begin;
+            s_home[1] = end;
+        }
+        __syncthreads();
+        const olc_u32 h0 = s_home[0], h1 = s_home[1];
+        if (h0 >= h1) {
+            __syncthreads();
+            continue;
+        }
+        // the 4 x 4 x 4 halo: bin t at brick-local (t & 3, (t >> 2) & 3, t >> 4) - 1
+        const int ox = 2 * (int)olc_compact9(B) - 1, oy = 2 * (int)olc_compact9(B >> 1) - 1,
+                  oz = 2 * (int)olc_compact9(B >> 2) - 1;
+        const int gx = ox + (t & 3), gy = oy + ((t >> 2) & 3), gz = oz + (t >> 4);
+        uint2 rg = make_uint2(0u, 0u);
+        if (gx >= 0 && gy >= 0 && gz >= 0 && gx < c.tdims[0] && gy < c.tdims[1] && gz < c.tdims[2])
+            rg = __ldg(ranges + olc_tissue_key(gx, gy, gz));
+        const olc_u32 cnt = rg.y - rg.x;
+        olc_u32 incl = cnt;  // inclusive scan over the 64 bins
+        for (int o = 1; o < 32; o <<= 1) {
+            const olc_u32 v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        if (warp == 1) incl += s_warp[0];
+        s_off[t] = incl - cnt;
+        s_row[t] = rg.x;
+        if (t == CB_THREADS - 1) s_off[64] = incl;
+        __syncthreads();
+        const bool staged = s_off[64] <= (olc_u32)CB_CAP;
+        if (staged)
+            for (olc_u32 k = 0; k < cnt; ++k) s_rec[s_off[t] + k] = __ldg(posr + rg.x + k);
+        __syncthreads();
+        for (olc_u32 i = h0 + t; i < h1; i += CB_THREADS) {
+            const float4 p = posr[i];
+            if (p.w < 0.0f) continue;  // dead this step: no move, no force
+            const int lx = olc_bin_coord(p.x, c.tvs, c.tdims[0]) - ox;
+            const int ly = olc_bin_coord(p.y, c.tvs, c.tdims[1]) - oy;
+            const int lz = olc_bin_coord(p.z, c.tvs, c.tdims[2]) - oz;
+            float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+            if (staged && lx >= 1 && lx <= 2 && ly >= 1 && ly <= 2 && lz >= 1 && lz <= 2) {
+                for (int dz = -1; dz <= 1; ++dz)
+                    for (int dy = -1; dy <= 1; ++dy)
+                        for (int dx = -1; dx <= 1; ++dx) {
+                            // bins outside the grid are empty here, as the reference skips them
+                            const int b = ((lz + dz) << 4) | ((ly + dy) << 2) | (lx + dx);
+                            const olc_u32 k0 = s_off[b], k1 = s_off[b + 1], row0 = s_row[b];
+                            for (olc_u32 k = k0; k < k1; ++k) contact_pair(p, s_rec[k], i, row0 + (k - k0), c, fx, fy, fz);
+                        }
+            } else {
+                contact_walk_global(posr, ranges, p, i, c, fx, fy, fz);
+            }
+            float mx = __fmul_rn(fx, md), my = __fmul_rn(fy, md), mz = __fmul_rn(fz, md);
+            const float len = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz)));
+            if (len > c.max_disp) {
+                const float sc = __fdiv_rn(c.max_disp, len);
+                mx = __fmul_rn(mx, sc);
+                my = __fmul_rn(my, sc);
+                mz = __fmul_rn(mz, sc);
+            }
+            xo[i] = fminf(fmaxf(__fadd_rn(p.x, mx), c.lo[0]), c.hi[0]);
+            yo[i] = fminf(fmaxf(__fadd_rn(p.y, my), c.lo[1]), c.hi[1]);
+            zo[i] = fminf(fmaxf(__fadd_rn(p.z, mz), c.lo[2]), c.hi[2]);
+        }
+        __syncthreads();  // the next brick reuses the shared arrays
+    }
+}
+
 // The two walks (olc.h OLC_CONTACT_*): bit-identical, chosen per handle by
 // measurement (OlcTuning.contact_variant).  On the 1 M-agent scale workload
 // the flat walk took 0.92 ms per step over 200 steps against 1.04 for the
 // nested loops; sparser or denser populations can order them the other way.
 void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
-                    olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s, int variant) {
+                    olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s, int variant,
+                    olc_u32 n_table) {
+    if (variant == OLC_CONTACT_BRICK && n_table > 0) {
+        // rows come from the bin table, so the live count is not needed here
+        const olc_u32 n_bricks = (n_table + 7u) / 8u;
+        olc_u32 blocks = n_bricks < 148u * 16u ? n_bricks : 148u * 16u;
+        if (blocks == 0) blocks = 1;
+        k_contact_brick<<<blocks, CB_THREADS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_bricks,
+                                                      n_table, c, x, y, z);
+        return;
+    }
     if (variant != OLC_CONTACT_NESTED) {
         olc_u32 blocks = (n_cap + CF_THREADS - 1) / CF_THREADS;
         if (blocks == 0) blocks = 1;

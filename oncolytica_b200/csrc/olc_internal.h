@@ -175,7 +175,7 @@ struct ContactDev {
 };
 void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
                     olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s,
-                    int variant = OLC_CONTACT_FLAT);
+                    int variant = OLC_CONTACT_FLAT, olc_u32 n_table = 0);
 // The rest of the engine's force law (OlcMechanics): necrotic repulsion
 // factor, adhesion, damped velocity integration.
 struct MechDev {

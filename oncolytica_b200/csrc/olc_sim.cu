@@ -465,7 +465,7 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
     } else if (s->contact.enabled) {
         launch_contact(s->posr, s->ranges, s->counters + OLC_CTR_N, 0, cap, s->contact_dev,
                        static_cast<float*>(s->col[cc][0]), static_cast<float*>(s->col[cc][1]),
-                       static_cast<float*>(s->col[cc][2]), st, s->tuning.contact_variant);
+                       static_cast<float*>(s->col[cc][2]), st, s->tuning.contact_variant, s->n_table);
         ++launches;
     }
     mark(s, 5, st);
@@ -2569,8 +2569,9 @@ int olc_set_tuning(OlcSim* s, const OlcTuning* t) {
         return fail(s, OLC_ERR_ARG, "olc_set_tuning: stencil tile (" + std::to_string(t->stencil_tile_y) + ", " +
                                         std::to_string(t->stencil_tile_z) +
                                         ") is not one of (8,8), (16,8), (8,16), (16,4)");
-    if (t->contact_variant != OLC_CONTACT_FLAT && t->contact_variant != OLC_CONTACT_NESTED)
-        return fail(s, OLC_ERR_ARG, "olc_set_tuning: contact_variant must be OLC_CONTACT_FLAT or OLC_CONTACT_NESTED");
+    if (t->contact_variant != OLC_CONTACT_FLAT && t->contact_variant != OLC_CONTACT_NESTED &&
+        t->contact_variant != OLC_CONTACT_BRICK)
+        return fail(s, OLC_ERR_ARG, "olc_set_tuning: contact_variant must be an OLC_CONTACT_* value");
     if (t->batch_tile_depth != 8 && t->batch_tile_depth != 16 && t->batch_tile_depth != 32)
         return fail(s, OLC_ERR_ARG, "olc_set_tuning: batch_tile_depth must be 8, 16 or 32");
     OLC_TRY(check(s, cudaDeviceSynchronize(), "sync"));

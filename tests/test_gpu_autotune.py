@@ -17,9 +17,12 @@ from oncolytica_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 
-def _spec():
-    return W.scaled(W.SCALE, n_agents=30_000, domain=320.0, ball_radius=90.0, field_dims=(64, 64, 64),
-                    capacity=150_000, seed=4, uptake=2.0, death_k=0.2, init_drug=0.1, v_lo=1.85, v_hi=2.0)
+def _spec(dense: bool = False):
+    # dense: ~100 agents per 10 um bin, so brick halos overflow the staging
+    # buffer and the brick walk falls back to global memory
+    return W.scaled(W.SCALE, n_agents=30_000, domain=320.0, ball_radius=40.0 if dense else 90.0,
+                    field_dims=(64, 64, 64), capacity=150_000, seed=4, uptake=2.0, death_k=0.2, init_drug=0.1,
+                    v_lo=1.85, v_hi=2.0)
 
 
 def _same(a: dict, b: dict, what: str) -> None:
@@ -43,6 +46,18 @@ def test_every_choice_gives_the_same_bits(cuda, tile, contact):
     assert eng._backend_impl.get_tuning()["stencil_tile"] == tuple(tile)
     eng.run_steps(3)
     _same(eng._backend_impl.snapshot(), ref._backend_impl.snapshot(), f"tile {tile} contact {contact}")
+
+
+@pytest.mark.parametrize("contact", autotune.CONTACT_VARIANTS)
+def test_contact_variants_agree_on_a_dense_population(cuda, contact):
+    spec = _spec(dense=True)
+    state = W.initial_state(spec)
+    ref = W.build_engine(spec, state)
+    ref.run_steps(2)
+    eng = W.build_engine(spec, state)
+    eng._backend_impl.set_tuning(contact_variant=contact)
+    eng.run_steps(2)
+    _same(eng._backend_impl.snapshot(), ref._backend_impl.snapshot(), f"dense, contact {contact}")
 
 
 def test_tuning_restores_the_run_and_caches(cuda, tmp_path, monkeypatch):
