@@ -86,7 +86,8 @@ class BatchEngine:
         contact = e0._contact
         radius_field = contact.radius if (contact and isinstance(contact.radius, str)) else None
         self.layout = L = make_layout(s0._spec, radius_field, batched=True)
-        self.program = translate_model(s0, L, radius_field) if (e0._cell_rules or e0._metric_rules) else None
+        self.program = (translate_model(s0, L, radius_field)
+                        if (e0._cell_rules or e0._metric_rules or e0._chemistry_rules or e0._tissue_rules) else None)
         n = len(self.engines)
         geoms = (_lib.OlcGeom * n)(*[self._geom(e) for e in self.engines])
         caps = _lib.OlcCaps()
@@ -175,6 +176,9 @@ class BatchEngine:
             kinds = (C.c_int * len(self.program.kernels))(*[kind for _, kind in self.program.kernels])
             self._check(self.lib.olc_set_rule_source(self.handle, self.program.source.encode(), names, kinds,
                                                      len(self.program.kernels), _lib.CSRC_DIR.encode()))
+            if any(kind == 3 for _, kind in self.program.kernels):
+                its = (C.c_int * len(self.program.kernels))(*self.program.iterations)
+                self._check(self.lib.olc_set_rule_iterations(self.handle, its, len(self.program.kernels)))
         self.metrics_words = max(1, len(L.metrics))
         self._check(self.lib.olc_set_user_metrics_size(self.handle, 4 * self.metrics_words))
         self.upload_params()

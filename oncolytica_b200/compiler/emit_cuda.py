@@ -556,6 +556,9 @@ class Translator:
         lines.append("__device__ __forceinline__ Tissue_t olc_tissue_at(const OlcP& P, olc_vec3 p) {\n"
                      "    const olc_ivec3 t = olc_tissue_coord(P, p);\n"
                      "    return olc_tissue_voxel(P, t.x, t.y, t.z);\n}")
+        chem_writes = "\n".join(f"    olc_field_out(P, {i}, v, c.{n});" for i, n in enumerate(L.chem_fields))
+        lines.append("__device__ __forceinline__ void olc_store_chem(const OlcP& P, olc_u32 v, "
+                     "const Chem_t& c) {\n" + chem_writes + "\n}")
         if not L.batched:
             # voxel-rule stores: the other buffer of the tissue grid / of every field
             tis_writes = []
@@ -571,9 +574,6 @@ class Translator:
                     tis_writes.append(f"    olc_tissue_col_out<int>(P, {i}, k, c.{n});")
             lines.append("__device__ __forceinline__ void olc_store_tissue(const OlcP& P, olc_u32 k, "
                          "const Tissue_t& c) {\n" + "\n".join(tis_writes) + "\n}")
-            chem_writes = "\n".join(f"    olc_field_out(P, {i}, v, c.{n});" for i, n in enumerate(L.chem_fields))
-            lines.append("__device__ __forceinline__ void olc_store_chem(const OlcP& P, olc_u32 v, "
-                         "const Chem_t& c) {\n" + chem_writes + "\n}")
         lines.append("__device__ __forceinline__ olc_vec3 olc_rand_dir3(olc_u32& s) {\n"
                      "    float3 d = olc_rand_dir(s);\n    return olc_v3(d.x, d.y, d.z);\n}")
         lines.append("__device__ __forceinline__ void olc_divide(OlcCtx& ctx, olc_u32 rng, const Cell_t& child) {\n"
@@ -677,7 +677,9 @@ class Translator:
         load the voxel from the current buffer, run the rule, store it to the
         other buffer (the host flips the buffers after the launch)."""
         if self.L.batched:
-            raise CompilationError("tissue/chemistry rules are not compiled in batched mode")
+            if kind == "Tissue":
+                raise CompilationError("tissue rules are not compiled in batched mode (members have no tissue grids)")
+            return self.batched_chem_kernel(kname, fn)
         dims = "P.tdims" if kind == "Tissue" else "P.cdims"
         load = "olc_tissue_voxel(P, x, y, z)" if kind == "Tissue" else "olc_chem_voxel(P, x, y, z)"
         store = "olc_store_tissue(P, olc_tissue_key(x, y, z), v)" if kind == "Tissue" else "olc_store_chem(P, w, v)"
@@ -695,6 +697,37 @@ class Translator:
         ctx.multi = false;
         {fn}(P, rng, ctx, v);
         {store};
+    }}
+}}"""
+
+    def batched_chem_kernel(self, kname: str, fn: str) -> str:
+        """A chemistry rule over every member of a batch: one CTA per field
+        tile of the batch's tile list (P.vtiles: member, tile coordinates), one
+        thread per voxel of the tile, each member seen through its own view
+        (grid, fields, bin table); stores go to the member's other buffer and
+        the host flips every member's parity after the launch."""
+        return f"""extern "C" __global__ void __launch_bounds__(OLC_RULE_THREADS) {kname}(OlcRuleParams P) {{
+    const int tx = P.vtile[0], ty = P.vtile[1], tz = P.vtile[2];
+    const olc_u32 per = (olc_u32)(tx * ty * tz);
+    for (olc_u32 ti = blockIdx.x; ti < P.n_vtiles; ti += gridDim.x) {{
+        const uint4 t = P.vtiles[ti];
+        const OlcSimView V = olc_sim_view(P, t.x);
+        for (olc_u32 e = threadIdx.x; e < per; e += blockDim.x) {{
+            const int x = (int)t.y * tx + (int)(e % (olc_u32)tx);
+            const int y = (int)t.z * ty + (int)((e / (olc_u32)tx) % (olc_u32)ty);
+            const int z = (int)t.w * tz + (int)(e / (olc_u32)(tx * ty));
+            if (x >= V.cdims[0] || y >= V.cdims[1] || z >= V.cdims[2]) continue;
+            const olc_u32 w = ((olc_u32)z * (olc_u32)V.cdims[1] + (olc_u32)y) * (olc_u32)V.cdims[0] + (olc_u32)x;
+            Chem_t v = olc_chem_voxel(V, x, y, z);
+            olc_u32 rng = 0u;  // voxels have no RNG state
+            OlcCtx ctx;
+            ctx.i = 0xffffffffu;
+            ctx.dead = false;
+            ctx.born = false;
+            ctx.multi = false;
+            {fn}(V, rng, ctx, v);
+            olc_store_chem(V, w, v);
+        }}
     }}
 }}"""
 
@@ -1151,6 +1184,8 @@ class FuncEmitter:
             raise self.err(f"loop variable {nb!r} shadows a variable", n.target)
         if attr == "tissues" and kind != "Chemistry":
             raise self.err(".tissues is a chemistry voxel's loop", n.iter)
+        if attr == "tissues" and self.tr.L.batched:
+            raise self.err(".tissues needs a tissue grid, which batch members do not have", n.iter)
         if attr in ("cells", "tissues") and kind == "Chemistry":
             self.tied_geometry(n.iter)
         lab = self.fresh("_vx_done")

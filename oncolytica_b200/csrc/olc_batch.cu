@@ -328,6 +328,19 @@ void launch_flip_parity(const FieldStep* steps, int field, int n_fields, olc_u32
     k_flip_parity<<<(n_sims + 255) / 256, 256, 0, s>>>(steps, field, n_fields, n_sims, fpar);
 }
 
+// After a chemistry rule: every member holds every field in its other buffer.
+__global__ void k_flip_parity_all(int n_fields, olc_u32 n_sims, unsigned char* fpar) {
+    const size_t total = (size_t)n_sims * n_fields;
+    for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < total; j += (size_t)gridDim.x * blockDim.x)
+        fpar[j] ^= (unsigned char)1;
+}
+
+void launch_flip_parity_all(int n_fields, olc_u32 n_sims, unsigned char* fpar, cudaStream_t s) {
+    const size_t total = (size_t)n_sims * n_fields;
+    if (total == 0) return;
+    k_flip_parity_all<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(n_fields, n_sims, fpar);
+}
+
 // ------------------------------------------------------------------ 16-bit fields
 // The reaction pass and the reductions on BF16 / FP16 storage
 // (olc_field16.cu's arithmetic).

@@ -306,6 +306,7 @@ void launch_substep_batch_t16(const BatchArgs& b, int storage, int encoding, con
                               olc_u32* status, cudaStream_t s);
 void launch_sink_batch(const BatchArgs& b, const uint4* tiles, olc_u32 n_tiles, const FieldStep* steps, int field,
                        int n_fields, const unsigned char* fpar, float* fa, float* fb, float* sink, cudaStream_t s);
+void launch_flip_parity_all(int n_fields, olc_u32 n_sims, unsigned char* fpar, cudaStream_t s);
 void launch_flip_parity(const FieldStep* steps, int field, int n_fields, olc_u32 n_sims, unsigned char* fpar,
                         cudaStream_t s);
 void launch_reduce_agents_batch(const BatchArgs& b, const ReduceArgs& a, const olc_u32* sim, const olc_u32* counters,

@@ -97,6 +97,11 @@ struct OlcRuleParams {
     // neighbours' previous values)
     unsigned char* tissue_out;
     void* field_out[OLC_MAX_FIELD_COLS];
+    // batched chemistry rules: the members' field tiles (member, tile x, y, z
+    // of vtile[0] x vtile[1] x vtile[2] voxels) a voxel kernel walks
+    const uint4* vtiles;
+    olc_u32 n_vtiles;
+    int vtile[3];
 };
 
 // What a rule body sees of one simulation of a batch (batched mode).  Member
@@ -107,6 +112,7 @@ struct OlcSimView {
     const void* field[OLC_MAX_FIELD_COLS];
     int field_type[OLC_MAX_FIELD_COLS];
     float field_bval[OLC_MAX_FIELD_COLS];
+    void* field_out[OLC_MAX_FIELD_COLS];  // the member's other buffer (chemistry rules write it)
     float* sink[OLC_MAX_FIELD_COLS];
     const olc_u32* ranges;
     float4* posr;
@@ -133,6 +139,8 @@ __device__ __forceinline__ OlcSimView olc_sim_view(const OlcRuleParams& P, olc_u
         V.field_type[f] = P.field_type[f];
         V.field_bval[f] = P.field_bval[f];
         V.field[f] = base ? base + d.field_off * (P.field_type[f] ? 2u : 4u) : nullptr;
+        unsigned char* other = static_cast<unsigned char*>(const_cast<void*>(alt ? P.field[f] : P.field_alt[f]));
+        V.field_out[f] = other ? other + d.field_off * (P.field_type[f] ? 2u : 4u) : nullptr;
         V.sink[f] = P.sink[f] ? P.sink[f] + d.field_off : nullptr;
     }
     V.ranges = P.ranges + 2ull * d.ranges_base;
@@ -354,7 +362,8 @@ __device__ __forceinline__ void olc_tissue_col_out(const OlcRuleParams& P, int c
 __device__ __forceinline__ float olc_field_in(const OlcRuleParams& P, int f, olc_u32 v) {
     return static_cast<const float*>(P.field[f])[v];
 }
-__device__ __forceinline__ void olc_field_out(const OlcRuleParams& P, int f, olc_u32 v, float x) {
+template <class PT>
+__device__ __forceinline__ void olc_field_out(const PT& P, int f, olc_u32 v, float x) {
     static_cast<float*>(P.field_out[f])[v] = x;
 }
 

@@ -272,6 +272,11 @@ OlcRuleParams make_rule_params(OlcSim* s, int rule_index, int in_buf) {
         P.fpar = s->fpar_dev;
         P.n_fields = (int)s->caps.n_fields;
         P.sim_col = (int)s->caps.n_agent_fields - 1;
+        P.vtiles = s->btiles_all;
+        P.n_vtiles = (olc_u32)s->n_btiles;
+        P.vtile[0] = BATCH_TILE_X;
+        P.vtile[1] = BATCH_TILE_Y;
+        P.vtile[2] = BATCH_TILE_Z;
         P.tissue = nullptr;
         P.n_tissue_cols = 0;
     }
@@ -606,6 +611,20 @@ int step_once_batch(OlcSim* s, int collect, cudaStream_t st) {
     launch_permute(s->vals, s->counters, cap, pa, st);
     s->agent_cur = 1 - ac;
     launches += 4 + (uint64_t)passes;
+    // 3a. chemistry rules over every member (a CTA per field tile), each
+    // iteration writing the members' other buffers, whose parity then flips
+    for (size_t k = 0; k < s->funcs.size(); ++k) {
+        if (s->kinds[k] != 3) continue;
+        for (olc_u32 f = 0; f < F; ++f)
+            if (!s->field_bound[f] || s->fstep[f].storage != OLC_FIELD_F32)
+                return fail(s, OLC_ERR_STATE, "chemistry rule: every chemistry field must be bound with FP32 storage");
+        for (int it = 0; it < s->iters[k]; ++it) {
+            const OlcRuleParams P = make_rule_params(s, 0, s->agent_cur);
+            OLC_TRY(launch_rule(s, (int)k, P, st, (olc_u32)s->n_btiles * (BATCH_TILE_X * BATCH_TILE_Y * BATCH_TILE_Z)));
+            launch_flip_parity_all((int)F, s->n_sims, s->fpar_dev, st);
+            launches += 2;
+        }
+    }
     mark(s, 3, st);
     // 3. cell rules
     if (s->n_cell_rules > 0) {
@@ -1420,8 +1439,8 @@ int olc_set_rule_source(OlcSim* s, const char* src, const char* const* kernels, 
     int ncell = 0;
     for (int i = 0; i < n; ++i) {
         if (kinds[i] < 0 || kinds[i] > 3) return fail(s, OLC_ERR_ARG, "olc_set_rule_source: kind must be 0..3");
-        if (kinds[i] >= 2 && s->n_sims)
-            return fail(s, OLC_ERR_STATE, "olc_set_rule_source: tissue/chemistry rules need a solo handle");
+        if (kinds[i] == 2 && s->n_sims)
+            return fail(s, OLC_ERR_STATE, "olc_set_rule_source: tissue rules need a solo handle");
         ncell += kinds[i] == 0;
     }
     OLC_TRY(ensure_context(s));

@@ -462,7 +462,8 @@ class PoolDevice:
         self.contact = contact
         radius_field = contact.radius if (contact and isinstance(contact.radius, str)) else None
         self.layout = L = make_layout(sim._spec, radius_field, batched=True)
-        self.program = translate_model(sim, L, radius_field) if (eng._cell_rules or eng._metric_rules) else None
+        self.program = (translate_model(sim, L, radius_field)
+                        if (eng._cell_rules or eng._metric_rules or eng._chemistry_rules or eng._tissue_rules) else None)
         self.sinks = self.program.sink_fields if self.program else set()
         self.storage, self.encoding, self.bval = {}, {}, {}
         for name in L.chem_fields:
@@ -529,6 +530,9 @@ class PoolDevice:
             kinds = (C.c_int * len(self.program.kernels))(*[kind for _, kind in self.program.kernels])
             self._check(self.lib.olc_set_rule_source(self.handle, self.program.source.encode(), names, kinds,
                                                      len(self.program.kernels), _lib.CSRC_DIR.encode()))
+            if any(kind == 3 for _, kind in self.program.kernels):
+                its = (C.c_int * len(self.program.kernels))(*self.program.iterations)
+                self._check(self.lib.olc_set_rule_iterations(self.handle, its, len(self.program.kernels)))
         self.metrics_words = max(1, len(L.metrics))
         self._check(self.lib.olc_set_user_metrics_size(self.handle, 4 * self.metrics_words))
         self.sim_col = len(L.cell_cols) - 1

@@ -96,3 +96,46 @@ def test_batch_sync_to_host_splits_members(cuda):
             np.testing.assert_array_equal(a[col], b[col], err_msg=f"{col} member {k}")
         for f in ("o2", "drug"):
             np.testing.assert_array_equal(e.chemistry.column(f), batch.engines[k].chemistry.column(f))
+
+
+def _chem_engine(shape, seed, n):
+    import chem_model as CM
+    import oncolytica_b200 as ol
+
+    rng = np.random.default_rng(seed)
+    eng = ol.Engine(backend="cuda", max_agents=8 * n)
+    eng.setup_geometry(tissue_shape=shape, tissue_voxel_size=4.0)
+    eng.setup_chemistry(CM.CChem)
+    eng.chemistry.column("signal")[...] = rng.uniform(0.0, 0.5, size=eng.chemistry_shape).astype(np.float32)
+    hi = np.array(shape, np.float32) * 4.0
+    eng.cells.add_arrays(CM.CCell, pos=(rng.uniform(0.1, 0.9, size=(n, 3)) * hi).astype(np.float32),
+                         kind=rng.integers(0, 2, n), energy=rng.uniform(0.3, 0.9, n).astype(np.float32))
+    return eng, CM.ChemSim()
+
+
+@pytest.mark.parametrize("graphs", [False, True])
+def test_batched_chemistry_rules_match_solo_runs(cuda, graphs):
+    """Chemistry rules in a batch: members of three grid sizes (chemistry
+    8^3, 12^3 and 16x16x8) each give their solo run's agents and field bits."""
+    from oncolytica_b200.batch import BatchEngine
+
+    cases = [((16, 16, 16), 1, 300), ((24, 24, 24), 2, 700), ((32, 32, 16), 3, 500)]
+    solos = []
+    for shape, seed, n in cases:
+        e, sim = _chem_engine(shape, seed, n)
+        e.load_model(sim)
+        e.set_graphs(graphs)
+        e.run_steps(4)
+        solos.append(e._backend_impl.snapshot())
+    pairs = [_chem_engine(shape, seed, n) for shape, seed, n in cases]
+    b = BatchEngine([e for e, _ in pairs], [s for _, s in pairs])
+    b.set_graphs(graphs)
+    b.run_steps(4)
+    for k, ref in enumerate(solos):
+        got = b.snapshot(k)
+        assert got["rows"] == ref["rows"], k
+        np.testing.assert_array_equal(got["life"], ref["life"])
+        for c in ref["cols"]:
+            np.testing.assert_array_equal(got["cols"][c], ref["cols"][c], err_msg=f"member {k} {c}")
+        np.testing.assert_array_equal(got["fields"]["signal"], ref["fields"]["signal"], err_msg=f"member {k}")
+    assert any(s["rows"] != n for s, (_, _, n) in zip(solos, cases)), "births or deaths should happen"

@@ -211,7 +211,7 @@ def test_batched_translation_compiles():
 
 # ---- tissue and chemistry rules ---------------------------------------------
 
-def _translate_all(sim_cls, tissue_shape=(12, 12, 12), vs=10.0, chem_shape=None, chem_vs=None):
+def _translate_all(sim_cls, tissue_shape=(12, 12, 12), vs=10.0, chem_shape=None, chem_vs=None, batched=False):
     sim = sim_cls()
     rules = {"cell": [], "metric": [], "tissue": [], "chemistry": []}
     for name in dir(sim):
@@ -224,7 +224,22 @@ def _translate_all(sim_cls, tissue_shape=(12, 12, 12), vs=10.0, chem_shape=None,
                                   tissue_shape=tissue_shape, tissue_voxel_size=vs,
                                   chemistry_shape=chem_shape or tuple(t // 2 for t in tissue_shape),
                                   chemistry_voxel_size=chem_vs or 2.0 * vs)
-    return translate_model(sim, make_layout(sim._spec, None), None)
+    return translate_model(sim, make_layout(sim._spec, None, batched=batched), None)
+
+
+def test_batched_chemistry_rules_compile():
+    """Chemistry rules in batched mode: one kernel over the batch's field
+    tiles, each member through its own view; tissue rules and .tissues loops
+    are refused there (members have no tissue grids)."""
+    import chem_model as CM
+    import voxel_model as VM
+
+    prog = _translate_all(CM.ChemSim, batched=True)
+    assert dict(prog.kernels)["Kernel_ChemRule_0"] == 3
+    assert "olc_sim_view(P, t.x)" in prog.source and "P.vtiles" in prog.source
+    _nvrtc_ok(prog)
+    with pytest.raises(ol.CompilationError, match="tissue"):
+        _translate_all(VM.VoxelSim, batched=True)
 
 
 def test_voxel_rules_compile():
