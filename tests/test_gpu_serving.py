@@ -144,3 +144,49 @@ def test_mismatched_requests_are_rejected(cuda):
     assert pool.results[1].status == "rejected" and "storage" in pool.results[1].error
     _check_same(specs[0], pool.results[2], _solo(specs[0], 2))
     dev.close()
+
+
+def test_served_chemistry_rules_match_solo_runs(cuda):
+    """A model with a chemistry rule (chem_model: neighbour Laplacian, .cells
+    secretion, three iterations) through the pool: three requests of two grid
+    sizes, one joining two steps late, each return their solo run's agents
+    and field."""
+    import chem_model as CM
+
+    import oncolytica_b200 as ol
+    from oncolytica_b200._geometry import voxel_table_size
+
+    def engine(shape, seed, n):
+        rng = np.random.default_rng(seed)
+        e = ol.Engine(backend="cuda", max_agents=8 * n)
+        e.setup_geometry(tissue_shape=shape, tissue_voxel_size=4.0)
+        e.setup_chemistry(CM.CChem)
+        e.chemistry.column("signal")[...] = rng.uniform(0.0, 0.5, size=e.chemistry_shape).astype(np.float32)
+        hi = np.array(shape, np.float32) * 4.0
+        e.cells.add_arrays(CM.CCell, pos=(rng.uniform(0.1, 0.9, size=(n, 3)) * hi).astype(np.float32),
+                           kind=rng.integers(0, 2, n), energy=rng.uniform(0.3, 0.9, n).astype(np.float32))
+        return e
+
+    cases = [((16, 16, 16), 5, 300, 5), ((24, 24, 24), 6, 600, 4), ((16, 16, 16), 7, 200, 3)]
+    dev = PoolDevice((engine(*cases[0][:3]), CM.ChemSim()), max_slots=3, max_rows=sum(8 * c[2] for c in cases),
+                     table_entries=sum(voxel_table_size(c[0]) for c in cases),
+                     field_voxels=sum(int(np.prod([d // 2 for d in c[0]])) + 64 for c in cases),
+                     max_tissue_dims=(24, 24, 24))
+    pool = ServingPool(dev, depth=1)
+    ids = [pool.submit(SimRequest(engine(*c[:3]), CM.ChemSim(), c[3], return_state=True)) for c in cases[:2]]
+    pool.step()
+    pool.step()
+    ids.append(pool.submit(SimRequest(engine(*cases[2][:3]), CM.ChemSim(), cases[2][3], return_state=True)))
+    pool.drain()
+    for rid, (shape, seed, n, steps) in zip(ids, cases):
+        res = pool.results[rid]
+        assert res.status == "done", res.error
+        e = engine(shape, seed, n)
+        e.load_model(CM.ChemSim())
+        e.run_steps(steps)
+        snap = e._backend_impl.snapshot()
+        live = snap["life"] == 0
+        for col, a in snap["cols"].items():
+            np.testing.assert_array_equal(res.agents[col], a[live], err_msg=f"request {rid} {col}")
+        np.testing.assert_array_equal(res.fields["signal"].ravel(order="F"), snap["fields"]["signal"])
+    dev.close()
