@@ -204,7 +204,9 @@ class Engine:
         stay near their boundary value, like O2); "offset3" (the value minus
         the nearest of 0, b/2 and b, for fields spread over [0, b], like a
         decaying drug); "auto" picks by storage, decay and the initial values
-        (_fieldcodec.resolve).  Encoded fields stay within [0, boundary]."""
+        (_fieldcodec.resolve).  Encoded fields are clamped to [0, boundary]
+        (FP32 and value-encoded fields at 0 only), so a BF16 field whose
+        values may exceed its boundary value needs ``encoding="value"``."""
         from oncolytica_b200._fieldcodec import ENCODINGS
 
         if storage not in STORAGE_CODES:
