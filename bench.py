@@ -586,6 +586,10 @@ def measure_field_error(spec, storages: tuple, steps: int, checkpoints: tuple = 
     o2_0, drug_0 = W.initial_fields(spec)
     shp = tuple(spec.field_dims[::-1])
     engines = {st: W.build_engine(replace(spec, storage=st), state0) for st in storages}
+    for eng in engines.values():
+        # children dropped at capacity change the agents' trajectory, not the
+        # comparison: each run's own sinks are replayed into its FP64 field
+        eng.on_device_status = "warn"
     ref = {st: np.ascontiguousarray(o2_0, dtype=np.float64) for st in storages}
     tmp = np.zeros(shp, np.float64)
     drug = np.ascontiguousarray(drug_0, dtype=np.float64) if spec.has_drug else None
@@ -632,6 +636,8 @@ def measure_field_error(spec, storages: tuple, steps: int, checkpoints: tuple = 
     errors(steps)
     out["final"] = out["by_step"][str(steps)]
     out["status"] = {st: eng._backend_impl.counters()["status"] for st, eng in engines.items()}
+    out["agents_end"] = {st: eng._backend_impl.counters()["n_agents"] for st, eng in engines.items()}
+    out["max_agents"] = spec.capacity
     out["fp64_host_seconds"] = t_cpu
     for eng in engines.values():
         eng.close()
@@ -647,7 +653,10 @@ def run_precision_workload(args) -> None:
     torch.cuda.set_device(local)
     from oncolytica_b200 import workloads as W
 
-    spec = replace(W.CONFIGS[args.workload_base], seed=W.CONFIGS[args.workload_base].seed + rank)
+    base = W.CONFIGS[args.workload_base]
+    # room for the population of a long run (unchecked growth doubles it about
+    # every 140 steps until O2 runs short)
+    spec = replace(base, seed=base.seed + rank, capacity=32 * base.n_agents)
     storages = tuple(s for s in args.storages.split(",") if s)
     cps = tuple(sorted({max(1, args.steps * k // 4) for k in (1, 2, 3)}))
     r = measure_field_error(spec, storages, args.steps, checkpoints=cps)
