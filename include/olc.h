@@ -157,10 +157,16 @@ typedef struct {
     int32_t contact_variant;  /* OLC_CONTACT_FLAT, OLC_CONTACT_NESTED or OLC_CONTACT_BRICK */
     int32_t batch_tile_depth; /* planes per tile of the batched FP32 substep: 8, 16 or
                                  32 (members without their own, olc_set_batch_tile_depths) */
+    int32_t stencil_pair_threads; /* two FP32 substeps per pass (temporal blocking) with
+                                     CTAs of 128, 256, 512 or 1024 threads where the field's
+                                     rows fit one TMA box (x extent <= 256); 0 = one
+                                     substep per pass */
+    int32_t stencil_pair_planes;  /* planes per CTA of the two-substep pass; 0 = as few
+                                     as keep the whole grid resident in one wave */
 } OlcTuning;
 
 /* Sets / reads a handle's kernel shapes and variants (OlcTuning; defaults
- * (8, 8), OLC_CONTACT_FLAT, 16).  Every choice gives the same bits.  Rebuilds
+ * (8, 8), OLC_CONTACT_FLAT, 16, 0, 0).  Every choice gives the same bits.  Rebuilds
  * what depends on them (tensor maps, tile lists) and drops captured graphs;
  * waits for the device. */
 int olc_set_tuning(OlcSim* sim, const OlcTuning* tuning);
@@ -641,6 +647,12 @@ int olc_stage_bin_ranges(const uint32_t* sorted_keys_dev, uint32_t n, uint32_t n
  * after use). */
 int olc_stage_diffuse(float* f_dev, float* tmp_dev, float* sink_dev, const int32_t dims[3],
                       float dx, float dt, const OlcDiffusion* spec, void* stream);
+
+/* olc_stage_diffuse with the stencil choices of an OlcTuning (tile, and two
+ * substeps per pass); every choice gives the same result.  NULL = defaults. */
+int olc_stage_diffuse_tuned(float* f_dev, float* tmp_dev, float* sink_dev, const int32_t dims[3],
+                            float dx, float dt, const OlcDiffusion* spec, const OlcTuning* tuning,
+                            void* stream);
 
 /* olc_stage_diffuse with pinned voxels (olc_set_pinned's rule). */
 int olc_stage_diffuse_pinned(float* f_dev, float* tmp_dev, float* sink_dev, const int32_t dims[3], float dx,

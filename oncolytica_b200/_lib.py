@@ -55,6 +55,7 @@ EXPORTS = (
     "olc_stage_contact_mech", "olc_stage_contact_motion", "olc_bind_tissue_pair", "olc_current_tissue", "olc_set_rule_iterations",
     "olc_set_pinned", "olc_stage_diffuse_pinned", "olc_sort_noalloc_status", "olc_sort_status_offset",
     "olc_selftest_bounded_waits", "olc_set_tuning", "olc_get_tuning", "olc_set_batch_tile_depths",
+    "olc_stage_diffuse_tuned",
 )
 
 
@@ -189,6 +190,8 @@ class OlcTuning(C.Structure):
         ("stencil_tile_z", C.c_int32),
         ("contact_variant", C.c_int32),
         ("batch_tile_depth", C.c_int32),
+        ("stencil_pair_threads", C.c_int32),
+        ("stencil_pair_planes", C.c_int32),
     ]
 
 
@@ -375,6 +378,8 @@ _SIGS = {
     "olc_stage_bin_ranges": (C.c_int, [_VP, C.c_uint32, C.c_uint32, _VP, _VP]),
     "olc_stage_diffuse": (C.c_int, [_VP, _VP, _VP, C.POINTER(C.c_int32 * 3), C.c_float, C.c_float,
                                     C.POINTER(OlcDiffusion), _VP]),
+    "olc_stage_diffuse_tuned": (C.c_int, [_VP, _VP, _VP, C.POINTER(C.c_int32 * 3), C.c_float, C.c_float,
+                                          C.POINTER(OlcDiffusion), C.POINTER(OlcTuning), _VP]),
     "olc_stage_contact": (C.c_int, [_VP, _VP, C.c_uint32, C.POINTER(OlcGeom), C.POINTER(OlcContact), C.c_float,
                                     _VP, _VP, _VP, _VP]),
     "olc_create_pool": (C.c_int, [C.POINTER(OlcPoolConfig), C.POINTER(OlcCaps), C.POINTER(_VP)]),

@@ -5,7 +5,9 @@ candidate on the caller's own workload with per-stage CUDA events
 (olc_set_profiling) and keeps the fastest.
 
 * ``tune_engine(engine)``: the FP32 stencil tile (rows x planes of the TMA
-  substep) and the contact walk of a solo engine.  The engine's state is saved
+  substep), whether FP32 fields take two substeps per pass (temporal
+  blocking, and the CTA size of that kernel) and the contact walk of a solo
+  engine.  The engine's state is saved
   with ``state_dict()`` first and restored after, so tuning leaves the run
   exactly where it was.
 * ``tune_batch(make_batch)``: the batched FP32 substep's tile depth for each
@@ -30,7 +32,19 @@ STENCIL_TILES = ((8, 8), (16, 8), (8, 16), (16, 4))
 CONTACT_VARIANTS = (_lib.OLC_CONTACT_FLAT, _lib.OLC_CONTACT_NESTED, _lib.OLC_CONTACT_BRICK)
 CONTACT_NAMES = {_lib.OLC_CONTACT_FLAT: "flat", _lib.OLC_CONTACT_NESTED: "nested", _lib.OLC_CONTACT_BRICK: "brick"}
 BATCH_DEPTHS = (8, 16, 32)
-DEFAULT = {"stencil_tile": (8, 8), "contact_variant": _lib.OLC_CONTACT_FLAT, "batch_tile_depth": 16}
+# (threads per CTA, planes per CTA) of the two-substeps-per-pass kernel; (0, 0) = one substep per pass
+STENCIL_PAIRS = ((0, 0), (1024, 0), (512, 0), (256, 0), (128, 0))
+DEFAULT = {"stencil_tile": (8, 8), "contact_variant": _lib.OLC_CONTACT_FLAT, "batch_tile_depth": 16,
+           "stencil_pair": (0, 0)}
+VERSION = 2  # cache entries of earlier tuners lack choices; they are measured again
+
+
+def pair_applies(threads: int, dims) -> bool:
+    """Whether the two-substep kernel with ``threads`` per CTA runs on a field
+    of ``dims`` (x, y, z): rows of at most 256 voxels, x a multiple of 4, and
+    at least three intermediate rows per CTA (olc_field.cu pair_rows)."""
+    nx = int(dims[0])
+    return threads == 0 or (8 <= nx <= 256 and nx % 4 == 0 and threads // (nx // 4) >= 3)
 
 CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_cache", "tuning.json")
 _lock = threading.Lock()
@@ -74,7 +88,7 @@ def engine_key(eng) -> str:
         fields.append(f"{name}:{st}:{enc}:{eng.substeps_for(name) if name in eng._diffusion else 0}")
     contact = "mech" if (eng._contact is not None and be.mech_enabled()) else ("on" if eng._contact else "off")
     n = be.counters()["n_agents"]
-    return "|".join(["solo", _device_name(), "x".join(map(str, eng.chemistry_shape)),
+    return "|".join([f"solo{VERSION}", _device_name(), "x".join(map(str, eng.chemistry_shape)),
                      "x".join(map(str, eng.tissue_shape)), ",".join(fields), contact, f"n{_bucket(n)}"])
 
 
@@ -102,9 +116,7 @@ def tune_engine(eng, steps: int = 4, cache: bool = True) -> dict:
     if cache:
         hit = _load_cache().get(key)
         if hit:
-            t = hit["tuning"]
-            be.set_tuning(stencil_tile=tuple(t["stencil_tile"]), contact_variant=t["contact_variant"],
-                          batch_tile_depth=t["batch_tile_depth"])
+            be.set_tuning(**_tuning_args(hit["tuning"]))
             return dict(hit, cached=True)
     sd = be.state_dict()
     engine_step, graphs = eng._step, eng.use_graphs
@@ -118,6 +130,14 @@ def tune_engine(eng, steps: int = 4, cache: bool = True) -> dict:
                 times[tile] = _measure(eng, sd, dict(best, stencil_tile=tile), "ms_substeps", steps)
             best["stencil_tile"] = min(times, key=times.get)
             measured["substeps"] = {f"{a}x{b}": v for (a, b), v in times.items()}
+            # two substeps per pass, on the fastest single-pass tile (the odd
+            # substep of a field and pinned fields keep single passes)
+            times = {}
+            for pair in STENCIL_PAIRS:
+                if pair_applies(pair[0], eng.chemistry_shape):
+                    times[pair] = _measure(eng, sd, dict(best, stencil_pair=pair), "ms_substeps", steps)
+            best["stencil_pair"] = min(times, key=times.get)
+            measured["substep_pairs"] = {f"{a}/{b}": v for (a, b), v in times.items()}
         if eng._contact is not None and not be.mech_enabled():
             times = {}
             for v in CONTACT_VARIANTS:
@@ -130,11 +150,24 @@ def tune_engine(eng, steps: int = 4, cache: bool = True) -> dict:
         eng._step = engine_step
         eng.set_graphs(graphs)
     rec = {"tuning": {"stencil_tile": list(best["stencil_tile"]), "contact_variant": int(best["contact_variant"]),
-                      "batch_tile_depth": int(best["batch_tile_depth"])},
+                      "batch_tile_depth": int(best["batch_tile_depth"]), "stencil_pair": list(best["stencil_pair"])},
            "measured_ms": measured, "steps": steps}
     if cache:
         _store(key, rec)
     return dict(rec, cached=False)
+
+
+def _tuning_args(t: dict) -> dict:
+    """set_tuning keyword arguments from a record's "tuning" object."""
+    return {"stencil_tile": tuple(t["stencil_tile"]), "contact_variant": int(t["contact_variant"]),
+            "batch_tile_depth": int(t["batch_tile_depth"]), "stencil_pair": tuple(t.get("stencil_pair", (0, 0)))}
+
+
+def apply_engine(eng, rec: dict) -> None:
+    """Sets a tuning record's choices on another solo engine of the same
+    workload shape."""
+    if rec.get("tuning"):
+        eng._backend_impl.set_tuning(**_tuning_args(rec["tuning"]))
 
 
 def batch_key(batch) -> str:
@@ -199,5 +232,5 @@ def summary(rec: dict) -> dict:
     return out
 
 
-__all__ = ["tune_engine", "tune_batch", "apply_batch", "summary", "STENCIL_TILES", "CONTACT_VARIANTS",
-           "BATCH_DEPTHS"]
+__all__ = ["tune_engine", "tune_batch", "apply_engine", "apply_batch", "summary", "pair_applies", "STENCIL_TILES",
+           "STENCIL_PAIRS", "CONTACT_VARIANTS", "BATCH_DEPTHS"]

@@ -296,15 +296,21 @@ class CudaBackend:
 
     # ---- tuning (olc.h OlcTuning; oncolytica_b200.autotune measures it) -------
     def set_tuning(self, stencil_tile=(8, 8), contact_variant: int = _lib.OLC_CONTACT_FLAT,
-                   batch_tile_depth: int = 16) -> None:
-        t = _lib.OlcTuning(int(stencil_tile[0]), int(stencil_tile[1]), int(contact_variant), int(batch_tile_depth))
+                   batch_tile_depth: int = 16, stencil_pair=(0, 0)) -> None:
+        """Kernel shapes and variants (olc_set_tuning): the FP32 stencil tile
+        (rows, planes), the contact walk, the batched tile depth, and
+        ``stencil_pair`` = (threads per CTA, planes per CTA) of the
+        two-substeps-per-pass kernel ((0, 0): one substep per pass)."""
+        t = _lib.OlcTuning(int(stencil_tile[0]), int(stencil_tile[1]), int(contact_variant), int(batch_tile_depth),
+                           int(stencil_pair[0]), int(stencil_pair[1]))
         self._check(self.lib.olc_set_tuning(self.handle, C.byref(t)))
 
     def get_tuning(self) -> dict:
         t = _lib.OlcTuning()
         self._check(self.lib.olc_get_tuning(self.handle, C.byref(t)))
         return {"stencil_tile": (t.stencil_tile_y, t.stencil_tile_z), "contact_variant": t.contact_variant,
-                "batch_tile_depth": t.batch_tile_depth}
+                "batch_tile_depth": t.batch_tile_depth,
+                "stencil_pair": (t.stencil_pair_threads, t.stencil_pair_planes)}
 
     def has_tma_fields(self) -> bool:
         """Whether a diffusing FP32 field takes the TMA substep (the tuned tile)."""

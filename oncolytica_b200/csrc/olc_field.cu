@@ -18,6 +18,7 @@
 
 #include <cuda.h>  // CUtensorMap (types only; the encoder comes from cudaGetDriverEntryPoint)
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -253,6 +254,160 @@ __global__ void __launch_bounds__(16 * TYR, 1) k_substep_x4(const __grid_constan
     x4_tile<TYR, TZ>(tile, out, x0, y0, z0, nx, ny, nz, r, inv_decay, bval);
 }
 
+// ---------------------------------------------------------------- two substeps per pass
+// k_substep_pair<NT>: two substeps in one pass (temporal blocking), for FP32
+// fields whose rows fit one TMA box (nx <= 256, nx % 4 == 0).  A CTA owns
+// full-width rows [y0, y0 + TY) and planes [z0, z0 + ZL) and marches up z.
+// Each thread owns four consecutive x voxels of one row of the intermediate
+// (first-substep) field, which covers the CTA's rows plus one on each side
+// (MR = TY + 2 rows, MR = NT / (nx / 4)); full rows need no x halo.
+//   * Input planes z0-2 .. z0+ZL+1 (TY + 4 rows each, one TMA box per plane)
+//     stream through a ring of PAIR_RING shared-memory slots, each refilled as
+//     soon as every thread is past its last read of it.
+//   * Step p computes intermediate plane p (7-point update of the input, the
+//     thread's own column of planes p-1 and p held in registers) into one of
+//     three intermediate planes in shared memory and keeps it in registers;
+//     after the step's one barrier it computes output plane p-1 from the
+//     intermediate planes p-2, p-1 (registers), p (registers) and the x/y
+//     neighbours of plane p-1 (shared memory).
+// Every voxel of both substeps is computed with stencil_update4 and the
+// boundary rule of x4_tile (faces hold bval), so the output equals two
+// k_substep_x4 launches bit for bit; intermediate rows and planes outside
+// the grid are never read by an output inside it.  DRAM traffic is one read
+// and one write of the field per two substeps.
+constexpr int PAIR_RING = 4;
+
+__host__ __device__ inline int pair_round32(int v) { return (v + 31) & ~31; }
+
+// Shared memory of k_substep_pair for a row width and output rows per CTA.
+__host__ __device__ inline int pair_slot_floats(int nx, int ty) { return pair_round32(nx * (ty + 4)); }
+__host__ __device__ inline int pair_mid_floats(int nx, int ty) { return pair_round32(nx * (ty + 2)); }
+inline size_t pair_smem_bytes(int nx, int ty) {
+    return (size_t)(PAIR_RING * pair_slot_floats(nx, ty) + 3 * pair_mid_floats(nx, ty)) * 4 + 8 * PAIR_RING + 128;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_substep_pair(const __grid_constant__ CUtensorMap in_map,
+                                                               float* __restrict__ out, int nx, int ny, int nz,
+                                                               float r, float inv_decay, float bval,
+                                                               olc_u32* status, int rev, int ty, int zl) {
+    extern __shared__ unsigned char pair_raw[];
+    const olc_u32 pad = (128u - (smem_u32(pair_raw) & 127u)) & 127u;
+    float* ring = reinterpret_cast<float*>(pair_raw + pad);
+    const int slot_f = pair_slot_floats(nx, ty), mid_f = pair_mid_floats(nx, ty);
+    float* mid = ring + PAIR_RING * slot_f;
+    const olc_u32 bar0 = smem_u32(mid + 3 * mid_f);
+    const int by = rev ? gridDim.x - 1 - blockIdx.x : blockIdx.x;
+    const int bz = rev ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
+    const int y0 = by * ty, z0 = bz * zl;
+    const int z_end = min(z0 + zl, nz);
+    const int nq = z_end - z0 + 4;  // input planes z0-2 .. z_end+1
+    const olc_u32 plane_bytes = (olc_u32)(nx * (ty + 4) * 4);
+    const int G = nx >> 2, MR = ty + 2;
+    const int mr = threadIdx.x / G, g = threadIdx.x - mr * G;
+    const bool live = mr < MR;
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < PAIR_RING; ++k)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0 + 8 * k) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    // input plane z0 - 2 + q lives in slot q % PAIR_RING; its mbarrier phase is (q / PAIR_RING) & 1
+    int issued = 0;  // thread 0: planes issued so far
+    auto issue_upto = [&](int last_free) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        for (; issued < nq && issued - PAIR_RING <= last_free; ++issued) {
+            const olc_u32 bar = bar0 + 8 * (issued % PAIR_RING);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(plane_bytes)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+                "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(ring + (issued % PAIR_RING) * slot_f)),
+                "l"(reinterpret_cast<unsigned long long>(&in_map)), "r"(0), "r"(y0 - 2), "r"(z0 - 2 + issued),
+                "r"(bar)
+                : "memory");
+        }
+    };
+    auto wait_plane = [&](int q) {
+        return olc_mbar_wait_bounded(bar0 + 8 * (q % PAIR_RING), (olc_u32)((q / PAIR_RING) & 1), status);
+    };
+    if (threadIdx.x == 0) issue_upto(-1);
+    const int row_off = (mr + 1) * nx + 4 * g;  // this thread's voxels in an input slot
+    const int y = y0 - 1 + mr, x = 4 * g;
+    const bool y_face = y <= 0 || y >= ny - 1;  // rows outside the grid too (never read)
+    const bool ex0 = x == 0, ex3 = x + 3 == nx - 1;
+    const bool out_row = live && mr >= 1 && mr <= MR - 2 && y < ny;
+    const float4 b4 = make_float4(bval, bval, bval, bval);
+    const size_t sz = (size_t)nx * ny;
+    bool ok = wait_plane(0) && wait_plane(1);
+    float4 in_zm = b4, in_c = b4, mid_a = b4, mid_b = b4;
+    if (live) {
+        in_zm = *reinterpret_cast<const float4*>(ring + row_off);
+        in_c = *reinterpret_cast<const float4*>(ring + slot_f + row_off);
+    }
+    for (int p = z0 - 1, i = 0; p <= z_end; ++p, ++i) {
+        const int qn = i + 2;  // input plane p + 1
+        ok = ok && wait_plane(qn);
+        float4 v = b4;
+        if (live) {
+            const float* pc = ring + ((qn - 1) % PAIR_RING) * slot_f + row_off;
+            const float4 zp = *reinterpret_cast<const float4*>(ring + (qn % PAIR_RING) * slot_f + row_off);
+            const float4 ym = *reinterpret_cast<const float4*>(pc - nx);
+            const float4 yp = *reinterpret_cast<const float4*>(pc + nx);
+            v = stencil_update4(pc[-1], pc[4], in_c, ym, yp, in_zm, zp, r, inv_decay);
+            if (y_face || p <= 0 || p >= nz - 1) {
+                v = b4;
+            } else {
+                if (ex0) v.x = bval;
+                if (ex3) v.w = bval;
+            }
+            *reinterpret_cast<float4*>(mid + (i % 3) * mid_f + mr * nx + 4 * g) = v;
+            in_zm = in_c;
+            in_c = zp;
+        }
+        if (__syncthreads_or(!ok)) {
+            // a plane never arrived: let the copies still in flight land, then leave
+            if (threadIdx.x == 0)
+                for (int q = issued > PAIR_RING ? issued - PAIR_RING : 0; q < issued; ++q)
+                    for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it)
+                        if (olc_mbar_try_wait(bar0 + 8 * (q % PAIR_RING), (olc_u32)((q / PAIR_RING) & 1))) break;
+            return;
+        }
+        if (threadIdx.x == 0) issue_upto(qn - 1);  // input plane p is read for the last time
+        if (p - 1 >= z0 && out_row) {
+            const int z = p - 1;
+            const float* mb = mid + ((i + 2) % 3) * mid_f + mr * nx + 4 * g;  // intermediate plane p - 1
+            const float4 ym = *reinterpret_cast<const float4*>(mb - nx);
+            const float4 yp = *reinterpret_cast<const float4*>(mb + nx);
+            float4 o = stencil_update4(mb[-1], mb[4], mid_b, ym, yp, mid_a, v, r, inv_decay);
+            if (y == 0 || y == ny - 1 || z == 0 || z == nz - 1) {
+                o = b4;
+            } else {
+                if (ex0) o.x = bval;
+                if (ex3) o.w = bval;
+            }
+            *reinterpret_cast<float4*>(out + (size_t)z * sz + (size_t)y * nx + x) = o;
+        }
+        mid_a = mid_b;
+        mid_b = v;
+    }
+}
+
+// The CTA shape of k_substep_pair<nt> on a field: output rows per CTA (0 when
+// the field does not fit: nx > 256, nx % 4 != 0, or fewer than three
+// intermediate rows).
+int pair_rows(int nt, const int dims[3]) {
+    if (nt <= 0 || dims[0] > 256 || dims[0] % 4 != 0 || dims[0] < 8) return 0;
+    const int mr = nt / (dims[0] / 4);
+    if (mr < 3) return 0;
+    return std::min(std::min(mr - 2, dims[1]), 252);  // a box is at most 256 rows
+}
+
+bool pair_threads_known(int nt) { return nt == 0 || nt == 128 || nt == 256 || nt == 512 || nt == 1024; }
+
 // ---------------------------------------------------------------- batched substep
 // TMA box of a member's tensor map for the batched 16-bit substep.
 void batch_substep_box(int storage, cuuint32_t box[3]) {
@@ -321,14 +476,33 @@ bool stencil_tile_known(int tile_y, int tile_z) {
     return known;
 }
 
-bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3], int tile_y, int tile_z) {
+template <int NT>
+static int pair_default_planes(const int dims[3], int ty);
+
+bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3], int tile_y, int tile_z, int pair_threads,
+                     int pair_planes) {
     m->ok = false;
-    if (!stencil_tile_known(tile_y, tile_z)) return false;
+    m->pair_nt = m->pair_ty = m->pair_zl = 0;
+    if (!stencil_tile_known(tile_y, tile_z) || !pair_threads_known(pair_threads) || pair_planes < 0) return false;
     m->VY = tile_y;
     m->VZ = tile_z;
     const cuuint32_t boxv[3] = {72, (cuuint32_t)(tile_y + 2), (cuuint32_t)(tile_z + 2)};
     if (!encode_map(&m->vec[0], a, dims, boxv) || !encode_map(&m->vec[1], b, dims, boxv)) return false;
     m->ok = true;
+    // two substeps per pass where the rows fit one box (else single passes)
+    const int ty = pair_threads ? pair_rows(pair_threads, dims) : 0;
+    if (ty > 0) {
+        const cuuint32_t boxp[3] = {(cuuint32_t)dims[0], (cuuint32_t)(ty + 4), 1};
+        if (encode_map(&m->pair[0], a, dims, boxp) && encode_map(&m->pair[1], b, dims, boxp)) {
+            m->pair_nt = pair_threads;
+            m->pair_ty = ty;
+            m->pair_zl = pair_planes ? pair_planes
+                         : pair_threads == 128 ? pair_default_planes<128>(dims, ty)
+                         : pair_threads == 256 ? pair_default_planes<256>(dims, ty)
+                         : pair_threads == 512 ? pair_default_planes<512>(dims, ty)
+                                               : pair_default_planes<1024>(dims, ty);
+        }
+    }
     return true;
 }
 
@@ -355,6 +529,61 @@ static void launch_x4(const CUtensorMap& map, float* out, const FieldStep& fs, o
     cfg.numAttrs = 1;
     cudaLaunchKernelEx(&cfg, k_substep_x4<TYR, TZ>, map, out, fs.dims[0], fs.dims[1], fs.dims[2], fs.r,
                        fs.inv_decay, fs.bval, status, rev);
+}
+
+template <int NT>
+static void configure_pair() {
+    static int configured_mask = 0;  // per device (up to 32)
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 32 && !(configured_mask & (1 << dev))) {
+        cudaFuncSetAttribute(k_substep_pair<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+        configured_mask |= 1 << dev;
+    }
+}
+
+// Planes per CTA of k_substep_pair<NT>: as few as keep every CTA of the grid
+// resident in one wave (at least 8, so the z halo stays a small share).
+template <int NT>
+static int pair_default_planes(const int dims[3], int ty) {
+    configure_pair<NT>();
+    int dev = 0, sms = 148, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_substep_pair<NT>, NT, pair_smem_bytes(dims[0], ty));
+    const int slots = std::max(1, per_sm) * std::max(1, sms);
+    const int gy = (dims[1] + ty - 1) / ty;
+    const int chunks = std::max(1, slots / gy);
+    return std::max(8, (dims[2] + chunks - 1) / chunks);
+}
+
+template <int NT>
+static void launch_pair_nt(const FieldMaps& m, int cur, float* out, const FieldStep& fs, olc_u32* status, int rev,
+                           cudaStream_t s) {
+    configure_pair<NT>();
+    const int ny = fs.dims[1], nz = fs.dims[2], ty = m.pair_ty, zl = m.pair_zl;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((ny + ty - 1) / ty, (nz + zl - 1) / zl, 1);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = pair_smem_bytes(fs.dims[0], ty);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_substep_pair<NT>, m.pair[cur], out, fs.dims[0], ny, nz, fs.r, fs.inv_decay, fs.bval,
+                       status, rev, ty, zl);
+}
+
+static void launch_pair(const FieldMaps& m, int cur, float* out, const FieldStep& fs, olc_u32* status, int rev,
+                        cudaStream_t s) {
+    switch (m.pair_nt) {
+        case 128: launch_pair_nt<128>(m, cur, out, fs, status, rev, s); break;
+        case 256: launch_pair_nt<256>(m, cur, out, fs, status, rev, s); break;
+        case 512: launch_pair_nt<512>(m, cur, out, fs, status, rev, s); break;
+        default: launch_pair_nt<1024>(m, cur, out, fs, status, rev, s); break;
+    }
 }
 
 static void launch_single(const FieldMaps& m, int cur, float* out, const FieldStep& fs, olc_u32* status, int rev,
@@ -390,12 +619,27 @@ float* run_substeps_tma(float* a, float* b, const FieldMaps& m, int a_index, con
     bufs[a_index] = a;
     bufs[1 - a_index] = b;
     int cur = a_index;
-    for (int i = 0; i < fs.substeps; ++i) {
+    int i = 0;
+    if (m.pair_nt && !(pins && pins->n)) {
+        // two substeps per launch (pinned voxels are re-pinned after every
+        // substep, so fields with pins take single passes)
+        for (; i + 1 < fs.substeps; i += 2) {
+            launch_pair(m, cur, bufs[1 - cur], fs, status, (i >> 1) & 1, s);
+            cur = 1 - cur;
+        }
+    }
+    for (; i < fs.substeps; ++i) {
         launch_single(m, cur, bufs[1 - cur], fs, status, i & 1, s);
         launch_pins(bufs[1 - cur], pins, s);
         cur = 1 - cur;
     }
     return bufs[cur];
+}
+
+int substep_launches(const FieldMaps& m, const FieldStep& fs, const Pins* pins) {
+    if (pins && pins->n) return 2 * fs.substeps;
+    if (m.ok && m.pair_nt) return fs.substeps / 2 + (fs.substeps & 1);
+    return fs.substeps;
 }
 
 // Status word of the stateless stage entry points (bounded waits report here).

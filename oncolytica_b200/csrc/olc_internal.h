@@ -137,11 +137,22 @@ struct FieldMaps {
     bool ok = false;
     int VY = 8, VZ = 8;  // tile of k_substep_x4: rows and planes (a compiled shape)
     CUtensorMap vec[2];
+    // two substeps per pass (k_substep_pair): threads per CTA (0: off), output
+    // rows per CTA, planes per CTA (0: as many as fill one wave of CTAs)
+    int pair_nt = 0, pair_ty = 0, pair_zl = 0;
+    CUtensorMap pair[2];
 };
 // The TMA tensor maps of a FP32 field's two buffers for the (tile_y, tile_z)
 // tile; false when the tile is not compiled in or the field cannot be mapped
 // (the plain kernel runs then).
-bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3], int tile_y = 8, int tile_z = 8);
+bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3], int tile_y = 8, int tile_z = 8,
+                     int pair_threads = 0, int pair_planes = 0);
+// k_substep_pair's output rows per CTA of nt threads on a field (0: it does
+// not apply), and whether nt is a compiled CTA size (0 included: off).
+int pair_rows(int nt, const int dims[3]);
+bool pair_threads_known(int nt);
+// Kernel launches of run_substeps_tma for one field step.
+int substep_launches(const FieldMaps& m, const FieldStep& fs, const Pins* pins);
 bool stencil_tile_known(int tile_y, int tile_z);
 // Runs fs.substeps substeps starting from a (buffer index a_index of m).
 float* run_substeps_tma(float* a, float* b, const FieldMaps& m, int a_index, const FieldStep& fs, olc_u32* status,

@@ -69,7 +69,7 @@ struct OlcSim {
     int field_cur[OLC_MAX_FIELDS] = {};
     bool field_bound[OLC_MAX_FIELDS] = {};
     FieldMaps fmaps[OLC_MAX_FIELDS];           // TMA descriptors of both buffers
-    OlcTuning tuning = {8, 8, OLC_CONTACT_FLAT, 16};  // kernel shapes and variants (olc_set_tuning)
+    OlcTuning tuning = {8, 8, OLC_CONTACT_FLAT, 16, 0, 0};  // kernel shapes and variants (olc_set_tuning)
     std::vector<int> member_depth;                    // batched FP32 tile depth per member (0: tuning's)
     FieldMaps16 fmaps16[OLC_MAX_FIELDS];       // the same for 16-bit storage
     float* comp[OLC_MAX_FIELDS] = {};          // 16-bit storage: reaction residual per voxel (FP32)
@@ -373,7 +373,8 @@ int step_once(OlcSim* s, int collect, cudaStream_t st) {
                               : run_substeps(a, b, s->fstep[f], st, pins);
         s->field_cur[f] = (res == a) ? cur : 1 - cur;
         substeps += (uint32_t)s->fstep[f].substeps;
-        launches += (uint64_t)(pins ? 2 * s->fstep[f].substeps : s->fstep[f].substeps);
+        launches += (uint64_t)(tma_path ? substep_launches(s->fmaps[f], s->fstep[f], pins)
+                                        : (pins ? 2 * s->fstep[f].substeps : s->fstep[f].substeps));
     }
     mark(s, 2, st);
     // 2. grid + compaction
@@ -1259,7 +1260,8 @@ int olc_bind_field_ex(OlcSim* s, int index, void* a_, void* b_, float* sink, flo
     s->fmaps[index].ok = false;
     s->fmaps16[index].ok = false;
     if (spec->substeps > 0 && !half)
-        make_field_maps(&s->fmaps[index], a, b, s->geom.chem_dims, s->tuning.stencil_tile_y, s->tuning.stencil_tile_z);
+        make_field_maps(&s->fmaps[index], a, b, s->geom.chem_dims, s->tuning.stencil_tile_y, s->tuning.stencil_tile_z,
+                        s->tuning.stencil_pair_threads, s->tuning.stencil_pair_planes);
     if (spec->substeps > 0 && half && !make_field_maps16(&s->fmaps16[index], a, b, s->geom.chem_dims))
         return fail(s, OLC_ERR_ARG, "olc_bind_field_ex: TMA descriptors of the 16-bit field failed (16-byte aligned "
                                     "buffers, x extent a multiple of 8)");
@@ -2382,19 +2384,25 @@ int olc_stage_bin_ranges(const uint32_t* keys, uint32_t n, uint32_t n_bins, uint
     return cuda_status(cudaGetLastError(), "olc_stage_bin_ranges");
 }
 
-int olc_stage_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], float dx, float dt,
-                      const OlcDiffusion* spec, void* stream) {
-    if (!f || !tmp || !dims || !spec) return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse: null argument");
+static int stage_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], float dx, float dt,
+                         const OlcDiffusion* spec, const OlcTuning* t, void* stream, const char* who) {
+    if (!f || !tmp || !dims || !spec) return fail(nullptr, OLC_ERR_ARG, std::string(who) + ": null argument");
     if (spec->storage != OLC_FIELD_F32)
-        return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse: FP32 storage only (olc_stage_diffuse16 for 16-bit)");
+        return fail(nullptr, OLC_ERR_ARG, std::string(who) + ": FP32 storage only (olc_stage_diffuse16 for 16-bit)");
     std::string err;
     FieldStep fs;
-    if (!make_field_step(*spec, dims, dx, dt, &fs, &err)) return fail(nullptr, OLC_ERR_ARG, "olc_stage_diffuse: " + err);
+    if (!make_field_step(*spec, dims, dx, dt, &fs, &err)) return fail(nullptr, OLC_ERR_ARG, std::string(who) + ": " + err);
+    const OlcTuning def = {8, 8, OLC_CONTACT_FLAT, 16, 0, 0};
+    if (!t) t = &def;
+    if (!stencil_tile_known(t->stencil_tile_y, t->stencil_tile_z) || !pair_threads_known(t->stencil_pair_threads) ||
+        t->stencil_pair_planes < 0 || t->stencil_pair_planes > 4096)
+        return fail(nullptr, OLC_ERR_ARG, std::string(who) + ": unknown stencil tile or pair shape");
     cudaStream_t st = as_stream(stream);
     FieldMaps maps;
     olc_u32* status = stage_status_word();
     float* res;
-    if (status && make_field_maps(&maps, f, tmp, dims)) {
+    if (status && make_field_maps(&maps, f, tmp, dims, t->stencil_tile_y, t->stencil_tile_z, t->stencil_pair_threads,
+                                  t->stencil_pair_planes)) {
         launch_sink(f, spec->has_sink ? sink : nullptr, fs, st);
         res = run_substeps_tma(f, tmp, maps, 0, fs, status, st);
     } else {
@@ -2404,7 +2412,17 @@ int olc_stage_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], 
         const size_t bytes = (size_t)dims[0] * dims[1] * dims[2] * 4;
         cudaMemcpyAsync(f, res, bytes, cudaMemcpyDeviceToDevice, st);
     }
-    return cuda_status(cudaGetLastError(), "olc_stage_diffuse");
+    return cuda_status(cudaGetLastError(), who);
+}
+
+int olc_stage_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3], float dx, float dt,
+                      const OlcDiffusion* spec, void* stream) {
+    return stage_diffuse(f, tmp, sink, dims, dx, dt, spec, nullptr, stream, "olc_stage_diffuse");
+}
+
+int olc_stage_diffuse_tuned(float* f, float* tmp, float* sink, const int32_t dims[3], float dx, float dt,
+                            const OlcDiffusion* spec, const OlcTuning* tuning, void* stream) {
+    return stage_diffuse(f, tmp, sink, dims, dx, dt, spec, tuning, stream, "olc_stage_diffuse_tuned");
 }
 
 int olc_stage_diffuse_pinned(float* f, float* tmp, float* sink, const int32_t dims[3], float dx, float dt,
@@ -2593,6 +2611,9 @@ int olc_set_tuning(OlcSim* s, const OlcTuning* t) {
         return fail(s, OLC_ERR_ARG, "olc_set_tuning: contact_variant must be an OLC_CONTACT_* value");
     if (t->batch_tile_depth != 8 && t->batch_tile_depth != 16 && t->batch_tile_depth != 32)
         return fail(s, OLC_ERR_ARG, "olc_set_tuning: batch_tile_depth must be 8, 16 or 32");
+    if (!pair_threads_known(t->stencil_pair_threads) || t->stencil_pair_planes < 0 || t->stencil_pair_planes > 4096)
+        return fail(s, OLC_ERR_ARG, "olc_set_tuning: stencil_pair_threads must be 0, 128, 256, 512 or 1024 and "
+                                    "stencil_pair_planes in [0, 4096]");
     OLC_TRY(check(s, cudaDeviceSynchronize(), "sync"));
     drop_graphs(s);
     const bool depth_changed = t->batch_tile_depth != s->tuning.batch_tile_depth;
@@ -2602,7 +2623,7 @@ int olc_set_tuning(OlcSim* s, const OlcTuning* t) {
         for (olc_u32 f = 0; f < s->caps.n_fields; ++f) {
             if (!s->field_bound[f] || s->fstep[f].storage != OLC_FIELD_F32 || s->fstep[f].substeps == 0) continue;
             make_field_maps(&s->fmaps[f], s->field[0][f], s->field[1][f], s->geom.chem_dims, t->stencil_tile_y,
-                            t->stencil_tile_z);
+                            t->stencil_tile_z, t->stencil_pair_threads, t->stencil_pair_planes);
         }
     } else if (depth_changed && !s->pool) {
         for (olc_u32 f = 0; f < s->caps.n_fields; ++f)

@@ -48,6 +48,19 @@ def test_every_choice_gives_the_same_bits(cuda, tile, contact):
     _same(eng._backend_impl.snapshot(), ref._backend_impl.snapshot(), f"tile {tile} contact {contact}")
 
 
+@pytest.mark.parametrize("pair", [p for p in autotune.STENCIL_PAIRS if p[0]] + [(256, 7)])
+def test_two_substeps_per_pass_give_the_same_bits(cuda, pair):
+    spec = _spec()
+    state = W.initial_state(spec)
+    ref = W.build_engine(spec, state)
+    ref.run_steps(3)
+    eng = W.build_engine(spec, state)
+    eng._backend_impl.set_tuning(stencil_pair=pair)
+    assert eng._backend_impl.get_tuning()["stencil_pair"] == tuple(pair)
+    eng.run_steps(3)
+    _same(eng._backend_impl.snapshot(), ref._backend_impl.snapshot(), f"pair {pair}")
+
+
 @pytest.mark.parametrize("contact", autotune.CONTACT_VARIANTS)
 def test_contact_variants_agree_on_a_dense_population(cuda, contact):
     spec = _spec(dense=True)
@@ -72,7 +85,8 @@ def test_tuning_restores_the_run_and_caches(cuda, tmp_path, monkeypatch):
     assert not rec["cached"]
     assert tuple(rec["tuning"]["stencil_tile"]) in autotune.STENCIL_TILES
     assert rec["tuning"]["contact_variant"] in autotune.CONTACT_VARIANTS
-    assert set(rec["measured_ms"]) == {"substeps", "contact"}
+    assert set(rec["measured_ms"]) == {"substeps", "substep_pairs", "contact"}
+    assert tuple(rec["tuning"]["stencil_pair"]) in autotune.STENCIL_PAIRS
     assert eng._backend_impl.get_tuning()["stencil_tile"] == tuple(rec["tuning"]["stencil_tile"])
     assert eng._step == 1 and eng._backend_impl.counters()["steps"] == 1
     eng.run_steps(1)
@@ -88,6 +102,8 @@ def test_tuning_rejects_unknown_shapes(cuda):
         eng._backend_impl.set_tuning(stencil_tile=(4, 4))
     with pytest.raises(_lib.OlcError):
         eng._backend_impl.set_tuning(batch_tile_depth=12)
+    with pytest.raises(_lib.OlcError):
+        eng._backend_impl.set_tuning(stencil_pair=(384, 0))
 
 
 def test_batch_tile_depths_give_the_same_bits(cuda, tmp_path, monkeypatch):

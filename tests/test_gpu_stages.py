@@ -219,49 +219,53 @@ def test_diffuse_bit_exact(cuda, olc, dims, substeps, decay, with_sink):
         assert float(to_host(sd).max()) == 0.0
 
 
-TB_SHAPES = ["2,8,16", "2,8,32", "2,16,16", "3,8,16", "3,16,16", "4,16,16", "2,4,32"]
-VX_SHAPES = ["16,8", "16,4", "8,8", "8,16", "16,16", "32,4"]
-PIPE_SHAPES = ["8,8,2", "8,8,3", "8,8,4", "16,4,2", "16,4,3", "16,8,2", "32,4,2"]
-T2_SHAPES = ["8,16,6", "8,32,6", "12,16,6", "12,32,6", "16,16,6", "16,32,6", "8,32,8", "8,16,8", "16,16,8"]
-_ONE = {"OLC_TB": "1,8,16", "OLC_VX": "0", "OLC_PIPE": "0", "OLC_T2": "0"}
-# environment of each stencil path: scalar TMA tiles, 4-wide tiles, persistent
-# pipelines, temporal blocks (alone and with 4-wide remainders), register columns
-STENCIL_MODES = ([dict(_ONE)] + [dict(_ONE, OLC_VX=v) for v in VX_SHAPES]
-                 + [dict(_ONE, OLC_PIPE=p) for p in PIPE_SHAPES]
-                 + [dict(_ONE, OLC_T2=t, OLC_VX="8,8") for t in T2_SHAPES]
-                 + [dict(_ONE, OLC_T2=T2_SHAPES[0], OLC_VX="8,8", OLC_STENCIL_ORDER="forward")]
-                 + [dict(_ONE, OLC_TB=t) for t in TB_SHAPES] + [dict(_ONE, OLC_TB=TB_SHAPES[0], OLC_VX="8,8")]
-                 + [dict(_ONE, OLC_STENCIL_ORDER="forward", OLC_VX="8,8")]
-                 + [dict(_ONE, OLC_STENCIL="plain")])
+# (stencil tile, (threads, planes) of the two-substeps-per-pass kernel): every
+# single-pass tile, and the pair kernel at each CTA size, with the planes per
+# CTA chosen by occupancy (0) and forced small and odd (ragged z chunks)
+STENCIL_CHOICES = ([(tile, (0, 0)) for tile in ((8, 8), (16, 8), (8, 16), (16, 4))]
+                   + [((8, 8), pair) for pair in ((1024, 0), (512, 0), (256, 0), (128, 0), (1024, 9), (512, 13),
+                                                  (256, 5), (128, 8))]
+                   + [((16, 4), (256, 3))])
 
 
-@pytest.mark.parametrize("dims", [(68, 41, 37), (128, 34, 19), (64, 64, 70)])
-def test_diffuse_plain_and_tma_paths_agree(cuda, olc, monkeypatch, dims):
-    """The scalar TMA tile kernel, every 4-wide tile shape, every persistent
-    pipeline shape, every two-substeps-per-pass shape, every temporal-block
-    shape (T substeps per pass) and the register-column kernel give the
-    oracle's bits; 7 substeps so odd remainders run too, and ragged tiles and
-    z chunks in every direction."""
+@pytest.mark.parametrize("substeps", [7, 8])
+@pytest.mark.parametrize("dims", [(68, 41, 37), (128, 34, 19), (64, 64, 70), (256, 30, 21), (66, 23, 17)])
+def test_diffuse_every_stencil_choice_bit_exact(cuda, olc, dims, substeps):
+    """Every single-pass tile and every two-substeps-per-pass shape
+    (olc_stage_diffuse_tuned) gives the oracle's bits: odd and even substep
+    counts (a pair kernel's odd substep is a single pass), ragged tiles and z
+    chunks in every direction, rows of 256 voxels where the smallest pair CTA
+    does not apply, and an x extent the TMA cannot map (66: the plain
+    register-column kernel runs for every choice)."""
     import torch
 
-    rng = np.random.default_rng(77)
+    rng = np.random.default_rng(77 + substeps)
     nx, ny, nz = dims
     f = rng.random((nz, ny, nx), dtype=np.float32)
-    spec = _lib.OlcDiffusion(diffusion=1.0, decay=0.02, boundary=0.4, substeps=7, has_sink=0)
+    spec = _lib.OlcDiffusion(diffusion=1.0, decay=0.02, boundary=0.4, substeps=substeps, has_sink=0)
     dims_c = (C.c_int32 * 3)(nx, ny, nz)
-    outs = []
-    for mode in STENCIL_MODES:
-        for k in ("OLC_STENCIL", "OLC_STENCIL_ORDER"):
-            monkeypatch.delenv(k, raising=False)
-        for k, v in mode.items():
-            monkeypatch.setenv(k, v)
+    ref = oracle.diffuse(f, None, dx=1.0, dt=0.5 * substeps / 7, D=1.0, decay=0.02, boundary=0.4, substeps=substeps)
+    for tile, pair in STENCIL_CHOICES:
+        t = _lib.OlcTuning(tile[0], tile[1], 0, 16, pair[0], pair[1])
         fd = to_dev(f, cuda)
         tmp = torch.empty_like(fd)
-        _lib.check(olc.olc_stage_diffuse(dptr(fd), dptr(tmp), None, C.byref(dims_c), 1.0, 0.5, C.byref(spec), None))
-        outs.append(to_host(fd))
-    ref = oracle.diffuse(f, None, dx=1.0, dt=0.5, D=1.0, decay=0.02, boundary=0.4, substeps=7)
-    for mode, out in zip(STENCIL_MODES, outs):
-        np.testing.assert_array_equal(out, ref, err_msg=str(mode))
+        _lib.check(olc.olc_stage_diffuse_tuned(dptr(fd), dptr(tmp), None, C.byref(dims_c), 1.0, 0.5 * substeps / 7,
+                                               C.byref(spec), C.byref(t), None))
+        np.testing.assert_array_equal(to_host(fd), ref, err_msg=f"tile {tile} pair {pair}")
+
+
+def test_diffuse_tuned_rejects_unknown_shapes(cuda, olc):
+    import torch
+
+    f = torch.zeros(16 * 16 * 16, dtype=torch.float32, device="cuda")
+    tmp = torch.empty_like(f)
+    spec = _lib.OlcDiffusion(diffusion=1.0, decay=0.0, boundary=0.4, substeps=2, has_sink=0)
+    dims_c = (C.c_int32 * 3)(16, 16, 16)
+    for t in (_lib.OlcTuning(8, 8, 0, 16, 64, 0), _lib.OlcTuning(4, 4, 0, 16, 0, 0),
+              _lib.OlcTuning(8, 8, 0, 16, 256, -1)):
+        rc = olc.olc_stage_diffuse_tuned(dptr(f), dptr(tmp), None, C.byref(dims_c), 1.0, 0.5, C.byref(spec),
+                                         C.byref(t), None)
+        assert rc == _lib.OLC_ERR_ARG
 
 
 def test_diffuse_pinned_voxels_bit_exact(cuda, olc):
