@@ -233,9 +233,10 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep16(const __grid_constan
             : "memory");
     }
     // bounded wait for the tile (olc_mbar_wait_bounded records a timeout); the
-    // decision is the CTA's, so every lane reaches the tile's shuffles or none
+    // decision is the warp's, so every lane of a warp reaches the tile's
+    // shuffles or none (the tile has no block-wide barrier)
     const bool tile_ready = olc_mbar_wait_bounded(bar, 0, status);
-    if (__syncthreads_or(!tile_ready)) return;
+    if (__any_sync(0xffffffffu, !tile_ready)) return;
     t16_tile<ST, EN>(tile, out, x0, y0, z0, fs.dims[0], fs.dims[1], fs.dims[2], fs,
                      olc_sr_key(step_ctr ? *step_ctr : step_host, sub, field));
 }
@@ -287,9 +288,10 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep_batch_t16(
             : "memory");
     }
     // bounded wait for the tile (olc_mbar_wait_bounded records a timeout); the
-    // decision is the CTA's, so every lane reaches the tile's shuffles or none
+    // decision is the warp's, so every lane of a warp reaches the tile's
+    // shuffles or none (the tile has no block-wide barrier)
     const bool tile_ready = olc_mbar_wait_bounded(bar, 0, status);
-    if (__syncthreads_or(!tile_ready)) return;
+    if (__any_sync(0xffffffffu, !tile_ready)) return;
     t16_tile<ST, EN>(tile, out, x0, y0, z0, d.cdims[0], d.cdims[1], d.cdims[2], fs,
                      olc_sr_key(*step_ctr - d.step_base, sub, field));
 }

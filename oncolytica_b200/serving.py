@@ -533,6 +533,10 @@ class PoolDevice:
             if any(kind == 3 for _, kind in self.program.kernels):
                 its = (C.c_int * len(self.program.kernels))(*self.program.iterations)
                 self._check(self.lib.olc_set_rule_iterations(self.handle, its, len(self.program.kernels)))
+        # every chemistry-rule iteration writes every field's other buffer and
+        # flips its parity (olc_sim.cu step_once_batch), as each substep does
+        self.chem_flips = (sum(it for (_, kind), it in zip(self.program.kernels, self.program.iterations)
+                               if kind == 3) if self.program is not None else 0)
         self.metrics_words = max(1, len(L.metrics))
         self._check(self.lib.olc_set_user_metrics_size(self.handle, 4 * self.metrics_words))
         self.sim_col = len(L.cell_cols) - 1
@@ -742,7 +746,7 @@ class PoolDevice:
                     t.record_stream(self.stream)
                 count.record_stream(self.stream)
                 for i, name in enumerate(L.chem_fields):
-                    par = (steps * m.substeps[i]) & 1
+                    par = (steps * (m.substeps[i] + self.chem_flips)) & 1
                     src = self.fields_dev[i][par][m.field_off:m.field_off + m.nvox]
                     h = torch.empty(m.nvox, dtype=src.dtype, pin_memory=True)
                     h.copy_(src, non_blocking=True)

@@ -109,7 +109,7 @@ def _chem_engine(shape, seed, n):
     eng.chemistry.column("signal")[...] = rng.uniform(0.0, 0.5, size=eng.chemistry_shape).astype(np.float32)
     hi = np.array(shape, np.float32) * 4.0
     eng.cells.add_arrays(CM.CCell, pos=(rng.uniform(0.1, 0.9, size=(n, 3)) * hi).astype(np.float32),
-                         kind=rng.integers(0, 2, n), energy=rng.uniform(0.3, 0.9, n).astype(np.float32))
+                         kind=rng.integers(0, 2, n), energy=rng.uniform(0.0, 1.1, n).astype(np.float32))
     return eng, CM.ChemSim()
 
 

@@ -164,7 +164,7 @@ def test_served_chemistry_rules_match_solo_runs(cuda):
         e.chemistry.column("signal")[...] = rng.uniform(0.0, 0.5, size=e.chemistry_shape).astype(np.float32)
         hi = np.array(shape, np.float32) * 4.0
         e.cells.add_arrays(CM.CCell, pos=(rng.uniform(0.1, 0.9, size=(n, 3)) * hi).astype(np.float32),
-                           kind=rng.integers(0, 2, n), energy=rng.uniform(0.3, 0.9, n).astype(np.float32))
+                           kind=rng.integers(0, 2, n), energy=rng.uniform(0.0, 1.1, n).astype(np.float32))
         return e
 
     cases = [((16, 16, 16), 5, 300, 5), ((24, 24, 24), 6, 600, 4), ((16, 16, 16), 7, 200, 3)]
