@@ -150,11 +150,12 @@ typedef struct {
  * (its dispatches are fixed 256-wide: _gpu_backend.py:134-136). */
 #define OLC_CONTACT_FLAT   0  /* one flat walk over each agent's listed non-empty Moore bins */
 #define OLC_CONTACT_NESTED 1  /* nested loops over the 27 Moore bins                       */
-#define OLC_CONTACT_BRICK  2  /* one CTA per 2x2x2 bin brick, its 4x4x4 halo in shared memory */
+#define OLC_CONTACT_WARP   2  /* one warp per bin: its Moore candidates staged in shared
+                                 memory, (agent, candidate) pairs over the lanes */
 typedef struct {
     int32_t stencil_tile_y;   /* FP32 TMA substep tile: rows (8 or 16) ...             */
     int32_t stencil_tile_z;   /* ... and planes; (y, z) in {(8,8), (16,8), (8,16), (16,4)} */
-    int32_t contact_variant;  /* OLC_CONTACT_FLAT, OLC_CONTACT_NESTED or OLC_CONTACT_BRICK */
+    int32_t contact_variant;  /* OLC_CONTACT_FLAT, OLC_CONTACT_NESTED or OLC_CONTACT_WARP */
     int32_t batch_tile_depth; /* planes per tile of the batched FP32 substep: 8, 16 or
                                  32 (members without their own, olc_set_batch_tile_depths) */
     int32_t stencil_pair_threads; /* two FP32 substeps per pass (temporal blocking) with
@@ -671,6 +672,12 @@ int olc_stage_diffuse16(void* f_dev, void* tmp_dev, float* sink_dev, float* comp
 int olc_stage_contact(const float* posr_dev, const uint32_t* ranges_dev, uint32_t n,
                       const OlcGeom* geom, const OlcContact* spec, float dt,
                       float* x_dev, float* y_dev, float* z_dev, void* stream);
+
+/* olc_stage_contact with a chosen walk (OLC_CONTACT_*); every walk gives the
+ * same positions.  ranges_dev must cover every bin of the tissue grid. */
+int olc_stage_contact_tuned(const float* posr_dev, const uint32_t* ranges_dev, uint32_t n, const OlcGeom* geom,
+                            const OlcContact* spec, float dt, int32_t contact_variant, float* x_dev,
+                            float* y_dev, float* z_dev, void* stream);
 
 /* The contact pass with OlcMechanics: state_dev (i32 per sorted row) may be
  * NULL; vx/vy/vz_dev (f32 per sorted row, updated in place) are used when

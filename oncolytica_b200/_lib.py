@@ -55,7 +55,7 @@ EXPORTS = (
     "olc_stage_contact_mech", "olc_stage_contact_motion", "olc_bind_tissue_pair", "olc_current_tissue", "olc_set_rule_iterations",
     "olc_set_pinned", "olc_stage_diffuse_pinned", "olc_sort_noalloc_status", "olc_sort_status_offset",
     "olc_selftest_bounded_waits", "olc_set_tuning", "olc_get_tuning", "olc_set_batch_tile_depths",
-    "olc_stage_diffuse_tuned",
+    "olc_stage_diffuse_tuned", "olc_stage_contact_tuned",
 )
 
 
@@ -181,7 +181,7 @@ class OlcDiffusion(C.Structure):
 
 OLC_CONTACT_FLAT = 0
 OLC_CONTACT_NESTED = 1
-OLC_CONTACT_BRICK = 2
+OLC_CONTACT_WARP = 2
 
 
 class OlcTuning(C.Structure):
@@ -382,6 +382,8 @@ _SIGS = {
                                           C.POINTER(OlcDiffusion), C.POINTER(OlcTuning), _VP]),
     "olc_stage_contact": (C.c_int, [_VP, _VP, C.c_uint32, C.POINTER(OlcGeom), C.POINTER(OlcContact), C.c_float,
                                     _VP, _VP, _VP, _VP]),
+    "olc_stage_contact_tuned": (C.c_int, [_VP, _VP, C.c_uint32, C.POINTER(OlcGeom), C.POINTER(OlcContact),
+                                          C.c_float, C.c_int32, _VP, _VP, _VP, _VP]),
     "olc_create_pool": (C.c_int, [C.POINTER(OlcPoolConfig), C.POINTER(OlcCaps), C.POINTER(_VP)]),
     "olc_bind_field_pool": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, _VP, C.c_int, C.c_int, C.c_float]),
     "olc_pool_admit": (C.c_int, [_VP, C.POINTER(OlcGeom), C.POINTER(OlcDiffusion), _VP, C.c_size_t,

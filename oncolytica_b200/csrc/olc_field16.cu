@@ -154,7 +154,7 @@ __device__ __forceinline__ void t16_tile(const unsigned short* tile, unsigned sh
     using namespace t16;
     const int g = threadIdx.x & 7, ty = threadIdx.x >> 3;
     const int x = x0 + 8 * g, y = y0 + ty;
-    // lanes past the grid still load (inside the box) and shuffle, but store nothing
+    // lanes past the grid still load (inside the box), but store nothing
     const bool active = x < nx && y < ny;
     const EncConst k = enc_const(fs);
     const float r = fs.r, inv_decay = fs.inv_decay, dec_sub = fs.dec_sub;
@@ -177,12 +177,10 @@ __device__ __forceinline__ void t16_tile(const unsigned short* tile, unsigned sh
         load8w<ST, EN>(pc + PS, zp, k);
         load8w<ST, EN>(pc - WX, ym, k);
         load8w<ST, EN>(pc + WX, yp, k);
-        // x neighbours of the group: the row's neighbouring lanes hold them
-        // (groups of 8 lanes span a 64-voxel row); the lanes at the tile's
-        // ends read the halo column from shared memory
-        float xl = __shfl_up_sync(0xffffffffu, c[7], 1, 8), xr = __shfl_down_sync(0xffffffffu, c[0], 1, 8);
-        if (g == 0) xl = Codec<ST, EN>::work(pc[-1], k);
-        if (g == 7) xr = Codec<ST, EN>::work(pc[8], k);
+        // x neighbours of the group from shared memory (2-byte loads with a
+        // 4-way bank conflict; lane shuffles of the neighbours' registers
+        // measured 14 % slower on B200)
+        const float xl = Codec<ST, EN>::work(pc[-1], k), xr = Codec<ST, EN>::work(pc[8], k);
         stencil_update8_enc<EN>(xl, xr, c, ym, yp, zm, zp, r, inv_decay, dec_sub, k.b, v);
         if (edge_y || z == 0 || z == nz - 1) {
 #pragma unroll
@@ -232,9 +230,8 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep16(const __grid_constan
             "l"(reinterpret_cast<unsigned long long>(&in_map)), "r"(x0 - HX), "r"(y0 - 1), "r"(z0 - 1), "r"(bar)
             : "memory");
     }
-    // bounded wait for the tile (olc_mbar_wait_bounded records a timeout); the
-    // decision is the warp's, so every lane of a warp reaches the tile's
-    // shuffles or none (the tile has no block-wide barrier)
+    // bounded wait for the tile (olc_mbar_wait_bounded records a timeout);
+    // a warp leaves as a whole (the tile has no block-wide barrier)
     const bool tile_ready = olc_mbar_wait_bounded(bar, 0, status);
     if (__any_sync(0xffffffffu, !tile_ready)) return;
     t16_tile<ST, EN>(tile, out, x0, y0, z0, fs.dims[0], fs.dims[1], fs.dims[2], fs,
@@ -287,9 +284,8 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep_batch_t16(
             "l"(reinterpret_cast<unsigned long long>(map)), "r"(x0 - HX), "r"(y0 - 1), "r"(z0 - 1), "r"(bar)
             : "memory");
     }
-    // bounded wait for the tile (olc_mbar_wait_bounded records a timeout); the
-    // decision is the warp's, so every lane of a warp reaches the tile's
-    // shuffles or none (the tile has no block-wide barrier)
+    // bounded wait for the tile (olc_mbar_wait_bounded records a timeout);
+    // a warp leaves as a whole (the tile has no block-wide barrier)
     const bool tile_ready = olc_mbar_wait_bounded(bar, 0, status);
     if (__any_sync(0xffffffffu, !tile_ready)) return;
     t16_tile<ST, EN>(tile, out, x0, y0, z0, d.cdims[0], d.cdims[1], d.cdims[2], fs,

@@ -2476,12 +2476,15 @@ int olc_stage_diffuse16(void* f, void* tmp, float* sink, float* comp, const int3
     return cuda_status(cudaGetLastError(), "olc_stage_diffuse16");
 }
 
-int olc_stage_contact(const float* posr, const uint32_t* ranges, uint32_t n, const OlcGeom* geom,
-                      const OlcContact* spec, float dt, float* x, float* y, float* z, void* stream) {
+static int stage_contact(const float* posr, const uint32_t* ranges, uint32_t n, const OlcGeom* geom,
+                         const OlcContact* spec, float dt, int variant, float* x, float* y, float* z, void* stream,
+                         const char* who) {
     if (!geom || !spec || (n && (!posr || !ranges || !x || !y || !z)))
-        return fail(nullptr, OLC_ERR_ARG, "olc_stage_contact: null argument");
+        return fail(nullptr, OLC_ERR_ARG, std::string(who) + ": null argument");
+    if (variant != OLC_CONTACT_FLAT && variant != OLC_CONTACT_NESTED && variant != OLC_CONTACT_WARP)
+        return fail(nullptr, OLC_ERR_ARG, std::string(who) + ": contact_variant must be an OLC_CONTACT_* value");
     std::string err;
-    if (!geom_ok(*geom, &err)) return fail(nullptr, OLC_ERR_ARG, "olc_stage_contact: " + err);
+    if (!geom_ok(*geom, &err)) return fail(nullptr, OLC_ERR_ARG, std::string(who) + ": " + err);
     if (n == 0) return OLC_OK;
     ContactDev d;
     for (int i = 0; i < 3; ++i) {
@@ -2494,8 +2497,21 @@ int olc_stage_contact(const float* posr, const uint32_t* ranges, uint32_t n, con
     d.mobility = spec->mobility;
     d.max_disp = spec->max_disp;
     d.dt = dt;
-    launch_contact(reinterpret_cast<const float4*>(posr), ranges, nullptr, n, n, d, x, y, z, as_stream(stream));
-    return cuda_status(cudaGetLastError(), "olc_stage_contact");
+    launch_contact(reinterpret_cast<const float4*>(posr), ranges, nullptr, n, n, d, x, y, z, as_stream(stream),
+                   variant);
+    return cuda_status(cudaGetLastError(), who);
+}
+
+int olc_stage_contact(const float* posr, const uint32_t* ranges, uint32_t n, const OlcGeom* geom,
+                      const OlcContact* spec, float dt, float* x, float* y, float* z, void* stream) {
+    return stage_contact(posr, ranges, n, geom, spec, dt, OLC_CONTACT_FLAT, x, y, z, stream, "olc_stage_contact");
+}
+
+int olc_stage_contact_tuned(const float* posr, const uint32_t* ranges, uint32_t n, const OlcGeom* geom,
+                            const OlcContact* spec, float dt, int32_t contact_variant, float* x, float* y, float* z,
+                            void* stream) {
+    return stage_contact(posr, ranges, n, geom, spec, dt, contact_variant, x, y, z, stream,
+                         "olc_stage_contact_tuned");
 }
 
 int olc_stage_contact_mech(const float* posr, const uint32_t* ranges, uint32_t n, const OlcGeom* geom,
@@ -2607,7 +2623,7 @@ int olc_set_tuning(OlcSim* s, const OlcTuning* t) {
                                         std::to_string(t->stencil_tile_z) +
                                         ") is not one of (8,8), (16,8), (8,16), (16,4)");
     if (t->contact_variant != OLC_CONTACT_FLAT && t->contact_variant != OLC_CONTACT_NESTED &&
-        t->contact_variant != OLC_CONTACT_BRICK)
+        t->contact_variant != OLC_CONTACT_WARP)
         return fail(s, OLC_ERR_ARG, "olc_set_tuning: contact_variant must be an OLC_CONTACT_* value");
     if (t->batch_tile_depth != 8 && t->batch_tile_depth != 16 && t->batch_tile_depth != 32)
         return fail(s, OLC_ERR_ARG, "olc_set_tuning: batch_tile_depth must be 8, 16 or 32");

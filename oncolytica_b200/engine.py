@@ -202,8 +202,8 @@ class Engine:
         reference, whose fields are FP32).  ``encoding`` says what a 16-bit
         element holds: "value"; "deficit" (boundary - value, for fields that
         stay near their boundary value, like O2); "offset3" (the value minus
-        the nearest of 0, b/2 and b, for fields spread over [0, b], like a
-        decaying drug); "auto" picks by storage, decay and the initial values
+        the nearest of 0, b/2 and b: fine near all three); "auto" picks
+        "offset3" for BF16 fields with 0 < b <= 4 and "value" otherwise
         (_fieldcodec.resolve).  Encoded fields are clamped to [0, boundary]
         (FP32 and value-encoded fields at 0 only), so a BF16 field whose
         values may exceed its boundary value needs ``encoding="value"``."""

@@ -83,9 +83,10 @@ def test_oracle_step_keeps_encoded_fields_in_range(storage, encoding):
 
 
 def test_auto_resolution():
-    assert fc.resolve("auto", 3, 0.0, 1.0, 1.0) == 1     # O2-like BF16: deficit
+    assert fc.resolve("auto", 3, 0.0, 1.0, 1.0) == 2     # O2-like BF16: three offsets (it may be depleted)
     assert fc.resolve("auto", 3, 0.1, 1.0, 0.0) == 2     # decaying drug: three offsets
-    assert fc.resolve("auto", 1, 0.0, 1.0, 0.0) == 2     # starts far from b: three offsets
+    assert fc.resolve("auto", 1, 0.0, 1.0, 0.0) == 2     # BF16, nearest: three offsets
+    assert fc.resolve("deficit", 3, 0.0, 1.0, 1.0) == 1  # the deficit on request
     assert fc.resolve("auto", 4, 0.0, 1.0, 1.0) == 0     # FP16 keeps values
     assert fc.resolve("auto", 3, 0.0, 0.0, 1.0) == 0     # no positive boundary value
     assert fc.resolve("value", 3, 0.0, 1.0, 1.0) == 0

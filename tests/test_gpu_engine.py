@@ -659,10 +659,9 @@ def test_tumour_step_parity_16bit_fields(cuda, storage, code):
     eng.sync_to_device()
     be = eng._backend_impl
     shp = tuple(spec.field_dims[::-1])
-    # what the elements hold: BF16 fields default to the deficit (O2, no
-    # decay, starts at its boundary value) and three offsets (the decaying drug)
+    # what the elements hold: BF16 fields default to three offsets, FP16 to values
     e_o2, e_dr = be.field_codec("o2")[1], be.field_codec("drug")[1]
-    assert (e_o2, e_dr) == ((1, 2) if code in (1, 3) else (0, 0))
+    assert (e_o2, e_dr) == ((2, 2) if code in (1, 3) else (0, 0))
     for step in range(4):
         snap = be.snapshot()
         k = be.counters()["steps"]  # the step count salts stochastic rounding, with the field's index

@@ -158,16 +158,17 @@ def test_bf16_encodings_meet_the_error_bar(cuda, olc):
         assert got.min() >= 0.0 and got.max() <= bnd + 1e-6
 
 
-def test_bf16_deficit_after_1000_steps(cuda, olc):
+@pytest.mark.parametrize("encoding", [1, 2])
+def test_bf16_encodings_after_1000_steps(cuda, olc, encoding):
     """The 1,000-step O2-like run of test_field_error_after_1000_steps in
-    BF16 with stochastic rounding, storing deficits: relative L2 below 1e-3
-    (BF16 storing values: 2.0e-3)."""
+    BF16 with stochastic rounding, storing deficits or three offsets:
+    relative L2 below 1e-3 (BF16 storing values: 2.0e-3)."""
     import os
 
     shape, K = _problem(n=64, seed=9)
     steps, dx, dt, D = 1000, 4.0, 0.1, 2000.0
     S = int(np.ceil(6.0 * D * dt / (dx * dx)))
-    got = _run_gpu(olc, cuda, 3, shape, K, D, 0.0, 1.0, 1.0, S, dx, dt, steps, encoding=1)
+    got = _run_gpu(olc, cuda, 3, shape, K, D, 0.0, 1.0, 1.0, S, dx, dt, steps, encoding=encoding)
     if "ref" not in _LONG_REF:
         ref = np.ones(shape, np.float64)
         threads = max(1, os.cpu_count() or 1)
@@ -176,5 +177,5 @@ def test_bf16_deficit_after_1000_steps(cuda, olc):
         _LONG_REF["ref"] = ref
     ref = _LONG_REF["ref"]
     rel = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
-    print(f"BF16-SR deficit 1000 steps 64^3: rel-L2 {rel:.3e} max {np.abs(got - ref).max():.3e}")
+    print(f"BF16-SR encoding {encoding} 1000 steps 64^3: rel-L2 {rel:.3e} max {np.abs(got - ref).max():.3e}")
     assert rel <= ENC_REL_L2, rel

@@ -333,6 +333,50 @@ def test_contact_bit_exact(cuda, olc):
     assert moved.sum() > n // 2
 
 
+@pytest.mark.parametrize("variant", [_lib.OLC_CONTACT_FLAT, _lib.OLC_CONTACT_NESTED, _lib.OLC_CONTACT_WARP])
+@pytest.mark.parametrize("case", ["sparse", "dense", "moved", "cluster"])
+def test_contact_walks_bit_exact(cuda, olc, variant, case):
+    """Every contact walk (olc_stage_contact_tuned) against orc_contact:
+    a sparse population; a dense one (bins of more agents than a warp holds
+    and neighbourhoods larger than its staging buffer, which take the global
+    walk); agents moved after the sort (a rule's displacement), whose current
+    bin differs from the one they are sorted in; and a cluster of 50 agents
+    in one bin of a sparse neighbourhood (two agents per lane on the warp
+    walk).  Coincident points and dead rows in each."""
+    rng = np.random.default_rng(31)
+    dims, vs = (20, 20, 20), 10.0
+    n, sd = {"sparse": (30000, 25.0), "dense": (40000, 16.0), "moved": (30000, 20.0), "cluster": (8000, 40.0)}[case]
+    pos = np.clip(rng.normal(100.0, sd, size=(n, 3)), 0.0, 199.0).astype(np.float32)
+    if case == "cluster":
+        pos[:50] = rng.uniform(100.5, 109.5, size=(50, 3)).astype(np.float32)
+    pos[5] = pos[6]
+    radius = rng.uniform(4.0, 6.0, size=n).astype(np.float32)
+    k = oracle.keys(pos, dims, vs)
+    ks, perm = oracle.sort_pairs(k)
+    ranges = oracle.bin_ranges(ks, oracle.tissue_key(*dims))
+    posr = np.concatenate([pos[perm], radius[perm, None]], axis=1).astype(np.float32)
+    posr[rng.random(n) < 0.02, 3] = -1.0
+    if case == "moved":
+        m = rng.random(n) < 0.05
+        posr[m, :3] = np.clip(posr[m, :3] + rng.normal(0.0, 6.0, size=(int(m.sum()), 3)), 0.0, 199.0)
+    lo, hi = (0.1, 0.1, 0.1), (199.9, 199.9, 199.9)
+    ref = oracle.contact(posr, ranges, dims, vs, 1.0, 10.0, 1.0, 0.1, lo, hi)
+    pr, rg = to_dev(posr, cuda), to_dev(ranges, cuda)
+    x, y, z = (to_dev(np.ascontiguousarray(posr[:, a]), cuda) for a in range(3))
+    g = geom(dims, vs, lo=(0, 0, 0), hi=(200, 200, 200))
+    spec = _lib.OlcContact(enabled=1, radius_field=-1, radius_const=0.0, stiffness=1.0, mobility=10.0,
+                           max_disp=1.0, margin=0.1)
+    _lib.check(olc.olc_stage_contact_tuned(dptr(pr), dptr(rg), n, C.byref(g), C.byref(spec), 0.1, variant, dptr(x),
+                                           dptr(y), dptr(z), None))
+    got = np.stack([to_host(x), to_host(y), to_host(z)], axis=1)
+    np.testing.assert_array_equal(got, ref)
+    counts = ranges[1::2] - ranges[0::2]
+    if case == "dense":
+        assert counts.max() > 64  # some bins take the global walk whole
+    if case == "cluster":
+        assert 32 < counts.max() <= 64
+
+
 @pytest.mark.parametrize("adhesion,velocity", [(False, True), (True, False), (True, True)])
 def test_contact_mechanics_matches_the_oracle(cuda, olc, adhesion, velocity):
     """The engine's force-law extras (necrotic factor, adhesion, damped
