@@ -136,9 +136,13 @@ struct Codec {
         // magnitude with the sign (bit 15) kept and bit 14 cleared, plus
         // (b/2) x (bit 15 + bit 14): codes 00 -> m, 01 -> b/2 + m,
         // 10 -> b/2 - m, 11 -> b - m
+        // The offset (b/2 per set flag bit; both products and their sum are
+        // exact) is formed with selects: an integer-to-float conversion runs
+        // on the quarter-rate conversion pipe and bounded the substep.
         const float m = Store16<ST>::to_f((unsigned short)(h & 0xBFFFu));
-        const olc_u32 units = (olc_u32)(h >> 15) + (olc_u32)((h >> 14) & 1u);
-        return __fadd_rn(m, __fmul_rn((float)units, k.half_b));
+        const float o15 = (h & 0x8000u) ? k.half_b : 0.0f;
+        const float o14 = (h & 0x4000u) ? k.half_b : 0.0f;
+        return __fadd_rn(m, __fadd_rn(o15, o14));
     }
     // field value from a working value
     static __device__ __forceinline__ float phys_of_work(float w, const EncConst& k) {
