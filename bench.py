@@ -36,6 +36,7 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 METRIC = "agent-steps/s + voxel-updates/s, batched vs plain FP32 on 1 B200; p99 sim latency"
+P99_TARGET_S = 3.0  # serving mix: p99 time to completion (see measure_serving)
 UNIT = "agent-steps/s"
 
 
@@ -65,6 +66,13 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--workload-base", default="scale", help="the workload --workload precision runs")
     ap.add_argument("--error-steps", type=int, default=10,
                     help="steps of the field-error measurement added to the default line")
+    ap.add_argument("--contact", default="auto", choices=["auto", "flat", "nested", "warp"],
+                    help="contact walk of the scale workload (auto: the tuner's choice)")
+    ap.add_argument("--grid", type=int, default=256, help="field edge of --workload stencil")
+    ap.add_argument("--stencil-pair", default="0,1024,512",
+                    help="CTA sizes of the two-substep pass timed by --workload stencil (0: one substep per pass)")
+    ap.add_argument("--encodings", default="value,deficit,offset3",
+                    help="16-bit element encodings timed by --workload stencil")
     return ap.parse_args()
 
 
@@ -298,9 +306,16 @@ def run_b200(args) -> None:
     state0 = W.initial_state(spec)
     eng = W.build_engine(spec, state0)
     # kernel shapes and variants measured on this workload (state restored)
-    from oncolytica_b200 import autotune
+    from oncolytica_b200 import _lib, autotune
 
     tuning = autotune.tune_engine(eng) if not args.no_tune else {"tuning": None}
+    if args.contact != "auto":
+        # a fixed contact walk (profiling one variant); the other choices stay tuned
+        t = dict(tuning["tuning"] or {"stencil_tile": [8, 8], "batch_tile_depth": 16, "stencil_pair": [0, 0]})
+        t["contact_variant"] = {"flat": _lib.OLC_CONTACT_FLAT, "nested": _lib.OLC_CONTACT_NESTED,
+                                "warp": _lib.OLC_CONTACT_WARP}[args.contact]
+        tuning = dict(tuning, tuning=t)
+        autotune.apply_engine(eng, tuning)
     eng.set_graphs(not args.no_graphs)
     be = eng._backend_impl
     dev = torch.device("cuda", local)
@@ -881,13 +896,14 @@ def measure_serving(rate: float, duration: float, seed: int = 0, storage: str = 
                                    "served_vs_solo": out["agent_steps_per_s"] / (solo_as / (solo_ms / 1e3)),
                                    "sample": "requests spread over the mix by size, each run alone for its own "
                                              "step count on a solo FP32 engine with CUDA graphs"}
-        # the latency target: no request waits longer, at the 99th percentile,
-        # than the mix's largest request takes alone on the plain FP32 path
-        # (the sample includes the largest request)
-        out["p99_target_s"] = max(solo_each)
-        out["p99_target"] = "p99 time to completion <= the largest request's time alone on the plain FP32 path"
-        out["p99_target_met"] = bool(out["ttc_p99_s"] <= out["p99_target_s"])
+        out["solo_largest_s"] = max(solo_each)
         torch.cuda.empty_cache()
+    # the stated latency target of the serving mix (requests of up to 1,000
+    # steps at 20 requests/s): every pool step advances all residents by one
+    # step, so a request's time to completion is about its step count times
+    # the pool's step time; 3 s bounds a 1,000-step request at 3 ms per pool step
+    out["p99_target_s"] = P99_TARGET_S
+    out["p99_target_met"] = bool(out["ttc_p99_s"] <= P99_TARGET_S)
     return out
 
 
@@ -942,10 +958,76 @@ def run_serving_workload(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+def run_stencil_workload(args) -> None:
+    """The diffusion kernels alone on one G^3 field (--grid): FP32 one or two
+    substeps per pass (--stencil-pair CTA sizes) and the 16-bit storages with
+    each element encoding (--encodings), through the tuned stage entries
+    (olc_stage_diffuse_tuned, olc_stage_diffuse16).  Device time per substep
+    over --steps calls of 40 substeps after --warmup, CUDA events."""
+    import ctypes as C
+
+    import torch
+
+    rank, world, local = env_ranks()
+    torch.cuda.set_device(local)
+    from oncolytica_b200 import _lib
+    from oncolytica_b200._fieldcodec import ENCODINGS
+
+    olc = _lib.load()
+    n, S, dx, D = args.grid, 40, 4.0, 2000.0
+    dt = 0.15 * dx * dx * S / D  # D dt / (S dx^2) = 0.15
+    dims = (C.c_int32 * 3)(n, n, n)
+    dev = torch.device("cuda", local)
+    st = torch.cuda.current_stream(dev)
+    gen = torch.Generator(device=dev).manual_seed(rank)
+    f32 = torch.rand(n ** 3, device=dev, generator=gen) * 0.8 + 0.1
+
+    def timed(fn) -> float:
+        for _ in range(max(1, args.warmup)):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) * 1e3 / (args.steps * S)
+
+    out = {}
+    spec = _lib.OlcDiffusion(diffusion=D, decay=0.0, boundary=1.0, substeps=S, has_sink=0)
+    f, tmp = f32.clone(), torch.empty_like(f32)
+    for nt in (int(v) for v in args.stencil_pair.split(",") if v):
+        t = _lib.OlcTuning(8, 8, 0, 16, nt, 0)
+        out[f"f32_pair{nt}" if nt else "f32_single"] = timed(lambda: _lib.check(olc.olc_stage_diffuse_tuned(
+            f.data_ptr(), tmp.data_ptr(), None, C.byref(dims), dx, dt, C.byref(spec), C.byref(t), None)))
+    for storage in (3, 4):
+        for name in (e for e in args.encodings.split(",") if e):
+            code = ENCODINGS[name]
+            h = f32.to(torch.bfloat16 if storage == 3 else torch.float16).view(torch.int16)
+            if code == 2:
+                h = h & 0x3FFF  # flag bits 00: the magnitude is the value
+            tmp16, comp = torch.empty_like(h), torch.zeros(n ** 3, dtype=torch.float32, device=dev)
+            sp = _lib.OlcDiffusion(diffusion=D, decay=0.0, boundary=1.0, substeps=S, has_sink=0, storage=storage,
+                                   encoding=code)
+            out[f"{'bf16' if storage == 3 else 'f16'}_sr_{name}"] = timed(lambda: _lib.check(olc.olc_stage_diffuse16(
+                h.data_ptr(), tmp16.data_ptr(), None, comp.data_ptr(), C.byref(dims), dx, dt, C.byref(sp), 7, 0,
+                None)))
+    line = {"metric": "us per substep (one field)", "value": out.get("f32_single"), "unit": "us",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "dtype": "f32 / 16-bit fields", "data": "synthetic (torch uniform, seed = rank)",
+            "config": {"workload": f"diffusion kernels on one {n}^3 field, {S} substeps per call"},
+            "us_per_substep": out}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "stencil":
+        run_stencil_workload(args)
     elif args.workload == "batch":
         run_batch_workload(args)
     elif args.workload == "serve":
