@@ -66,7 +66,7 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--workload-base", default="scale", help="the workload --workload precision runs")
     ap.add_argument("--error-steps", type=int, default=10,
                     help="steps of the field-error measurement added to the default line")
-    ap.add_argument("--contact", default="auto", choices=["auto", "flat", "nested", "warp"],
+    ap.add_argument("--contact", default="auto", choices=["auto", "flat", "nested", "warp", "brick"],
                     help="contact walk of the scale workload (auto: the tuner's choice)")
     ap.add_argument("--grid", type=int, default=256, help="field edge of --workload stencil")
     ap.add_argument("--stencil-pair", default="0,1024,512",
@@ -313,7 +313,7 @@ def run_b200(args) -> None:
         # a fixed contact walk (profiling one variant); the other choices stay tuned
         t = dict(tuning["tuning"] or {"stencil_tile": [8, 8], "batch_tile_depth": 16, "stencil_pair": [0, 0]})
         t["contact_variant"] = {"flat": _lib.OLC_CONTACT_FLAT, "nested": _lib.OLC_CONTACT_NESTED,
-                                "warp": _lib.OLC_CONTACT_WARP}[args.contact]
+                                "warp": _lib.OLC_CONTACT_WARP, "brick": _lib.OLC_CONTACT_BRICK}[args.contact]
         tuning = dict(tuning, tuning=t)
         autotune.apply_engine(eng, tuning)
     eng.set_graphs(not args.no_graphs)
@@ -997,12 +997,12 @@ def run_stencil_workload(args) -> None:
     out = {}
     spec = _lib.OlcDiffusion(diffusion=D, decay=0.0, boundary=1.0, substeps=S, has_sink=0)
     f, tmp = f32.clone(), torch.empty_like(f32)
-    for nt in (int(v) for v in args.stencil_pair.split(",") if v):
+    for nt in (int(v) for v in args.stencil_pair.split(",") if v and v != "none"):
         t = _lib.OlcTuning(8, 8, 0, 16, nt, 0)
         out[f"f32_pair{nt}" if nt else "f32_single"] = timed(lambda: _lib.check(olc.olc_stage_diffuse_tuned(
             f.data_ptr(), tmp.data_ptr(), None, C.byref(dims), dx, dt, C.byref(spec), C.byref(t), None)))
     for storage in (3, 4):
-        for name in (e for e in args.encodings.split(",") if e):
+        for name in (e for e in args.encodings.split(",") if e and e != "none"):
             code = ENCODINGS[name]
             h = f32.to(torch.bfloat16 if storage == 3 else torch.float16).view(torch.int16)
             if code == 2:

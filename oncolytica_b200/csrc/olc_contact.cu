@@ -604,6 +604,108 @@ __global__ void __launch_bounds__(32 * CW_WARPS) k_contact_warp(const float4* __
     }
 }
 
+// ---------------------------------------------------------------- bin bricks
+// k_contact_brick: one CTA per 4 x 4 x 4 brick of bins.  Its 64 bins are 64
+// consecutive keys (two Morton levels below the coarse grid's parity bits),
+// so its agents are one contiguous run of sorted rows.  The CTA stages the
+// records of the 6 x 6 x 6 bins around the brick (every home bin's Moore
+// neighbourhood) in shared memory once, then each thread walks one agent's
+// 27 bins there in k_contact's order with its pair law, so the sums are the
+// same bits.  Agents whose current position left the brick since the sort,
+// and every agent of a brick whose halo holds more records than the staging
+// buffer, take the global walk.
+constexpr int CB_THREADS = 256;
+constexpr int CB_HALO = 216;    // 6 x 6 x 6 bins
+constexpr int CB_CAP = 1536;    // staged records per brick
+
+__global__ void __launch_bounds__(CB_THREADS) k_contact_brick(const float4* __restrict__ posr,
+                                                             const uint2* __restrict__ ranges, olc_u32 n_keys,
+                                                             ContactDev c, float* __restrict__ xo,
+                                                             float* __restrict__ yo, float* __restrict__ zo) {
+    __shared__ float4 s_rec[CB_CAP];
+    __shared__ olc_u32 s_off[CB_HALO + 1];  // first staged record of halo bin h; s_off[216] = total
+    __shared__ olc_u32 s_row[CB_HALO];      // first row of halo bin h
+    __shared__ olc_u32 s_warp[CB_THREADS / 32];
+    __shared__ olc_u32 s_home[2];           // the brick's rows [begin, end)
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const float md = __fmul_rn(c.mobility, c.dt);
+    const olc_u32 n_bricks = (n_keys + 63u) / 64u;
+    for (olc_u32 B = blockIdx.x; B < n_bricks; B += gridDim.x) {
+        __syncthreads();  // the previous brick is done with the shared arrays
+        // the brick's rows: its 64 keys' ranges (empty keys hold [0, 0))
+        uint2 hr = make_uint2(0xffffffffu, 0u);
+        if (t < 64 && 64u * B + (olc_u32)t < n_keys) {
+            const uint2 r = __ldg(ranges + 64u * B + (olc_u32)t);
+            if (r.y > r.x) hr = r;
+        }
+        olc_u32 lo = hr.x, hi = hr.y;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if (t == 0) s_home[0] = lo, s_home[1] = hi;
+        __syncthreads();
+        if (t == 32) s_home[0] = min(s_home[0], lo), s_home[1] = max(s_home[1], hi);
+        __syncthreads();
+        const olc_u32 h0 = s_home[0], h1 = s_home[1];
+        if (h0 >= h1) continue;  // uniform: every thread read the same words
+        // brick origin in bins: key 64B + q is coarse key 8B + (q >> 3), parity q & 7
+        const int ox = 4 * (int)olc_compact9(B), oy = 4 * (int)olc_compact9(B >> 1), oz = 4 * (int)olc_compact9(B >> 2);
+        // halo bin t at brick-local (t % 6, (t / 6) % 6, t / 36) - 1
+        uint2 rg = make_uint2(0u, 0u);
+        if (t < CB_HALO) {
+            const int gx = ox - 1 + t % 6, gy = oy - 1 + (t / 6) % 6, gz = oz - 1 + t / 36;
+            if (gx >= 0 && gy >= 0 && gz >= 0 && gx < c.tdims[0] && gy < c.tdims[1] && gz < c.tdims[2])
+                rg = __ldg(ranges + olc_tissue_key(gx, gy, gz));
+        }
+        const olc_u32 cnt = rg.y - rg.x;
+        olc_u32 incl = cnt;  // inclusive scan over the 256 threads
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const olc_u32 v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        olc_u32 before = 0;
+        for (int w = 0; w < warp; ++w) before += s_warp[w];
+        incl += before;
+        if (t < CB_HALO) {
+            s_off[t] = incl - cnt;
+            s_row[t] = rg.x;
+        }
+        if (t == CB_HALO - 1) s_off[CB_HALO] = incl;
+        __syncthreads();
+        const bool staged = s_off[CB_HALO] <= (olc_u32)CB_CAP;
+        if (staged && t < CB_HALO)
+            for (olc_u32 k = 0; k < cnt; ++k) s_rec[incl - cnt + k] = __ldg(posr + rg.x + k);
+        __syncthreads();
+        for (olc_u32 i = h0 + (olc_u32)t; i < h1; i += CB_THREADS) {
+            const float4 p = __ldg(posr + i);
+            if (p.w < 0.0f) continue;  // dead this step: no move, no force
+            const int lx = olc_bin_coord(p.x, c.tvs, c.tdims[0]) - ox + 1;
+            const int ly = olc_bin_coord(p.y, c.tvs, c.tdims[1]) - oy + 1;
+            const int lz = olc_bin_coord(p.z, c.tvs, c.tdims[2]) - oz + 1;
+            float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+            if (staged && lx >= 1 && lx <= 4 && ly >= 1 && ly <= 4 && lz >= 1 && lz <= 4) {
+                for (int dz = -1; dz <= 1; ++dz)
+                    for (int dy = -1; dy <= 1; ++dy)
+                        for (int dx = -1; dx <= 1; ++dx) {
+                            // bins outside the grid are empty here, as k_contact skips them
+                            const int h = (lz + dz) * 36 + (ly + dy) * 6 + (lx + dx);
+                            const olc_u32 k0 = s_off[h], k1 = s_off[h + 1], row0 = s_row[h];
+                            for (olc_u32 k = k0; k < k1; ++k)
+                                contact_pair(p, s_rec[k], i, row0 + (k - k0), c, fx, fy, fz);
+                        }
+            } else {
+                contact_walk_global(posr, ranges, p, i, c, fx, fy, fz);
+            }
+            contact_move(p, i, fx, fy, fz, c, md, xo, yo, zo);
+        }
+    }
+}
+
 // The two walks (olc.h OLC_CONTACT_*): bit-identical, chosen per handle by
 // measurement (OlcTuning.contact_variant).  On the 1 M-agent scale workload
 // the flat walk took 0.92 ms per step over 200 steps against 1.04 for the
@@ -624,6 +726,16 @@ void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_
         if (blocks == 0) blocks = 1;
         k_contact_warp<<<blocks, 32 * CW_WARPS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_keys, c, x,
                                                          y, z);
+        return;
+    }
+    if (variant == OLC_CONTACT_BRICK) {
+        // rows come from the bin table; 64 keys per brick up to the far corner's key
+        const olc_u32 n_keys = olc_tissue_key(c.tdims[0] - 1, c.tdims[1] - 1, c.tdims[2] - 1) + 1u;
+        const olc_u32 n_bricks = (n_keys + 63u) / 64u;
+        olc_u32 blocks = n_bricks < 148u * 6u ? n_bricks : 148u * 6u;
+        if (blocks == 0) blocks = 1;
+        k_contact_brick<<<blocks, CB_THREADS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_keys, c, x, y,
+                                                      z);
         return;
     }
     if (variant != OLC_CONTACT_NESTED) {

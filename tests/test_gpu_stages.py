@@ -333,7 +333,8 @@ def test_contact_bit_exact(cuda, olc):
     assert moved.sum() > n // 2
 
 
-@pytest.mark.parametrize("variant", [_lib.OLC_CONTACT_FLAT, _lib.OLC_CONTACT_NESTED, _lib.OLC_CONTACT_WARP])
+@pytest.mark.parametrize("variant", [_lib.OLC_CONTACT_FLAT, _lib.OLC_CONTACT_NESTED, _lib.OLC_CONTACT_WARP,
+                                     _lib.OLC_CONTACT_BRICK])
 @pytest.mark.parametrize("case", ["sparse", "dense", "moved", "cluster"])
 def test_contact_walks_bit_exact(cuda, olc, variant, case):
     """Every contact walk (olc_stage_contact_tuned) against orc_contact:
