@@ -365,28 +365,7 @@ __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __res
     }
 }
 
-// ---------------------------------------------------------------- warp per bin
-// k_contact_warp: one warp per non-empty bin B.  Every agent whose current
-// position lies in B has the same candidates: the rows of B's 27 Moore bins,
-// in the order above.  The warp stages those C records (and their rows) in
-// its shared memory once, then evaluates the nB x C (agent, candidate) pairs
-// with the lanes over consecutive pairs, agent-major:
-//   1. prefilter: the contact test of contact_pair on every pair; the pairs
-//      in contact are appended to a queue in pair order (ballot + popc), so
-//      each agent's entries are contiguous and in candidate order;
-//   2. forces: lanes over queued pairs compute contact_pair's contribution
-//      (the same operations), into shared memory;
-//   3. sums: the lane owning an agent adds its queued contributions in queue
-//      order, i.e. in the order of k_contact's walk, so the sums are the same
-//      bits.
-// Agents whose current position left B since the sort (a rule moved them),
-// bins whose neighbourhood holds more records than the staging buffer, and
-// bins of more than CW_HOME agents take k_contact's walk over global memory.
-constexpr int CW_WARPS = 4;      // warps per CTA
-constexpr int CW_CAP = 384;      // staged candidate records per warp
-constexpr int CW_QCAP = 128;     // queued contact pairs per warp
-constexpr int CW_HOME = 64;      // agents per bin on the warp path (two per lane)
-
+// ---------------------------------------------------------------- shared helpers
 __device__ __forceinline__ olc_u32 olc_compact9(olc_u32 x) {
     x &= 0x09249249u;
     x = (x | (x >> 2)) & 0x030c30c3u;
@@ -434,174 +413,6 @@ __device__ __forceinline__ void contact_move(const float4& p, olc_u32 i, float f
     xo[i] = fminf(fmaxf(__fadd_rn(p.x, mx), c.lo[0]), c.hi[0]);
     yo[i] = fminf(fmaxf(__fadd_rn(p.y, my), c.lo[1]), c.hi[1]);
     zo[i] = fminf(fmaxf(__fadd_rn(p.z, mz), c.lo[2]), c.hi[2]);
-}
-
-// contact_pair's test: whether the pair (p, i) - (q, j) is in contact.
-__device__ __forceinline__ bool contact_test(const float4& p, const float4& q, olc_u32 i, olc_u32 j) {
-    if (j == i || q.w < 0.0f) return false;
-    const float ddx = __fsub_rn(p.x, q.x);
-    const float ddy = __fsub_rn(p.y, q.y);
-    const float ddz = __fsub_rn(p.z, q.z);
-    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), __fmul_rn(ddz, ddz));
-    const float rsum = __fadd_rn(p.w, q.w);
-    if (d2 > __fmul_rn(__fmul_rn(rsum, rsum), 1.00000095367431640625f)) return false;
-    return sqrtf(d2) < rsum;
-}
-
-struct ContactWarpSmem {
-    float4 rec[CW_CAP];      // candidate records (Moore order, rows ascending)
-    olc_u32 row[CW_CAP];     // their rows
-    olc_u32 qpair[CW_QCAP];  // queued pairs: agent << 16 | candidate
-    float qf[3][CW_QCAP];    // their force contributions
-    unsigned char flag[CW_HOME];  // per home agent: 0 warp path, 1 global walk, 2 dead
-};
-
-__global__ void __launch_bounds__(32 * CW_WARPS) k_contact_warp(const float4* __restrict__ posr,
-                                                               const uint2* __restrict__ ranges, olc_u32 n_keys,
-                                                               ContactDev c, float* __restrict__ xo,
-                                                               float* __restrict__ yo, float* __restrict__ zo) {
-    __shared__ ContactWarpSmem smem[CW_WARPS];
-    ContactWarpSmem& S = smem[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
-    const olc_u32 lt_mask = (1u << lane) - 1u;
-    const float md = __fmul_rn(c.mobility, c.dt);
-    const olc_u32 n_warps = gridDim.x * CW_WARPS;
-    const olc_u32 gw = blockIdx.x * CW_WARPS + (threadIdx.x >> 5);
-    // lane m < 27: Moore offset m (x fastest, then y, then z)
-    const int mdx = lane % 3 - 1, mdy = (lane / 3) % 3 - 1, mdz = lane / 9 - 1;
-    for (olc_u32 kb = gw * 32u; kb < n_keys; kb += n_warps * 32u) {
-        const olc_u32 kl = kb + (olc_u32)lane;
-        const uint2 own = kl < n_keys ? __ldg(ranges + kl) : make_uint2(0u, 0u);
-        olc_u32 busy = __ballot_sync(0xffffffffu, own.y > own.x);
-        while (busy) {
-            const int bl = __ffs(busy) - 1;
-            busy &= busy - 1u;
-            const olc_u32 key = kb + (olc_u32)bl;
-            const olc_u32 s0 = __shfl_sync(0xffffffffu, own.x, bl), s1 = __shfl_sync(0xffffffffu, own.y, bl);
-            const int nB = (int)(s1 - s0);
-            const olc_u32 brick = key >> 3;
-            const int bx = 2 * (int)olc_compact9(brick) + (int)(key & 1u);
-            const int by = 2 * (int)olc_compact9(brick >> 1) + (int)((key >> 1) & 1u);
-            const int bz = 2 * (int)olc_compact9(brick >> 2) + (int)((key >> 2) & 1u);
-            // the 27 Moore bins' ranges and their offsets among the candidates
-            uint2 rg = make_uint2(0u, 0u);
-            if (lane < 27) {
-                const int nx = bx + mdx, ny = by + mdy, nz = bz + mdz;
-                if (nx >= 0 && ny >= 0 && nz >= 0 && nx < c.tdims[0] && ny < c.tdims[1] && nz < c.tdims[2])
-                    rg = __ldg(ranges + olc_tissue_key(nx, ny, nz));
-            }
-            const olc_u32 cnt = rg.y - rg.x;
-            olc_u32 incl = cnt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const olc_u32 v = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += v;
-            }
-            const olc_u32 C = __shfl_sync(0xffffffffu, incl, 26);
-            const olc_u32 home0 = __shfl_sync(0xffffffffu, incl - cnt, 13);  // first home record
-            const bool warp_path = C <= (olc_u32)CW_CAP && nB <= CW_HOME;
-            if (warp_path) {
-                // stage the candidates: candidate k comes from the first bin m whose
-                // inclusive count exceeds k (every lane takes part in the shuffles)
-                for (olc_u32 k0 = 0; k0 < C; k0 += 32u) {
-                    const olc_u32 k = k0 + (olc_u32)lane;
-                    int m = 0;
-#pragma unroll
-                    for (int step = 16; step >= 1; step >>= 1) {
-                        const int probe = m + step - 1;
-                        const olc_u32 v = __shfl_sync(0xffffffffu, incl, probe < 27 ? probe : 26);
-                        if (probe < 27 && v <= k) m += step;
-                    }
-                    const olc_u32 first = __shfl_sync(0xffffffffu, rg.x, m);
-                    const olc_u32 before = __shfl_sync(0xffffffffu, incl - cnt, m);
-                    if (k < C) {
-                        const olc_u32 j = first + (k - before);
-                        S.rec[k] = __ldg(posr + j);
-                        S.row[k] = j;
-                    }
-                }
-            }
-            __syncwarp();
-            // home agents: on the warp path while they are alive and still in B
-            for (int a = lane; a < nB && a < CW_HOME; a += 32) {
-                const float4 p = warp_path ? S.rec[home0 + a] : __ldg(posr + s0 + a);
-                unsigned char fl = 0;
-                if (p.w < 0.0f) {
-                    fl = 2;
-                } else if (!warp_path || olc_bin_coord(p.x, c.tvs, c.tdims[0]) != bx ||
-                           olc_bin_coord(p.y, c.tvs, c.tdims[1]) != by ||
-                           olc_bin_coord(p.z, c.tvs, c.tdims[2]) != bz) {
-                    fl = 1;
-                }
-                S.flag[a] = fl;
-            }
-            __syncwarp();
-            if (warp_path) {
-                float f0x = 0.0f, f0y = 0.0f, f0z = 0.0f, f1x = 0.0f, f1y = 0.0f, f1z = 0.0f;
-                const olc_u32 T = (olc_u32)nB * C;
-                // this lane's first pair (agent a, candidate k)
-                olc_u32 a = (olc_u32)lane / C, k = (olc_u32)lane - a * C;
-                olc_u32 qn = 0;
-                for (olc_u32 t0 = 0; t0 < T; t0 += 32u) {
-                    bool hit = false;
-                    if (t0 + (olc_u32)lane < T && S.flag[a] == 0)
-                        hit = contact_test(S.rec[home0 + a], S.rec[k], s0 + a, S.row[k]);
-                    const olc_u32 mask = __ballot_sync(0xffffffffu, hit);
-                    if (hit) S.qpair[qn + __popc(mask & lt_mask)] = (a << 16) | k;
-                    qn += (olc_u32)__popc(mask);
-                    // the next chunk's pair of this lane
-                    k += 32u;
-                    while (k >= C) {
-                        k -= C;
-                        ++a;
-                    }
-                    // flush the queue before it can overflow, and after the last chunk
-                    if (qn + 32u > (olc_u32)CW_QCAP || t0 + 32u >= T) {
-                        __syncwarp();
-                        for (olc_u32 e = (olc_u32)lane; e < qn; e += 32u) {
-                            const olc_u32 pr = S.qpair[e];
-                            const olc_u32 ea = pr >> 16, ek = pr & 0xffffu;
-                            float cx = 0.0f, cy = 0.0f, cz = 0.0f;
-                            contact_pair(S.rec[home0 + ea], S.rec[ek], s0 + ea, S.row[ek], c, cx, cy, cz);
-                            S.qf[0][e] = cx;
-                            S.qf[1][e] = cy;
-                            S.qf[2][e] = cz;
-                        }
-                        __syncwarp();
-                        // lane a sums the entries of agents a and a + 32, in queue order
-                        for (olc_u32 e = 0; e < qn; ++e) {
-                            const olc_u32 ea = S.qpair[e] >> 16;
-                            if (ea == (olc_u32)lane) {
-                                f0x = __fadd_rn(f0x, S.qf[0][e]);
-                                f0y = __fadd_rn(f0y, S.qf[1][e]);
-                                f0z = __fadd_rn(f0z, S.qf[2][e]);
-                            } else if (ea == (olc_u32)lane + 32u) {
-                                f1x = __fadd_rn(f1x, S.qf[0][e]);
-                                f1y = __fadd_rn(f1y, S.qf[1][e]);
-                                f1z = __fadd_rn(f1z, S.qf[2][e]);
-                            }
-                        }
-                        __syncwarp();
-                        qn = 0;
-                    }
-                }
-                if (lane < nB && S.flag[lane] == 0)
-                    contact_move(S.rec[home0 + lane], s0 + lane, f0x, f0y, f0z, c, md, xo, yo, zo);
-                if (lane + 32 < nB && S.flag[lane + 32] == 0)
-                    contact_move(S.rec[home0 + lane + 32], s0 + lane + 32, f1x, f1y, f1z, c, md, xo, yo, zo);
-            }
-            // the global walk for the rest
-            for (int a = lane; a < nB; a += 32) {
-                if (a < CW_HOME && S.flag[a] != 1) continue;
-                const float4 p = __ldg(posr + s0 + a);
-                if (p.w < 0.0f) continue;
-                float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-                contact_walk_global(posr, ranges, p, s0 + a, c, fx, fy, fz);
-                contact_move(p, s0 + a, fx, fy, fz, c, md, xo, yo, zo);
-            }
-            __syncwarp();  // the next bin reuses the warp's shared memory
-        }
-    }
 }
 
 // ---------------------------------------------------------------- bin bricks
@@ -713,21 +524,6 @@ __global__ void __launch_bounds__(CB_THREADS) k_contact_brick(const float4* __re
 void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
                     olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s, int variant,
                     olc_u32 n_table) {
-    if (variant == OLC_CONTACT_WARP) {
-        // rows come from the bin table (the sorted rows are the ranges of the
-        // keys of in-grid bins; Morton keys grow with every coordinate, so the
-        // far corner's key is the largest), so the live count is not needed
-        // here; 32 keys per warp and round
-        (void)n_table;
-        const olc_u32 n_keys = olc_tissue_key(c.tdims[0] - 1, c.tdims[1] - 1, c.tdims[2] - 1) + 1u;
-        const olc_u32 rounds = (n_keys + 31u) / 32u;
-        olc_u32 blocks = (rounds + CW_WARPS - 1) / CW_WARPS;
-        if (blocks > 148u * 12u) blocks = 148u * 12u;
-        if (blocks == 0) blocks = 1;
-        k_contact_warp<<<blocks, 32 * CW_WARPS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_keys, c, x,
-                                                         y, z);
-        return;
-    }
     if (variant == OLC_CONTACT_BRICK) {
         // rows come from the bin table; 64 keys per brick up to the far corner's key
         const olc_u32 n_keys = olc_tissue_key(c.tdims[0] - 1, c.tdims[1] - 1, c.tdims[2] - 1) + 1u;

@@ -185,6 +185,7 @@ class TumourSpec:
     capacity: int = 0
     tissue_dims: tuple = field(default=())
     storage: str = "f32"      # field storage: "f32", "bf16" or "f16"
+    encoding: str = "auto"    # 16-bit element encoding (Engine.setup_diffusion)
 
     def __post_init__(self) -> None:
         if not self.tissue_dims:
@@ -224,13 +225,15 @@ CONFIGS = {s.name: s for s in (PLAIN_SMALL, SCALE)}
 
 
 def batched_specs(n_sims: int = 512, seed: int = 0, g_choices: tuple = (32, 48, 64, 96, 128),
-                  n_range: tuple = (1e3, 2e5), density: float = 3.73e-3) -> list:
+                  n_range: tuple = (1e3, 2e5), density: float = 3.73e-3, steps: int = 0) -> list:
     """Members of a parameter sweep (the batched configuration): per member a
     grid G from ``g_choices`` (domain G * 4 um, dx = 4 um, 10 um bins), an agent
     count log-uniform in ``n_range`` capped so the ball of radius 0.4 * domain is
     no denser than the scale workload (``density`` agents per um^3), D_O2 ~
     U(1000, 3000), uptake ~ U(0.01, 0.04), drug decay ~ U(0.05, 0.2), and seed
-    ``seed + k``.  Drawn from numpy default_rng(seed)."""
+    ``seed + k``.  Drawn from numpy default_rng(seed).  Agent capacity: twice
+    the start, or for a run of ``steps`` steps the serving mix's rule (the
+    population doubling every 300 steps, 50 % headroom)."""
     rng = np.random.default_rng(seed)
     out = []
     for k in range(n_sims):
@@ -243,7 +246,8 @@ def batched_specs(n_sims: int = 512, seed: int = 0, g_choices: tuple = (32, 48, 
         out.append(TumourSpec(name=f"sweep_{k}", n_agents=n, domain=domain, ball_radius=ball, field_dims=(g, g, g),
                               r_lo=4.0, r_hi=6.0, has_drug=True, D_o2=float(rng.uniform(1000.0, 3000.0)),
                               uptake=float(rng.uniform(0.01, 0.04)), decay_drug=float(rng.uniform(0.05, 0.2)),
-                              death_k=0.02, seed=seed + k, capacity=2 * n + 1024))
+                              death_k=0.02, seed=seed + k,
+                              capacity=(int(1.5 * n * 2.0 ** (steps / 300.0)) + 8192) if steps else 2 * n + 1024))
     return out
 
 
@@ -344,11 +348,12 @@ def configure_engine(spec: TumourSpec, state: dict | None = None) -> tuple[Engin
     chem_cls = O2DrugChem if spec.has_drug else O2Chem
     eng.setup_chemistry(chem_cls, shape=tuple(spec.field_dims), voxel_size=spec.dx)
     eng.chemistry.column("o2")[...] = spec.init_o2
-    eng.setup_diffusion("o2", diffusion=spec.D_o2, boundary=spec.bnd_o2, substeps=spec.S_o2, storage=spec.storage)
+    eng.setup_diffusion("o2", diffusion=spec.D_o2, boundary=spec.bnd_o2, substeps=spec.S_o2, storage=spec.storage,
+                        encoding=spec.encoding)
     if spec.has_drug:
         eng.chemistry.column("drug")[...] = spec.init_drug
         eng.setup_diffusion("drug", diffusion=spec.D_drug, decay=spec.decay_drug, boundary=spec.bnd_drug,
-                            substeps=spec.S_drug, storage=spec.storage)
+                            substeps=spec.S_drug, storage=spec.storage, encoding=spec.encoding)
     eng.setup_contact(radius="radius", stiffness=spec.stiffness, mobility=spec.mobility, max_disp=spec.max_disp,
                       margin=spec.margin)
     eng.cells.add_arrays(TumourCell, **{"pos.x": state["x"], "pos.y": state["y"], "pos.z": state["z"],

@@ -333,17 +333,15 @@ def test_contact_bit_exact(cuda, olc):
     assert moved.sum() > n // 2
 
 
-@pytest.mark.parametrize("variant", [_lib.OLC_CONTACT_FLAT, _lib.OLC_CONTACT_NESTED, _lib.OLC_CONTACT_WARP,
-                                     _lib.OLC_CONTACT_BRICK])
+@pytest.mark.parametrize("variant", [_lib.OLC_CONTACT_FLAT, _lib.OLC_CONTACT_NESTED, _lib.OLC_CONTACT_BRICK])
 @pytest.mark.parametrize("case", ["sparse", "dense", "moved", "cluster"])
 def test_contact_walks_bit_exact(cuda, olc, variant, case):
     """Every contact walk (olc_stage_contact_tuned) against orc_contact:
-    a sparse population; a dense one (bins of more agents than a warp holds
-    and neighbourhoods larger than its staging buffer, which take the global
-    walk); agents moved after the sort (a rule's displacement), whose current
+    a sparse population; a dense one (bricks whose halo holds more records
+    than the staging buffer, which take the global walk); agents moved after the sort (a rule's displacement), whose current
     bin differs from the one they are sorted in; and a cluster of 50 agents
-    in one bin of a sparse neighbourhood (two agents per lane on the warp
-    walk).  Coincident points and dead rows in each."""
+    in one bin of a sparse neighbourhood.  Coincident points and dead rows in
+    each."""
     rng = np.random.default_rng(31)
     dims, vs = (20, 20, 20), 10.0
     n, sd = {"sparse": (30000, 25.0), "dense": (40000, 16.0), "moved": (30000, 20.0), "cluster": (8000, 40.0)}[case]
@@ -373,7 +371,7 @@ def test_contact_walks_bit_exact(cuda, olc, variant, case):
     np.testing.assert_array_equal(got, ref)
     counts = ranges[1::2] - ranges[0::2]
     if case == "dense":
-        assert counts.max() > 64  # some bins take the global walk whole
+        assert counts.max() > 64  # dense bins: their bricks' halos overflow the staging buffer
     if case == "cluster":
         assert 32 < counts.max() <= 64
 
