@@ -141,6 +141,9 @@ __global__ void __launch_bounds__(256) k_contact_batch(const float4* __restrict_
         const int cy = olc_bin_coord(p.y, d.tvs, d.tdims[1]);
         const int cz = olc_bin_coord(p.z, d.tvs, d.tdims[2]);
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+        const olc_u32 kx[3] = {olc_tissue_axis(cx - 1, 0), olc_tissue_axis(cx, 0), olc_tissue_axis(cx + 1, 0)};
+        const olc_u32 ky[3] = {olc_tissue_axis(cy - 1, 1), olc_tissue_axis(cy, 1), olc_tissue_axis(cy + 1, 1)};
+        const olc_u32 kz[3] = {olc_tissue_axis(cz - 1, 2), olc_tissue_axis(cz, 2), olc_tissue_axis(cz + 1, 2)};
         for (int dz = -1; dz <= 1; ++dz) {
             const int nz = cz + dz;
             if (nz < 0 || nz >= d.tdims[2]) continue;
@@ -150,7 +153,7 @@ __global__ void __launch_bounds__(256) k_contact_batch(const float4* __restrict_
                 for (int dx = -1; dx <= 1; ++dx) {
                     const int nx = cx + dx;
                     if (nx < 0 || nx >= d.tdims[0]) continue;
-                    const uint2 rg = __ldg(rg0 + olc_tissue_key(nx, ny, nz));
+                    const uint2 rg = __ldg(rg0 + (kx[dx + 1] | ky[dy + 1] | kz[dz + 1]));
                     for (olc_u32 j = rg.x; j < rg.y; ++j) {
                         if (j == i) continue;
                         const float4 q = __ldg(posr + j);

@@ -32,6 +32,9 @@ __global__ void __launch_bounds__(256) k_contact(const float4* __restrict__ posr
         const int cy = olc_bin_coord(p.y, c.tvs, c.tdims[1]);
         const int cz = olc_bin_coord(p.z, c.tvs, c.tdims[2]);
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+        const olc_u32 kx[3] = {olc_tissue_axis(cx - 1, 0), olc_tissue_axis(cx, 0), olc_tissue_axis(cx + 1, 0)};
+        const olc_u32 ky[3] = {olc_tissue_axis(cy - 1, 1), olc_tissue_axis(cy, 1), olc_tissue_axis(cy + 1, 1)};
+        const olc_u32 kz[3] = {olc_tissue_axis(cz - 1, 2), olc_tissue_axis(cz, 2), olc_tissue_axis(cz + 1, 2)};
         for (int dz = -1; dz <= 1; ++dz) {
             const int nz = cz + dz;
             if (nz < 0 || nz >= c.tdims[2]) continue;
@@ -41,7 +44,7 @@ __global__ void __launch_bounds__(256) k_contact(const float4* __restrict__ posr
                 for (int dx = -1; dx <= 1; ++dx) {
                     const int nx = cx + dx;
                     if (nx < 0 || nx >= c.tdims[0]) continue;
-                    const uint2 rg = __ldg(ranges + olc_tissue_key(nx, ny, nz));
+                    const uint2 rg = __ldg(ranges + (kx[dx + 1] | ky[dy + 1] | kz[dz + 1]));
                     for (olc_u32 j = rg.x; j < rg.y; ++j) {
                         if (j == i) continue;
                         const float4 q = __ldg(posr + j);
@@ -132,6 +135,9 @@ __global__ void __launch_bounds__(256) k_contact_mech(const float4* __restrict__
         const int cy = olc_bin_coord(p.y, c.tvs, c.tdims[1]);
         const int cz = olc_bin_coord(p.z, c.tvs, c.tdims[2]);
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+        const olc_u32 kx[3] = {olc_tissue_axis(cx - 1, 0), olc_tissue_axis(cx, 0), olc_tissue_axis(cx + 1, 0)};
+        const olc_u32 ky[3] = {olc_tissue_axis(cy - 1, 1), olc_tissue_axis(cy, 1), olc_tissue_axis(cy + 1, 1)};
+        const olc_u32 kz[3] = {olc_tissue_axis(cz - 1, 2), olc_tissue_axis(cz, 2), olc_tissue_axis(cz + 1, 2)};
         for (int dz = -1; dz <= 1; ++dz) {
             const int nz = cz + dz;
             if (nz < 0 || nz >= c.tdims[2]) continue;
@@ -141,7 +147,7 @@ __global__ void __launch_bounds__(256) k_contact_mech(const float4* __restrict__
                 for (int dx = -1; dx <= 1; ++dx) {
                     const int nx = cx + dx;
                     if (nx < 0 || nx >= c.tdims[0]) continue;
-                    const uint2 rg = __ldg(ranges + olc_tissue_key(nx, ny, nz));
+                    const uint2 rg = __ldg(ranges + (kx[dx + 1] | ky[dy + 1] | kz[dz + 1]));
                     for (olc_u32 j = rg.x; j < rg.y; ++j) {
                         if (j == i) continue;
                         const float4 q = __ldg(posr + j);
@@ -308,6 +314,14 @@ __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __res
         const int cx = olc_bin_coord(p.x, c.tvs, c.tdims[0]);
         const int cy = olc_bin_coord(p.y, c.tvs, c.tdims[1]);
         const int cz = olc_bin_coord(p.z, c.tvs, c.tdims[2]);
+        // per-axis key terms of the neighbour coordinates (olc_tissue_axis)
+        olc_u32 kx[3], ky[3], kz[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            kx[d] = olc_tissue_axis(cx + d - 1, 0);
+            ky[d] = olc_tissue_axis(cy + d - 1, 1);
+            kz[d] = olc_tissue_axis(cz + d - 1, 2);
+        }
         int nb = 0;
         for (int dz = -1; dz <= 1; ++dz) {
             const int nz = cz + dz;
@@ -318,7 +332,7 @@ __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __res
                 for (int dx = -1; dx <= 1; ++dx) {
                     const int nx = cx + dx;
                     if (nx < 0 || nx >= c.tdims[0]) continue;
-                    const uint2 rg = __ldg(ranges + olc_tissue_key(nx, ny, nz));
+                    const uint2 rg = __ldg(ranges + (kx[dx + 1] | ky[dy + 1] | kz[dz + 1]));
                     if (rg.y > rg.x) s_bins[nb++][t] = rg;
                 }
             }
@@ -382,6 +396,9 @@ __device__ __forceinline__ void contact_walk_global(const float4* __restrict__ p
     const int cx = olc_bin_coord(p.x, c.tvs, c.tdims[0]);
     const int cy = olc_bin_coord(p.y, c.tvs, c.tdims[1]);
     const int cz = olc_bin_coord(p.z, c.tvs, c.tdims[2]);
+    const olc_u32 kx[3] = {olc_tissue_axis(cx - 1, 0), olc_tissue_axis(cx, 0), olc_tissue_axis(cx + 1, 0)};
+    const olc_u32 ky[3] = {olc_tissue_axis(cy - 1, 1), olc_tissue_axis(cy, 1), olc_tissue_axis(cy + 1, 1)};
+    const olc_u32 kz[3] = {olc_tissue_axis(cz - 1, 2), olc_tissue_axis(cz, 2), olc_tissue_axis(cz + 1, 2)};
     for (int dz = -1; dz <= 1; ++dz) {
         const int nz = cz + dz;
         if (nz < 0 || nz >= c.tdims[2]) continue;
@@ -391,7 +408,7 @@ __device__ __forceinline__ void contact_walk_global(const float4* __restrict__ p
             for (int dx = -1; dx <= 1; ++dx) {
                 const int nx = cx + dx;
                 if (nx < 0 || nx >= c.tdims[0]) continue;
-                const uint2 rg = __ldg(ranges + olc_tissue_key(nx, ny, nz));
+                const uint2 rg = __ldg(ranges + (kx[dx + 1] | ky[dy + 1] | kz[dz + 1]));
                 for (olc_u32 j = rg.x; j < rg.y; ++j) contact_pair(p, __ldg(posr + j), i, j, c, fx, fy, fz);
             }
         }

@@ -92,6 +92,14 @@ __device__ __host__ __forceinline__ olc_u32 olc_tissue_key(int cx, int cy, int c
     return (j << 3) | i;
 }
 
+// The tissue key splits into one term per axis, OR-ed:
+//   olc_tissue_key(x, y, z) = olc_tissue_axis(x, 0) | olc_tissue_axis(y, 1) | olc_tissue_axis(z, 2)
+// (the coarse coordinate's interleaved bits above the three parity bits), so
+// a walk over the 27 Moore bins needs 9 interleaves instead of 81.
+__device__ __host__ __forceinline__ olc_u32 olc_tissue_axis(int c, int axis) {
+    return (olc_interleave9((olc_u32)(c >> 1)) << (3 + axis)) | ((olc_u32)(c & 1) << axis);
+}
+
 // Bin coordinate of one position component: trunc(p / vs) with an IEEE
 // (correctly rounded) divide, clamped to [0, dim-1].  NaN maps to 0.
 __device__ __forceinline__ int olc_bin_coord(float p, float vs, int dim) {
