@@ -379,158 +379,116 @@ __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __res
     }
 }
 
-// ---------------------------------------------------------------- shared helpers
-__device__ __forceinline__ olc_u32 olc_compact9(olc_u32 x) {
-    x &= 0x09249249u;
-    x = (x | (x >> 2)) & 0x030c30c3u;
-    x = (x | (x >> 4)) & 0x0300f00fu;
-    x = (x | (x >> 8)) & 0x030000ffu;
-    x = (x | (x >> 16)) & 0x000001ffu;
-    return x;
-}
-
-// k_contact's walk for agent i at p (global memory), summed into f.
-__device__ __forceinline__ void contact_walk_global(const float4* __restrict__ posr, const uint2* __restrict__ ranges,
-                                                    const float4& p, olc_u32 i, const ContactDev& c, float& fx,
-                                                    float& fy, float& fz) {
-    const int cx = olc_bin_coord(p.x, c.tvs, c.tdims[0]);
-    const int cy = olc_bin_coord(p.y, c.tvs, c.tdims[1]);
-    const int cz = olc_bin_coord(p.z, c.tvs, c.tdims[2]);
-    const olc_u32 kx[3] = {olc_tissue_axis(cx - 1, 0), olc_tissue_axis(cx, 0), olc_tissue_axis(cx + 1, 0)};
-    const olc_u32 ky[3] = {olc_tissue_axis(cy - 1, 1), olc_tissue_axis(cy, 1), olc_tissue_axis(cy + 1, 1)};
-    const olc_u32 kz[3] = {olc_tissue_axis(cz - 1, 2), olc_tissue_axis(cz, 2), olc_tissue_axis(cz + 1, 2)};
-    for (int dz = -1; dz <= 1; ++dz) {
-        const int nz = cz + dz;
-        if (nz < 0 || nz >= c.tdims[2]) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
-            const int ny = cy + dy;
-            if (ny < 0 || ny >= c.tdims[1]) continue;
-            for (int dx = -1; dx <= 1; ++dx) {
-                const int nx = cx + dx;
-                if (nx < 0 || nx >= c.tdims[0]) continue;
-                const uint2 rg = __ldg(ranges + (kx[dx + 1] | ky[dy + 1] | kz[dz + 1]));
-                for (olc_u32 j = rg.x; j < rg.y; ++j) contact_pair(p, __ldg(posr + j), i, j, c, fx, fy, fz);
-            }
-        }
-    }
-}
-
-// The overdamped move of agent i from its force sum (k_contact's epilogue).
-__device__ __forceinline__ void contact_move(const float4& p, olc_u32 i, float fx, float fy, float fz,
-                                             const ContactDev& c, float md, float* __restrict__ xo,
-                                             float* __restrict__ yo, float* __restrict__ zo) {
-    float mx = __fmul_rn(fx, md), my = __fmul_rn(fy, md), mz = __fmul_rn(fz, md);
-    const float len = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz)));
-    if (len > c.max_disp) {
-        const float sc = __fdiv_rn(c.max_disp, len);
-        mx = __fmul_rn(mx, sc);
-        my = __fmul_rn(my, sc);
-        mz = __fmul_rn(mz, sc);
-    }
-    xo[i] = fminf(fmaxf(__fadd_rn(p.x, mx), c.lo[0]), c.hi[0]);
-    yo[i] = fminf(fmaxf(__fadd_rn(p.y, my), c.lo[1]), c.hi[1]);
-    zo[i] = fminf(fmaxf(__fadd_rn(p.z, mz), c.lo[2]), c.hi[2]);
-}
-
-// ---------------------------------------------------------------- bin bricks
-// k_contact_brick: one CTA per 4 x 4 x 4 brick of bins.  Its 64 bins are 64
-// consecutive keys (two Morton levels below the coarse grid's parity bits),
-// so its agents are one contiguous run of sorted rows.  The CTA stages the
-// records of the 6 x 6 x 6 bins around the brick (every home bin's Moore
-// neighbourhood) in shared memory once, then each thread walks one agent's
-// 27 bins there in k_contact's order with its pair law, so the sums are the
-// same bits.  Agents whose current position left the brick since the sort,
-// and every agent of a brick whose halo holds more records than the staging
-// buffer, take the global walk.
-constexpr int CB_THREADS = 256;
-constexpr int CB_HALO = 216;    // 6 x 6 x 6 bins
-constexpr int CB_CAP = 1536;    // staged records per brick
-
-__global__ void __launch_bounds__(CB_THREADS) k_contact_brick(const float4* __restrict__ posr,
-                                                             const uint2* __restrict__ ranges, olc_u32 n_keys,
-                                                             ContactDev c, float* __restrict__ xo,
-                                                             float* __restrict__ yo, float* __restrict__ zo) {
-    __shared__ float4 s_rec[CB_CAP];
-    __shared__ olc_u32 s_off[CB_HALO + 1];  // first staged record of halo bin h; s_off[216] = total
-    __shared__ olc_u32 s_row[CB_HALO];      // first row of halo bin h
-    __shared__ olc_u32 s_warp[CB_THREADS / 32];
-    __shared__ olc_u32 s_home[2];           // the brick's rows [begin, end)
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+// k_contact_near: the flat walk in two passes.  Pass 1 runs only the cheap
+// part of contact_pair's test on every candidate (not self, alive, d^2 within
+// (r_i + r_j)^2 (1 + 2^-20)) and queues the survivors' rows in shared memory,
+// in walk order; pass 2 runs contact_pair on the queued rows.  Every rejected
+// candidate would have returned early from contact_pair, so the sum sees the
+// same pairs in the same order: the same bits.  The warp no longer waits on
+// the square roots and divide of the few lanes in contact at every candidate;
+// it runs them together in the short second loop.  An agent with more near
+// candidates than the queue holds walks its bins again in one pass.
+constexpr int CN_QUEUE = 32;
+__global__ void __launch_bounds__(CF_THREADS) k_contact_near(const float4* __restrict__ posr,
+                                                            const uint2* __restrict__ ranges, const olc_u32* n_dev,
+                                                            olc_u32 n_host, ContactDev c, float* __restrict__ xo,
+                                                            float* __restrict__ yo, float* __restrict__ zo) {
+    __shared__ uint2 s_bins[27][CF_THREADS];
+    __shared__ olc_u32 s_near[CN_QUEUE][CF_THREADS];
+    const olc_u32 n = n_dev ? *n_dev : n_host;
     const float md = __fmul_rn(c.mobility, c.dt);
-    const olc_u32 n_bricks = (n_keys + 63u) / 64u;
-    for (olc_u32 B = blockIdx.x; B < n_bricks; B += gridDim.x) {
-        __syncthreads();  // the previous brick is done with the shared arrays
-        // the brick's rows: its 64 keys' ranges (empty keys hold [0, 0))
-        uint2 hr = make_uint2(0xffffffffu, 0u);
-        if (t < 64 && 64u * B + (olc_u32)t < n_keys) {
-            const uint2 r = __ldg(ranges + 64u * B + (olc_u32)t);
-            if (r.y > r.x) hr = r;
-        }
-        olc_u32 lo = hr.x, hi = hr.y;
+    const int t = threadIdx.x;
+    for (olc_u32 base = blockIdx.x * CF_THREADS; base < n; base += gridDim.x * CF_THREADS) {
+        const olc_u32 i = base + t;
+        if (i >= n) continue;
+        const float4 p = posr[i];
+        if (p.w < 0.0f) continue;  // dead this step: no move, no force
+        const int cx = olc_bin_coord(p.x, c.tvs, c.tdims[0]);
+        const int cy = olc_bin_coord(p.y, c.tvs, c.tdims[1]);
+        const int cz = olc_bin_coord(p.z, c.tvs, c.tdims[2]);
+        olc_u32 kx[3], ky[3], kz[3];
 #pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) {
-            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        for (int d = 0; d < 3; ++d) {
+            kx[d] = olc_tissue_axis(cx + d - 1, 0);
+            ky[d] = olc_tissue_axis(cy + d - 1, 1);
+            kz[d] = olc_tissue_axis(cz + d - 1, 2);
         }
-        if (t == 0) s_home[0] = lo, s_home[1] = hi;
-        __syncthreads();
-        if (t == 32) s_home[0] = min(s_home[0], lo), s_home[1] = max(s_home[1], hi);
-        __syncthreads();
-        const olc_u32 h0 = s_home[0], h1 = s_home[1];
-        if (h0 >= h1) continue;  // uniform: every thread read the same words
-        // brick origin in bins: key 64B + q is coarse key 8B + (q >> 3), parity q & 7
-        const int ox = 4 * (int)olc_compact9(B), oy = 4 * (int)olc_compact9(B >> 1), oz = 4 * (int)olc_compact9(B >> 2);
-        // halo bin t at brick-local (t % 6, (t / 6) % 6, t / 36) - 1
-        uint2 rg = make_uint2(0u, 0u);
-        if (t < CB_HALO) {
-            const int gx = ox - 1 + t % 6, gy = oy - 1 + (t / 6) % 6, gz = oz - 1 + t / 36;
-            if (gx >= 0 && gy >= 0 && gz >= 0 && gx < c.tdims[0] && gy < c.tdims[1] && gz < c.tdims[2])
-                rg = __ldg(ranges + olc_tissue_key(gx, gy, gz));
-        }
-        const olc_u32 cnt = rg.y - rg.x;
-        olc_u32 incl = cnt;  // inclusive scan over the 256 threads
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const olc_u32 v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
-        }
-        if (lane == 31) s_warp[warp] = incl;
-        __syncthreads();
-        olc_u32 before = 0;
-        for (int w = 0; w < warp; ++w) before += s_warp[w];
-        incl += before;
-        if (t < CB_HALO) {
-            s_off[t] = incl - cnt;
-            s_row[t] = rg.x;
-        }
-        if (t == CB_HALO - 1) s_off[CB_HALO] = incl;
-        __syncthreads();
-        const bool staged = s_off[CB_HALO] <= (olc_u32)CB_CAP;
-        if (staged && t < CB_HALO)
-            for (olc_u32 k = 0; k < cnt; ++k) s_rec[incl - cnt + k] = __ldg(posr + rg.x + k);
-        __syncthreads();
-        for (olc_u32 i = h0 + (olc_u32)t; i < h1; i += CB_THREADS) {
-            const float4 p = __ldg(posr + i);
-            if (p.w < 0.0f) continue;  // dead this step: no move, no force
-            const int lx = olc_bin_coord(p.x, c.tvs, c.tdims[0]) - ox + 1;
-            const int ly = olc_bin_coord(p.y, c.tvs, c.tdims[1]) - oy + 1;
-            const int lz = olc_bin_coord(p.z, c.tvs, c.tdims[2]) - oz + 1;
-            float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-            if (staged && lx >= 1 && lx <= 4 && ly >= 1 && ly <= 4 && lz >= 1 && lz <= 4) {
-                for (int dz = -1; dz <= 1; ++dz)
-                    for (int dy = -1; dy <= 1; ++dy)
-                        for (int dx = -1; dx <= 1; ++dx) {
-                            // bins outside the grid are empty here, as k_contact skips them
-                            const int h = (lz + dz) * 36 + (ly + dy) * 6 + (lx + dx);
-                            const olc_u32 k0 = s_off[h], k1 = s_off[h + 1], row0 = s_row[h];
-                            for (olc_u32 k = k0; k < k1; ++k)
-                                contact_pair(p, s_rec[k], i, row0 + (k - k0), c, fx, fy, fz);
-                        }
-            } else {
-                contact_walk_global(posr, ranges, p, i, c, fx, fy, fz);
+        int nb = 0;
+        for (int dz = -1; dz <= 1; ++dz) {
+            const int nz = cz + dz;
+            if (nz < 0 || nz >= c.tdims[2]) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int ny = cy + dy;
+                if (ny < 0 || ny >= c.tdims[1]) continue;
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int nx = cx + dx;
+                    if (nx < 0 || nx >= c.tdims[0]) continue;
+                    const uint2 rg = __ldg(ranges + (kx[dx + 1] | ky[dy + 1] | kz[dz + 1]));
+                    if (rg.y > rg.x) s_bins[nb++][t] = rg;
+                }
             }
-            contact_move(p, i, fx, fy, fz, c, md, xo, yo, zo);
         }
+        // pass 1: the next candidate's record is requested before this one is tested
+        int nq = 0, b = 0;
+        olc_u32 j = 0, end = 0;
+        float4 q = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+        if (nb > 0) {
+            const uint2 r = s_bins[0][t];
+            j = r.x;
+            end = r.y;
+            q = __ldg(posr + j);
+        }
+        while (b < nb) {
+            olc_u32 jn = j + 1, en = end;
+            int bn = b;
+            if (jn == en) {
+                if (++bn < nb) {
+                    const uint2 r = s_bins[bn][t];
+                    jn = r.x;
+                    en = r.y;
+                }
+            }
+            const float4 qn = bn < nb ? __ldg(posr + jn) : q;
+            if (j != i && q.w >= 0.0f) {
+                const float ddx = __fsub_rn(p.x, q.x);
+                const float ddy = __fsub_rn(p.y, q.y);
+                const float ddz = __fsub_rn(p.z, q.z);
+                const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), __fmul_rn(ddz, ddz));
+                const float rsum = __fadd_rn(p.w, q.w);
+                if (!(d2 > __fmul_rn(__fmul_rn(rsum, rsum), 1.00000095367431640625f))) {
+                    if (nq < CN_QUEUE) s_near[nq][t] = j;
+                    ++nq;
+                }
+            }
+            j = jn;
+            end = en;
+            b = bn;
+            q = qn;
+        }
+        // pass 2: contact_pair on the queued rows, in walk order
+        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+        if (nq <= CN_QUEUE) {
+            for (int k = 0; k < nq; ++k) {
+                const olc_u32 jj = s_near[k][t];
+                contact_pair(p, __ldg(posr + jj), i, jj, c, fx, fy, fz);
+            }
+        } else {
+            for (int bb = 0; bb < nb; ++bb) {
+                const uint2 r = s_bins[bb][t];
+                for (olc_u32 jj = r.x; jj < r.y; ++jj) contact_pair(p, __ldg(posr + jj), i, jj, c, fx, fy, fz);
+            }
+        }
+        float mx = __fmul_rn(fx, md), my = __fmul_rn(fy, md), mz = __fmul_rn(fz, md);
+        const float len = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz)));
+        if (len > c.max_disp) {
+            const float sc = __fdiv_rn(c.max_disp, len);
+            mx = __fmul_rn(mx, sc);
+            my = __fmul_rn(my, sc);
+            mz = __fmul_rn(mz, sc);
+        }
+        xo[i] = fminf(fmaxf(__fadd_rn(p.x, mx), c.lo[0]), c.hi[0]);
+        yo[i] = fminf(fmaxf(__fadd_rn(p.y, my), c.lo[1]), c.hi[1]);
+        zo[i] = fminf(fmaxf(__fadd_rn(p.z, mz), c.lo[2]), c.hi[2]);
     }
 }
 
@@ -541,14 +499,12 @@ __global__ void __launch_bounds__(CB_THREADS) k_contact_brick(const float4* __re
 void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
                     olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s, int variant,
                     olc_u32 n_table) {
-    if (variant == OLC_CONTACT_BRICK) {
-        // rows come from the bin table; 64 keys per brick up to the far corner's key
-        const olc_u32 n_keys = olc_tissue_key(c.tdims[0] - 1, c.tdims[1] - 1, c.tdims[2] - 1) + 1u;
-        const olc_u32 n_bricks = (n_keys + 63u) / 64u;
-        olc_u32 blocks = n_bricks < 148u * 6u ? n_bricks : 148u * 6u;
+    if (variant == OLC_CONTACT_NEAR) {
+        olc_u32 blocks = (n_cap + CF_THREADS - 1) / CF_THREADS;
         if (blocks == 0) blocks = 1;
-        k_contact_brick<<<blocks, CB_THREADS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_keys, c, x, y,
-                                                      z);
+        if (blocks > 148 * 16) blocks = 148 * 16;
+        k_contact_near<<<blocks, CF_THREADS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_dev, n_host, c,
+                                                      x, y, z);
         return;
     }
     if (variant != OLC_CONTACT_NESTED) {
