@@ -68,7 +68,7 @@ def parse() -> argparse.Namespace:
                     help="steps of the field-error measurement added to the default line")
     ap.add_argument("--encoding", default="auto", choices=["auto", "value", "deficit", "offset3"],
                     help="16-bit element encoding of --workload batch")
-    ap.add_argument("--contact", default="auto", choices=["auto", "flat", "nested", "near"],
+    ap.add_argument("--contact", default="auto", choices=["auto", "flat", "nested"],
                     help="contact walk of the scale workload (auto: the tuner's choice)")
     ap.add_argument("--grid", type=int, default=256, help="field edge of --workload stencil")
     ap.add_argument("--stencil-pair", default="0,1024,512",
@@ -314,8 +314,7 @@ def run_b200(args) -> None:
     if args.contact != "auto":
         # a fixed contact walk (profiling one variant); the other choices stay tuned
         t = dict(tuning["tuning"] or {"stencil_tile": [8, 8], "batch_tile_depth": 16, "stencil_pair": [0, 0]})
-        t["contact_variant"] = {"flat": _lib.OLC_CONTACT_FLAT, "nested": _lib.OLC_CONTACT_NESTED,
-                                "near": _lib.OLC_CONTACT_NEAR}[args.contact]
+        t["contact_variant"] = {"flat": _lib.OLC_CONTACT_FLAT, "nested": _lib.OLC_CONTACT_NESTED}[args.contact]
         tuning = dict(tuning, tuning=t)
         autotune.apply_engine(eng, tuning)
     eng.set_graphs(not args.no_graphs)

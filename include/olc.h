@@ -150,12 +150,10 @@ typedef struct {
  * (its dispatches are fixed 256-wide: _gpu_backend.py:134-136). */
 #define OLC_CONTACT_FLAT   0  /* one flat walk over each agent's listed non-empty Moore bins */
 #define OLC_CONTACT_NESTED 1  /* nested loops over the 27 Moore bins                       */
-#define OLC_CONTACT_NEAR   2  /* the flat walk in two passes: near candidates queued in
-                                 shared memory, then the pair law on the queue */
 typedef struct {
     int32_t stencil_tile_y;   /* FP32 TMA substep tile: rows (8 or 16) ...             */
     int32_t stencil_tile_z;   /* ... and planes; (y, z) in {(8,8), (16,8), (8,16), (16,4)} */
-    int32_t contact_variant;  /* OLC_CONTACT_FLAT, OLC_CONTACT_NESTED or OLC_CONTACT_NEAR */
+    int32_t contact_variant;  /* OLC_CONTACT_FLAT or OLC_CONTACT_NESTED */
     int32_t batch_tile_depth; /* planes per tile of the batched FP32 substep: 8, 16 or
                                  32 (members without their own, olc_set_batch_tile_depths) */
     int32_t stencil_pair_threads; /* two FP32 substeps per pass (temporal blocking) with

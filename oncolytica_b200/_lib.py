@@ -181,7 +181,6 @@ class OlcDiffusion(C.Structure):
 
 OLC_CONTACT_FLAT = 0
 OLC_CONTACT_NESTED = 1
-OLC_CONTACT_NEAR = 2
 
 
 class OlcTuning(C.Structure):

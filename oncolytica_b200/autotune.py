@@ -29,8 +29,8 @@ import threading
 from oncolytica_b200 import _lib
 
 STENCIL_TILES = ((8, 8), (16, 8), (8, 16), (16, 4))
-CONTACT_VARIANTS = (_lib.OLC_CONTACT_FLAT, _lib.OLC_CONTACT_NESTED, _lib.OLC_CONTACT_NEAR)
-CONTACT_NAMES = {_lib.OLC_CONTACT_FLAT: "flat", _lib.OLC_CONTACT_NESTED: "nested", _lib.OLC_CONTACT_NEAR: "near"}
+CONTACT_VARIANTS = (_lib.OLC_CONTACT_FLAT, _lib.OLC_CONTACT_NESTED)
+CONTACT_NAMES = {_lib.OLC_CONTACT_FLAT: "flat", _lib.OLC_CONTACT_NESTED: "nested"}
 BATCH_DEPTHS = (8, 16, 32)
 # (threads per CTA, planes per CTA) of the two-substeps-per-pass kernel; (0, 0) = one substep per pass
 STENCIL_PAIRS = ((0, 0), (1024, 0), (512, 0), (256, 0), (128, 0))

@@ -379,119 +379,6 @@ __global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __res
     }
 }
 
-// k_contact_near: the flat walk in two passes.  Pass 1 runs only the cheap
-// part of contact_pair's test on every candidate (not self, alive, d^2 within
-// (r_i + r_j)^2 (1 + 2^-20)) and queues the survivors' rows in shared memory,
-// in walk order; pass 2 runs contact_pair on the queued rows.  Every rejected
-// candidate would have returned early from contact_pair, so the sum sees the
-// same pairs in the same order: the same bits.  The warp no longer waits on
-// the square roots and divide of the few lanes in contact at every candidate;
-// it runs them together in the short second loop.  An agent with more near
-// candidates than the queue holds walks its bins again in one pass.
-constexpr int CN_QUEUE = 32;
-__global__ void __launch_bounds__(CF_THREADS) k_contact_near(const float4* __restrict__ posr,
-                                                            const uint2* __restrict__ ranges, const olc_u32* n_dev,
-                                                            olc_u32 n_host, ContactDev c, float* __restrict__ xo,
-                                                            float* __restrict__ yo, float* __restrict__ zo) {
-    __shared__ uint2 s_bins[27][CF_THREADS];
-    __shared__ olc_u32 s_near[CN_QUEUE][CF_THREADS];
-    const olc_u32 n = n_dev ? *n_dev : n_host;
-    const float md = __fmul_rn(c.mobility, c.dt);
-    const int t = threadIdx.x;
-    for (olc_u32 base = blockIdx.x * CF_THREADS; base < n; base += gridDim.x * CF_THREADS) {
-        const olc_u32 i = base + t;
-        if (i >= n) continue;
-        const float4 p = posr[i];
-        if (p.w < 0.0f) continue;  // dead this step: no move, no force
-        const int cx = olc_bin_coord(p.x, c.tvs, c.tdims[0]);
-        const int cy = olc_bin_coord(p.y, c.tvs, c.tdims[1]);
-        const int cz = olc_bin_coord(p.z, c.tvs, c.tdims[2]);
-        olc_u32 kx[3], ky[3], kz[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            kx[d] = olc_tissue_axis(cx + d - 1, 0);
-            ky[d] = olc_tissue_axis(cy + d - 1, 1);
-            kz[d] = olc_tissue_axis(cz + d - 1, 2);
-        }
-        int nb = 0;
-        for (int dz = -1; dz <= 1; ++dz) {
-            const int nz = cz + dz;
-            if (nz < 0 || nz >= c.tdims[2]) continue;
-            for (int dy = -1; dy <= 1; ++dy) {
-                const int ny = cy + dy;
-                if (ny < 0 || ny >= c.tdims[1]) continue;
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const int nx = cx + dx;
-                    if (nx < 0 || nx >= c.tdims[0]) continue;
-                    const uint2 rg = __ldg(ranges + (kx[dx + 1] | ky[dy + 1] | kz[dz + 1]));
-                    if (rg.y > rg.x) s_bins[nb++][t] = rg;
-                }
-            }
-        }
-        // pass 1: the next candidate's record is requested before this one is tested
-        int nq = 0, b = 0;
-        olc_u32 j = 0, end = 0;
-        float4 q = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
-        if (nb > 0) {
-            const uint2 r = s_bins[0][t];
-            j = r.x;
-            end = r.y;
-            q = __ldg(posr + j);
-        }
-        while (b < nb) {
-            olc_u32 jn = j + 1, en = end;
-            int bn = b;
-            if (jn == en) {
-                if (++bn < nb) {
-                    const uint2 r = s_bins[bn][t];
-                    jn = r.x;
-                    en = r.y;
-                }
-            }
-            const float4 qn = bn < nb ? __ldg(posr + jn) : q;
-            if (j != i && q.w >= 0.0f) {
-                const float ddx = __fsub_rn(p.x, q.x);
-                const float ddy = __fsub_rn(p.y, q.y);
-                const float ddz = __fsub_rn(p.z, q.z);
-                const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)), __fmul_rn(ddz, ddz));
-                const float rsum = __fadd_rn(p.w, q.w);
-                if (!(d2 > __fmul_rn(__fmul_rn(rsum, rsum), 1.00000095367431640625f))) {
-                    if (nq < CN_QUEUE) s_near[nq][t] = j;
-                    ++nq;
-                }
-            }
-            j = jn;
-            end = en;
-            b = bn;
-            q = qn;
-        }
-        // pass 2: contact_pair on the queued rows, in walk order
-        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-        if (nq <= CN_QUEUE) {
-            for (int k = 0; k < nq; ++k) {
-                const olc_u32 jj = s_near[k][t];
-                contact_pair(p, __ldg(posr + jj), i, jj, c, fx, fy, fz);
-            }
-        } else {
-            for (int bb = 0; bb < nb; ++bb) {
-                const uint2 r = s_bins[bb][t];
-                for (olc_u32 jj = r.x; jj < r.y; ++jj) contact_pair(p, __ldg(posr + jj), i, jj, c, fx, fy, fz);
-            }
-        }
-        float mx = __fmul_rn(fx, md), my = __fmul_rn(fy, md), mz = __fmul_rn(fz, md);
-        const float len = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my)), __fmul_rn(mz, mz)));
-        if (len > c.max_disp) {
-            const float sc = __fdiv_rn(c.max_disp, len);
-            mx = __fmul_rn(mx, sc);
-            my = __fmul_rn(my, sc);
-            mz = __fmul_rn(mz, sc);
-        }
-        xo[i] = fminf(fmaxf(__fadd_rn(p.x, mx), c.lo[0]), c.hi[0]);
-        yo[i] = fminf(fmaxf(__fadd_rn(p.y, my), c.lo[1]), c.hi[1]);
-        zo[i] = fminf(fmaxf(__fadd_rn(p.z, mz), c.lo[2]), c.hi[2]);
-    }
-}
-
 // The two walks (olc.h OLC_CONTACT_*): bit-identical, chosen per handle by
 // measurement (OlcTuning.contact_variant).  On the 1 M-agent scale workload
 // the flat walk took 0.92 ms per step over 200 steps against 1.04 for the
@@ -499,14 +386,6 @@ __global__ void __launch_bounds__(CF_THREADS) k_contact_near(const float4* __res
 void launch_contact(const float4* posr, const olc_u32* ranges, const olc_u32* n_dev, olc_u32 n_host,
                     olc_u32 n_cap, const ContactDev& c, float* x, float* y, float* z, cudaStream_t s, int variant,
                     olc_u32 n_table) {
-    if (variant == OLC_CONTACT_NEAR) {
-        olc_u32 blocks = (n_cap + CF_THREADS - 1) / CF_THREADS;
-        if (blocks == 0) blocks = 1;
-        if (blocks > 148 * 16) blocks = 148 * 16;
-        k_contact_near<<<blocks, CF_THREADS, 0, s>>>(posr, reinterpret_cast<const uint2*>(ranges), n_dev, n_host, c,
-                                                      x, y, z);
-        return;
-    }
     if (variant != OLC_CONTACT_NESTED) {
         olc_u32 blocks = (n_cap + CF_THREADS - 1) / CF_THREADS;
         if (blocks == 0) blocks = 1;

@@ -371,38 +371,30 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_substep_pair(const __grid_con
     const float4 b4 = make_float4(bval, bval, bval, bval);
     const size_t sz = (size_t)nx * ny;
     bool ok = wait_plane(0) && wait_plane(1);
-    // registers of the z march: input planes p-1, p, p+1 of the thread's
-    // column and intermediate planes p-2, p-1, p; three steps per loop trip
-    // rotate their roles (and the intermediate buffer), so nothing is copied
-    float4 ra = b4, rb = b4, rc = b4, ma = b4, mb = b4, mc = b4;
+    float4 in_zm = b4, in_c = b4, mid_a = b4, mid_b = b4;
     if (live) {
-        ra = *reinterpret_cast<const float4*>(ring + row_off);
-        rb = *reinterpret_cast<const float4*>(ring + slot_f + row_off);
+        in_zm = *reinterpret_cast<const float4*>(ring + row_off);
+        in_c = *reinterpret_cast<const float4*>(ring + slot_f + row_off);
     }
-    float* const mid_own = mid + mr * nx + 4 * g;
-    const float* const ring_own = ring + row_off;
-    // step p (i = p - z0 + 1): intermediate plane p from input planes p-1 (zm),
-    // p (c) and p+1 (read into zp) into buffer kw; then output plane p-1 from
-    // intermediate planes p-2 (m2), p-1 (m1, its neighbours in buffer kr) and p;
-    // false when a plane never arrived (the CTA leaves)
-    auto step = [&](int p, int i, const float4& zm, const float4& c, float4& zp, const float4& m2, const float4& m1,
-                    float4& v, int kw, int kr) -> bool {
+    for (int p = z0 - 1, i = 0; p <= z_end; ++p, ++i) {
         const int qn = i + 2;  // input plane p + 1
         ok = ok && wait_plane(qn);
-        v = b4;
+        float4 v = b4;
         if (live) {
-            const float* pc = ring_own + ((qn - 1) & (PAIR_RING - 1)) * slot_f;
-            zp = *reinterpret_cast<const float4*>(ring_own + (qn & (PAIR_RING - 1)) * slot_f);
+            const float* pc = ring + ((qn - 1) % PAIR_RING) * slot_f + row_off;
+            const float4 zp = *reinterpret_cast<const float4*>(ring + (qn % PAIR_RING) * slot_f + row_off);
             const float4 ym = *reinterpret_cast<const float4*>(pc - nx);
             const float4 yp = *reinterpret_cast<const float4*>(pc + nx);
-            v = stencil_update4(pc[-1], pc[4], c, ym, yp, zm, zp, r, inv_decay);
+            v = stencil_update4(pc[-1], pc[4], in_c, ym, yp, in_zm, zp, r, inv_decay);
             if (y_face || p <= 0 || p >= nz - 1) {
                 v = b4;
             } else {
                 if (ex0) v.x = bval;
                 if (ex3) v.w = bval;
             }
-            *reinterpret_cast<float4*>(mid_own + kw * mid_f) = v;
+            *reinterpret_cast<float4*>(mid + (i % 3) * mid_f + mr * nx + 4 * g) = v;
+            in_zm = in_c;
+            in_c = zp;
         }
         if (__syncthreads_or(!ok)) {
             // a plane never arrived: let the copies still in flight land, then leave
@@ -410,15 +402,15 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_substep_pair(const __grid_con
                 for (int q = issued > PAIR_RING ? issued - PAIR_RING : 0; q < issued; ++q)
                     for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it)
                         if (olc_mbar_try_wait(bar0 + 8 * (q % PAIR_RING), (olc_u32)((q / PAIR_RING) & 1))) break;
-            return false;
+            return;
         }
         if (threadIdx.x == 0) issue_upto(qn - 1);  // input plane p is read for the last time
         if (p - 1 >= z0 && out_row) {
             const int z = p - 1;
-            const float* mp = mid_own + kr * mid_f;  // intermediate plane p - 1
-            const float4 ym = *reinterpret_cast<const float4*>(mp - nx);
-            const float4 yp = *reinterpret_cast<const float4*>(mp + nx);
-            float4 o = stencil_update4(mp[-1], mp[4], m1, ym, yp, m2, v, r, inv_decay);
+            const float* mb = mid + ((i + 2) % 3) * mid_f + mr * nx + 4 * g;  // intermediate plane p - 1
+            const float4 ym = *reinterpret_cast<const float4*>(mb - nx);
+            const float4 yp = *reinterpret_cast<const float4*>(mb + nx);
+            float4 o = stencil_update4(mb[-1], mb[4], mid_b, ym, yp, mid_a, v, r, inv_decay);
             if (y == 0 || y == ny - 1 || z == 0 || z == nz - 1) {
                 o = b4;
             } else {
@@ -427,16 +419,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_substep_pair(const __grid_con
             }
             *reinterpret_cast<float4*>(out + (size_t)z * sz + (size_t)y * nx + x) = o;
         }
-        return true;
-    };
-    // roles per step of a trip: (zm, c, zp) = (ra, rb, rc), (rb, rc, ra), (rc, ra, rb);
-    // (m2, m1, new) = (ma, mb, mc), (mb, mc, ma), (mc, ma, mb); buffers 0, 1, 2
-    for (int p = z0 - 1, i = 0; p <= z_end; p += 3, i += 3) {
-        if (!step(p, i, ra, rb, rc, ma, mb, mc, 0, 2)) return;
-        if (p + 1 > z_end) break;
-        if (!step(p + 1, i + 1, rb, rc, ra, mb, mc, ma, 1, 0)) return;
-        if (p + 2 > z_end) break;
-        if (!step(p + 2, i + 2, rc, ra, rb, mc, ma, mb, 2, 1)) return;
+        mid_a = mid_b;
+        mid_b = v;
     }
 }
 

@@ -2481,7 +2481,7 @@ static int stage_contact(const float* posr, const uint32_t* ranges, uint32_t n, 
                          const char* who) {
     if (!geom || !spec || (n && (!posr || !ranges || !x || !y || !z)))
         return fail(nullptr, OLC_ERR_ARG, std::string(who) + ": null argument");
-    if (variant != OLC_CONTACT_FLAT && variant != OLC_CONTACT_NESTED && variant != OLC_CONTACT_NEAR)
+    if (variant != OLC_CONTACT_FLAT && variant != OLC_CONTACT_NESTED)
         return fail(nullptr, OLC_ERR_ARG, std::string(who) + ": contact_variant must be an OLC_CONTACT_* value");
     std::string err;
     if (!geom_ok(*geom, &err)) return fail(nullptr, OLC_ERR_ARG, std::string(who) + ": " + err);
@@ -2622,8 +2622,7 @@ int olc_set_tuning(OlcSim* s, const OlcTuning* t) {
         return fail(s, OLC_ERR_ARG, "olc_set_tuning: stencil tile (" + std::to_string(t->stencil_tile_y) + ", " +
                                         std::to_string(t->stencil_tile_z) +
                                         ") is not one of (8,8), (16,8), (8,16), (16,4)");
-    if (t->contact_variant != OLC_CONTACT_FLAT && t->contact_variant != OLC_CONTACT_NESTED &&
-        t->contact_variant != OLC_CONTACT_NEAR)
+    if (t->contact_variant != OLC_CONTACT_FLAT && t->contact_variant != OLC_CONTACT_NESTED)
         return fail(s, OLC_ERR_ARG, "olc_set_tuning: contact_variant must be an OLC_CONTACT_* value");
     if (t->batch_tile_depth != 8 && t->batch_tile_depth != 16 && t->batch_tile_depth != 32)
         return fail(s, OLC_ERR_ARG, "olc_set_tuning: batch_tile_depth must be 8, 16 or 32");

@@ -18,8 +18,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _spec(dense: bool = False):
-    # dense: ~100 agents per 10 um bin, so agents have more near candidates
-    # than the near walk's queue holds and walk their bins again in one pass
+    # dense: ~100 agents per 10 um bin
     return W.scaled(W.SCALE, n_agents=30_000, domain=320.0, ball_radius=40.0 if dense else 90.0,
                     field_dims=(64, 64, 64), capacity=150_000, seed=4, uptake=2.0, death_k=0.2, init_drug=0.1,
                     v_lo=1.85, v_hi=2.0)

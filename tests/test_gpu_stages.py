@@ -333,12 +333,11 @@ def test_contact_bit_exact(cuda, olc):
     assert moved.sum() > n // 2
 
 
-@pytest.mark.parametrize("variant", [_lib.OLC_CONTACT_FLAT, _lib.OLC_CONTACT_NESTED, _lib.OLC_CONTACT_NEAR])
+@pytest.mark.parametrize("variant", [_lib.OLC_CONTACT_FLAT, _lib.OLC_CONTACT_NESTED])
 @pytest.mark.parametrize("case", ["sparse", "dense", "moved", "cluster"])
 def test_contact_walks_bit_exact(cuda, olc, variant, case):
     """Every contact walk (olc_stage_contact_tuned) against orc_contact:
-    a sparse population; a dense one (agents with more near candidates than
-    the near walk's queue holds, which walk their bins again in one pass); agents moved after the sort (a rule's displacement), whose current
+    a sparse population; a dense one; agents moved after the sort (a rule's displacement), whose current
     bin differs from the one they are sorted in; and a cluster of 50 agents
     in one bin of a sparse neighbourhood.  Coincident points and dead rows in
     each."""
@@ -371,7 +370,7 @@ def test_contact_walks_bit_exact(cuda, olc, variant, case):
     np.testing.assert_array_equal(got, ref)
     counts = ranges[1::2] - ranges[0::2]
     if case == "dense":
-        assert counts.max() > 64  # dense bins: near-candidate queues overflow
+        assert counts.max() > 64  # dense bins
     if case == "cluster":
         assert 32 < counts.max() <= 64
 
