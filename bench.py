@@ -497,6 +497,9 @@ def run_b200(args) -> None:
         line["serving"] = measure_serving(args.rate, args.serve_seconds, seed=0, storage="f16_sr", solo_sample=4)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(spec)
+    rec = recorded_runs()
+    if rec:
+        line["recorded"] = rec
     line["summary"] = summarise(line)
     assert_clean(line)
     print(json.dumps(line), flush=True)
@@ -527,6 +530,17 @@ def assert_clean(line: dict) -> None:
         raise RuntimeError("device status set: " + "; ".join(f"{w}: {s:#x} {status_names(s)}" for w, s in bad))
 
 
+def recorded_runs() -> dict | None:
+    """The long runs measured with their own commands (profiles/recorded_runs.json:
+    the 1,000-step field error of the scale workload, the 500-step batched
+    sweep against the plain FP32 path), copied into the line as recorded."""
+    p = os.path.join(REPO, "profiles", "recorded_runs.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        return json.load(fh)
+
+
 def summarise(line: dict) -> dict:
     """The headline figures of a line's nested measurements, short, printed
     last so that a log that keeps only the end of the line still shows them."""
@@ -547,6 +561,12 @@ def summarise(line: dict) -> dict:
         if "p99_target_s" in sv:
             out["serving_p99_target_s"] = round(sv["p99_target_s"], 3)
             out["serving_p99_target_met"] = sv["p99_target_met"]
+    rec = line.get("recorded")
+    if rec:
+        pr = rec["precision_scale_1000_steps"]["rel_l2_and_max_abs_after_1000_steps"]
+        out["recorded_rel_l2_after_1000_steps"] = {st: {f: e["rel_l2"] for f, e in r.items()} for st, r in pr.items()}
+        out["recorded_batched_500_steps_vs_plain_fp32"] = {
+            k: v["vs_plain_fp32"] for k, v in rec["batched_sweep_500_steps"]["batched"].items()}
     return out
 
 
