@@ -75,6 +75,8 @@ def parse() -> argparse.Namespace:
                     help="CTA sizes of the two-substep pass timed by --workload stencil (0: one substep per pass)")
     ap.add_argument("--encodings", default="value,deficit,offset3",
                     help="16-bit element encodings timed by --workload stencil")
+    ap.add_argument("--l2-keep", default="0,30,45,60",
+                    help="shares (%%) of the FP32 field kept in L2 timed by --workload stencil (one substep per pass)")
     return ap.parse_args()
 
 
@@ -1021,8 +1023,12 @@ def run_stencil_workload(args) -> None:
     spec = _lib.OlcDiffusion(diffusion=D, decay=0.0, boundary=1.0, substeps=S, has_sink=0)
     f, tmp = f32.clone(), torch.empty_like(f32)
     for nt in (int(v) for v in args.stencil_pair.split(",") if v and v != "none"):
-        t = _lib.OlcTuning(8, 8, 0, 16, nt, 0)
+        t = _lib.OlcTuning(8, 8, 0, 16, nt, 0, 0)
         out[f"f32_pair{nt}" if nt else "f32_single"] = timed(lambda: _lib.check(olc.olc_stage_diffuse_tuned(
+            f.data_ptr(), tmp.data_ptr(), None, C.byref(dims), dx, dt, C.byref(spec), C.byref(t), None)))
+    for keep in (int(v) for v in args.l2_keep.split(",") if v and v != "none"):
+        t = _lib.OlcTuning(8, 8, 0, 16, 0, 0, keep)
+        out[f"f32_single_l2keep{keep}"] = timed(lambda: _lib.check(olc.olc_stage_diffuse_tuned(
             f.data_ptr(), tmp.data_ptr(), None, C.byref(dims), dx, dt, C.byref(spec), C.byref(t), None)))
     for storage in (3, 4):
         for name in (e for e in args.encodings.split(",") if e and e != "none"):

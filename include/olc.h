@@ -162,10 +162,15 @@ typedef struct {
                                      substep per pass */
     int32_t stencil_pair_planes;  /* planes per CTA of the two-substep pass; 0 = as few
                                      as keep the whole grid resident in one wave */
+    int32_t stencil_l2_keep_pct;  /* one-substep passes over an FP32 field read and write
+                                     the first pct % of its planes with L2 evict_last
+                                     and the rest with evict_first, so that slab of both
+                                     buffers stays in L2 from substep to substep; 0 =
+                                     no eviction hints (0..100) */
 } OlcTuning;
 
 /* Sets / reads a handle's kernel shapes and variants (OlcTuning; defaults
- * (8, 8), OLC_CONTACT_FLAT, 16, 0, 0).  Every choice gives the same bits.  Rebuilds
+ * (8, 8), OLC_CONTACT_FLAT, 16, 0, 0, 0).  Every choice gives the same bits.  Rebuilds
  * what depends on them (tensor maps, tile lists) and drops captured graphs;
  * waits for the device. */
 int olc_set_tuning(OlcSim* sim, const OlcTuning* tuning);

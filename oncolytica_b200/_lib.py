@@ -191,6 +191,7 @@ class OlcTuning(C.Structure):
         ("batch_tile_depth", C.c_int32),
         ("stencil_pair_threads", C.c_int32),
         ("stencil_pair_planes", C.c_int32),
+        ("stencil_l2_keep_pct", C.c_int32),
     ]
 
 

@@ -34,9 +34,11 @@ CONTACT_NAMES = {_lib.OLC_CONTACT_FLAT: "flat", _lib.OLC_CONTACT_NESTED: "nested
 BATCH_DEPTHS = (8, 16, 32)
 # (threads per CTA, planes per CTA) of the two-substeps-per-pass kernel; (0, 0) = one substep per pass
 STENCIL_PAIRS = ((0, 0), (1024, 0), (512, 0), (256, 0), (128, 0))
+# share of an FP32 field's planes kept in L2 across one-substep passes (eviction hints)
+L2_KEEP = (0, 30, 45, 60)
 DEFAULT = {"stencil_tile": (8, 8), "contact_variant": _lib.OLC_CONTACT_FLAT, "batch_tile_depth": 16,
-           "stencil_pair": (0, 0)}
-VERSION = 2  # cache entries of earlier tuners lack choices; they are measured again
+           "stencil_pair": (0, 0), "l2_keep_pct": 0}
+VERSION = 3  # cache entries of earlier tuners lack choices; they are measured again
 
 
 def pair_applies(threads: int, dims) -> bool:
@@ -138,6 +140,11 @@ def tune_engine(eng, steps: int = 4, cache: bool = True) -> dict:
                     times[pair] = _measure(eng, sd, dict(best, stencil_pair=pair), "ms_substeps", steps)
             best["stencil_pair"] = min(times, key=times.get)
             measured["substep_pairs"] = {f"{a}/{b}": v for (a, b), v in times.items()}
+            # the slab of planes kept in L2 from substep to substep
+            if best["stencil_pair"][0] == 0:
+                times = {k: _measure(eng, sd, dict(best, l2_keep_pct=k), "ms_substeps", steps) for k in L2_KEEP}
+                best["l2_keep_pct"] = min(times, key=times.get)
+                measured["substep_l2_keep_pct"] = {str(k): v for k, v in times.items()}
         if eng._contact is not None and not be.mech_enabled():
             times = {}
             for v in CONTACT_VARIANTS:
@@ -150,7 +157,8 @@ def tune_engine(eng, steps: int = 4, cache: bool = True) -> dict:
         eng._step = engine_step
         eng.set_graphs(graphs)
     rec = {"tuning": {"stencil_tile": list(best["stencil_tile"]), "contact_variant": int(best["contact_variant"]),
-                      "batch_tile_depth": int(best["batch_tile_depth"]), "stencil_pair": list(best["stencil_pair"])},
+                      "batch_tile_depth": int(best["batch_tile_depth"]), "stencil_pair": list(best["stencil_pair"]),
+                      "l2_keep_pct": int(best["l2_keep_pct"])},
            "measured_ms": measured, "steps": steps}
     if cache:
         _store(key, rec)
@@ -160,7 +168,8 @@ def tune_engine(eng, steps: int = 4, cache: bool = True) -> dict:
 def _tuning_args(t: dict) -> dict:
     """set_tuning keyword arguments from a record's "tuning" object."""
     return {"stencil_tile": tuple(t["stencil_tile"]), "contact_variant": int(t["contact_variant"]),
-            "batch_tile_depth": int(t["batch_tile_depth"]), "stencil_pair": tuple(t.get("stencil_pair", (0, 0)))}
+            "batch_tile_depth": int(t["batch_tile_depth"]), "stencil_pair": tuple(t.get("stencil_pair", (0, 0))),
+            "l2_keep_pct": int(t.get("l2_keep_pct", 0))}
 
 
 def apply_engine(eng, rec: dict) -> None:
@@ -233,4 +242,4 @@ def summary(rec: dict) -> dict:
 
 
 __all__ = ["tune_engine", "tune_batch", "apply_engine", "apply_batch", "summary", "pair_applies", "STENCIL_TILES",
-           "STENCIL_PAIRS", "CONTACT_VARIANTS", "BATCH_DEPTHS"]
+           "STENCIL_PAIRS", "L2_KEEP", "CONTACT_VARIANTS", "BATCH_DEPTHS"]

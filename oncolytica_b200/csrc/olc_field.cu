@@ -205,10 +205,34 @@ struct X4Shape {
     static constexpr size_t SMEM = BYTES + 16 + 128;  // tile + mbarrier + alignment slack
 };
 
-// The 64 x TYR x TZ output block at (x0, y0, z0) from its staged box.
+// L2 eviction priority of a tile's accesses (a cache policy for the
+// .L2::cache_hint forms): the planes a field keeps resident across substeps
+// are read and written with evict_last, the rest with evict_first, so the
+// streamed planes do not push the kept ones out; evict_normal when nothing is
+// kept.
+__device__ __forceinline__ unsigned long long l2_policy(int keep, bool kept) {
+    unsigned long long pol;
+    if (!keep)
+        asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(pol));
+    else if (kept)
+        asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    else
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ void st_hint4(float* p, float4 v, unsigned long long pol) {
+    asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "f"(v.x), "f"(v.y),
+                 "f"(v.z), "f"(v.w), "l"(pol)
+                 : "memory");
+}
+
+// The 64 x TYR x TZ output block at (x0, y0, z0) from its staged box (stores
+// with cache policy pol).
 template <int TYR, int TZ>
 __device__ __forceinline__ void x4_tile(const float* tile, float* __restrict__ out, int x0, int y0, int z0, int nx,
-                                        int ny, int nz, float r, float inv_decay, float bval) {
+                                        int ny, int nz, float r, float inv_decay, float bval,
+                                        unsigned long long pol) {
     using S = X4Shape<TYR, TZ>;
     const int g = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int x = x0 + 4 * g, y = y0 + ty;
@@ -237,17 +261,20 @@ __device__ __forceinline__ void x4_tile(const float* tile, float* __restrict__ o
             if (ex0) v.x = bval;
             if (ex3) v.w = bval;
         }
-        *reinterpret_cast<float4*>(o) = v;
+        st_hint4(o, v, pol);
         o += sz;
         zm = c;
         c = zp;
     }
 }
 
+// keep: planes [0, keep) of both buffers are the field's L2-resident slab
+// (0: no eviction hints).
 template <int TYR, int TZ>
 __global__ void __launch_bounds__(16 * TYR, 1) k_substep_x4(const __grid_constant__ CUtensorMap in_map,
                                                         float* __restrict__ out, int nx, int ny, int nz, float r,
-                                                        float inv_decay, float bval, olc_u32* status, int rev) {
+                                                        float inv_decay, float bval, olc_u32* status, int rev,
+                                                        int keep) {
     using S = X4Shape<TYR, TZ>;
     extern __shared__ unsigned char x4_raw[];
     const olc_u32 pad = (128u - (smem_u32(x4_raw) & 127u)) & 127u;
@@ -268,18 +295,19 @@ __global__ void __launch_bounds__(16 * TYR, 1) k_substep_x4(const __grid_constan
     }
     __syncthreads();
     asm volatile("griddepcontrol.wait;" ::: "memory");
+    const unsigned long long pol = l2_policy(keep, z0 < keep);
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(S::BYTES) : "memory");
         asm volatile(
-            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
-            "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(tile)),
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint "
+            "[%0], [%1, {%2, %3, %4}], [%5], %6;" ::"r"(smem_u32(tile)),
             "l"(reinterpret_cast<unsigned long long>(&in_map)), "r"(x0 - S::HX), "r"(y0 - 1), "r"(z0 - 1),
-            "r"(bar_a)
+            "r"(bar_a), "l"(pol)
             : "memory");
     }
     // bounded wait for the tile (olc_mbar_wait_bounded records a timeout)
     if (!olc_mbar_wait_bounded(bar_a, 0, status)) return;
-    x4_tile<TYR, TZ>(tile, out, x0, y0, z0, nx, ny, nz, r, inv_decay, bval);
+    x4_tile<TYR, TZ>(tile, out, x0, y0, z0, nx, ny, nz, r, inv_decay, bval, pol);
 }
 
 // ---------------------------------------------------------------- two substeps per pass
@@ -508,10 +536,13 @@ template <int NT>
 static int pair_default_planes(const int dims[3], int ty);
 
 bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3], int tile_y, int tile_z, int pair_threads,
-                     int pair_planes) {
+                     int pair_planes, int keep_pct) {
     m->ok = false;
     m->pair_nt = m->pair_ty = m->pair_zl = 0;
-    if (!stencil_tile_known(tile_y, tile_z) || !pair_threads_known(pair_threads) || pair_planes < 0) return false;
+    if (!stencil_tile_known(tile_y, tile_z) || !pair_threads_known(pair_threads) || pair_planes < 0 ||
+        keep_pct < 0 || keep_pct > 100)
+        return false;
+    m->keep = (int)((long long)dims[2] * keep_pct / 100);
     m->VY = tile_y;
     m->VZ = tile_z;
     const cuuint32_t boxv[3] = {72, (cuuint32_t)(tile_y + 2), (cuuint32_t)(tile_z + 2)};
@@ -536,7 +567,7 @@ bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3], int ti
 
 template <int TYR, int TZ>
 static void launch_x4(const CUtensorMap& map, float* out, const FieldStep& fs, olc_u32* status, int rev,
-                      cudaStream_t s) {
+                      int keep, cudaStream_t s) {
     using S = X4Shape<TYR, TZ>;
     static int configured_mask = 0;  // per device (up to 32)
     int dev = 0;
@@ -556,7 +587,7 @@ static void launch_x4(const CUtensorMap& map, float* out, const FieldStep& fs, o
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cudaLaunchKernelEx(&cfg, k_substep_x4<TYR, TZ>, map, out, fs.dims[0], fs.dims[1], fs.dims[2], fs.r,
-                       fs.inv_decay, fs.bval, status, rev);
+                       fs.inv_decay, fs.bval, status, rev, keep);
 }
 
 template <int NT>
@@ -618,7 +649,7 @@ static void launch_single(const FieldMaps& m, int cur, float* out, const FieldSt
                           cudaStream_t s) {
 #define OLC_VX_LAUNCH(p, q)                                   \
     if (m.VY == p && m.VZ == q) {                             \
-        launch_x4<p, q>(m.vec[cur], out, fs, status, rev, s); \
+        launch_x4<p, q>(m.vec[cur], out, fs, status, rev, m.keep, s); \
         return;                                               \
     }
     OLC_VX_SHAPES(OLC_VX_LAUNCH)
