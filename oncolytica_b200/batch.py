@@ -177,6 +177,10 @@ class BatchEngine:
             self._check(self.lib.olc_set_rule_source(self.handle, self.program.source.encode(), names, kinds,
                                                      len(self.program.kernels), _lib.CSRC_DIR.encode()))
             if any(kind == 3 for _, kind in self.program.kernels):
+                if any(d.storage != "f32" for e in self.engines for d in e._diffusion.values()):
+                    from oncolytica_b200._errors import CompilationError
+
+                    raise CompilationError("chemistry rules need FP32 chemistry fields (setup_diffusion storage='f32')")
                 its = (C.c_int * len(self.program.kernels))(*self.program.iterations)
                 self._check(self.lib.olc_set_rule_iterations(self.handle, its, len(self.program.kernels)))
         self.metrics_words = max(1, len(L.metrics))
