@@ -6,7 +6,8 @@ candidate on the caller's own workload with per-stage CUDA events
 
 * ``tune_engine(engine)``: the FP32 stencil tile (rows x planes of the TMA
   substep), whether FP32 fields take two substeps per pass (temporal
-  blocking, and the CTA size of that kernel) and the contact walk of a solo
+  blocking, and the CTA size of that kernel), the share of an FP32 field's
+  planes kept in L2 by eviction hints, and the contact walk of a solo
   engine.  The engine's state is saved
   with ``state_dict()`` first and restored after, so tuning leaves the run
   exactly where it was.
