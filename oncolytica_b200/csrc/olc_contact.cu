@@ -35,15 +35,12 @@ __global__ void __launch_bounds__(256) k_contact(const float4* __restrict__ posr
         const olc_u32 kx[3] = {olc_tissue_axis(cx - 1, 0), olc_tissue_axis(cx, 0), olc_tissue_axis(cx + 1, 0)};
         const olc_u32 ky[3] = {olc_tissue_axis(cy - 1, 1), olc_tissue_axis(cy, 1), olc_tissue_axis(cy + 1, 1)};
         const olc_u32 kz[3] = {olc_tissue_axis(cz - 1, 2), olc_tissue_axis(cz, 2), olc_tissue_axis(cz + 1, 2)};
-#pragma unroll
         for (int dz = -1; dz <= 1; ++dz) {
             const int nz = cz + dz;
             if (nz < 0 || nz >= c.tdims[2]) continue;
-#pragma unroll
             for (int dy = -1; dy <= 1; ++dy) {
                 const int ny = cy + dy;
                 if (ny < 0 || ny >= c.tdims[1]) continue;
-#pragma unroll
                 for (int dx = -1; dx <= 1; ++dx) {
                     const int nx = cx + dx;
                     if (nx < 0 || nx >= c.tdims[0]) continue;
@@ -301,14 +298,11 @@ __device__ __forceinline__ void contact_pair(const float4& p, const float4& q, o
 }
 
 constexpr int CF_THREADS = 128;
-__global__ void __launch_bounds__(CF_THREADS, 10) k_contact_flat(const float4* __restrict__ posr,
+__global__ void __launch_bounds__(CF_THREADS) k_contact_flat(const float4* __restrict__ posr,
                                                             const uint2* __restrict__ ranges, const olc_u32* n_dev,
                                                             olc_u32 n_host, ContactDev c, float* __restrict__ xo,
                                                             float* __restrict__ yo, float* __restrict__ zo) {
-    // the thread's non-empty bins: first row and row count (6 bytes an entry,
-    // so more CTAs fit on an SM than with 8-byte ranges)
-    __shared__ olc_u32 s_start[27][CF_THREADS];
-    __shared__ unsigned short s_cnt[27][CF_THREADS];
+    __shared__ uint2 s_bins[27][CF_THREADS];
     const olc_u32 n = n_dev ? *n_dev : n_host;
     const float md = __fmul_rn(c.mobility, c.dt);
     const int t = threadIdx.x;
@@ -329,57 +323,29 @@ __global__ void __launch_bounds__(CF_THREADS, 10) k_contact_flat(const float4* _
             kz[d] = olc_tissue_axis(cz + d - 1, 2);
         }
         int nb = 0;
-        bool big = false;  // a bin of more than 65,535 rows: walk the bins directly
-#pragma unroll
         for (int dz = -1; dz <= 1; ++dz) {
             const int nz = cz + dz;
             if (nz < 0 || nz >= c.tdims[2]) continue;
-#pragma unroll
             for (int dy = -1; dy <= 1; ++dy) {
                 const int ny = cy + dy;
                 if (ny < 0 || ny >= c.tdims[1]) continue;
-#pragma unroll
                 for (int dx = -1; dx <= 1; ++dx) {
                     const int nx = cx + dx;
                     if (nx < 0 || nx >= c.tdims[0]) continue;
                     const uint2 rg = __ldg(ranges + (kx[dx + 1] | ky[dy + 1] | kz[dz + 1]));
-                    if (rg.y > rg.x) {
-                        big = big || rg.y - rg.x > 0xffffu;
-                        s_start[nb][t] = rg.x;
-                        s_cnt[nb][t] = (unsigned short)(rg.y - rg.x);
-                        ++nb;
-                    }
+                    if (rg.y > rg.x) s_bins[nb++][t] = rg;
                 }
             }
         }
         float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-        if (big) {
-#pragma unroll
-            for (int dz = -1; dz <= 1; ++dz) {
-                const int nz = cz + dz;
-                if (nz < 0 || nz >= c.tdims[2]) continue;
-#pragma unroll
-                for (int dy = -1; dy <= 1; ++dy) {
-                    const int ny = cy + dy;
-                    if (ny < 0 || ny >= c.tdims[1]) continue;
-#pragma unroll
-                    for (int dx = -1; dx <= 1; ++dx) {
-                        const int nx = cx + dx;
-                        if (nx < 0 || nx >= c.tdims[0]) continue;
-                        const uint2 rg = __ldg(ranges + (kx[dx + 1] | ky[dy + 1] | kz[dz + 1]));
-                        for (olc_u32 jj = rg.x; jj < rg.y; ++jj) contact_pair(p, __ldg(posr + jj), i, jj, c, fx, fy, fz);
-                    }
-                }
-            }
-            nb = 0;  // the listed walk below has nothing left to do
-        }
         // the next candidate's record is requested before this one is used
         int b = 0;
         olc_u32 j = 0, end = 0;
         float4 q = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
         if (nb > 0) {
-            j = s_start[0][t];
-            end = j + s_cnt[0][t];
+            const uint2 r = s_bins[0][t];
+            j = r.x;
+            end = r.y;
             q = __ldg(posr + j);
         }
         while (b < nb) {
@@ -387,8 +353,9 @@ __global__ void __launch_bounds__(CF_THREADS, 10) k_contact_flat(const float4* _
             int bn = b;
             if (jn == en) {
                 if (++bn < nb) {
-                    jn = s_start[bn][t];
-                    en = jn + s_cnt[bn][t];
+                    const uint2 r = s_bins[bn][t];
+                    jn = r.x;
+                    en = r.y;
                 }
             }
             const float4 qn = bn < nb ? __ldg(posr + jn) : q;
