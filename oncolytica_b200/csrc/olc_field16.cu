@@ -135,42 +135,7 @@ constexpr int TYR = 16, TZ = 8, WY = TYR + 2, WZ = TZ + 2;
 constexpr int THREADS = 8 * TYR;
 constexpr unsigned BYTES = WX * WY * WZ * 2;
 constexpr size_t SMEM = BYTES + 16 + 128;
-// decode-once form: the box decoded into FP32 working values after the mbarrier
-constexpr unsigned FBYTES = WX * WY * WZ * 4;
-constexpr size_t SMEM_DEC = BYTES + 16 + FBYTES + 128;
 }  // namespace t16
-
-// Whether a tile of encoding EN decodes its box once into FP32 shared memory
-// (one barrier per tile) instead of decoding each element where it is read
-// (about 3.25 times per voxel: as the next plane of its own row and as a y
-// neighbour of two rows).  Three offsets cost about eight integer and select
-// operations per decode, so they take the decode-once form; values and
-// deficits decode in one operation and keep the barrier-free tile.
-template <int EN>
-struct T16Dec {
-    static constexpr bool value = EN == OLC_ENC_OFFSET3;
-    static constexpr size_t smem = value ? t16::SMEM_DEC : t16::SMEM;
-};
-
-// All threads of the CTA: the staged 16-bit box into FP32 working values
-// (eight elements per 16-byte chunk), the same values Codec::work gives.
-template <int ST, int EN>
-__device__ __forceinline__ void t16_decode_box(const unsigned short* tile, float* ftile, const EncConst& k) {
-    using namespace t16;
-    constexpr int CHUNKS = BYTES / 16;
-    for (int q = threadIdx.x; q < CHUNKS; q += THREADS) {
-        float w[8];
-        load8w<ST, EN>(tile + 8 * q, w, k);
-        *reinterpret_cast<float4*>(ftile + 8 * q) = make_float4(w[0], w[1], w[2], w[3]);
-        *reinterpret_cast<float4*>(ftile + 8 * q + 4) = make_float4(w[4], w[5], w[6], w[7]);
-    }
-}
-
-__device__ __forceinline__ void load8f(const float* p, float (&f)[8]) {
-    const float4 a = *reinterpret_cast<const float4*>(p);
-    const float4 b = *reinterpret_cast<const float4*>(p + 4);
-    f[0] = a.x, f[1] = a.y, f[2] = a.z, f[3] = a.w, f[4] = b.x, f[5] = b.y, f[6] = b.z, f[7] = b.w;
-}
 
 // The working value the Dirichlet faces hold (OLC_ENC_*): the boundary as
 // stored, its deficit 0, or b itself (OLC_ENC_OFFSET3 stores it exactly).
@@ -183,12 +148,9 @@ __device__ __forceinline__ float face_work(float bval) {
 
 // The 64 x TYR x TZ output block at (x0, y0, z0) from its staged 16-bit box
 // (stochastic-rounding key given), on the working values of encoding EN.
-// With DEC the box is read as its decoded FP32 working values (ftile, the same
-// geometry) instead of 16-bit elements; the arithmetic is the same.
-template <int ST, int EN, bool DEC = false>
+template <int ST, int EN>
 __device__ __forceinline__ void t16_tile(const unsigned short* tile, unsigned short* __restrict__ out, int x0, int y0,
-                                         int z0, int nx, int ny, int nz, const FieldStep& fs, olc_u32 key,
-                                         const float* ftile = nullptr) {
+                                         int z0, int nx, int ny, int nz, const FieldStep& fs, olc_u32 key) {
     using namespace t16;
     const int g = threadIdx.x & 7, ty = threadIdx.x >> 3;
     const int x = x0 + 8 * g, y = y0 + ty;
@@ -199,17 +161,10 @@ __device__ __forceinline__ void t16_tile(const unsigned short* tile, unsigned sh
     const bool edge_y = y == 0 || y == ny - 1;
     const bool ex0 = x == 0, ex7 = x + 7 == nx - 1;
     constexpr int PS = WY * WX;
-    const int col_off = (ty + 1) * WX + HX + 8 * g;
-    const unsigned short* col = tile + col_off;
-    const float* fcol = DEC ? ftile + col_off : nullptr;
+    const unsigned short* col = tile + (ty + 1) * WX + HX + 8 * g;
     float zm[8], c[8], zp[8], ym[8], yp[8], v[8];
-    if constexpr (DEC) {
-        load8f(fcol, zm);
-        load8f(fcol + PS, c);
-    } else {
-        load8w<ST, EN>(col, zm, k);
-        load8w<ST, EN>(col + PS, c, k);
-    }
+    load8w<ST, EN>(col, zm, k);
+    load8w<ST, EN>(col + PS, c, k);
     const size_t sz = (size_t)nx * ny;
     unsigned short* o = out + (size_t)z0 * sz + (size_t)y * nx + x;
     const float bf = face_work<ST, EN>(fs.bval);
@@ -218,25 +173,14 @@ __device__ __forceinline__ void t16_tile(const unsigned short* tile, unsigned sh
     for (int lz = 1; lz <= TZ; ++lz) {
         const int z = z0 + lz - 1;
         if (z >= nz) break;
-        float xl, xr;
-        if constexpr (DEC) {
-            const float* pc = fcol + lz * PS;
-            load8f(pc + PS, zp);
-            load8f(pc - WX, ym);
-            load8f(pc + WX, yp);
-            xl = pc[-1];
-            xr = pc[8];
-        } else {
-            const unsigned short* pc = col + lz * PS;
-            load8w<ST, EN>(pc + PS, zp, k);
-            load8w<ST, EN>(pc - WX, ym, k);
-            load8w<ST, EN>(pc + WX, yp, k);
-            // x neighbours of the group from shared memory (2-byte loads with a
-            // 4-way bank conflict; lane shuffles of the neighbours' registers
-            // measured 14 % slower on B200)
-            xl = Codec<ST, EN>::work(pc[-1], k);
-            xr = Codec<ST, EN>::work(pc[8], k);
-        }
+        const unsigned short* pc = col + lz * PS;
+        load8w<ST, EN>(pc + PS, zp, k);
+        load8w<ST, EN>(pc - WX, ym, k);
+        load8w<ST, EN>(pc + WX, yp, k);
+        // x neighbours of the group from shared memory (2-byte loads with a
+        // 4-way bank conflict; lane shuffles of the neighbours' registers
+        // measured 14 % slower on B200)
+        const float xl = Codec<ST, EN>::work(pc[-1], k), xr = Codec<ST, EN>::work(pc[8], k);
         stencil_update8_enc<EN>(xl, xr, c, ym, yp, zm, zp, r, inv_decay, dec_sub, k.b, v);
         if (edge_y || z == 0 || z == nz - 1) {
 #pragma unroll
@@ -287,19 +231,11 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep16(const __grid_constan
             : "memory");
     }
     // bounded wait for the tile (olc_mbar_wait_bounded records a timeout);
-    // a warp leaves as a whole (the barrier-free tile), or the CTA (decode-once)
+    // a warp leaves as a whole (the tile has no block-wide barrier)
     const bool tile_ready = olc_mbar_wait_bounded(bar, 0, status);
-    const olc_u32 key = olc_sr_key(step_ctr ? *step_ctr : step_host, sub, field);
-    if constexpr (T16Dec<EN>::value) {
-        if (__syncthreads_or(!tile_ready)) return;
-        float* ftile = reinterpret_cast<float*>(t16_raw + pad + BYTES + 16);
-        t16_decode_box<ST, EN>(tile, ftile, enc_const(fs));
-        __syncthreads();
-        t16_tile<ST, EN, true>(tile, out, x0, y0, z0, fs.dims[0], fs.dims[1], fs.dims[2], fs, key, ftile);
-    } else {
-        if (__any_sync(0xffffffffu, !tile_ready)) return;
-        t16_tile<ST, EN>(tile, out, x0, y0, z0, fs.dims[0], fs.dims[1], fs.dims[2], fs, key);
-    }
+    if (__any_sync(0xffffffffu, !tile_ready)) return;
+    t16_tile<ST, EN>(tile, out, x0, y0, z0, fs.dims[0], fs.dims[1], fs.dims[2], fs,
+                     olc_sr_key(step_ctr ? *step_ctr : step_host, sub, field));
 }
 
 // ------------------------------------------------------------------ batched substep
@@ -349,19 +285,11 @@ __global__ void __launch_bounds__(t16::THREADS) k_substep_batch_t16(
             : "memory");
     }
     // bounded wait for the tile (olc_mbar_wait_bounded records a timeout);
-    // a warp leaves as a whole (the barrier-free tile), or the CTA (decode-once)
+    // a warp leaves as a whole (the tile has no block-wide barrier)
     const bool tile_ready = olc_mbar_wait_bounded(bar, 0, status);
-    const olc_u32 key = olc_sr_key(*step_ctr - d.step_base, sub, field);
-    if constexpr (T16Dec<EN>::value) {
-        if (__syncthreads_or(!tile_ready)) return;
-        float* ftile = reinterpret_cast<float*>(t16_raw + pad + BYTES + 16);
-        t16_decode_box<ST, EN>(tile, ftile, enc_const(fs));
-        __syncthreads();
-        t16_tile<ST, EN, true>(tile, out, x0, y0, z0, d.cdims[0], d.cdims[1], d.cdims[2], fs, key, ftile);
-    } else {
-        if (__any_sync(0xffffffffu, !tile_ready)) return;
-        t16_tile<ST, EN>(tile, out, x0, y0, z0, d.cdims[0], d.cdims[1], d.cdims[2], fs, key);
-    }
+    if (__any_sync(0xffffffffu, !tile_ready)) return;
+    t16_tile<ST, EN>(tile, out, x0, y0, z0, d.cdims[0], d.cdims[1], d.cdims[2], fs,
+                     olc_sr_key(*step_ctr - d.step_base, sub, field));
 }
 
 template <int ST, int EN>
@@ -373,14 +301,13 @@ static void launch_bt16(const uint4* tiles, olc_u32 n_tiles, const OlcSimDesc* s
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 32 && !(configured_mask & (1 << dev))) {
-        cudaFuncSetAttribute(k_substep_batch_t16<ST, EN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)T16Dec<EN>::smem);
+        cudaFuncSetAttribute(k_substep_batch_t16<ST, EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
         configured_mask |= 1 << dev;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(n_tiles);
     cfg.blockDim = dim3(THREADS);
-    cfg.dynamicSmemBytes = T16Dec<EN>::smem;
+    cfg.dynamicSmemBytes = SMEM;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -419,13 +346,13 @@ static void launch_sub16(const CUtensorMap& map, void* out, const FieldStep& fs,
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 32 && !(configured_mask & (1 << dev))) {
-        cudaFuncSetAttribute(k_substep16<ST, EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T16Dec<EN>::smem);
+        cudaFuncSetAttribute(k_substep16<ST, EN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
         configured_mask |= 1 << dev;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((fs.dims[0] + TX - 1) / TX, (fs.dims[1] + TYR - 1) / TYR, (fs.dims[2] + TZ - 1) / TZ);
     cfg.blockDim = dim3(THREADS);
-    cfg.dynamicSmemBytes = T16Dec<EN>::smem;
+    cfg.dynamicSmemBytes = SMEM;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
