@@ -440,7 +440,8 @@ def run_b200(args) -> None:
     else:
         launch_ms = sub_ms
         kernel = "k_substep_x4 (7-point FTCS, FP32, 4-wide rows, TMA tiles)"
-        traffic = read_traffic("k_substep_x4", nvox)
+        keep = (tuning.get("tuning") or {}).get("l2_keep_pct", 0)
+        traffic = read_traffic("k_substep_x4_l2slab" if keep else "k_substep_x4_scale", nvox)
     achieved = alg_bytes / (launch_ms / 1e3) / 1e9
     steps_done = max(1, prof["steps"])
     stages = {k[3:]: prof[k] / steps_done for k in ("ms_sink", "ms_substeps", "ms_grid", "ms_rules",
