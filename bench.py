@@ -75,9 +75,6 @@ def parse() -> argparse.Namespace:
                     help="CTA sizes of the two-substep pass timed by --workload stencil (0: one substep per pass)")
     ap.add_argument("--encodings", default="value,deficit,offset3",
                     help="16-bit element encodings timed by --workload stencil")
-    ap.add_argument("--march", default="0,512,1024",
-                    help="CTA sizes of the one-substep z march timed by --workload stencil (0: tiles), with --march-keep")
-    ap.add_argument("--march-keep", type=int, default=45, help="L2 slab share of the --march timings")
     ap.add_argument("--l2-keep", default="0,30,45,60",
                     help="shares (%%) of the FP32 field kept in L2 timed by --workload stencil (one substep per pass)")
     return ap.parse_args()
@@ -1027,15 +1024,11 @@ def run_stencil_workload(args) -> None:
     spec = _lib.OlcDiffusion(diffusion=D, decay=0.0, boundary=1.0, substeps=S, has_sink=0)
     f, tmp = f32.clone(), torch.empty_like(f32)
     for nt in (int(v) for v in args.stencil_pair.split(",") if v and v != "none"):
-        t = _lib.OlcTuning(8, 8, 0, 16, nt, 0, 0, 0)
+        t = _lib.OlcTuning(8, 8, 0, 16, nt, 0, 0)
         out[f"f32_pair{nt}" if nt else "f32_single"] = timed(lambda: _lib.check(olc.olc_stage_diffuse_tuned(
             f.data_ptr(), tmp.data_ptr(), None, C.byref(dims), dx, dt, C.byref(spec), C.byref(t), None)))
-    for nt in (int(v) for v in args.march.split(",") if v and v != "none"):
-        t = _lib.OlcTuning(8, 8, 0, 16, 0, 0, args.march_keep, nt)
-        out[f"f32_march{nt}_keep{args.march_keep}"] = timed(lambda: _lib.check(olc.olc_stage_diffuse_tuned(
-            f.data_ptr(), tmp.data_ptr(), None, C.byref(dims), dx, dt, C.byref(spec), C.byref(t), None)))
     for keep in (int(v) for v in args.l2_keep.split(",") if v and v != "none"):
-        t = _lib.OlcTuning(8, 8, 0, 16, 0, 0, keep, 0)
+        t = _lib.OlcTuning(8, 8, 0, 16, 0, 0, keep)
         out[f"f32_single_l2keep{keep}"] = timed(lambda: _lib.check(olc.olc_stage_diffuse_tuned(
             f.data_ptr(), tmp.data_ptr(), None, C.byref(dims), dx, dt, C.byref(spec), C.byref(t), None)))
     for storage in (3, 4):

@@ -167,15 +167,10 @@ typedef struct {
                                      and the rest with evict_first, so that slab of both
                                      buffers stays in L2 from substep to substep; 0 =
                                      no eviction hints (0..100) */
-    int32_t stencil_march_threads; /* one-substep passes over an FP32 field whose rows fit
-                                      one TMA box (x extent <= 256) as a z march with
-                                      CTAs of 256, 512 or 1024 threads (each input plane
-                                      loaded once per CTA through a ring of TMA slots);
-                                      0 = the tile kernel */
 } OlcTuning;
 
 /* Sets / reads a handle's kernel shapes and variants (OlcTuning; defaults
- * (8, 8), OLC_CONTACT_FLAT, 16, 0, 0, 0, 0).  Every choice gives the same bits.  Rebuilds
+ * (8, 8), OLC_CONTACT_FLAT, 16, 0, 0, 0).  Every choice gives the same bits.  Rebuilds
  * what depends on them (tensor maps, tile lists) and drops captured graphs;
  * waits for the device. */
 int olc_set_tuning(OlcSim* sim, const OlcTuning* tuning);

@@ -192,7 +192,6 @@ class OlcTuning(C.Structure):
         ("stencil_pair_threads", C.c_int32),
         ("stencil_pair_planes", C.c_int32),
         ("stencil_l2_keep_pct", C.c_int32),
-        ("stencil_march_threads", C.c_int32),
     ]
 
 

@@ -37,19 +37,9 @@ BATCH_DEPTHS = (8, 16, 32)
 STENCIL_PAIRS = ((0, 0), (1024, 0), (512, 0), (256, 0), (128, 0))
 # share of an FP32 field's planes kept in L2 across one-substep passes (eviction hints)
 L2_KEEP = (0, 30, 45, 60)
-# CTA size of the one-substep z march (0: the tile kernel)
-MARCH = (0, 512, 1024)
 DEFAULT = {"stencil_tile": (8, 8), "contact_variant": _lib.OLC_CONTACT_FLAT, "batch_tile_depth": 16,
-           "stencil_pair": (0, 0), "l2_keep_pct": 0, "march_threads": 0}
-VERSION = 4  # cache entries of earlier tuners lack choices; they are measured again
-
-
-def march_applies(threads: int, dims) -> bool:
-    """Whether the one-substep z march with ``threads`` per CTA runs on a field
-    of ``dims``: rows of at most 256 voxels, x a multiple of 4 (olc_field.cu
-    march_rows)."""
-    nx = int(dims[0])
-    return threads == 0 or (8 <= nx <= 256 and nx % 4 == 0 and threads // (nx // 4) >= 1)
+           "stencil_pair": (0, 0), "l2_keep_pct": 0}
+VERSION = 3  # cache entries of earlier tuners lack choices; they are measured again
 
 
 def pair_applies(threads: int, dims) -> bool:
@@ -156,13 +146,6 @@ def tune_engine(eng, steps: int = 4, cache: bool = True) -> dict:
                 times = {k: _measure(eng, sd, dict(best, l2_keep_pct=k), "ms_substeps", steps) for k in L2_KEEP}
                 best["l2_keep_pct"] = min(times, key=times.get)
                 measured["substep_l2_keep_pct"] = {str(k): v for k, v in times.items()}
-                # the one-substep pass as a z march instead of tiles, with that slab
-                times = {}
-                for nt in MARCH:
-                    if march_applies(nt, eng.chemistry_shape):
-                        times[nt] = _measure(eng, sd, dict(best, march_threads=nt), "ms_substeps", steps)
-                best["march_threads"] = min(times, key=times.get)
-                measured["substep_march"] = {str(k): v for k, v in times.items()}
         if eng._contact is not None and not be.mech_enabled():
             times = {}
             for v in CONTACT_VARIANTS:
@@ -176,7 +159,7 @@ def tune_engine(eng, steps: int = 4, cache: bool = True) -> dict:
         eng.set_graphs(graphs)
     rec = {"tuning": {"stencil_tile": list(best["stencil_tile"]), "contact_variant": int(best["contact_variant"]),
                       "batch_tile_depth": int(best["batch_tile_depth"]), "stencil_pair": list(best["stencil_pair"]),
-                      "l2_keep_pct": int(best["l2_keep_pct"]), "march_threads": int(best["march_threads"])},
+                      "l2_keep_pct": int(best["l2_keep_pct"])},
            "measured_ms": measured, "steps": steps}
     if cache:
         _store(key, rec)
@@ -187,7 +170,7 @@ def _tuning_args(t: dict) -> dict:
     """set_tuning keyword arguments from a record's "tuning" object."""
     return {"stencil_tile": tuple(t["stencil_tile"]), "contact_variant": int(t["contact_variant"]),
             "batch_tile_depth": int(t["batch_tile_depth"]), "stencil_pair": tuple(t.get("stencil_pair", (0, 0))),
-            "l2_keep_pct": int(t.get("l2_keep_pct", 0)), "march_threads": int(t.get("march_threads", 0))}
+            "l2_keep_pct": int(t.get("l2_keep_pct", 0))}
 
 
 def apply_engine(eng, rec: dict) -> None:
@@ -260,4 +243,4 @@ def summary(rec: dict) -> dict:
 
 
 __all__ = ["tune_engine", "tune_batch", "apply_engine", "apply_batch", "summary", "pair_applies", "STENCIL_TILES",
-           "STENCIL_PAIRS", "L2_KEEP", "MARCH", "march_applies", "CONTACT_VARIANTS", "BATCH_DEPTHS"]
+           "STENCIL_PAIRS", "L2_KEEP", "CONTACT_VARIANTS", "BATCH_DEPTHS"]

@@ -296,17 +296,15 @@ class CudaBackend:
 
     # ---- tuning (olc.h OlcTuning; oncolytica_b200.autotune measures it) -------
     def set_tuning(self, stencil_tile=(8, 8), contact_variant: int = _lib.OLC_CONTACT_FLAT,
-                   batch_tile_depth: int = 16, stencil_pair=(0, 0), l2_keep_pct: int = 0,
-                   march_threads: int = 0) -> None:
+                   batch_tile_depth: int = 16, stencil_pair=(0, 0), l2_keep_pct: int = 0) -> None:
         """Kernel shapes and variants (olc_set_tuning): the FP32 stencil tile
         (rows, planes), the contact walk, the batched tile depth,
         ``stencil_pair`` = (threads per CTA, planes per CTA) of the
-        two-substeps-per-pass kernel ((0, 0): one substep per pass), the
+        two-substeps-per-pass kernel ((0, 0): one substep per pass), and the
         share of an FP32 field's planes kept in L2 across substeps by
-        eviction hints (``l2_keep_pct``, 0: none), and the CTA size of the
-        one-substep z march (``march_threads``, 0: the tile kernel)."""
+        eviction hints (``l2_keep_pct``, 0: none)."""
         t = _lib.OlcTuning(int(stencil_tile[0]), int(stencil_tile[1]), int(contact_variant), int(batch_tile_depth),
-                           int(stencil_pair[0]), int(stencil_pair[1]), int(l2_keep_pct), int(march_threads))
+                           int(stencil_pair[0]), int(stencil_pair[1]), int(l2_keep_pct))
         self._check(self.lib.olc_set_tuning(self.handle, C.byref(t)))
 
     def get_tuning(self) -> dict:
@@ -314,8 +312,7 @@ class CudaBackend:
         self._check(self.lib.olc_get_tuning(self.handle, C.byref(t)))
         return {"stencil_tile": (t.stencil_tile_y, t.stencil_tile_z), "contact_variant": t.contact_variant,
                 "batch_tile_depth": t.batch_tile_depth,
-                "stencil_pair": (t.stencil_pair_threads, t.stencil_pair_planes), "l2_keep_pct": t.stencil_l2_keep_pct,
-                "march_threads": t.stencil_march_threads}
+                "stencil_pair": (t.stencil_pair_threads, t.stencil_pair_planes), "l2_keep_pct": t.stencil_l2_keep_pct}
 
     def has_tma_fields(self) -> bool:
         """Whether a diffusing FP32 field takes the TMA substep (the tuned tile)."""

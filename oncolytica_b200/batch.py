@@ -200,11 +200,10 @@ class BatchEngine:
         self._check(self.lib.olc_set_graphs(self.handle, int(self.use_graphs)))
 
     def set_tuning(self, stencil_tile=(8, 8), contact_variant: int = _lib.OLC_CONTACT_FLAT,
-                   batch_tile_depth: int = 16, stencil_pair=(0, 0), l2_keep_pct: int = 0,
-                   march_threads: int = 0) -> None:
+                   batch_tile_depth: int = 16, stencil_pair=(0, 0), l2_keep_pct: int = 0) -> None:
         """Kernel shapes and variants of the batch handle (olc_set_tuning)."""
         t = _lib.OlcTuning(int(stencil_tile[0]), int(stencil_tile[1]), int(contact_variant), int(batch_tile_depth),
-                           int(stencil_pair[0]), int(stencil_pair[1]), int(l2_keep_pct), int(march_threads))
+                           int(stencil_pair[0]), int(stencil_pair[1]), int(l2_keep_pct))
         self._check(self.lib.olc_set_tuning(self.handle, C.byref(t)))
 
     def set_tile_depths(self, depths) -> None:

@@ -452,127 +452,6 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_substep_pair(const __grid_con
     }
 }
 
-// ---------------------------------------------------------------- one substep, z march
-// k_substep_march<NT>: one substep per pass as a z march over full-width rows
-// (the structure of k_substep_pair's first step, writing the output): a CTA
-// owns rows [y0, y0 + TY), TY = NT / (nx / 4), and planes [z0, z0 + ZL);
-// input planes z0-1 .. z0+ZL stream through a ring of PAIR_RING TMA slots
-// (TY + 2 rows each, refilled as soon as every thread is past its last read),
-// so each plane is loaded once per CTA and the next ones are in flight while
-// the current one is computed.  Each thread keeps its own column's planes z-1
-// and z in registers and reads plane z+1 and its x / y neighbours from the
-// ring.  Every voxel is stencil_update4 with x4_tile's boundary rule: the same
-// bits as k_substep_x4.  Stores and loads carry the L2 policy of the field's
-// resident slab (keep, as in k_substep_x4).
-__host__ __device__ inline int march_slot_floats(int nx, int ty) { return pair_round32(nx * (ty + 2)); }
-inline size_t march_smem_bytes(int nx, int ty) {
-    return (size_t)PAIR_RING * march_slot_floats(nx, ty) * 4 + 8 * PAIR_RING + 128;
-}
-
-template <int NT>
-__global__ void __launch_bounds__(NT, 1024 / NT) k_substep_march(const __grid_constant__ CUtensorMap in_map,
-                                                                float* __restrict__ out, int nx, int ny, int nz,
-                                                                float r, float inv_decay, float bval,
-                                                                olc_u32* status, int rev, int ty, int zl, int keep) {
-    extern __shared__ unsigned char march_raw[];
-    const olc_u32 pad = (128u - (smem_u32(march_raw) & 127u)) & 127u;
-    float* ring = reinterpret_cast<float*>(march_raw + pad);
-    const int slot_f = march_slot_floats(nx, ty);
-    const olc_u32 bar0 = smem_u32(ring + PAIR_RING * slot_f);
-    const int by = rev ? gridDim.x - 1 - blockIdx.x : blockIdx.x;
-    const int bz = rev ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
-    const int y0 = by * ty, z0 = bz * zl;
-    const int z_end = min(z0 + zl, nz);
-    const int nq = z_end - z0 + 2;  // input planes z0-1 .. z_end
-    const olc_u32 plane_bytes = (olc_u32)(nx * (ty + 2) * 4);
-    const int G = nx >> 2;
-    const int row = threadIdx.x / G, g = threadIdx.x - row * G;
-    const int y = y0 + row, x = 4 * g;
-    const bool live = row < ty && y < ny;
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < PAIR_RING; ++k)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0 + 8 * k) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    }
-    __syncthreads();
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    // input plane z0 - 1 + q lives in slot q % PAIR_RING; its mbarrier phase is (q / PAIR_RING) & 1
-    int issued = 0;  // thread 0: planes issued so far
-    auto issue_upto = [&](int last_free) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        for (; issued < nq && issued - PAIR_RING <= last_free; ++issued) {
-            const olc_u32 bar = bar0 + 8 * (issued % PAIR_RING);
-            const unsigned long long pol = l2_policy(keep, z0 - 1 + issued < keep);
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(plane_bytes)
-                         : "memory");
-            asm volatile(
-                "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint "
-                "[%0], [%1, {%2, %3, %4}], [%5], %6;" ::"r"(smem_u32(ring + (issued % PAIR_RING) * slot_f)),
-                "l"(reinterpret_cast<unsigned long long>(&in_map)), "r"(0), "r"(y0 - 1), "r"(z0 - 1 + issued),
-                "r"(bar), "l"(pol)
-                : "memory");
-        }
-    };
-    auto wait_plane = [&](int q) {
-        return olc_mbar_wait_bounded(bar0 + 8 * (q % PAIR_RING), (olc_u32)((q / PAIR_RING) & 1), status);
-    };
-    if (threadIdx.x == 0) issue_upto(-1);
-    const int row_off = (row + 1) * nx + 4 * g;  // this thread's voxels in an input slot
-    const bool y_face = y == 0 || y == ny - 1;
-    const bool ex0 = x == 0, ex3 = x + 3 == nx - 1;
-    const float4 b4 = make_float4(bval, bval, bval, bval);
-    const size_t sz = (size_t)nx * ny;
-    bool ok = wait_plane(0) && wait_plane(1);
-    float4 zm = b4, c = b4;
-    if (row < ty) {
-        zm = *reinterpret_cast<const float4*>(ring + row_off);
-        c = *reinterpret_cast<const float4*>(ring + slot_f + row_off);
-    }
-    for (int z = z0, i = 0; z < z_end; ++z, ++i) {
-        const int qn = i + 2;  // input plane z + 1
-        ok = ok && wait_plane(qn);
-        if (row < ty) {
-            const float* pc = ring + ((qn - 1) % PAIR_RING) * slot_f + row_off;
-            const float4 zp = *reinterpret_cast<const float4*>(ring + (qn % PAIR_RING) * slot_f + row_off);
-            if (live) {
-                const float4 ym = *reinterpret_cast<const float4*>(pc - nx);
-                const float4 yp = *reinterpret_cast<const float4*>(pc + nx);
-                float4 v = stencil_update4(pc[-1], pc[4], c, ym, yp, zm, zp, r, inv_decay);
-                if (y_face || z == 0 || z == nz - 1) {
-                    v = b4;
-                } else {
-                    if (ex0) v.x = bval;
-                    if (ex3) v.w = bval;
-                }
-                st_hint4(out + (size_t)z * sz + (size_t)y * nx + x, v, l2_policy(keep, z < keep));
-            }
-            zm = c;
-            c = zp;
-        }
-        if (__syncthreads_or(!ok)) {
-            // a plane never arrived: let the copies still in flight land, then leave
-            if (threadIdx.x == 0)
-                for (int q = issued > PAIR_RING ? issued - PAIR_RING : 0; q < issued; ++q)
-                    for (olc_u32 it = 0; it < OLC_SPIN_LIMIT; ++it)
-                        if (olc_mbar_try_wait(bar0 + 8 * (q % PAIR_RING), (olc_u32)((q / PAIR_RING) & 1))) break;
-            return;
-        }
-        if (threadIdx.x == 0) issue_upto(qn - 1);  // input plane z is read for the last time
-    }
-}
-
-// Output rows per CTA of k_substep_march<nt> on a field (0: it does not apply).
-int march_rows(int nt, const int dims[3]) {
-    if (nt <= 0 || dims[0] > 256 || dims[0] % 4 != 0 || dims[0] < 8) return 0;
-    const int rows = nt / (dims[0] / 4);
-    if (rows < 1) return 0;
-    return std::min(std::min(rows, dims[1]), 254);  // a box is at most 256 rows
-}
-
-bool march_threads_known(int nt) { return nt == 0 || nt == 256 || nt == 512 || nt == 1024; }
-
 // The CTA shape of k_substep_pair<nt> on a field: output rows per CTA (0 when
 // the field does not fit: nx > 256, nx % 4 != 0, or fewer than three
 // intermediate rows).
@@ -656,16 +535,12 @@ bool stencil_tile_known(int tile_y, int tile_z) {
 template <int NT>
 static int pair_default_planes(const int dims[3], int ty);
 
-template <int NT>
-static int march_default_planes(const int dims[3], int ty);
-
 bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3], int tile_y, int tile_z, int pair_threads,
-                     int pair_planes, int keep_pct, int march_threads) {
+                     int pair_planes, int keep_pct) {
     m->ok = false;
     m->pair_nt = m->pair_ty = m->pair_zl = 0;
-    m->march_nt = m->march_ty = m->march_zl = 0;
     if (!stencil_tile_known(tile_y, tile_z) || !pair_threads_known(pair_threads) || pair_planes < 0 ||
-        keep_pct < 0 || keep_pct > 100 || !march_threads_known(march_threads))
+        keep_pct < 0 || keep_pct > 100)
         return false;
     m->keep = (int)((long long)dims[2] * keep_pct / 100);
     m->VY = tile_y;
@@ -685,18 +560,6 @@ bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3], int ti
                          : pair_threads == 256 ? pair_default_planes<256>(dims, ty)
                          : pair_threads == 512 ? pair_default_planes<512>(dims, ty)
                                                : pair_default_planes<1024>(dims, ty);
-        }
-    }
-    // one substep per pass as a z march, where the rows fit one box
-    const int mty = march_threads ? march_rows(march_threads, dims) : 0;
-    if (mty > 0) {
-        const cuuint32_t boxm[3] = {(cuuint32_t)dims[0], (cuuint32_t)(mty + 2), 1};
-        if (encode_map(&m->march[0], a, dims, boxm) && encode_map(&m->march[1], b, dims, boxm)) {
-            m->march_nt = march_threads;
-            m->march_ty = mty;
-            m->march_zl = march_threads == 256 ? march_default_planes<256>(dims, mty)
-                          : march_threads == 512 ? march_default_planes<512>(dims, mty)
-                                                 : march_default_planes<1024>(dims, mty);
         }
     }
     return true;
@@ -782,61 +645,8 @@ static void launch_pair(const FieldMaps& m, int cur, float* out, const FieldStep
     }
 }
 
-template <int NT>
-static void configure_march() {
-    static int configured_mask = 0;  // per device (up to 32)
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 32 && !(configured_mask & (1 << dev))) {
-        cudaFuncSetAttribute(k_substep_march<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-        configured_mask |= 1 << dev;
-    }
-}
-
-// Planes per CTA of k_substep_march<NT>: as few as keep every CTA of the grid
-// resident in one wave (at least 8).
-template <int NT>
-static int march_default_planes(const int dims[3], int ty) {
-    configure_march<NT>();
-    int dev = 0, sms = 148, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_substep_march<NT>, NT, march_smem_bytes(dims[0], ty));
-    const int slots = std::max(1, per_sm) * std::max(1, sms);
-    const int gy = (dims[1] + ty - 1) / ty;
-    const int chunks = std::max(1, slots / gy);
-    return std::max(8, (dims[2] + chunks - 1) / chunks);
-}
-
-template <int NT>
-static void launch_march_nt(const FieldMaps& m, int cur, float* out, const FieldStep& fs, olc_u32* status, int rev,
-                            cudaStream_t s) {
-    configure_march<NT>();
-    const int ny = fs.dims[1], nz = fs.dims[2], ty = m.march_ty, zl = m.march_zl;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((ny + ty - 1) / ty, (nz + zl - 1) / zl, 1);
-    cfg.blockDim = dim3(NT);
-    cfg.dynamicSmemBytes = march_smem_bytes(fs.dims[0], ty);
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_substep_march<NT>, m.march[cur], out, fs.dims[0], ny, nz, fs.r, fs.inv_decay, fs.bval,
-                       status, rev, ty, zl, m.keep);
-}
-
 static void launch_single(const FieldMaps& m, int cur, float* out, const FieldStep& fs, olc_u32* status, int rev,
                           cudaStream_t s) {
-    if (m.march_nt) {
-        switch (m.march_nt) {
-            case 256: launch_march_nt<256>(m, cur, out, fs, status, rev, s); break;
-            case 512: launch_march_nt<512>(m, cur, out, fs, status, rev, s); break;
-            default: launch_march_nt<1024>(m, cur, out, fs, status, rev, s); break;
-        }
-        return;
-    }
 #define OLC_VX_LAUNCH(p, q)                                   \
     if (m.VY == p && m.VZ == q) {                             \
         launch_x4<p, q>(m.vec[cur], out, fs, status, rev, m.keep, s); \

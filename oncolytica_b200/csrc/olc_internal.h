@@ -142,20 +142,12 @@ struct FieldMaps {
     int pair_nt = 0, pair_ty = 0, pair_zl = 0;
     CUtensorMap pair[2];
     int keep = 0;  // planes [0, keep) kept L2-resident across substeps by eviction hints (0: none)
-    // one substep per pass as a z march (k_substep_march): threads per CTA (0:
-    // the tile kernel), output rows per CTA, planes per CTA
-    int march_nt = 0, march_ty = 0, march_zl = 0;
-    CUtensorMap march[2];
 };
 // The TMA tensor maps of a FP32 field's two buffers for the (tile_y, tile_z)
 // tile; false when the tile is not compiled in or the field cannot be mapped
 // (the plain kernel runs then).
 bool make_field_maps(FieldMaps* m, float* a, float* b, const int dims[3], int tile_y = 8, int tile_z = 8,
-                     int pair_threads = 0, int pair_planes = 0, int keep_pct = 0, int march_threads = 0);
-// k_substep_march's output rows per CTA of nt threads on a field (0: it does
-// not apply), and whether nt is a compiled CTA size (0 included: off).
-int march_rows(int nt, const int dims[3]);
-bool march_threads_known(int nt);
+                     int pair_threads = 0, int pair_planes = 0, int keep_pct = 0);
 // k_substep_pair's output rows per CTA of nt threads on a field (0: it does
 // not apply), and whether nt is a compiled CTA size (0 included: off).
 int pair_rows(int nt, const int dims[3]);

@@ -69,7 +69,7 @@ struct OlcSim {
     int field_cur[OLC_MAX_FIELDS] = {};
     bool field_bound[OLC_MAX_FIELDS] = {};
     FieldMaps fmaps[OLC_MAX_FIELDS];           // TMA descriptors of both buffers
-    OlcTuning tuning = {8, 8, OLC_CONTACT_FLAT, 16, 0, 0, 0, 0};  // kernel shapes and variants (olc_set_tuning)
+    OlcTuning tuning = {8, 8, OLC_CONTACT_FLAT, 16, 0, 0, 0};  // kernel shapes and variants (olc_set_tuning)
     std::vector<int> member_depth;                    // batched FP32 tile depth per member (0: tuning's)
     FieldMaps16 fmaps16[OLC_MAX_FIELDS];       // the same for 16-bit storage
     float* comp[OLC_MAX_FIELDS] = {};          // 16-bit storage: reaction residual per voxel (FP32)
@@ -1261,8 +1261,7 @@ int olc_bind_field_ex(OlcSim* s, int index, void* a_, void* b_, float* sink, flo
     s->fmaps16[index].ok = false;
     if (spec->substeps > 0 && !half)
         make_field_maps(&s->fmaps[index], a, b, s->geom.chem_dims, s->tuning.stencil_tile_y, s->tuning.stencil_tile_z,
-                        s->tuning.stencil_pair_threads, s->tuning.stencil_pair_planes, s->tuning.stencil_l2_keep_pct,
-                        s->tuning.stencil_march_threads);
+                        s->tuning.stencil_pair_threads, s->tuning.stencil_pair_planes, s->tuning.stencil_l2_keep_pct);
     if (spec->substeps > 0 && half && !make_field_maps16(&s->fmaps16[index], a, b, s->geom.chem_dims))
         return fail(s, OLC_ERR_ARG, "olc_bind_field_ex: TMA descriptors of the 16-bit field failed (16-byte aligned "
                                     "buffers, x extent a multiple of 8)");
@@ -2393,18 +2392,18 @@ static int stage_diffuse(float* f, float* tmp, float* sink, const int32_t dims[3
     std::string err;
     FieldStep fs;
     if (!make_field_step(*spec, dims, dx, dt, &fs, &err)) return fail(nullptr, OLC_ERR_ARG, std::string(who) + ": " + err);
-    const OlcTuning def = {8, 8, OLC_CONTACT_FLAT, 16, 0, 0, 0, 0};
+    const OlcTuning def = {8, 8, OLC_CONTACT_FLAT, 16, 0, 0, 0};
     if (!t) t = &def;
     if (!stencil_tile_known(t->stencil_tile_y, t->stencil_tile_z) || !pair_threads_known(t->stencil_pair_threads) ||
         t->stencil_pair_planes < 0 || t->stencil_pair_planes > 4096 || t->stencil_l2_keep_pct < 0 ||
-        t->stencil_l2_keep_pct > 100 || !march_threads_known(t->stencil_march_threads))
+        t->stencil_l2_keep_pct > 100)
         return fail(nullptr, OLC_ERR_ARG, std::string(who) + ": unknown stencil tile or pair shape");
     cudaStream_t st = as_stream(stream);
     FieldMaps maps;
     olc_u32* status = stage_status_word();
     float* res;
     if (status && make_field_maps(&maps, f, tmp, dims, t->stencil_tile_y, t->stencil_tile_z, t->stencil_pair_threads,
-                                  t->stencil_pair_planes, t->stencil_l2_keep_pct, t->stencil_march_threads)) {
+                                  t->stencil_pair_planes, t->stencil_l2_keep_pct)) {
         launch_sink(f, spec->has_sink ? sink : nullptr, fs, st);
         res = run_substeps_tma(f, tmp, maps, 0, fs, status, st);
     } else {
@@ -2633,8 +2632,6 @@ int olc_set_tuning(OlcSim* s, const OlcTuning* t) {
                                     "stencil_pair_planes in [0, 4096]");
     if (t->stencil_l2_keep_pct < 0 || t->stencil_l2_keep_pct > 100)
         return fail(s, OLC_ERR_ARG, "olc_set_tuning: stencil_l2_keep_pct must be in [0, 100]");
-    if (!march_threads_known(t->stencil_march_threads))
-        return fail(s, OLC_ERR_ARG, "olc_set_tuning: stencil_march_threads must be 0, 256, 512 or 1024");
     OLC_TRY(check(s, cudaDeviceSynchronize(), "sync"));
     drop_graphs(s);
     const bool depth_changed = t->batch_tile_depth != s->tuning.batch_tile_depth;
@@ -2645,7 +2642,7 @@ int olc_set_tuning(OlcSim* s, const OlcTuning* t) {
             if (!s->field_bound[f] || s->fstep[f].storage != OLC_FIELD_F32 || s->fstep[f].substeps == 0) continue;
             make_field_maps(&s->fmaps[f], s->field[0][f], s->field[1][f], s->geom.chem_dims, t->stencil_tile_y,
                             t->stencil_tile_z, t->stencil_pair_threads, t->stencil_pair_planes,
-                            t->stencil_l2_keep_pct, t->stencil_march_threads);
+                            t->stencil_l2_keep_pct);
         }
     } else if (depth_changed && !s->pool) {
         for (olc_u32 f = 0; f < s->caps.n_fields; ++f)

@@ -73,19 +73,6 @@ def test_l2_resident_slab_gives_the_same_bits(cuda, keep):
     _same(eng._backend_impl.snapshot(), ref._backend_impl.snapshot(), f"l2 keep {keep}")
 
 
-@pytest.mark.parametrize("march", [m for m in autotune.MARCH if m] + [256])
-def test_z_march_gives_the_same_bits(cuda, march):
-    spec = _spec()
-    state = W.initial_state(spec)
-    ref = W.build_engine(spec, state)
-    ref.run_steps(3)
-    eng = W.build_engine(spec, state)
-    eng._backend_impl.set_tuning(march_threads=march, l2_keep_pct=45)
-    assert eng._backend_impl.get_tuning()["march_threads"] == march
-    eng.run_steps(3)
-    _same(eng._backend_impl.snapshot(), ref._backend_impl.snapshot(), f"march {march}")
-
-
 @pytest.mark.parametrize("contact", autotune.CONTACT_VARIANTS)
 def test_contact_variants_agree_on_a_dense_population(cuda, contact):
     spec = _spec(dense=True)

@@ -226,16 +226,14 @@ STENCIL_CHOICES = ([(tile, (0, 0), 0) for tile in ((8, 8), (16, 8), (8, 16), (16
                    + [((8, 8), pair, 0) for pair in ((1024, 0), (512, 0), (256, 0), (128, 0), (1024, 9), (512, 13),
                                                      (256, 5), (128, 8))]
                    + [((16, 4), (256, 3), 0)]
-                   + [((8, 8), (0, 0), keep) for keep in (30, 60, 100)] + [((16, 8), (0, 0), 45)]
-                   + [((8, 8), (0, 0), keep, nt) for nt in (256, 512, 1024) for keep in (0, 45)])
+                   + [((8, 8), (0, 0), keep) for keep in (30, 60, 100)] + [((16, 8), (0, 0), 45)])
 
 
 @pytest.mark.parametrize("substeps", [7, 8])
 @pytest.mark.parametrize("dims", [(68, 41, 37), (128, 34, 19), (64, 64, 70), (256, 30, 21), (66, 23, 17)])
 def test_diffuse_every_stencil_choice_bit_exact(cuda, olc, dims, substeps):
     """Every single-pass tile (with and without a slab of planes kept in L2
-    by eviction hints), every one-substep z-march CTA size and every
-    two-substeps-per-pass shape
+    by eviction hints) and every two-substeps-per-pass shape
     (olc_stage_diffuse_tuned) gives the oracle's bits: odd and even substep
     counts (a pair kernel's odd substep is a single pass), ragged tiles and z
     chunks in every direction, rows of 256 voxels where the smallest pair CTA
@@ -249,13 +247,13 @@ def test_diffuse_every_stencil_choice_bit_exact(cuda, olc, dims, substeps):
     spec = _lib.OlcDiffusion(diffusion=1.0, decay=0.02, boundary=0.4, substeps=substeps, has_sink=0)
     dims_c = (C.c_int32 * 3)(nx, ny, nz)
     ref = oracle.diffuse(f, None, dx=1.0, dt=0.5 * substeps / 7, D=1.0, decay=0.02, boundary=0.4, substeps=substeps)
-    for tile, pair, keep, *march in STENCIL_CHOICES:
-        t = _lib.OlcTuning(tile[0], tile[1], 0, 16, pair[0], pair[1], keep, march[0] if march else 0)
+    for tile, pair, keep in STENCIL_CHOICES:
+        t = _lib.OlcTuning(tile[0], tile[1], 0, 16, pair[0], pair[1], keep)
         fd = to_dev(f, cuda)
         tmp = torch.empty_like(fd)
         _lib.check(olc.olc_stage_diffuse_tuned(dptr(fd), dptr(tmp), None, C.byref(dims_c), 1.0, 0.5 * substeps / 7,
                                                C.byref(spec), C.byref(t), None))
-        np.testing.assert_array_equal(to_host(fd), ref, err_msg=f"tile {tile} pair {pair} keep {keep} march {march}")
+        np.testing.assert_array_equal(to_host(fd), ref, err_msg=f"tile {tile} pair {pair} keep {keep}")
 
 
 def test_diffuse_tuned_rejects_unknown_shapes(cuda, olc):
@@ -265,9 +263,8 @@ def test_diffuse_tuned_rejects_unknown_shapes(cuda, olc):
     tmp = torch.empty_like(f)
     spec = _lib.OlcDiffusion(diffusion=1.0, decay=0.0, boundary=0.4, substeps=2, has_sink=0)
     dims_c = (C.c_int32 * 3)(16, 16, 16)
-    for t in (_lib.OlcTuning(8, 8, 0, 16, 64, 0, 0, 0), _lib.OlcTuning(4, 4, 0, 16, 0, 0, 0, 0),
-              _lib.OlcTuning(8, 8, 0, 16, 256, -1, 0, 0), _lib.OlcTuning(8, 8, 0, 16, 0, 0, 101, 0),
-              _lib.OlcTuning(8, 8, 0, 16, 0, 0, 0, 128)):
+    for t in (_lib.OlcTuning(8, 8, 0, 16, 64, 0, 0), _lib.OlcTuning(4, 4, 0, 16, 0, 0, 0),
+              _lib.OlcTuning(8, 8, 0, 16, 256, -1, 0), _lib.OlcTuning(8, 8, 0, 16, 0, 0, 101)):
         rc = olc.olc_stage_diffuse_tuned(dptr(f), dptr(tmp), None, C.byref(dims_c), 1.0, 0.5, C.byref(spec),
                                          C.byref(t), None)
         assert rc == _lib.OLC_ERR_ARG

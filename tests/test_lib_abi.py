@@ -33,7 +33,7 @@ def test_struct_sizes_match_header_layout():
     assert C.sizeof(_lib.OlcCaps) == 4 * 9
     assert C.sizeof(_lib.OlcDiffusion) == 28
     assert C.sizeof(_lib.OlcContact) == 28
-    assert C.sizeof(_lib.OlcTuning) == 4 * 8
+    assert C.sizeof(_lib.OlcTuning) == 4 * 7
     assert C.sizeof(_lib.OlcCounters) == 40
     assert C.sizeof(_lib.OlcProfile) == 16 + 6 * 8
     assert C.sizeof(_lib.OlcPoolConfig) == 4 + 12 + 8 + 8
