@@ -68,14 +68,23 @@ def _load_cache() -> dict:
 
 
 def _store(key: str, value: dict) -> None:
+    """Adds a record to the cache file.  Several processes (one per GPU) may
+    tune at once: each writes its own temporary file and renames it over the
+    cache, and a failed write only loses the record (it is measured again)."""
     with _lock:
         data = _load_cache()
         data[key] = value
-        os.makedirs(os.path.dirname(CACHE), exist_ok=True)
-        tmp = CACHE + ".tmp"
-        with open(tmp, "w") as fh:
-            json.dump(data, fh, indent=1, sort_keys=True)
-        os.replace(tmp, CACHE)
+        tmp = f"{CACHE}.{os.getpid()}.tmp"
+        try:
+            os.makedirs(os.path.dirname(CACHE), exist_ok=True)
+            with open(tmp, "w") as fh:
+                json.dump(data, fh, indent=1, sort_keys=True)
+            os.replace(tmp, CACHE)
+        except OSError:
+            try:
+                os.unlink(tmp)
+            except OSError:
+                pass
 
 
 def _bucket(n: int) -> int:
