@@ -8,9 +8,11 @@ A step is one simulation step of the tumour-spheroid workload (fields, grid,
 rule, contact).  The default workload ``scale`` is 1,000,000 agents with two
 256^3 FP32 fields (O2 and drug).  ``value`` is agent-steps/s of the whole job
 (sum over replicas / max device time over ranks) with the state resident in
-HBM; ``e2e`` runs the same steps through Engine.run_step(collect_metrics=True)
-with a parameter upload from host memory before each step and the metric
-readback after it.  One JSON line is printed by rank 0.
+HBM; ``e2e`` runs the same steps through Engine.run_step(collect_metrics=True,
+wait=False) with a parameter upload from pinned host memory before each step
+and the metric readback after it, each step's metrics read on the host once
+the next step is queued (``value_waiting``: read before it is queued).  One
+JSON line is printed by rank 0.
 
 Multi-GPU: the step does not shard (the stencil and the agents share one
 domain), so N GPUs run N independent replicas (different seeds), no
@@ -393,17 +395,48 @@ def run_b200(args) -> None:
     c2 = be.counters()
     if dist:
         dist.barrier()
+    # each step: params H2D from pinned memory, the step, its metrics D2H;
+    # step k's metrics are read on the host once step k+1 is queued
+    t0 = time.perf_counter()
+    pend = None
+    for _ in range(e2e_steps):
+        eng.update_params(**kw)
+        h = eng.run_step(collect_metrics=True, wait=False)
+        if pend is not None:
+            pend.result()
+        pend = h
+    pend.result()
+    torch.cuda.synchronize(dev)
+    e2e_s = time.perf_counter() - t0
+    c3 = be.counters()
+    e2e_agents = c3["agent_steps"] - c2["agent_steps"]
+    # the same steps on a fresh engine with every step's metrics read before
+    # the next is queued
+    eng.close()
+    del eng, be
+    gc.collect()
+    eng = tuned(W.build_engine(spec, state0))
+    eng.set_graphs(not args.no_graphs)
+    be = eng._backend_impl
+    eng.run_steps(args.warmup)
+    torch.cuda.synchronize(dev)
+    c3w = be.counters()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         eng.update_params(**kw)
         eng.run_step(collect_metrics=True)
     torch.cuda.synchronize(dev)
-    e2e_s = time.perf_counter() - t0
-    c3 = be.counters()
-    e2e_agents = c3["agent_steps"] - c2["agent_steps"]
+    wait_s = time.perf_counter() - t0
+    c4 = be.counters()
+    assert c4["agent_steps"] - c3w["agent_steps"] == e2e_agents, "waiting e2e run diverged from the queued one"
     t2 = torch.tensor([e2e_s, float(e2e_agents)], dtype=torch.float64, device=dev)
     e2e_s, t2 = reduce_over_ranks(dist, t2)
     e2e_value = float(t2[1]) / e2e_s
+    t3 = torch.tensor([wait_s, float(c4["agent_steps"] - c3w["agent_steps"])], dtype=torch.float64, device=dev)
+    wait_s, t3 = reduce_over_ranks(dist, t3)
+    e2e_wait_value = float(t3[1]) / wait_s
     h2d = len(pack_params(be.layout, params))
     d2h = 4 * max(1, len(be.layout.metrics))
     eng.close()
@@ -467,7 +500,12 @@ def run_b200(args) -> None:
         "gpu_launches": int(prof["kernel_launches"]),
         "graphs": not args.no_graphs,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "steps": e2e_steps, "api": "Engine.update_params + Engine.run_step(collect_metrics=True)"},
+                "steps": e2e_steps,
+                "api": "Engine.update_params + Engine.run_step(collect_metrics=True, wait=False); "
+                       "step k's metrics read on the host (PendingReadback.result) after step k+1 is queued",
+                "value_waiting": e2e_wait_value,
+                "api_waiting": "Engine.update_params + Engine.run_step(collect_metrics=True): each step's "
+                               "metrics read before the next step is queued (same steps, fresh engine)"},
         "clocks": clk,
         "status": c1["status"],
         "tuning": autotune.summary(tuning) if tuning["tuning"] else "defaults (--no-tune)",
@@ -547,7 +585,8 @@ def recorded_runs() -> dict | None:
 def summarise(line: dict) -> dict:
     """The headline figures of a line's nested measurements, short, printed
     last so that a log that keeps only the end of the line still shows them."""
-    out = {"agent_steps_per_s": line["value"], "e2e": line["e2e"]["value"], "roofline_frac": line["roofline"]["frac"]}
+    out = {"agent_steps_per_s": line["value"], "e2e": line["e2e"]["value"],
+           "e2e_waiting": line["e2e"].get("value_waiting"), "roofline_frac": line["roofline"]["frac"]}
     if line.get("cpu_baseline"):
         out["cpu_port"] = line["cpu_baseline"]["value"]
     for st, r in (line.get("batched") or {}).items():

@@ -450,6 +450,20 @@ int olc_engine_metrics(OlcSim* sim, const OlcEngineMetricsSpec* spec, double* ou
 int olc_read_reductions(OlcSim* sim, OlcReductions* out, void* stream);
 int olc_read_user_metrics(OlcSim* sim, void* out, size_t bytes, void* stream);
 
+/* Readback without waiting (solo handles; replaces the same readbacks of the
+ * reference, _gpu_backend.py:166-169, for callers that queue the next step
+ * before reading this one's results).  olc_queue_readback queues, on
+ * `stream`, copies of the counter block and of the metric accumulators into
+ * one of 4 pinned host slots and returns a ticket; olc_take_readback waits
+ * for that ticket's copies only and returns the first `bytes` of the
+ * accumulators and the counters (either output may be NULL / 0 bytes).  The
+ * 4 slots rotate: a ticket is taken before 4 later ones are queued, or its
+ * take fails with OLC_ERR_STATE.  olc_set_params likewise rotates over 4
+ * pinned staging slots and so waits for no earlier copy but the one 4
+ * uploads back. */
+int olc_queue_readback(OlcSim* sim, void* stream, uint64_t* ticket);
+int olc_take_readback(OlcSim* sim, uint64_t ticket, void* metrics_out, size_t bytes, OlcCounters* counters);
+
 /* Copies the life flags of rows [0, rows) (0 alive, 1 died this step) to host
  * memory; sync_to_host drops dead rows as the reference's sort does
  * (template.wgsl:152-159). */

@@ -34,6 +34,8 @@ OLC_MAX_FIELDS = 8
 OLC_MAX_RULES = 16
 OLC_RADIAL_BINS = 64
 OLC_STATE_BINS = 8
+# pinned host slots of olc_queue_readback / olc_take_readback
+READBACK_SLOTS = 4
 
 # Every symbol include/olc.h declares (the loader checks each one).
 EXPORTS = (
@@ -55,7 +57,7 @@ EXPORTS = (
     "olc_stage_contact_mech", "olc_stage_contact_motion", "olc_bind_tissue_pair", "olc_current_tissue", "olc_set_rule_iterations",
     "olc_set_pinned", "olc_stage_diffuse_pinned", "olc_sort_noalloc_status", "olc_sort_status_offset",
     "olc_selftest_bounded_waits", "olc_set_tuning", "olc_get_tuning", "olc_set_batch_tile_depths",
-    "olc_stage_diffuse_tuned", "olc_stage_contact_tuned",
+    "olc_stage_diffuse_tuned", "olc_stage_contact_tuned", "olc_queue_readback", "olc_take_readback",
 )
 
 
@@ -130,7 +132,14 @@ class StatusWatch:
         self.check()
 
     def check(self) -> int:
-        bits = int(self.read_status())
+        return self.report(int(self.read_status()))
+
+    def report(self, bits: int) -> int:
+        """The check of ``check`` on a status word read elsewhere (a queued
+        readback's counters)."""
+        if self.policy == "ignore":
+            return bits
+        bits = int(bits)
         new = bits & ~self.seen
         self.seen |= bits
         if new:
@@ -354,6 +363,8 @@ _SIGS = {
     "olc_read_counters": (C.c_int, [_VP, C.POINTER(OlcCounters), _VP]),
     "olc_read_reductions": (C.c_int, [_VP, C.POINTER(OlcReductions), _VP]),
     "olc_read_user_metrics": (C.c_int, [_VP, _VP, C.c_size_t, _VP]),
+    "olc_queue_readback": (C.c_int, [_VP, _VP, C.POINTER(C.c_uint64)]),
+    "olc_take_readback": (C.c_int, [_VP, C.c_uint64, _VP, C.c_size_t, C.POINTER(OlcCounters)]),
     "olc_create_batch": (C.c_int, [C.POINTER(OlcGeom), C.c_int, C.POINTER(OlcCaps), C.POINTER(_VP)]),
     "olc_batch_field_offsets": (C.c_int, [_VP, C.POINTER(C.c_uint64)]),
     "olc_bind_field_batch": (C.c_int, [_VP, C.c_int, _VP, _VP, _VP, _VP, C.POINTER(OlcDiffusion)]),

@@ -11,7 +11,7 @@ pointers.  Replaces GpuBackend (framework/src/oncolytica/gpu/runtime/_gpu_backen
 from __future__ import annotations
 
 import ctypes as C
-from typing import Any
+from typing import Any, Optional
 
 import numpy as np
 
@@ -41,6 +41,34 @@ def seed_rng(seed: int, idx: np.ndarray) -> np.ndarray:
     return h | np.uint32(1)
 
 
+class PendingReadback:
+    """The results of a collected step whose copies are queued on the stream
+    (``Engine.run_step(collect_metrics=True, wait=False)``): ``result()``
+    waits for those copies only, checks the device status word they carry,
+    writes the metric values into the engine's metrics object (unless a newer
+    step's are already there) and returns them as a dict."""
+
+    def __init__(self, backend: "CudaBackend", ticket: int):
+        self._backend = backend
+        self.ticket = ticket
+        self._values: dict | None = None
+        self.counters: dict | None = None
+
+    def result(self) -> dict:
+        if self._values is not None:
+            return self._values
+        be = self._backend
+        if self in be._pending:
+            be._pending.remove(self)
+        words, c = be._take_readback(self.ticket)
+        self._values = be._decode_metrics(words)
+        self.counters = {"n_agents": c.n_agents, "births": c.births, "deaths": c.deaths, "status": c.status,
+                         "steps": c.steps, "agent_steps": c.agent_steps}
+        be._apply_metrics(self.ticket, self._values)
+        be.status.report(c.status)
+        return self._values
+
+
 class CudaBackend:
     """ISimulationBackend on CUDA: compile / run_step / sync_to_host / sync_to_device / get_metrics."""
 
@@ -63,6 +91,8 @@ class CudaBackend:
         self.tissue_pair = None
         self._params_dirty = True
         self._last_reductions: dict | None = None
+        self._pending: list = []          # PendingReadback, oldest first
+        self._applied_ticket = 0          # newest readback written into the engine's metrics
         self.status = _lib.StatusWatch(lambda: self.counters()["status"], "CudaBackend.run_steps",
                                        every=engine.status_check_every, policy=engine.on_device_status)
 
@@ -245,44 +275,83 @@ class CudaBackend:
         buf = C.create_string_buffer(blob, len(blob))
         self._check(self.lib.olc_set_params(self.handle, C.cast(buf, C.c_void_p), len(blob), self._stream()))
 
-    def run_step(self, collect_metrics: bool = False) -> None:
-        self.run_steps(1, collect_metrics)
+    def run_step(self, collect_metrics: bool = False, wait: bool = True) -> Optional["PendingReadback"]:
+        return self.run_steps(1, collect_metrics, wait)
 
-    def run_steps(self, n: int, collect_metrics: bool = False) -> None:
+    def run_steps(self, n: int, collect_metrics: bool = False, wait: bool = True) -> Optional["PendingReadback"]:
         """n steps; the device status word is checked every
-        ``Engine.status_check_every`` steps and after every collected step
-        (StatusWatch: DeviceStatusError on new bits)."""
+        ``Engine.status_check_every`` steps and with every collected step's
+        results (StatusWatch: DeviceStatusError on new bits).  A collected
+        step queues the copies of its metric accumulators and counters
+        (olc_queue_readback); ``wait`` takes them at once, otherwise the
+        returned PendingReadback takes them when asked, so that the caller
+        can queue the next step first."""
         self.status.every = max(1, int(self.engine.status_check_every))
         self.status.policy = self.engine.on_device_status
         chunks = list(self.status.chunks(n))
+        pend = None
         for i, k in enumerate(chunks):
             last = i == len(chunks) - 1
             self._check(self.lib.olc_step(self.handle, int(k), int(bool(collect_metrics and last)), self._stream()))
             if collect_metrics and last:
-                self._read_metrics()
-            self.status.after(k, synced=collect_metrics and last)
+                pend = self._queue_readback()
+                self.status.since = 0
+            else:
+                self.status.after(k)
+        if pend is not None and wait:
+            pend.result()
+            return None
+        return pend
 
-    def _read_metrics(self) -> None:
-        L = self.layout
-        nm = max(1, len(L.metrics))
+    def _queue_readback(self) -> "PendingReadback":
+        # a ticket must be taken before READBACK_SLOTS later ones are queued
+        while len(self._pending) >= _lib.READBACK_SLOTS - 1:
+            self._pending[0].result()
+        t = C.c_uint64()
+        self._check(self.lib.olc_queue_readback(self.handle, self._stream(), C.byref(t)))
+        pend = PendingReadback(self, int(t.value))
+        self._pending.append(pend)
+        return pend
+
+    def resolve_pending(self) -> None:
+        """Takes every queued readback (oldest first)."""
+        while self._pending:
+            self._pending[0].result()
+
+    def _take_readback(self, ticket: int) -> tuple:
+        nm = max(1, len(self.layout.metrics))
         raw = (C.c_uint32 * nm)()
-        self._check(self.lib.olc_read_user_metrics(self.handle, C.cast(raw, C.c_void_p), 4 * nm, self._stream()))
-        words = np.frombuffer(bytes(raw), dtype=np.uint32)
-        m = self.engine._metrics
-        for name, (slot, ty) in L.metrics.items():
+        c = _lib.OlcCounters()
+        self._check(self.lib.olc_take_readback(self.handle, ticket, C.cast(raw, C.c_void_p), 4 * nm, C.byref(c)))
+        return np.frombuffer(bytes(raw), dtype=np.uint32), c
+
+    def _decode_metrics(self, words) -> dict:
+        out = {}
+        for name, (slot, ty) in self.layout.metrics.items():
             w = words[slot:slot + 1]
             if ty == "f32":
-                v = np.float32(w.view(np.float32)[0])
+                out[name] = np.float32(w.view(np.float32)[0])
             elif ty == "u32":
-                v = int(w[0])
+                out[name] = int(w[0])
             elif ty == "bool":
-                v = bool(w.view(np.int32)[0])
+                out[name] = bool(w.view(np.int32)[0])
             else:
-                v = int(w.view(np.int32)[0])
+                out[name] = int(w.view(np.int32)[0])
+        return out
+
+    def _apply_metrics(self, ticket: int, values: dict) -> None:
+        """Writes a readback's metric values into the engine's metrics object
+        unless a newer readback has already been written there."""
+        if ticket < self._applied_ticket:
+            return
+        self._applied_ticket = ticket
+        m = self.engine._metrics
+        for name, v in values.items():
             object.__setattr__(m, name, v)
         self._last_reductions = None
 
     def get_metrics(self) -> Any:
+        self.resolve_pending()
         return self.engine._metrics
 
     def counters(self) -> dict:
@@ -713,6 +782,7 @@ class CudaBackend:
         if self.handle:
             self.lib.olc_destroy(self.handle)
             self.handle = C.c_void_p()
+        self._pending = []
         self.cols_dev, self.fields_dev, self.comp_dev = [], [], []
         self.tissue_dev = self.tissue_pair = None
 

@@ -436,6 +436,8 @@ class Translator:
 
         src = "\n".join([
             "// Generated by oncolytica_b200.compiler from the model's Python rules.",
+            # solo metric rules add into per-block shared accumulators
+            "" if self.L.batched else f"#define OLC_SOLO_METRIC_WORDS {max(1, len(self.L.metrics))}",
             '#include "olc_rule_rt.cuh"',
             # rule bodies see the whole argument block, or one simulation of a batch
             "typedef OlcSimView OlcP;" if self.L.batched else "typedef OlcRuleParams OlcP;",
@@ -732,8 +734,26 @@ class Translator:
 }}"""
 
     def metric_kernel(self, kname: str, fn: str) -> str:
+        if self.L.batched:
+            clear = flush = ""
+        else:
+            # a solo handle's block adds its shared accumulators (cleared
+            # first) to the metric words once, one thread per word
+            clear = """    for (int k = threadIdx.x; k < OLC_SOLO_METRIC_WORDS; k += blockDim.x) olc_s_metrics[k] = 0u;
+    __syncthreads();
+"""
+            adds = []
+            for slot, ty in sorted(self.L.metrics.values()):
+                if ty == F32:
+                    add = (f"const float v = __uint_as_float(olc_s_metrics[{slot}]); "
+                           f"if (v != 0.0f) atomicAdd(reinterpret_cast<float*>(P.metrics) + {slot}, v);")
+                else:
+                    add = (f"const olc_u32 v = olc_s_metrics[{slot}]; "
+                           f"if (v != 0u) atomicAdd(reinterpret_cast<olc_u32*>(P.metrics) + {slot}, v);")
+                adds.append(f"    if (threadIdx.x == {slot} % OLC_RULE_THREADS) {{ {add} }}")
+            flush = "    __syncthreads();\n" + "\n".join(adds) + "\n"
         return f"""extern "C" __global__ void __launch_bounds__(OLC_RULE_THREADS) {kname}(OlcRuleParams P) {{
-    const olc_u32 rows = olc_total_rows(P.counters);
+{clear}    const olc_u32 rows = olc_total_rows(P.counters);
     for (olc_u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {{
         if (P.life[i]) continue;
 {self.view_decl("true")}
@@ -746,7 +766,7 @@ class Translator:
         ctx.multi = false;
         {fn}({self.pv}, rng, ctx, c);
     }}
-}}"""
+{flush}}}"""
 
 
 def mutated_names(node: ast.FunctionDef) -> set:

@@ -76,28 +76,47 @@ __global__ void __launch_bounds__(256) k_reduce_agents(ReduceArgs a, const olc_u
     __syncthreads();
     double sx = 0.0, sy = 0.0, sz = 0.0, sr2 = 0.0, mr = 0.0;
     olc_u32 live = 0;
-    for (olc_u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        if (a.life[i]) continue;
-        const float px = a.x[i], py = a.y[i], pz = a.z[i];
-        ++live;
-        sx += (double)px;
-        sy += (double)py;
-        sz += (double)pz;
-        const double dx = (double)px - (double)a.cx, dy = (double)py - (double)a.cy,
-                     dz = (double)pz - (double)a.cz;
-        const double r2 = dx * dx + dy * dy + dz * dz;
-        sr2 += r2;
-        const double r = sqrt(r2);
-        mr = fmax(mr, r);
-        int b = (int)(r / (double)a.bin_width);
-        if (b >= OLC_RADIAL_BINS) b = OLC_RADIAL_BINS - 1;
-        atomicAdd(&s_hist[b], 1u);
-        if (a.state) {
-            int st = a.state[i];
-            if (st >= 0 && st < OLC_STATE_BINS) atomicAdd(&s_state[st], 1u);
-        }
-    }
+    // per-thread state counts in registers; every row's loads are issued
+    // together (the life flag does not gate the position loads), and the lanes
+    // of a warp that fall into one radial bin (neighbouring rows, sorted by
+    // voxel) add to it once
+    olc_u32 sc[OLC_STATE_BINS];
+#pragma unroll
+    for (int k = 0; k < OLC_STATE_BINS; ++k) sc[k] = 0u;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const olc_u32 stride = gridDim.x * blockDim.x;
+    const olc_u32 first = blockIdx.x * blockDim.x + threadIdx.x;
+    for (olc_u32 base = first - lane; base < n; base += stride) {
+        const olc_u32 i = base + lane;
+        const bool row = i < n;
+        const bool dead = row ? a.life[i] != 0 : true;
+        const float px = row ? a.x[i] : 0.0f, py = row ? a.y[i] : 0.0f, pz = row ? a.z[i] : 0.0f;
+        const int st = (row && a.state) ? a.state[i] : -1;
+        int b = -1;
+        if (!dead) {
+            ++live;
+            sx += (double)px;
+            sy += (double)py;
+            sz += (double)pz;
+            const double dx = (double)px - (double)a.cx, dy = (double)py - (double)a.cy,
+                         dz = (double)pz - (double)a.cz;
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            sr2 += r2;
+            const double r = sqrt(r2);
+            mr = fmax(mr, r);
+            b = (int)(r / (double)a.bin_width);
+            if (b >= OLC_RADIAL_BINS) b = OLC_RADIAL_BINS - 1;
+#pragma unroll
+            for (int k = 0; k < OLC_STATE_BINS; ++k) sc[k] += st == k ? 1u : 0u;
+        }
+        const olc_u32 peers = __match_any_sync(0xffffffffu, b);
+        if (b >= 0 && lane == __ffs(peers) - 1) atomicAdd(&s_hist[b], (olc_u32)__popc(peers));
+    }
+#pragma unroll
+    for (int k = 0; k < OLC_STATE_BINS; ++k) {
+        const olc_u32 t = __reduce_add_sync(0xffffffffu, sc[k]);
+        if (lane == 0 && t) atomicAdd(&s_state[k], t);
+    }
     sx = warp_sum_d(sx);
     sy = warp_sum_d(sy);
     sz = warp_sum_d(sz);
@@ -155,12 +174,32 @@ __global__ void __launch_bounds__(256) k_reduce_field(const float* __restrict__ 
     double sum = 0.0, mn = 1e300, mx = 0.0;
     const size_t n4 = nvox / 4;
     const float4* f4 = reinterpret_cast<const float4*>(f);
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
-        float4 v = __ldg(f4 + i);
-        sum += ((double)v.x + (double)v.y) + ((double)v.z + (double)v.w);
-        mn = fmin(mn, fmin(fmin((double)v.x, (double)v.y), fmin((double)v.z, (double)v.w)));
-        mx = fmax(mx, fmax(fmax((double)v.x, (double)v.y), fmax((double)v.z, (double)v.w)));
+    // four independent 16-byte loads in flight per thread and iteration (one
+    // at a time left the kernel waiting on DRAM latency at half the copy
+    // rate); the minimum and maximum in FP32 (exact), the sum in FP64 in a
+    // fixed order
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    float lo = __int_as_float(0x7f800000), hi = 0.0f;
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < n4; i += 4 * stride) {
+        float4 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = __ldg(f4 + i + u * stride);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            sum += ((double)v[u].x + (double)v[u].y) + ((double)v[u].z + (double)v[u].w);
+            lo = fminf(lo, fminf(fminf(v[u].x, v[u].y), fminf(v[u].z, v[u].w)));
+            hi = fmaxf(hi, fmaxf(fmaxf(v[u].x, v[u].y), fmaxf(v[u].z, v[u].w)));
+        }
     }
+    for (; i < n4; i += stride) {
+        const float4 v = __ldg(f4 + i);
+        sum += ((double)v.x + (double)v.y) + ((double)v.z + (double)v.w);
+        lo = fminf(lo, fminf(fminf(v.x, v.y), fminf(v.z, v.w)));
+        hi = fmaxf(hi, fmaxf(fmaxf(v.x, v.y), fmaxf(v.z, v.w)));
+    }
+    mn = fmin(mn, (double)lo);
+    mx = fmax(mx, (double)hi);
     if (blockIdx.x == 0) {
         for (size_t i = n4 * 4 + threadIdx.x; i < nvox; i += blockDim.x) {
             double v = (double)f[i];

@@ -390,6 +390,27 @@ __device__ __forceinline__ void olc_metric_add_f(const PT& P, int slot, float v)
     if (v != 0.0f) atomicAdd(reinterpret_cast<float*>(P.metrics) + slot, v);
 }
 
+#ifdef OLC_SOLO_METRIC_WORDS
+// Solo handles: every lane of a block adds to the same words, so a metric
+// rule accumulates into the block's words in shared memory (its kernel clears
+// them first and adds them to the handle's words once at its end); integer
+// adds are still reduced across the converged lanes first.
+__shared__ olc_u32 olc_s_metrics[OLC_SOLO_METRIC_WORDS];
+__device__ __forceinline__ void olc_metric_add_i(const OlcRuleParams&, int slot, int v) {
+    const olc_u32 m = __activemask();
+    const int s = __reduce_add_sync(m, v);
+    if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && s != 0) atomicAdd(reinterpret_cast<int*>(olc_s_metrics) + slot, s);
+}
+__device__ __forceinline__ void olc_metric_add_u(const OlcRuleParams&, int slot, olc_u32 v) {
+    const olc_u32 m = __activemask();
+    const olc_u32 s = __reduce_add_sync(m, v);
+    if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && s != 0u) atomicAdd(olc_s_metrics + slot, s);
+}
+__device__ __forceinline__ void olc_metric_add_f(const OlcRuleParams&, int slot, float v) {
+    if (v != 0.0f) atomicAdd(reinterpret_cast<float*>(olc_s_metrics) + slot, v);
+}
+#endif
+
 // Block-wide birth scan + decoupled look-back.  Returns the row of this
 // thread's child (or 0xffffffff when it has none).  All threads must call it.
 __device__ __forceinline__ olc_u32 olc_birth_slot(const OlcRuleParams& P, bool born, olc_u32 tile,

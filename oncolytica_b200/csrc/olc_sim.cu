@@ -42,6 +42,8 @@ int cuda_status(cudaError_t e, const char* what) {
 using namespace olc;
 
 #define OLC_PROF_EVENTS 7
+// pinned host slots of the params upload ring and of the readback ring
+constexpr int HOST_SLOTS = 4;
 
 struct StepGraph {
     int key = 0;  // (agent buffer << 16) | (tissue buffer << 12) | (field parity mask << 1) | collect
@@ -106,6 +108,19 @@ struct OlcSim {
     void* metrics_dev = nullptr;
     size_t metrics_bytes = 0;
     olc_u32* ctr_host_words = nullptr;     // pinned copy of the counter block
+    // solo handles: params uploads rotate over HOST_SLOTS pinned staging
+    // slots of params_cap bytes, each reused once the copy that last read it
+    // has run (param_ev), so an upload never waits for the stream
+    cudaEvent_t param_ev[HOST_SLOTS] = {};
+    olc_u64 param_seq = 0;
+    // queued readbacks (olc_queue_readback): slot k of rb_host holds the
+    // counter block then the metric accumulators of ticket rb_ticket[k]
+    unsigned char* rb_host = nullptr;      // pinned, HOST_SLOTS x rb_stride
+    size_t rb_stride = 0;
+    cudaEvent_t rb_ev[HOST_SLOTS] = {};
+    olc_u64 rb_ticket[HOST_SLOTS] = {};
+    olc_u64 rb_steps[HOST_SLOTS] = {};
+    olc_u64 rb_next = 1;
     EngineMetricAcc* em_acc = nullptr;     // engine metrics (allocated on first use)
     double* em_partials = nullptr;
     EngineMetricAcc* em_host = nullptr;    // pinned
@@ -1202,6 +1217,11 @@ int olc_destroy(OlcSim* s) {
     }
     cudaFree(s->metrics_dev);
     if (s->params_host) cudaFreeHost(s->params_host);
+    if (s->rb_host) cudaFreeHost(s->rb_host);
+    for (int i = 0; i < HOST_SLOTS; ++i) {
+        if (s->param_ev[i]) cudaEventDestroy(s->param_ev[i]);
+        if (s->rb_ev[i]) cudaEventDestroy(s->rb_ev[i]);
+    }
     if (s->red_host) cudaFreeHost(s->red_host);
     if (s->ctr_host_words) cudaFreeHost(s->ctr_host_words);
     cudaFree(s->em_acc);
@@ -1494,22 +1514,28 @@ int olc_set_params(OlcSim* s, const void* blob, size_t bytes, void* stream) {
     cudaStream_t st = as_stream(stream);
     if (bytes > s->params_cap) {
         drop_graphs(s);
-        cudaStreamSynchronize(st);
+        OLC_TRY(check(s, cudaStreamSynchronize(st), "sync before params reallocation"));
         cudaFree(s->params_dev);
         if (s->params_host) cudaFreeHost(s->params_host);
         s->params_dev = nullptr;
         s->params_host = nullptr;
         size_t cap = (bytes + 255) & ~size_t(255);
         OLC_TRY(dev_alloc(s, &s->params_dev, cap, "params"));
-        OLC_TRY(check(s, cudaMallocHost(reinterpret_cast<void**>(&s->params_host), cap), "pinned params"));
+        OLC_TRY(check(s, cudaMallocHost(reinterpret_cast<void**>(&s->params_host), cap * HOST_SLOTS),
+                      "pinned params"));
         s->params_cap = cap;
-    } else {
-        // the staging buffer may still feed an earlier copy
-        OLC_TRY(check(s, cudaStreamSynchronize(st), "sync before params upload"));
     }
-    std::memcpy(s->params_host, blob, bytes);
-    return check(s, cudaMemcpyAsync(s->params_dev, s->params_host, bytes, cudaMemcpyHostToDevice, st),
-                 "params upload");
+    // the slot's previous copy was queued HOST_SLOTS uploads ago: wait for it
+    // (normally long done) instead of for the whole stream
+    const int slot = (int)(s->param_seq % HOST_SLOTS);
+    if (s->param_ev[slot]) OLC_TRY(check(s, cudaEventSynchronize(s->param_ev[slot]), "params staging reuse"));
+    else OLC_TRY(check(s, cudaEventCreateWithFlags(&s->param_ev[slot], cudaEventDisableTiming), "params event"));
+    unsigned char* h = s->params_host + (size_t)slot * s->params_cap;
+    std::memcpy(h, blob, bytes);
+    OLC_TRY(check(s, cudaMemcpyAsync(s->params_dev, h, bytes, cudaMemcpyHostToDevice, st), "params upload"));
+    OLC_TRY(check(s, cudaEventRecord(s->param_ev[slot], st), "params event"));
+    s->param_seq++;
+    return OLC_OK;
 }
 
 int olc_set_user_metrics_size(OlcSim* s, size_t bytes) {
@@ -1630,13 +1656,8 @@ int olc_step(OlcSim* s, int nsteps, int collect, void* stream) {
     return OLC_OK;
 }
 
-int olc_read_counters(OlcSim* s, OlcCounters* out, void* stream) {
-    if (!s || !out) return fail(s, OLC_ERR_ARG, "olc_read_counters: null argument");
-    cudaStream_t st = as_stream(stream);
-    OLC_TRY(check(s, cudaMemcpyAsync(s->ctr_host_words, s->counters, OLC_CTR_WORDS * 4, cudaMemcpyDeviceToHost, st),
-                  "counters readback"));
-    OLC_TRY(check(s, cudaStreamSynchronize(st), "sync"));
-    const olc_u32* w = s->ctr_host_words;
+// OlcCounters from a copy of the device counter block.
+static void counters_from_words(const olc_u32* w, uint64_t steps, OlcCounters* out) {
     olc_u32 births = 0;
     for (int j = 0; j < OLC_MAX_RULE_KERNELS; ++j) births += w[OLC_CTR_BIRTHS + j];
     out->n_agents = w[OLC_CTR_N] + births;
@@ -1645,8 +1666,64 @@ int olc_read_counters(OlcSim* s, OlcCounters* out, void* stream) {
     out->deaths = w[OLC_CTR_DEAD];
     out->status = w[OLC_CTR_STATUS];
     out->pad = 0;
-    out->steps = s->steps;
+    out->steps = steps;
     out->agent_steps = (uint64_t)w[OLC_CTR_AGENT_STEPS] | ((uint64_t)w[OLC_CTR_AGENT_STEPS + 1] << 32);
+}
+
+int olc_read_counters(OlcSim* s, OlcCounters* out, void* stream) {
+    if (!s || !out) return fail(s, OLC_ERR_ARG, "olc_read_counters: null argument");
+    cudaStream_t st = as_stream(stream);
+    OLC_TRY(check(s, cudaMemcpyAsync(s->ctr_host_words, s->counters, OLC_CTR_WORDS * 4, cudaMemcpyDeviceToHost, st),
+                  "counters readback"));
+    OLC_TRY(check(s, cudaStreamSynchronize(st), "sync"));
+    counters_from_words(s->ctr_host_words, s->steps, out);
+    return OLC_OK;
+}
+
+int olc_queue_readback(OlcSim* s, void* stream, uint64_t* ticket) {
+    if (!s || !ticket) return fail(s, OLC_ERR_ARG, "olc_queue_readback: null argument");
+    if (s->n_sims) return fail(s, OLC_ERR_STATE, "olc_queue_readback: batch handle");
+    cudaStream_t st = as_stream(stream);
+    const size_t ctr_bytes = OLC_CTR_WORDS * 4;
+    const size_t stride = (ctr_bytes + s->metrics_bytes + 63) & ~size_t(63);
+    if (stride != s->rb_stride) {
+        // metric size changed: every queued copy lands before the ring goes
+        for (int i = 0; i < HOST_SLOTS; ++i) {
+            if (s->rb_ev[i]) OLC_TRY(check(s, cudaEventSynchronize(s->rb_ev[i]), "readback reuse"));
+            s->rb_ticket[i] = 0;
+        }
+        if (s->rb_host) cudaFreeHost(s->rb_host);
+        s->rb_host = nullptr;
+        s->rb_stride = 0;
+        OLC_TRY(check(s, cudaMallocHost(reinterpret_cast<void**>(&s->rb_host), stride * HOST_SLOTS), "pinned readback"));
+        s->rb_stride = stride;
+    }
+    const int slot = (int)(s->rb_next % HOST_SLOTS);
+    if (s->rb_ev[slot]) OLC_TRY(check(s, cudaEventSynchronize(s->rb_ev[slot]), "readback reuse"));
+    else OLC_TRY(check(s, cudaEventCreateWithFlags(&s->rb_ev[slot], cudaEventDisableTiming), "readback event"));
+    unsigned char* h = s->rb_host + (size_t)slot * s->rb_stride;
+    s->rb_ticket[slot] = 0;
+    OLC_TRY(check(s, cudaMemcpyAsync(h, s->counters, ctr_bytes, cudaMemcpyDeviceToHost, st), "counters readback"));
+    if (s->metrics_bytes)
+        OLC_TRY(check(s, cudaMemcpyAsync(h + ctr_bytes, s->metrics_dev, s->metrics_bytes, cudaMemcpyDeviceToHost, st),
+                      "metrics readback"));
+    OLC_TRY(check(s, cudaEventRecord(s->rb_ev[slot], st), "readback event"));
+    s->rb_ticket[slot] = s->rb_next;
+    s->rb_steps[slot] = s->steps;
+    *ticket = s->rb_next++;
+    return OLC_OK;
+}
+
+int olc_take_readback(OlcSim* s, uint64_t ticket, void* metrics_out, size_t bytes, OlcCounters* counters) {
+    if (!s || (bytes && !metrics_out)) return fail(s, OLC_ERR_ARG, "olc_take_readback: bad arguments");
+    if (bytes > s->metrics_bytes) return fail(s, OLC_ERR_ARG, "olc_take_readback: more bytes than allocated");
+    const int slot = (int)(ticket % HOST_SLOTS);
+    if (ticket == 0 || s->rb_ticket[slot] != ticket)
+        return fail(s, OLC_ERR_STATE, "olc_take_readback: unknown ticket, or its slot was reused by a later one");
+    OLC_TRY(check(s, cudaEventSynchronize(s->rb_ev[slot]), "readback wait"));
+    const unsigned char* h = s->rb_host + (size_t)slot * s->rb_stride;
+    if (bytes) std::memcpy(metrics_out, h + OLC_CTR_WORDS * 4, bytes);
+    if (counters) counters_from_words(reinterpret_cast<const olc_u32*>(h), s->rb_steps[slot], counters);
     return OLC_OK;
 }
 

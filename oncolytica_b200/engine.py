@@ -352,18 +352,24 @@ class Engine:
                 raise CompilationError(f"setup_diffusion: chemistry class has no field {f!r}")
 
     # ---- execution ---------------------------------------------------------
-    def run_step(self, collect_metrics: bool = False) -> None:
+    def run_step(self, collect_metrics: bool = False, wait: bool = True):
+        """One step.  With ``collect_metrics`` the step's metric values reach
+        the host: at once (``wait``, as the reference), or, with
+        ``wait=False``, through the returned PendingReadback, whose
+        ``result()`` (or the next get_metrics()) waits for that step's copies
+        only, so the caller can queue the next step before reading this one."""
         if self._sim is None or self._backend_impl is None:
             raise RuntimeError("Engine.run_step() called before load_model().")
         self._step += 1
-        self._backend_impl.run_step(collect_metrics=collect_metrics)
+        return self._backend_impl.run_steps(1, collect_metrics=collect_metrics, wait=wait)
 
-    def run_steps(self, n: int, collect_metrics: bool = False) -> None:
-        """n steps enqueued back to back (metrics after the last when asked)."""
+    def run_steps(self, n: int, collect_metrics: bool = False, wait: bool = True):
+        """n steps enqueued back to back (metrics after the last when asked;
+        ``wait`` as in run_step)."""
         if self._sim is None or self._backend_impl is None:
             raise RuntimeError("Engine.run_steps() called before load_model().")
         self._step += n
-        self._backend_impl.run_steps(n, collect_metrics=collect_metrics)
+        return self._backend_impl.run_steps(n, collect_metrics=collect_metrics, wait=wait)
 
     def set_graphs(self, enable: bool) -> None:
         """Runs later steps through cached CUDA graphs of whole steps (no
@@ -373,6 +379,8 @@ class Engine:
             self._backend_impl.set_graphs(self.use_graphs)
 
     def get_metrics(self) -> Any:
+        if self._backend_impl is not None and hasattr(self._backend_impl, "resolve_pending"):
+            self._backend_impl.resolve_pending()
         return self._metrics
 
     def get_engine_metrics(self, **kw: Any) -> dict:

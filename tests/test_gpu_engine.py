@@ -692,3 +692,56 @@ def test_tumour_step_parity_16bit_fields(cuda, storage, code):
         for a, key in (("pos.x", "x"), ("pos.y", "y"), ("pos.z", "z")):
             np.testing.assert_allclose(got["cols"][a], orc.bufs[key][:n], rtol=0, atol=1e-4)
         np.testing.assert_array_equal(got["sinks"]["o2"], orc.o2_sink.ravel())
+
+
+def test_queued_readbacks_match_waiting_steps(cuda):
+    """Steps whose metrics are read one step late (run_step(collect_metrics=True,
+    wait=False), the next step queued before the previous result is taken)
+    give every step's metrics and counters exactly as waiting steps do, with
+    a parameter changed before each step (the pinned upload ring keeps each
+    upload's bytes until its copy ran); both engines end in the same state."""
+    from oncolytica_b200 import _lib
+
+    spec = W.scaled(_parity_spec(), n_agents=5000)
+    a, b = W.build_engine(spec), W.build_engine(spec)
+    for eng in (a, b):
+        eng.set_graphs(True)
+    want, got, pend = [], [], None
+    for step in range(12):
+        growth = 0.05 + 0.01 * (step % 5)
+        a.update_params(growth=growth)
+        a.run_step(collect_metrics=True)
+        want.append((metric_fields_values(a.get_metrics()), a._backend_impl.counters()["agent_steps"]))
+        b.update_params(growth=growth)
+        h = b.run_step(collect_metrics=True, wait=False)
+        assert h is not None
+        if pend is not None:
+            got.append((pend.result(), pend.counters["agent_steps"]))
+        pend = h
+    got.append((pend.result(), pend.counters["agent_steps"]))
+    assert got == want
+    assert metric_fields_values(b.get_metrics()) == want[-1][0]
+    sa, sb = a._backend_impl.snapshot(), b._backend_impl.snapshot()
+    assert sa["rows"] == sb["rows"]
+    for k in ("o2", "drug"):
+        np.testing.assert_array_equal(sa["fields"][k], sb["fields"][k])
+
+    # a ticket whose slot a later queue reused is refused, not misread
+    be = b._backend_impl
+    import ctypes as C
+
+    tickets = []
+    for _ in range(_lib.READBACK_SLOTS + 1):
+        t = C.c_uint64()
+        assert be.lib.olc_queue_readback(be.handle, be._stream(), C.byref(t)) == _lib.OLC_OK
+        tickets.append(t.value)
+    c = _lib.OlcCounters()
+    assert be.lib.olc_take_readback(be.handle, tickets[0], None, 0, C.byref(c)) == _lib.OLC_ERR_STATE
+    assert be.lib.olc_take_readback(be.handle, tickets[-1], None, 0, C.byref(c)) == _lib.OLC_OK
+    assert c.status == 0 and c.agent_steps == want[-1][1]
+    a.close()
+    b.close()
+
+
+def metric_fields_values(m) -> dict:
+    return {k: int(getattr(m, k)) for k in metric_fields(type(m))}

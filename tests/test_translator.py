@@ -37,6 +37,8 @@ def test_tumour_models_compile():
     for cls in (W.TumourSim, W.TumourDrugSim):
         prog = _translate(cls, "radius")
         assert [k for k, _ in prog.kernels] == ["Kernel_CellRule_0", "Kernel_MetricRule_0"]
+        # a solo handle's metric rule adds into per-block shared words
+        assert f"#define OLC_SOLO_METRIC_WORDS {len(prog.layout.metrics)}\n" in prog.source and "olc_s_metrics[k] = 0u" in prog.source
         assert prog.sink_fields == {"o2"}
         _nvrtc_ok(prog)
 
@@ -205,6 +207,7 @@ def test_batched_translation_compiles():
         assert layout.cell_cols[layout.rng_col][0] == "_rng_state"
         prog = translate_model(sim, layout, radius)
         assert "typedef OlcSimView OlcP;" in prog.source
+        assert "OLC_SOLO_METRIC_WORDS" not in prog.source
         assert "olc_sim_view(P, sim)" in prog.source
         _nvrtc_ok(prog)
 
