@@ -65,7 +65,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--serve-seconds", type=float, default=15.0,
                     help="seconds of arrivals of the serving run added to the default line")
     ap.add_argument("--storages", default="bf16_sr,f16_sr", help="field storages of --workload precision")
-    ap.add_argument("--workload-base", default="scale", help="the workload --workload precision runs")
+    ap.add_argument("--workload-base", default="scale",
+                    help="the workload --workload precision runs; batch:K[,K...] = members K of the batched sweep")
     ap.add_argument("--error-steps", type=int, default=10,
                     help="steps of the field-error measurement added to the default line")
     ap.add_argument("--encoding", default="auto", choices=["auto", "value", "deficit", "offset3"],
@@ -609,6 +610,14 @@ def summarise(line: dict) -> dict:
         out["recorded_rel_l2_after_1000_steps"] = {st: {f: e["rel_l2"] for f, e in r.items()} for st, r in pr.items()}
         out["recorded_batched_500_steps_vs_plain_fp32"] = {
             k: v["vs_plain_fp32"] for k, v in rec["batched_sweep_500_steps"]["batched"].items()}
+        mem = rec.get("batched_members_field_error_500_steps")
+        if mem:
+            # worst relative L2 over the checked sweep members, per storage (values stored)
+            worst = {}
+            for m in mem["by_member"].values():
+                for st, r in m["rel_l2"].items():
+                    worst[st] = max(worst.get(st, 0.0), *r.values())
+            out["recorded_sweep_members_worst_rel_l2_500_steps_values"] = worst
     return out
 
 
@@ -751,20 +760,31 @@ def run_precision_workload(args) -> None:
     torch.cuda.set_device(local)
     from oncolytica_b200 import workloads as W
 
-    base = W.CONFIGS[args.workload_base]
-    # room for the population of a long run (unchecked growth doubles it about
-    # every 140 steps until O2 runs short)
-    spec = replace(base, seed=base.seed + rank, capacity=32 * base.n_agents)
     storages = tuple(s for s in args.storages.split(",") if s)
     cps = tuple(sorted({max(1, args.steps * k // 4) for k in (1, 2, 3)}))
-    r = measure_field_error(spec, storages, args.steps, checkpoints=cps)
-    worst = max(e["rel_l2"] for st in r["final"].values() for e in st.values())
+    if args.workload_base.startswith("batch:"):
+        # members of the batched sweep (each reproduces its batched run bit for
+        # bit), with the batched run's capacity for this many steps
+        members = W.batched_specs(args.sims, steps=args.steps)
+        specs = [members[int(k)] for k in args.workload_base[len("batch:"):].split(",") if k]
+    else:
+        base = W.CONFIGS[args.workload_base]
+        # room for the population of a long run (unchecked growth doubles it
+        # about every 140 steps until O2 runs short)
+        specs = [replace(base, seed=base.seed + rank, capacity=32 * base.n_agents)]
+    if args.encoding != "auto":
+        specs = [replace(sp, encoding=args.encoding) for sp in specs]
+    runs = [measure_field_error(sp, storages, args.steps, checkpoints=cps) for sp in specs]
+    r = runs[0] if len(runs) == 1 else {"members": runs}
+    spec = specs[0]
+    worst = max(e["rel_l2"] for run in runs for st in run["final"].values() for e in st.values())
     line = {"metric": METRIC, "value": worst, "unit": "relative L2 field error vs FP64 (worst field and storage)",
             "n_gpus": world, "steps": args.steps, "warmup": 0, "ms_per_step": None, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "/".join(storages) + " fields, f32 update",
             "data": "synthetic (numpy default_rng, seed 0 + rank)",
-            "config": {"workload": f"{spec.name} with 16-bit fields (field error against FP64)",
-                       "field_dims": list(spec.field_dims), "storages": list(storages)},
+            "config": {"workload": ", ".join(sp.name for sp in specs) + " with 16-bit fields (field error against FP64)",
+                       "field_dims": [list(sp.field_dims) for sp in specs] if len(specs) > 1 else list(spec.field_dims),
+                       "storages": list(storages), "encoding": args.encoding},
             "precision": r}
     if rank == 0:
         print(json.dumps(line), flush=True)
