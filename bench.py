@@ -751,6 +751,28 @@ def measure_field_error(spec, storages: tuple, steps: int, checkpoints: tuple = 
     return out
 
 
+def precision_specs(workload_base: str, steps: int, sims: int = 512, encoding: str = "auto", rank: int = 0) -> list:
+    """The workloads of --workload precision: a named configuration, or with
+    ``batch:K[,K...]`` members K of the batched sweep (each reproduces its
+    batched run bit for bit) with the batched run's capacity for ``steps``
+    steps; ``encoding`` other than "auto" overrides the element encoding."""
+    from oncolytica_b200 import workloads as W
+
+    if workload_base.startswith("batch:"):
+        members = W.batched_specs(sims, steps=steps)
+        specs = [members[int(k)] for k in workload_base[len("batch:"):].split(",") if k]
+        if not specs:
+            raise ValueError("--workload-base batch: names no member")
+    else:
+        base = W.CONFIGS[workload_base]
+        # room for the population of a long run (unchecked growth doubles it
+        # about every 140 steps until O2 runs short)
+        specs = [replace(base, seed=base.seed + rank, capacity=32 * base.n_agents)]
+    if encoding != "auto":
+        specs = [replace(sp, encoding=encoding) for sp in specs]
+    return specs
+
+
 def run_precision_workload(args) -> None:
     """Field error of the scale workload with 16-bit fields against FP64
     (``--storages``, ``--steps`` steps; checkpoints every quarter)."""
@@ -758,22 +780,9 @@ def run_precision_workload(args) -> None:
 
     rank, world, local = env_ranks()
     torch.cuda.set_device(local)
-    from oncolytica_b200 import workloads as W
-
     storages = tuple(s for s in args.storages.split(",") if s)
     cps = tuple(sorted({max(1, args.steps * k // 4) for k in (1, 2, 3)}))
-    if args.workload_base.startswith("batch:"):
-        # members of the batched sweep (each reproduces its batched run bit for
-        # bit), with the batched run's capacity for this many steps
-        members = W.batched_specs(args.sims, steps=args.steps)
-        specs = [members[int(k)] for k in args.workload_base[len("batch:"):].split(",") if k]
-    else:
-        base = W.CONFIGS[args.workload_base]
-        # room for the population of a long run (unchecked growth doubles it
-        # about every 140 steps until O2 runs short)
-        specs = [replace(base, seed=base.seed + rank, capacity=32 * base.n_agents)]
-    if args.encoding != "auto":
-        specs = [replace(sp, encoding=args.encoding) for sp in specs]
+    specs = precision_specs(args.workload_base, args.steps, args.sims, args.encoding, rank)
     runs = [measure_field_error(sp, storages, args.steps, checkpoints=cps) for sp in specs]
     r = runs[0] if len(runs) == 1 else {"members": runs}
     spec = specs[0]
