@@ -17,7 +17,6 @@ import numpy as np
 
 from oncolytica_b200 import _lib
 from oncolytica_b200._errors import CompilationError
-from oncolytica_b200._types import metric_fields
 from oncolytica_b200.compiler.emit_cuda import make_layout, pack_params, translate_model
 from oncolytica_b200.engine import STORAGE_CODES
 from oncolytica_b200 import _fieldcodec
