@@ -27,10 +27,9 @@ import hashlib
 import inspect
 import math
 import textwrap
-import types
 import typing
 from dataclasses import dataclass, field
-from typing import Any, Optional
+from typing import Any
 
 import numpy as np
 

@@ -27,7 +27,6 @@ from __future__ import annotations
 
 import collections
 import ctypes as C
-import math
 import time
 from dataclasses import dataclass, field
 from typing import Any, Callable, Iterable, Sequence
